@@ -1,0 +1,158 @@
+// ORACLE (test infrastructure only): extern "C" entry points over orc_core.hpp for the Python tests
+// and bench.py's CPU-baseline leg.  Nothing in desert-search_b200/ links this library.
+#include "orc_core.hpp"
+#include <atomic>
+#include <cstring>
+#include <mutex>
+#include <thread>
+
+using namespace orc;
+
+extern "C" {
+struct OrcArea { uint64_t cells, sampled; int32_t minx, maxx, minz, maxz, edge, border; };
+
+int orc_phase(const uint64_t *seeds, int n, double *out, double *fy) {
+    for (int i = 0; i < n; i++) out[i] = phase(seeds[i], fy ? fy + 2 * i : nullptr);
+    return 0;
+}
+void orc_gate_taps(int R, float sig, float *k) { gate_taps(R, sig, k); }
+
+// Per-seed side amplitudes of the pre-gate (and of the full gate if want_full), multithreaded.
+int orc_gate(const uint64_t *seeds, int n, int want_full, const float *k9, const float *k15, float *pre, float *full, int threads) {
+    std::atomic<int> next(0);
+    auto work = [&] {
+        for (int i; (i = next++) < n;) {
+            const GateResult g = gate_eval(seeds[i], want_full != 0, k9, k15);
+            pre[2 * i] = g.pre[0]; pre[2 * i + 1] = g.pre[1];
+            if (want_full) { full[2 * i] = g.full[0]; full[2 * i + 1] = g.full[1]; }
+        }
+    };
+    std::vector<std::thread> pool;
+    for (int t = 1; t < std::max(1, threads); t++) pool.emplace_back(work);
+    work();
+    for (auto &t : pool) t.join();
+    return 0;
+}
+
+// The whole seed gate over seeds fmix(start + k), k < count: phase <= maxph, pre-gate amp >= pthr,
+// full amp >= amp.  Survivors (unordered across threads; the caller sorts) go to out_seed/out_amp.
+// counts = {seeds, phase-passed, pre-passed, full-passed}.
+int orc_gate_range(uint64_t start, uint64_t count, double maxph, float pthr, float amp, int threads,
+                   uint64_t *out_seed, float *out_amp, int cap, uint64_t *counts) {
+    std::atomic<uint64_t> next(0), n1(0), n2(0), n3(0);
+    std::mutex mu;
+    float k9[9], k15[15];
+    gate_taps(4, 1.0f, k9); gate_taps(7, 2.0f, k15);
+    auto work = [&] {
+        for (;;) {
+            const uint64_t k0 = next.fetch_add(256);
+            if (k0 >= count) break;
+            const uint64_t k1 = std::min(count, k0 + 256);
+            for (uint64_t k = k0; k < k1; k++) {
+                const uint64_t seed = fmix(start + k);
+                if (phase(seed) > maxph) continue;
+                n1++;
+                float pa = 0;
+                GateOctave p[2];
+                for (int s = 0; s < 2; s++) { p[s] = gate_octave(seed, s); pa += pregate_side(p[s], k9); }
+                if (!(pa >= pthr)) continue;
+                n2++;
+                float fa = 0;
+                for (int s = 0; s < 2; s++) fa += fullgate_side(p[s], k15);
+                if (!(fa >= amp)) continue;
+                const uint64_t i = n3++;
+                if (i < uint64_t(cap)) { std::lock_guard<std::mutex> l(mu); out_seed[i] = seed; out_amp[i] = fa; }
+            }
+        }
+    };
+    std::vector<std::thread> pool;
+    for (int t = 1; t < std::max(1, threads); t++) pool.emplace_back(work);
+    work();
+    for (auto &t : pool) t.join();
+    counts[0] = count; counts[1] = n1; counts[2] = n2; counts[3] = n3;
+    return 0;
+}
+
+// Climate noise channel `ch` of a seed at (x, y, z) triples.
+int orc_noise(uint64_t seed, int ch, const double *xyz, int n, double *out) {
+    const Seed S(seed);
+    for (int i = 0; i < n; i++) out[i] = S.nz[ch].sample(xyz[3 * i], xyz[3 * i + 1], xyz[3 * i + 2]);
+    return 0;
+}
+// pred: 0 bridged desert state, 1 unbridged desert (exact depth), 2 hot (T >= 0.55), 3 proxy prob (x1000)
+int orc_points(uint64_t seed, int pred, const int32_t *xz, int n, int32_t *out, int threads) {
+    const Seed S(seed);
+    std::atomic<int> next(0);
+    auto work = [&] {
+        for (int i; (i = next++) < n;) {
+            const int x = xz[2 * i], z = xz[2 * i + 1];
+            out[i] = pred == 0 ? S.desert_state(x, z) : pred == 1 ? S.desert_state_plain(x, z) : pred == 2 ? S.hot(x, z)
+                   : int32_t(std::lround(S.proxy_prob(x, z) * 1000.f));
+        }
+    };
+    std::vector<std::thread> pool;
+    for (int t = 1; t < std::max(1, threads); t++) pool.emplace_back(work);
+    work();
+    for (auto &t : pool) t.join();
+    return 0;
+}
+int orc_climate(uint64_t seed, const int32_t *xz, int n, int64_t *q) {
+    const Seed S(seed);
+    for (int i = 0; i < n; i++) S.climate(xz[2 * i], xz[2 * i + 1], q + 6 * i);
+    return 0;
+}
+int orc_biome(const int64_t *q, int n, int32_t *tree_biome, int32_t *grid_biome) {
+    for (int i = 0; i < n; i++) {
+        tree_biome[i] = classify(q + 6 * i);
+        grid_biome[i] = surface().lookup(q + 6 * i);
+    }
+    return 0;
+}
+// pred: 0 bridged desert state, 2 hot (T >= 0.55), 4 proxy passable at pcut
+int orc_flood(uint64_t seed, int qx, int qz, int step, int half, int conn8, int pred, float pcut, OrcArea *out) {
+    const Seed S(seed);
+    Area a;
+    if (pred == 0) a = flood([&](int x, int z) { return S.desert_state(x, z); }, qx, qz, step, half, conn8 != 0);
+    else if (pred == 2) a = flood([&](int x, int z) { return S.hot(x, z); }, qx, qz, step, half, conn8 != 0);
+    else if (pred == 4) a = flood([&](int x, int z) { return S.proxy_prob(x, z) >= pcut ? 2 : 0; }, qx, qz, step, half, conn8 != 0);
+    else return -1;
+    *out = {a.cells, a.sampled, a.minx, a.maxx, a.minz, a.maxz, a.edge, a.border};
+    return 0;
+}
+int orc_tabins(uint64_t seed, TabIn *out) { seed_tabins(Seed(seed), out); return 0; }
+void orc_blur_taps(double sigma, float *k, int *r) { const BlurTaps b = blur_taps(sigma); std::copy(b.k.begin(), b.k.end(), k); *r = b.r; }
+// Six blurred period tables {TA, TB, CA, CB, EA, EB} (6 * 512 * 512 floats) and maxta/maxtb.
+int orc_tables(uint64_t seed, double sigma, double sigmac, float *out, float *mx) {
+    TabIn t[6]; seed_tabins(Seed(seed), t);
+    const BlurTaps bt = blur_taps(sigma), bc = blur_taps(sigmac);
+    for (int k = 0; k < 6; k++) { tabulate(t[k], out + size_t(k) * TN * TN); blur(out + size_t(k) * TN * TN, k < 2 ? bt : bc); }
+    for (int s = 0; s < 2; s++) mx[s] = *std::max_element(out + size_t(s) * TN * TN, out + size_t(s + 1) * TN * TN);
+    return 0;
+}
+int orc_tmap(double lat, int16_t *ib, int8_t *lo, int8_t *hi) {
+    const TMap m = tmap(lat);
+    std::memcpy(ib, m.ib, sizeof m.ib); std::memcpy(lo, m.lo, TN); std::memcpy(hi, m.hi, TN);
+    return 0;
+}
+// Raw scan candidates of one seed from its blurred tables; returns the full count (may exceed cap).
+int orc_scan(const float *tabs, float ta, float tt, float wc, float we, Cand *out, int cap) {
+    static const TMap mt = tmap(1024.0), mc = tmap(512.0);
+    std::vector<Cand> v;
+    scan(tabs, mt, mc, ta, tt, wc, we, v);
+    std::copy_n(v.begin(), std::min<size_t>(v.size(), size_t(cap)), out);
+    return int(v.size());
+}
+// Proxy bitmap of a zone: cell (ci, cj) at quart (x0 + 32 ci, z0 + 32 cj), row-major with z outer.
+int orc_proxy_zone(uint64_t seed, int x0, int z0, int nx, int nz, float pcut, uint8_t *out, int threads) {
+    const Seed S(seed);
+    std::atomic<int> next(0);
+    auto work = [&] {
+        for (int c; (c = next++) < nx * nz;) out[c] = S.proxy_prob(x0 + 32 * (c % nx), z0 + 32 * (c / nx)) >= pcut;
+    };
+    std::vector<std::thread> pool;
+    for (int t = 1; t < std::max(1, threads); t++) pool.emplace_back(work);
+    work();
+    for (auto &t : pool) t.join();
+    return 0;
+}
+}

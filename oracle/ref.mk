@@ -1,0 +1,30 @@
+# Builds the reference's own code from its sources where they lie (REF, read-only) into oracle/_ref/.
+# Test infrastructure only: the outputs pin the oracle and serve as the timed CPU reference arm.
+# Flags follow the reference Makefile (-ffp-contract=off is what makes its sampler round like Java);
+# -march=x86-64-v3 (its `bundle` target's host flags) instead of -march=native so the binaries run on
+# any AVX2 host the build is copied to.
+REF      ?= /root/reference
+OUT      := oracle/_ref
+CXXFLAGS := -O3 -march=x86-64-v3 -ffp-contract=off -std=c++20 -pthread -I$(REF)/src
+NVCC     ?= nvcc
+GPUARCH  := -gencode arch=compute_100a,code=sm_100a
+
+REFHDR := $(wildcard $(REF)/src/*.hpp) $(REF)/src/dsearch_desert.cpp
+
+all: $(OUT)/dsearch_desert $(OUT)/dflood $(OUT)/libref_cpu.so $(OUT)/libref_gate.so $(OUT)/tgate
+
+$(OUT):
+	mkdir -p $@
+$(OUT)/dsearch_desert: $(REF)/src/dsearch_desert.cpp $(REFHDR) | $(OUT)
+	g++ $(CXXFLAGS) $< -o $@
+$(OUT)/dflood: $(REF)/tools/dflood.cpp $(REFHDR) | $(OUT)
+	g++ $(CXXFLAGS) $< -o $@
+$(OUT)/libref_cpu.so: oracle/ref/ref_cpu.cpp $(REFHDR) | $(OUT)
+	g++ $(CXXFLAGS) -fPIC -shared $< -o $@
+# The reference GPU gate for sm_100a (its Makefile uses -arch=native; the compute capability is the only change).
+$(OUT)/libref_gate.so: oracle/ref/ref_gate.cu $(REF)/src/gpu/gate.cuh $(REF)/src/gpu/tgate.cu | $(OUT)
+	$(NVCC) -O3 -std=c++20 $(GPUARCH) -I$(REF)/src -Xcompiler -fPIC -shared $< -o $@
+$(OUT)/tgate: $(REF)/src/gpu/tgate.cu $(REF)/src/gpu/gate.cuh | $(OUT)
+	$(NVCC) -O3 -std=c++20 $(GPUARCH) $< -o $@
+
+.PHONY: all
