@@ -11,7 +11,7 @@ GPUARCH  := -gencode arch=compute_100a,code=sm_100a
 # -fmad=false: every product kernel states its fused multiply-adds explicitly (__fmaf_rn / __fma_rn),
 # so results are fixed by the source, as the bit-exact contract with the CPU path requires.
 NVFLAGS  := -O3 -std=c++20 $(GPUARCH) -lineinfo -fmad=false -Xptxas -v -Xcompiler -fPIC -I$(PKG)/csrc -Iinclude
-HOSTFLAGS:= -O3 -march=x86-64-v3 -ffp-contract=off -std=c++20 -pthread -Iinclude -I$(PKG)/csrc
+HOSTFLAGS:= -I/usr/local/cuda/include -O3 -march=x86-64-v3 -ffp-contract=off -std=c++20 -pthread -Iinclude -I$(PKG)/csrc
 ORCFLAGS := -O3 -march=x86-64-v3 -ffp-contract=off -std=c++20 -pthread -fPIC
 
 CU_SRC   := $(wildcard $(PKG)/csrc/*.cu)
@@ -40,6 +40,9 @@ $(B)/orc_blob.o: $(B)/orc_blob.c
 	gcc -O1 -fPIC -c $< -o $@
 
 # ---- CUDA library (C ABI in include/dsgpu.h)
+# taps.cu alone keeps nvcc's default contraction: it evaluates expf exactly as the reference kernels do.
+$(B)/taps.o: $(PKG)/csrc/taps.cu $(CU_HDR) | $(B)
+	$(NVCC) $(filter-out -fmad=false,$(NVFLAGS)) -c $< -o $@ 2> $(B)/taps.ptxas.txt || (cat $(B)/taps.ptxas.txt; false)
 $(B)/%.o: $(PKG)/csrc/%.cu $(CU_HDR) | $(B)
 	$(NVCC) $(NVFLAGS) -c $< -o $@ 2> $(B)/$*.ptxas.txt || (cat $(B)/$*.ptxas.txt; false)
 $(B)/host_%.o: $(PKG)/csrc/%.cpp $(CU_HDR) | $(B)

@@ -1,0 +1,288 @@
+// Bridged biome floods (exact areas and the screening floods) on the device.
+//
+// Reference: src/dense_flood.hpp:52-86 (dense_flood_bridged), tools/dflood.cpp, the hot-zone floods of
+// src/dsearch_desert.cpp:326-366 and the step-8/step-4 exact floods of :498-523.  The reference runs a DFS
+// with an explicit stack over a dense (2*half+1)^2 byte window.  The result (cells, sampled, bbox, edge,
+// border) depends only on the set of cells the flood reaches, not on visit order: reached = the start plus
+// every cell adjacent to a reached passable cell; sampled = reached cells inside window and world.  So the
+// device runs a level-synchronous BFS instead, over any number of requests at once:
+//  * one kernel per BFS level; its input is the list of cells touched for the first time at the previous
+//    level (all requests mixed).  Each thread evaluates the FP64 predicate of one cell, counts it, and if it
+//    is passable touches its 4 (or 8) neighbours; first touches (atomicOr on the visited bit) form the next
+//    level's list (warp-aggregated appends).
+//  * visited state: 2 bits per cell (touched, passable) in 64x64-cell tiles of 1 KiB, allocated on first
+//    touch from a pre-zeroed pool through a per-request tile directory (atomicCAS; a thread that loses
+//    the race uses the winner's tile, so nothing ever waits).
+//  * list counters rotate through three slots so no level needs a host round trip; the host checks for
+//    completion every few levels through a per-level history array.
+#include "noise.cuh"
+#include <algorithm>
+#include <map>
+#include <mutex>
+#include <vector>
+
+namespace dsg {
+namespace flood {
+
+struct FloodCtl {                      // one request, as the level kernel sees it
+    int32_t qx, qz, step, half, n, tpr, conn8, pred;
+    float pcut; int32_t noise; int64_t dir_off;
+};
+struct FloodStat {
+    unsigned long long cells, sampled;
+    int32_t minx, maxx, minz, maxz, edge, border, overflow, pad;
+};
+static_assert(sizeof(FloodStat) == 48, "FloodStat layout");
+
+constexpr int kWorld = 7499996;
+constexpr int TILE = 64, TILE_WORDS = TILE * TILE * 2 / 32;     // 256 x 32-bit words per tile
+
+__device__ __forceinline__ uint32_t *tile_word(const FloodCtl &c, int32_t *__restrict__ dir, uint32_t *__restrict__ pool,
+                                               uint32_t pool_cap, uint32_t *__restrict__ pool_next, int i, int j, int &bit, bool &oom) {
+    const int64_t di = c.dir_off + int64_t(j >> 6) * c.tpr + (i >> 6);
+    int32_t d = __ldcg(&dir[di]);
+    if (d < 0) {
+        const uint32_t nt = atomicAdd(pool_next, 1u);
+        if (nt >= pool_cap) { oom = true; return nullptr; }
+        const int32_t old = atomicCAS(&dir[di], -1, int32_t(nt));
+        d = old == -1 ? int32_t(nt) : old;
+    }
+    bit = 2 * (i & 15);
+    return pool + size_t(d) * TILE_WORDS + (j & 63) * 4 + ((i & 63) >> 4);
+}
+
+__device__ __forceinline__ int eval_pred(const FloodCtl &c, const SeedNoise &S, const WorldDev &w, int x, int z) {
+    if (c.pred == DSG_PRED_DESERT) return desert_state(S, w, x, z);
+    if (c.pred == DSG_PRED_HOT) return hot_state(S, x, z);
+    return proxy_prob(S, w, x, z) >= c.pcut ? 2 : 0;
+}
+
+// Touch the start cell of every request (dense_flood.hpp:81): it is the first level's only cell.
+__global__ void k_flood_start(const FloodCtl *__restrict__ ctl, uint32_t nreq, FloodStat *__restrict__ st, int32_t *__restrict__ dir,
+                              uint32_t *__restrict__ pool, uint32_t pool_cap, uint32_t *__restrict__ pool_next,
+                              uint64_t *__restrict__ out, uint32_t *__restrict__ n_out, uint32_t *__restrict__ err) {
+    const uint32_t r = blockIdx.x * blockDim.x + threadIdx.x;
+    if (r >= nreq) return;
+    const FloodCtl c = ctl[r];
+    FloodStat &s = st[r];
+    s.cells = 0; s.sampled = 0; s.minx = s.maxx = c.qx; s.minz = s.maxz = c.qz; s.edge = s.border = s.overflow = 0;
+    int bit; bool oom = false;
+    uint32_t *wd = tile_word(c, dir, pool, pool_cap, pool_next, c.half, c.half, bit, oom);
+    if (oom) { s.overflow = 1; atomicOr(err, 1u); return; }
+    atomicOr(wd, 1u << bit);
+    if (c.qx < -kWorld || c.qx > kWorld || c.qz < -kWorld || c.qz > kWorld) { s.border = 1; return; }
+    const uint32_t k = atomicAdd(n_out, 1u);
+    out[k] = (uint64_t(r) << 32) | (uint64_t(c.half) << 16) | uint64_t(c.half);
+}
+
+__global__ void __launch_bounds__(128) k_flood_level(const FloodCtl *__restrict__ ctl, FloodStat *__restrict__ st,
+        const SeedNoise *__restrict__ noise, WorldDev w, int32_t *__restrict__ dir, uint32_t *__restrict__ pool, uint32_t pool_cap,
+        uint32_t *__restrict__ pool_next, const uint64_t *__restrict__ in, const uint32_t *__restrict__ n_in_p,
+        uint64_t *__restrict__ out, uint32_t *__restrict__ n_out, uint32_t *__restrict__ n_zero, uint32_t cap,
+        uint32_t *__restrict__ hist, int level, uint32_t *__restrict__ err) {
+    const uint32_t n_in_raw = *n_in_p, n_in = min(n_in_raw, cap);
+    if (blockIdx.x == 0 && threadIdx.x == 0) { *n_zero = 0; hist[level] = n_in_raw; if (n_in_raw > cap) atomicOr(err, 2u); }
+    const int lane = threadIdx.x & 31;
+    const uint32_t stride = gridDim.x * blockDim.x;
+    for (uint32_t base = blockIdx.x * blockDim.x + (threadIdx.x & ~31u); base < n_in; base += stride) {
+        const uint32_t idx = base + lane;
+        bool pass = false;
+        uint32_t r = 0; int i = 0, j = 0;
+        FloodCtl c{};
+        if (idx < n_in) {
+            const uint64_t e = in[idx];
+            r = uint32_t(e >> 32); j = int((e >> 16) & 0xFFFF); i = int(e & 0xFFFF);
+            c = ctl[r];
+            const int x = c.qx + (i - c.half) * c.step, z = c.qz + (j - c.half) * c.step;
+            const int v = eval_pred(c, noise[c.noise], w, x, z);
+            FloodStat &s = st[r];
+            atomicAdd(&s.sampled, 1ull);
+            if (v) {
+                pass = true;
+                int bit; bool oom = false;
+                uint32_t *wd = tile_word(c, dir, pool, pool_cap, pool_next, i, j, bit, oom);
+                if (wd) atomicOr(wd, 2u << bit);
+                if (v == 2) {
+                    atomicAdd(&s.cells, 1ull);
+                    atomicMin(&s.minx, x); atomicMax(&s.maxx, x);
+                    atomicMin(&s.minz, z); atomicMax(&s.maxz, z);
+                }
+            }
+        }
+        // expand: 4 orthogonal neighbours, then the diagonals for 8-connected requests (dense_flood.hpp:82-83)
+        #pragma unroll 1
+        for (int dd = 0; dd < 8; dd++) {
+            bool add = false;
+            int ni = 0, nj = 0;
+            if (pass && (dd < 4 || c.conn8)) {
+                const int di = dd == 0 ? -1 : dd == 1 ? 1 : dd == 2 ? 0 : dd == 3 ? 0 : (dd & 1) ? 1 : -1;
+                const int dj = dd < 2 ? 0 : dd == 2 ? -1 : dd == 3 ? 1 : dd < 6 ? -1 : 1;
+                ni = i + di; nj = j + dj;
+                FloodStat &s = st[r];
+                if (ni < 0 || nj < 0 || ni >= c.n || nj >= c.n) s.edge = 1;
+                else {
+                    int bit; bool oom = false;
+                    uint32_t *wd = tile_word(c, dir, pool, pool_cap, pool_next, ni, nj, bit, oom);
+                    if (oom) { s.overflow = 1; atomicOr(err, 1u); }
+                    else if (!((atomicOr(wd, 1u << bit) >> bit) & 1u)) {
+                        const int x = c.qx + (ni - c.half) * c.step, z = c.qz + (nj - c.half) * c.step;
+                        if (x < -kWorld || x > kWorld || z < -kWorld || z > kWorld) s.border = 1;
+                        else add = true;
+                    }
+                }
+            }
+            const uint32_t m = __ballot_sync(0xffffffffu, add);
+            if (m) {
+                uint32_t at = 0;
+                if (lane == __ffs(m) - 1) at = atomicAdd(n_out, uint32_t(__popc(m)));
+                at = __shfl_sync(0xffffffffu, at, __ffs(m) - 1);
+                if (add) {
+                    const uint32_t k = at + __popc(m & ((1u << lane) - 1));
+                    if (k < cap) out[k] = (uint64_t(r) << 32) | (uint64_t(nj) << 16) | uint64_t(ni);
+                }
+            }
+        }
+    }
+}
+
+// ---------------------------------------------------------------- host engine
+struct Engine {
+    std::mutex mu;
+    bool ready = false;
+    cudaStream_t st = nullptr;
+    uint32_t list_cap = 0;
+    uint64_t *d_list[2] = {nullptr, nullptr};
+    uint32_t *d_cnt = nullptr;                 // [0..2] rotating list counters, [3] pool_next, [4] error flags
+    uint32_t *d_hist = nullptr; uint32_t hist_cap = 0;
+    uint32_t *h_hist = nullptr;
+    uint32_t *d_pool = nullptr; uint32_t pool_cap = 0;
+    int32_t *d_dir = nullptr; size_t dir_cap = 0;
+    FloodCtl *d_ctl = nullptr; uint32_t ctl_cap = 0;
+    FloodStat *d_stat = nullptr; uint32_t stat_cap = 0;
+    SeedNoise *d_noise = nullptr; uint32_t noise_cap = 0;
+    uint64_t *d_seeds = nullptr; uint32_t seeds_cap = 0;
+    int grid = 0;
+};
+Engine &E() { static Engine e; return e; }
+
+void setup_locked(Engine &g) {
+    if (g.ready) return;
+    require_init();
+    int lo, hi;
+    DSG_CU(cudaDeviceGetStreamPriorityRange(&lo, &hi));
+    DSG_CU(cudaStreamCreateWithPriority(&g.st, cudaStreamNonBlocking, hi));
+    int occ = 0;
+    DSG_CU(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_flood_level, 128, 0));
+    g.grid = std::max(1, occ) * device_info().sms;
+    g.list_cap = 1u << 25;
+    for (auto &l : g.d_list) DSG_CU(cudaMalloc(&l, size_t(g.list_cap) * 8));
+    DSG_CU(cudaMalloc(&g.d_cnt, 8 * 4));
+    g.hist_cap = 1u << 20;
+    DSG_CU(cudaMalloc(&g.d_hist, size_t(g.hist_cap) * 4));
+    DSG_CU(cudaMallocHost(&g.h_hist, 64 * 4));
+    g.ready = true;
+}
+template <class T> void grow(T *&p, uint32_t &cap, size_t need) {
+    if (need <= cap) return;
+    cudaFree(p); p = nullptr;
+    const size_t c = std::max<size_t>(need, size_t(cap) * 2);
+    DSG_CU(cudaMalloc(&p, c * sizeof(T)));
+    cap = uint32_t(c);
+}
+
+// Run a batch of requests to completion.  Returns DSG_OK, or DSG_OVERFLOW if the tile pool or a level list
+// ran out (the affected requests have overflow set and must be rerun with more memory).
+int run_batch(const dsg_flood_req *reqs, uint32_t n, dsg_area *out, size_t pool_bytes) {
+    Engine &g = E();
+    std::lock_guard<std::mutex> l(g.mu);
+    setup_locked(g);
+    // distinct seeds -> noise tables
+    std::map<uint64_t, int32_t> slot;
+    std::vector<uint64_t> seeds;
+    std::vector<FloodCtl> ctl(n);
+    size_t dir_total = 0;
+    for (uint32_t r = 0; r < n; r++) {
+        const dsg_flood_req &q = reqs[r];
+        DSG_ARG(q.step >= 1 && q.half >= 0 && q.half <= 32767, "dsg_flood: need step >= 1 and 0 <= half <= 32767");
+        DSG_ARG(q.pred == DSG_PRED_DESERT || q.pred == DSG_PRED_HOT || q.pred == DSG_PRED_PROXY, "dsg_flood: unknown predicate");
+        DSG_ARG(int64_t(q.half) * q.step < (int64_t(1) << 30), "dsg_flood: window too large");
+        auto it = slot.find(q.seed);
+        if (it == slot.end()) { it = slot.emplace(q.seed, int32_t(seeds.size())).first; seeds.push_back(q.seed); }
+        FloodCtl &c = ctl[r];
+        c.qx = q.qx; c.qz = q.qz; c.step = q.step; c.half = q.half; c.n = 2 * q.half + 1; c.tpr = (c.n + TILE - 1) / TILE;
+        c.conn8 = q.conn8 ? 1 : 0; c.pred = q.pred; c.pcut = q.pcut; c.noise = it->second; c.dir_off = int64_t(dir_total);
+        dir_total += size_t(c.tpr) * c.tpr;
+    }
+    grow(g.d_ctl, g.ctl_cap, n);
+    grow(g.d_stat, g.stat_cap, n);
+    grow(g.d_noise, g.noise_cap, seeds.size());
+    grow(g.d_seeds, g.seeds_cap, seeds.size());
+    if (dir_total > g.dir_cap) {
+        cudaFree(g.d_dir); g.d_dir = nullptr;
+        DSG_CU(cudaMalloc(&g.d_dir, dir_total * 4));
+        g.dir_cap = dir_total;
+    }
+    const uint32_t want_pool = uint32_t(std::min<size_t>(pool_bytes / (TILE_WORDS * 4), 0x7fffffff));
+    if (want_pool > g.pool_cap) {                      // the pool is kept zeroed between batches
+        cudaFree(g.d_pool); g.d_pool = nullptr;
+        DSG_CU(cudaMalloc(&g.d_pool, size_t(want_pool) * TILE_WORDS * 4));
+        DSG_CU(cudaMemset(g.d_pool, 0, size_t(want_pool) * TILE_WORDS * 4));
+        g.pool_cap = want_pool;
+    }
+    cudaStream_t st = g.st;
+    DSG_CU(cudaMemcpyAsync(g.d_seeds, seeds.data(), seeds.size() * 8, cudaMemcpyHostToDevice, st));
+    seed_noise_build(g.d_seeds, uint32_t(seeds.size()), g.d_noise, st);
+    DSG_CU(cudaMemcpyAsync(g.d_ctl, ctl.data(), size_t(n) * sizeof(FloodCtl), cudaMemcpyHostToDevice, st));
+    DSG_CU(cudaMemsetAsync(g.d_dir, 0xFF, dir_total * 4, st));
+    DSG_CU(cudaMemsetAsync(g.d_cnt, 0, 8 * 4, st));
+    k_flood_start<<<(n + 127) / 128, 128, 0, st>>>(g.d_ctl, n, g.d_stat, g.d_dir, g.d_pool, g.pool_cap, g.d_cnt + 3, g.d_list[0], g.d_cnt + 0, g.d_cnt + 4);
+    DSG_CU(cudaGetLastError());
+    const WorldDev w = world_dev();
+    const int K = 8;                                   // levels enqueued between completion checks
+    int level = 0;
+    for (;;) {
+        for (int k = 0; k < K; k++, level++) {
+            DSG_ARG(uint32_t(level) < g.hist_cap, "dsg_flood: BFS deeper than the level history");
+            k_flood_level<<<g.grid, 128, 0, st>>>(g.d_ctl, g.d_stat, g.d_noise, w, g.d_dir, g.d_pool, g.pool_cap, g.d_cnt + 3,
+                                                  g.d_list[level & 1], g.d_cnt + (level % 3), g.d_list[(level + 1) & 1],
+                                                  g.d_cnt + ((level + 1) % 3), g.d_cnt + ((level + 2) % 3), g.list_cap, g.d_hist, level, g.d_cnt + 4);
+        }
+        DSG_CU(cudaGetLastError());
+        DSG_CU(cudaMemcpyAsync(g.h_hist, g.d_hist + (level - K), K * 4, cudaMemcpyDeviceToHost, st));
+        DSG_CU(cudaStreamSynchronize(st));
+        if (g.h_hist[K - 1] == 0) break;
+    }
+    std::vector<FloodStat> hs(n);
+    uint32_t flags[8];
+    DSG_CU(cudaMemcpyAsync(hs.data(), g.d_stat, size_t(n) * sizeof(FloodStat), cudaMemcpyDeviceToHost, st));
+    DSG_CU(cudaMemcpyAsync(flags, g.d_cnt, 8 * 4, cudaMemcpyDeviceToHost, st));
+    DSG_CU(cudaStreamSynchronize(st));
+    // return the tiles this batch used to the zeroed state
+    DSG_CU(cudaMemsetAsync(g.d_pool, 0, size_t(std::min(flags[3], g.pool_cap)) * TILE_WORDS * 4, st));
+    for (uint32_t r = 0; r < n; r++) {
+        const FloodStat &s = hs[r];
+        out[r].cells = s.cells; out[r].sampled = s.sampled;
+        out[r].minx = s.minx; out[r].maxx = s.maxx; out[r].minz = s.minz; out[r].maxz = s.maxz;
+        out[r].edge = s.edge; out[r].border = s.border;
+    }
+    if (flags[4]) {
+        set_error("dsg_flood: %s exhausted (pool %u tiles, list %u entries)", (flags[4] & 1) ? "tile pool" : "level list", g.pool_cap, g.list_cap);
+        return DSG_OVERFLOW;
+    }
+    return DSG_OK;
+}
+}  // namespace flood
+}  // namespace dsg
+
+extern "C" int dsg_flood_batch(const dsg_flood_req *reqs, uint32_t n, dsg_area *out) {
+    return dsg::guarded([&] {
+        DSG_ARG(n == 0 || (reqs && out), "dsg_flood_batch: null pointer");
+        if (!n) return DSG_OK;
+        size_t free_b = 0, total_b = 0;
+        DSG_CU(cudaMemGetInfo(&free_b, &total_b));
+        // tile pool: a quarter of free memory, at most 16 GiB
+        const size_t pool = std::min<size_t>(free_b / 4, size_t(16) << 30);
+        return dsg::flood::run_batch(reqs, n, out, pool);
+    });
+}
+extern "C" int dsg_flood(const dsg_flood_req *req, dsg_area *out) { return dsg_flood_batch(req, 1, out); }

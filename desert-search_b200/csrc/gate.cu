@@ -1,0 +1,568 @@
+// Seed gate (stage S0) for sm_100a: y-phase filter -> anti-aliased 256^2 amplitude pre-gate -> full 512^2
+// amplitude gate.  Restates src/gpu/gate.cuh (k_phase, k_init, k_amp2) with the same per-cell arithmetic
+// (summation orders, fused multiply-adds of the blur chains, device expf taps), so amplitudes match the
+// reference's GPU gate bit for bit, on a different schedule:
+//  * pre-gate: one CTA per (seed, side) pair inside a 2-CTA cluster; each warp owns a 64-row band of its
+//    side's 256^2 grid and streams it with all state in registers (a lane holds 8 columns: hashes, samples,
+//    the horizontal blur through lane shuffles, and the vertical blur as 8 pending FMA chains per column).
+//    No block barrier inside a side; the two side maxima meet through distributed shared memory.
+//  * full gate: one 512-thread CTA per (seed, side) in a 2-CTA cluster, thread = column, row blocks of 8
+//    staged in shared memory; the vertical blur again accumulates in registers.
+//  * the whole batch (phase -> init -> pre-gate -> full gate) runs from device-side counts: no host sync
+//    between stages, so a batch can be captured in a CUDA graph.
+#include "common.cuh"
+#include <cooperative_groups.h>
+#include <algorithm>
+#include <mutex>
+#include <vector>
+
+namespace cg = cooperative_groups;
+
+namespace dsg {
+namespace gate {
+
+// Temperature octave -10 of one side, as the gate needs it (PerlinParams, gate.cuh:49).
+struct __align__(16) Oct { uint8_t perm[256]; double ox, oz, fy, vy; int32_t iy, pad[3]; };
+static_assert(sizeof(Oct) == 304, "Oct layout");
+
+// Blur taps and normalisers, passed by value (they live in the kernel-parameter constant bank).
+struct Taps { float k9[9], k15[15], norm9, norm15, w; };
+
+constexpr int PG_THREADS = 128, PG_BAND = 64;        // pre-gate: 4 warps x 64 rows = 256 rows per side
+constexpr int FG_THREADS = 512, FG_RB = 8;           // full gate: thread per column, 8-row blocks
+
+// ---------------------------------------------------------------- device math
+// fade as the reference's GPU gate evaluates it: nvcc contracts t*6-15 and t*(..)+10 (gate.cuh:51).
+__device__ __forceinline__ double fade_fused(double t) { return t * t * t * __fma_rn(t, __fma_rn(t, 6.0, -15.0), 10.0); }
+// Minecraft's 16 gradients: two of (x, y, z) with signs; equal to gx*x + gy*y + gz*z for every nonzero value.
+__device__ __forceinline__ double gradd(int h, double x, double y, double z) {
+    h &= 15;
+    const double u = h < 8 ? x : y;
+    const double v = h < 4 ? y : ((h == 12 || h == 14) ? x : z);
+    return ((h & 1) ? -u : u) + ((h & 2) ? -v : v);
+}
+__device__ __forceinline__ double phase_of(uint64_t seed, double *fy = nullptr) {
+    Xoro w = Xoro::seeded(seed);
+    const uint64_t a = w.next(), b = w.next();
+    Xoro c{a ^ kTempA, b ^ kTempB};
+    double s = 0;
+    #pragma unroll
+    for (int side = 0; side < 2; side++) {
+        const uint64_t fa = c.next(), fb = c.next();
+        Xoro r{fa ^ kSalt10A, fb ^ kSalt10B};
+        r.next();
+        const double y = r.uniform() * 256.;
+        const double f = y - floor(y);
+        if (fy) fy[side] = f;
+        s += fabs(f - .5);
+    }
+    return s;
+}
+
+// ---------------------------------------------------------------- kernels
+// y-phase filter over seed indices [start, start + count): warp-aggregated append of passing seeds.
+__global__ void __launch_bounds__(256) k_phase(uint64_t start, uint64_t count, double maxph, uint64_t *__restrict__ out,
+                                                uint32_t *__restrict__ nout, uint32_t cap) {
+    const int lane = threadIdx.x & 31;
+    const uint64_t stride = uint64_t(gridDim.x) * blockDim.x;
+    for (uint64_t base = uint64_t(blockIdx.x) * blockDim.x + (threadIdx.x & ~31u); base < count; base += stride) {
+        const uint64_t k = base + lane;
+        const uint64_t seed = fmix64(start + k);
+        const bool pass = k < count && phase_of(seed) <= maxph;
+        const uint32_t m = __ballot_sync(0xffffffffu, pass);
+        if (m) {
+            uint32_t at = 0;
+            if (lane == __ffs(m) - 1) at = atomicAdd(nout, uint32_t(__popc(m)));
+            at = __shfl_sync(0xffffffffu, at, __ffs(m) - 1);
+            if (pass) {
+                const uint32_t i = at + __popc(m & ((1u << lane) - 1));
+                if (i < cap) out[i] = seed;
+            }
+        }
+    }
+}
+__global__ void k_phase_list(const uint64_t *__restrict__ seeds, uint32_t n, double *__restrict__ ph, double *__restrict__ fy) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) { double f[2]; ph[i] = phase_of(seeds[i], f); fy[2 * i] = f[0]; fy[2 * i + 1] = f[1]; }
+}
+
+// Temperature octave -10 of both sides of every listed seed (gate.cuh:59-70, k_init).
+__global__ void __launch_bounds__(128) k_octinit(const uint64_t *__restrict__ seeds, const uint32_t *__restrict__ n_in, uint32_t cap,
+                                                  Oct *__restrict__ oct) {
+    const uint32_t n = min(*n_in, cap);
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < 2 * n; i += gridDim.x * blockDim.x) {
+        const uint64_t seed = seeds[i >> 1];
+        const int side = int(i & 1);
+        Xoro w = Xoro::seeded(seed);
+        const uint64_t a = w.next(), b = w.next();
+        Xoro c{a ^ kTempA, b ^ kTempB};
+        uint64_t fa = c.next(), fb = c.next();
+        if (side) { fa = c.next(); fb = c.next(); }
+        Xoro r{fa ^ kSalt10A, fb ^ kSalt10B};
+        const double ox = r.uniform() * 256, oy = r.uniform() * 256, oz = r.uniform() * 256;
+        __align__(16) uint8_t perm[256];
+        for (int k = 0; k < 256; k++) perm[k] = uint8_t(k);
+        for (int k = 0; k < 256; k++) { const int j = k + int(r.below(256 - k)); const uint8_t t = perm[k]; perm[k] = perm[j]; perm[j] = t; }
+        Oct &o = oct[i];
+        #pragma unroll
+        for (int k = 0; k < 16; k++) reinterpret_cast<uint4 *>(o.perm)[k] = reinterpret_cast<const uint4 *>(perm)[k];
+        const double fl = floor(oy);
+        o.ox = ox; o.oz = oz; o.fy = oy - fl; o.vy = fade_fused(oy - fl); o.iy = int(fl);
+    }
+}
+
+// Hashes x4 (byte offsets into a 16-float table group) of one grid row for the lane's 10 lattice columns.
+// cv[dy][k] packs col[dy][c_t] for t = 4k..4k+3; columns t = 8, 9 come from the next lane (periodic).
+__device__ __forceinline__ void hash_row(const uint8_t *__restrict__ sP2, const uint32_t (&cv)[2][2], int mz, int lane, uint32_t (&h)[2][3]) {
+    #pragma unroll
+    for (int dy = 0; dy < 2; dy++) {
+        #pragma unroll
+        for (int k = 0; k < 2; k++) {
+            uint32_t w = 0;
+            #pragma unroll
+            for (int b = 0; b < 4; b++) {
+                const uint32_t c = (cv[dy][k] >> (8 * b)) & 255u;
+                w |= uint32_t(sP2[c + mz] & 15) << (8 * b + 2);
+            }
+            h[dy][k] = w;
+        }
+        h[dy][2] = __shfl_sync(0xffffffffu, h[dy][0], (lane + 1) & 31);
+    }
+}
+__device__ __forceinline__ uint32_t hbyte(const uint32_t (&h)[3], int t) { return (h[t >> 2] >> (8 * (t & 3))) & 255u; }
+
+// Anti-aliased pre-gate (gate.cuh stream_max<256,4,8,true>).  Cluster rank = noise side.
+__global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(PG_THREADS, 4)
+k_pregate(const Oct *__restrict__ oct, const uint64_t *__restrict__ seeds, const uint32_t *__restrict__ n_in, uint32_t cap_in,
+          float thr, Taps tp, uint64_t *__restrict__ out_seed, uint32_t *__restrict__ out_idx, uint32_t *__restrict__ n_out,
+          uint32_t cap_out, float *__restrict__ side_amp) {
+    __shared__ __align__(16) float sTc[288];
+    __shared__ __align__(16) uint8_t sP2[512];
+    __shared__ __align__(16) uint8_t sCol[2][256];
+    __shared__ float sRed[PG_THREADS / 32];
+    __shared__ float sPeer[2];
+    cg::cluster_group cl = cg::this_cluster();
+    const int side = int(cl.block_rank());
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const uint32_t n = min(*n_in, cap_in), ncl = gridDim.x / 2;
+    int it = 0;
+    for (uint32_t s = blockIdx.x / 2; s < n; s += ncl, it++) {
+        const Oct &p = oct[2 * size_t(s) + side];
+        if (tid < 16) {
+            const uint4 v = reinterpret_cast<const uint4 *>(p.perm)[tid];
+            reinterpret_cast<uint4 *>(sP2)[tid] = v; reinterpret_cast<uint4 *>(sP2)[tid + 16] = v;
+        }
+        const double ox = p.ox, oz = p.oz, fy = p.fy, vy = p.vy;
+        const int iy = p.iy;
+        __syncthreads();
+        for (int c = tid; c < 256; c += PG_THREADS) {
+            const int pc = sP2[c];
+            sCol[0][c] = sP2[pc + (iy & 255)];
+            sCol[1][c] = sP2[pc + ((iy + 1) & 255)];
+        }
+        {   // 18 merged corner tables of 16 gradients: 4 half-lattice parities averaged (gate.cuh:218-235)
+            double fr[2][2]; int sh[2][2];
+            #pragma unroll
+            for (int ax = 0; ax < 2; ax++) {
+                const double o = ax ? oz : ox;
+                #pragma unroll
+                for (int q = 0; q < 2; q++) { const double b = o + 0.5 * q; fr[ax][q] = b - floor(b); sh[ax][q] = int(floor(b) - floor(o)); }
+            }
+            for (int e = tid; e < 288; e += PG_THREADS) {
+                const int h = e & 15, dy = (e >> 4) & 1, uv = e >> 5, u = uv / 3, v = uv % 3;
+                double acc = 0;
+                #pragma unroll
+                for (int px = 0; px < 2; px++)
+                    #pragma unroll
+                    for (int pz = 0; pz < 2; pz++) {
+                        const int dx = u - sh[0][px], dz = v - sh[1][pz];
+                        if (dx < 0 || dx > 1 || dz < 0 || dz > 1) continue;
+                        const double fx = fr[0][px], fz = fr[1][pz], tx = fade_fused(fx), tz = fade_fused(fz);
+                        const double wc = (dx ? tx : 1 - tx) * (dy ? vy : 1 - vy) * (dz ? tz : 1 - tz);
+                        acc = __fma_rn(wc, gradd(h, fx - dx, fy - dy, fz - dz), acc);
+                    }
+                sTc[e] = float(0.25 * double(tp.w) * acc);
+            }
+        }
+        __syncthreads();
+        const int ix0 = int(floor(ox)), iz0 = int(floor(oz));
+        uint32_t cv[2][2];
+        #pragma unroll
+        for (int dy = 0; dy < 2; dy++)
+            #pragma unroll
+            for (int k = 0; k < 2; k++) {
+                uint32_t w = 0;
+                #pragma unroll
+                for (int b = 0; b < 4; b++) w |= uint32_t(sCol[dy][(8 * lane + ix0 + 4 * k + b) & 255]) << (8 * b);
+                cv[dy][k] = w;
+            }
+        // ---- stream this warp's band: output rows [o0, o0 + 64) need sample rows o0-4 .. o0+67
+        const int o0 = warp * PG_BAND;
+        float best = -1e9f;
+        uint32_t hA[2][3], hB[2][3], hC[2][3];
+        hash_row(sP2, cv, (o0 - 4 + iz0) & 255, lane, hA);
+        hash_row(sP2, cv, (o0 - 3 + iz0) & 255, lane, hB);
+        float pend[8][8];
+        #pragma unroll
+        for (int j = 0; j < 8; j++)
+            #pragma unroll
+            for (int e = 0; e < 8; e++) pend[j][e] = 0.f;
+        const char *tcb = reinterpret_cast<const char *>(sTc);
+        for (int r = o0 - 4; r < o0 + PG_BAND + 4; r++) {
+            hash_row(sP2, cv, (r + 2 + iz0) & 255, lane, hC);
+            float S[8];
+            #pragma unroll
+            for (int e = 0; e < 8; e++) {
+                float acc = 0.f;
+                #pragma unroll
+                for (int v = 0; v < 3; v++)
+                    #pragma unroll
+                    for (int dy = 0; dy < 2; dy++)
+                        #pragma unroll
+                        for (int u = 0; u < 3; u++) {
+                            const uint32_t h4 = hbyte(v == 0 ? hA[dy] : v == 1 ? hB[dy] : hC[dy], e + u);
+                            acc = __fadd_rn(acc, *reinterpret_cast<const float *>(tcb + ((u * 3 + v) * 2 + dy) * 64 + h4));
+                        }
+                S[e] = acc;
+            }
+            // horizontal blur over columns i-4 .. i+4 (periodic in 256 = the warp's 32 lanes x 8)
+            float X[16];
+            #pragma unroll
+            for (int k = 0; k < 4; k++) {
+                X[k] = __shfl_sync(0xffffffffu, S[4 + k], (lane + 31) & 31);
+                X[12 + k] = __shfl_sync(0xffffffffu, S[k], (lane + 1) & 31);
+            }
+            #pragma unroll
+            for (int e = 0; e < 8; e++) X[4 + e] = S[e];
+            #pragma unroll
+            for (int e = 0; e < 8; e++) {
+                float hv = __fmaf_rn(tp.k9[0], X[e], 0.f);
+                #pragma unroll
+                for (int d = 1; d < 9; d++) hv = __fmaf_rn(tp.k9[d], X[e + d], hv);
+                // vertical blur: this row is tap 8-j of pending output r-4+j
+                const float done = __fmaf_rn(tp.k9[8], hv, pend[0][e]);
+                #pragma unroll
+                for (int j = 1; j < 8; j++) pend[j - 1][e] = __fmaf_rn(tp.k9[8 - j], hv, pend[j][e]);
+                pend[7][e] = __fmaf_rn(tp.k9[0], hv, 0.f);
+                if (r - 4 >= o0) best = fmaxf(best, __fmul_rn(done, tp.norm9));
+            }
+            #pragma unroll
+            for (int dy = 0; dy < 2; dy++)
+                #pragma unroll
+                for (int k = 0; k < 3; k++) { hA[dy][k] = hB[dy][k]; hB[dy][k] = hC[dy][k]; }
+        }
+        #pragma unroll
+        for (int o = 16; o > 0; o >>= 1) best = fmaxf(best, __shfl_xor_sync(0xffffffffu, best, o));
+        if (lane == 0) sRed[warp] = best;
+        __syncthreads();
+        float m = 0.f;
+        if (tid == 0) {
+            m = sRed[0];
+            #pragma unroll
+            for (int w = 1; w < PG_THREADS / 32; w++) m = fmaxf(m, sRed[w]);
+            if (side == 1) *cl.map_shared_rank(&sPeer[it & 1], 0) = m;
+        }
+        cl.sync();
+        if (side == 0 && tid == 0) {
+            const float mb = sPeer[it & 1];
+            const float amp = __fadd_rn(__fadd_rn(0.f, m), mb);
+            if (side_amp) { side_amp[2 * size_t(s)] = m; side_amp[2 * size_t(s) + 1] = mb; }
+            if (amp >= thr) {
+                const uint32_t i = atomicAdd(n_out, 1u);
+                if (i < cap_out) { out_seed[i] = seeds[s]; out_idx[i] = s; }
+            }
+        }
+    }
+}
+
+// Full gate (gate.cuh stream_max<512,7,8,false>).  Cluster rank = noise side; thread = grid column.
+__global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(FG_THREADS, 2)
+k_fullgate(const Oct *__restrict__ oct, const uint64_t *__restrict__ seeds, const uint32_t *__restrict__ idx, const uint32_t *__restrict__ n_in,
+           uint32_t cap_in, float thr, Taps tp, uint64_t *__restrict__ out_seed, float *__restrict__ out_amp, uint32_t *__restrict__ n_out,
+           uint32_t cap_out, float *__restrict__ side_amp) {
+    __shared__ __align__(16) float sTc[512];
+    __shared__ __align__(16) uint8_t sP2[512];
+    __shared__ __align__(16) uint8_t sCol[2][256];
+    __shared__ __align__(16) uint8_t sHk[FG_RB][4][256];
+    __shared__ __align__(16) float sV[FG_RB][512];
+    __shared__ float sRed[FG_THREADS / 32];
+    __shared__ float sPeer[2];
+    cg::cluster_group cl = cg::this_cluster();
+    const int side = int(cl.block_rank());
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const uint32_t n = min(*n_in, cap_in), ncl = gridDim.x / 2;
+    int it = 0;
+    for (uint32_t s = blockIdx.x / 2; s < n; s += ncl, it++) {
+        const uint32_t oi = idx ? idx[s] : s;
+        const Oct &p = oct[2 * size_t(oi) + side];
+        if (tid < 16) {
+            const uint4 v = reinterpret_cast<const uint4 *>(p.perm)[tid];
+            reinterpret_cast<uint4 *>(sP2)[tid] = v; reinterpret_cast<uint4 *>(sP2)[tid + 16] = v;
+        }
+        const double ox = p.ox, oz = p.oz, fy = p.fy, vy = p.vy;
+        const int iy = p.iy;
+        __syncthreads();
+        if (tid < 256) {
+            const int pc = sP2[tid];
+            sCol[0][tid] = sP2[pc + (iy & 255)];
+            sCol[1][tid] = sP2[pc + ((iy + 1) & 255)];
+        }
+        {   // corner tables per parity (gate.cuh:237-244): Tc[(px*2+pz)*128 + c*16 + h]
+            const int e = tid, par = e >> 7, c = (e >> 4) & 7, h = e & 15, px = par >> 1, pz = par & 1;
+            const double bx = px * 0.5 + ox, bz = pz * 0.5 + oz;
+            const double fx = bx - floor(bx), fz = bz - floor(bz), tx = fade_fused(fx), tz = fade_fused(fz);
+            const int dx = c & 1, dy = (c >> 1) & 1, dz = c >> 2;
+            const double wc = (dx ? tx : 1 - tx) * (dy ? vy : 1 - vy) * (dz ? tz : 1 - tz);
+            sTc[e] = float(1.0 * double(tp.w) * wc * gradd(h, fx - dx, fy - dy, fz - dz));
+        }
+        const int ix0a = int(floor(ox)), ix0b = int(floor(0.5 + ox)), iz0a = int(floor(oz)), iz0b = int(floor(0.5 + oz));
+        __syncthreads();
+        // per-thread constants: hash column c and its two col values (dz = tid>>8 fixed, dy = 0/1 alternate)
+        const int hc = tid & 255, hdz = tid >> 8;
+        const int col0 = sCol[0][hc], col1 = sCol[1][hc];
+        const int px = tid & 1, ixp = (tid >> 1) + (px ? ix0b : ix0a);
+        float pend[14];
+        #pragma unroll
+        for (int j = 0; j < 14; j++) pend[j] = 0.f;
+        float best = -1e9f;
+        for (int r0 = -7; r0 <= 518; r0 += FG_RB) {
+            // hashes of rows r0 .. r0+7: sHk[k][q][c], q = dy*2 + dz
+            #pragma unroll
+            for (int k = 0; k < FG_RB; k++) {
+                const int j = (r0 + k) & 511, pz = j & 1, iz = (j >> 1) + (pz ? iz0b : iz0a);
+                const int zz = (iz + hdz) & 255;
+                sHk[k][hdz][hc] = sP2[col0 + zz] & 15;            // q = 0*2 + hdz
+                sHk[k][2 + hdz][hc] = sP2[col1 + zz] & 15;        // q = 1*2 + hdz
+            }
+            __syncthreads();
+            #pragma unroll
+            for (int k = 0; k < FG_RB; k++) {
+                const int j = (r0 + k) & 511, pz = j & 1;
+                const float *T = sTc + (px * 2 + pz) * 128;
+                float acc = 0.f;
+                #pragma unroll
+                for (int c = 0; c < 8; c++) {
+                    const int dx = c & 1, q = ((c >> 1) & 1) * 2 + (c >> 2);
+                    acc = __fadd_rn(acc, T[c * 16 + sHk[k][q][(ixp + dx) & 255]]);
+                }
+                sV[k][tid] = acc;
+            }
+            __syncthreads();
+            #pragma unroll
+            for (int k = 0; k < FG_RB; k++) {
+                const int r = r0 + k;
+                if (r > 518) break;
+                float hv = __fmaf_rn(tp.k15[0], sV[k][(tid - 7) & 511], 0.f);
+                #pragma unroll
+                for (int d = 1; d < 15; d++) hv = __fmaf_rn(tp.k15[d], sV[k][(tid + d - 7) & 511], hv);
+                const float done = __fmaf_rn(tp.k15[14], hv, pend[0]);
+                #pragma unroll
+                for (int j = 1; j < 14; j++) pend[j - 1] = __fmaf_rn(tp.k15[14 - j], hv, pend[j]);
+                pend[13] = __fmaf_rn(tp.k15[0], hv, 0.f);
+                if (r >= 7) best = fmaxf(best, __fmul_rn(done, tp.norm15));
+            }
+            __syncthreads();
+        }
+        #pragma unroll
+        for (int o = 16; o > 0; o >>= 1) best = fmaxf(best, __shfl_xor_sync(0xffffffffu, best, o));
+        if (lane == 0) sRed[warp] = best;
+        __syncthreads();
+        float m = 0.f;
+        if (tid == 0) {
+            m = sRed[0];
+            #pragma unroll
+            for (int w = 1; w < FG_THREADS / 32; w++) m = fmaxf(m, sRed[w]);
+            if (side == 1) *cl.map_shared_rank(&sPeer[it & 1], 0) = m;
+        }
+        cl.sync();
+        if (side == 0 && tid == 0) {
+            const float mb = sPeer[it & 1];
+            const float amp = __fadd_rn(__fadd_rn(0.f, m), mb);
+            if (side_amp) { side_amp[2 * size_t(s)] = m; side_amp[2 * size_t(s) + 1] = mb; }
+            if (amp >= thr) {
+                const uint32_t i = atomicAdd(n_out, 1u);
+                if (i < cap_out) { out_seed[i] = seeds[s]; out_amp[i] = amp; }
+            }
+        }
+    }
+}
+
+__global__ void k_iota(uint32_t *a, uint32_t n) { const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; if (i < n) a[i] = i; }
+
+// ---------------------------------------------------------------- host side
+void gate_taps_device(float out[24]);                     // taps.cu
+
+struct State {
+    std::mutex mu;
+    bool ready = false;
+    Taps taps{};
+    float raw[24];
+    cudaStream_t st = nullptr;
+    // batch buffers
+    uint64_t cap_batch = 0;
+    uint32_t cap1 = 0, cap2 = 0, cap3 = 0;
+    uint64_t *d_s1 = nullptr, *d_s2 = nullptr, *d_s3 = nullptr;
+    uint32_t *d_idx2 = nullptr, *d_n = nullptr, *h_n = nullptr;
+    float *d_a3 = nullptr;
+    Oct *d_oct = nullptr;
+    uint64_t *h_s3 = nullptr; float *h_a3 = nullptr;
+    int pg_blocks = 0, fg_blocks = 0;
+};
+State &S() { static State s; return s; }
+
+void setup_locked(State &g) {
+    if (g.ready) return;
+    require_init();
+    gate_taps_device(g.raw);
+    Taps &t = g.taps;
+    float s9 = 0, s15 = 0;
+    for (int i = 0; i < 9; i++) { t.k9[i] = g.raw[i]; s9 += g.raw[i]; }
+    for (int i = 0; i < 15; i++) { t.k15[i] = g.raw[9 + i]; s15 += g.raw[9 + i]; }
+    t.norm9 = 1.f / (s9 * s9); t.norm15 = 1.f / (s15 * s15);
+    t.w = float(1.25 * (32.0 / 63.0) * 1.5);              // octave-0 temperature weight, final units (gate.cuh:47)
+    int lo, hi;
+    DSG_CU(cudaDeviceGetStreamPriorityRange(&lo, &hi));
+    DSG_CU(cudaStreamCreateWithPriority(&g.st, cudaStreamNonBlocking, lo));   // the gate yields to scan/proxy/flood
+    int occ = 0;
+    DSG_CU(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_pregate, PG_THREADS, 0));
+    g.pg_blocks = std::max(2, (occ * device_info().sms) & ~1);
+    DSG_CU(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_fullgate, FG_THREADS, 0));
+    g.fg_blocks = std::max(2, (occ * device_info().sms) & ~1);
+    g.ready = true;
+}
+void ensure_buffers(State &g, uint64_t batch) {
+    if (batch <= g.cap_batch) return;
+    cudaFree(g.d_s1); cudaFree(g.d_s2); cudaFree(g.d_s3); cudaFree(g.d_idx2); cudaFree(g.d_a3); cudaFree(g.d_oct); cudaFree(g.d_n);
+    cudaFreeHost(g.h_n); cudaFreeHost(g.h_s3); cudaFreeHost(g.h_a3);
+    // caps as run_gate (gate.cuh:364) scaled to the batch: 1/16 of the indices, 1/4 of those, 1/16 of those
+    g.cap1 = uint32_t(std::max<uint64_t>(1024, batch / 16));
+    g.cap2 = std::max<uint32_t>(1024, g.cap1 / 4);
+    g.cap3 = std::max<uint32_t>(1024, g.cap2 / 16);
+    DSG_CU(cudaMalloc(&g.d_s1, size_t(g.cap1) * 8));
+    DSG_CU(cudaMalloc(&g.d_oct, size_t(g.cap1) * 2 * sizeof(Oct)));
+    DSG_CU(cudaMalloc(&g.d_s2, size_t(g.cap2) * 8));
+    DSG_CU(cudaMalloc(&g.d_idx2, size_t(g.cap2) * 4));
+    DSG_CU(cudaMalloc(&g.d_s3, size_t(g.cap3) * 8));
+    DSG_CU(cudaMalloc(&g.d_a3, size_t(g.cap3) * 4));
+    DSG_CU(cudaMalloc(&g.d_n, 4 * 4));
+    DSG_CU(cudaMallocHost(&g.h_n, 4 * 4));
+    DSG_CU(cudaMallocHost(&g.h_s3, size_t(g.cap3) * 8));
+    DSG_CU(cudaMallocHost(&g.h_a3, size_t(g.cap3) * 4));
+    g.cap_batch = batch;
+}
+// Enqueue one batch on `st` (no host synchronisation).
+void enqueue_batch(State &g, cudaStream_t st, uint64_t start, uint64_t nb, const dsg_gate_cfg &c) {
+    DSG_CU(cudaMemsetAsync(g.d_n, 0, 16, st));
+    const unsigned pb = unsigned(std::min<uint64_t>((nb + 255) / 256, uint64_t(device_info().sms) * 64));
+    k_phase<<<pb, 256, 0, st>>>(start, nb, double(c.maxph), g.d_s1, g.d_n, g.cap1);
+    k_octinit<<<unsigned(device_info().sms) * 16, 128, 0, st>>>(g.d_s1, g.d_n, g.cap1, g.d_oct);
+    k_pregate<<<g.pg_blocks, PG_THREADS, 0, st>>>(g.d_oct, g.d_s1, g.d_n, g.cap1, c.pthr, g.taps, g.d_s2, g.d_idx2, g.d_n + 1, g.cap2, nullptr);
+    k_fullgate<<<g.fg_blocks, FG_THREADS, 0, st>>>(g.d_oct, g.d_s2, g.d_idx2, g.d_n + 1, g.cap2, c.amp, g.taps, g.d_s3, g.d_a3, g.d_n + 2, g.cap3, nullptr);
+    DSG_CU(cudaGetLastError());
+}
+}  // namespace gate
+}  // namespace dsg
+
+using namespace dsg;
+using namespace dsg::gate;
+
+extern "C" int dsg_gate_taps(float taps[24]) {
+    return guarded([&] {
+        State &g = S(); std::lock_guard<std::mutex> l(g.mu); setup_locked(g);
+        std::memcpy(taps, g.raw, sizeof g.raw);
+        return DSG_OK;
+    });
+}
+
+extern "C" int dsg_phase(const uint64_t *seeds, uint32_t n, double *phase, double *fy) {
+    return guarded([&] {
+        require_init();
+        DSG_ARG(seeds && phase && fy, "dsg_phase: null pointer");
+        if (!n) return DSG_OK;
+        uint64_t *d_s; double *d_p, *d_f;
+        DSG_CU(cudaMalloc(&d_s, size_t(n) * 8)); DSG_CU(cudaMalloc(&d_p, size_t(n) * 8)); DSG_CU(cudaMalloc(&d_f, size_t(n) * 16));
+        DSG_CU(cudaMemcpy(d_s, seeds, size_t(n) * 8, cudaMemcpyHostToDevice));
+        k_phase_list<<<(n + 255) / 256, 256>>>(d_s, n, d_p, d_f);
+        DSG_CU(cudaGetLastError());
+        DSG_CU(cudaMemcpy(phase, d_p, size_t(n) * 8, cudaMemcpyDeviceToHost));
+        DSG_CU(cudaMemcpy(fy, d_f, size_t(n) * 16, cudaMemcpyDeviceToHost));
+        cudaFree(d_s); cudaFree(d_p); cudaFree(d_f);
+        return DSG_OK;
+    });
+}
+
+extern "C" int dsg_gate_amps(const uint64_t *seeds, uint32_t n, float *pre, float *full) {
+    return guarded([&] {
+        DSG_ARG(seeds && pre && full, "dsg_gate_amps: null pointer");
+        State &g = S(); std::lock_guard<std::mutex> l(g.mu); setup_locked(g);
+        if (!n) return DSG_OK;
+        uint64_t *d_s, *d_o; uint32_t *d_n, *d_i; float *d_pre, *d_full, *d_a; Oct *d_oct;
+        DSG_CU(cudaMalloc(&d_s, size_t(n) * 8)); DSG_CU(cudaMalloc(&d_o, size_t(n) * 8)); DSG_CU(cudaMalloc(&d_i, size_t(n) * 4));
+        DSG_CU(cudaMalloc(&d_n, 16)); DSG_CU(cudaMalloc(&d_pre, size_t(n) * 8)); DSG_CU(cudaMalloc(&d_full, size_t(n) * 8));
+        DSG_CU(cudaMalloc(&d_a, size_t(n) * 4)); DSG_CU(cudaMalloc(&d_oct, size_t(n) * 2 * sizeof(Oct)));
+        DSG_CU(cudaMemcpy(d_s, seeds, size_t(n) * 8, cudaMemcpyHostToDevice));
+        const uint32_t hn[4] = {n, 0, n, 0};
+        DSG_CU(cudaMemcpy(d_n, hn, 16, cudaMemcpyHostToDevice));
+        k_octinit<<<(2 * n + 127) / 128, 128>>>(d_s, d_n, n, d_oct);
+        k_pregate<<<g.pg_blocks, PG_THREADS>>>(d_oct, d_s, d_n, n, -1e30f, g.taps, d_o, d_i, d_n + 1, n, d_pre);
+        k_fullgate<<<g.fg_blocks, FG_THREADS>>>(d_oct, d_s, nullptr, d_n + 2, n, -1e30f, g.taps, d_o, d_a, d_n + 3, n, d_full);
+        DSG_CU(cudaGetLastError());
+        DSG_CU(cudaMemcpy(pre, d_pre, size_t(n) * 8, cudaMemcpyDeviceToHost));
+        DSG_CU(cudaMemcpy(full, d_full, size_t(n) * 8, cudaMemcpyDeviceToHost));
+        cudaFree(d_s); cudaFree(d_o); cudaFree(d_i); cudaFree(d_n); cudaFree(d_pre); cudaFree(d_full); cudaFree(d_a); cudaFree(d_oct);
+        return DSG_OK;
+    });
+}
+
+extern "C" int dsg_gate_run(uint64_t start, uint64_t count, const dsg_gate_cfg *cfg, uint64_t *out_seed, float *out_amp, uint32_t cap,
+                            uint32_t *n_out, uint64_t counts[4]) {
+    return guarded([&] {
+        DSG_ARG(cfg && n_out, "dsg_gate_run: null pointer");
+        DSG_ARG(cap == 0 || (out_seed && out_amp), "dsg_gate_run: null output");
+        State &g = S(); std::lock_guard<std::mutex> l(g.mu); setup_locked(g);
+        const uint64_t B = cfg->batch ? cfg->batch : (1ull << 26);
+        ensure_buffers(g, B);
+        uint64_t tot[4] = {0, 0, 0, 0};
+        uint32_t written = 0;
+        bool overflow = false;
+        std::vector<std::pair<uint64_t, float>> found;
+        for (uint64_t base = 0; base < count; base += B) {
+            const uint64_t nb = std::min(B, count - base);
+            enqueue_batch(g, g.st, start + base, nb, *cfg);
+            DSG_CU(cudaMemcpyAsync(g.h_n, g.d_n, 16, cudaMemcpyDeviceToHost, g.st));
+            DSG_CU(cudaStreamSynchronize(g.st));
+            const uint32_t n1 = g.h_n[0], n2 = g.h_n[1], n3 = g.h_n[2];
+            overflow |= n1 > g.cap1 || n2 > g.cap2 || n3 > g.cap3;
+            const uint32_t k3 = std::min(n3, g.cap3);
+            if (k3) {
+                DSG_CU(cudaMemcpyAsync(g.h_s3, g.d_s3, size_t(k3) * 8, cudaMemcpyDeviceToHost, g.st));
+                DSG_CU(cudaMemcpyAsync(g.h_a3, g.d_a3, size_t(k3) * 4, cudaMemcpyDeviceToHost, g.st));
+                DSG_CU(cudaStreamSynchronize(g.st));
+            }
+            found.clear();
+            for (uint32_t i = 0; i < k3; i++) found.push_back({g.h_s3[i], g.h_a3[i]});
+            std::sort(found.begin(), found.end());
+            for (auto &f : found) {
+                if (written < cap) { out_seed[written] = f.first; out_amp[written] = f.second; written++; }
+                else overflow = true;
+            }
+            tot[0] += nb; tot[1] += n1; tot[2] += n2; tot[3] += n3;
+        }
+        *n_out = written;
+        if (counts) std::memcpy(counts, tot, sizeof tot);
+        return overflow ? DSG_OVERFLOW : DSG_OK;
+    });
+}
+
+// Device-resident form for benchmarks and the fused pipeline: enqueue one batch on `stream` and leave the
+// counters {phase, pre, full} and survivors in device memory.
+namespace dsg { namespace gate {
+int run_device_batch(cudaStream_t st, uint64_t start, uint64_t nb, const dsg_gate_cfg &cfg, const uint32_t **d_counts,
+                     const uint64_t **d_seeds, const float **d_amps) {
+    State &g = S(); std::lock_guard<std::mutex> l(g.mu); setup_locked(g);
+    ensure_buffers(g, nb);
+    enqueue_batch(g, st, start, nb, cfg);
+    *d_counts = g.d_n; *d_seeds = g.d_s3; *d_amps = g.d_a3;
+    return DSG_OK;
+}
+}}

@@ -1,0 +1,155 @@
+// Worldgen tables on the device (biome tree, parameter intervals, depth-0 surface grid, terrain spline,
+// proxy probability table) and the lookups that use them: surface grid lookup, exact tree classify and the
+// terrain-offset spline (src/surface.hpp:12-71, src/standalone.hpp:154-196).  Header-only device code,
+// shared by every kernel that classifies climate points.
+#pragma once
+#include <cstdint>
+
+namespace dsg {
+
+struct SplineDev { int32_t axis, n; float value; float knot[12], slope[12]; int32_t kid[12]; };
+
+// Passed to kernels by value (it lives in the parameter constant bank); the large arrays are in HBM/L2.
+struct WorldDev {
+    const int16_t *cells;        // surface grid: biome id per grid cell, -1 = ambiguous (tree decides)
+    const uint64_t *tree;        // biome tree nodes
+    const int32_t *param;        // interval k = [param[2k], param[2k+1]]
+    const SplineDev *spl;        // terrain-offset spline graph (node 0 is the root)
+    const float *prob;           // 40 x 40 proxy desert probability (row = C bin, column = E bin)
+    int32_t ntree, nspl;
+    int32_t strides[8];
+    int32_t dim[5];              // grid cells per axis (T, H, C, E, W)
+    int32_t ncut[5];             // cut planes per axis (= dim + 1)
+    int32_t cut[5][32];          // sorted cut planes per axis
+};
+const WorldDev &world_dev();     // valid after dsg_init
+
+#ifdef __CUDACC__
+// Surface grid lookup (surface.hpp:58-70): the biome of the depth-0 surface box containing q, or -1 when q
+// lies outside the grid, on a cut plane, or in a cell that is ambiguous.
+__device__ __forceinline__ int grid_lookup(const WorldDev &w, const int64_t *q) {
+    constexpr int AX[5] = {0, 1, 2, 3, 5};
+    size_t flat = 0;
+    #pragma unroll
+    for (int a = 0; a < 5; a++) {
+        const int64_t v = q[AX[a]];
+        const int32_t *c = w.cut[a];
+        const int nc = w.ncut[a];
+        if (v < c[0] || v >= c[nc - 1]) return -1;
+        int lo = 0, hi = nc;                       // first cut > v (upper_bound)
+        while (lo < hi) { const int mid = (lo + hi) >> 1; if (int64_t(c[mid]) <= v) lo = mid + 1; else hi = mid; }
+        const int idx = lo - 1;
+        if (v == c[idx]) return -1;
+        flat = flat * size_t(w.dim[a]) + size_t(idx);
+    }
+    return w.cells[flat];
+}
+__device__ __forceinline__ uint64_t box_dist(const WorldDev &w, int node, const int64_t *v) {
+    const uint64_t e = w.tree[node];
+    uint64_t sum = 0;
+    #pragma unroll
+    for (int i = 0; i < 6; i++) {
+        const int k = int((e >> (8 * i)) & 255);
+        const int64_t lo = w.param[2 * k], hi = w.param[2 * k + 1];
+        int64_t d = lo - v[i];
+        if (v[i] - hi > d) d = v[i] - hi;
+        if (d < 0) d = 0;
+        sum += uint64_t(d * d);
+    }
+    return sum;
+}
+// Exact nearest-box search of the biome tree (standalone.hpp:182-196), with an explicit stack in place of
+// the recursion.  Children are visited in order and pruned against the running best distance exactly as
+// the recursive form does (the prune test is re-evaluated when a child is reached).
+__device__ inline int tree_classify(const WorldDev &w, const int64_t *v) {
+    struct Frame { int node, level, child, stride, i; };
+    Frame stk[8];
+    int sp = 0, best = 0;
+    uint64_t bestd = ~0ull;
+    // enter(node, level): leaf -> compare; inner -> push a frame iterating its children
+    int node = 0, level = 0;
+    for (;;) {
+        bool descended = false;
+        if ((w.tree[node] >> 56) == 255) {
+            const uint64_t d = box_dist(w, node, v);
+            if (d < bestd) { bestd = d; best = node; }
+        } else {
+            int stride, lv = level;
+            do { stride = w.strides[lv++]; } while (node + stride >= w.ntree);
+            stk[sp++] = {node, lv, int(w.tree[node] >> 48), stride, 0};
+        }
+        // advance the innermost frame to its next child that passes the prune test
+        while (sp > 0) {
+            Frame &f = stk[sp - 1];
+            bool found = false;
+            while (f.i < 6 && f.child < w.ntree) {
+                const int c = f.child;
+                f.i++; f.child += f.stride;
+                if (box_dist(w, c, v) < bestd) { node = c; level = f.level; found = true; break; }
+            }
+            if (found) { descended = true; break; }
+            sp--;
+        }
+        if (!descended) break;
+    }
+    return int((w.tree[best] >> 48) & 255);
+}
+__device__ __forceinline__ float lerpd_f(float t, float a, float b) { return float(double(a) + double(t) * (double(b) - double(a))); }
+// Terrain-offset spline (standalone.hpp:154-169) with an explicit stack.  The float/double mix of the
+// interpolation follows the reference expression by expression.
+__device__ inline float spline_eval(const WorldDev &w, const float *v) {
+    struct Frame { int node, lo, stage; float x, t, width, a; };
+    Frame stk[8];
+    int sp = 0;
+    float ret = 0.f;
+    int node = 0;
+    for (;;) {
+        // evaluate `node`: leaf values return immediately; inner nodes push a frame
+        const SplineDev &s = w.spl[node];
+        bool pushed = false;
+        if (s.n == 0) ret = s.value;
+        else {
+            const float x = v[s.axis];
+            int hi = 0;
+            while (hi < s.n && x > s.knot[hi]) hi++;
+            if (hi == 0 || hi == s.n) {
+                const int j = hi == 0 ? 0 : s.n - 1;
+                stk[sp++] = {node, j, 0, x, 0.f, 0.f, 0.f};      // stage 0: extrapolate from child j
+                node = s.kid[j]; pushed = true;
+            } else {
+                const int lo = hi - 1;
+                const float width = __fsub_rn(s.knot[hi], s.knot[lo]);
+                const float t = __fdiv_rn(__fsub_rn(x, s.knot[lo]), width);
+                stk[sp++] = {node, lo, 1, x, t, width, 0.f};      // stage 1: need child lo, then child hi
+                node = s.kid[lo]; pushed = true;
+            }
+        }
+        if (pushed) continue;
+        // unwind with ret = value of the node just evaluated
+        bool next = false;
+        while (sp > 0) {
+            Frame &f = stk[sp - 1];
+            const SplineDev &p = w.spl[f.node];
+            if (f.stage == 0) {
+                ret = __fadd_rn(ret, __fmul_rn(p.slope[f.lo], __fsub_rn(f.x, p.knot[f.lo])));
+                sp--;
+            } else if (f.stage == 1) {
+                f.a = ret; f.stage = 2; node = p.kid[f.lo + 1]; next = true; break;
+            } else {
+                const float a = f.a, b = ret, t = f.t, width = f.width;
+                const float dba = __fsub_rn(b, a);
+                const float pp = __fsub_rn(__fmul_rn(p.slope[f.lo], width), dba);
+                const float qq = __fadd_rn(__fmul_rn(-p.slope[f.lo + 1], width), dba);
+                const double lin = __dadd_rn(double(a), __dmul_rn(double(t), __dsub_rn(double(b), double(a))));
+                const double cur = __dadd_rn(double(pp), __dmul_rn(double(t), __dsub_rn(double(qq), double(pp))));
+                ret = float(__dadd_rn(lin, __dmul_rn(double(__fmul_rn(t, __fsub_rn(1.f, t))), cur)));
+                sp--;
+            }
+        }
+        if (!next) break;
+    }
+    return ret;
+}
+#endif
+
+}  // namespace dsg

@@ -37,12 +37,14 @@ int orc_gate(const uint64_t *seeds, int n, int want_full, const float *k9, const
 // The whole seed gate over seeds fmix(start + k), k < count: phase <= maxph, pre-gate amp >= pthr,
 // full amp >= amp.  Survivors (unordered across threads; the caller sorts) go to out_seed/out_amp.
 // counts = {seeds, phase-passed, pre-passed, full-passed}.
+// taps24 (may be NULL): the 9 + 15 blur taps; NULL uses the oracle's correctly rounded taps.
 int orc_gate_range(uint64_t start, uint64_t count, double maxph, float pthr, float amp, int threads,
-                   uint64_t *out_seed, float *out_amp, int cap, uint64_t *counts) {
+                   uint64_t *out_seed, float *out_amp, int cap, uint64_t *counts, const float *taps24) {
     std::atomic<uint64_t> next(0), n1(0), n2(0), n3(0);
     std::mutex mu;
     float k9[9], k15[15];
     gate_taps(4, 1.0f, k9); gate_taps(7, 2.0f, k15);
+    if (taps24) { std::copy(taps24, taps24 + 9, k9); std::copy(taps24 + 9, taps24 + 24, k15); }
     auto work = [&] {
         for (;;) {
             const uint64_t k0 = next.fetch_add(256);

@@ -1,0 +1,124 @@
+#!/usr/bin/env python3
+"""Generate the committed golden fixtures from the reference's own code.
+
+Runs where the reference checkout is present and oracle/_ref has been built (`make ref`):
+  finds.json        the 220 MC-Measure-verified finds (seed, block X, Z, step-1 cells) of the reference's
+                    results/desert_finds.jsonl: exact-area golden vectors
+  ref_phase.npz     phase_t and both fractional y offsets for 2,000 seeds (src/dsearch_desert.cpp:80-94)
+  ref_points.npz    bridged desert state, unbridged desert, hot (T >= 0.55) and proxy probability x1000 at
+                    random points near four finds; climate vectors q[6]; raw channel noise values
+  ref_floods.json   dense_flood_bridged areas (cells, sampled, bbox, edge, border) at the screening lattices
+  ref_tables.npz    tab_setup inputs, translation maps, blur taps, and a checksum of the six blurred tables
+  ref_cli.json      the reference CLI's per-seed scan summary (maxta, maxtb, NMS buckets, sites) for
+                    gated seeds fed through stdin=1, with the hot-zone stage switched off (hot_min=1e9)
+Usage: python tests/golden/make_golden.py [REFERENCE_ROOT]
+"""
+import hashlib
+import json
+import os
+import subprocess
+import sys
+import tempfile
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(os.path.dirname(HERE))
+sys.path.insert(0, os.path.join(ROOT, "tests"))
+import libs  # noqa: E402
+
+M64 = (1 << 64) - 1
+
+
+def main():
+    refroot = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
+    r = libs.ref()
+    assert r is not None, "build oracle/_ref first (make ref)"
+    rows = [json.loads(l) for l in open(os.path.join(refroot, "results", "desert_finds.jsonl"))]
+    finds = [{"seed": int(x["seed"]), "x": x["x"], "z": x["z"], "cells": x["cells"], "blocks2": x["blocks2"]}
+             for x in rows if "cells" in x]
+    # the `make check` pair (Makefile:67-71), areas as published in README.md:5-6,14
+    for seed, x, z, b2 in [(1106000410148237774, 7341586, -22019902, 70927696), (-8125596009223775875, -22910974, 2295170, 100674560)]:
+        if not any(f["seed"] == seed for f in finds):
+            finds.append({"seed": seed, "x": x, "z": z, "cells": b2 // 16, "blocks2": b2})
+    json.dump(finds, open(os.path.join(HERE, "finds.json"), "w"), indent=0)
+
+    seeds = np.array([libs.mix(k) for k in range(2000)], dtype=np.uint64)
+    ph, fy = r.phase(seeds)
+    np.savez_compressed(os.path.join(HERE, "ref_phase.npz"), seeds=seeds, phase=ph, fy=fy)
+
+    rng = np.random.default_rng(20261203)
+    pts = {}
+    for n, f in enumerate(finds[:4]):
+        seed = f["seed"] & M64
+        qx, qz = f["x"] >> 2, f["z"] >> 2
+        xz = np.c_[qx + rng.integers(-6000, 6000, 4000), qz + rng.integers(-6000, 6000, 4000)].astype(np.int32)
+        pts[f"seed{n}"] = np.uint64(seed)
+        pts[f"xz{n}"] = xz
+        for pred in range(4):
+            pts[f"p{pred}_{n}"] = r.points(seed, pred, xz)
+        pts[f"q{n}"] = r.climate(seed, xz[:500])
+        xyz = np.c_[rng.integers(-3e7, 3e7, 300) + rng.random(300), rng.integers(-64, 64, 300) * (rng.random(300) < .3),
+                    rng.integers(-3e7, 3e7, 300) + rng.random(300)]
+        pts[f"xyz{n}"] = xyz
+        for ch in range(6):
+            pts[f"noise{ch}_{n}"] = r.noise(seed, ch, xyz)
+    np.savez_compressed(os.path.join(HERE, "ref_points.npz"), **pts)
+
+    floods = []
+    for f in finds[:3]:
+        seed = f["seed"] & M64
+        qx, qz = f["x"] >> 2, f["z"] >> 2
+        for (step, half, c8, pred) in [(8, 2000, True, 0), (4, 4000, False, 0), (32, 500, True, 4),
+                                       (128, 250, False, 2), (256, 125, False, 2), (16, 300, False, 0)]:
+            floods.append({"seed": f["seed"], "qx": qx, "qz": qz, "step": step, "half": half, "conn8": c8, "pred": pred,
+                           "pcut": 0.35, "area": list(r.flood(seed, qx, qz, step, half, c8, pred, 0.35))})
+    # window edge and world border cases: a tiny window and a start next to the world border
+    f = finds[0]
+    seed = f["seed"] & M64
+    floods.append({"seed": f["seed"], "qx": f["x"] >> 2, "qz": f["z"] >> 2, "step": 4, "half": 60, "conn8": False, "pred": 0,
+                   "pcut": 0.35, "area": list(r.flood(seed, f["x"] >> 2, f["z"] >> 2, 4, 60, False, 0, 0.35))})
+    for s0 in range(40):
+        s = libs.mix(777 + s0)
+        bx = 7499996 - 40
+        for dz in range(0, 4000, 16):
+            if r.points(s, 2, np.array([[bx, dz]], dtype=np.int32))[0] == 2:
+                floods.append({"seed": s - (1 << 64) if s >= 1 << 63 else s, "qx": bx, "qz": dz, "step": 8, "half": 600, "conn8": False,
+                               "pred": 2, "pcut": 0.35, "area": list(r.flood(s, bx, dz, 8, 600, False, 2, 0.35))})
+                break
+        if sum(1 for x in floods if x["qx"] == bx) >= 2:
+            break
+    json.dump(floods, open(os.path.join(HERE, "ref_floods.json"), "w"), indent=0)
+
+    tab = {}
+    for n, f in enumerate(finds[:2]):
+        seed = f["seed"] & M64
+        tab[f"seed{n}"] = np.uint64(seed)
+        tab[f"tabin{n}"] = r.tabins(seed)
+        t, mx = r.tables(seed)
+        tab[f"sha{n}"] = np.frombuffer(hashlib.sha256(t.tobytes()).digest(), dtype=np.uint8)
+        tab[f"max{n}"] = mx
+        tab[f"row{n}"] = t[:, 123, :].copy()                  # one full row of each table, for diagnostics
+    for lat in (1024, 512):
+        ib, lo, hi = r.tmap(float(lat))
+        tab[f"ib{lat}"], tab[f"lo{lat}"], tab[f"hi{lat}"] = ib, lo, hi
+    for sg in (1.0, 2.0):
+        tab[f"taps{int(sg)}"] = r.blur_taps(sg)[0]
+    np.savez_compressed(os.path.join(HERE, "ref_tables.npz"), **tab)
+
+    # reference CLI scan summary: gated seeds through stdin=1, hot-zone stage off
+    cli = []
+    with tempfile.TemporaryDirectory() as td:
+        gated = [f["seed"] for f in finds[:6]]
+        inp = "".join(f"{s}\n" for s in gated)
+        subprocess.run([os.path.join(ROOT, "oracle", "_ref", "dsearch_desert"), "0", "0", os.path.join(td, "g"), "4", "stdin=1",
+                        "hot_min=1e9"], input=inp.encode(), check=True, capture_output=True)
+        for line in open(os.path.join(td, "g.seeds.csv")).read().splitlines()[1:]:
+            s, fa, fb, ma, mb, cand, sites, best = line.split(",")
+            cli.append({"seed": int(s), "fyA": fa, "fyB": fb, "maxta": ma, "maxtb": mb, "buckets": int(cand), "sites": int(sites)})
+    json.dump(sorted(cli, key=lambda x: x["seed"]), open(os.path.join(HERE, "ref_cli.json"), "w"), indent=0)
+    print("fixtures written to", HERE)
+
+
+if __name__ == "__main__":
+    main()

@@ -140,8 +140,11 @@ def ref():
 
 
 def orc_gate(seeds, want_full=True, k9=None, k15=None, threads=8):
-    """Oracle pre-gate and full-gate side amplitudes, arrays of shape (n, 2)."""
+    """Oracle pre-gate and full-gate side amplitudes, arrays of shape (n, 2); taps default to the
+    reference GPU gate's."""
     lib = orc().lib
+    if k9 is None:
+        k9, k15 = ref_gpu_taps()
     s = np.ascontiguousarray(seeds, dtype=np.uint64)
     pre = np.empty(2 * len(s), dtype=np.float32); full = np.empty(2 * len(s), dtype=np.float32)
     k9p = ptr(np.ascontiguousarray(k9, dtype=np.float32), f32p) if k9 is not None else None
@@ -157,17 +160,28 @@ def side_sum(a):
 
 
 def orc_gate_taps():
+    """Correctly rounded exp taps, the oracle's own (float(exp(double)))."""
     k9 = np.empty(9, dtype=np.float32); k15 = np.empty(15, dtype=np.float32)
     orc().lib.orc_gate_taps(C.c_int(4), C.c_float(1.0), ptr(k9, f32p))
     orc().lib.orc_gate_taps(C.c_int(7), C.c_float(2.0), ptr(k15, f32p))
     return k9, k15
 
 
+def ref_gpu_taps():
+    """The blur taps the reference's GPU gate computes with device expf (tests/golden/ref_gate_gpu.npz,
+    made by make_gate_golden.py on a B200); exp(-2) is 1 ulp below the correctly rounded value."""
+    t = np.load(os.path.join(ROOT, "tests", "golden", "ref_gate_gpu.npz"))["taps"]
+    return t[:9].copy(), t[9:].copy()
+
+
 def orc_gate_range(start, count, maxph=0.06, pthr=0.645, amp=0.70, threads=8, cap=1 << 16):
+    """The whole gate over mix(start + k) on the CPU with the reference GPU gate's taps."""
     lib = orc().lib
+    k9, k15 = ref_gpu_taps()
+    taps = np.ascontiguousarray(np.r_[k9, k15], dtype=np.float32)
     seeds = np.empty(cap, dtype=np.uint64); amps = np.empty(cap, dtype=np.float32); counts = np.zeros(4, dtype=np.uint64)
     lib.orc_gate_range(C.c_uint64(start), C.c_uint64(count), C.c_double(maxph), C.c_float(pthr), C.c_float(amp), C.c_int(threads),
-                       ptr(seeds, u64p), ptr(amps, f32p), C.c_int(cap), ptr(counts, u64p))
+                       ptr(seeds, u64p), ptr(amps, f32p), C.c_int(cap), ptr(counts, u64p), ptr(taps, f32p))
     n = int(min(counts[3], cap))
     order = np.argsort(seeds[:n])
     return seeds[:n][order], amps[:n][order], counts

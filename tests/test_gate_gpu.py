@@ -1,0 +1,85 @@
+"""GPU seed gate (libdsgpu through the C ABI) against the oracle, bit for bit, and against the reference's
+own GPU kernels (oracle/_ref/libref_gate.so) where they were built."""
+import ctypes as C
+import os
+
+import numpy as np
+import pytest
+
+import libs
+
+pytestmark = pytest.mark.gpu
+
+
+def phase_passed(start, count, cut=0.06):
+    seeds = np.array([libs.mix(start + k) for k in range(count)], dtype=np.uint64)
+    ph, _ = libs.orc().phase(seeds)
+    return seeds[ph <= np.float64(np.float32(cut))]
+
+
+def test_taps_equal_reference_gpu_taps(dsg):
+    """The gate's blur taps are device expf values, computed as the reference kernels compute them."""
+    k9, k15 = dsg.gate_taps()
+    d = np.load(os.path.join(os.path.dirname(__file__), "golden", "ref_gate_gpu.npz"))
+    assert np.array_equal(k9, d["taps"][:9]) and np.array_equal(k15, d["taps"][9:])
+
+
+def test_phase_bit_exact(dsg):
+    seeds = np.array([libs.mix(k) for k in range(5000)], dtype=np.uint64)
+    p1, f1 = dsg.phase(seeds)
+    p2, f2 = libs.orc().phase(seeds)
+    assert np.array_equal(p1, p2) and np.array_equal(f1, f2)
+
+
+def test_gate_amps_bit_exact_vs_oracle(dsg):
+    seeds = phase_passed(10**12, 65536)                     # the gate microbench's seeds: ~470 phase-passed
+    assert 300 < len(seeds) < 700
+    k9, k15 = dsg.gate_taps()
+    pre, full = dsg.gate_amps(seeds)
+    opre, ofull = libs.orc_gate(seeds, True, k9, k15)
+    assert np.array_equal(pre, opre), f"pre-gate mismatches: {np.sum(pre != opre)}"
+    assert np.array_equal(full, ofull), f"full-gate mismatches: {np.sum(full != ofull)}"
+
+
+def test_gate_run_matches_oracle_range(dsg):
+    start, count = 2 * 10**13, 1 << 18
+    s, a, counts, rc = dsg.gate_run(start, count, batch=1 << 16)
+    assert rc == 0
+    os_, oa, ocounts = libs.orc_gate_range(start, count, threads=os.cpu_count() or 8)
+    assert list(counts) == [int(x) for x in ocounts]
+    assert np.array_equal(np.sort(s), os_) and np.array_equal(a[np.argsort(s)], oa)
+
+
+def test_gate_run_batches_and_ragged_count(dsg):
+    """Survivor set does not depend on the batch size; counts add up over a ragged last batch."""
+    start, count = 10**12, 200_003
+    s1, a1, c1, _ = dsg.gate_run(start, count, pthr=0.60, amp=0.62, batch=0)
+    s2, a2, c2, _ = dsg.gate_run(start, count, pthr=0.60, amp=0.62, batch=30_000)
+    assert list(c1) == list(c2) and c1[0] == count
+    assert np.array_equal(np.sort(s1), np.sort(s2))
+    z, _, c0, rc = dsg.gate_run(start, 0)
+    assert len(z) == 0 and c0[0] == 0 and rc == 0
+
+
+def test_gate_run_overflow_is_reported(dsg):
+    s, a, counts, rc = dsg.gate_run(10**12, 100_000, pthr=0.0, amp=0.0, cap=3)
+    assert rc == dsg.DSG_OVERFLOW and len(s) == 3 and counts[3] > 3
+
+
+def test_gate_matches_reference_gpu_kernels(dsg):
+    p = os.path.join(libs.REF_DIR, "libref_gate.so")
+    if not os.path.exists(p):
+        pytest.skip("oracle/_ref/libref_gate.so not built")
+    g = C.CDLL(p)
+    seeds = phase_passed(10**12, 65536)
+    pre = np.empty(len(seeds), dtype=np.float32); full = np.empty(len(seeds), dtype=np.float32)
+    rc = g.ref_gate_gpu(seeds.ctypes.data_as(C.POINTER(C.c_uint64)), C.c_int(len(seeds)),
+                        pre.ctypes.data_as(C.POINTER(C.c_float)), full.ctypes.data_as(C.POINTER(C.c_float)))
+    assert rc == 0
+    mpre, mfull = dsg.gate_amps(seeds)
+    assert np.array_equal(libs.side_sum(mpre), pre), f"pre-gate amp mismatches: {np.sum(libs.side_sum(mpre) != pre)}"
+    assert np.array_equal(libs.side_sum(mfull), full), f"full amp mismatches: {np.sum(libs.side_sum(mfull) != full)}"
+    k = np.empty(24, dtype=np.float32)
+    assert g.ref_gate_taps_gpu(k.ctypes.data_as(C.POINTER(C.c_float))) == 0
+    k9, k15 = dsg.gate_taps()
+    assert np.array_equal(k[:9], k9) and np.array_equal(k[9:], k15)
