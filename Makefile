@@ -18,7 +18,7 @@ CU_SRC   := $(wildcard $(PKG)/csrc/*.cu)
 CU_HDR   := $(wildcard $(PKG)/csrc/*.cuh) $(wildcard $(PKG)/csrc/*.h) $(wildcard include/*.h)
 CU_OBJ   := $(patsubst $(PKG)/csrc/%.cu,$(B)/%.o,$(CU_SRC))
 LIB      := $(PKG)/lib/libdsgpu.so
-HOST_BIN := $(PKG)/bin/dsearch_desert $(PKG)/bin/tgate $(PKG)/bin/dflood
+HOST_BIN := $(patsubst $(PKG)/host/%.cpp,$(PKG)/bin/%,$(wildcard $(PKG)/host/*.cpp))
 ORC_LIB  := oracle/liborc.so
 
 all: $(LIB) $(HOST_BIN) $(ORC_LIB)

@@ -1,0 +1,234 @@
+#!/usr/bin/env python3
+"""Benchmark: gated seeds/s of the B200 seed gate, and the timed CPU reference arm.
+
+Workload: the batched search's seed stream, seeds mix(2*10^13 + k), processed in steps of 2^26 seed
+indices.  One step is one pass of the plain per-stage gate (y-phase -> octave init -> anti-aliased 256^2
+pre-gate -> full 512^2 gate) on the device; the metric counts the seeds that pass all three (about 1 in
+13,000).  Multi-GPU: one process per GPU, each on its own seed range 10^12 apart (weak scaling, no
+data-path collective); device time is the max over ranks.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+--impl reference times the reference's own CPU searcher (oracle/_ref/dsearch_desert, compiled from the
+reference sources) on the same seed stream with all host cores: its CPU gate (y-phase, sub-grid pre-gate,
+full tables) plus the tables+scan of every gated seed, with the hot-zone stage reduced to one site.
+"""
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.join(ROOT, "desert-search_b200"))
+sys.path.insert(0, os.path.join(ROOT, "tests"))
+
+METRIC = "gated seeds/s on 1 B200, fused vs plain; flood-request p50/p99 latency"
+UNIT = "gated seeds/s"
+START = 2 * 10**13
+PER_STEP = 1 << 26
+RANK_STRIDE = 10**12            # per-GPU seed ranges, as deploy/prun.sh assigns them
+# pre-gate: 2 sides x 256^2 cells x 18 corner-table gathers of 4 bytes per phase-passed seed
+PRE_BYTES_PER_SEED = 2 * 256 * 256 * 18 * 4
+SMEM_BYTES_PER_CLK_PER_SM = 128  # 32 banks x 4 bytes
+
+
+def dist():
+    rank, world, local = int(os.environ.get("RANK", 0)), int(os.environ.get("WORLD_SIZE", 1)), int(os.environ.get("LOCAL_RANK", 0))
+    return rank, world, local
+
+
+class Clocks:
+    """nvidia-smi samples of this GPU's clocks during the timed region."""
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+         "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu):
+        self.gpu = gpu
+        self.f = tempfile.TemporaryFile(mode="w+")
+        try:
+            self.p = subprocess.Popen(["nvidia-smi", f"--query-gpu={self.Q}", "--format=csv,noheader,nounits", "-lms", "200", "-i", str(gpu)],
+                                      stdout=self.f, stderr=subprocess.DEVNULL)
+        except OSError:
+            self.p = None
+
+    def stop(self):
+        if self.p is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.p.terminate()
+        self.p.wait()
+        self.f.seek(0)
+        rows = [r.split(",") for r in self.f.read().strip().splitlines() if r.count(",") >= 8]
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for r in rows:
+            try:
+                sm.append(float(r[1])); mx = float(r[2])
+            except ValueError:
+                continue
+            for n, v in zip(names, r[5:9]):
+                if v.strip() == "Active":
+                    reasons.add(n)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": mx, "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def cpu_baseline(seconds_budget=20.0):
+    """The oracle's CPU restatement of the same gate, on all host threads, over a bounded sample."""
+    import libs
+    threads = os.cpu_count() or 1
+    count = 1 << 19
+    t0 = time.perf_counter()
+    _, _, c = libs.orc_gate_range(START + (1 << 40), count, threads=threads)
+    dt = time.perf_counter() - t0
+    if dt < seconds_budget / 4:                     # grow the sample towards the budget
+        count = int(count * min(16, seconds_budget / max(dt, 1e-3)))
+        t0 = time.perf_counter()
+        _, _, c = libs.orc_gate_range(START + (1 << 40), count, threads=threads)
+        dt = time.perf_counter() - t0
+    return {"value": float(c[3]) / dt, "unit": UNIT, "cores": threads, "kind": "port",
+            "sample": f"seeds mix(2e13 + 2^40 + k), k < {count}: {int(c[1])} phase-passed, {int(c[3])} gated in {dt:.2f} s",
+            "seeds_per_s": count / dt}
+
+
+def run_ours(args):
+    rank, world, local = dist()
+    import dsgpu
+    pg = None
+    if world > 1:
+        import torch
+        import torch.distributed as td
+        torch.cuda.set_device(local)
+        td.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=120))
+        pg = td
+    dsgpu.init(local, 0.35)
+    base = START + rank * RANK_STRIDE
+
+    def barrier():
+        if pg:
+            pg.barrier()
+
+    def reduce(vals, op):
+        if not pg:
+            return vals
+        import torch
+        t = torch.tensor(vals, dtype=torch.float64, device="cuda")
+        pg.all_reduce(t, op=op)
+        return t.tolist()
+
+    barrier()
+    clk = Clocks(local)
+    ms, mk, counts = dsgpu.gate_bench(base, PER_STEP, args.steps, args.warmup)
+    clocks = clk.stop()
+    barrier()
+    if pg:
+        ms_max = reduce([ms], pg.ReduceOp.MAX)[0]
+        tot = reduce([float(x) for x in counts], pg.ReduceOp.SUM)
+    else:
+        ms_max, tot = ms, [float(x) for x in counts]
+    value = tot[3] / (ms_max / 1e3)
+
+    if args.profile_run:
+        if rank == 0:
+            print(json.dumps({"profile_run": True, "ms": ms_max, "kernel_ms": [float(x) for x in mk], "counts": [int(x) for x in tot]}))
+        return
+    # end to end through the C ABI: host output buffers, device->host copies inside the timed region
+    barrier()
+    t0 = time.perf_counter()
+    s, a, c, rc = dsgpu.gate_run(base + (args.steps + args.warmup) * PER_STEP, args.steps * PER_STEP, batch=PER_STEP, cap=1 << 20)
+    e2e_s = time.perf_counter() - t0
+    barrier()
+    if pg:
+        e2e_s = reduce([e2e_s], pg.ReduceOp.MAX)[0]
+        e2e_n = reduce([float(c[3])], pg.ReduceOp.SUM)[0]
+    else:
+        e2e_n = float(c[3])
+    d2h = 16 + int(c[3]) * 12 // max(1, args.steps)      # counters + (seed, amp) of survivors per step
+
+    # roofline of the dominant kernel (the anti-aliased pre-gate): corner-table gathers from shared memory
+    pre_ms = float(mk[2])
+    achieved = counts[1] * PRE_BYTES_PER_SEED / (pre_ms / 1e3) / 1e9
+    sm_mhz = clocks.get("sm_mhz") or 1965.0
+    props = __import__("torch").cuda.get_device_properties(local)
+    peak = props.multi_processor_count * SMEM_BYTES_PER_CLK_PER_SM * sm_mhz * 1e6 / 1e9
+    if rank != 0:
+        return
+    out = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": ms_max / args.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "fp32", "data": "synthetic",
+        "config": {"workload": "seed gate (y-phase <= 0.06, AA pre-gate >= 0.645, full gate >= 0.70) over seeds mix(2e13 + k)",
+                   "seeds_per_step": PER_STEP, "global_seeds": PER_STEP * args.steps * world, "parallelism": f"replicas{world}",
+                   "l2": "no input data: seeds are generated on the device; the per-step octave table (~0.6 KB per phase-passed seed, ~290 MB) exceeds L2"},
+        "counts": {"seeds": int(tot[0]), "phase_passed": int(tot[1]), "pre_passed": int(tot[2]), "gated": int(tot[3])},
+        "seeds_per_s": tot[0] / (ms_max / 1e3),
+        "kernel_ms": {"phase": float(mk[0]), "octave_init": float(mk[1]), "pregate": float(mk[2]), "fullgate": float(mk[3])},
+        "e2e": {"value": e2e_n / e2e_s, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": d2h},
+        "roofline": {"bound": "smem", "kernel": "k_pregate", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                     "frac": achieved / peak, "traffic": None,
+                     "note": "shared-memory gather bytes (18 corner-table words per cell); peak = SMs x 128 B/clk at the median SM clock sampled during the run"},
+        "gpu_launches": 4 * args.steps,
+        "clocks": clocks,
+    }
+    if world == 1:
+        out["cpu_baseline"] = cpu_baseline()
+    print(json.dumps(out), flush=True)
+    if pg:
+        pg.destroy_process_group()
+
+
+def run_reference(args):
+    rank, world, local = dist()
+    if rank != 0:
+        return
+    exe = os.path.join(ROOT, "oracle", "_ref", "dsearch_desert")
+    if not os.path.exists(exe):
+        print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref/dsearch_desert not built (make ref needs the reference checkout)"}))
+        return
+    cores = os.cpu_count() or 1
+    per_step = max(100_000, 50_000 * cores)          # ~2.6 core-s per 50k seeds: a few seconds per step
+    total_s, scanned, done = 0.0, 0, 0
+    with tempfile.TemporaryDirectory() as td:
+        for it in range(args.warmup + args.steps):
+            pre = os.path.join(td, f"s{it}")
+            t0 = time.perf_counter()
+            subprocess.run([exe, str(START + it * per_step), str(per_step), pre, str(cores), "phase=0.06", "hot_min=1e9", "sites=1",
+                            "exact_n=0"], check=True, capture_output=True)
+            dt = time.perf_counter() - t0
+            if it >= args.warmup:
+                j = json.load(open(pre + ".json"))
+                total_s += dt; scanned += j["scanned"]; done += j["done"]
+    value = scanned / total_s
+    print(json.dumps({
+        "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": total_s * 1e3 / args.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "fp64/fp32",
+        "data": "synthetic",
+        "config": {"workload": "seed gate over seeds mix(2e13 + k): reference CPU gate (y-phase <= 0.06, sub-grid pre-gate, full tables) "
+                               "plus tables+scan of each gated seed", "seeds_per_step": per_step, "parallelism": f"{cores} host threads"},
+        "counts": {"seeds": done, "gated": scanned},
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": "reference",
+                         "sample": f"{args.steps} x {per_step} seeds through oracle/_ref/dsearch_desert (reference sources)"},
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }), flush=True)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--per-step-log2", type=int, default=26, help="seed indices per step = 2^N")
+    ap.add_argument("--profile-run", action="store_true", help="device steps only (no e2e pass, no CPU baseline): for ncu captures")
+    args = ap.parse_args()
+    global PER_STEP
+    PER_STEP = 1 << args.per_step_log2
+    if args.warmup < 3 and args.impl == "ours":
+        args.warmup = 3
+    (run_reference if args.impl == "reference" else run_ours)(args)
+
+
+if __name__ == "__main__":
+    main()

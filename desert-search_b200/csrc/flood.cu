@@ -196,6 +196,7 @@ int run_batch(const dsg_flood_req *reqs, uint32_t n, dsg_area *out, size_t pool_
     Engine &g = E();
     std::lock_guard<std::mutex> l(g.mu);
     setup_locked(g);
+    DSG_ARG(n <= g.list_cap, "dsg_flood_batch: too many requests in one batch");
     // distinct seeds -> noise tables
     std::map<uint64_t, int32_t> slot;
     std::vector<uint64_t> seeds;

@@ -29,7 +29,7 @@ static_assert(sizeof(Oct) == 304, "Oct layout");
 struct Taps { float k9[9], k15[15], norm9, norm15, w; };
 
 constexpr int PG_THREADS = 128, PG_BAND = 64;        // pre-gate: 4 warps x 64 rows = 256 rows per side
-constexpr int FG_THREADS = 512, FG_RB = 8;           // full gate: thread per column, 8-row blocks
+constexpr int FG_THREADS = 128, FG_RB = 8;           // full gate: thread per 4 columns, 8-row blocks
 
 // ---------------------------------------------------------------- device math
 // fade as the reference's GPU gate evaluates it: nvcc contracts t*6-15 and t*(..)+10 (gate.cuh:51).
@@ -210,21 +210,25 @@ k_pregate(const Oct *__restrict__ oct, const uint64_t *__restrict__ seeds, const
         const char *tcb = reinterpret_cast<const char *>(sTc);
         for (int r = o0 - 4; r < o0 + PG_BAND + 4; r++) {
             hash_row(sP2, cv, (r + 2 + iz0) & 255, lane, hC);
+            // samples: for each (v, dy) hash row, unpack its 10 bytes once, then add the three u terms of
+            // all 8 cells; each cell still sums in the order v, dy, u (gate.cuh:274-281)
             float S[8];
             #pragma unroll
-            for (int e = 0; e < 8; e++) {
-                float acc = 0.f;
+            for (int e = 0; e < 8; e++) S[e] = 0.f;
+            #pragma unroll
+            for (int v = 0; v < 3; v++)
                 #pragma unroll
-                for (int v = 0; v < 3; v++)
+                for (int dy = 0; dy < 2; dy++) {
+                    const uint32_t (&hw)[3] = v == 0 ? hA[dy] : v == 1 ? hB[dy] : hC[dy];
+                    uint32_t hb[10];
                     #pragma unroll
-                    for (int dy = 0; dy < 2; dy++)
+                    for (int t = 0; t < 10; t++) hb[t] = hbyte(hw, t);
+                    #pragma unroll
+                    for (int e = 0; e < 8; e++)
                         #pragma unroll
-                        for (int u = 0; u < 3; u++) {
-                            const uint32_t h4 = hbyte(v == 0 ? hA[dy] : v == 1 ? hB[dy] : hC[dy], e + u);
-                            acc = __fadd_rn(acc, *reinterpret_cast<const float *>(tcb + ((u * 3 + v) * 2 + dy) * 64 + h4));
-                        }
-                S[e] = acc;
-            }
+                        for (int u = 0; u < 3; u++)
+                            S[e] = __fadd_rn(S[e], *reinterpret_cast<const float *>(tcb + ((u * 3 + v) * 2 + dy) * 64 + hb[e + u]));
+                }
             // horizontal blur over columns i-4 .. i+4 (periodic in 256 = the warp's 32 lanes x 8)
             float X[16];
             #pragma unroll
@@ -275,15 +279,20 @@ k_pregate(const Oct *__restrict__ oct, const uint64_t *__restrict__ seeds, const
     }
 }
 
-// Full gate (gate.cuh stream_max<512,7,8,false>).  Cluster rank = noise side; thread = grid column.
-__global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(FG_THREADS, 2)
+// Full gate (gate.cuh stream_max<512,7,8,false>).  Cluster rank = noise side.  A thread owns 4 adjacent
+// columns of the 512^2 grid (128 threads = one row).  Rows stream in blocks of 8: the 4 corner hashes of a
+// lattice column are packed in one word, the samples go to shared memory once, the horizontal blur reads
+// them back as 128-bit vectors, and the vertical blur accumulates 14 pending FMA chains per column in
+// registers.
+constexpr int FG_COLS = 4;
+__global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(FG_THREADS, 4)
 k_fullgate(const Oct *__restrict__ oct, const uint64_t *__restrict__ seeds, const uint32_t *__restrict__ idx, const uint32_t *__restrict__ n_in,
            uint32_t cap_in, float thr, Taps tp, uint64_t *__restrict__ out_seed, float *__restrict__ out_amp, uint32_t *__restrict__ n_out,
            uint32_t cap_out, float *__restrict__ side_amp) {
     __shared__ __align__(16) float sTc[512];
     __shared__ __align__(16) uint8_t sP2[512];
     __shared__ __align__(16) uint8_t sCol[2][256];
-    __shared__ __align__(16) uint8_t sHk[FG_RB][4][256];
+    __shared__ __align__(16) uint32_t sHk[FG_RB][256];     // byte q = dy*2 + dz: hash of corner (dy, dz)
     __shared__ __align__(16) float sV[FG_RB][512];
     __shared__ float sRed[FG_THREADS / 32];
     __shared__ float sPeer[2];
@@ -302,13 +311,15 @@ k_fullgate(const Oct *__restrict__ oct, const uint64_t *__restrict__ seeds, cons
         const double ox = p.ox, oz = p.oz, fy = p.fy, vy = p.vy;
         const int iy = p.iy;
         __syncthreads();
-        if (tid < 256) {
-            const int pc = sP2[tid];
-            sCol[0][tid] = sP2[pc + (iy & 255)];
-            sCol[1][tid] = sP2[pc + ((iy + 1) & 255)];
+        #pragma unroll
+        for (int h = 0; h < 2; h++) {
+            const int c = tid + 128 * h, pc = sP2[c];
+            sCol[0][c] = sP2[pc + (iy & 255)];
+            sCol[1][c] = sP2[pc + ((iy + 1) & 255)];
         }
-        {   // corner tables per parity (gate.cuh:237-244): Tc[(px*2+pz)*128 + c*16 + h]
-            const int e = tid, par = e >> 7, c = (e >> 4) & 7, h = e & 15, px = par >> 1, pz = par & 1;
+        #pragma unroll
+        for (int m = 0; m < 4; m++) {   // corner tables per parity (gate.cuh:237-244): Tc[(px*2+pz)*128 + c*16 + h]
+            const int e = tid + 128 * m, par = e >> 7, c = (e >> 4) & 7, h = e & 15, px = par >> 1, pz = par & 1;
             const double bx = px * 0.5 + ox, bz = pz * 0.5 + oz;
             const double fx = bx - floor(bx), fz = bz - floor(bz), tx = fade_fused(fx), tz = fade_fused(fz);
             const int dx = c & 1, dy = (c >> 1) & 1, dz = c >> 2;
@@ -317,49 +328,69 @@ k_fullgate(const Oct *__restrict__ oct, const uint64_t *__restrict__ seeds, cons
         }
         const int ix0a = int(floor(ox)), ix0b = int(floor(0.5 + ox)), iz0a = int(floor(oz)), iz0b = int(floor(0.5 + oz));
         __syncthreads();
-        // per-thread constants: hash column c and its two col values (dz = tid>>8 fixed, dy = 0/1 alternate)
-        const int hc = tid & 255, hdz = tid >> 8;
-        const int col0 = sCol[0][hc], col1 = sCol[1][hc];
-        const int px = tid & 1, ixp = (tid >> 1) + (px ? ix0b : ix0a);
-        float pend[14];
+        const int ca0 = sCol[0][tid], ca1 = sCol[0][tid + 128], cb0 = sCol[1][tid], cb1 = sCol[1][tid + 128];
+        const int lxa = 2 * tid + ix0a, lxb = 2 * tid + ix0b;    // lattice column of grid columns 4t (px 0) and 4t+1 (px 1)
+        float pend[14][FG_COLS];
         #pragma unroll
-        for (int j = 0; j < 14; j++) pend[j] = 0.f;
+        for (int j = 0; j < 14; j++)
+            #pragma unroll
+            for (int e = 0; e < FG_COLS; e++) pend[j][e] = 0.f;
         float best = -1e9f;
         for (int r0 = -7; r0 <= 518; r0 += FG_RB) {
-            // hashes of rows r0 .. r0+7: sHk[k][q][c], q = dy*2 + dz
             #pragma unroll
             for (int k = 0; k < FG_RB; k++) {
-                const int j = (r0 + k) & 511, pz = j & 1, iz = (j >> 1) + (pz ? iz0b : iz0a);
-                const int zz = (iz + hdz) & 255;
-                sHk[k][hdz][hc] = sP2[col0 + zz] & 15;            // q = 0*2 + hdz
-                sHk[k][2 + hdz][hc] = sP2[col1 + zz] & 15;        // q = 1*2 + hdz
+                const int j = (r0 + k) & 511, iz = (j >> 1) + ((j & 1) ? iz0b : iz0a);
+                const int z0 = iz & 255, z1 = (iz + 1) & 255;
+                sHk[k][tid] = uint32_t(sP2[ca0 + z0] & 15) | uint32_t(sP2[ca0 + z1] & 15) << 8 |
+                              uint32_t(sP2[cb0 + z0] & 15) << 16 | uint32_t(sP2[cb0 + z1] & 15) << 24;
+                sHk[k][tid + 128] = uint32_t(sP2[ca1 + z0] & 15) | uint32_t(sP2[ca1 + z1] & 15) << 8 |
+                                    uint32_t(sP2[cb1 + z0] & 15) << 16 | uint32_t(sP2[cb1 + z1] & 15) << 24;
             }
             __syncthreads();
             #pragma unroll
             for (int k = 0; k < FG_RB; k++) {
-                const int j = (r0 + k) & 511, pz = j & 1;
-                const float *T = sTc + (px * 2 + pz) * 128;
-                float acc = 0.f;
+                const int pz = (r0 + k) & 1;
+                const uint32_t wa0 = sHk[k][lxa & 255], wa1 = sHk[k][(lxa + 1) & 255], wa2 = sHk[k][(lxa + 2) & 255];
+                const uint32_t wb0 = sHk[k][lxb & 255], wb1 = sHk[k][(lxb + 1) & 255], wb2 = sHk[k][(lxb + 2) & 255];
+                float S[FG_COLS];
                 #pragma unroll
-                for (int c = 0; c < 8; c++) {
-                    const int dx = c & 1, q = ((c >> 1) & 1) * 2 + (c >> 2);
-                    acc = __fadd_rn(acc, T[c * 16 + sHk[k][q][(ixp + dx) & 255]]);
+                for (int e = 0; e < FG_COLS; e++) {
+                    const int px = e & 1;
+                    const float *T = sTc + (px * 2 + pz) * 128;
+                    const uint32_t w0 = px ? ((e >> 1) ? wb1 : wb0) : ((e >> 1) ? wa1 : wa0);
+                    const uint32_t w1 = px ? ((e >> 1) ? wb2 : wb1) : ((e >> 1) ? wa2 : wa1);
+                    float acc = 0.f;
+                    #pragma unroll
+                    for (int c = 0; c < 8; c++) {
+                        const int dx = c & 1, q = ((c >> 1) & 1) * 2 + (c >> 2);
+                        acc = __fadd_rn(acc, T[c * 16 + (((dx ? w1 : w0) >> (8 * q)) & 15)]);
+                    }
+                    S[e] = acc;
                 }
-                sV[k][tid] = acc;
+                *reinterpret_cast<float4 *>(&sV[k][FG_COLS * tid]) = make_float4(S[0], S[1], S[2], S[3]);
             }
             __syncthreads();
             #pragma unroll
             for (int k = 0; k < FG_RB; k++) {
                 const int r = r0 + k;
                 if (r > 518) break;
-                float hv = __fmaf_rn(tp.k15[0], sV[k][(tid - 7) & 511], 0.f);
+                float X[20];                                 // columns 4t-8 .. 4t+11 (periodic)
                 #pragma unroll
-                for (int d = 1; d < 15; d++) hv = __fmaf_rn(tp.k15[d], sV[k][(tid + d - 7) & 511], hv);
-                const float done = __fmaf_rn(tp.k15[14], hv, pend[0]);
+                for (int m = 0; m < 5; m++) {
+                    const float4 v = *reinterpret_cast<const float4 *>(&sV[k][(FG_COLS * tid - 8 + 4 * m) & 511]);
+                    X[4 * m] = v.x; X[4 * m + 1] = v.y; X[4 * m + 2] = v.z; X[4 * m + 3] = v.w;
+                }
                 #pragma unroll
-                for (int j = 1; j < 14; j++) pend[j - 1] = __fmaf_rn(tp.k15[14 - j], hv, pend[j]);
-                pend[13] = __fmaf_rn(tp.k15[0], hv, 0.f);
-                if (r >= 7) best = fmaxf(best, __fmul_rn(done, tp.norm15));
+                for (int e = 0; e < FG_COLS; e++) {
+                    float hv = __fmaf_rn(tp.k15[0], X[e + 1], 0.f);
+                    #pragma unroll
+                    for (int d = 1; d < 15; d++) hv = __fmaf_rn(tp.k15[d], X[e + 1 + d], hv);
+                    const float done = __fmaf_rn(tp.k15[14], hv, pend[0][e]);
+                    #pragma unroll
+                    for (int j = 1; j < 14; j++) pend[j - 1][e] = __fmaf_rn(tp.k15[14 - j], hv, pend[j][e]);
+                    pend[13][e] = __fmaf_rn(tp.k15[0], hv, 0.f);
+                    if (r >= 7) best = fmaxf(best, __fmul_rn(done, tp.norm15));
+                }
             }
             __syncthreads();
         }
@@ -566,3 +597,53 @@ int run_device_batch(cudaStream_t st, uint64_t start, uint64_t nb, const dsg_gat
     return DSG_OK;
 }
 }}
+
+// Benchmark hook: `warmup` untimed batches, then `steps` timed batches of `per_step` seed indices each
+// (fresh ranges), timed with CUDA events on the gate's own stream.  ms_kernel[0..3] = summed device time
+// of the phase, octave-init, pre-gate and full-gate kernels; counts = summed {indices, phase, pre, full}.
+extern "C" int dsg_gate_bench(uint64_t start, uint64_t per_step, uint32_t steps, uint32_t warmup, const dsg_gate_cfg *cfg,
+                              float *ms_total, float ms_kernel[4], uint64_t counts[4]) {
+    return guarded([&] {
+        DSG_ARG(cfg && ms_total && ms_kernel && counts && per_step > 0, "dsg_gate_bench: bad arguments");
+        State &g = S(); std::lock_guard<std::mutex> l(g.mu); setup_locked(g);
+        ensure_buffers(g, per_step);
+        const uint32_t total = warmup + steps;
+        std::vector<cudaEvent_t> ev(size_t(steps) * 5 + 2);
+        for (auto &e : ev) DSG_CU(cudaEventCreate(&e));
+        uint32_t *h_cnt = nullptr;
+        DSG_CU(cudaMallocHost(&h_cnt, size_t(total) * 16));
+        const dsg_gate_cfg c = *cfg;
+        const unsigned pb = unsigned(std::min<uint64_t>((per_step + 255) / 256, uint64_t(device_info().sms) * 64));
+        for (uint32_t it = 0; it < total; it++) {
+            const bool timed = it >= warmup;
+            const uint32_t k = it - warmup;
+            if (timed && k == 0) DSG_CU(cudaEventRecord(ev[0], g.st));
+            DSG_CU(cudaMemsetAsync(g.d_n, 0, 16, g.st));
+            if (timed) DSG_CU(cudaEventRecord(ev[2 + 5 * k], g.st));
+            k_phase<<<pb, 256, 0, g.st>>>(start + uint64_t(it) * per_step, per_step, double(c.maxph), g.d_s1, g.d_n, g.cap1);
+            if (timed) DSG_CU(cudaEventRecord(ev[3 + 5 * k], g.st));
+            k_octinit<<<unsigned(device_info().sms) * 16, 128, 0, g.st>>>(g.d_s1, g.d_n, g.cap1, g.d_oct);
+            if (timed) DSG_CU(cudaEventRecord(ev[4 + 5 * k], g.st));
+            k_pregate<<<g.pg_blocks, PG_THREADS, 0, g.st>>>(g.d_oct, g.d_s1, g.d_n, g.cap1, c.pthr, g.taps, g.d_s2, g.d_idx2, g.d_n + 1, g.cap2, nullptr);
+            if (timed) DSG_CU(cudaEventRecord(ev[5 + 5 * k], g.st));
+            k_fullgate<<<g.fg_blocks, FG_THREADS, 0, g.st>>>(g.d_oct, g.d_s2, g.d_idx2, g.d_n + 1, g.cap2, c.amp, g.taps, g.d_s3, g.d_a3, g.d_n + 2, g.cap3, nullptr);
+            if (timed) DSG_CU(cudaEventRecord(ev[6 + 5 * k], g.st));
+            DSG_CU(cudaGetLastError());
+            DSG_CU(cudaMemcpyAsync(h_cnt + 4 * it, g.d_n, 16, cudaMemcpyDeviceToHost, g.st));
+        }
+        DSG_CU(cudaEventRecord(ev[1], g.st));
+        DSG_CU(cudaStreamSynchronize(g.st));
+        DSG_CU(cudaEventElapsedTime(ms_total, ev[0], ev[1]));
+        for (int q = 0; q < 4; q++) ms_kernel[q] = 0;
+        for (uint32_t k = 0; k < steps; k++)
+            for (int q = 0; q < 4; q++) { float t; DSG_CU(cudaEventElapsedTime(&t, ev[2 + 5 * k + q], ev[3 + 5 * k + q])); ms_kernel[q] += t; }
+        for (int q = 0; q < 4; q++) counts[q] = 0;
+        for (uint32_t k = 0; k < steps; k++) {
+            counts[0] += per_step;
+            for (int q = 0; q < 3; q++) counts[1 + q] += h_cnt[4 * (warmup + k) + q];
+        }
+        cudaFreeHost(h_cnt);
+        for (auto &e : ev) cudaEventDestroy(e);
+        return DSG_OK;
+    });
+}

@@ -73,9 +73,9 @@ __device__ inline int tree_classify(const WorldDev &w, const int64_t *v) {
         if ((w.tree[node] >> 56) == 255) {
             const uint64_t d = box_dist(w, node, v);
             if (d < bestd) { bestd = d; best = node; }
-        } else {
+        } else if (sp < 8) {                       // tree depth is 6; the bound only guards the array
             int stride, lv = level;
-            do { stride = w.strides[lv++]; } while (node + stride >= w.ntree);
+            do { stride = w.strides[lv & 7]; lv++; } while (node + stride >= w.ntree && lv < 8);
             stk[sp++] = {node, lv, int(w.tree[node] >> 48), stride, 0};
         }
         // advance the innermost frame to its next child that passes the prune test
@@ -112,7 +112,8 @@ __device__ inline float spline_eval(const WorldDev &w, const float *v) {
             const float x = v[s.axis];
             int hi = 0;
             while (hi < s.n && x > s.knot[hi]) hi++;
-            if (hi == 0 || hi == s.n) {
+            if (sp >= 8) { ret = s.value; }            // spline depth is 4; the bound only guards the array
+            else if (hi == 0 || hi == s.n) {
                 const int j = hi == 0 ? 0 : s.n - 1;
                 stk[sp++] = {node, j, 0, x, 0.f, 0.f, 0.f};      // stage 0: extrapolate from child j
                 node = s.kid[j]; pushed = true;

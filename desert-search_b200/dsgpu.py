@@ -118,3 +118,68 @@ def flood_batch(reqs):
 
 def flood(seed, qx, qz, step, half, conn8=False, pred=PRED_DESERT, pcut=0.35):
     return flood_batch([flood_req(seed, qx, qz, step, half, conn8, pred, pcut)])[0]
+
+
+def gate_bench(start, per_step, steps, warmup, maxph=0.06, pthr=0.645, amp=0.70):
+    """Device-timed gate batches: (ms_total, ms per kernel [phase, init, pre, full], counts)."""
+    cfg = GateCfg(maxph, pthr, amp, 0)
+    ms = C.c_float(); mk = np.zeros(4, dtype=np.float32); counts = np.zeros(4, dtype=np.uint64)
+    _ck(lib.dsg_gate_bench(C.c_uint64(start), C.c_uint64(per_step), C.c_uint32(steps), C.c_uint32(warmup), C.byref(cfg),
+                           C.byref(ms), ptr(mk, f32p), ptr(counts, u64p)), "dsg_gate_bench")
+    return ms.value, mk, counts
+
+
+CAND_DTYPE = np.dtype([("s", "<f4"), ("t", "<f4"), ("c", "<f4"), ("e", "<f4"), ("x", "<i4"), ("z", "<i4")])
+TABIN_BYTES = 256 + 512 + 2 * 2 * 8 * 16 * 4 + 16
+
+
+class ScanParams(C.Structure):
+    _fields_ = [("ta", C.c_float), ("tt", C.c_float), ("wc", C.c_float), ("we", C.c_float)]
+
+
+def scan_init(ibT, loT, hiT, ibC, kernT, kernC, cell=512, period=262144, kmin=-30):
+    ibT = np.ascontiguousarray(ibT, dtype=np.int16); ibC = np.ascontiguousarray(ibC, dtype=np.int16)
+    loT = np.ascontiguousarray(loT, dtype=np.int8); hiT = np.ascontiguousarray(hiT, dtype=np.int8)
+    kT = np.ascontiguousarray(kernT, dtype=np.float32); kC = np.ascontiguousarray(kernC, dtype=np.float32)
+    _ck(lib.dsg_scan_init(ibT.ctypes.data_as(C.c_void_p), loT.ctypes.data_as(C.c_void_p), hiT.ctypes.data_as(C.c_void_p),
+                          ibC.ctypes.data_as(C.c_void_p), C.c_int(ibT.shape[1]), ptr(kT, f32p), C.c_int(len(kT) // 2),
+                          ptr(kC, f32p), C.c_int(len(kC) // 2), C.c_int(cell), C.c_int(period), C.c_int(kmin)), "dsg_scan_init")
+
+
+def tables(tabins):
+    """Blurred tables (n, 6, 512, 512) and maxima (n, 2) of n seeds' TabIn bytes (n * 6 * TABIN_BYTES)."""
+    t = np.ascontiguousarray(tabins, dtype=np.uint8)
+    n = t.size // (6 * TABIN_BYTES)
+    out = np.empty((n, 6, 512, 512), dtype=np.float32); mx = np.empty((n, 2), dtype=np.float32)
+    _ck(lib.dsg_tables(t.ctypes.data_as(C.c_void_p), C.c_uint32(n), ptr(out, f32p), ptr(mx, f32p)), "dsg_tables")
+    return out, mx
+
+
+def scan_batch(tabins, ta=0.25, tt=0.55, wc=0.25, we=0.41, cap=1 << 18):
+    """Per seed: (maxta, maxtb, raw candidate array).  Raises on overflow."""
+    t = np.ascontiguousarray(tabins, dtype=np.uint8)
+    n = t.size // (6 * TABIN_BYTES)
+    sp = ScanParams(ta, tt, wc, we)
+    mx = np.empty((n, 2), dtype=np.float32); out = np.empty(n * cap, dtype=CAND_DTYPE); cnt = np.empty(n, dtype=np.uint32)
+    rc = _ck(lib.dsg_scan_batch(t.ctypes.data_as(C.c_void_p), C.c_uint32(n), C.byref(sp), ptr(mx, f32p), out.ctypes.data_as(C.c_void_p),
+                                C.c_uint32(cap), ptr(cnt, u32p)), "dsg_scan_batch")
+    if rc != DSG_OK:
+        raise DsgError(f"dsg_scan_batch: rc={rc}")
+    return [(mx[s, 0], mx[s, 1], out[s * cap: s * cap + cnt[s]].copy()) for s in range(n)]
+
+
+class Zone(C.Structure):
+    _fields_ = [("x0", C.c_int32), ("z0", C.c_int32), ("nx", C.c_int32), ("nz", C.c_int32)]
+
+
+def proxy(seed, zones):
+    """Proxy bitmaps (list of (nz, nx) uint8 arrays) of (x0, z0, nx, nz) zones of one seed."""
+    zs = (Zone * len(zones))(*[Zone(*z) for z in zones])
+    total = sum(z[2] * z[3] for z in zones)
+    bits = np.zeros(max(total, 1), dtype=np.uint8)
+    _ck(lib.dsg_proxy(C.c_uint64(seed & ((1 << 64) - 1)), zs, C.c_uint32(len(zones)), bits.ctypes.data_as(C.c_void_p)), "dsg_proxy")
+    out, off = [], 0
+    for z in zones:
+        out.append(bits[off: off + z[2] * z[3]].reshape(z[3], z[2]))
+        off += z[2] * z[3]
+    return out

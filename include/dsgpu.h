@@ -58,6 +58,49 @@ int dsg_phase(const uint64_t *seeds, uint32_t n, double *phase, double *fy);
 /* Blur taps the gate kernels use (9 for sigma 1, then 15 for sigma 2), as computed on the device. */
 int dsg_gate_taps(float taps[24]);
 
+/* Timing hook (no reference counterpart; the reference prints kernel seconds on its gate progress line,
+ * src/gpu/gate.cuh:413): `warmup` untimed batches, then `steps` batches of `per_step` indices, timed with
+ * CUDA events on the gate's stream.  ms_kernel = summed device ms of the phase, octave-init, pre-gate and
+ * full-gate kernels; counts as dsg_gate_run. */
+int dsg_gate_bench(uint64_t start, uint64_t per_step, uint32_t steps, uint32_t warmup, const dsg_gate_cfg *cfg,
+                   float *ms_total, float ms_kernel[4], uint64_t counts[4]);
+
+/* ---------------------------------------------------------------- period tables + translation scan (S1-S2) */
+/* One octave-0 period table input, prepared as tab_setup does (src/lowfield.hpp:14-33); gproxy::TabIn
+ * (src/gpu/gproxy.h:26), same layout. */
+typedef struct dsg_tabin { uint8_t perm[256]; uint8_t col[2][256]; float T[2][2][8][16]; int32_t i0[2], k0[2]; } dsg_tabin;
+typedef struct dsg_scan_params { float ta, tt, wc, we; } dsg_scan_params;      /* gproxy::ScanParams (gproxy.h:27) */
+typedef struct dsg_cand { float s, t, c, e; int32_t x, z; } dsg_cand;          /* gproxy::RawCand (gproxy.h:28) */
+
+/* Translation maps (ib[i*nt + t], lo[i], hi[i], i < 512) for T and C/E, blur taps and the world lattice
+ * constants.  Replaces gproxy::scan_init (src/gpu/gproxy.h:30-31). */
+int dsg_scan_init(const int16_t *ibT, const int8_t *loT, const int8_t *hiT, const int16_t *ibC, int nt,
+                  const float *kernT, int rT, const float *kernC, int rC, int cell, int period, int kmin);
+/* Tables + blur + translation scan of one seed, tabs = {TA, TB, CA, CB, EA, EB}: maxima of the blurred
+ * TA/TB and the raw candidates (score >= tt), unordered.  Replaces gproxy::scan (src/gpu/gproxy.h:33);
+ * DSG_OVERFLOW where the reference returns false (more than `cap` candidates). */
+int dsg_scan(const dsg_tabin tabs[6], const dsg_scan_params *sp, float *maxta, float *maxtb, dsg_cand *out, uint32_t cap, uint32_t *n);
+/* The same for n seeds at once (tabs[6*s + k]); maxt[2s] = maxta, maxt[2s+1] = maxtb; seed s's candidates
+ * at out[s*cap], count n_out[s].  The batching the reference's scan_loop does across worker threads
+ * (src/gpu/gproxy.cu:221-281), made explicit. */
+int dsg_scan_batch(const dsg_tabin *tabs, uint32_t nseeds, const dsg_scan_params *sp, float *maxt, dsg_cand *out,
+                   uint32_t cap, uint32_t *n_out);
+/* The six blurred tables of n seeds (6*512*512 floats each, row-major, z outer) and maxta/maxtb; the
+ * gscancheck view (src/dsearch_desert.cpp:292-296). */
+int dsg_tables(const dsg_tabin *tabs, uint32_t nseeds, float *out, float *maxt);
+
+/* ---------------------------------------------------------------- low-octave proxy on zone grids (S4) */
+typedef struct dsg_zone { int32_t x0, z0, nx, nz; } dsg_zone;   /* gproxy::Zone (gproxy.h:22): origin in quarts, step-32 cells */
+
+/* Proxy bitmaps of a seed's zones: bits holds sum(nx*nz) bytes, zone after zone, each row-major with z
+ * outer; 1 = passable (probability >= the cut given to dsg_init).  FP64, so every cell equals the CPU
+ * proxy DesertProxy::prob (src/desert_proxy.hpp:24-32); replaces gproxy::evaluate (src/gpu/gproxy.h:37,
+ * FP32 there).  The seed itself is passed: the device derives its noise octaves. */
+int dsg_proxy(uint64_t seed, const dsg_zone *zones, uint32_t nzones, uint8_t *bits);
+/* Zones of several seeds in one launch: zone k belongs to seeds[zone_seed[k]]. */
+int dsg_proxy_batch(const uint64_t *seeds, uint32_t nseeds, const uint32_t *zone_seed, const dsg_zone *zones, uint32_t nzones,
+                    uint8_t *bits);
+
 /* ---------------------------------------------------------------- floods (S3 hot zones, S5 exact areas) */
 #define DSG_PRED_DESERT 0   /* bridged desert state at Y=256: desert counted, river to desert crossed (surface.hpp:98-124) */
 #define DSG_PRED_HOT    1   /* temperature >= 0.55, unwarped (dsearch_desert.cpp:334) */
@@ -78,6 +121,14 @@ typedef struct dsg_area {
     int32_t minx, maxx, minz, maxz;   /* quart bounds of counted cells (and the start) */
     int32_t edge, border;             /* reached the window edge / the world border */
 } dsg_area;
+
+/* Predicate values at explicit quart points: DSG_PRED_DESERT gives the bridged state 0/1/2 (desert_state,
+ * src/surface.hpp:98-124; 2 <=> SurfaceSampler::desert), DSG_PRED_HOT and DSG_PRED_PROXY give 0/2.
+ * xz = n (x, z) pairs.  The start-point searches of dsearch_desert.cpp:328-332,505-510 and dflood.cpp:16. */
+int dsg_points(uint64_t seed, int pred, float pcut, const int32_t *xz, uint32_t n, int8_t *out);
+/* Raw channel noise (0 T, 1 H, 2 C, 3 E, 4 shift, 5 W; both octave sides, final units) at n (x, y, z)
+ * triples: NormalNoise::sample (src/standalone.hpp:140-151), FP64. */
+int dsg_noise(uint64_t seed, int channel, const double *xyz, uint32_t n, double *out);
 
 /* Flood a batch of requests concurrently (any mix of seeds, steps, windows, predicates).  Results are
  * identical to dense_flood_bridged (src/dense_flood.hpp:52-86) run per request.  Replaces the CPU floods
