@@ -145,6 +145,30 @@ __global__ void __launch_bounds__(128) k_flood_level(const FloodCtl *__restrict_
     }
 }
 
+// Passable cells of each request (touched + passable bits), counted then listed.  One block per request.
+__global__ void k_cells(const FloodCtl *__restrict__ ctl, const int32_t *__restrict__ dir, const uint32_t *__restrict__ pool,
+                        unsigned long long *__restrict__ cnt, const unsigned long long *__restrict__ off, int32_t *__restrict__ xz, uint64_t cap) {
+    const uint32_t r = blockIdx.x;
+    const FloodCtl c = ctl[r];
+    const int64_t words = int64_t(c.tpr) * c.tpr * TILE_WORDS;
+    unsigned long long mine = 0;
+    for (int64_t e = threadIdx.x; e < words; e += blockDim.x) {
+        const int t = int(e / TILE_WORDS), wi = int(e % TILE_WORDS);
+        const int32_t d = dir[c.dir_off + t];
+        if (d < 0) continue;
+        uint32_t bits = pool[size_t(d) * TILE_WORDS + wi] & 0xAAAAAAAAu;     // passable bit of each 2-bit cell
+        if (!off) { mine += __popc(bits); continue; }
+        const int ti = t % c.tpr, tj = t / c.tpr, j = tj * TILE + (wi >> 2), i0 = ti * TILE + (wi & 3) * 16;
+        while (bits) {
+            const int b = __ffs(bits) - 1;
+            bits &= bits - 1;
+            const unsigned long long k = off[r] + atomicAdd(&cnt[r], 1ull);
+            if (k < cap) { xz[2 * k] = c.qx + (i0 + b / 2 - c.half) * c.step; xz[2 * k + 1] = c.qz + (j - c.half) * c.step; }
+        }
+    }
+    if (!off) atomicAdd(&cnt[r], mine);
+}
+
 // ---------------------------------------------------------------- host engine
 struct Engine {
     std::mutex mu;
@@ -192,7 +216,8 @@ template <class T> void grow(T *&p, uint32_t &cap, size_t need) {
 
 // Run a batch of requests to completion.  Returns DSG_OK, or DSG_OVERFLOW if the tile pool or a level list
 // ran out (the affected requests have overflow set and must be rerun with more memory).
-int run_batch(const dsg_flood_req *reqs, uint32_t n, dsg_area *out, size_t pool_bytes) {
+int run_batch(const dsg_flood_req *reqs, uint32_t n, dsg_area *out, size_t pool_bytes, uint64_t *cell_off = nullptr,
+              int32_t *cell_xz = nullptr, uint64_t cell_cap = 0) {
     Engine &g = E();
     std::lock_guard<std::mutex> l(g.mu);
     setup_locked(g);
@@ -258,6 +283,33 @@ int run_batch(const dsg_flood_req *reqs, uint32_t n, dsg_area *out, size_t pool_
     DSG_CU(cudaMemcpyAsync(hs.data(), g.d_stat, size_t(n) * sizeof(FloodStat), cudaMemcpyDeviceToHost, st));
     DSG_CU(cudaMemcpyAsync(flags, g.d_cnt, 8 * 4, cudaMemcpyDeviceToHost, st));
     DSG_CU(cudaStreamSynchronize(st));
+    int rc_cells = DSG_OK;
+    if (cell_off) {                                      // list passable cells before the tiles are cleared
+        unsigned long long *d_cnt = nullptr, *d_off = nullptr; int32_t *d_xz = nullptr;
+        std::vector<unsigned long long> cnt(n), offs(n + 1, 0);
+        auto fin = [&] { cudaFree(d_cnt); cudaFree(d_off); cudaFree(d_xz); };
+        try {
+            DSG_CU(cudaMalloc(&d_cnt, size_t(n) * 8)); DSG_CU(cudaMalloc(&d_off, size_t(n) * 8));
+            DSG_CU(cudaMemsetAsync(d_cnt, 0, size_t(n) * 8, st));
+            k_cells<<<n, 256, 0, st>>>(g.d_ctl, g.d_dir, g.d_pool, d_cnt, nullptr, nullptr, 0);
+            DSG_CU(cudaGetLastError());
+            DSG_CU(cudaMemcpyAsync(cnt.data(), d_cnt, size_t(n) * 8, cudaMemcpyDeviceToHost, st));
+            DSG_CU(cudaStreamSynchronize(st));
+            for (uint32_t r = 0; r < n; r++) offs[r + 1] = offs[r] + cnt[r];
+            for (uint32_t r = 0; r <= n; r++) cell_off[r] = offs[r];
+            if (offs[n] > cell_cap) { set_error("dsg_flood_batch_cells: %llu cells, capacity %llu", offs[n], (unsigned long long)cell_cap); rc_cells = DSG_OVERFLOW; }
+            else if (offs[n]) {
+                DSG_CU(cudaMalloc(&d_xz, size_t(offs[n]) * 8));
+                DSG_CU(cudaMemcpyAsync(d_off, offs.data(), size_t(n) * 8, cudaMemcpyHostToDevice, st));
+                DSG_CU(cudaMemsetAsync(d_cnt, 0, size_t(n) * 8, st));
+                k_cells<<<n, 256, 0, st>>>(g.d_ctl, g.d_dir, g.d_pool, d_cnt, d_off, d_xz, offs[n]);
+                DSG_CU(cudaGetLastError());
+                DSG_CU(cudaMemcpyAsync(cell_xz, d_xz, size_t(offs[n]) * 8, cudaMemcpyDeviceToHost, st));
+                DSG_CU(cudaStreamSynchronize(st));
+            }
+        } catch (...) { fin(); throw; }
+        fin();
+    }
     // return the tiles this batch used to the zeroed state
     DSG_CU(cudaMemsetAsync(g.d_pool, 0, size_t(std::min(flags[3], g.pool_cap)) * TILE_WORDS * 4, st));
     for (uint32_t r = 0; r < n; r++) {
@@ -270,7 +322,7 @@ int run_batch(const dsg_flood_req *reqs, uint32_t n, dsg_area *out, size_t pool_
         set_error("dsg_flood: %s exhausted (pool %u tiles, list %u entries)", (flags[4] & 1) ? "tile pool" : "level list", g.pool_cap, g.list_cap);
         return DSG_OVERFLOW;
     }
-    return DSG_OK;
+    return rc_cells;
 }
 }  // namespace flood
 }  // namespace dsg
@@ -287,3 +339,14 @@ extern "C" int dsg_flood_batch(const dsg_flood_req *reqs, uint32_t n, dsg_area *
     });
 }
 extern "C" int dsg_flood(const dsg_flood_req *req, dsg_area *out) { return dsg_flood_batch(req, 1, out); }
+
+extern "C" int dsg_flood_batch_cells(const dsg_flood_req *reqs, uint32_t n, dsg_area *out, uint64_t *off, int32_t *xz, uint64_t cap) {
+    return dsg::guarded([&] {
+        DSG_ARG(n == 0 || (reqs && out && off && (cap == 0 || xz)), "dsg_flood_batch_cells: null pointer");
+        if (!n) { if (off) off[0] = 0; return DSG_OK; }
+        size_t free_b = 0, total_b = 0;
+        DSG_CU(cudaMemGetInfo(&free_b, &total_b));
+        const size_t pool = std::min<size_t>(free_b / 4, size_t(16) << 30);
+        return dsg::flood::run_batch(reqs, n, out, pool, off, xz, cap);
+    });
+}

@@ -100,6 +100,8 @@ template <class T> const T *upload(const std::vector<T> &v) {
 }  // namespace
 
 const WorldDev &world_dev() { return g_world; }
+namespace { std::vector<float> g_prob; }
+const std::vector<float> &proxy_table() { return g_prob; }
 
 void world_upload(int) {
     const Blob b = parse_blob();
@@ -111,5 +113,15 @@ void world_upload(int) {
     w.ntree = int(b.tree.size()); w.nspl = int(b.spl.size());
     w.cells = upload(cells); w.tree = upload(b.tree); w.param = upload(b.param); w.spl = upload(b.spl); w.prob = upload(b.prob);
     g_world = w;
+    g_prob = b.prob;
 }
 }  // namespace dsg
+
+extern "C" int dsg_proxy_table(float prob[1600]) {
+    return dsg::guarded([&] {
+        dsg::require_init();
+        DSG_ARG(prob, "dsg_proxy_table: null pointer");
+        std::copy(dsg::proxy_table().begin(), dsg::proxy_table().end(), prob);
+        return DSG_OK;
+    });
+}

@@ -9,6 +9,7 @@
 #include <algorithm>
 #include <cmath>
 #include <cstdint>
+#include <unordered_map>
 #include <vector>
 
 namespace hostcheck {
@@ -226,5 +227,63 @@ inline float cpu_amp(uint64_t seed) {
         amp += m;
     }
     return amp;
+}
+}  // namespace hostcheck
+
+namespace hostcheck {
+// y-phase of temperature octave -10 and both fractional y offsets (dsearch_desert.cpp:80-94): RNG only.
+inline double phase(uint64_t seed, double *fy) {
+    Xoro w = Xoro::seeded(seed);
+    const uint64_t a = w.next(), b = w.next();
+    Xoro c{a ^ dsg::kTempA, b ^ dsg::kTempB};
+    double s = 0;
+    for (int side = 0; side < 2; side++) {
+        const uint64_t fa = c.next(), fb = c.next();
+        Xoro r{fa ^ dsg::kSalt10A, fb ^ dsg::kSalt10B};
+        r.next();
+        const double y = r.uniform() * 256.;
+        fy[side] = y - std::floor(y);
+        s += std::abs(fy[side] - .5);
+    }
+    return s;
+}
+}  // namespace hostcheck
+
+namespace hostcheck {
+// Translation maps for the CPU scan of gscancheck (the same arrays dsg_scan_init receives).
+struct ScanMaps { const int16_t *ibT = nullptr, *ibC = nullptr; const int8_t *lo = nullptr, *hi = nullptr; };
+inline ScanMaps &scan_maps() { static ScanMaps m; return m; }
+inline void scan_tmaps(const int16_t *ibT, const int8_t *lo, const int8_t *hi, const int16_t *ibC) { scan_maps() = {ibT, ibC, lo, hi}; }
+// CPU translation scan + best per NMS bucket in loop order (dsearch_desert.cpp:256-280).
+inline std::vector<dsg_cand> scan_buckets(const std::vector<float> *tab, double ta_, double t_, double wc_, double we_, int nms) {
+    const ScanMaps &m = scan_maps();
+    const int NTR = 60, CELLQ = 512, PER = 262144, KM = -30;
+    const float tt = float(t_), ta = float(ta_), wc = float(wc_), we = float(we_);
+    std::vector<dsg_cand> cand;
+    std::unordered_map<uint64_t, uint32_t> bucket;
+    auto key = [&](int x, int z) { return (uint64_t(uint32_t((x + 8000000) / nms)) << 32) | uint32_t((z + 8000000) / nms); };
+    const float *TA = tab[0].data(), *TB = tab[1].data(), *CA = tab[2].data(), *CB = tab[3].data(), *EA = tab[4].data(), *EB = tab[5].data();
+    for (int j = 0; j < TN; j++) for (int i = 0; i < TN; i++) {
+        const float sa = TA[j * TN + i];
+        if (sa < ta) continue;
+        const int ca = ((2 * j) & (TN - 1)) * TN + ((2 * i) & (TN - 1));
+        const float cA = CA[ca], eA = EA[ca];
+        for (int tz = m.lo[j]; tz <= m.hi[j]; tz++) {
+            const float *rT = TB + m.ibT[j * NTR + tz] * TN, *rC = CB + m.ibC[j * NTR + tz] * TN, *rE = EB + m.ibC[j * NTR + tz] * TN;
+            for (int tx = m.lo[i]; tx <= m.hi[i]; tx++) {
+                const float tv = sa + rT[m.ibT[i * NTR + tx]];
+                if (tv < tt - 0.3f) continue;
+                const int cb = m.ibC[i * NTR + tx];
+                const float cv = cA + rC[cb], ev = eA + rE[cb];
+                const float sc = tv + wc * cv + we * ev;
+                if (sc < tt) continue;
+                const int x = i * CELLQ + (tx + KM) * PER, z = j * CELLQ + (tz + KM) * PER;
+                auto [it, fresh] = bucket.try_emplace(key(x, z), uint32_t(cand.size()));
+                if (fresh) cand.push_back({sc, tv, cv, ev, x, z});
+                else if (sc > cand[it->second].s) cand[it->second] = {sc, tv, cv, ev, x, z};
+            }
+        }
+    }
+    return cand;
 }
 }  // namespace hostcheck

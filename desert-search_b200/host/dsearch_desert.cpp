@@ -1,0 +1,521 @@
+// dsearch_desert START COUNT OUT_PREFIX [THREADS] [key=value ...]: the whole-world desert searcher
+// (src/dsearch_desert.cpp) on the B200 engine.  Same CLI, Params keys and defaults, output files
+// (PREFIX.csv, PREFIX.seeds.csv, PREFIX.json; exclusive create), stderr lines (progress, best, CANDIDATE,
+// gscancheck, gpucheck) and exit codes, so deploy/gpipe.sh runs it unchanged with gate=1 gpu=1 gscan=1.
+//
+// Stage placement: every stage runs on the GPU through libdsgpu's C ABI; the host keeps the bookkeeping
+// the reference keeps on the host (NMS, hot-zone coverage, component labelling, result lines).  Seeds are
+// processed in batches: each stage is one batched call for all seeds of the batch, and where the
+// reference's per-seed loop is sequential (a site is skipped if an earlier site's hot zone covers it; a
+// later exact-flood start is tried only if the earlier ones fell short) the GPU evaluates every candidate
+// speculatively and the host replays the reference's sequential decisions over the results, so the output
+// is what the reference's loop computes.  gpu=0 (the reference's CPU-only search) and study=1 are not part
+// of this build; gscan=0 runs the tables and scan on the GPU anyway (bit-identical to the CPU path).
+#include "dsgpu.h"
+#include "cpu_check.hpp"
+#include <algorithm>
+#include <array>
+#include <atomic>
+#include <chrono>
+#include <cmath>
+#include <condition_variable>
+#include <csignal>
+#include <cstdio>
+#include <cstring>
+#include <deque>
+#include <mutex>
+#include <string>
+#include <thread>
+#include <unordered_map>
+#include <unordered_set>
+#include <vector>
+
+using Clock = std::chrono::steady_clock;
+static volatile sig_atomic_t interrupted = 0;
+static void on_signal(int) { interrupted = 1; }
+
+constexpr double BS = 337.0 / 331.0;
+constexpr int WORLD = 7499996, PERIOD = 262144, NT = 60, KMIN = -30, CELL = 512, TN = 512;
+
+struct Params {                                    // dsearch_desert.cpp:50-78 (same keys and defaults)
+    double max_phase = 0.10, amp = 0.70, amp_margin = 0.01, sigma = 2.0, sigmac = 2.0, wc = 0.25, we = 0.41, t = 0.55, ta = 0.25;
+    int max_sites = 300;
+    double pcut = 0.35, hot_min = 180;
+    int multi = 1, exact_n = 2;
+    double exact_min = 75, hot_pre = 0.8, csv_min = 50;
+    int nms = 5000;
+    double refine_mb = 70, verify_mb = 80;
+    int study = 0, gpu = 0, gpucheck = 0, gscan = 0, gscancheck = 0, gate = 0;
+    double gate_phase = 0.06, gate_amp = 0.70, gate_pthr = 0.645;
+    int from_stdin = 0;
+};
+
+// A cell i of a side-A table translated by t periods -> B table cell (dsearch_desert.cpp:98-113).
+struct TMap {
+    int16_t ib[TN][NT]; int8_t lo[TN], hi[TN];
+    explicit TMap(double lat) {
+        for (int i = 0; i < TN; i++) {
+            lo[i] = NT; hi[i] = -1;
+            for (int t = 0; t < NT; t++) {
+                const long x = long(i) * CELL + long(t + KMIN) * PERIOD;
+                const bool ok = x >= -WORLD + 6000 && x <= WORLD - 6000;
+                double u = x * BS / lat; u -= std::floor(u / 256.0) * 256.0;
+                ib[i][t] = int16_t(int(u * (TN / 256.0) + 0.5) & (TN - 1));
+                if (ok) { lo[i] = int8_t(std::min<int>(lo[i], t)); hi[i] = int8_t(std::max<int>(hi[i], t)); }
+            }
+        }
+    }
+};
+
+struct Site { float s, t, c, e; int x, z; };
+struct Eval { size_t rank; int x, z; double proxy, s8 = -1, s4 = 0; bool edge = false; double hot = 0; std::vector<std::pair<int, int>> alt; bool nostart = false; };
+
+[[noreturn]] static void die(const char *what) { fprintf(stderr, "%s: %s\n", what, dsg_last_error()); fflush(nullptr); std::_Exit(3); }
+static void ck(int rc, const char *what) { if (rc < 0) die(what); }
+
+struct Search {
+    Params P;
+    uint64_t start = 0, count = 0;
+    int threads = 11;
+    FILE *out = nullptr, *sout = nullptr;
+    std::mutex mu;                                 // output files, best, stderr lines
+    double best = 0;
+    std::atomic<uint64_t> done{0}, passed{0}, scanned{0}, nsites{0}, nhot{0}, nbig{0};
+    double t_tab = 0, t_scan = 0, t_site = 0, t_proxy = 0, t_hot = 0, t_gpu = 0;
+    Clock::time_point begin = Clock::now(), last = begin;
+    int gscan_checks = 0;
+    std::vector<float> kT, kC; int rT = 0, rC = 0;
+    float prob[1600];
+
+    // ---- per-batch stages
+    void process(const std::vector<uint64_t> &seeds);
+};
+
+static uint64_t bucket_key(int x, int z, int nms) {
+    return (uint64_t(uint32_t((x + 8000000) / nms)) << 32) | uint32_t((z + 8000000) / nms);
+}
+static uint64_t hotkey(int x, int z) { return (uint64_t(uint32_t((x + 8000000) >> 7)) << 32) | uint32_t((z + 8000000) >> 7); }
+
+// CPU loop order of a raw candidate (j, i, tz, tx): the order the reference's scan loop meets it.
+static uint64_t scan_order(const dsg_cand &c) {
+    const int i = ((c.x % PERIOD) + PERIOD) % PERIOD / CELL, tx = int(std::floor(double(c.x) / PERIOD)) - KMIN;
+    const int j = ((c.z % PERIOD) + PERIOD) % PERIOD / CELL, tz = int(std::floor(double(c.z) / PERIOD)) - KMIN;
+    return (uint64_t(j) << 32) | (uint64_t(i) << 16) | (uint64_t(tz) << 8) | uint64_t(tx);
+}
+
+void Search::process(const std::vector<uint64_t> &seeds) {
+    const size_t n = seeds.size();
+    const auto t0 = Clock::now();
+    std::vector<std::array<double, 2>> fy(n);
+    for (size_t s = 0; s < n; s++) hostcheck::phase(seeds[s], fy[s].data());
+    // ---------------- S1-S2: tables + scan (dsearch_desert.cpp:228-281)
+    std::vector<dsg_tabin> tin(6 * n);
+    {
+        std::atomic<size_t> nx(0);
+        std::vector<std::thread> pool;
+        for (int t = 0; t < std::max(1, threads); t++)
+            pool.emplace_back([&] { for (size_t s; (s = nx++) < n;) hostcheck::seed_tabins(seeds[s], &tin[6 * s]); });
+        for (auto &t : pool) t.join();
+    }
+    const dsg_scan_params sp{float(P.ta), float(P.t), float(P.wc), float(P.we)};
+    uint32_t cap = 1u << 16;
+    std::vector<float> maxt(2 * n);
+    std::vector<dsg_cand> raw;
+    std::vector<uint32_t> nraw(n);
+    for (;;) {
+        raw.resize(size_t(cap) * n);
+        const int rc = dsg_scan_batch(tin.data(), uint32_t(n), &sp, maxt.data(), raw.data(), cap, nraw.data());
+        ck(rc, "gscan");
+        if (rc == DSG_OK) break;
+        cap *= 4;                                   // the reference falls back to the CPU here; the GPU simply retries larger
+    }
+    const auto t1 = Clock::now();
+    std::vector<std::vector<Site>> sites(n);
+    std::vector<size_t> ncand(n);
+    for (size_t s = 0; s < n; s++) {
+        const uint64_t seed = seeds[s];
+        std::vector<const dsg_cand *> rs(nraw[s]);
+        for (uint32_t k = 0; k < nraw[s]; k++) rs[k] = &raw[size_t(s) * cap + k];
+        std::sort(rs.begin(), rs.end(), [](const dsg_cand *a, const dsg_cand *b) { return scan_order(*a) < scan_order(*b); });
+        std::vector<Site> cand;
+        std::unordered_map<uint64_t, uint32_t> bucket;
+        for (const dsg_cand *r : rs) {                      // best per NMS bucket, first in CPU loop order on ties
+            auto [it, fresh] = bucket.try_emplace(bucket_key(r->x, r->z, P.nms), uint32_t(cand.size()));
+            if (fresh) cand.push_back({r->s, r->t, r->c, r->e, r->x, r->z});
+            else if (r->s > cand[it->second].s) cand[it->second] = {r->s, r->t, r->c, r->e, r->x, r->z};
+        }
+        if (gscan_checks > 0) {                             // gscancheck: the CPU path side by side (:292-296)
+            gscan_checks--;
+            std::vector<float> tab[6];
+            for (int k = 0; k < 6; k++) { hostcheck::tabulate(tin[6 * s + k], tab[k]); hostcheck::blur(tab[k], k < 2 ? kT : kC, k < 2 ? rT : rC); }
+            const float cmaxta = *std::max_element(tab[0].begin(), tab[0].end()), cmaxtb = *std::max_element(tab[1].begin(), tab[1].end());
+            const std::vector<dsg_cand> cc = hostcheck::scan_buckets(tab, P.ta, P.t, P.wc, P.we, P.nms);
+            long miss = 0;
+            for (auto &c : cc) { auto it = bucket.find(bucket_key(c.x, c.z, P.nms)); if (it == bucket.end() || cand[it->second].s != c.s) miss++; }
+            std::lock_guard<std::mutex> g(mu);
+            fprintf(stderr, "gscancheck seed %lld: maxta %.6f/%.6f maxtb %.6f/%.6f, buckets cpu %zu gpu %zu, mismatched %ld, raw %u\n",
+                    (long long)seed, cmaxta, maxt[2 * s], cmaxtb, maxt[2 * s + 1], cc.size(), cand.size(), miss, nraw[s]);
+        }
+        ncand[s] = cand.size();
+        std::sort(cand.begin(), cand.end(), [](auto &a, auto &b) { return a.s > b.s; });
+        for (auto &c : cand) {
+            bool near = false;
+            for (auto &q : sites[s]) if (std::abs(q.x - c.x) < P.nms && std::abs(q.z - c.z) < P.nms) { near = true; break; }
+            if (!near) sites[s].push_back(c);
+            if ((int)sites[s].size() >= P.max_sites) break;
+        }
+    }
+    scanned += n;
+    const auto t2 = Clock::now();
+    // ---------------- S3: hot zones (dsearch_desert.cpp:326-372)
+    struct Zone { size_t seed, rank; double hot; int x0, z0, nx, nz; };
+    std::vector<Zone> zones;
+    {
+        // hottest of 7x7 points at 256-quart spacing around every site (first strict maximum in dz, dx order)
+        std::vector<int32_t> xz; std::vector<uint32_t> ps;
+        for (size_t s = 0; s < n; s++)
+            for (const Site &st : sites[s])
+                for (int dz = -3; dz <= 3; dz++) for (int dx = -3; dx <= 3; dx++) { xz.push_back(st.x + dx * 256); xz.push_back(st.z + dz * 256); ps.push_back(uint32_t(s)); }
+        std::vector<double> tv(ps.size());
+        if (!ps.empty()) ck(dsg_query_batch(seeds.data(), uint32_t(n), ps.data(), 0, xz.data(), uint32_t(ps.size()), tv.data()), "hot-zone points");
+        struct Hot { size_t s, rank; int hx, hz; double bt; };
+        std::vector<Hot> hot;
+        size_t k = 0;
+        for (size_t s = 0; s < n; s++)
+            for (size_t r = 0; r < sites[s].size(); r++) {
+                const Site &st = sites[s][r];
+                Hot h{s, r, st.x, st.z, -9};
+                for (int q = 0; q < 49; q++, k++) if (tv[k] > h.bt) { h.bt = tv[k]; h.hx = st.x + (q % 7 - 3) * 256; h.hz = st.z + (q / 7 - 3) * 256; }
+                hot.push_back(h);
+            }
+        nsites += hot.size();
+        // speculative step-256 and step-128 hot floods of every site whose hottest point reaches 0.55
+        std::vector<dsg_flood_req> q256; std::vector<size_t> q256_of;
+        for (size_t h = 0; h < hot.size(); h++)
+            if (hot[h].bt >= 0.55 && P.hot_pre > 0) { q256.push_back({seeds[hot[h].s], hot[h].hx, hot[h].hz, 256, 32000 / 256, 0, DSG_PRED_HOT, 0.f, 0}); q256_of.push_back(h); }
+        auto flood_cells = [&](const std::vector<dsg_flood_req> &q, std::vector<dsg_area> &a, std::vector<uint64_t> &off, std::vector<int32_t> &cells) {
+            a.resize(q.size()); off.assign(q.size() + 1, 0);
+            uint64_t capc = std::max<uint64_t>(1 << 20, q.size() * 4096);
+            for (;;) {
+                cells.resize(2 * capc);
+                const int rc = q.empty() ? DSG_OK : dsg_flood_batch_cells(q.data(), uint32_t(q.size()), a.data(), off.data(), cells.data(), capc);
+                ck(rc, "hot-zone flood");
+                if (rc == DSG_OK) return;
+                capc = off.back() + 1;
+            }
+        };
+        const auto th0 = Clock::now();
+        std::vector<dsg_area> a256; std::vector<uint64_t> o256; std::vector<int32_t> c256;
+        flood_cells(q256, a256, o256, c256);
+        std::vector<int> big(hot.size(), P.hot_pre > 0 ? 0 : 1);
+        std::vector<long> idx256(hot.size(), -1);
+        for (size_t k2 = 0; k2 < q256.size(); k2++) {
+            idx256[q256_of[k2]] = long(k2);
+            if (a256[k2].cells * 256.0 * 256 * 16 / 1e6 >= P.hot_pre * P.hot_min) big[q256_of[k2]] = 1;
+        }
+        std::vector<dsg_flood_req> q128; std::vector<long> idx128(hot.size(), -1);
+        for (size_t h = 0; h < hot.size(); h++)
+            if (hot[h].bt >= 0.55 && big[h]) { idx128[h] = long(q128.size()); q128.push_back({seeds[hot[h].s], hot[h].hx, hot[h].hz, 128, 32000 / 128, 0, DSG_PRED_HOT, 0.f, 0}); }
+        std::vector<dsg_area> a128; std::vector<uint64_t> o128; std::vector<int32_t> c128;
+        flood_cells(q128, a128, o128, c128);
+        t_hot += std::chrono::duration<double>(Clock::now() - th0).count();
+        // replay the reference's sequential site loop per seed
+        size_t h = 0;
+        for (size_t s = 0; s < n; s++) {
+            std::unordered_set<uint64_t> hotcovered;
+            for (size_t r = 0; r < sites[s].size(); r++, h++) {
+                const Hot &ht = hot[h];
+                if (ht.bt < 0.55 || hotcovered.count(hotkey(ht.hx, ht.hz))) continue;
+                if (P.hot_pre > 0 && !big[h]) {                 // small pre-flood: cover its cells (4 sub-keys each)
+                    const long k2 = idx256[h];
+                    for (uint64_t c = o256[k2]; c < o256[k2 + 1]; c++)
+                        for (int d = 0; d < 4; d++) hotcovered.insert(hotkey(c256[2 * c] + (d & 1) * 128, c256[2 * c + 1] + (d >> 1) * 128));
+                    nhot++;
+                    continue;
+                }
+                const long k2 = idx128[h];
+                const dsg_area &hz = a128[k2];
+                const double hot_area = hz.cells * 128.0 * 128 * 16 / 1e6;
+                for (uint64_t c = o128[k2]; c < o128[k2 + 1]; c++) hotcovered.insert(hotkey(c128[2 * c], c128[2 * c + 1]));
+                nhot++;
+                if (hot_area < P.hot_min) continue;
+                nbig++;
+                const int x0 = int(std::floor((hz.minx - 128) / 32.0)) * 32, z0 = int(std::floor((hz.minz - 128) / 32.0)) * 32;
+                zones.push_back({s, r, hot_area, x0, z0, (hz.maxx + 128 - x0) / 32 + 1, (hz.maxz + 128 - z0) / 32 + 1});
+            }
+        }
+    }
+    // ---------------- S4: proxy bitmaps + components (dsearch_desert.cpp:425-492)
+    std::vector<std::vector<Eval>> ev(n);
+    const auto tp0 = Clock::now();
+    if (!zones.empty()) {
+        std::vector<dsg_zone> dz; std::vector<uint32_t> zs; size_t total = 0;
+        for (auto &z : zones) { dz.push_back({z.x0, z.z0, z.nx, z.nz}); zs.push_back(uint32_t(z.seed)); total += size_t(z.nx) * z.nz; }
+        std::vector<uint8_t> bits(total);
+        const auto tg0 = Clock::now();
+        ck(dsg_proxy_batch(seeds.data(), uint32_t(n), zs.data(), dz.data(), uint32_t(dz.size()), bits.data()), "gproxy");
+        t_gpu += std::chrono::duration<double>(Clock::now() - tg0).count();
+        size_t off = 0;
+        std::vector<std::vector<std::pair<int, int>>> seen(n);
+        for (auto &zn : zones) {
+            uint8_t *b = &bits[off];
+            off += size_t(zn.nx) * zn.nz;
+            if (P.gpucheck > 0) {                           // spot-check every 7th cell against the CPU proxy (:445-450)
+                const hostcheck::Proxy PX(seeds[zn.seed], prob);
+                long diff = 0, tot = 0;
+                for (int c = 0; c < zn.nx * zn.nz; c += 7) { tot++; diff += (PX.p(zn.x0 + (c % zn.nx) * 32, zn.z0 + (c / zn.nx) * 32) >= float(P.pcut)) != (b[c] != 0); }
+                std::lock_guard<std::mutex> g(mu);
+                fprintf(stderr, "gpucheck zone %dx%d: %ld/%ld cells differ\n", zn.nx, zn.nz, diff, tot);
+                P.gpucheck--;
+            }
+            for (int c0 = 0; c0 < zn.nx * zn.nz; c0++) {       // 8-connected components
+                if (b[c0] != 1) continue;
+                long cells = 0; int mx = zn.nx, mz = zn.nz;
+                std::vector<int> stk{c0}, comp; b[c0] = 2;
+                while (!stk.empty()) {
+                    const int c = stk.back(); stk.pop_back(); cells++; comp.push_back(c);
+                    const int cx = c % zn.nx, cz = c / zn.nx;
+                    mx = std::min(mx, cx); mz = std::min(mz, cz);
+                    for (int dzz = -1; dzz <= 1; dzz++) for (int dxx = -1; dxx <= 1; dxx++) {
+                        const int nx2 = cx + dxx, nz2 = cz + dzz;
+                        if (nx2 < 0 || nz2 < 0 || nx2 >= zn.nx || nz2 >= zn.nz) continue;
+                        const int k2 = nz2 * zn.nx + nx2;
+                        if (b[k2] == 1) { b[k2] = 2; stk.push_back(k2); }
+                    }
+                }
+                const double area = cells * 32.0 * 32 * 16 / 1e6;
+                if (area < 1) continue;
+                const std::pair<int, int> sig(zn.x0 + mx * 32, zn.z0 + mz * 32);
+                auto &sn = seen[zn.seed];
+                if (std::find(sn.begin(), sn.end(), sig) != sn.end()) continue;
+                sn.push_back(sig);
+                double cx = 0, cz = 0;
+                for (int c : comp) { cx += c % zn.nx; cz += c / zn.nx; }
+                cx /= comp.size(); cz /= comp.size();
+                std::vector<std::pair<double, int>> inner;
+                for (int c : comp) {
+                    const int x = c % zn.nx, z = c / zn.nx;
+                    bool ok = x > 0 && z > 0 && x < zn.nx - 1 && z < zn.nz - 1;
+                    for (int dzz = -1; ok && dzz <= 1; dzz++) for (int dxx = -1; dxx <= 1; dxx++) if (b[(z + dzz) * zn.nx + x + dxx] != 2) { ok = false; break; }
+                    if (ok) inner.push_back({(x - cx) * (x - cx) + (z - cz) * (z - cz), c});
+                }
+                std::sort(inner.begin(), inner.end());
+                auto cell_xy = [&](int c) { return std::pair<int, int>(zn.x0 + (c % zn.nx) * 32, zn.z0 + (c / zn.nx) * 32); };
+                const auto first = inner.empty() ? cell_xy(c0) : cell_xy(inner[0].second);
+                Eval e{zn.rank, first.first, first.second, area};
+                e.hot = zn.hot;
+                for (int t = 1; t < 3 && size_t(t) * inner.size() / 3 < inner.size() && !inner.empty(); t++) e.alt.push_back(cell_xy(inner[size_t(t) * inner.size() / 3].second));
+                ev[zn.seed].push_back(e);
+            }
+        }
+    }
+    for (auto &e : ev) std::sort(e.begin(), e.end(), [](auto &a, auto &b) { return a.proxy > b.proxy; });
+    t_proxy += std::chrono::duration<double>(Clock::now() - tp0).count();
+    // ---------------- S5: exact floods (dsearch_desert.cpp:498-533)
+    struct Try { size_t s, k2, t; int sx, sz; int bx = 0, bz = 0; bool found = false; };
+    std::vector<Try> tries;
+    for (size_t s = 0; s < n; s++)
+        for (size_t k2 = 0; k2 < ev[s].size() && int(k2) < P.exact_n && ev[s][k2].proxy >= P.exact_min; k2++) {
+            const Eval &e = ev[s][k2];
+            tries.push_back({s, k2, 0, e.x, e.z});
+            for (size_t a = 0; a < e.alt.size(); a++) tries.push_back({s, k2, a + 1, e.alt[a].first, e.alt[a].second});
+        }
+    if (!tries.empty()) {
+        // nearest desert point to each start: rings r = 0..8 of 16 quarts, first in (r, dz, dx) order
+        std::vector<int32_t> xz; std::vector<uint32_t> ps;
+        std::vector<std::array<int, 3>> ring;
+        for (int r = 0; r <= 8; r++) for (int dz = -r; dz <= r; dz++) for (int dx = -r; dx <= r; dx++) if (std::max(std::abs(dx), std::abs(dz)) == r) ring.push_back({r, dx, dz});
+        for (auto &t : tries) for (auto &q : ring) { xz.push_back(t.sx + q[1] * 16); xz.push_back(t.sz + q[2] * 16); ps.push_back(uint32_t(t.s)); }
+        std::vector<double> st(ps.size());
+        ck(dsg_query_batch(seeds.data(), uint32_t(n), ps.data(), DSG_Q_STATE, xz.data(), uint32_t(ps.size()), st.data()), "exact start");
+        for (size_t k = 0; k < tries.size(); k++)
+            for (size_t q = 0; q < ring.size(); q++)
+                if (st[k * ring.size() + q] == 2) { tries[k].found = true; tries[k].bx = tries[k].sx + ring[q][1] * 16; tries[k].bz = tries[k].sz + ring[q][2] * 16; break; }
+        std::vector<dsg_flood_req> q8; std::vector<size_t> q8_of;
+        for (size_t k = 0; k < tries.size(); k++)
+            if (tries[k].found) { q8.push_back({seeds[tries[k].s], tries[k].bx, tries[k].bz, 8, 16000 / 8, 1, DSG_PRED_DESERT, 0.f, 0}); q8_of.push_back(k); }
+        std::vector<dsg_area> a8(q8.size());
+        if (!q8.empty()) ck(dsg_flood_batch(q8.data(), uint32_t(q8.size()), a8.data()), "step-8 flood");
+        std::vector<long> a8_of(tries.size(), -1);
+        for (size_t k = 0; k < q8.size(); k++) a8_of[q8_of[k]] = long(k);
+        // replay the retry loop (stop once a start reaches 0.6 x proxy), then step-4 refinements in one batch
+        std::vector<dsg_flood_req> q4; std::vector<std::pair<size_t, size_t>> q4_of;
+        for (size_t k = 0; k < tries.size();) {
+            const size_t s = tries[k].s, k2 = tries[k].k2;
+            Eval &e = ev[s][k2];
+            double best8 = -1; int bx = e.x, bz = e.z; bool bedge = false;
+            size_t j = k;
+            for (; j < tries.size() && tries[j].s == s && tries[j].k2 == k2; j++) {
+                if (best8 >= 0.6 * e.proxy) continue;               // loop already broke
+                if (!tries[j].found) continue;
+                const dsg_area &a = a8[a8_of[j]];
+                const double v8 = a.cells * 64.0 * 16 / 1e6;
+                if (v8 > best8) { best8 = v8; bx = tries[j].bx; bz = tries[j].bz; bedge = a.edge != 0; }
+            }
+            k = j;
+            if (best8 < 0) { e.s8 = 0; e.nostart = true; continue; }
+            e.x = bx; e.z = bz; e.s8 = best8; e.edge = bedge;
+            if (e.s8 >= P.refine_mb) { q4.push_back({seeds[s], bx, bz, 4, 16000 / 4, 0, DSG_PRED_DESERT, 0.f, 0}); q4_of.push_back({s, k2}); }
+        }
+        std::vector<dsg_area> a4(q4.size());
+        if (!q4.empty()) ck(dsg_flood_batch(q4.data(), uint32_t(q4.size()), a4.data()), "step-4 flood");
+        for (size_t k = 0; k < q4.size(); k++) {
+            Eval &e = ev[q4_of[k].first][q4_of[k].second];
+            e.s4 = a4[k].cells * 16.0 * 16 / 1e6; e.edge |= a4[k].edge != 0;
+        }
+    }
+    const auto t3 = Clock::now();
+    // ---------------- results (dsearch_desert.cpp:524-556)
+    std::lock_guard<std::mutex> g(mu);
+    for (size_t s = 0; s < n; s++) {
+        const long long seed = (long long)seeds[s];
+        double seed_best = 0;
+        for (size_t k2 = 0; !P.study && k2 < ev[s].size() && int(k2) < P.exact_n && ev[s][k2].proxy >= P.exact_min; k2++) {
+            const Eval &e = ev[s][k2];
+            if (e.nostart) continue;                       // no desert start near this component (:517)
+            const double v = e.s4 > 0 ? e.s4 : e.s8;
+            seed_best = std::max(seed_best, v);
+            if (e.s4 >= P.verify_mb)
+                fprintf(stderr, "CANDIDATE step4=%.2fM seed=%lld x=%d z=%d -> verify with exact flood (Y=256)\n", e.s4, seed, e.x * 4 + 2, e.z * 4 + 2);
+            if (v > best) {
+                best = v;
+                fprintf(stderr, "best %.2fM (step %d) seed=%lld x=%d z=%d proxy=%.1fM\n", v, e.s4 > 0 ? 4 : 8, seed, e.x * 4 + 2, e.z * 4 + 2, e.proxy);
+            }
+        }
+        for (auto &e : ev[s]) {
+            if (e.proxy < P.csv_min && e.s8 <= 0 && e.s4 <= 0) continue;
+            const Site &st = sites[s][e.rank];
+            fprintf(out, "%lld,%.4f,%.4f,%.4f,%.4f,%zu,%d,%d,%.4f,%.4f,%.4f,%.4f,%.3f,%.3f,%.3f,%d,%.1f\n", seed, fy[s][0], fy[s][1], maxt[2 * s], maxt[2 * s + 1],
+                    e.rank, e.x * 4 + 2, e.z * 4 + 2, st.s, st.t, st.c, st.e, e.proxy, e.s8, e.s4, int(e.edge), e.hot);
+        }
+        fprintf(sout, "%lld,%.4f,%.4f,%.4f,%.4f,%zu,%zu,%.3f\n", seed, fy[s][0], fy[s][1], maxt[2 * s], maxt[2 * s + 1], ncand[s], sites[s].size(), seed_best);
+    }
+    t_tab += std::chrono::duration<double>(t1 - t0).count();
+    t_scan += std::chrono::duration<double>(t2 - t1).count();
+    t_site += std::chrono::duration<double>(t3 - t2).count();
+    const auto now = Clock::now();
+    if (std::chrono::duration<double>(now - last).count() > 30) {
+        last = now; fflush(out); fflush(sout);
+        fprintf(stderr, "%llu seeds, %llu passed, %llu scanned, %llu sites; %.2f passed/s; core-s tables %.0f scan %.0f sites %.0f (proxy %.0f hot %.0f gpu %.0f); hot zones %llu, big %llu\n",
+                (unsigned long long)done.load(), (unsigned long long)passed.load(), (unsigned long long)scanned.load(), (unsigned long long)nsites.load(),
+                passed.load() / std::chrono::duration<double>(now - begin).count(), t_tab, t_scan, t_site, t_proxy, t_hot, t_gpu,
+                (unsigned long long)nhot.load(), (unsigned long long)nbig.load());
+    }
+}
+
+int main(int argc, char **argv) {
+    if (argc < 4) { fprintf(stderr, "dsearch_desert START COUNT OUT_PREFIX [threads] [key=value...]\n"); return 2; }
+    Search S;
+    S.start = std::stoull(argv[1]); S.count = std::stoull(argv[2]);
+    const std::string prefix = argv[3];
+    S.threads = argc > 4 ? std::stoi(argv[4]) : 11;
+    Params &P = S.P;
+    for (int i = 5; i < argc; i++) {                       // dsearch_desert.cpp:126-135
+        const std::string kv = argv[i]; const auto eq = kv.find('=');
+        const std::string k = kv.substr(0, eq); const double v = std::stod(kv.substr(eq + 1));
+        if (k == "gpu") P.gpu = int(v); else if (k == "gpucheck") P.gpucheck = int(v); else if (k == "stdin") P.from_stdin = int(v);
+        else if (k == "study") P.study = int(v); else if (k == "phase") P.max_phase = v; else if (k == "amp") P.amp = v;
+        else if (k == "amp_margin") P.amp_margin = v; else if (k == "sigma") P.sigma = v; else if (k == "sigmac") P.sigmac = v;
+        else if (k == "wc") P.wc = v; else if (k == "we") P.we = v; else if (k == "t") P.t = v; else if (k == "ta") P.ta = v;
+        else if (k == "sites") P.max_sites = int(v); else if (k == "nms") P.nms = int(v);
+        else if (k == "pcut") P.pcut = v; else if (k == "multi") P.multi = int(v); else if (k == "hot_min") P.hot_min = v;
+        else if (k == "exact_n") P.exact_n = int(v); else if (k == "exact_min") P.exact_min = v; else if (k == "csv_min") P.csv_min = v;
+        else if (k == "hot_pre") P.hot_pre = v; else if (k == "gate") P.gate = int(v); else if (k == "gscan") P.gscan = int(v);
+        else if (k == "gscancheck") P.gscancheck = int(v); else if (k == "gate_phase") P.gate_phase = v; else if (k == "gate_amp") P.gate_amp = v;
+        else if (k == "gate_pthr") P.gate_pthr = v; else if (k == "refine") P.refine_mb = v; else if (k == "verify") P.verify_mb = v;
+        else { fprintf(stderr, "unknown key %s\n", k.c_str()); return 2; }
+    }
+    if ((P.gscan || P.gscancheck) && !P.gpu) { fprintf(stderr, "gscan=1 needs gpu=1\n"); return 2; }
+    if (P.gate) {
+        if (!P.gpu) { fprintf(stderr, "gate=1 needs gpu=1\n"); return 2; }
+        P.from_stdin = 1;
+    }
+    if (!P.gpu) { fprintf(stderr, "gpu=0 selects the CPU-only search, which this B200 build does not provide: run with gpu=1 (gate=1 gscan=1)\n"); return 2; }
+    if (P.study) { fprintf(stderr, "study=1 is not provided by this build\n"); return 2; }
+    if (P.hot_min <= 0) { fprintf(stderr, "hot_min <= 0 (per-site proxy floods without hot zones) is not provided by this build\n"); return 2; }
+    S.out = fopen((prefix + ".csv").c_str(), "wx");
+    S.sout = fopen((prefix + ".seeds.csv").c_str(), "wx");
+    if (!S.out || !S.sout) { fprintf(stderr, "cannot create %s outputs (exist?)\n", prefix.c_str()); return 2; }
+    fprintf(S.out, "seed,fyA,fyB,maxta,maxtb,rank,x,z,score,t0,c0,e0,proxy,s8,s4,edge,hot\n");
+    fprintf(S.sout, "seed,fyA,fyB,maxta,maxtb,candidates,sites,best\n");
+    signal(SIGINT, on_signal); signal(SIGTERM, on_signal);
+    ck(dsg_init(0, float(P.pcut)), "dsg_init");
+    {
+        static TMap TMT(1024.0), TMC(512.0);
+        hostcheck::blur_taps(P.sigma, S.kT, S.rT); hostcheck::blur_taps(P.sigmac, S.kC, S.rC);
+        ck(dsg_scan_init(&TMT.ib[0][0], TMT.lo, TMT.hi, &TMC.ib[0][0], NT, S.kT.data(), S.rT, S.kC.data(), S.rC, CELL, PERIOD, KMIN), "scan_init");
+        hostcheck::scan_tmaps(&TMT.ib[0][0], TMT.lo, TMT.hi, &TMC.ib[0][0]);
+    }
+    ck(dsg_proxy_table(S.prob), "proxy table");
+    S.gscan_checks = P.gscancheck;
+    // ---- seed source: GPU gate thread, stdin reader, or the enumerated range through the GPU gate
+    std::mutex qmu; std::condition_variable qcv; std::deque<uint64_t> q; bool qdone = false;
+    auto push = [&](uint64_t sd) {
+        std::unique_lock<std::mutex> l(qmu);
+        qcv.wait(l, [&] { return q.size() < 20000 || interrupted; });   // backpressure on the gate
+        q.push_back(sd);
+        qcv.notify_all();
+    };
+    std::thread source;
+    if (P.from_stdin && !P.gate) {
+        source = std::thread([&] {
+            char line[256];
+            while (!interrupted && fgets(line, sizeof line, stdin)) push(std::strtoull(line, nullptr, 10));
+            std::lock_guard<std::mutex> l(qmu); qdone = true; qcv.notify_all();
+        });
+    } else {
+        // gate=1: the production GPU gate; without gate/stdin the enumerated range goes through the same gate
+        // with the CPU mode's phase cut (its sub-grid pre-gate is replaced by the anti-aliased one)
+        dsg_gate_cfg g{float(P.gate ? P.gate_phase : P.max_phase), float(P.gate_pthr), float(P.gate ? P.gate_amp : P.amp), 0};
+        const uint64_t total = (P.gate && S.count == 0) ? 100000000000000ULL : S.count;
+        source = std::thread([&, g, total] {
+            const uint64_t B = 1ull << 26;
+            std::vector<uint64_t> sd(1u << 20); std::vector<float> am(1u << 20);
+            uint64_t tot[4] = {0, 0, 0, 0};
+            const auto tg = Clock::now();
+            for (uint64_t base = 0; base < total && !interrupted; base += B) {
+                const uint64_t nb = std::min(B, total - base);
+                dsg_gate_cfg gb = g; gb.batch = uint32_t(nb);
+                uint32_t nn = 0; uint64_t c[4];
+                ck(dsg_gate_run(S.start + base, nb, &gb, sd.data(), am.data(), uint32_t(sd.size()), &nn, c), "gate");
+                for (int k = 0; k < 4; k++) tot[k] += c[k];
+                S.done += P.gate ? 0 : nb;
+                const double sec = std::chrono::duration<double>(Clock::now() - tg).count();
+                fprintf(stderr, "gate: %llu seeds, %llu phase-passed, %llu pre-gate, %llu passed; %.0f seeds/s, %.1f passed/s\n",
+                        (unsigned long long)(base + nb), (unsigned long long)tot[1], (unsigned long long)tot[2], (unsigned long long)tot[3],
+                        (base + nb) / sec, tot[3] / sec);
+                for (uint32_t i = 0; i < nn && !interrupted; i++) push(sd[i]);
+            }
+            std::lock_guard<std::mutex> l(qmu); qdone = true; qcv.notify_all();
+        });
+    }
+    // ---- batches of seeds through the stages
+    const size_t BATCH = 256;
+    for (;;) {
+        std::vector<uint64_t> batch;
+        {
+            std::unique_lock<std::mutex> l(qmu);
+            qcv.wait_for(l, std::chrono::milliseconds(200), [&] { return q.size() >= BATCH || qdone || interrupted; });
+            while (!q.empty() && batch.size() < BATCH) { batch.push_back(q.front()); q.pop_front(); }
+            qcv.notify_all();
+            if (batch.empty() && (qdone || interrupted)) break;
+        }
+        if (batch.empty()) continue;
+        S.passed += batch.size();
+        if (P.from_stdin) S.done += batch.size();
+        S.process(batch);
+        if (interrupted) break;
+    }
+    if (source.joinable()) { if (qdone) source.join(); else source.detach(); }
+    fclose(S.out); fclose(S.sout);
+    const double sec = std::chrono::duration<double>(Clock::now() - S.begin).count();
+    FILE *m = fopen((prefix + ".json").c_str(), "w");
+    fprintf(m, "{\"start\":%llu,\"done\":%llu,\"passed\":%llu,\"scanned\":%llu,\"amp\":%g,\"sites\":%llu,\"seconds\":%.3f,\"threads\":%d,\"phase\":%g,\"sigma\":%g,"
+               "\"wc\":%g,\"we\":%g,\"t\":%g,\"ta\":%g,\"max_sites\":%d,\"nms\":%d,\"cpu_tables\":%.3f,\"cpu_scan\":%.3f,\"cpu_sites\":%.3f}\n",
+            (unsigned long long)S.start, (unsigned long long)S.done.load(), (unsigned long long)S.passed.load(), (unsigned long long)S.scanned.load(), P.amp,
+            (unsigned long long)S.nsites.load(), sec, S.threads, P.max_phase, P.sigma, P.wc, P.we, P.t, P.ta, P.max_sites, P.nms, S.t_tab, S.t_scan, S.t_site);
+    fclose(m);
+    fprintf(stderr, "done: %llu seeds (%llu passed) in %.1fs\n", (unsigned long long)S.done.load(), (unsigned long long)S.passed.load(), sec);
+    std::fflush(nullptr);
+    std::_Exit(0);
+}

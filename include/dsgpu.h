@@ -92,6 +92,9 @@ int dsg_tables(const dsg_tabin *tabs, uint32_t nseeds, float *out, float *maxt);
 /* ---------------------------------------------------------------- low-octave proxy on zone grids (S4) */
 typedef struct dsg_zone { int32_t x0, z0, nx, nz; } dsg_zone;   /* gproxy::Zone (gproxy.h:22): origin in quarts, step-32 cells */
 
+/* The 40 x 40 proxy probability table the device uses (row = C bin, column = E bin): desert_pass_prob
+ * (src/desert_dtable.hpp:5-46), for host-side cross-checks. */
+int dsg_proxy_table(float prob[1600]);
 /* Proxy bitmaps of a seed's zones: bits holds sum(nx*nz) bytes, zone after zone, each row-major with z
  * outer; 1 = passable (probability >= the cut given to dsg_init).  FP64, so every cell equals the CPU
  * proxy DesertProxy::prob (src/desert_proxy.hpp:24-32); replaces gproxy::evaluate (src/gpu/gproxy.h:37,
@@ -130,11 +133,22 @@ int dsg_points(uint64_t seed, int pred, float pcut, const int32_t *xz, uint32_t 
  * triples: NormalNoise::sample (src/standalone.hpp:140-151), FP64. */
 int dsg_noise(uint64_t seed, int channel, const double *xyz, uint32_t n, double *out);
 
+/* Point queries over many seeds at once: point k (x = xz[2k], z = xz[2k+1]) belongs to seeds[pseed[k]].
+ * kind 0..5: channel noise at the unwarped point (x, 0, z) (NormalNoise::sample, T.sample in
+ * dsearch_desert.cpp:330); DSG_Q_STATE: bridged desert state (0/1/2); DSG_Q_PROXY: proxy probability. */
+#define DSG_Q_STATE 6
+#define DSG_Q_PROXY 7
+int dsg_query_batch(const uint64_t *seeds, uint32_t nseeds, const uint32_t *pseed, int kind, const int32_t *xz, uint32_t n, double *out);
+
 /* Flood a batch of requests concurrently (any mix of seeds, steps, windows, predicates).  Results are
  * identical to dense_flood_bridged (src/dense_flood.hpp:52-86) run per request.  Replaces the CPU floods
  * of dsearch_desert.cpp:337,352,387,512,521 and tools/dflood.cpp:20.  DSG_OVERFLOW: device memory for the
  * visited tiles ran out; rerun the batch in smaller pieces. */
 int dsg_flood_batch(const dsg_flood_req *reqs, uint32_t n, dsg_area *out);
+/* As dsg_flood_batch, and also list each request's passable cells (quart coordinates x, z), the cells the
+ * reference leaves in state 2 or 3 (dense_flood.hpp:76; the hot-zone bookkeeping of dsearch_desert.cpp:340-363
+ * reads them).  Request r's cells are xz[2*off[r] ..] with off[n] = total; DSG_OVERFLOW if more than cap cells. */
+int dsg_flood_batch_cells(const dsg_flood_req *reqs, uint32_t n, dsg_area *out, uint64_t *off, int32_t *xz, uint64_t cap);
 /* A single flood (dflood SEED X Z STEP: qx = X>>2, qz = Z>>2, half = 20000/STEP). */
 int dsg_flood(const dsg_flood_req *req, dsg_area *out);
 

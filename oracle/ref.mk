@@ -11,7 +11,7 @@ GPUARCH  := -gencode arch=compute_100a,code=sm_100a
 
 REFHDR := $(wildcard $(REF)/src/*.hpp) $(REF)/src/dsearch_desert.cpp
 
-all: $(OUT)/dsearch_desert $(OUT)/dflood $(OUT)/libref_cpu.so $(OUT)/libref_gate.so $(OUT)/tgate
+all: $(OUT)/dsearch_desert $(OUT)/dflood $(OUT)/libref_cpu.so $(OUT)/libref_gate.so $(OUT)/tgate $(OUT)/dsearch_desert_gpu
 
 $(OUT):
 	mkdir -p $@
@@ -28,3 +28,9 @@ $(OUT)/tgate: $(REF)/src/gpu/tgate.cu $(REF)/src/gpu/gate.cuh | $(OUT)
 	$(NVCC) -O3 -std=c++20 $(GPUARCH) $< -o $@
 
 .PHONY: all
+
+# The reference's GPU searcher (Makefile:43-46): its engine gproxy.cu for sm_100a, the searcher with -DDRIP_GPU.
+$(OUT)/gproxy.o: $(REF)/src/gpu/gproxy.cu $(REF)/src/gpu/gate.cuh $(REF)/src/gpu/gproxy.h | $(OUT)
+	$(NVCC) -O3 -std=c++20 $(GPUARCH) -c $< -o $@
+$(OUT)/dsearch_desert_gpu: $(REF)/src/dsearch_desert.cpp $(REFHDR) $(OUT)/gproxy.o | $(OUT)
+	g++ $(CXXFLAGS) -DDRIP_GPU -I/usr/local/cuda/include $< $(OUT)/gproxy.o -L/usr/local/cuda/lib64 -lcudart_static -ldl -lrt -o $@
