@@ -647,3 +647,24 @@ extern "C" int dsg_gate_bench(uint64_t start, uint64_t per_step, uint32_t steps,
         return DSG_OK;
     });
 }
+
+// Launch of the amplitude kernels on caller-provided buffers (used by the allocation-free entry point in
+// gate_noalloc.cu).  counters[0..3] must hold {n, 0, n, 0} when the launches start.
+namespace dsg { namespace gate {
+void launch_amps_on(const uint64_t *d_seeds, uint32_t n, void *d_oct, uint32_t *d_counters, uint64_t *d_tmp_seeds, uint32_t *d_tmp_idx,
+                    float *d_tmp_amp, float *d_pre, float *d_full, const float taps24[24], int pg_blocks, int fg_blocks, cudaStream_t st) {
+    Taps t{};
+    float s9 = 0, s15 = 0;
+    for (int i = 0; i < 9; i++) { t.k9[i] = taps24[i]; s9 += taps24[i]; }
+    for (int i = 0; i < 15; i++) { t.k15[i] = taps24[9 + i]; s15 += taps24[9 + i]; }
+    t.norm9 = 1.f / (s9 * s9); t.norm15 = 1.f / (s15 * s15);
+    t.w = float(1.25 * (32.0 / 63.0) * 1.5);
+    Oct *oct = static_cast<Oct *>(d_oct);
+    k_octinit<<<(2 * n + 127) / 128, 128, 0, st>>>(d_seeds, d_counters, n, oct);
+    k_pregate<<<pg_blocks, PG_THREADS, 0, st>>>(oct, d_seeds, d_counters, n, -1e30f, t, d_tmp_seeds, d_tmp_idx, d_counters + 1, n, d_pre);
+    k_fullgate<<<fg_blocks, FG_THREADS, 0, st>>>(oct, d_seeds, nullptr, d_counters + 2, n, -1e30f, t, d_tmp_seeds, d_tmp_amp, d_counters + 3, n, d_full);
+}
+size_t oct_bytes() { return sizeof(Oct); }
+int pregate_blocks_per_sm() { int occ = 0; cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_pregate, PG_THREADS, 0); return occ; }
+int fullgate_blocks_per_sm() { int occ = 0; cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_fullgate, FG_THREADS, 0); return occ; }
+}}

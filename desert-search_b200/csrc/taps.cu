@@ -22,3 +22,10 @@ void gate_taps_device(float out[24]) {
 }
 }  // namespace gate
 }  // namespace dsg
+
+namespace dsg {
+namespace gate {
+// The same taps written into a caller-provided device buffer of 24 floats, on `st` (no allocation).
+void gate_taps_into(float *d_out, cudaStream_t st) { k_taps<<<1, 32, 0, st>>>(d_out, 1.0f, 2.0f); }
+}  // namespace gate
+}  // namespace dsg

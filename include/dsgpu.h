@@ -51,6 +51,18 @@ int dsg_gate_run(uint64_t start, uint64_t count, const dsg_gate_cfg *cfg,
  * s of seed i.  The calibration view of the gate; replaces tgate's calib=N mode (src/gpu/tgate.cu:53-86). */
 int dsg_gate_amps(const uint64_t *seeds, uint32_t n, float *pre, float *full);
 
+/* Allocation-free form of dsg_gate_amps, for callers that may not allocate device memory (their memory
+ * is owned by another allocator, or cudaMalloc's implicit synchronisation is not acceptable in their
+ * loop, or they are a plug-in handed buffers only).  No counterpart in the reference.  seeds (n), pre and
+ * full (2n floats each) are DEVICE pointers owned by the caller; all intermediates live in one fixed
+ * device array of this library, so n <= DSG_NOALLOC_MAX_SEEDS (larger n returns DSG_E_ARG).  Work is
+ * enqueued on `stream` (a cudaStream_t, NULL = default stream) and the call returns without waiting.
+ * Does not need dsg_init; uses the current device.  The first call on each device sets up the array
+ * (address lookup, blur taps, one synchronous copy): make it before any stream capture.  All calls share
+ * the array: calls whose work overlaps on the GPU race and must be serialised by the caller. */
+#define DSG_NOALLOC_MAX_SEEDS 4096
+int dsg_gate_amps_noalloc(const uint64_t *seeds, uint32_t n, float *pre, float *full, void *stream);
+
 /* y-phase of explicit seeds and the two fractional y offsets (fy[2i], fy[2i+1]); phase_t
  * (src/dsearch_desert.cpp:80-94). */
 int dsg_phase(const uint64_t *seeds, uint32_t n, double *phase, double *fy);
