@@ -1,0 +1,346 @@
+// Flood service: continuous batching of exact-flood requests (the on-device replacement of the fleet's
+// MC-Measure verification step, deploy/gpipe.sh:7-10, and of per-request dflood runs).
+//
+// Requests (any seed, start, lattice, window, predicate) are submitted from any host thread and answered
+// with the same DenseArea dense_flood_bridged gives (src/dense_flood.hpp:52-86).  One engine thread keeps
+// every admitted request's BFS in flight together: each BFS level is one launch of the shared level kernel
+// (flood_kernels.cuh) over the cells of all requests, so requests of very different sizes overlap on the
+// device; new requests join at the next level boundary and finished ones leave, releasing their memory.
+// Per-request state lives in HBM: a tile directory carved from an arena, visited tiles (2 bits per cell)
+// taken from a ring of free tiles and zeroed on release, and the request's slot in the level lists.
+// Admission is by memory: a request is admitted when a slot is free, its directory fits the arena and the
+// free tile count stays above a reserve; otherwise it waits in the queue.
+#include "flood_kernels.cuh"
+#include <algorithm>
+#include <condition_variable>
+#include <deque>
+#include <map>
+#include <mutex>
+#include <thread>
+#include <vector>
+
+namespace dsg {
+namespace flood {
+namespace {
+
+// Release the tiles of finished requests: zero them and append them to the free ring.
+__global__ void k_release(const FloodCtl *__restrict__ ctl, const uint32_t *__restrict__ slots, int32_t *__restrict__ dir,
+                          uint32_t *__restrict__ pool, uint32_t *__restrict__ ring, uint32_t cap, uint32_t tail, uint32_t *__restrict__ returned) {
+    const FloodCtl c = ctl[slots[blockIdx.x]];
+    const int64_t entries = int64_t(c.tpr) * c.tpr;
+    for (int64_t e = 0; e < entries; e++) {
+        const int32_t d = dir[c.dir_off + e];
+        if (d < 0) continue;
+        uint32_t *t = pool + size_t(d) * TILE_WORDS;
+        for (int w = threadIdx.x; w < TILE_WORDS; w += blockDim.x) t[w] = 0;
+        if (threadIdx.x == 0) ring[(tail + atomicAdd(returned, 1u)) % cap] = uint32_t(d);
+    }
+}
+__global__ void k_iota(uint32_t *a, uint32_t n) { for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) a[i] = i; }
+
+struct Ticket { dsg_area area{}; int status = 2; };        // 2 = pending
+
+struct Service {
+    std::mutex mu;
+    std::condition_variable cv_engine, cv_done;
+    std::thread engine;
+    bool open = false, stop = false;
+    dsg_service_cfg cfg{};
+    // host bookkeeping
+    uint64_t next_ticket = 1;
+    std::deque<std::pair<uint64_t, dsg_flood_req>> pending;
+    std::map<uint64_t, Ticket> results;
+    struct Slot { bool used = false; uint64_t ticket = 0; int64_t dir_off = 0, dir_len = 0; };
+    std::vector<Slot> slots;
+    std::vector<std::pair<int64_t, int64_t>> dir_free;       // free arena ranges (offset, length)
+    uint64_t admitted = 0, completed = 0, levels = 0, overflowed = 0;
+    // device
+    cudaStream_t st = nullptr;
+    FloodCtl *d_ctl = nullptr; FloodStat *d_stat = nullptr; SeedNoise *d_noise = nullptr, *d_noise_stage = nullptr;
+    uint32_t *d_active = nullptr, *h_active = nullptr;
+    int32_t *d_dir = nullptr; int64_t dir_cap = 0;
+    uint32_t *d_pool = nullptr, *d_ring = nullptr; uint32_t pool_cap = 0, head = 0, avail = 0;
+    uint32_t *d_ctr = nullptr, *h_ctr = nullptr;               // [0] taken, [1] returned, [2..4] list counters, [5] error flags
+    uint64_t *d_list[2] = {nullptr, nullptr}; uint32_t list_cap = 0;
+    uint32_t *d_hist = nullptr;
+    uint32_t *d_slots = nullptr; uint64_t *d_seeds = nullptr;
+    int grid = 0;
+};
+Service &SV() { static Service s; return s; }
+constexpr uint32_t HIST = 1u << 16;
+
+bool dir_alloc(Service &g, int64_t len, int64_t &off) {
+    for (auto it = g.dir_free.begin(); it != g.dir_free.end(); ++it)
+        if (it->second >= len) { off = it->first; it->first += len; it->second -= len; if (!it->second) g.dir_free.erase(it); return true; }
+    return false;
+}
+void dir_release(Service &g, int64_t off, int64_t len) {
+    g.dir_free.push_back({off, len});
+    std::sort(g.dir_free.begin(), g.dir_free.end());
+    std::vector<std::pair<int64_t, int64_t>> m;
+    for (auto &r : g.dir_free) { if (!m.empty() && m.back().first + m.back().second == r.first) m.back().second += r.second; else m.push_back(r); }
+    g.dir_free.swap(m);
+}
+
+void engine_loop(Service &g) {
+    cudaSetDevice(device_info().device);
+    const uint32_t S = g.cfg.max_requests, K = std::max<uint32_t>(1, g.cfg.levels_per_check);
+    const uint32_t reserve = std::max<uint32_t>(64, g.pool_cap / 64);
+    const WorldDev w = world_dev();
+    uint32_t level = 0;
+    std::vector<uint32_t> adm_slots; std::vector<uint64_t> adm_seeds;
+    for (;;) {
+        adm_slots.clear(); adm_seeds.clear();
+        std::vector<FloodCtl> adm_ctl;
+        {
+            std::unique_lock<std::mutex> l(g.mu);
+            g.cv_engine.wait(l, [&] {
+                const bool busy = std::any_of(g.slots.begin(), g.slots.end(), [](const Service::Slot &s) { return s.used; });
+                return g.stop || busy || !g.pending.empty();
+            });
+            const bool busy = std::any_of(g.slots.begin(), g.slots.end(), [](const Service::Slot &s) { return s.used; });
+            if (g.stop && !busy && g.pending.empty()) return;
+            // admission: free slot, directory space, and a tile reserve per in-flight request
+            uint32_t inflight = 0;
+            for (auto &s : g.slots) inflight += s.used;
+            for (uint32_t si = 0; si < S && !g.pending.empty(); si++) {
+                if (g.slots[si].used) continue;
+                if (g.avail < reserve * (inflight + 1)) break;
+                const dsg_flood_req q = g.pending.front().second;
+                FloodCtl c{};
+                c.qx = q.qx; c.qz = q.qz; c.step = q.step; c.half = q.half; c.n = 2 * q.half + 1; c.tpr = (c.n + TILE - 1) / TILE;
+                c.conn8 = q.conn8 ? 1 : 0; c.pred = q.pred; c.pcut = q.pcut; c.noise = int32_t(si);
+                const int64_t len = int64_t(c.tpr) * c.tpr;
+                int64_t off;
+                if (!dir_alloc(g, len, off)) break;
+                c.dir_off = off;
+                g.slots[si] = {true, g.pending.front().first, off, len};
+                g.pending.pop_front();
+                adm_slots.push_back(si); adm_seeds.push_back(q.seed); adm_ctl.push_back(c);
+                inflight++; g.admitted++;
+            }
+        }
+        try {
+            cudaStream_t st = g.st;
+            const TileAlloc ta{g.d_ring, g.head, g.avail, g.pool_cap, g.d_ctr + 0, g.d_ctr + 1, (g.head + g.avail) % g.pool_cap};
+            if (!adm_slots.empty()) {
+                const uint32_t na = uint32_t(adm_slots.size());
+                DSG_CU(cudaMemcpyAsync(g.d_seeds, adm_seeds.data(), na * 8, cudaMemcpyHostToDevice, st));
+                seed_noise_build(g.d_seeds, na, g.d_noise_stage, st);
+                for (uint32_t k = 0; k < na; k++) {
+                    DSG_CU(cudaMemcpyAsync(g.d_noise + adm_slots[k], g.d_noise_stage + k, sizeof(SeedNoise), cudaMemcpyDeviceToDevice, st));
+                    DSG_CU(cudaMemcpyAsync(g.d_ctl + adm_slots[k], &adm_ctl[k], sizeof(FloodCtl), cudaMemcpyHostToDevice, st));
+                    DSG_CU(cudaMemsetAsync(g.d_dir + adm_ctl[k].dir_off, 0xFF, size_t(g.slots[adm_slots[k]].dir_len) * 4, st));
+                }
+                DSG_CU(cudaMemcpyAsync(g.d_slots, adm_slots.data(), na * 4, cudaMemcpyHostToDevice, st));
+                // ctl/slots are host vectors: finish these copies before they go out of scope
+                k_flood_start<<<(na + 127) / 128, 128, 0, st>>>(g.d_ctl, g.d_slots, na, g.d_stat, g.d_dir, g.d_pool, ta, g.d_list[level & 1],
+                                                                g.d_ctr + 2 + (level % 3), g.d_ctr + 5, Stamp{g.d_active, int(level)});
+                DSG_CU(cudaGetLastError());
+                DSG_CU(cudaStreamSynchronize(st));
+            }
+            for (uint32_t k = 0; k < K; k++, level++) {
+                k_flood_level<<<g.grid, 128, 0, st>>>(g.d_ctl, g.d_stat, g.d_noise, w, g.d_dir, g.d_pool, ta, g.d_list[level & 1],
+                                                      g.d_ctr + 2 + (level % 3), g.d_list[(level + 1) & 1], g.d_ctr + 2 + ((level + 1) % 3),
+                                                      g.d_ctr + 2 + ((level + 2) % 3), g.list_cap, g.d_hist, int(level % HIST), g.d_ctr + 5,
+                                                      Stamp{g.d_active, int(level)});
+            }
+            DSG_CU(cudaGetLastError());
+            DSG_CU(cudaMemcpyAsync(g.h_active, g.d_active, size_t(S) * 4, cudaMemcpyDeviceToHost, st));
+            DSG_CU(cudaMemcpyAsync(g.h_ctr, g.d_ctr, 8 * 4, cudaMemcpyDeviceToHost, st));
+            DSG_CU(cudaStreamSynchronize(st));
+            const uint32_t taken = std::min(g.h_ctr[0], g.avail);
+            uint32_t returned = g.h_ctr[1];
+            g.head = (g.head + taken) % g.pool_cap;
+            g.avail -= taken;
+            // finished requests: no cell queued for the next level
+            std::vector<uint32_t> fin;
+            {
+                std::lock_guard<std::mutex> l(g.mu);
+                for (uint32_t si = 0; si < S; si++) if (g.slots[si].used && g.h_active[si] != level) fin.push_back(si);
+            }
+            std::vector<FloodStat> fs(fin.size());
+            if (!fin.empty()) {
+                for (size_t k = 0; k < fin.size(); k++) DSG_CU(cudaMemcpyAsync(&fs[k], g.d_stat + fin[k], sizeof(FloodStat), cudaMemcpyDeviceToHost, st));
+                DSG_CU(cudaMemcpyAsync(g.d_slots, fin.data(), fin.size() * 4, cudaMemcpyHostToDevice, st));
+                // the returned counter continues from the tiles lost in the directory races of these levels
+                k_release<<<unsigned(fin.size()), 256, 0, st>>>(g.d_ctl, g.d_slots, g.d_dir, g.d_pool, g.d_ring, g.pool_cap,
+                                                                (g.head + g.avail) % g.pool_cap, g.d_ctr + 1);
+                DSG_CU(cudaGetLastError());
+                DSG_CU(cudaMemcpyAsync(g.h_ctr + 1, g.d_ctr + 1, 4, cudaMemcpyDeviceToHost, st));
+                DSG_CU(cudaStreamSynchronize(st));
+                returned = g.h_ctr[1];
+            }
+            g.avail += returned;
+            DSG_CU(cudaMemsetAsync(g.d_ctr, 0, 8, st));              // taken, returned
+            {
+                std::lock_guard<std::mutex> l(g.mu);
+                for (size_t k = 0; k < fin.size(); k++) {
+                    Service::Slot &s = g.slots[fin[k]];
+                    Ticket &t = g.results[s.ticket];
+                    const FloodStat &f = fs[k];
+                    t.area = {f.cells, f.sampled, f.minx, f.maxx, f.minz, f.maxz, f.edge, f.border};
+                    t.status = f.overflow ? DSG_OVERFLOW : DSG_OK;
+                    g.overflowed += f.overflow != 0;
+                    dir_release(g, s.dir_off, s.dir_len);
+                    s = Service::Slot{};
+                    g.completed++;
+                }
+                g.levels = level;
+            }
+            if (!fin.empty()) g.cv_done.notify_all();
+            if (g.h_ctr[5] & 2) throw std::runtime_error("flood service: level list capacity exceeded");
+        } catch (...) {
+            std::lock_guard<std::mutex> l(g.mu);
+            for (auto &s : g.slots) if (s.used) { g.results[s.ticket].status = DSG_E_CUDA; s = Service::Slot{}; }
+            for (auto &p : g.pending) g.results[p.first].status = DSG_E_CUDA;
+            g.pending.clear();
+            g.stop = true;
+            g.cv_done.notify_all();
+            return;
+        }
+    }
+}
+}  // namespace
+}  // namespace flood
+}  // namespace dsg
+
+using namespace dsg;
+using namespace dsg::flood;
+
+extern "C" int dsg_service_open(const dsg_service_cfg *cfg_in) {
+    return guarded([&] {
+        require_init();
+        Service &g = SV();
+        std::lock_guard<std::mutex> l(g.mu);
+        DSG_ARG(!g.open, "dsg_service_open: already open");
+        dsg_service_cfg c = cfg_in ? *cfg_in : dsg_service_cfg{0, 0, 0};
+        if (!c.budget_bytes) c.budget_bytes = uint64_t(8) << 30;
+        if (!c.max_requests) c.max_requests = 4096;
+        if (!c.levels_per_check) c.levels_per_check = 4;
+        DSG_ARG(c.max_requests <= (1u << 20), "dsg_service_open: max_requests too large");
+        g.cfg = c;
+        const uint32_t S = c.max_requests;
+        int lo, hi;
+        DSG_CU(cudaDeviceGetStreamPriorityRange(&lo, &hi));
+        DSG_CU(cudaStreamCreateWithPriority(&g.st, cudaStreamNonBlocking, hi));
+        DSG_CU(cudaMalloc(&g.d_ctl, size_t(S) * sizeof(FloodCtl)));
+        DSG_CU(cudaMalloc(&g.d_stat, size_t(S) * sizeof(FloodStat)));
+        DSG_CU(cudaMalloc(&g.d_noise, size_t(S) * sizeof(SeedNoise)));
+        DSG_CU(cudaMalloc(&g.d_noise_stage, size_t(S) * sizeof(SeedNoise)));
+        DSG_CU(cudaMalloc(&g.d_active, size_t(S) * 4));
+        DSG_CU(cudaMemset(g.d_active, 0xFF, size_t(S) * 4));
+        DSG_CU(cudaMallocHost(&g.h_active, size_t(S) * 4));
+        DSG_CU(cudaMalloc(&g.d_slots, size_t(S) * 4));
+        DSG_CU(cudaMalloc(&g.d_seeds, size_t(S) * 8));
+        // budget: a quarter for tile directories, the rest for visited tiles and their free ring
+        g.dir_cap = int64_t(c.budget_bytes / 4 / 4);
+        DSG_CU(cudaMalloc(&g.d_dir, size_t(g.dir_cap) * 4));
+        g.dir_free = {{0, g.dir_cap}};
+        g.pool_cap = uint32_t(std::min<uint64_t>((c.budget_bytes - c.budget_bytes / 4) / (TILE_WORDS * 4 + 4), 0x7fffffffu));
+        DSG_CU(cudaMalloc(&g.d_pool, size_t(g.pool_cap) * TILE_WORDS * 4));
+        DSG_CU(cudaMemset(g.d_pool, 0, size_t(g.pool_cap) * TILE_WORDS * 4));
+        DSG_CU(cudaMalloc(&g.d_ring, size_t(g.pool_cap) * 4));
+        k_iota<<<1024, 256>>>(g.d_ring, g.pool_cap);
+        DSG_CU(cudaGetLastError());
+        g.head = 0; g.avail = g.pool_cap;
+        g.list_cap = 1u << 25;
+        for (auto &p : g.d_list) DSG_CU(cudaMalloc(&p, size_t(g.list_cap) * 8));
+        DSG_CU(cudaMalloc(&g.d_ctr, 8 * 4));
+        DSG_CU(cudaMemset(g.d_ctr, 0, 8 * 4));
+        DSG_CU(cudaMallocHost(&g.h_ctr, 8 * 4));
+        DSG_CU(cudaMalloc(&g.d_hist, size_t(HIST) * 4));
+        DSG_CU(cudaDeviceSynchronize());
+        int occ = 0;
+        DSG_CU(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_flood_level, 128, 0));
+        g.grid = std::max(1, occ) * device_info().sms;
+        g.slots.assign(S, Service::Slot{});
+        g.stop = false; g.open = true;
+        g.engine = std::thread(engine_loop, std::ref(g));
+        return DSG_OK;
+    });
+}
+
+extern "C" int dsg_service_submit(const dsg_flood_req *req, uint64_t *ticket) {
+    return guarded([&] {
+        DSG_ARG(req && ticket, "dsg_service_submit: null pointer");
+        DSG_ARG(req->step >= 1 && req->half >= 0 && req->half <= 32767, "dsg_service_submit: need step >= 1 and 0 <= half <= 32767");
+        DSG_ARG(req->pred == DSG_PRED_DESERT || req->pred == DSG_PRED_HOT || req->pred == DSG_PRED_PROXY, "dsg_service_submit: unknown predicate");
+        Service &g = SV();
+        std::lock_guard<std::mutex> l(g.mu);
+        DSG_ARG(g.open && !g.stop, "dsg_service_submit: service not open");
+        const int64_t tpr = (2 * int64_t(req->half) + 1 + TILE - 1) / TILE;
+        DSG_ARG(tpr * tpr <= g.dir_cap, "dsg_service_submit: window larger than the directory arena");
+        *ticket = g.next_ticket++;
+        g.results[*ticket] = Ticket{};
+        g.pending.push_back({*ticket, *req});
+        g.cv_engine.notify_all();
+        return DSG_OK;
+    });
+}
+
+// DSG_OK (result in out, ticket retired), DSG_PENDING (not finished yet), DSG_OVERFLOW (ticket retired;
+// the request ran out of tile memory), DSG_E_ARG (unknown ticket).
+extern "C" int dsg_service_poll(uint64_t ticket, dsg_area *out) {
+    return guarded([&] {
+        Service &g = SV();
+        std::lock_guard<std::mutex> l(g.mu);
+        auto it = g.results.find(ticket);
+        DSG_ARG(it != g.results.end(), "dsg_service_poll: unknown ticket");
+        if (it->second.status == DSG_PENDING) return DSG_PENDING;
+        const int st = it->second.status;
+        if (out) *out = it->second.area;
+        g.results.erase(it);
+        return st;
+    });
+}
+
+extern "C" int dsg_service_wait(uint64_t ticket, dsg_area *out, int timeout_ms) {
+    return guarded([&] {
+        Service &g = SV();
+        std::unique_lock<std::mutex> l(g.mu);
+        auto done = [&] { auto it = g.results.find(ticket); return it == g.results.end() || it->second.status != DSG_PENDING; };
+        if (timeout_ms < 0) g.cv_done.wait(l, done);
+        else if (!g.cv_done.wait_for(l, std::chrono::milliseconds(timeout_ms), done)) { set_error("dsg_service_wait: timed out"); return DSG_E_TIMEOUT; }
+        auto it = g.results.find(ticket);
+        DSG_ARG(it != g.results.end(), "dsg_service_wait: unknown ticket");
+        const int st = it->second.status;
+        if (out) *out = it->second.area;
+        g.results.erase(it);
+        return st;
+    });
+}
+
+extern "C" int dsg_service_stats(uint64_t stats[6]) {
+    return guarded([&] {
+        Service &g = SV();
+        std::lock_guard<std::mutex> l(g.mu);
+        uint64_t inflight = 0;
+        for (auto &s : g.slots) inflight += s.used;
+        const uint64_t v[6] = {g.admitted, g.completed, inflight, uint64_t(g.pending.size()), g.levels, g.overflowed};
+        std::copy(v, v + 6, stats);
+        return DSG_OK;
+    });
+}
+
+extern "C" int dsg_service_close(void) {
+    return guarded([&] {
+        Service &g = SV();
+        {
+            std::lock_guard<std::mutex> l(g.mu);
+            if (!g.open) return DSG_OK;
+            g.stop = true;
+            g.cv_engine.notify_all();
+        }
+        if (g.engine.joinable()) g.engine.join();
+        std::lock_guard<std::mutex> l(g.mu);
+        cudaStreamSynchronize(g.st);
+        cudaFree(g.d_ctl); cudaFree(g.d_stat); cudaFree(g.d_noise); cudaFree(g.d_noise_stage); cudaFree(g.d_active); cudaFreeHost(g.h_active);
+        cudaFree(g.d_slots); cudaFree(g.d_seeds); cudaFree(g.d_dir); cudaFree(g.d_pool); cudaFree(g.d_ring); cudaFree(g.d_ctr);
+        cudaFreeHost(g.h_ctr); cudaFree(g.d_hist); cudaFree(g.d_list[0]); cudaFree(g.d_list[1]);
+        cudaStreamDestroy(g.st);
+        g.results.clear(); g.pending.clear(); g.slots.clear(); g.dir_free.clear();
+        g.open = false; g.stop = false;
+        return DSG_OK;
+    });
+}

@@ -183,3 +183,51 @@ def proxy(seed, zones):
         out.append(bits[off: off + z[2] * z[3]].reshape(z[3], z[2]))
         off += z[2] * z[3]
     return out
+
+
+DSG_PENDING = 2
+
+
+class ServiceCfg(C.Structure):
+    _fields_ = [("budget_bytes", C.c_uint64), ("max_requests", C.c_uint32), ("levels_per_check", C.c_uint32)]
+
+
+class Service:
+    """The continuously batched flood service (dsg_service_*)."""
+
+    def __init__(self, budget_bytes=8 << 30, max_requests=4096, levels_per_check=4):
+        cfg = ServiceCfg(budget_bytes, max_requests, levels_per_check)
+        _ck(lib.dsg_service_open(C.byref(cfg)), "dsg_service_open")
+
+    def submit(self, req):
+        t = C.c_uint64()
+        _ck(lib.dsg_service_submit(C.byref(req), C.byref(t)), "dsg_service_submit")
+        return t.value
+
+    def poll(self, ticket):
+        a = Area()
+        rc = _ck(lib.dsg_service_poll(C.c_uint64(ticket), C.byref(a)), "dsg_service_poll")
+        return None if rc == DSG_PENDING else (rc, a.as_tuple())
+
+    def wait(self, ticket, timeout_ms=-1):
+        a = Area()
+        rc = _ck(lib.dsg_service_wait(C.c_uint64(ticket), C.byref(a), C.c_int(timeout_ms)), "dsg_service_wait")
+        return rc, a.as_tuple()
+
+    def stats(self):
+        s = np.zeros(6, dtype=np.uint64)
+        _ck(lib.dsg_service_stats(ptr(s, u64p)), "dsg_service_stats")
+        return dict(zip(["admitted", "completed", "inflight", "queued", "levels", "overflowed"], [int(x) for x in s]))
+
+    def close(self):
+        _ck(lib.dsg_service_close(), "dsg_service_close")
+
+
+def query(seeds, pseed, kind, xz):
+    """Multi-seed point queries (dsg_query_batch): kind 0..5 channel noise, 6 desert state, 7 proxy prob."""
+    s = np.ascontiguousarray(seeds, dtype=np.uint64); p = np.ascontiguousarray(pseed, dtype=np.uint32)
+    xz = np.ascontiguousarray(xz, dtype=np.int32).reshape(-1, 2)
+    out = np.empty(len(xz))
+    _ck(lib.dsg_query_batch(ptr(s, u64p), C.c_uint32(len(s)), ptr(p, u32p), C.c_int(kind), ptr(xz, i32p), C.c_uint32(len(xz)),
+                            ptr(out, f64p)), "dsg_query_batch")
+    return out

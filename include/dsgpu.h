@@ -19,7 +19,8 @@ extern "C" {
 #define DSG_E_CUDA       -1    /* CUDA runtime error (message in dsg_last_error) */
 #define DSG_E_ARG        -2    /* invalid argument */
 #define DSG_E_STATE      -3    /* called before dsg_init, or after a fatal error */
-#define DSG_E_TIMEOUT    -4    /* a bounded device wait gave up (service kernels) */
+#define DSG_PENDING       2    /* service request not finished yet */
+#define DSG_E_TIMEOUT    -4    /* a bounded wait gave up */
 
 /* Last error message of the calling thread (static storage, valid until the next call). */
 const char *dsg_last_error(void);
@@ -161,6 +162,27 @@ int dsg_flood_batch(const dsg_flood_req *reqs, uint32_t n, dsg_area *out);
  * reference leaves in state 2 or 3 (dense_flood.hpp:76; the hot-zone bookkeeping of dsearch_desert.cpp:340-363
  * reads them).  Request r's cells are xz[2*off[r] ..] with off[n] = total; DSG_OVERFLOW if more than cap cells. */
 int dsg_flood_batch_cells(const dsg_flood_req *reqs, uint32_t n, dsg_area *out, uint64_t *off, int32_t *xz, uint64_t cap);
+/* ---------------------------------------------------------------- flood service (continuous batching) */
+/* Replaces the fleet's per-CANDIDATE MC-Measure run (deploy/gpipe.sh:7-10) and per-request dflood runs: any
+ * number of host threads submit flood requests; one engine keeps all admitted requests' floods in flight
+ * together (each BFS level is one launch over every request's cells), admits new requests at level
+ * boundaries while slots, directory arena and visited-tile memory allow, and retires finished ones.
+ * Results equal dsg_flood's. */
+typedef struct dsg_service_cfg {
+    uint64_t budget_bytes;      /* device memory for tile directories and visited tiles (0 = 8 GiB) */
+    uint32_t max_requests;      /* requests in flight at once (0 = 4096) */
+    uint32_t levels_per_check;  /* BFS levels launched between host checks (0 = 4) */
+} dsg_service_cfg;
+int dsg_service_open(const dsg_service_cfg *cfg);
+int dsg_service_submit(const dsg_flood_req *req, uint64_t *ticket);
+/* DSG_OK with the result (ticket retired), DSG_PENDING, DSG_OVERFLOW (retired; out of tile memory), or an error. */
+int dsg_service_poll(uint64_t ticket, dsg_area *out);
+/* Blocking form of poll; timeout_ms < 0 waits forever, else DSG_E_TIMEOUT. */
+int dsg_service_wait(uint64_t ticket, dsg_area *out, int timeout_ms);
+/* {admitted, completed, in flight, queued, BFS levels run, overflowed}. */
+int dsg_service_stats(uint64_t stats[6]);
+int dsg_service_close(void);
+
 /* A single flood (dflood SEED X Z STEP: qx = X>>2, qz = Z>>2, half = 20000/STEP). */
 int dsg_flood(const dsg_flood_req *req, dsg_area *out);
 
