@@ -93,6 +93,105 @@ def cpu_baseline(seconds_budget=20.0):
             "seeds_per_s": count / dt}
 
 
+def flood_sites(dsgpu, n_small, rng_seed=20261203):
+    """Synthetic flood sites.  Small class: random int64 seeds from a fixed RNG stream, each paired with the
+    first of 64 uniform blocks in |X|, |Z| <= 3e7 whose bridged Y=256 state is desert.  Large class: the
+    220 MC-Measure-verified finds of the reference's results (72M-100M blocks^2) and the two `make check`
+    records (tests/golden/finds.json) -- the stand-in for the searcher's proxy >= 50M candidates."""
+    import numpy as np
+    rng = np.random.default_rng(rng_seed)
+    small = []
+    while len(small) < n_small:
+        m = 256
+        seeds = rng.integers(-(1 << 63), (1 << 63) - 1, m, dtype=np.int64).view(np.uint64)
+        xz = (rng.integers(-30_000_000, 30_000_001, (m * 64, 2)) >> 2).astype(np.int32)
+        st = dsgpu.query(seeds, np.repeat(np.arange(m, dtype=np.uint32), 64), 6, xz).reshape(m, 64)
+        for i in range(m):
+            k = np.nonzero(st[i] == 2)[0]
+            if len(k):
+                small.append((int(seeds[i]), int(xz[i * 64 + k[0], 0]), int(xz[i * 64 + k[0], 1])))
+    finds = json.load(open(os.path.join(ROOT, "tests", "golden", "finds.json")))
+    large = [(f["seed"] & ((1 << 64) - 1), f["x"] >> 2, f["z"] >> 2) for f in finds]
+    return small[:n_small], large
+
+
+def bench_floods(dsgpu, n_small=4096, rate=500.0, n_service=1500, n_seq=120, batch_only=False, n_large=None):
+    """Exact step-1 floods: one batch of every site, and the flood service under Poisson arrivals."""
+    import threading
+    import numpy as np
+    small, large = flood_sites(dsgpu, n_small)
+    if n_large is not None:
+        large = large[:n_large]
+    req = lambda s: dsgpu.flood_req(s[0], s[1], s[2], 1, 20000)
+    # batch: all sites in one dsg_flood_batch call
+    reqs = [req(s) for s in small + large]
+    t0 = time.perf_counter()
+    areas = dsgpu.flood_batch(reqs)
+    t_batch = time.perf_counter() - t0
+    sampled = sum(a[1] for a in areas)
+    cells = np.array([a[0] for a in areas], dtype=np.float64)
+    batch = {"floods": len(reqs), "small": len(small), "large": len(large), "seconds": t_batch, "floods_per_s": len(reqs) / t_batch,
+             "cells_per_s": float(cells.sum()) / t_batch, "evaluations_per_s": sampled / t_batch,
+             "area_blocks2_min_median_max": [float(cells.min() * 16), float(np.median(cells) * 16), float(cells.max() * 16)]}
+    if batch_only:
+        return {"batch": batch}
+    # service: 90% small, 10% large, Poisson arrivals at `rate`
+    rng = np.random.default_rng(7)
+    kinds = rng.random(n_service) < 0.1
+    mix = [large[rng.integers(len(large))] if k else small[rng.integers(len(small))] for k in kinds]
+    arrive = np.cumsum(rng.exponential(1.0 / rate, n_service))
+    svc = dsgpu.Service(budget_bytes=24 << 30, max_requests=4096, rounds_per_check=4)
+    done_t = np.zeros(n_service); tickets = [0] * n_service
+    lock = threading.Lock(); ready = threading.Semaphore(0)
+    def waiter():
+        while True:
+            ready.acquire()
+            with lock:
+                if not todo:
+                    return
+                i = todo.pop(0)
+            svc.wait(tickets[i])
+            done_t[i] = time.perf_counter()
+    todo = []
+    ws = [threading.Thread(target=waiter) for _ in range(16)]
+    for w in ws:
+        w.start()
+    t_start = time.perf_counter()
+    for i in range(n_service):
+        d = t_start + arrive[i] - time.perf_counter()
+        if d > 0:
+            time.sleep(d)
+        tickets[i] = svc.submit(req(mix[i]))
+        with lock:
+            todo.append(i)
+        ready.release()
+    for _ in ws:
+        ready.release()
+    for w in ws:
+        w.join()
+    svc.close()
+    lat = done_t - (t_start + arrive)
+    t_svc = done_t.max() - t_start
+    # sequential plain per-request launches: measured service times of a sample, FIFO queue on the same arrivals
+    seq_t = []
+    for i in range(n_seq):
+        t1 = time.perf_counter(); dsgpu.flood(*mix[i][:3], 1, 20000); seq_t.append(time.perf_counter() - t1)
+    mean_seq = float(np.mean(seq_t))
+    svc_times = np.array([seq_t[i % n_seq] for i in range(n_service)])
+    fin = np.zeros(n_service); prev = 0.0
+    for i in range(n_service):
+        prev = max(prev, arrive[i]) + svc_times[i]; fin[i] = prev
+    seq_lat = fin - arrive
+    return {
+        "batch": batch,
+        "service": {"rate_req_per_s": rate, "requests": n_service, "mix": "90% random desert sites, 10% verified finds (step 1, half 20000)",
+                    "floods_per_s": n_service / t_svc, "p50_ms": float(np.percentile(lat, 50) * 1e3), "p99_ms": float(np.percentile(lat, 99) * 1e3)},
+        "sequential_plain": {"floods_per_s": 1.0 / mean_seq, "p50_ms": float(np.percentile(seq_lat, 50) * 1e3),
+                             "p99_ms": float(np.percentile(seq_lat, 99) * 1e3),
+                             "how": f"dsg_flood per request, measured on {n_seq} requests of the same mix, FIFO queue on the same arrival times"},
+    }
+
+
 def run_ours(args):
     rank, world, local = dist()
     import dsgpu
@@ -118,6 +217,11 @@ def run_ours(args):
         pg.all_reduce(t, op=op)
         return t.tolist()
 
+    if args.flood_only:
+        if rank == 0:
+            print(json.dumps({"flood": bench_floods(dsgpu, n_small=args.flood_small, rate=args.flood_rate, n_service=args.flood_requests,
+                                                    batch_only=args.flood_batch_only, n_large=args.flood_large)}), flush=True)
+        return
     barrier()
     clk = Clocks(local)
     ms, mk, counts = dsgpu.gate_bench(base, PER_STEP, args.steps, args.warmup)
@@ -222,6 +326,12 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--per-step-log2", type=int, default=26, help="seed indices per step = 2^N")
     ap.add_argument("--profile-run", action="store_true", help="device steps only (no e2e pass, no CPU baseline): for ncu captures")
+    ap.add_argument("--flood-only", action="store_true", help="only the flood measurements (batch + service)")
+    ap.add_argument("--flood-small", type=int, default=4096)
+    ap.add_argument("--flood-large", type=int, default=None, help="limit the large (verified-find) flood class")
+    ap.add_argument("--flood-batch-only", action="store_true")
+    ap.add_argument("--flood-rate", type=float, default=500.0)
+    ap.add_argument("--flood-requests", type=int, default=1500)
     args = ap.parse_args()
     global PER_STEP
     PER_STEP = 1 << args.per_step_log2

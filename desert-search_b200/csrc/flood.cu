@@ -1,20 +1,9 @@
-// Bridged biome floods (exact areas and the screening floods) on the device.
+// Bridged biome floods (exact areas and the screening floods) on the device, one-shot batches.
 //
-// Reference: src/dense_flood.hpp:52-86 (dense_flood_bridged), tools/dflood.cpp, the hot-zone floods of
-// src/dsearch_desert.cpp:326-366 and the step-8/step-4 exact floods of :498-523.  The reference runs a DFS
-// with an explicit stack over a dense (2*half+1)^2 byte window.  The result (cells, sampled, bbox, edge,
-// border) depends only on the set of cells the flood reaches, not on visit order: reached = the start plus
-// every cell adjacent to a reached passable cell; sampled = reached cells inside window and world.  So the
-// device runs a level-synchronous BFS instead, over any number of requests at once:
-//  * one kernel per BFS level; its input is the list of cells touched for the first time at the previous
-//    level (all requests mixed).  Each thread evaluates the FP64 predicate of one cell, counts it, and if it
-//    is passable touches its 4 (or 8) neighbours; first touches (atomicOr on the visited bit) form the next
-//    level's list (warp-aggregated appends).
-//  * visited state: 2 bits per cell (touched, passable) in 64x64-cell tiles of 1 KiB, allocated on first
-//    touch from a pre-zeroed pool through a per-request tile directory (atomicCAS; a thread that loses
-//    the race uses the winner's tile, so nothing ever waits).
-//  * list counters rotate through three slots so no level needs a host round trip; the host checks for
-//    completion every few levels through a per-level history array.
+// Reference: src/dense_flood.hpp:20-86 (dense_flood, dense_flood_bridged), tools/dflood.cpp, the hot-zone
+// floods of src/dsearch_desert.cpp:326-366 and the exact floods of :498-523.  Every request of a batch runs
+// through the tile rounds of flood_kernels.cuh together; the host only checks every few rounds whether any
+// tile is still queued.
 #include "flood_kernels.cuh"
 #include <algorithm>
 #include <map>
@@ -24,23 +13,18 @@
 namespace dsg {
 namespace flood {
 
-// ---------------------------------------------------------------- host engine
 struct Engine {
     std::mutex mu;
     bool ready = false;
     cudaStream_t st = nullptr;
-    uint32_t list_cap = 0;
-    uint64_t *d_list[2] = {nullptr, nullptr};
-    uint32_t *d_cnt = nullptr;                 // [0..2] rotating list counters, [3] pool_next, [4] error flags
-    uint32_t *d_hist = nullptr; uint32_t hist_cap = 0;
-    uint32_t *h_hist = nullptr;
-    uint32_t *d_pool = nullptr; uint32_t pool_cap = 0;
+    TilePool pool;
+    uint32_t *d_cnt = nullptr, *h_cnt = nullptr;   // [0..2] claim-queue counters, [3..5] connect-queue, [6] taken, [7] error flags
     int32_t *d_dir = nullptr; size_t dir_cap = 0;
     FloodCtl *d_ctl = nullptr; uint32_t ctl_cap = 0;
     FloodStat *d_stat = nullptr; uint32_t stat_cap = 0;
     SeedNoise *d_noise = nullptr; uint32_t noise_cap = 0;
     uint64_t *d_seeds = nullptr; uint32_t seeds_cap = 0;
-    int grid = 0;
+    int grid_eval = 0, grid_conn = 0;
 };
 Engine &E() { static Engine e; return e; }
 
@@ -50,15 +34,9 @@ void setup_locked(Engine &g) {
     int lo, hi;
     DSG_CU(cudaDeviceGetStreamPriorityRange(&lo, &hi));
     DSG_CU(cudaStreamCreateWithPriority(&g.st, cudaStreamNonBlocking, hi));
-    int occ = 0;
-    DSG_CU(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_flood_level, 128, 0));
-    g.grid = std::max(1, occ) * device_info().sms;
-    g.list_cap = 1u << 25;
-    for (auto &l : g.d_list) DSG_CU(cudaMalloc(&l, size_t(g.list_cap) * 8));
+    round_grids(g.grid_eval, g.grid_conn);
     DSG_CU(cudaMalloc(&g.d_cnt, 8 * 4));
-    g.hist_cap = 1u << 20;
-    DSG_CU(cudaMalloc(&g.d_hist, size_t(g.hist_cap) * 4));
-    DSG_CU(cudaMallocHost(&g.h_hist, 64 * 4));
+    DSG_CU(cudaMallocHost(&g.h_cnt, 8 * 4));
     g.ready = true;
 }
 template <class T> void grow(T *&p, uint32_t &cap, size_t need) {
@@ -69,19 +47,20 @@ template <class T> void grow(T *&p, uint32_t &cap, size_t need) {
     cap = uint32_t(c);
 }
 
-// Run a batch of requests to completion.  Returns DSG_OK, or DSG_OVERFLOW if the tile pool or a level list
-// ran out (the affected requests have overflow set and must be rerun with more memory).
+// Run a batch of requests to completion.  Returns DSG_OK, or DSG_OVERFLOW if the tile pool ran out (the
+// affected requests must be rerun with more memory).
 int run_batch(const dsg_flood_req *reqs, uint32_t n, dsg_area *out, size_t pool_bytes, uint64_t *cell_off = nullptr,
               int32_t *cell_xz = nullptr, uint64_t cell_cap = 0) {
     Engine &g = E();
     std::lock_guard<std::mutex> l(g.mu);
     setup_locked(g);
-    DSG_ARG(n <= g.list_cap, "dsg_flood_batch: too many requests in one batch");
+    DSG_ARG(n <= (1u << 24), "dsg_flood_batch: too many requests in one batch");
     // distinct seeds -> noise tables
     std::map<uint64_t, int32_t> slot;
     std::vector<uint64_t> seeds;
     std::vector<FloodCtl> ctl(n);
     size_t dir_total = 0;
+    int64_t dir_max = 0;
     for (uint32_t r = 0; r < n; r++) {
         const dsg_flood_req &q = reqs[r];
         DSG_ARG(q.step >= 1 && q.half >= 0 && q.half <= 32767, "dsg_flood: need step >= 1 and 0 <= half <= 32767");
@@ -93,7 +72,9 @@ int run_batch(const dsg_flood_req *reqs, uint32_t n, dsg_area *out, size_t pool_
         c.qx = q.qx; c.qz = q.qz; c.step = q.step; c.half = q.half; c.n = 2 * q.half + 1; c.tpr = (c.n + TILE - 1) / TILE;
         c.conn8 = q.conn8 ? 1 : 0; c.pred = q.pred; c.pcut = q.pcut; c.noise = it->second; c.dir_off = int64_t(dir_total);
         dir_total += size_t(c.tpr) * c.tpr;
+        dir_max = std::max<int64_t>(dir_max, int64_t(c.tpr) * c.tpr);
     }
+    const dim3 scan_grid(n, dir_chunks(dir_max));
     grow(g.d_ctl, g.ctl_cap, n);
     grow(g.d_stat, g.stat_cap, n);
     grow(g.d_noise, g.noise_cap, seeds.size());
@@ -103,52 +84,43 @@ int run_batch(const dsg_flood_req *reqs, uint32_t n, dsg_area *out, size_t pool_
         DSG_CU(cudaMalloc(&g.d_dir, dir_total * 4));
         g.dir_cap = dir_total;
     }
-    const uint32_t want_pool = uint32_t(std::min<size_t>(pool_bytes / (TILE_WORDS * 4), 0x7fffffff));
-    if (want_pool > g.pool_cap) {                      // the pool is kept zeroed between batches
-        cudaFree(g.d_pool); g.d_pool = nullptr;
-        DSG_CU(cudaMalloc(&g.d_pool, size_t(want_pool) * TILE_WORDS * 4));
-        DSG_CU(cudaMemset(g.d_pool, 0, size_t(want_pool) * TILE_WORDS * 4));
-        g.pool_cap = want_pool;
-    }
+    const uint32_t want_pool = uint32_t(std::min<size_t>(pool_bytes / TilePool::kBytesPerTile, 0x7fffffff));
+    if (want_pool > g.pool.cap) g.pool.allocate(want_pool);
     cudaStream_t st = g.st;
     DSG_CU(cudaMemcpyAsync(g.d_seeds, seeds.data(), seeds.size() * 8, cudaMemcpyHostToDevice, st));
     seed_noise_build(g.d_seeds, uint32_t(seeds.size()), g.d_noise, st);
     DSG_CU(cudaMemcpyAsync(g.d_ctl, ctl.data(), size_t(n) * sizeof(FloodCtl), cudaMemcpyHostToDevice, st));
     DSG_CU(cudaMemsetAsync(g.d_dir, 0xFF, dir_total * 4, st));
     DSG_CU(cudaMemsetAsync(g.d_cnt, 0, 8 * 4, st));
-    const TileAlloc ta{nullptr, 0, g.pool_cap, g.pool_cap, g.d_cnt + 3, nullptr, 0};
-    k_flood_start<<<(n + 127) / 128, 128, 0, st>>>(g.d_ctl, nullptr, n, g.d_stat, g.d_dir, g.d_pool, ta, g.d_list[0], g.d_cnt + 0, g.d_cnt + 4, Stamp{nullptr, 0});
+    const TileAlloc ta{nullptr, 0, g.pool.cap, g.pool.cap, g.d_cnt + 6, nullptr, 0};
+    k_tile_start<<<(n + 127) / 128, 128, 0, st>>>(g.d_ctl, nullptr, n, g.d_stat, g.d_dir, g.pool.T, ta, g.pool.n_list[0], g.d_cnt + 0,
+                                                  0, nullptr, g.d_cnt + 7);
     DSG_CU(cudaGetLastError());
-    const WorldDev w = world_dev();
-    const int K = 8;                                   // levels enqueued between completion checks
-    int level = 0;
+    const int K = 4;                                   // rounds enqueued between completion checks
+    uint32_t round = 0;
     for (;;) {
-        for (int k = 0; k < K; k++, level++) {
-            DSG_ARG(uint32_t(level) < g.hist_cap, "dsg_flood: BFS deeper than the level history");
-            k_flood_level<<<g.grid, 128, 0, st>>>(g.d_ctl, g.d_stat, g.d_noise, w, g.d_dir, g.d_pool, ta,
-                                                  g.d_list[level & 1], g.d_cnt + (level % 3), g.d_list[(level + 1) & 1],
-                                                  g.d_cnt + ((level + 1) % 3), g.d_cnt + ((level + 2) % 3), g.list_cap, g.d_hist, level, g.d_cnt + 4,
-                                                  Stamp{nullptr, 0});
-        }
+        for (int k = 0; k < K; k++, round++)
+            launch_round(g.pool, round, g.d_cnt, nullptr, g.d_cnt + 7, g.d_ctl, g.d_noise, g.d_dir, g.d_stat, ta, g.grid_eval, g.grid_conn, st);
         DSG_CU(cudaGetLastError());
-        DSG_CU(cudaMemcpyAsync(g.h_hist, g.d_hist + (level - K), K * 4, cudaMemcpyDeviceToHost, st));
+        DSG_CU(cudaMemcpyAsync(g.h_cnt, g.d_cnt, 8 * 4, cudaMemcpyDeviceToHost, st));
         DSG_CU(cudaStreamSynchronize(st));
-        if (g.h_hist[K - 1] == 0) break;
+        if (g.h_cnt[round % 3] == 0 && g.h_cnt[3 + round % 3] == 0) break;
     }
+    const uint32_t taken = g.h_cnt[6], flags = g.h_cnt[7];
+    k_tile_finish<<<scan_grid, 256, 0, st>>>(g.d_ctl, nullptr, g.d_dir, g.pool.T, g.d_stat, nullptr, 0, 0, nullptr);
+    DSG_CU(cudaGetLastError());
     std::vector<FloodStat> hs(n);
-    uint32_t flags[8];
     DSG_CU(cudaMemcpyAsync(hs.data(), g.d_stat, size_t(n) * sizeof(FloodStat), cudaMemcpyDeviceToHost, st));
-    DSG_CU(cudaMemcpyAsync(flags, g.d_cnt, 8 * 4, cudaMemcpyDeviceToHost, st));
     DSG_CU(cudaStreamSynchronize(st));
     int rc_cells = DSG_OK;
-    if (cell_off) {                                      // list passable cells before the tiles are cleared
+    if (cell_off) {                                      // list reached passable cells before the pool is reused
         unsigned long long *d_cnt = nullptr, *d_off = nullptr; int32_t *d_xz = nullptr;
         std::vector<unsigned long long> cnt(n), offs(n + 1, 0);
         auto fin = [&] { cudaFree(d_cnt); cudaFree(d_off); cudaFree(d_xz); };
         try {
             DSG_CU(cudaMalloc(&d_cnt, size_t(n) * 8)); DSG_CU(cudaMalloc(&d_off, size_t(n) * 8));
             DSG_CU(cudaMemsetAsync(d_cnt, 0, size_t(n) * 8, st));
-            k_cells<<<n, 256, 0, st>>>(g.d_ctl, g.d_dir, g.d_pool, d_cnt, nullptr, nullptr, 0);
+            k_cells<<<scan_grid, 256, 0, st>>>(g.d_ctl, g.d_dir, g.pool.T, d_cnt, nullptr, nullptr, 0);
             DSG_CU(cudaGetLastError());
             DSG_CU(cudaMemcpyAsync(cnt.data(), d_cnt, size_t(n) * 8, cudaMemcpyDeviceToHost, st));
             DSG_CU(cudaStreamSynchronize(st));
@@ -159,7 +131,7 @@ int run_batch(const dsg_flood_req *reqs, uint32_t n, dsg_area *out, size_t pool_
                 DSG_CU(cudaMalloc(&d_xz, size_t(offs[n]) * 8));
                 DSG_CU(cudaMemcpyAsync(d_off, offs.data(), size_t(n) * 8, cudaMemcpyHostToDevice, st));
                 DSG_CU(cudaMemsetAsync(d_cnt, 0, size_t(n) * 8, st));
-                k_cells<<<n, 256, 0, st>>>(g.d_ctl, g.d_dir, g.d_pool, d_cnt, d_off, d_xz, offs[n]);
+                k_cells<<<scan_grid, 256, 0, st>>>(g.d_ctl, g.d_dir, g.pool.T, d_cnt, d_off, d_xz, offs[n]);
                 DSG_CU(cudaGetLastError());
                 DSG_CU(cudaMemcpyAsync(cell_xz, d_xz, size_t(offs[n]) * 8, cudaMemcpyDeviceToHost, st));
                 DSG_CU(cudaStreamSynchronize(st));
@@ -167,16 +139,15 @@ int run_batch(const dsg_flood_req *reqs, uint32_t n, dsg_area *out, size_t pool_
         } catch (...) { fin(); throw; }
         fin();
     }
-    // return the tiles this batch used to the zeroed state
-    DSG_CU(cudaMemsetAsync(g.d_pool, 0, size_t(std::min(flags[3], g.pool_cap)) * TILE_WORDS * 4, st));
+    g.pool.reset(taken, st);                             // the next batch allocates from tile 0 again
     for (uint32_t r = 0; r < n; r++) {
         const FloodStat &s = hs[r];
         out[r].cells = s.cells; out[r].sampled = s.sampled;
         out[r].minx = s.minx; out[r].maxx = s.maxx; out[r].minz = s.minz; out[r].maxz = s.maxz;
         out[r].edge = s.edge; out[r].border = s.border;
     }
-    if (flags[4]) {
-        set_error("dsg_flood: %s exhausted (pool %u tiles, list %u entries)", (flags[4] & 1) ? "tile pool" : "level list", g.pool_cap, g.list_cap);
+    if (flags & 1) {
+        set_error("dsg_flood: tile pool exhausted (%u tiles of %d x %d cells)", g.pool.cap, TILE, TILE);
         return DSG_OVERFLOW;
     }
     return rc_cells;

@@ -1,12 +1,30 @@
-// Device side of the bridged flood engine, shared by the one-shot batch (flood.cu) and the continuously
-// batched service (service.cu).  See flood.cu for the algorithm.
+// Device side of the tile flood engine, shared by the one-shot batch (flood.cu) and the continuously
+// batched service (service.cu).
+//
+// The reference floods by a depth-first walk over a (2*half+1)^2 byte window (src/dense_flood.hpp:20-86):
+// each cell it touches is evaluated once, and passable cells push their neighbours.  Its result depends only
+// on the set R of passable cells connected to the start (and on the cells adjacent to R), not on the visit
+// order.  The engine therefore evaluates the predicate speculatively over whole 64x64 tiles of the window and
+// finds R by bit-parallel fills:
+//  * a tile is claimed (directory atomicCAS) when R reaches its edge; claimed tiles are evaluated in the next
+//    round by k_tile_eval, every cell at once (16 blocks of 256 cells per tile), into bit rows P (passable)
+//    and D (desert, counted); the rare cells the surface grid cannot decide are finished in the same block
+//    by warp-cooperative tree searches;
+//  * k_tile_connect grows R inside each queued tile to its fixed point (row fills, column fills across the
+//    warp, the diagonal step for 8-connectivity), seeded from the R edges of the neighbouring tiles; when R
+//    changes on an edge it queues the neighbour, or claims it if it does not exist yet.  R only grows, so the
+//    rounds reach the unique fixed point whatever the interleaving;
+//  * when a request has no queued tile left, k_tile_finish derives DenseArea from R, D and the neighbours:
+//    cells = |R & D|, bbox over R & D, touched = start + R + neighbours of R, sampled = touched cells inside
+//    window and world, border = a touched cell outside the world, edge = an R cell on the window boundary.
 #pragma once
 #include "noise.cuh"
+#include <algorithm>
 
 namespace dsg {
 namespace flood {
 
-struct FloodCtl {                      // one request, as the level kernel sees it
+struct FloodCtl {                      // one request
     int32_t qx, qz, step, half, n, tpr, conn8, pred;
     float pcut; int32_t noise; int64_t dir_off;
 };
@@ -17,154 +35,497 @@ struct FloodStat {
 static_assert(sizeof(FloodStat) == 48, "FloodStat layout");
 
 constexpr int kWorld = 7499996;
-constexpr int TILE = 64, TILE_WORDS = TILE * TILE * 2 / 32;     // 256 x 32-bit words per tile
+constexpr int TILE = 64;
+constexpr int TILE_U64 = 3 * TILE;     // rows of P, D, R
+constexpr int EVAL_THREADS = 256, EVAL_ITEMS = TILE * TILE / EVAL_THREADS;   // 16 blocks of 4 rows per tile
 
-// Tiles come from a pre-zeroed pool: the k-th tile taken since the last host update is ring[(head + k) % cap]
+// Tiles come from a pool: the k-th tile taken since the last host update is ring[(head + k) % cap]
 // (ring == nullptr: tile k itself, a bump allocator).  Taking never waits; `avail` bounds it.
 // returned (service only): a tile taken by a thread that then lost the directory race goes back to the ring
 // at (tail + k) % cap, k counted by *returned (those ring positions are free while head..head+avail are not).
 struct TileAlloc { uint32_t *ring; uint32_t head, avail, cap; uint32_t *taken; uint32_t *returned; uint32_t tail; };
-// Level stamps (service): active[r] = level + 1 when level `level` appends a cell of request r.
-struct Stamp { uint32_t *active; int level; };
+// Per-tile storage.  bits: tile t holds P rows at [t*192, +64), D rows at +64, R rows at +128 (bit c of
+// row r = cell (64*ti + c, 64*tj + r) of the window).  state: 1 once evaluated (0 while claimed, reset on
+// release); done: evaluated row blocks; mark: 1 + the round the tile was last queued for connect.
+struct Tiles { uint64_t *bits; uint32_t *owner, *pos, *state, *done, *mark; };
+// Queues of one round: n (claimed, to evaluate), w (to connect); *_next are the next round's.
+struct Round {
+    uint32_t round;
+    const uint32_t *n_list; const uint32_t *n_cnt;
+    uint32_t *w_list; uint32_t *w_cnt;
+    uint32_t *n_next; uint32_t *n_next_cnt;
+    uint32_t *w_next; uint32_t *w_next_cnt;
+    uint32_t *zero_a, *zero_b;         // counters of the round after next, cleared by connect
+    uint32_t *active;                  // per request: the last round it has queued work for (service)
+    uint32_t *err;                     // bit 0: tile pool exhausted
+};
 
-__device__ __forceinline__ uint32_t *tile_word(const FloodCtl &c, int32_t *__restrict__ dir, uint32_t *__restrict__ pool,
-                                               const TileAlloc &ta, int i, int j, int &bit, bool &oom) {
-    const int64_t di = c.dir_off + int64_t(j >> 6) * c.tpr + (i >> 6);
-    int32_t d = __ldcg(&dir[di]);
-    if (d < 0) {
-        const uint32_t k = atomicAdd(ta.taken, 1u);
-        if (k >= ta.avail) { oom = true; return nullptr; }
-        const int32_t nt = int32_t(ta.ring ? ta.ring[(ta.head + k) % ta.cap] : k);
-        const int32_t old = atomicCAS(&dir[di], -1, nt);
-        d = old == -1 ? nt : old;
-        if (old != -1 && ta.returned) ta.ring[(ta.tail + atomicAdd(ta.returned, 1u)) % ta.cap] = uint32_t(nt);
-    }
-    bit = 2 * (i & 15);
-    return pool + size_t(d) * TILE_WORDS + (j & 63) * 4 + ((i & 63) >> 4);
-}
-
-__device__ __forceinline__ int eval_pred(const FloodCtl &c, const SeedNoise &S, const WorldDev &w, int x, int z) {
-    if (c.pred == DSG_PRED_DESERT) return desert_state(S, w, x, z);
+// Predicate value, or -1 when a desert point needs the tree search (finished by classify_deferred_warp).
+__device__ __forceinline__ int eval_pred(const FloodCtl &c, const SeedNoise &S, const WorldDev &w, int x, int z, Deferred &fb) {
+    if (c.pred == DSG_PRED_DESERT) return desert_state_grid(S, w, x, z, fb);
     if (c.pred == DSG_PRED_HOT) return hot_state(S, x, z);
     return proxy_prob(S, w, x, z) >= c.pcut ? 2 : 0;
 }
 
-// Touch the start cell of every request (dense_flood.hpp:81): it is the first level's only cell.
-// slots (may be nullptr): the request indices to start; else requests 0..nreq-1.
-static __global__ void k_flood_start(const FloodCtl *__restrict__ ctl, const uint32_t *__restrict__ slots, uint32_t nreq, FloodStat *__restrict__ st,
-                              int32_t *__restrict__ dir, uint32_t *__restrict__ pool, TileAlloc ta, uint64_t *__restrict__ out,
-                              uint32_t *__restrict__ n_out, uint32_t *__restrict__ err, Stamp stamp) {
+// Claim tile (ti, tj) of request r for evaluation in round `eval_round`, or return the existing one.
+// Returns the pool index, or -1 when the pool is exhausted (the request is marked overflowed).
+__device__ inline int32_t claim_tile(const FloodCtl &c, uint32_t r, int ti, int tj, int32_t *__restrict__ dir, const Tiles &T,
+                                     const TileAlloc &ta, uint32_t *n_out, uint32_t *n_out_cnt, uint32_t eval_round,
+                                     uint32_t *active, FloodStat *__restrict__ st, uint32_t *err) {
+    int32_t *e = dir + c.dir_off + int64_t(tj) * c.tpr + ti;
+    const int32_t d = __ldcg(e);
+    if (d >= 0) return d;
+    const uint32_t k = atomicAdd(ta.taken, 1u);
+    if (k >= ta.avail) { st[r].overflow = 1; atomicOr(err, 1u); return -1; }
+    const int32_t nt = int32_t(ta.ring ? ta.ring[(ta.head + k) % ta.cap] : k);
+    const int32_t old = atomicCAS(e, -1, nt);
+    if (old != -1) {
+        if (ta.returned) ta.ring[(ta.tail + atomicAdd(ta.returned, 1u)) % ta.cap] = uint32_t(nt);
+        return old;
+    }
+    T.owner[nt] = r;
+    T.pos[nt] = uint32_t(ti) | (uint32_t(tj) << 16);
+    n_out[atomicAdd(n_out_cnt, 1u)] = uint32_t(nt);
+    if (active) active[r] = eval_round;
+    return nt;
+}
+
+// Start requests (slots, or 0..nreq-1): statistics reset, start tile claimed for evaluation in `round`.
+static __global__ void k_tile_start(const FloodCtl *__restrict__ ctl, const uint32_t *__restrict__ slots, uint32_t nreq,
+                                    FloodStat *__restrict__ st, int32_t *__restrict__ dir, Tiles T, TileAlloc ta,
+                                    uint32_t *n_list, uint32_t *n_cnt, uint32_t round, uint32_t *active, uint32_t *err) {
     const uint32_t q = blockIdx.x * blockDim.x + threadIdx.x;
     if (q >= nreq) return;
     const uint32_t r = slots ? slots[q] : q;
     const FloodCtl c = ctl[r];
     FloodStat &s = st[r];
     s.cells = 0; s.sampled = 0; s.minx = s.maxx = c.qx; s.minz = s.maxz = c.qz; s.edge = s.border = s.overflow = 0;
-    int bit; bool oom = false;
-    uint32_t *wd = tile_word(c, dir, pool, ta, c.half, c.half, bit, oom);
-    if (oom) { s.overflow = 1; atomicOr(err, 1u); return; }
-    atomicOr(wd, 1u << bit);
-    if (c.qx < -kWorld || c.qx > kWorld || c.qz < -kWorld || c.qz > kWorld) { s.border = 1; return; }
-    const uint32_t k = atomicAdd(n_out, 1u);
-    out[k] = (uint64_t(r) << 32) | (uint64_t(c.half) << 16) | uint64_t(c.half);
-    if (stamp.active) stamp.active[r] = uint32_t(stamp.level);
+    claim_tile(c, r, c.half >> 6, c.half >> 6, dir, T, ta, n_list, n_cnt, round, active, st, err);
 }
 
-static __global__ void __launch_bounds__(128) k_flood_level(const FloodCtl *__restrict__ ctl, FloodStat *__restrict__ st,
-        const SeedNoise *__restrict__ noise, WorldDev w, int32_t *__restrict__ dir, uint32_t *__restrict__ pool, TileAlloc ta,
-        const uint64_t *__restrict__ in, const uint32_t *__restrict__ n_in_p,
-        uint64_t *__restrict__ out, uint32_t *__restrict__ n_out, uint32_t *__restrict__ n_zero, uint32_t cap,
-        uint32_t *__restrict__ hist, int level, uint32_t *__restrict__ err, Stamp stamp) {
-    const uint32_t n_in_raw = *n_in_p, n_in = min(n_in_raw, cap);
-    if (blockIdx.x == 0 && threadIdx.x == 0) { *n_zero = 0; hist[level] = n_in_raw; if (n_in_raw > cap) atomicOr(err, 2u); }
-    const int lane = threadIdx.x & 31;
-    const uint32_t stride = gridDim.x * blockDim.x;
-    for (uint32_t base = blockIdx.x * blockDim.x + (threadIdx.x & ~31u); base < n_in; base += stride) {
-        const uint32_t idx = base + lane;
-        bool pass = false;
-        uint32_t r = 0; int i = 0, j = 0;
-        FloodCtl c{};
-        if (idx < n_in) {
-            const uint64_t e = in[idx];
-            r = uint32_t(e >> 32); j = int((e >> 16) & 0xFFFF); i = int(e & 0xFFFF);
-            c = ctl[r];
+// Evaluate claimed tiles: block item = (tile, 4 rows); warp = half a row.  Deferred desert cells are listed
+// in shared memory and finished by the block's warps, one cooperative tree search per cell.  The last row
+// block of a tile to finish marks it evaluated and queues it for this round's connect.
+static __global__ void __launch_bounds__(EVAL_THREADS) k_tile_eval(const FloodCtl *__restrict__ ctl, const SeedNoise *__restrict__ noise,
+                                                                   WorldDev w, Tiles T, Round q) {
+    __shared__ int32_t s_param[512];
+    __shared__ Deferred s_def[EVAL_THREADS];
+    __shared__ int32_t s_res[EVAL_THREADS];
+    __shared__ int s_n;
+    const uint32_t items = *q.n_cnt * EVAL_ITEMS;
+    if (blockIdx.x >= items) return;
+    for (int k = threadIdx.x; k < 2 * w.nparam; k += blockDim.x) s_param[k] = w.param[k];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    for (uint32_t item = blockIdx.x; item < items; item += gridDim.x) {
+        const uint32_t t = q.n_list[item / EVAL_ITEMS];
+        const int row = int(item % EVAL_ITEMS) * 4 + (warp >> 1), col = ((warp & 1) << 5) | lane;
+        const uint32_t r = T.owner[t], pos = T.pos[t];
+        const FloodCtl c = ctl[r];
+        const int i = int(pos & 0xffff) * TILE + col, j = int(pos >> 16) * TILE + row;
+        __syncthreads();                                  // previous item's list consumed; parameters staged
+        if (threadIdx.x == 0) s_n = 0;
+        __syncthreads();
+        int v = 0, slot = -1;
+        if (i < c.n && j < c.n) {
             const int x = c.qx + (i - c.half) * c.step, z = c.qz + (j - c.half) * c.step;
-            const int v = eval_pred(c, noise[c.noise], w, x, z);
-            FloodStat &s = st[r];
-            atomicAdd(&s.sampled, 1ull);
-            if (v) {
-                pass = true;
-                int bit; bool oom = false;
-                uint32_t *wd = tile_word(c, dir, pool, ta, i, j, bit, oom);
-                if (wd) atomicOr(wd, 2u << bit);
-                if (v == 2) {
-                    atomicAdd(&s.cells, 1ull);
-                    atomicMin(&s.minx, x); atomicMax(&s.maxx, x);
-                    atomicMin(&s.minz, z); atomicMax(&s.maxz, z);
-                }
+            if (x >= -kWorld && x <= kWorld && z >= -kWorld && z <= kWorld) {
+                Deferred fb;
+                v = eval_pred(c, noise[c.noise], w, x, z, fb);
+                if (v < 0) { slot = atomicAdd(&s_n, 1); s_def[slot] = fb; }
             }
         }
-        // expand: 4 orthogonal neighbours, then the diagonals for 8-connected requests (dense_flood.hpp:82-83)
-        #pragma unroll 1
-        for (int dd = 0; dd < 8; dd++) {
-            bool add = false;
-            int ni = 0, nj = 0;
-            if (pass && (dd < 4 || c.conn8)) {
-                const int di = dd == 0 ? -1 : dd == 1 ? 1 : dd == 2 ? 0 : dd == 3 ? 0 : (dd & 1) ? 1 : -1;
-                const int dj = dd < 2 ? 0 : dd == 2 ? -1 : dd == 3 ? 1 : dd < 6 ? -1 : 1;
-                ni = i + di; nj = j + dj;
-                FloodStat &s = st[r];
-                if (ni < 0 || nj < 0 || ni >= c.n || nj >= c.n) s.edge = 1;
-                else {
-                    int bit; bool oom = false;
-                    uint32_t *wd = tile_word(c, dir, pool, ta, ni, nj, bit, oom);
-                    if (oom) { s.overflow = 1; atomicOr(err, 1u); }
-                    else if (!((atomicOr(wd, 1u << bit) >> bit) & 1u)) {
-                        const int x = c.qx + (ni - c.half) * c.step, z = c.qz + (nj - c.half) * c.step;
-                        if (x < -kWorld || x > kWorld || z < -kWorld || z > kWorld) s.border = 1;
-                        else add = true;
-                    }
-                }
-            }
-            const uint32_t m = __ballot_sync(0xffffffffu, add);
-            if (m) {
-                uint32_t at = 0;
-                if (lane == __ffs(m) - 1) at = atomicAdd(n_out, uint32_t(__popc(m)));
-                at = __shfl_sync(0xffffffffu, at, __ffs(m) - 1);
-                if (add) {
-                    const uint32_t k = at + __popc(m & ((1u << lane) - 1));
-                    if (k < cap) out[k] = (uint64_t(r) << 32) | (uint64_t(nj) << 16) | uint64_t(ni);
-                    if (stamp.active) stamp.active[r] = uint32_t(stamp.level + 1);
-                }
+        __syncthreads();
+        const int nd = s_n;
+        for (int e = warp; e < nd; e += EVAL_THREADS / 32) {
+            const int res = classify_deferred_warp(w, s_param, s_def[e]);
+            if (lane == 0) s_res[e] = res;
+        }
+        __syncthreads();
+        if (slot >= 0) v = s_res[slot];
+        const uint32_t pm = __ballot_sync(0xffffffffu, v > 0), dm = __ballot_sync(0xffffffffu, v == 2);
+        if (lane == 0) {
+            uint32_t *b = reinterpret_cast<uint32_t *>(T.bits + size_t(t) * TILE_U64);
+            const int h = 2 * row + (warp & 1);
+            b[h] = pm; b[2 * TILE + h] = dm; b[4 * TILE + h] = 0;
+        }
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            __threadfence();
+            if (atomicAdd(&T.done[t], 1u) == EVAL_ITEMS - 1) {
+                T.state[t] = 1;
+                if (atomicExch(&T.mark[t], q.round + 1) != q.round + 1) q.w_list[atomicAdd(q.w_cnt, 1u)] = t;
             }
         }
     }
 }
 
-// Passable cells of each request (touched + passable bits), counted then listed.  One block per request.
-static __global__ void k_cells(const FloodCtl *__restrict__ ctl, const int32_t *__restrict__ dir, const uint32_t *__restrict__ pool,
-                        unsigned long long *__restrict__ cnt, const unsigned long long *__restrict__ off, int32_t *__restrict__ xz, uint64_t cap) {
+// ---------------------------------------------------------------- bit rows of one tile across a warp
+// Lane l holds rows l ("a") and l + 32 ("b").
+// Rows moved by k (1 <= k <= 32) towards higher row numbers: row r receives row r - k (0 above the tile).
+__device__ __forceinline__ void rows_down(uint64_t a, uint64_t b, int k, uint64_t &oa, uint64_t &ob) {
+    const int lane = threadIdx.x & 31;
+    const int src = (lane - k) & 31;
+    const uint64_t xa = __shfl_sync(0xffffffffu, a, src), xb = __shfl_sync(0xffffffffu, b, src);
+    oa = lane >= k ? xa : 0;
+    ob = lane >= k ? xb : xa;
+}
+// Rows moved by k towards lower row numbers: row r receives row r + k (0 below the tile).
+__device__ __forceinline__ void rows_up(uint64_t a, uint64_t b, int k, uint64_t &oa, uint64_t &ob) {
+    const int lane = threadIdx.x & 31;
+    const int src = (lane + k) & 31;
+    const uint64_t xa = __shfl_sync(0xffffffffu, a, src), xb = __shfl_sync(0xffffffffu, b, src);
+    oa = lane + k < 32 ? xa : xb;
+    ob = lane + k < 32 ? xb : 0;
+}
+__device__ __forceinline__ uint64_t h1(uint64_t x) { return x | (x << 1) | (x >> 1); }
+// Cells of p connected to g along the row (occluded fills towards both ends in log steps).
+__device__ __forceinline__ uint64_t row_fill(uint64_t g, uint64_t p) {
+    uint64_t q = p, h = g;
+    h |= q & (h << 1);  q &= q << 1;
+    h |= q & (h << 2);  q &= q << 2;
+    h |= q & (h << 4);  q &= q << 4;
+    h |= q & (h << 8);  q &= q << 8;
+    h |= q & (h << 16); q &= q << 16;
+    h |= q & (h << 32);
+    q = p;
+    h |= q & (h >> 1);  q &= q >> 1;
+    h |= q & (h >> 2);  q &= q >> 2;
+    h |= q & (h >> 4);  q &= q >> 4;
+    h |= q & (h >> 8);  q &= q >> 8;
+    h |= q & (h >> 16); q &= q >> 16;
+    h |= q & (h >> 32);
+    return h;
+}
+// Cells of p connected to g along the columns, across the warp.
+__device__ __forceinline__ void col_fill(uint64_t &ga, uint64_t &gb, uint64_t pa, uint64_t pb) {
+    uint64_t qa = pa, qb = pb, sa, sb;
+    #pragma unroll
+    for (int k = 1; k <= 32; k <<= 1) {
+        rows_down(ga, gb, k, sa, sb); ga |= qa & sa; gb |= qb & sb;
+        if (k < 32) { rows_down(qa, qb, k, sa, sb); qa &= sa; qb &= sb; }
+    }
+    qa = pa; qb = pb;
+    #pragma unroll
+    for (int k = 1; k <= 32; k <<= 1) {
+        rows_up(ga, gb, k, sa, sb); ga |= qa & sa; gb |= qb & sb;
+        if (k < 32) { rows_up(qa, qb, k, sa, sb); qa &= sa; qb &= sb; }
+    }
+}
+// R and the 4 (or 8) neighbours of every R cell, inside the tile.
+__device__ __forceinline__ void dilate(uint64_t ra, uint64_t rb, bool conn8, uint64_t &oa, uint64_t &ob) {
+    const uint64_t xa = conn8 ? h1(ra) : ra, xb = conn8 ? h1(rb) : rb;
+    uint64_t da, db, ua, ub;
+    rows_down(xa, xb, 1, da, db);
+    rows_up(xa, xb, 1, ua, ub);
+    oa = h1(ra) | da | ua;
+    ob = h1(rb) | db | ub;
+}
+
+// Tile of request c at (ti, tj), or -1 (outside the window, not claimed, or, with need_eval, not evaluated).
+__device__ __forceinline__ int32_t tile_at(const FloodCtl &c, const int32_t *__restrict__ dir, const Tiles &T, int ti, int tj, bool need_eval) {
+    if (ti < 0 || tj < 0 || ti >= c.tpr || tj >= c.tpr) return -1;
+    const int32_t d = __ldcg(dir + c.dir_off + int64_t(tj) * c.tpr + ti);
+    if (d < 0 || (need_eval && __ldcg(&T.state[d]) != 1)) return -1;
+    return d;
+}
+__device__ __forceinline__ uint64_t r_row(const Tiles &T, int32_t d, int row) {
+    return d < 0 ? 0 : __ldcg(&T.bits[size_t(d) * TILE_U64 + 2 * TILE + row]);
+}
+// Cells of this tile adjacent (4 or 8) to R cells of the neighbouring tiles, rows a/b of this lane.
+__device__ inline void outside_seeds(const FloodCtl &c, const int32_t *__restrict__ dir, const Tiles &T, int ti, int tj,
+                                     bool need_eval, uint64_t &sa, uint64_t &sb) {
+    const int lane = threadIdx.x & 31;
+    const bool c8 = c.conn8 != 0;
+    const int32_t L = tile_at(c, dir, T, ti - 1, tj, need_eval), Rt = tile_at(c, dir, T, ti + 1, tj, need_eval);
+    const int32_t U = tile_at(c, dir, T, ti, tj - 1, need_eval), Dn = tile_at(c, dir, T, ti, tj + 1, need_eval);
+    // column 63 of the left tile and column 0 of the right one, as bit 0 / bit 63 of each row
+    uint64_t xa = (r_row(T, L, lane) >> 63) | ((r_row(T, Rt, lane) & 1) << 63);
+    uint64_t xb = (r_row(T, L, lane + 32) >> 63) | ((r_row(T, Rt, lane + 32) & 1) << 63);
+    if (c8) {                                            // rows r - 1 and r + 1 of those columns as well
+        uint64_t d0, d1, u0, u1;
+        rows_down(xa, xb, 1, d0, d1);
+        rows_up(xa, xb, 1, u0, u1);
+        xa |= d0 | u0; xb |= d1 | u1;
+    }
+    sa = xa; sb = xb;
+    if (lane == 0) {                                     // row 0 from row 63 of the tile above
+        const uint64_t u = r_row(T, U, 63);
+        sa |= c8 ? h1(u) : u;
+        if (c8) {
+            sa |= r_row(T, tile_at(c, dir, T, ti - 1, tj - 1, need_eval), 63) >> 63;
+            sa |= (r_row(T, tile_at(c, dir, T, ti + 1, tj - 1, need_eval), 63) & 1) << 63;
+        }
+    }
+    if (lane == 31) {                                    // row 63 from row 0 of the tile below
+        const uint64_t d = r_row(T, Dn, 0);
+        sb |= c8 ? h1(d) : d;
+        if (c8) {
+            sb |= r_row(T, tile_at(c, dir, T, ti - 1, tj + 1, need_eval), 0) >> 63;
+            sb |= (r_row(T, tile_at(c, dir, T, ti + 1, tj + 1, need_eval), 0) & 1) << 63;
+        }
+    }
+}
+__device__ __forceinline__ void start_bit(const FloodCtl &c, int ti, int tj, uint64_t &sa, uint64_t &sb) {
+    const int lane = threadIdx.x & 31;
+    if (ti != (c.half >> 6) || tj != (c.half >> 6)) return;
+    const int row = c.half & 63;
+    const uint64_t bit = 1ull << (c.half & 63);
+    if (row == lane) sa |= bit;
+    if (row == lane + 32) sb |= bit;
+}
+
+// Grow R of every queued tile to its fixed point; queue or claim the neighbours its new edge cells reach.
+static __global__ void __launch_bounds__(256) k_tile_connect(const FloodCtl *__restrict__ ctl, int32_t *__restrict__ dir, Tiles T,
+                                                             TileAlloc ta, FloodStat *__restrict__ st, Round q) {
+    if (blockIdx.x == 0 && threadIdx.x == 0) { *q.zero_a = 0; *q.zero_b = 0; }
+    const uint32_t n = *q.w_cnt;
+    const int lane = threadIdx.x & 31;
+    const uint32_t nw = gridDim.x * (blockDim.x >> 5);
+    for (uint32_t idx = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5); idx < n; idx += nw) {
+        const uint32_t t = q.w_list[idx];
+        const uint32_t r = T.owner[t], pos = T.pos[t];
+        const FloodCtl c = ctl[r];
+        const int ti = int(pos & 0xffff), tj = int(pos >> 16);
+        const bool c8 = c.conn8 != 0;
+        uint64_t *tb = T.bits + size_t(t) * TILE_U64;
+        const uint64_t pa = __ldcg(&tb[lane]), pb = __ldcg(&tb[lane + 32]);
+        const uint64_t ra0 = __ldcg(&tb[2 * TILE + lane]), rb0 = __ldcg(&tb[2 * TILE + lane + 32]);
+        uint64_t sa, sb;
+        outside_seeds(c, dir, T, ti, tj, true, sa, sb);
+        start_bit(c, ti, tj, sa, sb);
+        uint64_t ra = ra0 | (sa & pa), rb = rb0 | (sb & pb);
+        for (;;) {                                       // R grows monotonically inside P: this terminates
+            const uint64_t oa = ra, ob = rb;
+            ra = row_fill(ra, pa); rb = row_fill(rb, pb);
+            col_fill(ra, rb, pa, pb);
+            if (c8) {
+                uint64_t da, db;
+                dilate(ra, rb, true, da, db);
+                ra |= da & pa; rb |= db & pb;
+            }
+            if (!__any_sync(0xffffffffu, ra != oa || rb != ob)) break;
+        }
+        const uint64_t na = ra ^ ra0, nb = rb ^ rb0;
+        if (!__any_sync(0xffffffffu, (na | nb) != 0)) continue;
+        tb[2 * TILE + lane] = ra; tb[2 * TILE + lane + 32] = rb;
+        // neighbours reached through new edge cells: lane k < 8 handles neighbour k
+        const uint64_t top = __shfl_sync(0xffffffffu, na, 0), bot = __shfl_sync(0xffffffffu, nb, 31);
+        const bool left = __any_sync(0xffffffffu, ((na | nb) & 1) != 0), right = __any_sync(0xffffffffu, ((na | nb) >> 63) != 0);
+        bool need = false; int dti = 0, dtj = 0;
+        switch (lane) {
+            case 0: need = top != 0; dtj = -1; break;
+            case 1: need = bot != 0; dtj = 1; break;
+            case 2: need = left; dti = -1; break;
+            case 3: need = right; dti = 1; break;
+            case 4: need = c8 && (top & 1); dti = -1; dtj = -1; break;
+            case 5: need = c8 && (top >> 63); dti = 1; dtj = -1; break;
+            case 6: need = c8 && (bot & 1); dti = -1; dtj = 1; break;
+            case 7: need = c8 && (bot >> 63); dti = 1; dtj = 1; break;
+            default: break;
+        }
+        const int nti = ti + dti, ntj = tj + dtj;
+        if (need && nti >= 0 && ntj >= 0 && nti < c.tpr && ntj < c.tpr) {
+            const int32_t d = __ldcg(dir + c.dir_off + int64_t(ntj) * c.tpr + nti);
+            if (d < 0) claim_tile(c, r, nti, ntj, dir, T, ta, q.n_next, q.n_next_cnt, q.round + 1, q.active, st, q.err);
+            else if (__ldcg(&T.state[d]) == 1) {         // evaluated: connect it again next round
+                if (atomicExch(&T.mark[d], q.round + 2) != q.round + 2) {
+                    q.w_next[atomicAdd(q.w_next_cnt, 1u)] = uint32_t(d);
+                    if (q.active) q.active[r] = q.round + 1;
+                }
+            }                                            // else claimed this round: connected after its evaluation
+        }
+    }
+}
+
+__device__ __forceinline__ int64_t floor_div(int64_t a, int64_t b) { const int64_t q = a / b; return (a % b != 0 && a < 0) ? q - 1 : q; }
+__device__ __forceinline__ int clamp_bit(int64_t v) { return int(v < -1 ? -1 : v > 64 ? 64 : v); }
+__device__ __forceinline__ uint64_t span_mask(int lo, int hi) {          // bits lo..hi of a row (empty if lo > hi)
+    lo = max(lo, 0); hi = min(hi, 63);
+    if (lo > hi) return 0;
+    return (~0ull >> (63 - hi)) & (~0ull << lo);
+}
+
+// DenseArea contribution of one finished tile (whole warp): counts, bbox and flags into st.
+__device__ inline void tile_stats(const FloodCtl &c, const int32_t *__restrict__ dir, const Tiles &T, int32_t t, int ti, int tj,
+                                  FloodStat &st) {
+    const int lane = threadIdx.x & 31;
+    const uint64_t *tb = T.bits + size_t(t) * TILE_U64;
+    const uint64_t ra = __ldcg(&tb[2 * TILE + lane]), rb = __ldcg(&tb[2 * TILE + lane + 32]);
+    const uint64_t xa = ra & __ldcg(&tb[TILE + lane]), xb = rb & __ldcg(&tb[TILE + lane + 32]);
+    // touched cells: R, its neighbours in this tile, neighbours of the adjacent tiles' R, the start
+    uint64_t ua, ub, sa, sb;
+    dilate(ra, rb, c.conn8 != 0, ua, ub);
+    outside_seeds(c, dir, T, ti, tj, false, sa, sb);
+    start_bit(c, ti, tj, sa, sb);
+    ua |= sa; ub |= sb;
+    // window and world (cell (i, j) is quart (qx + (i - half) * step, qz + (j - half) * step))
+    const int i0 = ti * TILE, j0 = tj * TILE;
+    const uint64_t win_cols = span_mask(0, c.n - 1 - i0);
+    const int64_t ilo = c.half + floor_div(-int64_t(kWorld) - c.qx + c.step - 1, c.step), ihi = c.half + floor_div(int64_t(kWorld) - c.qx, c.step);
+    const int64_t jlo = c.half + floor_div(-int64_t(kWorld) - c.qz + c.step - 1, c.step), jhi = c.half + floor_div(int64_t(kWorld) - c.qz, c.step);
+    const uint64_t world_cols = span_mask(clamp_bit(ilo - i0), clamp_bit(ihi - i0));
+    const int ja = j0 + lane, jb = j0 + lane + 32;
+    const uint64_t tva = ja < c.n ? ua & win_cols : 0, tvb = jb < c.n ? ub & win_cols : 0;
+    const bool ina = ja >= jlo && ja <= jhi, inb = jb >= jlo && jb <= jhi;
+    unsigned long long sampled = __popcll(ina ? tva & world_cols : 0) + __popcll(inb ? tvb & world_cols : 0);
+    const bool border = (ina ? tva & ~world_cols : tva) != 0 || (inb ? tvb & ~world_cols : tvb) != 0;
+    unsigned long long cells = __popcll(xa) + __popcll(xb);
+    // edge: an R cell on the window boundary
+    const uint64_t bcols = (i0 == 0 ? 1ull : 0ull) | span_mask(c.n - 1 - i0, c.n - 1 - i0);
+    const bool edge = (ra & bcols) || (rb & bcols) || (ra && (ja == 0 || ja == c.n - 1)) || (rb && jb == c.n - 1);
+    // bbox of R & D
+    int cmin = 64, cmax = -1, rmin = 64, rmax = -1;
+    if (xa) { cmin = __ffsll(xa) - 1; cmax = 63 - __clzll(xa); rmin = lane; rmax = lane; }
+    if (xb) { cmin = min(cmin, __ffsll(xb) - 1); cmax = max(cmax, 63 - __clzll(xb)); rmin = xa ? rmin : lane + 32; rmax = lane + 32; }
+    #pragma unroll
+    for (int o = 16; o; o >>= 1) {
+        sampled += __shfl_xor_sync(0xffffffffu, sampled, o);
+        cells += __shfl_xor_sync(0xffffffffu, cells, o);
+        cmin = min(cmin, __shfl_xor_sync(0xffffffffu, cmin, o)); cmax = max(cmax, __shfl_xor_sync(0xffffffffu, cmax, o));
+        rmin = min(rmin, __shfl_xor_sync(0xffffffffu, rmin, o)); rmax = max(rmax, __shfl_xor_sync(0xffffffffu, rmax, o));
+    }
+    const bool any_border = __any_sync(0xffffffffu, border), any_edge = __any_sync(0xffffffffu, edge);
+    if (lane == 0) {
+        if (sampled) atomicAdd(&st.sampled, sampled);
+        if (cells) {
+            atomicAdd(&st.cells, cells);
+            atomicMin(&st.minx, c.qx + (i0 + cmin - c.half) * c.step); atomicMax(&st.maxx, c.qx + (i0 + cmax - c.half) * c.step);
+            atomicMin(&st.minz, c.qz + (j0 + rmin - c.half) * c.step); atomicMax(&st.maxz, c.qz + (j0 + rmax - c.half) * c.step);
+        }
+        if (any_border) st.border = 1;
+        if (any_edge) st.edge = 1;
+    }
+}
+
+// Directory entries one block of k_tile_finish / k_cells scans (blockIdx.y = chunk of the directory).
+constexpr int DIR_CHUNK = 4096;
+inline unsigned dir_chunks(int64_t max_entries) { return unsigned((max_entries + DIR_CHUNK - 1) / DIR_CHUNK); }
+// Finished requests (slots, or 0..gridDim.x-1; blockIdx.y = directory chunk): statistics of every tile.  With ring != nullptr
+// the tiles are then released (state cleared, index appended to the free ring at tail + *returned).
+static __global__ void __launch_bounds__(256) k_tile_finish(const FloodCtl *__restrict__ ctl, const uint32_t *__restrict__ slots,
+                                                            const int32_t *__restrict__ dir, Tiles T, FloodStat *__restrict__ st,
+                                                            uint32_t *__restrict__ ring, uint32_t cap, uint32_t tail, uint32_t *__restrict__ returned) {
+    const uint32_t r = slots ? slots[blockIdx.x] : blockIdx.x;
+    const FloodCtl c = ctl[r];
+    const int lane = threadIdx.x & 31;
+    const int64_t entries = min(int64_t(c.tpr) * c.tpr, int64_t(blockIdx.y + 1) * DIR_CHUNK);
+    for (int64_t base = int64_t(blockIdx.y) * DIR_CHUNK + (threadIdx.x & ~31); base < entries; base += blockDim.x) {
+        const int64_t e = base + lane;
+        const int32_t d = e < entries ? __ldcg(dir + c.dir_off + e) : -1;
+        uint32_t m = __ballot_sync(0xffffffffu, d >= 0);
+        while (m) {
+            const int l = __ffs(m) - 1;
+            m &= m - 1;
+            const int32_t t = __shfl_sync(0xffffffffu, d, l);
+            const int64_t te = base + l;
+            tile_stats(c, dir, T, t, int(te % c.tpr), int(te / c.tpr), st[r]);
+            if (ring && lane == 0) {
+                T.state[t] = 0; T.done[t] = 0;
+                ring[(tail + atomicAdd(returned, 1u)) % cap] = uint32_t(t);
+            }
+        }
+    }
+}
+
+// Reached passable cells (R) of each request (blockIdx.x = request, blockIdx.y = directory chunk), counted (off == nullptr) or listed as quart
+// (x, z) pairs from off[r] on, in no particular order.
+static __global__ void __launch_bounds__(256) k_cells(const FloodCtl *__restrict__ ctl, const int32_t *__restrict__ dir, const Tiles T,
+                                                      unsigned long long *__restrict__ cnt, const unsigned long long *__restrict__ off,
+                                                      int32_t *__restrict__ xz, uint64_t cap) {
     const uint32_t r = blockIdx.x;
     const FloodCtl c = ctl[r];
-    const int64_t words = int64_t(c.tpr) * c.tpr * TILE_WORDS;
-    unsigned long long mine = 0;
-    for (int64_t e = threadIdx.x; e < words; e += blockDim.x) {
-        const int t = int(e / TILE_WORDS), wi = int(e % TILE_WORDS);
-        const int32_t d = dir[c.dir_off + t];
-        if (d < 0) continue;
-        uint32_t bits = pool[size_t(d) * TILE_WORDS + wi] & 0xAAAAAAAAu;     // passable bit of each 2-bit cell
-        if (!off) { mine += __popc(bits); continue; }
-        const int ti = t % c.tpr, tj = t / c.tpr, j = tj * TILE + (wi >> 2), i0 = ti * TILE + (wi & 3) * 16;
-        while (bits) {
-            const int b = __ffs(bits) - 1;
-            bits &= bits - 1;
-            const unsigned long long k = off[r] + atomicAdd(&cnt[r], 1ull);
-            if (k < cap) { xz[2 * k] = c.qx + (i0 + b / 2 - c.half) * c.step; xz[2 * k + 1] = c.qz + (j - c.half) * c.step; }
+    const int lane = threadIdx.x & 31;
+    const int64_t entries = min(int64_t(c.tpr) * c.tpr, int64_t(blockIdx.y + 1) * DIR_CHUNK);
+    for (int64_t base = int64_t(blockIdx.y) * DIR_CHUNK + (threadIdx.x & ~31); base < entries; base += blockDim.x) {
+        const int64_t e = base + lane;
+        const int32_t d = e < entries ? __ldcg(dir + c.dir_off + e) : -1;
+        uint32_t m = __ballot_sync(0xffffffffu, d >= 0);
+        while (m) {
+            const int l = __ffs(m) - 1;
+            m &= m - 1;
+            const int32_t t = __shfl_sync(0xffffffffu, d, l);
+            const int64_t te = base + l;
+            const uint64_t *tb = T.bits + size_t(t) * TILE_U64 + 2 * TILE;
+            uint64_t ra = __ldcg(&tb[lane]), rb = __ldcg(&tb[lane + 32]);
+            const unsigned long long k = __popcll(ra) + __popcll(rb);
+            unsigned long long pre = k;                  // inclusive prefix over the warp
+            #pragma unroll
+            for (int o = 1; o < 32; o <<= 1) { const unsigned long long y = __shfl_up_sync(0xffffffffu, pre, o); if (lane >= o) pre += y; }
+            const unsigned long long total = __shfl_sync(0xffffffffu, pre, 31);
+            if (!total) continue;
+            unsigned long long at = 0;
+            if (lane == 0) at = atomicAdd(&cnt[r], total);
+            at = __shfl_sync(0xffffffffu, at, 0) + pre - k;
+            if (!off) continue;
+            const int i0 = int(te % c.tpr) * TILE, j0 = int(te / c.tpr) * TILE;
+            for (int h = 0; h < 2; h++) {
+                uint64_t bits = h ? rb : ra;
+                const int z = c.qz + (j0 + lane + 32 * h - c.half) * c.step;
+                while (bits) {
+                    const int b = __ffsll(bits) - 1;
+                    bits &= bits - 1;
+                    const unsigned long long o = off[r] + at++;
+                    if (o < cap) { xz[2 * o] = c.qx + (i0 + b - c.half) * c.step; xz[2 * o + 1] = z; }
+                }
+            }
         }
     }
-    if (!off) atomicAdd(&cnt[r], mine);
 }
 
+}  // namespace flood
+}  // namespace dsg
 
+namespace dsg {
+namespace flood {
+// ---------------------------------------------------------------- host side shared by batch and service
+// Tile pool with its round queues (each queue can hold every tile: a tile enters a queue at most once per
+// round, by the directory claim or the connect mark).
+struct TilePool {
+    Tiles T{};
+    uint32_t cap = 0;
+    uint32_t *n_list[2] = {nullptr, nullptr}, *w_list[2] = {nullptr, nullptr};
+    static constexpr size_t kBytesPerTile = TILE_U64 * 8 + 5 * 4 + 4 * 4;
+    void release() {
+        cudaFree(T.bits); cudaFree(T.owner); cudaFree(T.pos); cudaFree(T.state); cudaFree(T.done); cudaFree(T.mark);
+        for (int k = 0; k < 2; k++) { cudaFree(n_list[k]); cudaFree(w_list[k]); n_list[k] = w_list[k] = nullptr; }
+        T = Tiles{}; cap = 0;
+    }
+    void allocate(uint32_t tiles) {
+        release();
+        DSG_CU(cudaMalloc(&T.bits, size_t(tiles) * TILE_U64 * 8));
+        uint32_t **meta[5] = {&T.owner, &T.pos, &T.state, &T.done, &T.mark};
+        for (auto m : meta) DSG_CU(cudaMalloc(m, size_t(tiles) * 4));
+        for (uint32_t *m : {T.state, T.done, T.mark}) DSG_CU(cudaMemset(m, 0, size_t(tiles) * 4));
+        for (int k = 0; k < 2; k++) {
+            DSG_CU(cudaMalloc(&n_list[k], size_t(tiles) * 4));
+            DSG_CU(cudaMalloc(&w_list[k], size_t(tiles) * 4));
+        }
+        cap = tiles;
+    }
+    // state, done and mark of tiles [0, used) back to zero (batch reuse of a bump-allocated pool)
+    void reset(uint32_t used, cudaStream_t st) {
+        used = std::min(used, cap);
+        if (!used) return;
+        for (uint32_t *m : {T.state, T.done, T.mark}) DSG_CU(cudaMemsetAsync(m, 0, size_t(used) * 4, st));
+    }
+};
+// Launch one round: evaluate the tiles claimed last round, then connect.  cnt[0..2] are the rotating
+// claim-queue counters, cnt[3..5] the connect-queue ones.
+inline void launch_round(const TilePool &p, uint32_t round, uint32_t *cnt, uint32_t *active, uint32_t *err, const FloodCtl *ctl,
+                         const SeedNoise *noise, int32_t *dir, FloodStat *st, const TileAlloc &ta, int grid_eval, int grid_conn,
+                         cudaStream_t s) {
+    const Round q{round, p.n_list[round & 1], cnt + round % 3, p.w_list[round & 1], cnt + 3 + round % 3,
+                  p.n_list[(round + 1) & 1], cnt + (round + 1) % 3, p.w_list[(round + 1) & 1], cnt + 3 + (round + 1) % 3,
+                  cnt + (round + 2) % 3, cnt + 3 + (round + 2) % 3, active, err};
+    k_tile_eval<<<grid_eval, EVAL_THREADS, 0, s>>>(ctl, noise, world_dev(), p.T, q);
+    k_tile_connect<<<grid_conn, 256, 0, s>>>(ctl, dir, p.T, ta, st, q);
+}
+inline void round_grids(int &grid_eval, int &grid_conn) {
+    int occ = 0;
+    DSG_CU(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_tile_eval, EVAL_THREADS, 0));
+    grid_eval = std::max(1, occ) * device_info().sms;
+    DSG_CU(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_tile_connect, 256, 0));
+    grid_conn = std::max(1, occ) * device_info().sms;
+}
 }  // namespace flood
 }  // namespace dsg

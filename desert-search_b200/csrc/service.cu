@@ -3,13 +3,12 @@
 //
 // Requests (any seed, start, lattice, window, predicate) are submitted from any host thread and answered
 // with the same DenseArea dense_flood_bridged gives (src/dense_flood.hpp:52-86).  One engine thread keeps
-// every admitted request's BFS in flight together: each BFS level is one launch of the shared level kernel
-// (flood_kernels.cuh) over the cells of all requests, so requests of very different sizes overlap on the
-// device; new requests join at the next level boundary and finished ones leave, releasing their memory.
-// Per-request state lives in HBM: a tile directory carved from an arena, visited tiles (2 bits per cell)
-// taken from a ring of free tiles and zeroed on release, and the request's slot in the level lists.
-// Admission is by memory: a request is admitted when a slot is free, its directory fits the arena and the
-// free tile count stays above a reserve; otherwise it waits in the queue.
+// every admitted request in flight together: each round (flood_kernels.cuh) evaluates and connects the
+// queued tiles of all requests, so requests of very different sizes overlap on the device; new requests
+// join between rounds and finished ones leave, releasing their memory.  Per-request state lives in HBM: a
+// tile directory carved from an arena and tiles taken from a ring of free tiles.  Admission is by memory: a
+// request is admitted when a slot is free, its directory fits the arena and the free tile count stays above
+// a reserve; otherwise it waits in the queue.
 #include "flood_kernels.cuh"
 #include <algorithm>
 #include <condition_variable>
@@ -23,19 +22,6 @@ namespace dsg {
 namespace flood {
 namespace {
 
-// Release the tiles of finished requests: zero them and append them to the free ring.
-__global__ void k_release(const FloodCtl *__restrict__ ctl, const uint32_t *__restrict__ slots, int32_t *__restrict__ dir,
-                          uint32_t *__restrict__ pool, uint32_t *__restrict__ ring, uint32_t cap, uint32_t tail, uint32_t *__restrict__ returned) {
-    const FloodCtl c = ctl[slots[blockIdx.x]];
-    const int64_t entries = int64_t(c.tpr) * c.tpr;
-    for (int64_t e = 0; e < entries; e++) {
-        const int32_t d = dir[c.dir_off + e];
-        if (d < 0) continue;
-        uint32_t *t = pool + size_t(d) * TILE_WORDS;
-        for (int w = threadIdx.x; w < TILE_WORDS; w += blockDim.x) t[w] = 0;
-        if (threadIdx.x == 0) ring[(tail + atomicAdd(returned, 1u)) % cap] = uint32_t(d);
-    }
-}
 __global__ void k_iota(uint32_t *a, uint32_t n) { for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) a[i] = i; }
 
 struct Ticket { dsg_area area{}; int status = 2; };        // 2 = pending
@@ -53,21 +39,20 @@ struct Service {
     struct Slot { bool used = false; uint64_t ticket = 0; int64_t dir_off = 0, dir_len = 0; };
     std::vector<Slot> slots;
     std::vector<std::pair<int64_t, int64_t>> dir_free;       // free arena ranges (offset, length)
-    uint64_t admitted = 0, completed = 0, levels = 0, overflowed = 0;
+    uint64_t admitted = 0, completed = 0, rounds = 0, overflowed = 0;
     // device
     cudaStream_t st = nullptr;
     FloodCtl *d_ctl = nullptr; FloodStat *d_stat = nullptr; SeedNoise *d_noise = nullptr, *d_noise_stage = nullptr;
     uint32_t *d_active = nullptr, *h_active = nullptr;
     int32_t *d_dir = nullptr; int64_t dir_cap = 0;
-    uint32_t *d_pool = nullptr, *d_ring = nullptr; uint32_t pool_cap = 0, head = 0, avail = 0;
-    uint32_t *d_ctr = nullptr, *h_ctr = nullptr;               // [0] taken, [1] returned, [2..4] list counters, [5] error flags
-    uint64_t *d_list[2] = {nullptr, nullptr}; uint32_t list_cap = 0;
-    uint32_t *d_hist = nullptr;
+    TilePool pool;
+    uint32_t *d_ring = nullptr; uint32_t head = 0, avail = 0;
+    uint32_t *d_ctr = nullptr, *h_ctr = nullptr;               // [0] taken, [1] returned, [2..4] claim queues, [5..7] connect queues, [8] error flags
     uint32_t *d_slots = nullptr; uint64_t *d_seeds = nullptr;
-    int grid = 0;
+    int grid_eval = 0, grid_conn = 0;
+    int64_t dir_max = 0;                                       // largest directory of an admitted request
 };
 Service &SV() { static Service s; return s; }
-constexpr uint32_t HIST = 1u << 16;
 
 bool dir_alloc(Service &g, int64_t len, int64_t &off) {
     for (auto it = g.dir_free.begin(); it != g.dir_free.end(); ++it)
@@ -84,10 +69,9 @@ void dir_release(Service &g, int64_t off, int64_t len) {
 
 void engine_loop(Service &g) {
     cudaSetDevice(device_info().device);
-    const uint32_t S = g.cfg.max_requests, K = std::max<uint32_t>(1, g.cfg.levels_per_check);
-    const uint32_t reserve = std::max<uint32_t>(64, g.pool_cap / 64);
-    const WorldDev w = world_dev();
-    uint32_t level = 0;
+    const uint32_t S = g.cfg.max_requests, K = std::max<uint32_t>(1, g.cfg.rounds_per_check);
+    const uint32_t cap = g.pool.cap, reserve = std::max<uint32_t>(64, cap / 64);
+    uint32_t round = 0;                                        // the next round to run
     std::vector<uint32_t> adm_slots; std::vector<uint64_t> adm_seeds;
     for (;;) {
         adm_slots.clear(); adm_seeds.clear();
@@ -116,13 +100,14 @@ void engine_loop(Service &g) {
                 c.dir_off = off;
                 g.slots[si] = {true, g.pending.front().first, off, len};
                 g.pending.pop_front();
+                g.dir_max = std::max(g.dir_max, len);
                 adm_slots.push_back(si); adm_seeds.push_back(q.seed); adm_ctl.push_back(c);
                 inflight++; g.admitted++;
             }
         }
         try {
             cudaStream_t st = g.st;
-            const TileAlloc ta{g.d_ring, g.head, g.avail, g.pool_cap, g.d_ctr + 0, g.d_ctr + 1, (g.head + g.avail) % g.pool_cap};
+            const TileAlloc ta{g.d_ring, g.head, g.avail, cap, g.d_ctr + 0, g.d_ctr + 1, (g.head + g.avail) % cap};
             if (!adm_slots.empty()) {
                 const uint32_t na = uint32_t(adm_slots.size());
                 DSG_CU(cudaMemcpyAsync(g.d_seeds, adm_seeds.data(), na * 8, cudaMemcpyHostToDevice, st));
@@ -133,40 +118,37 @@ void engine_loop(Service &g) {
                     DSG_CU(cudaMemsetAsync(g.d_dir + adm_ctl[k].dir_off, 0xFF, size_t(g.slots[adm_slots[k]].dir_len) * 4, st));
                 }
                 DSG_CU(cudaMemcpyAsync(g.d_slots, adm_slots.data(), na * 4, cudaMemcpyHostToDevice, st));
-                // ctl/slots are host vectors: finish these copies before they go out of scope
-                k_flood_start<<<(na + 127) / 128, 128, 0, st>>>(g.d_ctl, g.d_slots, na, g.d_stat, g.d_dir, g.d_pool, ta, g.d_list[level & 1],
-                                                                g.d_ctr + 2 + (level % 3), g.d_ctr + 5, Stamp{g.d_active, int(level)});
+                k_tile_start<<<(na + 127) / 128, 128, 0, st>>>(g.d_ctl, g.d_slots, na, g.d_stat, g.d_dir, g.pool.T, ta,
+                                                               g.pool.n_list[round & 1], g.d_ctr + 2 + round % 3, round, g.d_active, g.d_ctr + 8);
                 DSG_CU(cudaGetLastError());
+                // ctl/slots are host vectors: finish these copies before they go out of scope
                 DSG_CU(cudaStreamSynchronize(st));
             }
-            for (uint32_t k = 0; k < K; k++, level++) {
-                k_flood_level<<<g.grid, 128, 0, st>>>(g.d_ctl, g.d_stat, g.d_noise, w, g.d_dir, g.d_pool, ta, g.d_list[level & 1],
-                                                      g.d_ctr + 2 + (level % 3), g.d_list[(level + 1) & 1], g.d_ctr + 2 + ((level + 1) % 3),
-                                                      g.d_ctr + 2 + ((level + 2) % 3), g.list_cap, g.d_hist, int(level % HIST), g.d_ctr + 5,
-                                                      Stamp{g.d_active, int(level)});
-            }
+            for (uint32_t k = 0; k < K; k++, round++)
+                launch_round(g.pool, round, g.d_ctr + 2, g.d_active, g.d_ctr + 8, g.d_ctl, g.d_noise, g.d_dir, g.d_stat, ta,
+                             g.grid_eval, g.grid_conn, st);
             DSG_CU(cudaGetLastError());
             DSG_CU(cudaMemcpyAsync(g.h_active, g.d_active, size_t(S) * 4, cudaMemcpyDeviceToHost, st));
-            DSG_CU(cudaMemcpyAsync(g.h_ctr, g.d_ctr, 8 * 4, cudaMemcpyDeviceToHost, st));
+            DSG_CU(cudaMemcpyAsync(g.h_ctr, g.d_ctr, 16 * 4, cudaMemcpyDeviceToHost, st));
             DSG_CU(cudaStreamSynchronize(st));
             const uint32_t taken = std::min(g.h_ctr[0], g.avail);
             uint32_t returned = g.h_ctr[1];
-            g.head = (g.head + taken) % g.pool_cap;
+            g.head = (g.head + taken) % cap;
             g.avail -= taken;
-            // finished requests: no cell queued for the next level
+            // finished requests: nothing queued for the next round
             std::vector<uint32_t> fin;
             {
                 std::lock_guard<std::mutex> l(g.mu);
-                for (uint32_t si = 0; si < S; si++) if (g.slots[si].used && g.h_active[si] != level) fin.push_back(si);
+                for (uint32_t si = 0; si < S; si++) if (g.slots[si].used && g.h_active[si] != round) fin.push_back(si);
             }
             std::vector<FloodStat> fs(fin.size());
             if (!fin.empty()) {
-                for (size_t k = 0; k < fin.size(); k++) DSG_CU(cudaMemcpyAsync(&fs[k], g.d_stat + fin[k], sizeof(FloodStat), cudaMemcpyDeviceToHost, st));
                 DSG_CU(cudaMemcpyAsync(g.d_slots, fin.data(), fin.size() * 4, cudaMemcpyHostToDevice, st));
-                // the returned counter continues from the tiles lost in the directory races of these levels
-                k_release<<<unsigned(fin.size()), 256, 0, st>>>(g.d_ctl, g.d_slots, g.d_dir, g.d_pool, g.d_ring, g.pool_cap,
-                                                                (g.head + g.avail) % g.pool_cap, g.d_ctr + 1);
+                // statistics, then release; the returned counter continues from the tiles lost in directory races
+                k_tile_finish<<<dim3(unsigned(fin.size()), dir_chunks(g.dir_max)), 256, 0, st>>>(g.d_ctl, g.d_slots, g.d_dir, g.pool.T, g.d_stat,
+                                                                                                  g.d_ring, cap, (g.head + g.avail) % cap, g.d_ctr + 1);
                 DSG_CU(cudaGetLastError());
+                for (size_t k = 0; k < fin.size(); k++) DSG_CU(cudaMemcpyAsync(&fs[k], g.d_stat + fin[k], sizeof(FloodStat), cudaMemcpyDeviceToHost, st));
                 DSG_CU(cudaMemcpyAsync(g.h_ctr + 1, g.d_ctr + 1, 4, cudaMemcpyDeviceToHost, st));
                 DSG_CU(cudaStreamSynchronize(st));
                 returned = g.h_ctr[1];
@@ -186,10 +168,9 @@ void engine_loop(Service &g) {
                     s = Service::Slot{};
                     g.completed++;
                 }
-                g.levels = level;
+                g.rounds = round;
             }
             if (!fin.empty()) g.cv_done.notify_all();
-            if (g.h_ctr[5] & 2) throw std::runtime_error("flood service: level list capacity exceeded");
         } catch (...) {
             std::lock_guard<std::mutex> l(g.mu);
             for (auto &s : g.slots) if (s.used) { g.results[s.ticket].status = DSG_E_CUDA; s = Service::Slot{}; }
@@ -217,7 +198,7 @@ extern "C" int dsg_service_open(const dsg_service_cfg *cfg_in) {
         dsg_service_cfg c = cfg_in ? *cfg_in : dsg_service_cfg{0, 0, 0};
         if (!c.budget_bytes) c.budget_bytes = uint64_t(8) << 30;
         if (!c.max_requests) c.max_requests = 4096;
-        if (!c.levels_per_check) c.levels_per_check = 4;
+        if (!c.rounds_per_check) c.rounds_per_check = 4;
         DSG_ARG(c.max_requests <= (1u << 20), "dsg_service_open: max_requests too large");
         g.cfg = c;
         const uint32_t S = c.max_requests;
@@ -233,27 +214,22 @@ extern "C" int dsg_service_open(const dsg_service_cfg *cfg_in) {
         DSG_CU(cudaMallocHost(&g.h_active, size_t(S) * 4));
         DSG_CU(cudaMalloc(&g.d_slots, size_t(S) * 4));
         DSG_CU(cudaMalloc(&g.d_seeds, size_t(S) * 8));
-        // budget: a quarter for tile directories, the rest for visited tiles and their free ring
+        // budget: a quarter for tile directories, the rest for tiles, their queues and their free ring
         g.dir_cap = int64_t(c.budget_bytes / 4 / 4);
         DSG_CU(cudaMalloc(&g.d_dir, size_t(g.dir_cap) * 4));
         g.dir_free = {{0, g.dir_cap}};
-        g.pool_cap = uint32_t(std::min<uint64_t>((c.budget_bytes - c.budget_bytes / 4) / (TILE_WORDS * 4 + 4), 0x7fffffffu));
-        DSG_CU(cudaMalloc(&g.d_pool, size_t(g.pool_cap) * TILE_WORDS * 4));
-        DSG_CU(cudaMemset(g.d_pool, 0, size_t(g.pool_cap) * TILE_WORDS * 4));
-        DSG_CU(cudaMalloc(&g.d_ring, size_t(g.pool_cap) * 4));
-        k_iota<<<1024, 256>>>(g.d_ring, g.pool_cap);
+        g.dir_max = 0;
+        const uint32_t tiles = uint32_t(std::min<uint64_t>((c.budget_bytes - c.budget_bytes / 4) / (TilePool::kBytesPerTile + 4), 0x7fffffffu));
+        g.pool.allocate(tiles);
+        DSG_CU(cudaMalloc(&g.d_ring, size_t(tiles) * 4));
+        k_iota<<<1024, 256>>>(g.d_ring, tiles);
         DSG_CU(cudaGetLastError());
-        g.head = 0; g.avail = g.pool_cap;
-        g.list_cap = 1u << 25;
-        for (auto &p : g.d_list) DSG_CU(cudaMalloc(&p, size_t(g.list_cap) * 8));
-        DSG_CU(cudaMalloc(&g.d_ctr, 8 * 4));
-        DSG_CU(cudaMemset(g.d_ctr, 0, 8 * 4));
-        DSG_CU(cudaMallocHost(&g.h_ctr, 8 * 4));
-        DSG_CU(cudaMalloc(&g.d_hist, size_t(HIST) * 4));
+        g.head = 0; g.avail = tiles;
+        DSG_CU(cudaMalloc(&g.d_ctr, 16 * 4));
+        DSG_CU(cudaMemset(g.d_ctr, 0, 16 * 4));
+        DSG_CU(cudaMallocHost(&g.h_ctr, 16 * 4));
         DSG_CU(cudaDeviceSynchronize());
-        int occ = 0;
-        DSG_CU(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_flood_level, 128, 0));
-        g.grid = std::max(1, occ) * device_info().sms;
+        round_grids(g.grid_eval, g.grid_conn);
         g.slots.assign(S, Service::Slot{});
         g.stop = false; g.open = true;
         g.engine = std::thread(engine_loop, std::ref(g));
@@ -317,7 +293,7 @@ extern "C" int dsg_service_stats(uint64_t stats[6]) {
         std::lock_guard<std::mutex> l(g.mu);
         uint64_t inflight = 0;
         for (auto &s : g.slots) inflight += s.used;
-        const uint64_t v[6] = {g.admitted, g.completed, inflight, uint64_t(g.pending.size()), g.levels, g.overflowed};
+        const uint64_t v[6] = {g.admitted, g.completed, inflight, uint64_t(g.pending.size()), g.rounds, g.overflowed};
         std::copy(v, v + 6, stats);
         return DSG_OK;
     });
@@ -336,8 +312,9 @@ extern "C" int dsg_service_close(void) {
         std::lock_guard<std::mutex> l(g.mu);
         cudaStreamSynchronize(g.st);
         cudaFree(g.d_ctl); cudaFree(g.d_stat); cudaFree(g.d_noise); cudaFree(g.d_noise_stage); cudaFree(g.d_active); cudaFreeHost(g.h_active);
-        cudaFree(g.d_slots); cudaFree(g.d_seeds); cudaFree(g.d_dir); cudaFree(g.d_pool); cudaFree(g.d_ring); cudaFree(g.d_ctr);
-        cudaFreeHost(g.h_ctr); cudaFree(g.d_hist); cudaFree(g.d_list[0]); cudaFree(g.d_list[1]);
+        cudaFree(g.d_slots); cudaFree(g.d_seeds); cudaFree(g.d_dir); cudaFree(g.d_ring); cudaFree(g.d_ctr);
+        cudaFreeHost(g.h_ctr);
+        g.pool.release();
         cudaStreamDestroy(g.st);
         g.results.clear(); g.pending.clear(); g.slots.clear(); g.dir_free.clear();
         g.open = false; g.stop = false;

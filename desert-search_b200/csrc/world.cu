@@ -91,6 +91,52 @@ void build_grid(const Blob &b, WorldDev &w, std::vector<int16_t> &cells) {
     }
     for (int16_t &c : cells) if (c == UNSET) c = -1;
 }
+// Pruning blocks for classify_warp.  Walks the tree in the reference's depth-first order (children of a node
+// at `node + stride` steps, standalone.hpp:182-196) and checks what the warp search relies on: leaves appear
+// in increasing node order, every box below the root contains its children's boxes, and every leaf lies
+// below depth 3.  The root's box is a placeholder and is never tested by the search.
+void build_blocks(const Blob &b, std::vector<uint64_t> &leaf, std::vector<uint64_t> &blk, std::vector<uint32_t> &rng) {
+    const int n = int(b.tree.size());
+    auto is_leaf = [&](int k) { return (b.tree[k] >> 56) == 255; };
+    auto inside = [&](int child, int parent) {
+        for (int i = 0; i < 6; i++) {
+            const int kc = int((b.tree[child] >> (8 * i)) & 255), kp = int((b.tree[parent] >> (8 * i)) & 255);
+            if (b.param[2 * kc] < b.param[2 * kp] || b.param[2 * kc + 1] > b.param[2 * kp + 1]) return false;
+        }
+        return true;
+    };
+    struct Fr { int node, level, depth; };
+    std::vector<Fr> stk{{0, 0, 0}};
+    int last_leaf = -1;
+    // iterative pre-order walk; children pushed in reverse so they pop in order
+    while (!stk.empty()) {
+        const Fr f = stk.back(); stk.pop_back();
+        if (f.depth == 3) {                        // leaves of this block follow contiguously in pre-order
+            blk.push_back(b.tree[f.node]);
+            rng.push_back(uint32_t(leaf.size()));
+        }
+        if (is_leaf(f.node)) {
+            if (f.depth <= 3) throw std::runtime_error("biome tree: leaf above depth 4");
+            if (f.node <= last_leaf) throw std::runtime_error("biome tree: leaves out of node order");
+            last_leaf = f.node;
+            leaf.push_back(b.tree[f.node]);
+            continue;
+        }
+        int stride = 0, lv = f.level;
+        do { stride = b.strides[lv & 7]; lv++; } while (f.node + stride >= n && lv < 8);
+        std::vector<Fr> kids;
+        for (int i = 0, c = int(b.tree[f.node] >> 48); i < 6 && c < n; i++, c += stride) {
+            if (f.node != 0 && !inside(c, f.node)) throw std::runtime_error("biome tree: child box outside its parent");
+            kids.push_back({c, lv, f.depth + 1});
+        }
+        for (auto it = kids.rbegin(); it != kids.rend(); ++it) stk.push_back(*it);
+    }
+    for (size_t k = 0; k < rng.size(); k++) {
+        const uint32_t lo = rng[k], hi = k + 1 < rng.size() ? rng[k + 1] : uint32_t(leaf.size());
+        rng[k] = lo | (hi << 16);
+    }
+    if (blk.size() > size_t(32 * kBlkPerLane) || leaf.size() > 0xffff) throw std::runtime_error("biome tree: too many blocks or leaves");
+}
 template <class T> const T *upload(const std::vector<T> &v) {
     T *d = nullptr;
     DSG_CU(cudaMalloc(&d, v.size() * sizeof(T)));
@@ -110,7 +156,13 @@ void world_upload(int) {
     build_grid(b, w, cells);
     if (b.strides.size() > 8 || b.prob.size() != 1600) throw std::runtime_error("worldgen blob: bad sizes");
     for (size_t i = 0; i < b.strides.size(); i++) w.strides[i] = b.strides[i];
-    w.ntree = int(b.tree.size()); w.nspl = int(b.spl.size());
+    w.ntree = int(b.tree.size()); w.nspl = int(b.spl.size()); w.nparam = int(b.param.size() / 2);
+    std::vector<uint64_t> leaf, blk;
+    std::vector<uint32_t> rng;
+    build_blocks(b, leaf, blk, rng);
+    if (b.param.size() > 2 * 256) throw std::runtime_error("worldgen blob: too many parameter intervals");
+    w.nleaf = int(leaf.size()); w.nblk = int(blk.size());
+    w.leaf = upload(leaf); w.blk = upload(blk); w.blk_rng = upload(rng);
     w.cells = upload(cells); w.tree = upload(b.tree); w.param = upload(b.param); w.spl = upload(b.spl); w.prob = upload(b.prob);
     g_world = w;
     g_prob = b.prob;

@@ -189,14 +189,14 @@ DSG_PENDING = 2
 
 
 class ServiceCfg(C.Structure):
-    _fields_ = [("budget_bytes", C.c_uint64), ("max_requests", C.c_uint32), ("levels_per_check", C.c_uint32)]
+    _fields_ = [("budget_bytes", C.c_uint64), ("max_requests", C.c_uint32), ("rounds_per_check", C.c_uint32)]
 
 
 class Service:
     """The continuously batched flood service (dsg_service_*)."""
 
-    def __init__(self, budget_bytes=8 << 30, max_requests=4096, levels_per_check=4):
-        cfg = ServiceCfg(budget_bytes, max_requests, levels_per_check)
+    def __init__(self, budget_bytes=8 << 30, max_requests=4096, rounds_per_check=4):
+        cfg = ServiceCfg(budget_bytes, max_requests, rounds_per_check)
         _ck(lib.dsg_service_open(C.byref(cfg)), "dsg_service_open")
 
     def submit(self, req):

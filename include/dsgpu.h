@@ -156,7 +156,7 @@ int dsg_query_batch(const uint64_t *seeds, uint32_t nseeds, const uint32_t *psee
 /* Flood a batch of requests concurrently (any mix of seeds, steps, windows, predicates).  Results are
  * identical to dense_flood_bridged (src/dense_flood.hpp:52-86) run per request.  Replaces the CPU floods
  * of dsearch_desert.cpp:337,352,387,512,521 and tools/dflood.cpp:20.  DSG_OVERFLOW: device memory for the
- * visited tiles ran out; rerun the batch in smaller pieces. */
+ * tiles ran out; rerun the batch in smaller pieces. */
 int dsg_flood_batch(const dsg_flood_req *reqs, uint32_t n, dsg_area *out);
 /* As dsg_flood_batch, and also list each request's passable cells (quart coordinates x, z), the cells the
  * reference leaves in state 2 or 3 (dense_flood.hpp:76; the hot-zone bookkeeping of dsearch_desert.cpp:340-363
@@ -165,13 +165,13 @@ int dsg_flood_batch_cells(const dsg_flood_req *reqs, uint32_t n, dsg_area *out, 
 /* ---------------------------------------------------------------- flood service (continuous batching) */
 /* Replaces the fleet's per-CANDIDATE MC-Measure run (deploy/gpipe.sh:7-10) and per-request dflood runs: any
  * number of host threads submit flood requests; one engine keeps all admitted requests' floods in flight
- * together (each BFS level is one launch over every request's cells), admits new requests at level
- * boundaries while slots, directory arena and visited-tile memory allow, and retires finished ones.
+ * together (each round evaluates and connects the queued 64x64-cell tiles of every request), admits new
+ * requests between rounds while slots, directory arena and tile memory allow, and retires finished ones.
  * Results equal dsg_flood's. */
 typedef struct dsg_service_cfg {
-    uint64_t budget_bytes;      /* device memory for tile directories and visited tiles (0 = 8 GiB) */
+    uint64_t budget_bytes;      /* device memory for tile directories and tiles (0 = 8 GiB) */
     uint32_t max_requests;      /* requests in flight at once (0 = 4096) */
-    uint32_t levels_per_check;  /* BFS levels launched between host checks (0 = 4) */
+    uint32_t rounds_per_check;  /* tile rounds launched between host checks (0 = 4) */
 } dsg_service_cfg;
 int dsg_service_open(const dsg_service_cfg *cfg);
 int dsg_service_submit(const dsg_flood_req *req, uint64_t *ticket);
@@ -179,7 +179,7 @@ int dsg_service_submit(const dsg_flood_req *req, uint64_t *ticket);
 int dsg_service_poll(uint64_t ticket, dsg_area *out);
 /* Blocking form of poll; timeout_ms < 0 waits forever, else DSG_E_TIMEOUT. */
 int dsg_service_wait(uint64_t ticket, dsg_area *out, int timeout_ms);
-/* {admitted, completed, in flight, queued, BFS levels run, overflowed}. */
+/* {admitted, completed, in flight, queued, tile rounds run, overflowed}. */
 int dsg_service_stats(uint64_t stats[6]);
 int dsg_service_close(void);
 

@@ -81,6 +81,25 @@ int orc_noise(uint64_t seed, int ch, const double *xyz, int n, double *out) {
     for (int i = 0; i < n; i++) out[i] = S.nz[ch].sample(xyz[3 * i], xyz[3 * i + 1], xyz[3 * i + 2]);
     return 0;
 }
+// Nearest-leaf node index two ways: the reference's pruned depth-first search (tree_nearest), and the
+// lexicographic minimum of (box distance, node index) over all leaves, the form the device's warp search
+// computes.  Test infrastructure: the two agree when every box below the root contains its children's.
+int orc_leaf_two_ways(const int64_t *q, int n, int32_t *dfs_leaf, int32_t *argmin_leaf) {
+    const World &W = world();
+    for (int i = 0; i < n; i++) {
+        uint64_t d = std::numeric_limits<uint64_t>::max();
+        dfs_leaf[i] = tree_nearest(0, 0, q + 6 * i, 0, d);
+        uint64_t bd = std::numeric_limits<uint64_t>::max();
+        int32_t bi = -1;
+        for (int k = 0; k < int(W.tree.size()); k++) {
+            if ((W.tree[k] >> 56) != 255) continue;
+            const uint64_t x = box_dist(k, q + 6 * i);
+            if (x < bd) { bd = x; bi = k; }
+        }
+        argmin_leaf[i] = bi;
+    }
+    return 0;
+}
 // pred: 0 bridged desert state, 1 unbridged desert (exact depth), 2 hot (T >= 0.55), 3 proxy prob (x1000)
 int orc_points(uint64_t seed, int pred, const int32_t *xz, int n, int32_t *out, int threads) {
     const Seed S(seed);

@@ -39,7 +39,7 @@ def ptr(a, t):
 
 def _bind(lib, prefix):
     fns = {}
-    for name in ["phase", "noise", "points", "climate", "biome", "flood", "tabins", "tables", "tmap", "blur_taps"]:
+    for name in ["phase", "noise", "points", "climate", "biome", "leaf_two_ways", "flood", "tabins", "tables", "tmap", "blur_taps"]:
         f = getattr(lib, f"{prefix}_{name}", None)
         if f is not None:
             fns[name] = f
@@ -87,6 +87,12 @@ class CpuPath:
         t = np.empty(len(q), dtype=np.int32); g = np.empty(len(q), dtype=np.int32)
         self.f["biome"](ptr(q, i64p), C.c_int(len(q)), ptr(t, i32p), ptr(g, i32p))
         return t, g
+
+    def leaf_two_ways(self, q):
+        q = np.ascontiguousarray(q, dtype=np.int64).reshape(-1, 6)
+        a = np.empty(len(q), dtype=np.int32); b = np.empty(len(q), dtype=np.int32)
+        self.f["leaf_two_ways"](ptr(q, i64p), C.c_int(len(q)), ptr(a, i32p), ptr(b, i32p))
+        return a, b
 
     def flood(self, seed, qx, qz, step, half, conn8=False, pred=0, pcut=0.35):
         a = Area()

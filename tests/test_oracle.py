@@ -53,6 +53,29 @@ def test_biome_grid_and_tree_agree_with_reference(ref_cpu):
     assert np.array_equal(g1[known], t1[known]), "grid lookup must agree with the tree wherever it decides"
 
 
+def test_tree_search_equals_leaf_argmin():
+    """The device classifies by the (box distance, leaf index) minimum over all leaves; that equals the
+    reference's pruned depth-first search because boxes below the root nest.  Checked on the reference
+    fixture's climate points, on fresh climate points of several seeds, and on points pushed onto box
+    boundaries (where ties and prunes are decided)."""
+    d = np.load(os.path.join(G, "ref_points.npz"))
+    qs = [np.concatenate([d[f"q{n}"] for n in range(4)])]
+    rng = np.random.default_rng(11)
+    o = libs.orc()
+    for seed in rng.integers(0, 2**63, 6, dtype=np.uint64):
+        xz = rng.integers(-2_000_000, 2_000_001, (1500, 2)).astype(np.int32)
+        qs.append(o.climate(int(seed), xz))
+    q = np.concatenate(qs)
+    edge = q.copy()
+    cuts = np.unique(np.concatenate([d[f"q{n}"] for n in range(4)]).ravel())
+    pick = rng.integers(0, 6, len(edge))
+    edge[np.arange(len(edge)), pick] = rng.choice(np.array([-10000, -4500, -1500, -1050, -450, 0, 300, 500, 501, 550, 2000, 3000, 5500, 10000]), len(edge))
+    q = np.concatenate([q, edge])
+    assert len(cuts) > 0 and len(q) > 15000
+    dfs, arg = o.leaf_two_ways(q)
+    assert np.array_equal(dfs, arg), f"{np.sum(dfs != arg)} of {len(q)} points differ"
+
+
 def test_floods_match_reference_fixture():
     o = libs.orc()
     for f in json.load(open(os.path.join(G, "ref_floods.json"))):

@@ -25,7 +25,7 @@ def test_service_results_equal_batch_alone_and_mixed(dsg):
     finds = json.load(open(os.path.join(G, "finds.json")))
     big = [dsg.flood_req(f["seed"], f["x"] >> 2, f["z"] >> 2, 1, 20000) for f in finds[:3]]
     big_want = [(f["cells"],) for f in finds[:3]]
-    svc = dsg.Service(budget_bytes=4 << 30, max_requests=256, levels_per_check=4)
+    svc = dsg.Service(budget_bytes=4 << 30, max_requests=256, rounds_per_check=4)
     try:
         # alone: one request at a time
         for q, w in zip(reqs[:6], want[:6]):
@@ -57,7 +57,7 @@ def test_service_results_equal_batch_alone_and_mixed(dsg):
 
 def test_service_reopen_and_poll(dsg):
     reqs, want = fixture_reqs(dsg)
-    svc = dsg.Service(budget_bytes=1 << 30, max_requests=8, levels_per_check=2)
+    svc = dsg.Service(budget_bytes=1 << 30, max_requests=8, rounds_per_check=2)
     try:
         ts = [svc.submit(q) for q in reqs]          # more requests than slots: the rest queue
         got = {}
