@@ -128,11 +128,14 @@ def bench_floods(dsgpu, n_small=4096, rate=500.0, n_service=1500, n_seq=120, bat
     t0 = time.perf_counter()
     areas = dsgpu.flood_batch(reqs)
     t_batch = time.perf_counter() - t0
+    work = dsgpu.flood_last_stats()
     sampled = sum(a[1] for a in areas)
     cells = np.array([a[0] for a in areas], dtype=np.float64)
     batch = {"floods": len(reqs), "small": len(small), "large": len(large), "seconds": t_batch, "floods_per_s": len(reqs) / t_batch,
              "cells_per_s": float(cells.sum()) / t_batch, "evaluations_per_s": sampled / t_batch,
-             "area_blocks2_min_median_max": [float(cells.min() * 16), float(np.median(cells) * 16), float(cells.max() * 16)]}
+             "area_blocks2_min_median_max": [float(cells.min() * 16), float(np.median(cells) * 16), float(cells.max() * 16)],
+             "rounds": work["rounds"], "tiles": work["tiles"], "cells_evaluated_per_s": work["tiles"] * 4096 / t_batch,
+             "speculation_overhead": work["tiles"] * 4096 / max(1, work["touched"])}
     if batch_only:
         return {"batch": batch}
     # service: 90% small, 10% large, Poisson arrivals at `rate`

@@ -18,13 +18,14 @@ struct Engine {
     bool ready = false;
     cudaStream_t st = nullptr;
     TilePool pool;
-    uint32_t *d_cnt = nullptr, *h_cnt = nullptr;   // [0..2] claim-queue counters, [3..5] connect-queue, [6] taken, [7] error flags
+    uint32_t *d_cnt = nullptr, *h_cnt = nullptr;   // [0..8] round counters (launch_round), [9] taken, [10] error flags
     int32_t *d_dir = nullptr; size_t dir_cap = 0;
     FloodCtl *d_ctl = nullptr; uint32_t ctl_cap = 0;
     FloodStat *d_stat = nullptr; uint32_t stat_cap = 0;
     SeedNoise *d_noise = nullptr; uint32_t noise_cap = 0;
     uint64_t *d_seeds = nullptr; uint32_t seeds_cap = 0;
     int grid_eval = 0, grid_conn = 0;
+    uint64_t last[3] = {0, 0, 0};                  // rounds, tiles evaluated, cells touched of the last batch
 };
 Engine &E() { static Engine e; return e; }
 
@@ -35,8 +36,8 @@ void setup_locked(Engine &g) {
     DSG_CU(cudaDeviceGetStreamPriorityRange(&lo, &hi));
     DSG_CU(cudaStreamCreateWithPriority(&g.st, cudaStreamNonBlocking, hi));
     round_grids(g.grid_eval, g.grid_conn);
-    DSG_CU(cudaMalloc(&g.d_cnt, 8 * 4));
-    DSG_CU(cudaMallocHost(&g.h_cnt, 8 * 4));
+    DSG_CU(cudaMalloc(&g.d_cnt, 16 * 4));
+    DSG_CU(cudaMallocHost(&g.h_cnt, 16 * 4));
     g.ready = true;
 }
 template <class T> void grow(T *&p, uint32_t &cap, size_t need) {
@@ -91,22 +92,22 @@ int run_batch(const dsg_flood_req *reqs, uint32_t n, dsg_area *out, size_t pool_
     seed_noise_build(g.d_seeds, uint32_t(seeds.size()), g.d_noise, st);
     DSG_CU(cudaMemcpyAsync(g.d_ctl, ctl.data(), size_t(n) * sizeof(FloodCtl), cudaMemcpyHostToDevice, st));
     DSG_CU(cudaMemsetAsync(g.d_dir, 0xFF, dir_total * 4, st));
-    DSG_CU(cudaMemsetAsync(g.d_cnt, 0, 8 * 4, st));
-    const TileAlloc ta{nullptr, 0, g.pool.cap, g.pool.cap, g.d_cnt + 6, nullptr, 0};
+    DSG_CU(cudaMemsetAsync(g.d_cnt, 0, 16 * 4, st));
+    const TileAlloc ta{nullptr, 0, g.pool.cap, g.pool.cap, g.d_cnt + 9, nullptr, 0};
     k_tile_start<<<(n + 127) / 128, 128, 0, st>>>(g.d_ctl, nullptr, n, g.d_stat, g.d_dir, g.pool.T, ta, g.pool.n_list[0], g.d_cnt + 0,
-                                                  0, nullptr, g.d_cnt + 7);
+                                                  0, nullptr, g.d_cnt + 10);
     DSG_CU(cudaGetLastError());
     const int K = 4;                                   // rounds enqueued between completion checks
     uint32_t round = 0;
     for (;;) {
         for (int k = 0; k < K; k++, round++)
-            launch_round(g.pool, round, g.d_cnt, nullptr, g.d_cnt + 7, g.d_ctl, g.d_noise, g.d_dir, g.d_stat, ta, g.grid_eval, g.grid_conn, st);
+            launch_round(g.pool, round, g.d_cnt, nullptr, g.d_cnt + 10, g.d_ctl, g.d_noise, g.d_dir, g.d_stat, ta, g.grid_eval, g.grid_conn, st);
         DSG_CU(cudaGetLastError());
-        DSG_CU(cudaMemcpyAsync(g.h_cnt, g.d_cnt, 8 * 4, cudaMemcpyDeviceToHost, st));
+        DSG_CU(cudaMemcpyAsync(g.h_cnt, g.d_cnt, 16 * 4, cudaMemcpyDeviceToHost, st));
         DSG_CU(cudaStreamSynchronize(st));
         if (g.h_cnt[round % 3] == 0 && g.h_cnt[3 + round % 3] == 0) break;
     }
-    const uint32_t taken = g.h_cnt[6], flags = g.h_cnt[7];
+    const uint32_t taken = g.h_cnt[9], flags = g.h_cnt[10];
     k_tile_finish<<<scan_grid, 256, 0, st>>>(g.d_ctl, nullptr, g.d_dir, g.pool.T, g.d_stat, nullptr, 0, 0, nullptr);
     DSG_CU(cudaGetLastError());
     std::vector<FloodStat> hs(n);
@@ -140,6 +141,8 @@ int run_batch(const dsg_flood_req *reqs, uint32_t n, dsg_area *out, size_t pool_
         fin();
     }
     g.pool.reset(taken, st);                             // the next batch allocates from tile 0 again
+    g.last[0] = round; g.last[1] = std::min(taken, g.pool.cap); g.last[2] = 0;
+    for (uint32_t r = 0; r < n; r++) g.last[2] += hs[r].sampled;
     for (uint32_t r = 0; r < n; r++) {
         const FloodStat &s = hs[r];
         out[r].cells = s.cells; out[r].sampled = s.sampled;
@@ -167,6 +170,16 @@ extern "C" int dsg_flood_batch(const dsg_flood_req *reqs, uint32_t n, dsg_area *
     });
 }
 extern "C" int dsg_flood(const dsg_flood_req *req, dsg_area *out) { return dsg_flood_batch(req, 1, out); }
+
+extern "C" int dsg_flood_last_stats(uint64_t stats[3]) {
+    return dsg::guarded([&] {
+        DSG_ARG(stats, "dsg_flood_last_stats: null pointer");
+        dsg::flood::Engine &g = dsg::flood::E();
+        std::lock_guard<std::mutex> l(g.mu);
+        std::copy(g.last, g.last + 3, stats);
+        return DSG_OK;
+    });
+}
 
 extern "C" int dsg_flood_batch_cells(const dsg_flood_req *reqs, uint32_t n, dsg_area *out, uint64_t *off, int32_t *xz, uint64_t cap) {
     return dsg::guarded([&] {

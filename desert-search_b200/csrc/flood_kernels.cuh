@@ -8,8 +8,7 @@
 // finds R by bit-parallel fills:
 //  * a tile is claimed (directory atomicCAS) when R reaches its edge; claimed tiles are evaluated in the next
 //    round by k_tile_eval, every cell at once (16 blocks of 256 cells per tile), into bit rows P (passable)
-//    and D (desert, counted); the rare cells the surface grid cannot decide are finished in the same block
-//    by warp-cooperative tree searches;
+//    and D (desert, counted);
 //  * k_tile_connect grows R inside each queued tile to its fixed point (row fills, column fills across the
 //    warp, the diagonal step for 8-connectivity), seeded from the R edges of the neighbouring tiles; when R
 //    changes on an edge it queues the neighbour, or claims it if it does not exist yet.  R only grows, so the
@@ -55,14 +54,16 @@ struct Round {
     uint32_t *w_list; uint32_t *w_cnt;
     uint32_t *n_next; uint32_t *n_next_cnt;
     uint32_t *w_next; uint32_t *w_next_cnt;
-    uint32_t *zero_a, *zero_b;         // counters of the round after next, cleared by connect
+    uint32_t *work;                    // items of this round's evaluation handed out so far
+    uint32_t *zero_a, *zero_b, *zero_c; // counters of the round after next, cleared by connect
     uint32_t *active;                  // per request: the last round it has queued work for (service)
     uint32_t *err;                     // bit 0: tile pool exhausted
 };
 
-// Predicate value, or -1 when a desert point needs the tree search (finished by classify_deferred_warp).
-__device__ __forceinline__ int eval_pred(const FloodCtl &c, const SeedNoise &S, const WorldDev &w, int x, int z, Deferred &fb) {
-    if (c.pred == DSG_PRED_DESERT) return desert_state_grid(S, w, x, z, fb);
+// Predicate value of request c at quart (x, z): 2 counted, 1 crossed (bridged river), 0 boundary; -1 with `p`
+// filled when a desert point needs desert_state_finish.
+__device__ __forceinline__ int eval_pred(const FloodCtl &c, const SeedNoise &S, const WorldDev &w, int x, int z, PendingState &p) {
+    if (c.pred == DSG_PRED_DESERT) return desert_state_begin(S, w, x, z, p);
     if (c.pred == DSG_PRED_HOT) return hot_state(S, x, z);
     return proxy_prob(S, w, x, z) >= c.pcut ? 2 : 0;
 }
@@ -103,57 +104,74 @@ static __global__ void k_tile_start(const FloodCtl *__restrict__ ctl, const uint
     claim_tile(c, r, c.half >> 6, c.half >> 6, dir, T, ta, n_list, n_cnt, round, active, st, err);
 }
 
-// Evaluate claimed tiles: block item = (tile, 4 rows); warp = half a row.  Deferred desert cells are listed
-// in shared memory and finished by the block's warps, one cooperative tree search per cell.  The last row
-// block of a tile to finish marks it evaluated and queues it for this round's connect.
+// Evaluate claimed tiles: block item = (tile, 4 rows); warp = half a row, written as 32-bit halves of the P
+// and D rows (R cleared).  Blocks take runs of consecutive items from a round counter (up to a whole tile
+// at a time when the round is large), which balances tiles of very different cost and keeps a block on one
+// request for many items; the request's noise tables stay in shared memory while it does, so every Perlin
+// lookup is a shared-memory access.  Points the surface grid cannot decide (about one in eight near desert
+// edges) are gathered in shared memory and finished by the first threads of the block, so the exact
+// searches run in full warps instead of as one diverged lane per warp.  The last row block of a tile to
+// finish marks it evaluated and queues it for this round's connect.
 static __global__ void __launch_bounds__(EVAL_THREADS) k_tile_eval(const FloodCtl *__restrict__ ctl, const SeedNoise *__restrict__ noise,
                                                                    WorldDev w, Tiles T, Round q) {
-    __shared__ int32_t s_param[512];
-    __shared__ Deferred s_def[EVAL_THREADS];
-    __shared__ int32_t s_res[EVAL_THREADS];
-    __shared__ int s_n;
+    __shared__ SeedNoise s_noise;
+    __shared__ PendingState s_pend[EVAL_THREADS];
+    __shared__ int8_t s_res[EVAL_THREADS];
+    __shared__ int s_n, s_seed;
+    __shared__ uint32_t s_run;
     const uint32_t items = *q.n_cnt * EVAL_ITEMS;
-    if (blockIdx.x >= items) return;
-    for (int k = threadIdx.x; k < 2 * w.nparam; k += blockDim.x) s_param[k] = w.param[k];
+    const uint32_t run = max(1u, min(uint32_t(EVAL_ITEMS), items / (4 * gridDim.x)));
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    for (uint32_t item = blockIdx.x; item < items; item += gridDim.x) {
-        const uint32_t t = q.n_list[item / EVAL_ITEMS];
-        const int row = int(item % EVAL_ITEMS) * 4 + (warp >> 1), col = ((warp & 1) << 5) | lane;
-        const uint32_t r = T.owner[t], pos = T.pos[t];
-        const FloodCtl c = ctl[r];
-        const int i = int(pos & 0xffff) * TILE + col, j = int(pos >> 16) * TILE + row;
-        __syncthreads();                                  // previous item's list consumed; parameters staged
-        if (threadIdx.x == 0) s_n = 0;
+    if (threadIdx.x == 0) s_seed = -1;
+    for (;;) {
+        __syncthreads();                                      // s_run of the previous run has been read
+        if (threadIdx.x == 0) s_run = atomicAdd(q.work, run);
         __syncthreads();
-        int v = 0, slot = -1;
-        if (i < c.n && j < c.n) {
-            const int x = c.qx + (i - c.half) * c.step, z = c.qz + (j - c.half) * c.step;
-            if (x >= -kWorld && x <= kWorld && z >= -kWorld && z <= kWorld) {
-                Deferred fb;
-                v = eval_pred(c, noise[c.noise], w, x, z, fb);
-                if (v < 0) { slot = atomicAdd(&s_n, 1); s_def[slot] = fb; }
+        const uint32_t begin = s_run;
+        if (begin >= items) break;
+        for (uint32_t item = begin; item < min(items, begin + run); item++) {
+            const uint32_t t = q.n_list[item / EVAL_ITEMS];
+            const int row = int(item % EVAL_ITEMS) * 4 + (warp >> 1), col = ((warp & 1) << 5) | lane;
+            const uint32_t r = T.owner[t], pos = T.pos[t];
+            const FloodCtl c = ctl[r];
+            const int i = int(pos & 0xffff) * TILE + col, j = int(pos >> 16) * TILE + row;
+            __syncthreads();                                  // the previous item is done with shared memory
+            const bool restage = s_seed != c.noise;
+            __syncthreads();
+            if (restage) {
+                const uint4 *src = reinterpret_cast<const uint4 *>(noise + c.noise);
+                uint4 *dst = reinterpret_cast<uint4 *>(&s_noise);
+                for (int k = threadIdx.x; k < int(sizeof(SeedNoise) / 16); k += blockDim.x) dst[k] = __ldg(src + k);
+                if (threadIdx.x == 0) s_seed = c.noise;
             }
-        }
-        __syncthreads();
-        const int nd = s_n;
-        for (int e = warp; e < nd; e += EVAL_THREADS / 32) {
-            const int res = classify_deferred_warp(w, s_param, s_def[e]);
-            if (lane == 0) s_res[e] = res;
-        }
-        __syncthreads();
-        if (slot >= 0) v = s_res[slot];
-        const uint32_t pm = __ballot_sync(0xffffffffu, v > 0), dm = __ballot_sync(0xffffffffu, v == 2);
-        if (lane == 0) {
-            uint32_t *b = reinterpret_cast<uint32_t *>(T.bits + size_t(t) * TILE_U64);
-            const int h = 2 * row + (warp & 1);
-            b[h] = pm; b[2 * TILE + h] = dm; b[4 * TILE + h] = 0;
-        }
-        __syncthreads();
-        if (threadIdx.x == 0) {
-            __threadfence();
-            if (atomicAdd(&T.done[t], 1u) == EVAL_ITEMS - 1) {
-                T.state[t] = 1;
-                if (atomicExch(&T.mark[t], q.round + 1) != q.round + 1) q.w_list[atomicAdd(q.w_cnt, 1u)] = t;
+            if (threadIdx.x == 0) s_n = 0;
+            __syncthreads();
+            int v = 0, slot = -1;
+            if (i < c.n && j < c.n) {
+                const int x = c.qx + (i - c.half) * c.step, z = c.qz + (j - c.half) * c.step;
+                if (x >= -kWorld && x <= kWorld && z >= -kWorld && z <= kWorld) {
+                    PendingState p;
+                    v = eval_pred(c, s_noise, w, x, z, p);
+                    if (v < 0) { slot = atomicAdd(&s_n, 1); s_pend[slot] = p; }
+                }
+            }
+            __syncthreads();
+            if (int(threadIdx.x) < s_n) s_res[threadIdx.x] = int8_t(desert_state_finish(w, s_pend[threadIdx.x]));
+            __syncthreads();
+            if (slot >= 0) v = s_res[slot];
+            const uint32_t pm = __ballot_sync(0xffffffffu, v > 0), dm = __ballot_sync(0xffffffffu, v == 2);
+            if (lane == 0) {
+                uint32_t *b = reinterpret_cast<uint32_t *>(T.bits + size_t(t) * TILE_U64);
+                const int h = 2 * row + (warp & 1);
+                b[h] = pm; b[2 * TILE + h] = dm; b[4 * TILE + h] = 0;
+            }
+            __syncthreads();
+            if (threadIdx.x == 0) {
+                __threadfence();
+                if (atomicAdd(&T.done[t], 1u) == EVAL_ITEMS - 1) {
+                    T.state[t] = 1;
+                    if (atomicExch(&T.mark[t], q.round + 1) != q.round + 1) q.w_list[atomicAdd(q.w_cnt, 1u)] = t;
+                }
             }
         }
     }
@@ -277,7 +295,7 @@ __device__ __forceinline__ void start_bit(const FloodCtl &c, int ti, int tj, uin
 // Grow R of every queued tile to its fixed point; queue or claim the neighbours its new edge cells reach.
 static __global__ void __launch_bounds__(256) k_tile_connect(const FloodCtl *__restrict__ ctl, int32_t *__restrict__ dir, Tiles T,
                                                              TileAlloc ta, FloodStat *__restrict__ st, Round q) {
-    if (blockIdx.x == 0 && threadIdx.x == 0) { *q.zero_a = 0; *q.zero_b = 0; }
+    if (blockIdx.x == 0 && threadIdx.x == 0) { *q.zero_a = 0; *q.zero_b = 0; *q.zero_c = 0; }
     const uint32_t n = *q.w_cnt;
     const int lane = threadIdx.x & 31;
     const uint32_t nw = gridDim.x * (blockDim.x >> 5);
@@ -510,13 +528,13 @@ struct TilePool {
     }
 };
 // Launch one round: evaluate the tiles claimed last round, then connect.  cnt[0..2] are the rotating
-// claim-queue counters, cnt[3..5] the connect-queue ones.
+// claim-queue counters, cnt[3..5] the connect-queue ones, cnt[6..8] the evaluation work counters.
 inline void launch_round(const TilePool &p, uint32_t round, uint32_t *cnt, uint32_t *active, uint32_t *err, const FloodCtl *ctl,
                          const SeedNoise *noise, int32_t *dir, FloodStat *st, const TileAlloc &ta, int grid_eval, int grid_conn,
                          cudaStream_t s) {
     const Round q{round, p.n_list[round & 1], cnt + round % 3, p.w_list[round & 1], cnt + 3 + round % 3,
                   p.n_list[(round + 1) & 1], cnt + (round + 1) % 3, p.w_list[(round + 1) & 1], cnt + 3 + (round + 1) % 3,
-                  cnt + (round + 2) % 3, cnt + 3 + (round + 2) % 3, active, err};
+                  cnt + 6 + round % 3, cnt + (round + 2) % 3, cnt + 3 + (round + 2) % 3, cnt + 6 + (round + 2) % 3, active, err};
     k_tile_eval<<<grid_eval, EVAL_THREADS, 0, s>>>(ctl, noise, world_dev(), p.T, q);
     k_tile_connect<<<grid_conn, 256, 0, s>>>(ctl, dir, p.T, ta, st, q);
 }

@@ -87,7 +87,10 @@ __device__ __forceinline__ int64_t depth_q(const WorldDev &w, float c, float e, 
     return q10k(float(1. - (64 * 4) / 128. - 83. / 160. + off));
 }
 // Desert flood state at quart (x, 64, z) (surface.hpp:98-124): 2 desert, 1 river bridged to desert, 0 other.
-__device__ inline int desert_state(const SeedNoise &S, const WorldDev &w, int x, int z) {
+// In two parts so callers can batch the points the surface grid cannot decide: desert_state_begin returns the
+// state, or -1 with the climate `p` that desert_state_finish completes (exact depth, then the exact search).
+struct PendingState { int64_t q[6]; float c, e, w; int32_t stage; };
+__device__ __forceinline__ int desert_state_begin(const SeedNoise &S, const WorldDev &w, int x, int z, PendingState &p) {
     const double px = x + 4. * channel(S, CH_S, x, 0, z);
     const double pz = z + 4. * channel(S, CH_S, z, x, 0);
     const float t = float(channel(S, CH_T, px, 0, pz));
@@ -95,58 +98,39 @@ __device__ inline int desert_state(const SeedNoise &S, const WorldDev &w, int x,
     const float c = float(channel(S, CH_C, px, 0, pz)), e = float(channel(S, CH_E, px, 0, pz));
     const float wv = float(channel(S, CH_W, px, 0, pz)), h = float(channel(S, CH_H, px, 0, pz));
     int64_t q[6] = {q10k(t), q10k(h), q10k(c), q10k(e), -10000, q10k(wv)};
-    bool exact = false;
-    int b = grid_lookup(w, q);
-    if (b < 0) { q[4] = depth_q(w, c, e, wv); exact = true; b = tree_classify(w, q); }
-    if (b == 2) return 2;
-    if (b != 7 && b != 11) return 0;
-    if (q[5] > 500 || q[5] < -500) return 0;
-    q[5] = q[5] >= 0 ? 501 : -501;
-    b = grid_lookup(w, q);
-    if (b < 0) { if (!exact) q[4] = depth_q(w, c, e, wv); b = tree_classify(w, q); }
-    return b == 2 ? 1 : 0;
-}
-// desert_state without the tree search: returns the state when the surface grid decides both picks, or -1
-// with `fb` filled for classify_deferred_warp (the rare points on cut planes or in ambiguous grid cells).
-struct Deferred { int64_t q[6]; float c, e, w; int32_t stage; };
-__device__ inline int desert_state_grid(const SeedNoise &S, const WorldDev &w, int x, int z, Deferred &fb) {
-    const double px = x + 4. * channel(S, CH_S, x, 0, z);
-    const double pz = z + 4. * channel(S, CH_S, z, x, 0);
-    const float t = float(channel(S, CH_T, px, 0, pz));
-    if (q10k(t) < 5500) return 0;
-    const float c = float(channel(S, CH_C, px, 0, pz)), e = float(channel(S, CH_E, px, 0, pz));
-    const float wv = float(channel(S, CH_W, px, 0, pz)), h = float(channel(S, CH_H, px, 0, pz));
-    int64_t q[6] = {q10k(t), q10k(h), q10k(c), q10k(e), -10000, q10k(wv)};
-    auto defer = [&](int stage) {
-        for (int k = 0; k < 6; k++) fb.q[k] = q[k];
-        fb.c = c; fb.e = e; fb.w = wv; fb.stage = stage;
+    auto pend = [&](int stage) {
+        for (int k = 0; k < 6; k++) p.q[k] = q[k];
+        p.c = c; p.e = e; p.w = wv; p.stage = stage;
         return -1;
     };
     int b = grid_lookup(w, q);
-    if (b < 0) return defer(1);
+    if (b < 0) return pend(1);                     // first pick needs the exact search
     if (b == 2) return 2;
     if (b != 7 && b != 11) return 0;
     if (q[5] > 500 || q[5] < -500) return 0;
     q[5] = q[5] >= 0 ? 501 : -501;
     b = grid_lookup(w, q);
-    if (b < 0) return defer(2);
+    if (b < 0) return pend(2);                     // second pick (bridged river) needs it
     return b == 2 ? 1 : 0;
 }
-// Finish a deferred point exactly as desert_state would (surface.hpp:106-123): exact depth, then the tree
-// search, by the whole warp (classify_warp); `fb` must be the same in every lane.
-__device__ inline int classify_deferred_warp(const WorldDev &w, const int32_t *__restrict__ sp, const Deferred &fb) {
+__device__ inline int desert_state_finish(const WorldDev &w, const PendingState &p) {
     int64_t q[6];
-    for (int k = 0; k < 6; k++) q[k] = fb.q[k];
-    q[4] = depth_q(w, fb.c, fb.e, fb.w);
-    if (fb.stage == 2) return classify_warp(w, sp, q) == 2 ? 1 : 0;
-    int b = classify_warp(w, sp, q);
+    for (int k = 0; k < 6; k++) q[k] = p.q[k];
+    q[4] = depth_q(w, p.c, p.e, p.w);
+    if (p.stage == 2) return classify_exact(w, q) == 2 ? 1 : 0;
+    int b = classify_exact(w, q);
     if (b == 2) return 2;
     if (b != 7 && b != 11) return 0;
     if (q[5] > 500 || q[5] < -500) return 0;
     q[5] = q[5] >= 0 ? 501 : -501;
     b = grid_lookup(w, q);
-    if (b < 0) b = classify_warp(w, sp, q);
+    if (b < 0) b = classify_exact(w, q);
     return b == 2 ? 1 : 0;
+}
+__device__ inline int desert_state(const SeedNoise &S, const WorldDev &w, int x, int z) {
+    PendingState p;
+    const int v = desert_state_begin(S, w, x, z, p);
+    return v >= 0 ? v : desert_state_finish(w, p);
 }
 // Hot-zone predicate: temperature at the unwarped point >= 0.55 (dsearch_desert.cpp:334).
 __device__ __forceinline__ int hot_state(const SeedNoise &S, int x, int z) { return channel(S, CH_T, x, 0, z) >= 0.55 ? 2 : 0; }

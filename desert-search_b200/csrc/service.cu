@@ -47,7 +47,7 @@ struct Service {
     int32_t *d_dir = nullptr; int64_t dir_cap = 0;
     TilePool pool;
     uint32_t *d_ring = nullptr; uint32_t head = 0, avail = 0;
-    uint32_t *d_ctr = nullptr, *h_ctr = nullptr;               // [0] taken, [1] returned, [2..4] claim queues, [5..7] connect queues, [8] error flags
+    uint32_t *d_ctr = nullptr, *h_ctr = nullptr;               // [0] taken, [1] returned, [2..10] round counters (launch_round), [11] error flags
     uint32_t *d_slots = nullptr; uint64_t *d_seeds = nullptr;
     int grid_eval = 0, grid_conn = 0;
     int64_t dir_max = 0;                                       // largest directory of an admitted request
@@ -119,13 +119,13 @@ void engine_loop(Service &g) {
                 }
                 DSG_CU(cudaMemcpyAsync(g.d_slots, adm_slots.data(), na * 4, cudaMemcpyHostToDevice, st));
                 k_tile_start<<<(na + 127) / 128, 128, 0, st>>>(g.d_ctl, g.d_slots, na, g.d_stat, g.d_dir, g.pool.T, ta,
-                                                               g.pool.n_list[round & 1], g.d_ctr + 2 + round % 3, round, g.d_active, g.d_ctr + 8);
+                                                               g.pool.n_list[round & 1], g.d_ctr + 2 + round % 3, round, g.d_active, g.d_ctr + 11);
                 DSG_CU(cudaGetLastError());
                 // ctl/slots are host vectors: finish these copies before they go out of scope
                 DSG_CU(cudaStreamSynchronize(st));
             }
             for (uint32_t k = 0; k < K; k++, round++)
-                launch_round(g.pool, round, g.d_ctr + 2, g.d_active, g.d_ctr + 8, g.d_ctl, g.d_noise, g.d_dir, g.d_stat, ta,
+                launch_round(g.pool, round, g.d_ctr + 2, g.d_active, g.d_ctr + 11, g.d_ctl, g.d_noise, g.d_dir, g.d_stat, ta,
                              g.grid_eval, g.grid_conn, st);
             DSG_CU(cudaGetLastError());
             DSG_CU(cudaMemcpyAsync(g.h_active, g.d_active, size_t(S) * 4, cudaMemcpyDeviceToHost, st));

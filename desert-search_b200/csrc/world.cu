@@ -91,11 +91,65 @@ void build_grid(const Blob &b, WorldDev &w, std::vector<int16_t> &cells) {
     }
     for (int16_t &c : cells) if (c == UNSET) c = -1;
 }
-// Pruning blocks for classify_warp.  Walks the tree in the reference's depth-first order (children of a node
-// at `node + stride` steps, standalone.hpp:182-196) and checks what the warp search relies on: leaves appear
-// in increasing node order, every box below the root contains its children's boxes, and every leaf lies
-// below depth 3.  The root's box is a placeholder and is never tested by the search.
-void build_blocks(const Blob &b, std::vector<uint64_t> &leaf, std::vector<uint64_t> &blk, std::vector<uint32_t> &rng) {
+// Candidate leaves of every surface grid cell, for classify_exact.  A leaf's distance to a point of the cell
+// is its 5-axis distance (T, H, C, E, W) plus its depth-axis term, and the depth term is the same for every
+// leaf with the same depth interval.  So a leaf L cannot be the nearest anywhere in the cell when some leaf
+// K of its depth interval has max-distance(K, cell) < min-distance(L, cell); every other leaf is kept.  The
+// tree walk checks first that below the root every box contains its children's boxes and that leaves come
+// in increasing node order in the reference's depth-first walk (standalone.hpp:182-196), which together make
+// the walk's result the (distance, node index) minimum over all leaves.
+struct LeafBox { int32_t lo[5], hi[5]; int32_t node, cls; };
+constexpr int kMaxDepthClasses = 8;
+__device__ __forceinline__ void leaf_span(const LeafBox &l, const int64_t *A, const int64_t *B, uint64_t &mn, uint64_t &mx) {
+    mn = 0; mx = 0;
+    #pragma unroll
+    for (int a = 0; a < 5; a++) {
+        const int64_t lo = l.lo[a], hi = l.hi[a];
+        const int64_t d0 = max(max(lo - B[a], A[a] - hi), int64_t(0));
+        const int64_t da = max(max(lo - A[a], A[a] - hi), int64_t(0)), db = max(max(lo - B[a], B[a] - hi), int64_t(0));
+        const int64_t d1 = max(da, db);
+        mn += uint64_t(d0 * d0); mx += uint64_t(d1 * d1);
+    }
+}
+// One block per grid cell.  off == nullptr: count the candidates into cnt[cell]; else write them, in leaf
+// order, from cand[off[cell]].
+__global__ void __launch_bounds__(256) k_cand(const LeafBox *__restrict__ leaves, int nleaf, WorldDev w, uint32_t *__restrict__ cnt,
+                                              const uint32_t *__restrict__ off, uint16_t *__restrict__ cand) {
+    __shared__ unsigned long long s_m[kMaxDepthClasses];
+    __shared__ uint32_t s_warp[8];
+    uint32_t r = blockIdx.x;
+    int64_t A[5], B[5];
+    for (int a = 4; a >= 0; a--) {
+        const uint32_t i = r % uint32_t(w.cdim[a]);
+        r /= uint32_t(w.cdim[a]);
+        A[a] = w.ccut[a][i]; B[a] = int64_t(w.ccut[a][i + 1]) - 1;
+    }
+    if (threadIdx.x < kMaxDepthClasses) s_m[threadIdx.x] = ~0ull;
+    __syncthreads();
+    for (int k = threadIdx.x; k < nleaf; k += blockDim.x) {
+        uint64_t mn, mx;
+        leaf_span(leaves[k], A, B, mn, mx);
+        atomicMin(&s_m[leaves[k].cls], mx);
+    }
+    __syncthreads();
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    uint32_t base = off ? off[blockIdx.x] : 0;
+    for (int k0 = 0; k0 < nleaf; k0 += blockDim.x) {
+        const int k = k0 + threadIdx.x;
+        bool keep = false;
+        if (k < nleaf) { uint64_t mn, mx; leaf_span(leaves[k], A, B, mn, mx); keep = mn <= s_m[leaves[k].cls]; }
+        const uint32_t m = __ballot_sync(0xffffffffu, keep);
+        if (lane == 0) s_warp[warp] = __popc(m);
+        __syncthreads();
+        uint32_t before = 0, total = 0;
+        for (int q = 0; q < 8; q++) { if (q < warp) before += s_warp[q]; total += s_warp[q]; }
+        if (keep && off) cand[base + before + __popc(m & ((1u << lane) - 1))] = uint16_t(leaves[k].node);
+        base += total;
+        __syncthreads();
+    }
+    if (!off && threadIdx.x == 0) cnt[blockIdx.x] = base;
+}
+void check_tree(const Blob &b) {
     const int n = int(b.tree.size());
     auto is_leaf = [&](int k) { return (b.tree[k] >> 56) == 255; };
     auto inside = [&](int child, int parent) {
@@ -105,21 +159,14 @@ void build_blocks(const Blob &b, std::vector<uint64_t> &leaf, std::vector<uint64
         }
         return true;
     };
-    struct Fr { int node, level, depth; };
-    std::vector<Fr> stk{{0, 0, 0}};
+    struct Fr { int node, level; };
+    std::vector<Fr> stk{{0, 0}};
     int last_leaf = -1;
-    // iterative pre-order walk; children pushed in reverse so they pop in order
-    while (!stk.empty()) {
+    while (!stk.empty()) {                         // pre-order walk; children pushed in reverse so they pop in order
         const Fr f = stk.back(); stk.pop_back();
-        if (f.depth == 3) {                        // leaves of this block follow contiguously in pre-order
-            blk.push_back(b.tree[f.node]);
-            rng.push_back(uint32_t(leaf.size()));
-        }
         if (is_leaf(f.node)) {
-            if (f.depth <= 3) throw std::runtime_error("biome tree: leaf above depth 4");
             if (f.node <= last_leaf) throw std::runtime_error("biome tree: leaves out of node order");
             last_leaf = f.node;
-            leaf.push_back(b.tree[f.node]);
             continue;
         }
         int stride = 0, lv = f.level;
@@ -127,15 +174,70 @@ void build_blocks(const Blob &b, std::vector<uint64_t> &leaf, std::vector<uint64
         std::vector<Fr> kids;
         for (int i = 0, c = int(b.tree[f.node] >> 48); i < 6 && c < n; i++, c += stride) {
             if (f.node != 0 && !inside(c, f.node)) throw std::runtime_error("biome tree: child box outside its parent");
-            kids.push_back({c, lv, f.depth + 1});
+            kids.push_back({c, lv});
         }
         for (auto it = kids.rbegin(); it != kids.rend(); ++it) stk.push_back(*it);
     }
-    for (size_t k = 0; k < rng.size(); k++) {
-        const uint32_t lo = rng[k], hi = k + 1 < rng.size() ? rng[k + 1] : uint32_t(leaf.size());
-        rng[k] = lo | (hi << 16);
+}
+// Candidate grid: the surface grid's cuts plus extra temperature cuts above it, since points inside desert
+// floods often have T > 1, beyond every surface box (up to T = 2; a point past the candidate grid on any
+// axis takes the tree search).
+void build_cand_grid(WorldDev &w) {
+    static const int32_t kHotCuts[] = {11001, 12001, 13001, 14001, 15001, 17001, 20001};
+    for (int a = 0; a < 5; a++) {
+        std::vector<int32_t> c(w.cut[a], w.cut[a] + w.ncut[a]);
+        if (a == 0) c.insert(c.end(), std::begin(kHotCuts), std::end(kHotCuts));
+        std::sort(c.begin(), c.end());
+        c.erase(std::unique(c.begin(), c.end()), c.end());
+        if (c.size() > 48) throw std::runtime_error("candidate grid: too many cuts");
+        w.nccut[a] = int(c.size()); w.cdim[a] = w.nccut[a] - 1;
+        std::copy(c.begin(), c.end(), w.ccut[a]);
     }
-    if (blk.size() > size_t(32 * kBlkPerLane) || leaf.size() > 0xffff) throw std::runtime_error("biome tree: too many blocks or leaves");
+}
+void build_candidates(const Blob &b, WorldDev &w) {
+    static const int SLOT[5] = {0, 1, 2, 3, 5};
+    build_cand_grid(w);
+    std::vector<LeafBox> leaves;
+    std::vector<std::pair<int32_t, int32_t>> classes;
+    for (int k = 0; k < int(b.tree.size()); k++) {
+        const uint64_t e = b.tree[k];
+        if ((e >> 56) != 255) continue;
+        LeafBox l{};
+        for (int a = 0; a < 5; a++) { const int q = int((e >> (8 * SLOT[a])) & 255); l.lo[a] = b.param[2 * q]; l.hi[a] = b.param[2 * q + 1]; }
+        const int dq = int((e >> 32) & 255);
+        const std::pair<int32_t, int32_t> depth{b.param[2 * dq], b.param[2 * dq + 1]};
+        auto it = std::find(classes.begin(), classes.end(), depth);
+        if (it == classes.end()) { classes.push_back(depth); it = classes.end() - 1; }
+        l.node = k; l.cls = int(it - classes.begin());
+        leaves.push_back(l);
+    }
+    if (classes.size() > size_t(kMaxDepthClasses) || b.tree.size() > 0xffff) throw std::runtime_error("biome tree: too many depth intervals or nodes");
+    uint32_t ncell = 1;
+    for (int a = 0; a < 5; a++) ncell *= uint32_t(w.cdim[a]);
+    LeafBox *d_leaves = nullptr; uint32_t *d_cnt = nullptr, *d_off = nullptr; uint16_t *d_cand = nullptr;
+    try {
+        DSG_CU(cudaMalloc(&d_leaves, leaves.size() * sizeof(LeafBox)));
+        DSG_CU(cudaMemcpy(d_leaves, leaves.data(), leaves.size() * sizeof(LeafBox), cudaMemcpyHostToDevice));
+        DSG_CU(cudaMalloc(&d_cnt, size_t(ncell) * 4));
+        k_cand<<<ncell, 256>>>(d_leaves, int(leaves.size()), w, d_cnt, nullptr, nullptr);
+        DSG_CU(cudaGetLastError());
+        std::vector<uint32_t> cnt(ncell), off(size_t(ncell) + 1, 0);
+        DSG_CU(cudaMemcpy(cnt.data(), d_cnt, size_t(ncell) * 4, cudaMemcpyDeviceToHost));
+        uint64_t total = 0;
+        for (uint32_t c = 0; c < ncell; c++) {
+            total += cnt[c];
+            if (total > (uint64_t(1) << 28)) throw std::runtime_error("candidate lists: more than 2^28 entries");
+            off[c + 1] = uint32_t(total);
+        }
+        DSG_CU(cudaMalloc(&d_off, off.size() * 4));
+        DSG_CU(cudaMemcpy(d_off, off.data(), off.size() * 4, cudaMemcpyHostToDevice));
+        DSG_CU(cudaMalloc(&d_cand, size_t(off[ncell]) * 2 + 2));
+        k_cand<<<ncell, 256>>>(d_leaves, int(leaves.size()), w, nullptr, d_off, d_cand);
+        DSG_CU(cudaGetLastError());
+        DSG_CU(cudaDeviceSynchronize());
+    } catch (...) { cudaFree(d_leaves); cudaFree(d_cnt); cudaFree(d_off); cudaFree(d_cand); throw; }
+    cudaFree(d_leaves); cudaFree(d_cnt);
+    w.cand_off = d_off; w.cand = d_cand;
 }
 template <class T> const T *upload(const std::vector<T> &v) {
     T *d = nullptr;
@@ -157,12 +259,9 @@ void world_upload(int) {
     if (b.strides.size() > 8 || b.prob.size() != 1600) throw std::runtime_error("worldgen blob: bad sizes");
     for (size_t i = 0; i < b.strides.size(); i++) w.strides[i] = b.strides[i];
     w.ntree = int(b.tree.size()); w.nspl = int(b.spl.size()); w.nparam = int(b.param.size() / 2);
-    std::vector<uint64_t> leaf, blk;
-    std::vector<uint32_t> rng;
-    build_blocks(b, leaf, blk, rng);
     if (b.param.size() > 2 * 256) throw std::runtime_error("worldgen blob: too many parameter intervals");
-    w.nleaf = int(leaf.size()); w.nblk = int(blk.size());
-    w.leaf = upload(leaf); w.blk = upload(blk); w.blk_rng = upload(rng);
+    check_tree(b);
+    build_candidates(b, w);
     w.cells = upload(cells); w.tree = upload(b.tree); w.param = upload(b.param); w.spl = upload(b.spl); w.prob = upload(b.prob);
     g_world = w;
     g_prob = b.prob;

@@ -16,36 +16,46 @@ struct WorldDev {
     const int32_t *param;        // interval k = [param[2k], param[2k+1]]
     const SplineDev *spl;        // terrain-offset spline graph (node 0 is the root)
     const float *prob;           // 40 x 40 proxy desert probability (row = C bin, column = E bin)
-    const uint64_t *leaf;        // leaf nodes of the tree in depth-first order (their node words)
-    const uint64_t *blk;         // depth-3 nodes in depth-first order (node words): the pruning blocks
-    const uint32_t *blk_rng;     // leaves of block b: leaf[lo, hi) with lo = rng & 0xffff, hi = rng >> 16
-    int32_t ntree, nspl, nparam, nleaf, nblk;
+    const uint32_t *cand_off;    // candidate leaves of candidate-grid cell f: cand[cand_off[f] .. cand_off[f + 1])
+    const uint16_t *cand;        // tree node indices, ascending within a cell
+    int32_t ntree, nspl, nparam;
     int32_t strides[8];
     int32_t dim[5];              // grid cells per axis (T, H, C, E, W)
     int32_t ncut[5];             // cut planes per axis (= dim + 1)
     int32_t cut[5][32];          // sorted cut planes per axis
+    int32_t cdim[5], nccut[5];   // candidate grid: the surface cuts and extra temperature cuts above the
+    int32_t ccut[5][48];         //   surface grid
 };
 const WorldDev &world_dev();     // valid after dsg_init
 
 #ifdef __CUDACC__
-// Surface grid lookup (surface.hpp:58-70): the biome of the depth-0 surface box containing q, or -1 when q
-// lies outside the grid, on a cut plane, or in a cell that is ambiguous.
-__device__ __forceinline__ int grid_lookup(const WorldDev &w, const int64_t *q) {
+// Cell of q in the surface grid, axes T, H, C, E, W, each cell the half-open range [cut_k, cut_k+1): false when q
+// lies outside the grid.  on_cut: a coordinate equals a cut plane.
+__device__ __forceinline__ bool grid_locate(const WorldDev &w, const int64_t *q, uint32_t &flat, bool &on_cut) {
     constexpr int AX[5] = {0, 1, 2, 3, 5};
-    size_t flat = 0;
+    uint32_t f = 0;
+    on_cut = false;
     #pragma unroll
     for (int a = 0; a < 5; a++) {
         const int64_t v = q[AX[a]];
         const int32_t *c = w.cut[a];
         const int nc = w.ncut[a];
-        if (v < c[0] || v >= c[nc - 1]) return -1;
+        if (v < c[0] || v >= c[nc - 1]) return false;
         int lo = 0, hi = nc;                       // first cut > v (upper_bound)
         while (lo < hi) { const int mid = (lo + hi) >> 1; if (int64_t(c[mid]) <= v) lo = mid + 1; else hi = mid; }
         const int idx = lo - 1;
-        if (v == c[idx]) return -1;
-        flat = flat * size_t(w.dim[a]) + size_t(idx);
+        on_cut |= v == c[idx];
+        f = f * uint32_t(w.dim[a]) + uint32_t(idx);
     }
-    return w.cells[flat];
+    flat = f;
+    return true;
+}
+// Surface grid lookup (surface.hpp:58-70): the biome of the depth-0 surface box containing q, or -1 when q
+// lies outside the grid, on a cut plane, or in a cell that is ambiguous.
+__device__ __forceinline__ int grid_lookup(const WorldDev &w, const int64_t *q) {
+    uint32_t f; bool on_cut;
+    if (!grid_locate(w, q, f, on_cut) || on_cut) return -1;
+    return w.cells[f];
 }
 __device__ __forceinline__ uint64_t box_dist(const WorldDev &w, int node, const int64_t *v) {
     const uint64_t e = w.tree[node];
@@ -97,74 +107,41 @@ __device__ inline int tree_classify(const WorldDev &w, const int64_t *v) {
     }
     return int((w.tree[best] >> 48) & 255);
 }
-// Box distance of a node word with the parameter table in shared memory.
-__device__ __forceinline__ uint64_t box_dist_w(uint64_t e, const int32_t *__restrict__ sp, const int64_t *v) {
-    uint64_t sum = 0;
+// Cell of q in the candidate grid (half-open cells as in grid_locate); false outside it.
+__device__ __forceinline__ bool cand_locate(const WorldDev &w, const int64_t *q, uint32_t &flat) {
+    constexpr int AX[5] = {0, 1, 2, 3, 5};
+    uint32_t f = 0;
     #pragma unroll
-    for (int i = 0; i < 6; i++) {
-        const int k = int((e >> (8 * i)) & 255);
-        const int64_t lo = sp[2 * k], hi = sp[2 * k + 1];
-        int64_t d = lo - v[i];
-        if (v[i] - hi > d) d = v[i] - hi;
-        if (d < 0) d = 0;
-        sum += uint64_t(d * d);
+    for (int a = 0; a < 5; a++) {
+        const int64_t v = q[AX[a]];
+        const int32_t *c = w.ccut[a];
+        const int nc = w.nccut[a];
+        if (v < c[0] || v >= c[nc - 1]) return false;
+        int lo = 0, hi = nc;
+        while (lo < hi) { const int mid = (lo + hi) >> 1; if (int64_t(c[mid]) <= v) lo = mid + 1; else hi = mid; }
+        f = f * uint32_t(w.cdim[a]) + uint32_t(lo - 1);
     }
-    return sum;
+    flat = f;
+    return true;
 }
-// Lexicographic (distance, index) minimum over the warp; every lane ends with the result.
-__device__ __forceinline__ void warp_argmin(uint64_t &d, int &i) {
-    #pragma unroll
-    for (int o = 16; o; o >>= 1) {
-        const uint64_t od = __shfl_xor_sync(0xffffffffu, d, o);
-        const int oi = __shfl_xor_sync(0xffffffffu, i, o);
-        if (od < d || (od == d && oi < i)) { d = od; i = oi; }
+// Exact nearest leaf (the reference's tree search, standalone.hpp:182-196): the (box distance, node index)
+// minimum over the candidate leaves of the point's candidate-grid cell.  Below the root every box contains
+// its children's boxes, so the pruned depth-first search returns exactly that minimum over all leaves; the
+// candidates of a cell are every leaf that can attain it for some point of the cell and any depth
+// (world_upload drops a leaf only when a leaf of the same depth interval is nearer everywhere in the cell).
+// Points outside the candidate grid (rare: climate values beyond the surface boxes other than hot
+// temperatures) take the tree search itself.
+__device__ inline int classify_exact(const WorldDev &w, const int64_t *v) {
+    uint32_t f;
+    if (!cand_locate(w, v, f)) return tree_classify(w, v);
+    uint64_t bestd = ~0ull;
+    int best = 0;
+    for (uint32_t k = __ldg(&w.cand_off[f]), e = __ldg(&w.cand_off[f + 1]); k < e; k++) {
+        const int node = __ldg(&w.cand[k]);
+        const uint64_t d = box_dist(w, node, v);
+        if (d < bestd) { bestd = d; best = node; }
     }
-}
-constexpr int kBlkPerLane = 7;                     // blocks per lane in classify_warp (nblk <= 224)
-// Nearest leaf by the whole warp: the leaf minimising (box distance, depth-first position).  That is what
-// the reference's pruned depth-first search returns (standalone.hpp:182-196): below the root every node's
-// box contains its children's boxes (world_upload checks it), so a pruned subtree cannot hold a strictly
-// nearer leaf, and a leaf replaces the best only when strictly nearer, so among equally near leaves the
-// first in depth-first order wins.  The warp first takes the box distances of the 216 depth-3 blocks,
-// scans the leaves of the nearest block for a bound, then scans every other block that can still beat it.
-// `v` must be the same in every lane; the parameter table `sp` is in shared memory.
-__device__ inline int classify_warp(const WorldDev &w, const int32_t *__restrict__ sp, const int64_t *v) {
-    const int lane = threadIdx.x & 31;
-    uint64_t bd[kBlkPerLane];
-    uint64_t md = ~0ull; int mi = 0x7fffffff;
-    #pragma unroll
-    for (int k = 0; k < kBlkPerLane; k++) {
-        const int b = lane + 32 * k;
-        bd[k] = b < w.nblk ? box_dist_w(__ldg(&w.blk[b]), sp, v) : ~0ull;
-        if (bd[k] < md) { md = bd[k]; mi = b; }
-    }
-    warp_argmin(md, mi);
-    uint64_t bestd = ~0ull; int besti = 0x7fffffff;
-    auto scan = [&](uint32_t rg) {
-        uint64_t d = ~0ull; int idx = 0x7fffffff;
-        for (int i = int(rg & 0xffff) + lane; i < int(rg >> 16); i += 32) {
-            const uint64_t x = box_dist_w(__ldg(&w.leaf[i]), sp, v);
-            if (x < d) { d = x; idx = i; }
-        }
-        warp_argmin(d, idx);
-        if (d < bestd || (d == bestd && idx < besti)) { bestd = d; besti = idx; }
-    };
-    scan(__ldg(&w.blk_rng[mi]));
-    #pragma unroll
-    for (int k = 0; k < kBlkPerLane; k++) {
-        uint32_t m = __ballot_sync(0xffffffffu, bd[k] <= bestd);
-        while (m) {
-            const int l = __ffs(m) - 1;
-            m &= m - 1;
-            const int b = 32 * k + l;
-            const uint64_t db = __shfl_sync(0xffffffffu, bd[k], l);
-            if (b == mi || db > bestd) continue;
-            const uint32_t rg = __ldg(&w.blk_rng[b]);
-            if (db == bestd && int(rg & 0xffff) > besti) continue;     // ties go to the earlier leaf
-            scan(rg);
-        }
-    }
-    return int((__ldg(&w.leaf[besti]) >> 48) & 255);
+    return int((__ldg(&w.tree[best]) >> 48) & 255);
 }
 __device__ __forceinline__ float lerpd_f(float t, float a, float b) { return float(double(a) + double(t) * (double(b) - double(a))); }
 // Terrain-offset spline (standalone.hpp:154-169) with an explicit stack.  The float/double mix of the

@@ -116,6 +116,13 @@ def flood_batch(reqs):
     return [a.as_tuple() for a in out]
 
 
+def flood_last_stats():
+    """{rounds, tiles, touched} of the last flood batch: tile rounds run, 64x64 tiles evaluated, cells touched."""
+    st = (C.c_uint64 * 3)()
+    _ck(lib.dsg_flood_last_stats(st), "dsg_flood_last_stats")
+    return {"rounds": int(st[0]), "tiles": int(st[1]), "touched": int(st[2])}
+
+
 def flood(seed, qx, qz, step, half, conn8=False, pred=PRED_DESERT, pcut=0.35):
     return flood_batch([flood_req(seed, qx, qz, step, half, conn8, pred, pcut)])[0]
 
