@@ -134,8 +134,8 @@ def bench_floods(dsgpu, n_small=4096, rate=500.0, n_service=1500, n_seq=120, bat
     batch = {"floods": len(reqs), "small": len(small), "large": len(large), "seconds": t_batch, "floods_per_s": len(reqs) / t_batch,
              "cells_per_s": float(cells.sum()) / t_batch, "evaluations_per_s": sampled / t_batch,
              "area_blocks2_min_median_max": [float(cells.min() * 16), float(np.median(cells) * 16), float(cells.max() * 16)],
-             "rounds": work["rounds"], "tiles": work["tiles"], "cells_evaluated_per_s": work["tiles"] * 4096 / t_batch,
-             "speculation_overhead": work["tiles"] * 4096 / max(1, work["touched"])}
+             "rounds": work["rounds"], "subblocks": work["blocks"], "cells_evaluated_per_s": work["blocks"] * 256 / t_batch,
+             "speculation_overhead": work["blocks"] * 256 / max(1, work["touched"])}
     if batch_only:
         return {"batch": batch}
     # service: 90% small, 10% large, Poisson arrivals at `rate`

@@ -19,13 +19,16 @@ struct Engine {
     cudaStream_t st = nullptr;
     TilePool pool;
     uint32_t *d_cnt = nullptr, *h_cnt = nullptr;   // [0..8] round counters (launch_round), [9] taken, [10] error flags
+    unsigned long long *d_evals = nullptr;          // sub-blocks evaluated
     int32_t *d_dir = nullptr; size_t dir_cap = 0;
     FloodCtl *d_ctl = nullptr; uint32_t ctl_cap = 0;
     FloodStat *d_stat = nullptr; uint32_t stat_cap = 0;
     SeedNoise *d_noise = nullptr; uint32_t noise_cap = 0;
     uint64_t *d_seeds = nullptr; uint32_t seeds_cap = 0;
     int grid_eval = 0, grid_conn = 0;
-    uint64_t last[3] = {0, 0, 0};                  // rounds, tiles evaluated, cells touched of the last batch
+    uint64_t last[3] = {0, 0, 0};                  // rounds, 16x16 sub-blocks evaluated, cells touched of the last batch
+    unsigned long long *d_ccnt = nullptr, *d_coff = nullptr; uint32_t ccnt_cap = 0, coff_cap = 0;   // cell export
+    int32_t *d_xz = nullptr; uint64_t xz_cap = 0;
 };
 Engine &E() { static Engine e; return e; }
 
@@ -38,6 +41,7 @@ void setup_locked(Engine &g) {
     round_grids(g.grid_eval, g.grid_conn);
     DSG_CU(cudaMalloc(&g.d_cnt, 16 * 4));
     DSG_CU(cudaMallocHost(&g.h_cnt, 16 * 4));
+    DSG_CU(cudaMalloc(&g.d_evals, 8));
     g.ready = true;
 }
 template <class T> void grow(T *&p, uint32_t &cap, size_t need) {
@@ -93,6 +97,7 @@ int run_batch(const dsg_flood_req *reqs, uint32_t n, dsg_area *out, size_t pool_
     DSG_CU(cudaMemcpyAsync(g.d_ctl, ctl.data(), size_t(n) * sizeof(FloodCtl), cudaMemcpyHostToDevice, st));
     DSG_CU(cudaMemsetAsync(g.d_dir, 0xFF, dir_total * 4, st));
     DSG_CU(cudaMemsetAsync(g.d_cnt, 0, 16 * 4, st));
+    DSG_CU(cudaMemsetAsync(g.d_evals, 0, 8, st));
     const TileAlloc ta{nullptr, 0, g.pool.cap, g.pool.cap, g.d_cnt + 9, nullptr, 0};
     k_tile_start<<<(n + 127) / 128, 128, 0, st>>>(g.d_ctl, nullptr, n, g.d_stat, g.d_dir, g.pool.T, ta, g.pool.n_list[0], g.d_cnt + 0,
                                                   0, nullptr, g.d_cnt + 10);
@@ -101,47 +106,50 @@ int run_batch(const dsg_flood_req *reqs, uint32_t n, dsg_area *out, size_t pool_
     uint32_t round = 0;
     for (;;) {
         for (int k = 0; k < K; k++, round++)
-            launch_round(g.pool, round, g.d_cnt, nullptr, g.d_cnt + 10, g.d_ctl, g.d_noise, g.d_dir, g.d_stat, ta, g.grid_eval, g.grid_conn, st);
+            launch_round(g.pool, round, g.d_cnt, nullptr, g.d_cnt + 10, g.d_evals, g.d_ctl, g.d_noise, g.d_dir, g.d_stat, ta, g.grid_eval, g.grid_conn, st);
         DSG_CU(cudaGetLastError());
         DSG_CU(cudaMemcpyAsync(g.h_cnt, g.d_cnt, 16 * 4, cudaMemcpyDeviceToHost, st));
         DSG_CU(cudaStreamSynchronize(st));
         if (g.h_cnt[round % 3] == 0 && g.h_cnt[3 + round % 3] == 0) break;
     }
     const uint32_t taken = g.h_cnt[9], flags = g.h_cnt[10];
-    k_tile_finish<<<scan_grid, 256, 0, st>>>(g.d_ctl, nullptr, g.d_dir, g.pool.T, g.d_stat, nullptr, 0, 0, nullptr);
+    k_tile_finish<<<scan_grid, 256, 0, st>>>(g.d_ctl, nullptr, g.d_dir, g.pool.T, g.d_stat);
     DSG_CU(cudaGetLastError());
     std::vector<FloodStat> hs(n);
     DSG_CU(cudaMemcpyAsync(hs.data(), g.d_stat, size_t(n) * sizeof(FloodStat), cudaMemcpyDeviceToHost, st));
     DSG_CU(cudaStreamSynchronize(st));
     int rc_cells = DSG_OK;
     if (cell_off) {                                      // list reached passable cells before the pool is reused
-        unsigned long long *d_cnt = nullptr, *d_off = nullptr; int32_t *d_xz = nullptr;
         std::vector<unsigned long long> cnt(n), offs(n + 1, 0);
-        auto fin = [&] { cudaFree(d_cnt); cudaFree(d_off); cudaFree(d_xz); };
-        try {
-            DSG_CU(cudaMalloc(&d_cnt, size_t(n) * 8)); DSG_CU(cudaMalloc(&d_off, size_t(n) * 8));
-            DSG_CU(cudaMemsetAsync(d_cnt, 0, size_t(n) * 8, st));
-            k_cells<<<scan_grid, 256, 0, st>>>(g.d_ctl, g.d_dir, g.pool.T, d_cnt, nullptr, nullptr, 0);
-            DSG_CU(cudaGetLastError());
-            DSG_CU(cudaMemcpyAsync(cnt.data(), d_cnt, size_t(n) * 8, cudaMemcpyDeviceToHost, st));
-            DSG_CU(cudaStreamSynchronize(st));
-            for (uint32_t r = 0; r < n; r++) offs[r + 1] = offs[r] + cnt[r];
-            for (uint32_t r = 0; r <= n; r++) cell_off[r] = offs[r];
-            if (offs[n] > cell_cap) { set_error("dsg_flood_batch_cells: %llu cells, capacity %llu", offs[n], (unsigned long long)cell_cap); rc_cells = DSG_OVERFLOW; }
-            else if (offs[n]) {
-                DSG_CU(cudaMalloc(&d_xz, size_t(offs[n]) * 8));
-                DSG_CU(cudaMemcpyAsync(d_off, offs.data(), size_t(n) * 8, cudaMemcpyHostToDevice, st));
-                DSG_CU(cudaMemsetAsync(d_cnt, 0, size_t(n) * 8, st));
-                k_cells<<<scan_grid, 256, 0, st>>>(g.d_ctl, g.d_dir, g.pool.T, d_cnt, d_off, d_xz, offs[n]);
-                DSG_CU(cudaGetLastError());
-                DSG_CU(cudaMemcpyAsync(cell_xz, d_xz, size_t(offs[n]) * 8, cudaMemcpyDeviceToHost, st));
-                DSG_CU(cudaStreamSynchronize(st));
+        grow(g.d_ccnt, g.ccnt_cap, n);
+        grow(g.d_coff, g.coff_cap, n);
+        DSG_CU(cudaMemsetAsync(g.d_ccnt, 0, size_t(n) * 8, st));
+        k_cells<<<scan_grid, 256, 0, st>>>(g.d_ctl, g.d_dir, g.pool.T, g.d_ccnt, nullptr, nullptr, 0);
+        DSG_CU(cudaGetLastError());
+        DSG_CU(cudaMemcpyAsync(cnt.data(), g.d_ccnt, size_t(n) * 8, cudaMemcpyDeviceToHost, st));
+        DSG_CU(cudaStreamSynchronize(st));
+        for (uint32_t r = 0; r < n; r++) offs[r + 1] = offs[r] + cnt[r];
+        for (uint32_t r = 0; r <= n; r++) cell_off[r] = offs[r];
+        if (offs[n] > cell_cap) { set_error("dsg_flood_batch_cells: %llu cells, capacity %llu", offs[n], (unsigned long long)cell_cap); rc_cells = DSG_OVERFLOW; }
+        else if (offs[n]) {
+            if (offs[n] > g.xz_cap) {
+                cudaFree(g.d_xz); g.d_xz = nullptr;
+                const uint64_t c = std::max<uint64_t>(offs[n], 2 * g.xz_cap);
+                DSG_CU(cudaMalloc(&g.d_xz, size_t(c) * 8));
+                g.xz_cap = c;
             }
-        } catch (...) { fin(); throw; }
-        fin();
+            DSG_CU(cudaMemcpyAsync(g.d_coff, offs.data(), size_t(n) * 8, cudaMemcpyHostToDevice, st));
+            DSG_CU(cudaMemsetAsync(g.d_ccnt, 0, size_t(n) * 8, st));
+            k_cells<<<scan_grid, 256, 0, st>>>(g.d_ctl, g.d_dir, g.pool.T, g.d_ccnt, g.d_coff, g.d_xz, offs[n]);
+            DSG_CU(cudaGetLastError());
+            DSG_CU(cudaMemcpyAsync(cell_xz, g.d_xz, size_t(offs[n]) * 8, cudaMemcpyDeviceToHost, st));
+            DSG_CU(cudaStreamSynchronize(st));
+        }
     }
     g.pool.reset(taken, st);                             // the next batch allocates from tile 0 again
-    g.last[0] = round; g.last[1] = std::min(taken, g.pool.cap); g.last[2] = 0;
+    unsigned long long evals = 0;
+    DSG_CU(cudaMemcpy(&evals, g.d_evals, 8, cudaMemcpyDeviceToHost));
+    g.last[0] = round; g.last[1] = evals; g.last[2] = 0;
     for (uint32_t r = 0; r < n; r++) g.last[2] += hs[r].sampled;
     for (uint32_t r = 0; r < n; r++) {
         const FloodStat &s = hs[r];

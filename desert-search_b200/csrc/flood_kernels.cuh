@@ -4,16 +4,18 @@
 // The reference floods by a depth-first walk over a (2*half+1)^2 byte window (src/dense_flood.hpp:20-86):
 // each cell it touches is evaluated once, and passable cells push their neighbours.  Its result depends only
 // on the set R of passable cells connected to the start (and on the cells adjacent to R), not on the visit
-// order.  The engine therefore evaluates the predicate speculatively over whole 64x64 tiles of the window and
-// finds R by bit-parallel fills:
-//  * a tile is claimed (directory atomicCAS) when R reaches its edge; claimed tiles are evaluated in the next
-//    round by k_tile_eval, every cell at once (16 blocks of 256 cells per tile), into bit rows P (passable)
-//    and D (desert, counted);
+// order.  The engine therefore evaluates the predicate speculatively over 16x16-cell sub-blocks and finds R
+// by bit-parallel fills over 64x64-cell tiles:
+//  * a tile (4x4 sub-blocks, zeroed when claimed) is claimed through the request's directory (atomicCAS);
+//    a sub-block is requested when a cell of R becomes adjacent to it, and evaluated in the next round by
+//    k_tile_eval, every cell at once, into bit rows P (passable) and D (desert, counted).  Cells of
+//    sub-blocks not yet evaluated read as impassable;
 //  * k_tile_connect grows R inside each queued tile to its fixed point (row fills, column fills across the
-//    warp, the diagonal step for 8-connectivity), seeded from the R edges of the neighbouring tiles; when R
-//    changes on an edge it queues the neighbour, or claims it if it does not exist yet.  R only grows, so the
-//    rounds reach the unique fixed point whatever the interleaving;
-//  * when a request has no queued tile left, k_tile_finish derives DenseArea from R, D and the neighbours:
+//    warp, the diagonal step for 8-connectivity), seeded from the R edges of the neighbouring tiles; it
+//    requests the sub-blocks next to R (in this tile and across its edges) and queues evaluated neighbours
+//    whose shared edge changed.  R only grows, so the rounds reach the unique fixed point whatever the
+//    interleaving, and at that point every cell adjacent to R has been evaluated;
+//  * when a request has no queued work left, k_tile_finish derives DenseArea from R, D and the neighbours:
 //    cells = |R & D|, bbox over R & D, touched = start + R + neighbours of R, sampled = touched cells inside
 //    window and world, border = a touched cell outside the world, edge = an R cell on the window boundary.
 #pragma once
@@ -36,28 +38,31 @@ static_assert(sizeof(FloodStat) == 48, "FloodStat layout");
 constexpr int kWorld = 7499996;
 constexpr int TILE = 64;
 constexpr int TILE_U64 = 3 * TILE;     // rows of P, D, R
-constexpr int EVAL_THREADS = 256, EVAL_ITEMS = TILE * TILE / EVAL_THREADS;   // 16 blocks of 4 rows per tile
+constexpr int SUB = 16;                // sub-block edge; a tile has 4 x 4 sub-blocks, bit (row/16)*4 + col/16
+constexpr int EVAL_THREADS = SUB * SUB;
 
 // Tiles come from a pool: the k-th tile taken since the last host update is ring[(head + k) % cap]
 // (ring == nullptr: tile k itself, a bump allocator).  Taking never waits; `avail` bounds it.
 // returned (service only): a tile taken by a thread that then lost the directory race goes back to the ring
 // at (tail + k) % cap, k counted by *returned (those ring positions are free while head..head+avail are not).
 struct TileAlloc { uint32_t *ring; uint32_t head, avail, cap; uint32_t *taken; uint32_t *returned; uint32_t tail; };
-// Per-tile storage.  bits: tile t holds P rows at [t*192, +64), D rows at +64, R rows at +128 (bit c of
-// row r = cell (64*ti + c, 64*tj + r) of the window).  state: 1 once evaluated (0 while claimed, reset on
-// release); done: evaluated row blocks; mark: 1 + the round the tile was last queued for connect.
-struct Tiles { uint64_t *bits; uint32_t *owner, *pos, *state, *done, *mark; };
-// Queues of one round: n (claimed, to evaluate), w (to connect); *_next are the next round's.
+// Per-tile storage, all zero while a tile is free.  bits: tile t holds P rows at [t*192, +64), D rows at +64,
+// R rows at +128 (bit c of row r = cell (64*ti + c, 64*tj + r) of the window).  emask / qmask: sub-blocks
+// evaluated / requested.  mark: 1 + the round the tile was last queued for connect.
+struct Tiles { uint64_t *bits; uint32_t *owner, *pos, *emask, *qmask, *mark; };
+// Queues of one round: n (sub-blocks to evaluate, entries tile * 16 + sub-block), w (tiles to connect);
+// *_next are the next round's.
 struct Round {
     uint32_t round;
     const uint32_t *n_list; const uint32_t *n_cnt;
     uint32_t *w_list; uint32_t *w_cnt;
     uint32_t *n_next; uint32_t *n_next_cnt;
     uint32_t *w_next; uint32_t *w_next_cnt;
-    uint32_t *work;                    // items of this round's evaluation handed out so far
+    uint32_t *work;                    // sub-blocks of this round's evaluation handed out so far
     uint32_t *zero_a, *zero_b, *zero_c; // counters of the round after next, cleared by connect
     uint32_t *active;                  // per request: the last round it has queued work for (service)
     uint32_t *err;                     // bit 0: tile pool exhausted
+    unsigned long long *evaluated;     // sub-blocks evaluated (statistics)
 };
 
 // Predicate value of request c at quart (x, z): 2 counted, 1 crossed (bridged river), 0 boundary; -1 with `p`
@@ -68,11 +73,10 @@ __device__ __forceinline__ int eval_pred(const FloodCtl &c, const SeedNoise &S, 
     return proxy_prob(S, w, x, z) >= c.pcut ? 2 : 0;
 }
 
-// Claim tile (ti, tj) of request r for evaluation in round `eval_round`, or return the existing one.
-// Returns the pool index, or -1 when the pool is exhausted (the request is marked overflowed).
+// Tile (ti, tj) of request r: the existing one, or a newly claimed zeroed tile.  -1 when the pool is
+// exhausted (the request is marked overflowed).
 __device__ inline int32_t claim_tile(const FloodCtl &c, uint32_t r, int ti, int tj, int32_t *__restrict__ dir, const Tiles &T,
-                                     const TileAlloc &ta, uint32_t *n_out, uint32_t *n_out_cnt, uint32_t eval_round,
-                                     uint32_t *active, FloodStat *__restrict__ st, uint32_t *err) {
+                                     const TileAlloc &ta, FloodStat *__restrict__ st, uint32_t *err) {
     int32_t *e = dir + c.dir_off + int64_t(tj) * c.tpr + ti;
     const int32_t d = __ldcg(e);
     if (d >= 0) return d;
@@ -86,12 +90,25 @@ __device__ inline int32_t claim_tile(const FloodCtl &c, uint32_t r, int ti, int 
     }
     T.owner[nt] = r;
     T.pos[nt] = uint32_t(ti) | (uint32_t(tj) << 16);
-    n_out[atomicAdd(n_out_cnt, 1u)] = uint32_t(nt);
-    if (active) active[r] = eval_round;
     return nt;
 }
+// Queue the sub-blocks of `mask` in tile t that were not requested before, for evaluation in `eval_round`.
+__device__ inline void request_blocks(const Tiles &T, int32_t t, uint32_t mask, uint32_t r, uint32_t *n_out, uint32_t *n_out_cnt,
+                                      uint32_t eval_round, uint32_t *active) {
+    if (t < 0 || !mask) return;
+    uint32_t fresh = mask & ~atomicOr(&T.qmask[t], mask);
+    if (!fresh) return;
+    const uint32_t at = atomicAdd(n_out_cnt, uint32_t(__popc(fresh)));
+    for (uint32_t k = 0; fresh; k++) {
+        const int b = __ffs(fresh) - 1;
+        fresh &= fresh - 1;
+        n_out[at + k] = (uint32_t(t) << 4) | uint32_t(b);
+    }
+    if (active) active[r] = eval_round;
+}
 
-// Start requests (slots, or 0..nreq-1): statistics reset, start tile claimed for evaluation in `round`.
+// Start requests (slots, or 0..nreq-1): statistics reset, start tile claimed and the start's sub-block
+// requested for evaluation in `round`.
 static __global__ void k_tile_start(const FloodCtl *__restrict__ ctl, const uint32_t *__restrict__ slots, uint32_t nreq,
                                     FloodStat *__restrict__ st, int32_t *__restrict__ dir, Tiles T, TileAlloc ta,
                                     uint32_t *n_list, uint32_t *n_cnt, uint32_t round, uint32_t *active, uint32_t *err) {
@@ -101,17 +118,19 @@ static __global__ void k_tile_start(const FloodCtl *__restrict__ ctl, const uint
     const FloodCtl c = ctl[r];
     FloodStat &s = st[r];
     s.cells = 0; s.sampled = 0; s.minx = s.maxx = c.qx; s.minz = s.maxz = c.qz; s.edge = s.border = s.overflow = 0;
-    claim_tile(c, r, c.half >> 6, c.half >> 6, dir, T, ta, n_list, n_cnt, round, active, st, err);
+    const int32_t t = claim_tile(c, r, c.half >> 6, c.half >> 6, dir, T, ta, st, err);
+    const int sb = (((c.half & 63) >> 4) << 2) | ((c.half & 63) >> 4);
+    request_blocks(T, t, 1u << sb, r, n_list, n_cnt, round, active);
 }
 
-// Evaluate claimed tiles: block item = (tile, 4 rows); warp = half a row, written as 32-bit halves of the P
-// and D rows (R cleared).  Blocks take runs of consecutive items from a round counter (up to a whole tile
-// at a time when the round is large), which balances tiles of very different cost and keeps a block on one
-// request for many items; the request's noise tables stay in shared memory while it does, so every Perlin
-// lookup is a shared-memory access.  Points the surface grid cannot decide (about one in eight near desert
-// edges) are gathered in shared memory and finished by the first threads of the block, so the exact
-// searches run in full warps instead of as one diverged lane per warp.  The last row block of a tile to
-// finish marks it evaluated and queues it for this round's connect.
+// Evaluate requested sub-blocks: one block of 256 threads per sub-block, a cell per thread (warp = two rows
+// of 16 cells), written as 16-bit pieces of the P and D rows.  Blocks take runs of consecutive sub-blocks
+// from a round counter (up to 16 at a time when the round is large), which balances sub-blocks of very
+// different cost and keeps a block on one request for many items; the request's noise tables stay in
+// shared memory while it does, so every Perlin lookup is a shared-memory access.  Points the surface grid
+// cannot decide (about one in eight near desert edges) are gathered in shared memory and finished by the
+// first threads of the block, so the exact searches run in full warps instead of as one diverged lane per
+// warp.  Each evaluated sub-block marks its tile and queues it for this round's connect.
 static __global__ void __launch_bounds__(EVAL_THREADS) k_tile_eval(const FloodCtl *__restrict__ ctl, const SeedNoise *__restrict__ noise,
                                                                    WorldDev w, Tiles T, Round q) {
     __shared__ SeedNoise s_noise;
@@ -119,23 +138,23 @@ static __global__ void __launch_bounds__(EVAL_THREADS) k_tile_eval(const FloodCt
     __shared__ int8_t s_res[EVAL_THREADS];
     __shared__ int s_n, s_seed;
     __shared__ uint32_t s_run;
-    const uint32_t items = *q.n_cnt * EVAL_ITEMS;
-    const uint32_t run = max(1u, min(uint32_t(EVAL_ITEMS), items / (4 * gridDim.x)));
+    const uint32_t items = *q.n_cnt;
+    const uint32_t run = max(1u, min(16u, items / (4 * gridDim.x)));
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     if (threadIdx.x == 0) s_seed = -1;
     for (;;) {
-        __syncthreads();                                      // s_run of the previous run has been read
+        __syncthreads();                                  // s_run of the previous run has been read
         if (threadIdx.x == 0) s_run = atomicAdd(q.work, run);
         __syncthreads();
         const uint32_t begin = s_run;
         if (begin >= items) break;
         for (uint32_t item = begin; item < min(items, begin + run); item++) {
-            const uint32_t t = q.n_list[item / EVAL_ITEMS];
-            const int row = int(item % EVAL_ITEMS) * 4 + (warp >> 1), col = ((warp & 1) << 5) | lane;
+            const uint32_t e = q.n_list[item], t = e >> 4, sb = e & 15;
+            const int row = int(sb >> 2) * SUB + (threadIdx.x >> 4), col = int(sb & 3) * SUB + (threadIdx.x & 15);
             const uint32_t r = T.owner[t], pos = T.pos[t];
             const FloodCtl c = ctl[r];
             const int i = int(pos & 0xffff) * TILE + col, j = int(pos >> 16) * TILE + row;
-            __syncthreads();                                  // the previous item is done with shared memory
+            __syncthreads();                              // the previous item is done with shared memory
             const bool restage = s_seed != c.noise;
             __syncthreads();
             if (restage) {
@@ -160,18 +179,18 @@ static __global__ void __launch_bounds__(EVAL_THREADS) k_tile_eval(const FloodCt
             __syncthreads();
             if (slot >= 0) v = s_res[slot];
             const uint32_t pm = __ballot_sync(0xffffffffu, v > 0), dm = __ballot_sync(0xffffffffu, v == 2);
-            if (lane == 0) {
-                uint32_t *b = reinterpret_cast<uint32_t *>(T.bits + size_t(t) * TILE_U64);
-                const int h = 2 * row + (warp & 1);
-                b[h] = pm; b[2 * TILE + h] = dm; b[4 * TILE + h] = 0;
+            if (lane == 0) {                              // lanes 0-15: row `row`, lanes 16-31: row + 1
+                uint16_t *b = reinterpret_cast<uint16_t *>(T.bits + size_t(t) * TILE_U64);
+                const int h = row * 4 + int(sb & 3);
+                b[h] = uint16_t(pm); b[h + 4] = uint16_t(pm >> 16);
+                b[4 * TILE + h] = uint16_t(dm); b[4 * TILE + h + 4] = uint16_t(dm >> 16);
             }
             __syncthreads();
             if (threadIdx.x == 0) {
                 __threadfence();
-                if (atomicAdd(&T.done[t], 1u) == EVAL_ITEMS - 1) {
-                    T.state[t] = 1;
-                    if (atomicExch(&T.mark[t], q.round + 1) != q.round + 1) q.w_list[atomicAdd(q.w_cnt, 1u)] = t;
-                }
+                atomicOr(&T.emask[t], 1u << sb);
+                if (atomicExch(&T.mark[t], q.round + 1) != q.round + 1) q.w_list[atomicAdd(q.w_cnt, 1u)] = t;
+                atomicAdd(q.evaluated, 1ull);
             }
         }
     }
@@ -238,24 +257,40 @@ __device__ __forceinline__ void dilate(uint64_t ra, uint64_t rb, bool conn8, uin
     oa = h1(ra) | da | ua;
     ob = h1(rb) | db | ub;
 }
+// Sub-block bits (row/16 * 4 + col/16) of the set cells of row `row`.
+__device__ __forceinline__ uint32_t row_blocks(uint64_t x, int row) {
+    const uint32_t g = (uint32_t((x & 0xffffull) != 0)) | (uint32_t(((x >> 16) & 0xffffull) != 0) << 1) |
+                       (uint32_t(((x >> 32) & 0xffffull) != 0) << 2) | (uint32_t((x >> 48) != 0) << 3);
+    return g << ((row >> 4) * 4);
+}
+// Columns of the evaluated sub-blocks of row `row`.
+__device__ __forceinline__ uint64_t evaluated_cols(uint32_t emask, int row) {
+    const uint32_t g = (emask >> ((row >> 4) * 4)) & 15u;
+    return (g & 1 ? 0xffffull : 0) | (g & 2 ? 0xffff0000ull : 0) | (g & 4 ? 0xffff00000000ull : 0) | (g & 8 ? 0xffff000000000000ull : 0);
+}
+// Sub-block bits of the 16-row groups holding the set bits of a 64-bit row mask, in column group `cg`.
+__device__ __forceinline__ uint32_t col_blocks(uint64_t rows, int cg) {
+    uint32_t m = 0;
+    #pragma unroll
+    for (int g = 0; g < 4; g++) if ((rows >> (16 * g)) & 0xffffull) m |= 1u << (g * 4 + cg);
+    return m;
+}
 
-// Tile of request c at (ti, tj), or -1 (outside the window, not claimed, or, with need_eval, not evaluated).
-__device__ __forceinline__ int32_t tile_at(const FloodCtl &c, const int32_t *__restrict__ dir, const Tiles &T, int ti, int tj, bool need_eval) {
+// Tile of request c at (ti, tj), or -1 (outside the window or not claimed).  Unclaimed and unevaluated cells
+// read as zero either way.
+__device__ __forceinline__ int32_t tile_at(const FloodCtl &c, const int32_t *__restrict__ dir, int ti, int tj) {
     if (ti < 0 || tj < 0 || ti >= c.tpr || tj >= c.tpr) return -1;
-    const int32_t d = __ldcg(dir + c.dir_off + int64_t(tj) * c.tpr + ti);
-    if (d < 0 || (need_eval && __ldcg(&T.state[d]) != 1)) return -1;
-    return d;
+    return __ldcg(dir + c.dir_off + int64_t(tj) * c.tpr + ti);
 }
 __device__ __forceinline__ uint64_t r_row(const Tiles &T, int32_t d, int row) {
     return d < 0 ? 0 : __ldcg(&T.bits[size_t(d) * TILE_U64 + 2 * TILE + row]);
 }
 // Cells of this tile adjacent (4 or 8) to R cells of the neighbouring tiles, rows a/b of this lane.
-__device__ inline void outside_seeds(const FloodCtl &c, const int32_t *__restrict__ dir, const Tiles &T, int ti, int tj,
-                                     bool need_eval, uint64_t &sa, uint64_t &sb) {
+__device__ inline void outside_seeds(const FloodCtl &c, const int32_t *__restrict__ dir, const Tiles &T, int ti, int tj, uint64_t &sa, uint64_t &sb) {
     const int lane = threadIdx.x & 31;
     const bool c8 = c.conn8 != 0;
-    const int32_t L = tile_at(c, dir, T, ti - 1, tj, need_eval), Rt = tile_at(c, dir, T, ti + 1, tj, need_eval);
-    const int32_t U = tile_at(c, dir, T, ti, tj - 1, need_eval), Dn = tile_at(c, dir, T, ti, tj + 1, need_eval);
+    const int32_t L = tile_at(c, dir, ti - 1, tj), Rt = tile_at(c, dir, ti + 1, tj);
+    const int32_t U = tile_at(c, dir, ti, tj - 1), Dn = tile_at(c, dir, ti, tj + 1);
     // column 63 of the left tile and column 0 of the right one, as bit 0 / bit 63 of each row
     uint64_t xa = (r_row(T, L, lane) >> 63) | ((r_row(T, Rt, lane) & 1) << 63);
     uint64_t xb = (r_row(T, L, lane + 32) >> 63) | ((r_row(T, Rt, lane + 32) & 1) << 63);
@@ -270,16 +305,16 @@ __device__ inline void outside_seeds(const FloodCtl &c, const int32_t *__restric
         const uint64_t u = r_row(T, U, 63);
         sa |= c8 ? h1(u) : u;
         if (c8) {
-            sa |= r_row(T, tile_at(c, dir, T, ti - 1, tj - 1, need_eval), 63) >> 63;
-            sa |= (r_row(T, tile_at(c, dir, T, ti + 1, tj - 1, need_eval), 63) & 1) << 63;
+            sa |= r_row(T, tile_at(c, dir, ti - 1, tj - 1), 63) >> 63;
+            sa |= (r_row(T, tile_at(c, dir, ti + 1, tj - 1), 63) & 1) << 63;
         }
     }
     if (lane == 31) {                                    // row 63 from row 0 of the tile below
         const uint64_t d = r_row(T, Dn, 0);
         sb |= c8 ? h1(d) : d;
         if (c8) {
-            sb |= r_row(T, tile_at(c, dir, T, ti - 1, tj + 1, need_eval), 0) >> 63;
-            sb |= (r_row(T, tile_at(c, dir, T, ti + 1, tj + 1, need_eval), 0) & 1) << 63;
+            sb |= r_row(T, tile_at(c, dir, ti - 1, tj + 1), 0) >> 63;
+            sb |= (r_row(T, tile_at(c, dir, ti + 1, tj + 1), 0) & 1) << 63;
         }
     }
 }
@@ -292,7 +327,9 @@ __device__ __forceinline__ void start_bit(const FloodCtl &c, int ti, int tj, uin
     if (row == lane + 32) sb |= bit;
 }
 
-// Grow R of every queued tile to its fixed point; queue or claim the neighbours its new edge cells reach.
+// Grow R of every queued tile to its fixed point; request the unevaluated sub-blocks next to R (here and in
+// the neighbouring tiles, claiming those that do not exist yet) and queue evaluated neighbours whose shared
+// edge changed.
 static __global__ void __launch_bounds__(256) k_tile_connect(const FloodCtl *__restrict__ ctl, int32_t *__restrict__ dir, Tiles T,
                                                              TileAlloc ta, FloodStat *__restrict__ st, Round q) {
     if (blockIdx.x == 0 && threadIdx.x == 0) { *q.zero_a = 0; *q.zero_b = 0; *q.zero_c = 0; }
@@ -309,7 +346,7 @@ static __global__ void __launch_bounds__(256) k_tile_connect(const FloodCtl *__r
         const uint64_t pa = __ldcg(&tb[lane]), pb = __ldcg(&tb[lane + 32]);
         const uint64_t ra0 = __ldcg(&tb[2 * TILE + lane]), rb0 = __ldcg(&tb[2 * TILE + lane + 32]);
         uint64_t sa, sb;
-        outside_seeds(c, dir, T, ti, tj, true, sa, sb);
+        outside_seeds(c, dir, T, ti, tj, sa, sb);
         start_bit(c, ti, tj, sa, sb);
         uint64_t ra = ra0 | (sa & pa), rb = rb0 | (sb & pb);
         for (;;) {                                       // R grows monotonically inside P: this terminates
@@ -326,31 +363,44 @@ static __global__ void __launch_bounds__(256) k_tile_connect(const FloodCtl *__r
         const uint64_t na = ra ^ ra0, nb = rb ^ rb0;
         if (!__any_sync(0xffffffffu, (na | nb) != 0)) continue;
         tb[2 * TILE + lane] = ra; tb[2 * TILE + lane + 32] = rb;
-        // neighbours reached through new edge cells: lane k < 8 handles neighbour k
-        const uint64_t top = __shfl_sync(0xffffffffu, na, 0), bot = __shfl_sync(0xffffffffu, nb, 31);
-        const bool left = __any_sync(0xffffffffu, ((na | nb) & 1) != 0), right = __any_sync(0xffffffffu, ((na | nb) >> 63) != 0);
-        bool need = false; int dti = 0, dtj = 0;
+        // sub-blocks of this tile next to R that are not evaluated yet
+        const uint32_t em = __ldcg(&T.emask[t]);
+        uint64_t da, db;
+        dilate(ra, rb, c8, da, db);
+        const uint32_t self = __reduce_or_sync(0xffffffffu, row_blocks(da & ~evaluated_cols(em, lane), lane) |
+                                                               row_blocks(db & ~evaluated_cols(em, lane + 32), lane + 32));
+        // R on the edges: rows 0 and 63, and columns 0 and 63 as 64-row masks
+        const uint64_t top = __shfl_sync(0xffffffffu, ra, 0), bot = __shfl_sync(0xffffffffu, rb, 31);
+        const uint64_t top_new = __shfl_sync(0xffffffffu, na, 0), bot_new = __shfl_sync(0xffffffffu, nb, 31);
+        uint64_t lcol = uint64_t(__ballot_sync(0xffffffffu, ra & 1)) | (uint64_t(__ballot_sync(0xffffffffu, rb & 1)) << 32);
+        uint64_t rcol = uint64_t(__ballot_sync(0xffffffffu, ra >> 63)) | (uint64_t(__ballot_sync(0xffffffffu, rb >> 63)) << 32);
+        const bool left_new = __any_sync(0xffffffffu, ((na | nb) & 1) != 0), right_new = __any_sync(0xffffffffu, ((na | nb) >> 63) != 0);
+        if (c8) { lcol = h1(lcol); rcol = h1(rcol); }
+        // lane 0..7: neighbour k, lane 8: this tile
+        uint32_t mask = 0; bool changed = false; int dti = 0, dtj = 0;
         switch (lane) {
-            case 0: need = top != 0; dtj = -1; break;
-            case 1: need = bot != 0; dtj = 1; break;
-            case 2: need = left; dti = -1; break;
-            case 3: need = right; dti = 1; break;
-            case 4: need = c8 && (top & 1); dti = -1; dtj = -1; break;
-            case 5: need = c8 && (top >> 63); dti = 1; dtj = -1; break;
-            case 6: need = c8 && (bot & 1); dti = -1; dtj = 1; break;
-            case 7: need = c8 && (bot >> 63); dti = 1; dtj = 1; break;
+            case 0: mask = row_blocks(c8 ? h1(top) : top, 63); changed = top_new != 0; dtj = -1; break;
+            case 1: mask = row_blocks(c8 ? h1(bot) : bot, 0); changed = bot_new != 0; dtj = 1; break;
+            case 2: mask = col_blocks(lcol, 3); changed = left_new; dti = -1; break;
+            case 3: mask = col_blocks(rcol, 0); changed = right_new; dti = 1; break;
+            case 4: mask = c8 && (top & 1) ? 1u << 15 : 0; changed = (top_new & 1) != 0; dti = -1; dtj = -1; break;
+            case 5: mask = c8 && (top >> 63) ? 1u << 12 : 0; changed = (top_new >> 63) != 0; dti = 1; dtj = -1; break;
+            case 6: mask = c8 && (bot & 1) ? 1u << 3 : 0; changed = (bot_new & 1) != 0; dti = -1; dtj = 1; break;
+            case 7: mask = c8 && (bot >> 63) ? 1u : 0; changed = (bot_new >> 63) != 0; dti = 1; dtj = 1; break;
+            case 8: mask = self; break;
             default: break;
         }
+        if (lane == 8) request_blocks(T, int32_t(t), mask, r, q.n_next, q.n_next_cnt, q.round + 1, q.active);
         const int nti = ti + dti, ntj = tj + dtj;
-        if (need && nti >= 0 && ntj >= 0 && nti < c.tpr && ntj < c.tpr) {
-            const int32_t d = __ldcg(dir + c.dir_off + int64_t(ntj) * c.tpr + nti);
-            if (d < 0) claim_tile(c, r, nti, ntj, dir, T, ta, q.n_next, q.n_next_cnt, q.round + 1, q.active, st, q.err);
-            else if (__ldcg(&T.state[d]) == 1) {         // evaluated: connect it again next round
+        if (lane < 8 && mask && nti >= 0 && ntj >= 0 && nti < c.tpr && ntj < c.tpr) {
+            const int32_t d = claim_tile(c, r, nti, ntj, dir, T, ta, st, q.err);
+            request_blocks(T, d, mask, r, q.n_next, q.n_next_cnt, q.round + 1, q.active);
+            if (d >= 0 && changed && (__ldcg(&T.emask[d]) & mask)) {      // evaluated cells next to new R: reconnect
                 if (atomicExch(&T.mark[d], q.round + 2) != q.round + 2) {
                     q.w_next[atomicAdd(q.w_next_cnt, 1u)] = uint32_t(d);
                     if (q.active) q.active[r] = q.round + 1;
                 }
-            }                                            // else claimed this round: connected after its evaluation
+            }
         }
     }
 }
@@ -373,7 +423,7 @@ __device__ inline void tile_stats(const FloodCtl &c, const int32_t *__restrict__
     // touched cells: R, its neighbours in this tile, neighbours of the adjacent tiles' R, the start
     uint64_t ua, ub, sa, sb;
     dilate(ra, rb, c.conn8 != 0, ua, ub);
-    outside_seeds(c, dir, T, ti, tj, false, sa, sb);
+    outside_seeds(c, dir, T, ti, tj, sa, sb);
     start_bit(c, ti, tj, sa, sb);
     ua |= sa; ub |= sb;
     // window and world (cell (i, j) is quart (qx + (i - half) * step, qz + (j - half) * step))
@@ -418,11 +468,10 @@ __device__ inline void tile_stats(const FloodCtl &c, const int32_t *__restrict__
 // Directory entries one block of k_tile_finish / k_cells scans (blockIdx.y = chunk of the directory).
 constexpr int DIR_CHUNK = 4096;
 inline unsigned dir_chunks(int64_t max_entries) { return unsigned((max_entries + DIR_CHUNK - 1) / DIR_CHUNK); }
-// Finished requests (slots, or 0..gridDim.x-1; blockIdx.y = directory chunk): statistics of every tile.  With ring != nullptr
-// the tiles are then released (state cleared, index appended to the free ring at tail + *returned).
+// Finished requests (slots, or 0..gridDim.x-1; blockIdx.y = directory chunk): statistics of every tile.
+// Releasing the tiles is a separate launch (k_tile_release), since the statistics read neighbouring tiles.
 static __global__ void __launch_bounds__(256) k_tile_finish(const FloodCtl *__restrict__ ctl, const uint32_t *__restrict__ slots,
-                                                            const int32_t *__restrict__ dir, Tiles T, FloodStat *__restrict__ st,
-                                                            uint32_t *__restrict__ ring, uint32_t cap, uint32_t tail, uint32_t *__restrict__ returned) {
+                                                            const int32_t *__restrict__ dir, Tiles T, FloodStat *__restrict__ st) {
     const uint32_t r = slots ? slots[blockIdx.x] : blockIdx.x;
     const FloodCtl c = ctl[r];
     const int lane = threadIdx.x & 31;
@@ -437,8 +486,28 @@ static __global__ void __launch_bounds__(256) k_tile_finish(const FloodCtl *__re
             const int32_t t = __shfl_sync(0xffffffffu, d, l);
             const int64_t te = base + l;
             tile_stats(c, dir, T, t, int(te % c.tpr), int(te / c.tpr), st[r]);
-            if (ring && lane == 0) {
-                T.state[t] = 0; T.done[t] = 0;
+        }
+    }
+}
+// Release the tiles of finished requests (after k_tile_finish): zero them, append them to the free ring.
+static __global__ void __launch_bounds__(256) k_tile_release(const FloodCtl *__restrict__ ctl, const uint32_t *__restrict__ slots,
+                                                             const int32_t *__restrict__ dir, Tiles T, uint32_t *__restrict__ ring,
+                                                             uint32_t cap, uint32_t tail, uint32_t *__restrict__ returned) {
+    const FloodCtl c = ctl[slots[blockIdx.x]];
+    const int lane = threadIdx.x & 31;
+    const int64_t entries = min(int64_t(c.tpr) * c.tpr, int64_t(blockIdx.y + 1) * DIR_CHUNK);
+    for (int64_t base = int64_t(blockIdx.y) * DIR_CHUNK + (threadIdx.x & ~31); base < entries; base += blockDim.x) {
+        const int64_t e = base + lane;
+        const int32_t d = e < entries ? __ldcg(dir + c.dir_off + e) : -1;
+        uint32_t m = __ballot_sync(0xffffffffu, d >= 0);
+        while (m) {
+            const int l = __ffs(m) - 1;
+            m &= m - 1;
+            const int32_t t = __shfl_sync(0xffffffffu, d, l);
+            uint64_t *tb = T.bits + size_t(t) * TILE_U64;
+            for (int k = lane; k < TILE_U64; k += 32) tb[k] = 0;
+            if (lane == 0) {
+                T.emask[t] = 0; T.qmask[t] = 0; T.mark[t] = 0;
                 ring[(tail + atomicAdd(returned, 1u)) % cap] = uint32_t(t);
             }
         }
@@ -496,45 +565,47 @@ static __global__ void __launch_bounds__(256) k_cells(const FloodCtl *__restrict
 namespace dsg {
 namespace flood {
 // ---------------------------------------------------------------- host side shared by batch and service
-// Tile pool with its round queues (each queue can hold every tile: a tile enters a queue at most once per
-// round, by the directory claim or the connect mark).
+// Tile pool with its round queues (a tile enters the connect queue at most once per round, through its mark,
+// and each sub-block enters an evaluation queue at most once, through its tile's request mask).
 struct TilePool {
     Tiles T{};
     uint32_t cap = 0;
     uint32_t *n_list[2] = {nullptr, nullptr}, *w_list[2] = {nullptr, nullptr};
-    static constexpr size_t kBytesPerTile = TILE_U64 * 8 + 5 * 4 + 4 * 4;
+    static constexpr size_t kBytesPerTile = TILE_U64 * 8 + 5 * 4 + 2 * 4 + 2 * 16 * 4;
     void release() {
-        cudaFree(T.bits); cudaFree(T.owner); cudaFree(T.pos); cudaFree(T.state); cudaFree(T.done); cudaFree(T.mark);
+        cudaFree(T.bits); cudaFree(T.owner); cudaFree(T.pos); cudaFree(T.emask); cudaFree(T.qmask); cudaFree(T.mark);
         for (int k = 0; k < 2; k++) { cudaFree(n_list[k]); cudaFree(w_list[k]); n_list[k] = w_list[k] = nullptr; }
         T = Tiles{}; cap = 0;
     }
     void allocate(uint32_t tiles) {
         release();
         DSG_CU(cudaMalloc(&T.bits, size_t(tiles) * TILE_U64 * 8));
-        uint32_t **meta[5] = {&T.owner, &T.pos, &T.state, &T.done, &T.mark};
+        DSG_CU(cudaMemset(T.bits, 0, size_t(tiles) * TILE_U64 * 8));
+        uint32_t **meta[5] = {&T.owner, &T.pos, &T.emask, &T.qmask, &T.mark};
         for (auto m : meta) DSG_CU(cudaMalloc(m, size_t(tiles) * 4));
-        for (uint32_t *m : {T.state, T.done, T.mark}) DSG_CU(cudaMemset(m, 0, size_t(tiles) * 4));
+        for (uint32_t *m : {T.emask, T.qmask, T.mark}) DSG_CU(cudaMemset(m, 0, size_t(tiles) * 4));
         for (int k = 0; k < 2; k++) {
-            DSG_CU(cudaMalloc(&n_list[k], size_t(tiles) * 4));
+            DSG_CU(cudaMalloc(&n_list[k], size_t(tiles) * 16 * 4));
             DSG_CU(cudaMalloc(&w_list[k], size_t(tiles) * 4));
         }
         cap = tiles;
     }
-    // state, done and mark of tiles [0, used) back to zero (batch reuse of a bump-allocated pool)
+    // tiles [0, used) back to zero (batch reuse of a bump-allocated pool)
     void reset(uint32_t used, cudaStream_t st) {
         used = std::min(used, cap);
         if (!used) return;
-        for (uint32_t *m : {T.state, T.done, T.mark}) DSG_CU(cudaMemsetAsync(m, 0, size_t(used) * 4, st));
+        DSG_CU(cudaMemsetAsync(T.bits, 0, size_t(used) * TILE_U64 * 8, st));
+        for (uint32_t *m : {T.emask, T.qmask, T.mark}) DSG_CU(cudaMemsetAsync(m, 0, size_t(used) * 4, st));
     }
 };
-// Launch one round: evaluate the tiles claimed last round, then connect.  cnt[0..2] are the rotating
-// claim-queue counters, cnt[3..5] the connect-queue ones, cnt[6..8] the evaluation work counters.
-inline void launch_round(const TilePool &p, uint32_t round, uint32_t *cnt, uint32_t *active, uint32_t *err, const FloodCtl *ctl,
-                         const SeedNoise *noise, int32_t *dir, FloodStat *st, const TileAlloc &ta, int grid_eval, int grid_conn,
-                         cudaStream_t s) {
+// Launch one round: evaluate the sub-blocks requested last round, then connect.  cnt[0..2] are the rotating
+// evaluation-queue counters, cnt[3..5] the connect-queue ones, cnt[6..8] the evaluation work counters.
+inline void launch_round(const TilePool &p, uint32_t round, uint32_t *cnt, uint32_t *active, uint32_t *err, unsigned long long *evaluated,
+                         const FloodCtl *ctl, const SeedNoise *noise, int32_t *dir, FloodStat *st, const TileAlloc &ta, int grid_eval,
+                         int grid_conn, cudaStream_t s) {
     const Round q{round, p.n_list[round & 1], cnt + round % 3, p.w_list[round & 1], cnt + 3 + round % 3,
                   p.n_list[(round + 1) & 1], cnt + (round + 1) % 3, p.w_list[(round + 1) & 1], cnt + 3 + (round + 1) % 3,
-                  cnt + 6 + round % 3, cnt + (round + 2) % 3, cnt + 3 + (round + 2) % 3, cnt + 6 + (round + 2) % 3, active, err};
+                  cnt + 6 + round % 3, cnt + (round + 2) % 3, cnt + 3 + (round + 2) % 3, cnt + 6 + (round + 2) % 3, active, err, evaluated};
     k_tile_eval<<<grid_eval, EVAL_THREADS, 0, s>>>(ctl, noise, world_dev(), p.T, q);
     k_tile_connect<<<grid_conn, 256, 0, s>>>(ctl, dir, p.T, ta, st, q);
 }

@@ -48,6 +48,7 @@ struct Service {
     TilePool pool;
     uint32_t *d_ring = nullptr; uint32_t head = 0, avail = 0;
     uint32_t *d_ctr = nullptr, *h_ctr = nullptr;               // [0] taken, [1] returned, [2..10] round counters (launch_round), [11] error flags
+    unsigned long long *d_evals = nullptr;                     // sub-blocks evaluated since open
     uint32_t *d_slots = nullptr; uint64_t *d_seeds = nullptr;
     int grid_eval = 0, grid_conn = 0;
     int64_t dir_max = 0;                                       // largest directory of an admitted request
@@ -125,7 +126,7 @@ void engine_loop(Service &g) {
                 DSG_CU(cudaStreamSynchronize(st));
             }
             for (uint32_t k = 0; k < K; k++, round++)
-                launch_round(g.pool, round, g.d_ctr + 2, g.d_active, g.d_ctr + 11, g.d_ctl, g.d_noise, g.d_dir, g.d_stat, ta,
+                launch_round(g.pool, round, g.d_ctr + 2, g.d_active, g.d_ctr + 11, g.d_evals, g.d_ctl, g.d_noise, g.d_dir, g.d_stat, ta,
                              g.grid_eval, g.grid_conn, st);
             DSG_CU(cudaGetLastError());
             DSG_CU(cudaMemcpyAsync(g.h_active, g.d_active, size_t(S) * 4, cudaMemcpyDeviceToHost, st));
@@ -145,8 +146,9 @@ void engine_loop(Service &g) {
             if (!fin.empty()) {
                 DSG_CU(cudaMemcpyAsync(g.d_slots, fin.data(), fin.size() * 4, cudaMemcpyHostToDevice, st));
                 // statistics, then release; the returned counter continues from the tiles lost in directory races
-                k_tile_finish<<<dim3(unsigned(fin.size()), dir_chunks(g.dir_max)), 256, 0, st>>>(g.d_ctl, g.d_slots, g.d_dir, g.pool.T, g.d_stat,
-                                                                                                  g.d_ring, cap, (g.head + g.avail) % cap, g.d_ctr + 1);
+                const dim3 grid(unsigned(fin.size()), dir_chunks(g.dir_max));
+                k_tile_finish<<<grid, 256, 0, st>>>(g.d_ctl, g.d_slots, g.d_dir, g.pool.T, g.d_stat);
+                k_tile_release<<<grid, 256, 0, st>>>(g.d_ctl, g.d_slots, g.d_dir, g.pool.T, g.d_ring, cap, (g.head + g.avail) % cap, g.d_ctr + 1);
                 DSG_CU(cudaGetLastError());
                 for (size_t k = 0; k < fin.size(); k++) DSG_CU(cudaMemcpyAsync(&fs[k], g.d_stat + fin[k], sizeof(FloodStat), cudaMemcpyDeviceToHost, st));
                 DSG_CU(cudaMemcpyAsync(g.h_ctr + 1, g.d_ctr + 1, 4, cudaMemcpyDeviceToHost, st));
@@ -228,6 +230,8 @@ extern "C" int dsg_service_open(const dsg_service_cfg *cfg_in) {
         DSG_CU(cudaMalloc(&g.d_ctr, 16 * 4));
         DSG_CU(cudaMemset(g.d_ctr, 0, 16 * 4));
         DSG_CU(cudaMallocHost(&g.h_ctr, 16 * 4));
+        DSG_CU(cudaMalloc(&g.d_evals, 8));
+        DSG_CU(cudaMemset(g.d_evals, 0, 8));
         DSG_CU(cudaDeviceSynchronize());
         round_grids(g.grid_eval, g.grid_conn);
         g.slots.assign(S, Service::Slot{});
@@ -313,7 +317,7 @@ extern "C" int dsg_service_close(void) {
         cudaStreamSynchronize(g.st);
         cudaFree(g.d_ctl); cudaFree(g.d_stat); cudaFree(g.d_noise); cudaFree(g.d_noise_stage); cudaFree(g.d_active); cudaFreeHost(g.h_active);
         cudaFree(g.d_slots); cudaFree(g.d_seeds); cudaFree(g.d_dir); cudaFree(g.d_ring); cudaFree(g.d_ctr);
-        cudaFreeHost(g.h_ctr);
+        cudaFreeHost(g.h_ctr); cudaFree(g.d_evals);
         g.pool.release();
         cudaStreamDestroy(g.st);
         g.results.clear(); g.pending.clear(); g.slots.clear(); g.dir_free.clear();

@@ -117,10 +117,10 @@ def flood_batch(reqs):
 
 
 def flood_last_stats():
-    """{rounds, tiles, touched} of the last flood batch: tile rounds run, 64x64 tiles evaluated, cells touched."""
+    """{rounds, blocks, touched} of the last flood batch: rounds run, 16x16-cell sub-blocks evaluated, cells touched."""
     st = (C.c_uint64 * 3)()
     _ck(lib.dsg_flood_last_stats(st), "dsg_flood_last_stats")
-    return {"rounds": int(st[0]), "tiles": int(st[1]), "touched": int(st[2])}
+    return {"rounds": int(st[0]), "blocks": int(st[1]), "touched": int(st[2])}
 
 
 def flood(seed, qx, qz, step, half, conn8=False, pred=PRED_DESERT, pcut=0.35):

@@ -81,9 +81,11 @@ struct Search {
     std::mutex mu;                                 // output files, best, stderr lines
     double best = 0;
     std::atomic<uint64_t> done{0}, passed{0}, scanned{0}, nsites{0}, nhot{0}, nbig{0};
-    double t_tab = 0, t_scan = 0, t_site = 0, t_proxy = 0, t_hot = 0, t_gpu = 0;
+    std::atomic<uint64_t> pre_work[3] = {0, 0, 0};   // pre-flood rounds, sub-blocks, touched cells
+    // stage times summed over the worker threads (core-seconds, as in the reference's progress line)
+    std::atomic<double> t_tab{0}, t_scan{0}, t_site{0}, t_proxy{0}, t_hot{0}, t_gpu{0}, t_exact{0}, t_pre{0}, t_wave{0}, t_hq{0};
     Clock::time_point begin = Clock::now(), last = begin;
-    int gscan_checks = 0;
+    std::atomic<int> gscan_checks{0};
     std::vector<float> kT, kC; int rT = 0, rC = 0;
     float prob[1600];
 
@@ -144,8 +146,7 @@ void Search::process(const std::vector<uint64_t> &seeds) {
             if (fresh) cand.push_back({r->s, r->t, r->c, r->e, r->x, r->z});
             else if (r->s > cand[it->second].s) cand[it->second] = {r->s, r->t, r->c, r->e, r->x, r->z};
         }
-        if (gscan_checks > 0) {                             // gscancheck: the CPU path side by side (:292-296)
-            gscan_checks--;
+        if (gscan_checks.fetch_sub(1) > 0) {                // gscancheck: the CPU path side by side (:292-296)
             std::vector<float> tab[6];
             for (int k = 0; k < 6; k++) { hostcheck::tabulate(tin[6 * s + k], tab[k]); hostcheck::blur(tab[k], k < 2 ? kT : kC, k < 2 ? rT : rC); }
             const float cmaxta = *std::max_element(tab[0].begin(), tab[0].end()), cmaxtb = *std::max_element(tab[1].begin(), tab[1].end());
@@ -172,12 +173,14 @@ void Search::process(const std::vector<uint64_t> &seeds) {
     std::vector<Zone> zones;
     {
         // hottest of 7x7 points at 256-quart spacing around every site (first strict maximum in dz, dx order)
+        const auto tq0 = Clock::now();
         std::vector<int32_t> xz; std::vector<uint32_t> ps;
         for (size_t s = 0; s < n; s++)
             for (const Site &st : sites[s])
                 for (int dz = -3; dz <= 3; dz++) for (int dx = -3; dx <= 3; dx++) { xz.push_back(st.x + dx * 256); xz.push_back(st.z + dz * 256); ps.push_back(uint32_t(s)); }
         std::vector<double> tv(ps.size());
         if (!ps.empty()) ck(dsg_query_batch(seeds.data(), uint32_t(n), ps.data(), 0, xz.data(), uint32_t(ps.size()), tv.data()), "hot-zone points");
+        t_hq += std::chrono::duration<double>(Clock::now() - tq0).count();
         struct Hot { size_t s, rank; int hx, hz; double bt; };
         std::vector<Hot> hot;
         size_t k = 0;
@@ -189,61 +192,110 @@ void Search::process(const std::vector<uint64_t> &seeds) {
                 hot.push_back(h);
             }
         nsites += hot.size();
-        // speculative step-256 and step-128 hot floods of every site whose hottest point reaches 0.55
-        std::vector<dsg_flood_req> q256; std::vector<size_t> q256_of;
-        for (size_t h = 0; h < hot.size(); h++)
-            if (hot[h].bt >= 0.55 && P.hot_pre > 0) { q256.push_back({seeds[hot[h].s], hot[h].hx, hot[h].hz, 256, 32000 / 256, 0, DSG_PRED_HOT, 0.f, 0}); q256_of.push_back(h); }
+        // The reference walks each seed's sites in rank order and floods a site's hot zone only when its
+        // hottest point is not yet covered by an earlier flood of the same seed (dsearch_desert.cpp:326-366).
+        // Each flood a seed uses is kept as a bitmap of its cells, against which later sites test their key.
+        struct Cover { int64_t x0, z0; int step, nx, nz; std::vector<uint64_t> bits; };   // cells over their bounding box
+        std::vector<std::vector<Cover>> covers(n);
+        auto add_cover = [&](size_t s, const dsg_flood_req &q, const int32_t *cells, uint64_t nc) {
+            if (!nc) return;
+            int32_t xmin = cells[0], xmax = cells[0], zmin = cells[1], zmax = cells[1];
+            for (uint64_t k2 = 1; k2 < nc; k2++) {
+                xmin = std::min(xmin, cells[2 * k2]); xmax = std::max(xmax, cells[2 * k2]);
+                zmin = std::min(zmin, cells[2 * k2 + 1]); zmax = std::max(zmax, cells[2 * k2 + 1]);
+            }
+            Cover c{xmin, zmin, q.step, (xmax - xmin) / q.step + 1, (zmax - zmin) / q.step + 1, {}};
+            c.bits.assign((size_t(c.nx) * c.nz + 63) / 64, 0);
+            for (uint64_t k2 = 0; k2 < nc; k2++) {
+                const size_t b = size_t((cells[2 * k2 + 1] - zmin) / q.step) * c.nx + size_t((cells[2 * k2] - xmin) / q.step);
+                c.bits[b >> 6] |= 1ull << (b & 63);
+            }
+            covers[s].push_back(std::move(c));
+        };
+        // hotcovered.count(hotkey(hx, hz)): a step-128 flood covers the key of each of its cells, a step-256
+        // pre-flood the keys of its cells offset by 0 or 128 on each axis (dsearch_desert.cpp:341-345,357-361);
+        // the key's 128-quart block holds at most one lattice point of either flood per offset.
+        auto covered = [&](size_t s, int hx, int hz) {
+            const int64_t bx = int64_t((hx + 8000000) >> 7) * 128 - 8000000, bz = int64_t((hz + 8000000) >> 7) * 128 - 8000000;
+            for (const Cover &c : covers[s]) {
+                const int offs = c.step == 256 ? 2 : 1;
+                for (int dz = 0; dz < offs; dz++) for (int dx = 0; dx < offs; dx++) {
+                    auto index = [&](int64_t lo, int64_t o, int n2, int64_t &i) {    // lattice index with point in [lo, lo + 127]
+                        const int64_t d = lo - o;
+                        i = d >= 0 ? (d + c.step - 1) / c.step : -((-d) / c.step);
+                        return o + i * c.step <= lo + 127 && i >= 0 && i < n2;
+                    };
+                    int64_t i, j;
+                    if (!index(bx - dx * 128, c.x0, c.nx, i) || !index(bz - dz * 128, c.z0, c.nz, j)) continue;
+                    const size_t b = size_t(j) * c.nx + size_t(i);
+                    if ((c.bits[b >> 6] >> (b & 63)) & 1) return true;
+                }
+            }
+            return false;
+        };
+        // cells land in a buffer kept across batches (grown, never value-initialised again); an overflow reruns
+        // the batch with the exact size the library reported
         auto flood_cells = [&](const std::vector<dsg_flood_req> &q, std::vector<dsg_area> &a, std::vector<uint64_t> &off, std::vector<int32_t> &cells) {
             a.resize(q.size()); off.assign(q.size() + 1, 0);
-            uint64_t capc = std::max<uint64_t>(1 << 20, q.size() * 4096);
+            if (q.empty()) return;
+            if (cells.size() < 2 * q.size() * 256) cells.resize(2 * q.size() * 256);
             for (;;) {
-                cells.resize(2 * capc);
-                const int rc = q.empty() ? DSG_OK : dsg_flood_batch_cells(q.data(), uint32_t(q.size()), a.data(), off.data(), cells.data(), capc);
+                const int rc = dsg_flood_batch_cells(q.data(), uint32_t(q.size()), a.data(), off.data(), cells.data(), cells.size() / 2);
                 ck(rc, "hot-zone flood");
                 if (rc == DSG_OK) return;
-                capc = off.back() + 1;
+                cells.resize(2 * (off.back() + 1));
             }
         };
+        // Speculatively, all at once: the step-256 pre-flood of every hot site, then the step-128 flood of every
+        // site whose pre-flood is large.  Each seed then replays its sites in rank order against the coverage
+        // bitmaps and uses only the floods of the sites it does not skip, so the result is the reference's;
+        // sites skipped that way are rare (their floods are the only work wasted).
         const auto th0 = Clock::now();
-        std::vector<dsg_area> a256; std::vector<uint64_t> o256; std::vector<int32_t> c256;
-        flood_cells(q256, a256, o256, c256);
-        std::vector<int> big(hot.size(), P.hot_pre > 0 ? 0 : 1);
-        std::vector<long> idx256(hot.size(), -1);
-        for (size_t k2 = 0; k2 < q256.size(); k2++) {
-            idx256[q256_of[k2]] = long(k2);
-            if (a256[k2].cells * 256.0 * 256 * 16 / 1e6 >= P.hot_pre * P.hot_min) big[q256_of[k2]] = 1;
-        }
-        std::vector<dsg_flood_req> q128; std::vector<long> idx128(hot.size(), -1);
+        const bool pre = P.hot_pre > 0;
+        std::vector<long> f1_of(hot.size(), -1), f2_of(hot.size(), -1);
+        std::vector<dsg_flood_req> q1, q2;
         for (size_t h = 0; h < hot.size(); h++)
-            if (hot[h].bt >= 0.55 && big[h]) { idx128[h] = long(q128.size()); q128.push_back({seeds[hot[h].s], hot[h].hx, hot[h].hz, 128, 32000 / 128, 0, DSG_PRED_HOT, 0.f, 0}); }
-        std::vector<dsg_area> a128; std::vector<uint64_t> o128; std::vector<int32_t> c128;
-        flood_cells(q128, a128, o128, c128);
-        t_hot += std::chrono::duration<double>(Clock::now() - th0).count();
-        // replay the reference's sequential site loop per seed
-        size_t h = 0;
-        for (size_t s = 0; s < n; s++) {
-            std::unordered_set<uint64_t> hotcovered;
-            for (size_t r = 0; r < sites[s].size(); r++, h++) {
+            if (hot[h].bt >= 0.55) {
+                const int step = pre ? 256 : 128;
+                f1_of[h] = long(q1.size());
+                q1.push_back({seeds[hot[h].s], hot[h].hx, hot[h].hz, step, 32000 / step, 0, DSG_PRED_HOT, 0.f, 0});
+            }
+        std::vector<dsg_area> a1, a2; std::vector<uint64_t> o1, o2;
+        static thread_local std::vector<int32_t> cellbuf[2];   // cell lists (x, z), reused across this worker's batches
+        std::vector<int32_t> &c1 = cellbuf[0], &c2 = cellbuf[1];
+        flood_cells(q1, a1, o1, c1);
+        if (!q1.empty()) { uint64_t w[3]; ck(dsg_flood_last_stats(w), "flood stats"); for (int k = 0; k < 3; k++) pre_work[k] += w[k]; }
+        t_pre += std::chrono::duration<double>(Clock::now() - th0).count();
+        auto small = [&](long k) { return pre && a1[k].cells * 256.0 * 256 * 16 / 1e6 < P.hot_pre * P.hot_min; };
+        if (pre) {
+            for (size_t h = 0; h < hot.size(); h++)
+                if (f1_of[h] >= 0 && !small(f1_of[h])) { f2_of[h] = long(q2.size()); q2.push_back({seeds[hot[h].s], hot[h].hx, hot[h].hz, 128, 32000 / 128, 0, DSG_PRED_HOT, 0.f, 0}); }
+            const auto tw0 = Clock::now();
+            flood_cells(q2, a2, o2, c2);
+            t_wave += std::chrono::duration<double>(Clock::now() - tw0).count();
+        }
+        for (size_t s2 = 0, h = 0; s2 < n; s2++)
+            for (size_t r = 0; r < sites[s2].size(); r++, h++) {
                 const Hot &ht = hot[h];
-                if (ht.bt < 0.55 || hotcovered.count(hotkey(ht.hx, ht.hz))) continue;
-                if (P.hot_pre > 0 && !big[h]) {                 // small pre-flood: cover its cells (4 sub-keys each)
-                    const long k2 = idx256[h];
-                    for (uint64_t c = o256[k2]; c < o256[k2 + 1]; c++)
-                        for (int d = 0; d < 4; d++) hotcovered.insert(hotkey(c256[2 * c] + (d & 1) * 128, c256[2 * c + 1] + (d >> 1) * 128));
+                if (ht.bt < 0.55 || covered(s2, ht.hx, ht.hz)) continue;
+                const long k1 = f1_of[h];
+                if (small(k1)) {                                                   // small zone: cover, done
+                    add_cover(s2, q1[k1], c1.data() + 2 * o1[k1], o1[k1 + 1] - o1[k1]);
                     nhot++;
                     continue;
                 }
-                const long k2 = idx128[h];
-                const dsg_area &hz = a128[k2];
-                const double hot_area = hz.cells * 128.0 * 128 * 16 / 1e6;
-                for (uint64_t c = o128[k2]; c < o128[k2 + 1]; c++) hotcovered.insert(hotkey(c128[2 * c], c128[2 * c + 1]));
+                const bool use2 = pre;
+                const long k2 = use2 ? f2_of[h] : k1;
+                const dsg_area &hz = use2 ? a2[k2] : a1[k2];
+                add_cover(s2, use2 ? q2[k2] : q1[k2], (use2 ? c2 : c1).data() + 2 * (use2 ? o2 : o1)[k2], (use2 ? o2 : o1)[k2 + 1] - (use2 ? o2 : o1)[k2]);
                 nhot++;
+                const double hot_area = hz.cells * 128.0 * 128 * 16 / 1e6;
                 if (hot_area < P.hot_min) continue;
                 nbig++;
                 const int x0 = int(std::floor((hz.minx - 128) / 32.0)) * 32, z0 = int(std::floor((hz.minz - 128) / 32.0)) * 32;
-                zones.push_back({s, r, hot_area, x0, z0, (hz.maxx + 128 - x0) / 32 + 1, (hz.maxz + 128 - z0) / 32 + 1});
+                zones.push_back({s2, r, hot_area, x0, z0, (hz.maxx + 128 - x0) / 32 + 1, (hz.maxz + 128 - z0) / 32 + 1});
             }
-        }
+        t_hot += std::chrono::duration<double>(Clock::now() - th0).count();
     }
     // ---------------- S4: proxy bitmaps + components (dsearch_desert.cpp:425-492)
     std::vector<std::vector<Eval>> ev(n);
@@ -311,6 +363,7 @@ void Search::process(const std::vector<uint64_t> &seeds) {
     }
     for (auto &e : ev) std::sort(e.begin(), e.end(), [](auto &a, auto &b) { return a.proxy > b.proxy; });
     t_proxy += std::chrono::duration<double>(Clock::now() - tp0).count();
+    const auto te0 = Clock::now();
     // ---------------- S5: exact floods (dsearch_desert.cpp:498-533)
     struct Try { size_t s, k2, t; int sx, sz; int bx = 0, bz = 0; bool found = false; };
     std::vector<Try> tries;
@@ -365,6 +418,7 @@ void Search::process(const std::vector<uint64_t> &seeds) {
         }
     }
     const auto t3 = Clock::now();
+    t_exact += std::chrono::duration<double>(t3 - te0).count();
     // ---------------- results (dsearch_desert.cpp:524-556)
     std::lock_guard<std::mutex> g(mu);
     for (size_t s = 0; s < n; s++) {
@@ -398,7 +452,7 @@ void Search::process(const std::vector<uint64_t> &seeds) {
         last = now; fflush(out); fflush(sout);
         fprintf(stderr, "%llu seeds, %llu passed, %llu scanned, %llu sites; %.2f passed/s; core-s tables %.0f scan %.0f sites %.0f (proxy %.0f hot %.0f gpu %.0f); hot zones %llu, big %llu\n",
                 (unsigned long long)done.load(), (unsigned long long)passed.load(), (unsigned long long)scanned.load(), (unsigned long long)nsites.load(),
-                passed.load() / std::chrono::duration<double>(now - begin).count(), t_tab, t_scan, t_site, t_proxy, t_hot, t_gpu,
+                passed.load() / std::chrono::duration<double>(now - begin).count(), t_tab.load(), t_scan.load(), t_site.load(), t_proxy.load(), t_hot.load(), t_gpu.load(),
                 (unsigned long long)nhot.load(), (unsigned long long)nbig.load());
     }
 }
@@ -489,23 +543,31 @@ int main(int argc, char **argv) {
             std::lock_guard<std::mutex> l(qmu); qdone = true; qcv.notify_all();
         });
     }
-    // ---- batches of seeds through the stages
-    const size_t BATCH = 256;
-    for (;;) {
-        std::vector<uint64_t> batch;
-        {
-            std::unique_lock<std::mutex> l(qmu);
-            qcv.wait_for(l, std::chrono::milliseconds(200), [&] { return q.size() >= BATCH || qdone || interrupted; });
-            while (!q.empty() && batch.size() < BATCH) { batch.push_back(q.front()); q.pop_front(); }
-            qcv.notify_all();
-            if (batch.empty() && (qdone || interrupted)) break;
+    // ---- batches of seeds through the stages, on several host threads: the library serialises each kind of
+    // device call, so one worker's host work (table setup, coverage replay, labelling, output) overlaps the
+    // other workers' device stages
+    const size_t BATCH = 128;
+    const int workers = std::max(1, std::min(S.threads, 8));
+    auto work = [&] {
+        for (;;) {
+            std::vector<uint64_t> batch;
+            {
+                std::unique_lock<std::mutex> l(qmu);
+                qcv.wait_for(l, std::chrono::milliseconds(200), [&] { return q.size() >= BATCH || qdone || interrupted; });
+                while (!q.empty() && batch.size() < BATCH) { batch.push_back(q.front()); q.pop_front(); }
+                qcv.notify_all();
+                if (batch.empty() && (qdone || interrupted)) return;
+            }
+            if (batch.empty()) continue;
+            S.passed += batch.size();
+            if (P.from_stdin) S.done += batch.size();
+            S.process(batch);
+            if (interrupted) return;
         }
-        if (batch.empty()) continue;
-        S.passed += batch.size();
-        if (P.from_stdin) S.done += batch.size();
-        S.process(batch);
-        if (interrupted) break;
-    }
+    };
+    std::vector<std::thread> pool;
+    for (int k = 0; k < workers; k++) pool.emplace_back(work);
+    for (auto &t : pool) t.join();
     if (source.joinable()) { if (qdone) source.join(); else source.detach(); }
     fclose(S.out); fclose(S.sout);
     const double sec = std::chrono::duration<double>(Clock::now() - S.begin).count();
@@ -513,9 +575,11 @@ int main(int argc, char **argv) {
     fprintf(m, "{\"start\":%llu,\"done\":%llu,\"passed\":%llu,\"scanned\":%llu,\"amp\":%g,\"sites\":%llu,\"seconds\":%.3f,\"threads\":%d,\"phase\":%g,\"sigma\":%g,"
                "\"wc\":%g,\"we\":%g,\"t\":%g,\"ta\":%g,\"max_sites\":%d,\"nms\":%d,\"cpu_tables\":%.3f,\"cpu_scan\":%.3f,\"cpu_sites\":%.3f}\n",
             (unsigned long long)S.start, (unsigned long long)S.done.load(), (unsigned long long)S.passed.load(), (unsigned long long)S.scanned.load(), P.amp,
-            (unsigned long long)S.nsites.load(), sec, S.threads, P.max_phase, P.sigma, P.wc, P.we, P.t, P.ta, P.max_sites, P.nms, S.t_tab, S.t_scan, S.t_site);
+            (unsigned long long)S.nsites.load(), sec, S.threads, P.max_phase, P.sigma, P.wc, P.we, P.t, P.ta, P.max_sites, P.nms, S.t_tab.load(), S.t_scan.load(), S.t_site.load());
     fclose(m);
     fprintf(stderr, "done: %llu seeds (%llu passed) in %.1fs\n", (unsigned long long)S.done.load(), (unsigned long long)S.passed.load(), sec);
+    fprintf(stderr, "stage seconds: tables %.3f scan %.3f sites %.3f (hot points %.3f; hot-zone floods %.3f: pre-floods %.3f [rounds %llu sub-blocks %llu touched %llu], %llu floods used, step-128 floods %.3f; proxy %.3f of which kernel %.3f; exact floods %.3f)\n",
+            S.t_tab.load(), S.t_scan.load(), S.t_site.load(), S.t_hq.load(), S.t_hot.load(), S.t_pre.load(), (unsigned long long)S.pre_work[0].load(), (unsigned long long)S.pre_work[1].load(), (unsigned long long)S.pre_work[2].load(), (unsigned long long)S.nhot.load(), S.t_wave.load(), S.t_proxy.load(), S.t_gpu.load(), S.t_exact.load());
     std::fflush(nullptr);
     std::_Exit(0);
 }

@@ -185,9 +185,9 @@ int dsg_service_close(void);
 
 /* A single flood (dflood SEED X Z STEP: qx = X>>2, qz = Z>>2, half = 20000/STEP). */
 int dsg_flood(const dsg_flood_req *req, dsg_area *out);
-/* Work of the last dsg_flood / dsg_flood_batch(_cells) call in this process: {tile rounds, 64x64-cell tiles
+/* Work of the last dsg_flood / dsg_flood_batch(_cells) call in this process: {rounds, 16x16-cell sub-blocks
  * evaluated, cells touched (sum of sampled)}.  No reference counterpart (the reference's floods evaluate
- * exactly the touched cells); tiles * 4096 / touched is the speculative-evaluation overhead. */
+ * exactly the touched cells); sub-blocks * 256 / touched is the speculative-evaluation overhead. */
 int dsg_flood_last_stats(uint64_t stats[3]);
 
 #ifdef __cplusplus
