@@ -9,8 +9,10 @@
 //    and writes them horizontally blurred (the row never round-trips through HBM unblurred).
 //  * k_blur_v: one CTA per 32-row block; thread = column; a register ring holds the 15 rows the vertical
 //    blur needs, so each blurred row is read once per block.  T tables also reduce their maximum.
-//  * k_scan: one CTA per active side-A cell (TA >= ta), threads over the (tz, tx) translation pairs.
-#include "common.cuh"
+//  * k_scan: CTAs loop over the active side-A cells (TA >= ta), threads over the (tz, tx) translation pairs.
+//  * k_tabins: the table inputs of a seed (tab_setup, lowfield.hpp:14-33) from its device noise tables, for
+//    dsg_scan_seeds.
+#include "noise.cuh"
 #include <algorithm>
 #include <mutex>
 #include <vector>
@@ -111,8 +113,9 @@ __global__ void __launch_bounds__(256) k_scan(const float *__restrict__ tabs, co
         const int16_t *__restrict__ ibT, const int16_t *__restrict__ ibC, const int8_t *__restrict__ loT, const int8_t *__restrict__ hiT,
         dsg_scan_params sp, ScanConst sc, Cand *__restrict__ out, uint32_t *__restrict__ ncand, uint32_t cap) {
     const int sd = blockIdx.y;
-    if (blockIdx.x >= nact[sd]) return;
-    const int cell = act[size_t(sd) * TN * TN + blockIdx.x], j = cell >> 9, i = cell & (TN - 1);
+    const uint32_t na = nact[sd];
+    for (uint32_t a = blockIdx.x; a < na; a += gridDim.x) {
+    const int cell = act[size_t(sd) * TN * TN + a], j = cell >> 9, i = cell & (TN - 1);
     const int nt = sc.nt;
     const float *TA = tabs + size_t(sd) * 6 * TN * TN, *TB = TA + TN * TN, *CA = TB + TN * TN, *CB = CA + TN * TN,
                 *EA = CB + TN * TN, *EB = EA + TN * TN;
@@ -132,6 +135,38 @@ __global__ void __launch_bounds__(256) k_scan(const float *__restrict__ tabs, co
         const uint32_t k = atomicAdd(&ncand[sd], 1u);
         if (k < cap) out[size_t(sd) * cap + k] = {s, tv, cv, ev, i * sc.cell + (tx + sc.kmin) * sc.period, j * sc.cell + (tz + sc.kmin) * sc.period};
     }
+    }
+}
+constexpr int SCAN_BLOCKS = 512;                    // CTAs per seed of k_scan
+
+// Table inputs {TA, TB, CA, CB, EA, EB} of each seed from its noise tables, as tab_setup computes them on the
+// host (lowfield.hpp:14-33; octave 0 of each side of channels T, C, E, weight factor * amplitude).  Block =
+// (seed, table); thread x = permutation entry x, column-hash entries x of both y offsets, and corner terms
+// x and x + 256 in [px][pz][c][h] order.  The double-precision expressions are the host's, in its order.
+__global__ void __launch_bounds__(256) k_tabins(const SeedNoise *__restrict__ noise, TabIn *__restrict__ out) {
+    constexpr int CH[3] = {CH_T, CH_C, CH_E};
+    const uint32_t s = blockIdx.x / 6, k = blockIdx.x % 6;
+    const SeedNoise &S = noise[s];
+    const int ch = CH[k / 2], idx = S.off[ch] + int(k & 1) * S.cnt[ch];
+    const NOct &p = S.oct[idx];
+    const uint8_t *P = S.perm[idx];
+    TabIn &t = out[blockIdx.x];
+    const int x = threadIdx.x;
+    t.perm[x] = P[x];
+    t.col[0][x] = P[(P[x] + p.iy) & 255];
+    t.col[1][x] = P[(P[x] + p.iy + 1) & 255];
+    if (x < 2) { t.i0[x] = int(floor(x * 0.5 + p.ox)); t.k0[x] = int(floor(x * 0.5 + p.oz)); }
+    const double w = S.factor[ch] * p.amp;
+    #pragma unroll
+    for (int e = x; e < 512; e += 256) {
+        const int h = e & 15, c = (e >> 4) & 7, pz = (e >> 7) & 1, px = e >> 8;
+        const double bx = px * 0.5 + p.ox, bz = pz * 0.5 + p.oz;
+        const double fx = bx - floor(bx), fz = bz - floor(bz);
+        const double tx = fade_d(fx), tz = fade_d(fz), ty = p.vy;
+        const int dx = c & 1, dy = (c >> 1) & 1, dz = c >> 2;
+        const double wc = (dx ? tx : 1 - tx) * (dy ? ty : 1 - ty) * (dz ? tz : 1 - tz);
+        t.T[px][pz][c][h] = float(w * wc * grad_d(h, fx - dx, p.fy - dy, fz - dz));
+    }
 }
 
 // ---------------------------------------------------------------- host engine
@@ -145,6 +180,7 @@ struct State {
     TabIn *d_in = nullptr; float *d_tab = nullptr, *d_h = nullptr, *d_mx = nullptr;
     int32_t *d_act = nullptr; uint32_t *d_nact = nullptr, *d_ncand = nullptr;
     Cand *d_out = nullptr; uint32_t cap_cand = 0;
+    uint64_t *d_seeds = nullptr; SeedNoise *d_noise = nullptr;   // dsg_scan_seeds
 };
 State &S() { static State s; return s; }
 
@@ -152,7 +188,9 @@ void ensure(State &g, uint32_t seeds, uint32_t cap) {
     if (seeds <= g.cap_seeds && cap <= g.cap_cand) return;
     const uint32_t ns = std::max(seeds, g.cap_seeds), nc = std::max(cap, g.cap_cand);
     cudaFree(g.d_in); cudaFree(g.d_tab); cudaFree(g.d_h); cudaFree(g.d_mx); cudaFree(g.d_act); cudaFree(g.d_nact);
-    cudaFree(g.d_ncand); cudaFree(g.d_out);
+    cudaFree(g.d_ncand); cudaFree(g.d_out); cudaFree(g.d_seeds); cudaFree(g.d_noise);
+    DSG_CU(cudaMalloc(&g.d_seeds, size_t(ns) * 8));
+    DSG_CU(cudaMalloc(&g.d_noise, size_t(ns) * sizeof(SeedNoise)));
     DSG_CU(cudaMalloc(&g.d_in, size_t(ns) * 6 * sizeof(TabIn)));
     DSG_CU(cudaMalloc(&g.d_tab, size_t(ns) * 6 * TN * TN * 4));
     DSG_CU(cudaMalloc(&g.d_h, size_t(ns) * 6 * TN * TN * 4));
@@ -175,7 +213,7 @@ void enqueue(State &g, uint32_t S, const dsg_scan_params *sp, uint32_t cap, bool
         DSG_CU(cudaMemsetAsync(g.d_nact, 0, size_t(S) * 4, g.st));
         DSG_CU(cudaMemsetAsync(g.d_ncand, 0, size_t(S) * 4, g.st));
         k_active<<<dim3(TN * TN / 256, S), 256, 0, g.st>>>(g.d_tab, sp->ta, g.d_act, g.d_nact);
-        k_scan<<<dim3(TN * TN, S), 256, 0, g.st>>>(g.d_tab, g.d_act, g.d_nact, g.d_ibT, g.d_ibC, g.d_loT, g.d_hiT, *sp, g.sc, g.d_out, g.d_ncand, cap);
+        k_scan<<<dim3(SCAN_BLOCKS, S), 256, 0, g.st>>>(g.d_tab, g.d_act, g.d_nact, g.d_ibT, g.d_ibC, g.d_loT, g.d_hiT, *sp, g.sc, g.d_out, g.d_ncand, cap);
     }
     DSG_CU(cudaGetLastError());
 }
@@ -230,6 +268,25 @@ extern "C" int dsg_tables(const dsg_tabin *tabs, uint32_t nseeds, float *out, fl
     });
 }
 
+namespace {
+// Candidates and maxima of the S seeds just enqueued: counts first, then each seed's candidates.
+int collect(State &g, uint32_t nseeds, float *maxt, dsg_cand *out, uint32_t cap, uint32_t dcap, uint32_t *n) {
+    std::vector<uint32_t> hn(nseeds);
+    DSG_CU(cudaMemcpyAsync(hn.data(), g.d_ncand, size_t(nseeds) * 4, cudaMemcpyDeviceToHost, g.st));
+    DSG_CU(cudaMemcpyAsync(maxt, g.d_mx, size_t(nseeds) * 8, cudaMemcpyDeviceToHost, g.st));
+    DSG_CU(cudaStreamSynchronize(g.st));
+    bool over = false;
+    for (uint32_t s = 0; s < nseeds; s++) {
+        n[s] = std::min(hn[s], cap);
+        over |= hn[s] > cap;
+        if (n[s]) DSG_CU(cudaMemcpyAsync(out + size_t(s) * cap, g.d_out + size_t(s) * dcap, size_t(n[s]) * sizeof(Cand), cudaMemcpyDeviceToHost, g.st));
+    }
+    DSG_CU(cudaStreamSynchronize(g.st));
+    if (over) { set_error("dsg_scan: candidate buffer overflow"); return DSG_OVERFLOW; }
+    return DSG_OK;
+}
+}  // namespace
+
 extern "C" int dsg_scan_batch(const dsg_tabin *tabs, uint32_t nseeds, const dsg_scan_params *sp, float *maxt, dsg_cand *out, uint32_t cap,
                               uint32_t *n) {
     return guarded([&] {
@@ -241,19 +298,25 @@ extern "C" int dsg_scan_batch(const dsg_tabin *tabs, uint32_t nseeds, const dsg_
         ensure(g, nseeds, dcap);
         DSG_CU(cudaMemcpyAsync(g.d_in, tabs, size_t(nseeds) * 6 * sizeof(TabIn), cudaMemcpyHostToDevice, g.st));
         enqueue(g, nseeds, sp, dcap, true);
-        std::vector<uint32_t> hn(nseeds);
-        DSG_CU(cudaMemcpyAsync(hn.data(), g.d_ncand, size_t(nseeds) * 4, cudaMemcpyDeviceToHost, g.st));
-        DSG_CU(cudaMemcpyAsync(maxt, g.d_mx, size_t(nseeds) * 8, cudaMemcpyDeviceToHost, g.st));
-        DSG_CU(cudaStreamSynchronize(g.st));
-        bool over = false;
-        for (uint32_t s = 0; s < nseeds; s++) {
-            n[s] = std::min(hn[s], cap);
-            over |= hn[s] > cap;
-            if (n[s]) DSG_CU(cudaMemcpyAsync(out + size_t(s) * cap, g.d_out + size_t(s) * dcap, size_t(n[s]) * sizeof(Cand), cudaMemcpyDeviceToHost, g.st));
-        }
-        DSG_CU(cudaStreamSynchronize(g.st));
-        if (over) { set_error("dsg_scan: candidate buffer overflow"); return DSG_OVERFLOW; }
-        return DSG_OK;
+        return collect(g, nseeds, maxt, out, cap, dcap, n);
+    });
+}
+
+extern "C" int dsg_scan_seeds(const uint64_t *seeds, uint32_t nseeds, const dsg_scan_params *sp, float *maxt, dsg_cand *out, uint32_t cap,
+                              uint32_t *n) {
+    return guarded([&] {
+        DSG_ARG(seeds && sp && maxt && n && (cap == 0 || out), "dsg_scan_seeds: null pointer");
+        State &g = S(); std::lock_guard<std::mutex> l(g.mu);
+        DSG_ARG(g.init, "dsg_scan_seeds: dsg_scan_init has not been called");
+        if (!nseeds) return DSG_OK;
+        const uint32_t dcap = std::max<uint32_t>(cap, 1);
+        ensure(g, nseeds, dcap);
+        DSG_CU(cudaMemcpyAsync(g.d_seeds, seeds, size_t(nseeds) * 8, cudaMemcpyHostToDevice, g.st));
+        seed_noise_build(g.d_seeds, nseeds, g.d_noise, g.st);
+        k_tabins<<<6 * nseeds, 256, 0, g.st>>>(g.d_noise, g.d_in);
+        DSG_CU(cudaGetLastError());
+        enqueue(g, nseeds, sp, dcap, true);
+        return collect(g, nseeds, maxt, out, cap, dcap, n);
     });
 }
 

@@ -175,6 +175,19 @@ def scan_batch(tabins, ta=0.25, tt=0.55, wc=0.25, we=0.41, cap=1 << 18):
     return [(mx[s, 0], mx[s, 1], out[s * cap: s * cap + cnt[s]].copy()) for s in range(n)]
 
 
+def scan_seeds(seeds, ta=0.25, tt=0.55, wc=0.25, we=0.41, cap=1 << 18):
+    """scan_batch with the table inputs built on the device from the seeds."""
+    s = np.ascontiguousarray(seeds, dtype=np.uint64)
+    n = len(s)
+    sp = ScanParams(ta, tt, wc, we)
+    mx = np.empty((n, 2), dtype=np.float32); out = np.empty(n * cap, dtype=CAND_DTYPE); cnt = np.empty(n, dtype=np.uint32)
+    rc = _ck(lib.dsg_scan_seeds(ptr(s, u64p), C.c_uint32(n), C.byref(sp), ptr(mx, f32p), out.ctypes.data_as(C.c_void_p),
+                                C.c_uint32(cap), ptr(cnt, u32p)), "dsg_scan_seeds")
+    if rc != DSG_OK:
+        raise DsgError(f"dsg_scan_seeds: rc={rc}")
+    return [(mx[s2, 0], mx[s2, 1], out[s2 * cap: s2 * cap + cnt[s2]].copy()) for s2 in range(n)]
+
+
 class Zone(C.Structure):
     _fields_ = [("x0", C.c_int32), ("z0", C.c_int32), ("nx", C.c_int32), ("nz", C.c_int32)]
 

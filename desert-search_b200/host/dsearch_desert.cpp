@@ -110,23 +110,15 @@ void Search::process(const std::vector<uint64_t> &seeds) {
     const auto t0 = Clock::now();
     std::vector<std::array<double, 2>> fy(n);
     for (size_t s = 0; s < n; s++) hostcheck::phase(seeds[s], fy[s].data());
-    // ---------------- S1-S2: tables + scan (dsearch_desert.cpp:228-281)
-    std::vector<dsg_tabin> tin(6 * n);
-    {
-        std::atomic<size_t> nx(0);
-        std::vector<std::thread> pool;
-        for (int t = 0; t < std::max(1, threads); t++)
-            pool.emplace_back([&] { for (size_t s; (s = nx++) < n;) hostcheck::seed_tabins(seeds[s], &tin[6 * s]); });
-        for (auto &t : pool) t.join();
-    }
+    // ---------------- S1-S2: tables + scan (dsearch_desert.cpp:228-281); the table inputs are built on the device
     const dsg_scan_params sp{float(P.ta), float(P.t), float(P.wc), float(P.we)};
     uint32_t cap = 1u << 16;
     std::vector<float> maxt(2 * n);
-    std::vector<dsg_cand> raw;
+    static thread_local std::vector<dsg_cand> raw;            // kept across this worker's batches
     std::vector<uint32_t> nraw(n);
     for (;;) {
-        raw.resize(size_t(cap) * n);
-        const int rc = dsg_scan_batch(tin.data(), uint32_t(n), &sp, maxt.data(), raw.data(), cap, nraw.data());
+        if (raw.size() < size_t(cap) * n) raw.resize(size_t(cap) * n);
+        const int rc = dsg_scan_seeds(seeds.data(), uint32_t(n), &sp, maxt.data(), raw.data(), cap, nraw.data());
         ck(rc, "gscan");
         if (rc == DSG_OK) break;
         cap *= 4;                                   // the reference falls back to the CPU here; the GPU simply retries larger
@@ -148,7 +140,9 @@ void Search::process(const std::vector<uint64_t> &seeds) {
         }
         if (gscan_checks.fetch_sub(1) > 0) {                // gscancheck: the CPU path side by side (:292-296)
             std::vector<float> tab[6];
-            for (int k = 0; k < 6; k++) { hostcheck::tabulate(tin[6 * s + k], tab[k]); hostcheck::blur(tab[k], k < 2 ? kT : kC, k < 2 ? rT : rC); }
+            dsg_tabin tin[6];
+            hostcheck::seed_tabins(seed, tin);
+            for (int k = 0; k < 6; k++) { hostcheck::tabulate(tin[k], tab[k]); hostcheck::blur(tab[k], k < 2 ? kT : kC, k < 2 ? rT : rC); }
             const float cmaxta = *std::max_element(tab[0].begin(), tab[0].end()), cmaxtb = *std::max_element(tab[1].begin(), tab[1].end());
             const std::vector<dsg_cand> cc = hostcheck::scan_buckets(tab, P.ta, P.t, P.wc, P.we, P.nms);
             long miss = 0;
@@ -501,6 +495,7 @@ int main(int argc, char **argv) {
         hostcheck::scan_tmaps(&TMT.ib[0][0], TMT.lo, TMT.hi, &TMC.ib[0][0]);
     }
     ck(dsg_proxy_table(S.prob), "proxy table");
+    const double t_ready = std::chrono::duration<double>(Clock::now() - S.begin).count();
     S.gscan_checks = P.gscancheck;
     // ---- seed source: GPU gate thread, stdin reader, or the enumerated range through the GPU gate
     std::mutex qmu; std::condition_variable qcv; std::deque<uint64_t> q; bool qdone = false;
@@ -511,10 +506,12 @@ int main(int argc, char **argv) {
         qcv.notify_all();
     };
     std::thread source;
+    std::atomic<double> gate_end{0};
     if (P.from_stdin && !P.gate) {
         source = std::thread([&] {
             char line[256];
             while (!interrupted && fgets(line, sizeof line, stdin)) push(std::strtoull(line, nullptr, 10));
+            gate_end = std::chrono::duration<double>(Clock::now() - S.begin).count();
             std::lock_guard<std::mutex> l(qmu); qdone = true; qcv.notify_all();
         });
     } else {
@@ -540,6 +537,7 @@ int main(int argc, char **argv) {
                         (base + nb) / sec, tot[3] / sec);
                 for (uint32_t i = 0; i < nn && !interrupted; i++) push(sd[i]);
             }
+            gate_end = std::chrono::duration<double>(Clock::now() - S.begin).count();
             std::lock_guard<std::mutex> l(qmu); qdone = true; qcv.notify_all();
         });
     }
@@ -578,6 +576,7 @@ int main(int argc, char **argv) {
             (unsigned long long)S.nsites.load(), sec, S.threads, P.max_phase, P.sigma, P.wc, P.we, P.t, P.ta, P.max_sites, P.nms, S.t_tab.load(), S.t_scan.load(), S.t_site.load());
     fclose(m);
     fprintf(stderr, "done: %llu seeds (%llu passed) in %.1fs\n", (unsigned long long)S.done.load(), (unsigned long long)S.passed.load(), sec);
+    fprintf(stderr, "startup %.3f s, gate done at %.3f s\n", t_ready, gate_end.load());
     fprintf(stderr, "stage seconds: tables %.3f scan %.3f sites %.3f (hot points %.3f; hot-zone floods %.3f: pre-floods %.3f [rounds %llu sub-blocks %llu touched %llu], %llu floods used, step-128 floods %.3f; proxy %.3f of which kernel %.3f; exact floods %.3f)\n",
             S.t_tab.load(), S.t_scan.load(), S.t_site.load(), S.t_hq.load(), S.t_hot.load(), S.t_pre.load(), (unsigned long long)S.pre_work[0].load(), (unsigned long long)S.pre_work[1].load(), (unsigned long long)S.pre_work[2].load(), (unsigned long long)S.nhot.load(), S.t_wave.load(), S.t_proxy.load(), S.t_gpu.load(), S.t_exact.load());
     std::fflush(nullptr);

@@ -98,6 +98,11 @@ int dsg_scan(const dsg_tabin tabs[6], const dsg_scan_params *sp, float *maxta, f
  * (src/gpu/gproxy.cu:221-281), made explicit. */
 int dsg_scan_batch(const dsg_tabin *tabs, uint32_t nseeds, const dsg_scan_params *sp, float *maxt, dsg_cand *out,
                    uint32_t cap, uint32_t *n_out);
+/* dsg_scan_batch from the seeds alone: the six table inputs of each seed are computed on the device (the
+ * host's tab_setup, src/lowfield.hpp:14-33, on octave 0 of T, C and E), identical to host-built ones.  No
+ * reference counterpart (the reference builds them on the host, dsearch_desert.cpp:232-238). */
+int dsg_scan_seeds(const uint64_t *seeds, uint32_t nseeds, const dsg_scan_params *sp, float *maxt, dsg_cand *out,
+                   uint32_t cap, uint32_t *n);
 /* The six blurred tables of n seeds (6*512*512 floats each, row-major, z outer) and maxta/maxtb; the
  * gscancheck view (src/dsearch_desert.cpp:292-296). */
 int dsg_tables(const dsg_tabin *tabs, uint32_t nseeds, float *out, float *maxt);

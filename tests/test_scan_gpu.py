@@ -52,6 +52,20 @@ def test_scan_candidates_match_oracle(scan_ready):
         assert np.array_equal(key(cand).view(np.uint8), key(want).view(np.uint8))
 
 
+def test_scan_from_seeds_equals_host_table_inputs(scan_ready):
+    """dsg_scan_seeds builds the table inputs on the device; results must equal the scan of the oracle-built
+    inputs exactly (maxima and the candidate set, field for field)."""
+    o = libs.orc()
+    rng = np.random.default_rng(4)
+    ss = seeds() + [libs.mix(int(v)) for v in rng.integers(0, 1 << 40, 10)]
+    a = scan_ready.scan_batch(np.concatenate([o.tabins(s) for s in ss]))
+    b = scan_ready.scan_seeds(np.array(ss, dtype=np.uint64))
+    key = lambda c: np.sort(c, order=["x", "z", "s"]).view(np.uint8)
+    for s, (ma, mb, ca), (na, nb, cb) in zip(ss, a, b):
+        assert (ma, mb) == (na, nb), s
+        assert np.array_equal(key(ca), key(cb)), s
+
+
 def test_scan_overflow_reported(scan_ready):
     o = libs.orc()
     tin = o.tabins(seeds()[0])
