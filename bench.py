@@ -12,6 +12,11 @@ data-path collective); device time is the max over ranks.
 --impl reference times the reference's own CPU searcher (oracle/_ref/dsearch_desert, compiled from the
 reference sources) on the same seed stream with all host cores: its CPU gate (y-phase, sub-grid pre-gate,
 full tables) plus the tables+scan of every gated seed, with the hot-zone stage reduced to one site.
+
+Besides the gate line, the default run adds (single GPU): "pipeline", the whole per-seed search through the
+drop-in searcher (ours overlapped, ours plain, the reference's GPU searcher; wall clock; outputs compared),
+and "flood", exact step-1 floods of uneven size as one batch, through the flood service under Poisson
+arrivals, and as sequential per-request launches.
 """
 import argparse
 import json
@@ -115,7 +120,7 @@ def flood_sites(dsgpu, n_small, rng_seed=20261203):
     return small[:n_small], large
 
 
-def bench_floods(dsgpu, n_small=4096, rate=500.0, n_service=1500, n_seq=120, batch_only=False, n_large=None):
+def bench_floods(dsgpu, n_small=4096, rates=(200.0, 1000.0, 3000.0), n_service=1500, n_seq=120, batch_only=False, n_large=None):
     """Exact step-1 floods: one batch of every site, and the flood service under Poisson arrivals."""
     import threading
     import numpy as np
@@ -138,43 +143,50 @@ def bench_floods(dsgpu, n_small=4096, rate=500.0, n_service=1500, n_seq=120, bat
              "speculation_overhead": work["blocks"] * 256 / max(1, work["touched"])}
     if batch_only:
         return {"batch": batch}
-    # service: 90% small, 10% large, Poisson arrivals at `rate`
+    # service: 90% small, 10% large, Poisson arrivals, at each rate of the sweep
     rng = np.random.default_rng(7)
     kinds = rng.random(n_service) < 0.1
     mix = [large[rng.integers(len(large))] if k else small[rng.integers(len(small))] for k in kinds]
-    arrive = np.cumsum(rng.exponential(1.0 / rate, n_service))
-    svc = dsgpu.Service(budget_bytes=24 << 30, max_requests=4096, rounds_per_check=4)
-    done_t = np.zeros(n_service); tickets = [0] * n_service
-    lock = threading.Lock(); ready = threading.Semaphore(0)
-    def waiter():
-        while True:
-            ready.acquire()
+    gaps = rng.exponential(1.0, n_service)
+
+    def serve(rate):
+        arrive = np.cumsum(gaps / rate)
+        svc = dsgpu.Service(budget_bytes=24 << 30, max_requests=4096, rounds_per_check=4)
+        done_t = np.zeros(n_service); tickets = [0] * n_service
+        lock = threading.Lock(); ready = threading.Semaphore(0)
+        todo = []
+
+        def waiter():
+            while True:
+                ready.acquire()
+                with lock:
+                    if not todo:
+                        return
+                    i = todo.pop(0)
+                svc.wait(tickets[i])
+                done_t[i] = time.perf_counter()
+        ws = [threading.Thread(target=waiter) for _ in range(16)]
+        for w in ws:
+            w.start()
+        t_start = time.perf_counter()
+        for i in range(n_service):
+            d = t_start + arrive[i] - time.perf_counter()
+            if d > 0:
+                time.sleep(d)
+            tickets[i] = svc.submit(req(mix[i]))
             with lock:
-                if not todo:
-                    return
-                i = todo.pop(0)
-            svc.wait(tickets[i])
-            done_t[i] = time.perf_counter()
-    todo = []
-    ws = [threading.Thread(target=waiter) for _ in range(16)]
-    for w in ws:
-        w.start()
-    t_start = time.perf_counter()
-    for i in range(n_service):
-        d = t_start + arrive[i] - time.perf_counter()
-        if d > 0:
-            time.sleep(d)
-        tickets[i] = svc.submit(req(mix[i]))
-        with lock:
-            todo.append(i)
-        ready.release()
-    for _ in ws:
-        ready.release()
-    for w in ws:
-        w.join()
-    svc.close()
-    lat = done_t - (t_start + arrive)
-    t_svc = done_t.max() - t_start
+                todo.append(i)
+            ready.release()
+        for _ in ws:
+            ready.release()
+        for w in ws:
+            w.join()
+        svc.close()
+        lat = done_t - (t_start + arrive)
+        return {"rate_req_per_s": rate, "requests": n_service, "floods_per_s": n_service / (done_t.max() - t_start),
+                "p50_ms": float(np.percentile(lat, 50) * 1e3), "p99_ms": float(np.percentile(lat, 99) * 1e3)}, arrive
+    sweep = [serve(r) for r in rates]
+    arrive = sweep[0][1]
     # sequential plain per-request launches: measured service times of a sample, FIFO queue on the same arrivals
     seq_t = []
     for i in range(n_seq):
@@ -187,12 +199,55 @@ def bench_floods(dsgpu, n_small=4096, rate=500.0, n_service=1500, n_seq=120, bat
     seq_lat = fin - arrive
     return {
         "batch": batch,
-        "service": {"rate_req_per_s": rate, "requests": n_service, "mix": "90% random desert sites, 10% verified finds (step 1, half 20000)",
-                    "floods_per_s": n_service / t_svc, "p50_ms": float(np.percentile(lat, 50) * 1e3), "p99_ms": float(np.percentile(lat, 99) * 1e3)},
-        "sequential_plain": {"floods_per_s": 1.0 / mean_seq, "p50_ms": float(np.percentile(seq_lat, 50) * 1e3),
+        "service": {"mix": "90% random desert sites, 10% verified finds (step 1, half 20000)", "rates": [r for r, _ in sweep]},
+        "sequential_plain": {"floods_per_s": 1.0 / mean_seq, "rate_req_per_s": rates[0], "p50_ms": float(np.percentile(seq_lat, 50) * 1e3),
                              "p99_ms": float(np.percentile(seq_lat, 99) * 1e3),
-                             "how": f"dsg_flood per request, measured on {n_seq} requests of the same mix, FIFO queue on the same arrival times"},
+                             "how": f"dsg_flood per request, measured on {n_seq} requests of the same mix, FIFO queue on the first rate's arrival times"},
     }
+
+
+def pipeline(count=1 << 24):
+    """The whole per-seed pipeline through the drop-in searcher (gate -> tables/blur/scan -> hot-zone floods ->
+    proxy -> exact floods), seeds mix(2e13 + k), k < count, timed by wall clock around each process: ours with
+    one worker per host core up to 8 (device stages of different batches overlap; the library serialises
+    each kind of device call), ours with one worker (plain: every stage of a batch in turn), and the
+    reference's own GPU searcher built from its sources, with the same arguments.  Outputs are compared."""
+    import re
+    cores = os.cpu_count() or 1
+    ours = os.path.join(ROOT, "desert-search_b200", "bin", "dsearch_desert")
+    ref = os.path.join(ROOT, "oracle", "_ref", "dsearch_desert_gpu")
+    out = {"seeds": count, "args": "START=2e13 gate=1 gpu=1 gscan=1", "host_cores": cores}
+
+    def run(exe, threads, td, tag):
+        pre = os.path.join(td, tag)
+        t0 = time.perf_counter()
+        r = subprocess.run([exe, str(START), str(count), pre, str(threads), "gate=1", "gpu=1", "gscan=1"], capture_output=True, text=True)
+        wall = time.perf_counter() - t0
+        if r.returncode != 0:
+            return {"error": r.stderr[-300:]}, None
+        m = re.search(r"done: (\d+) seeds \((\d+) passed\)", r.stderr)
+        gated = int(m.group(2)) if m else 0
+        st = re.search(r"startup ([\d.]+) s", r.stderr)
+        res = {"threads": threads, "wall_s": wall, "gated": gated, "gated_per_s": gated / wall}
+        if st:
+            res["startup_s"] = float(st.group(1))
+            res["gated_per_s_after_startup"] = gated / max(1e-9, wall - float(st.group(1)))
+        rows = sorted(open(pre + ".csv").read().splitlines()[1:])
+        return res, rows
+
+    with tempfile.TemporaryDirectory() as td:
+        out["ours"], rows = run(ours, cores, td, "ours")
+        out["ours_plain"], rows1 = run(ours, 1, td, "plain")
+        if os.path.exists(ref):
+            out["reference_gpu_searcher"], rrows = run(ref, cores, td, "ref")
+            if rows is not None and rrows is not None:
+                out["csv_rows"] = len(rows)
+                out["csv_identical_to_reference"] = rows == rrows
+        else:
+            out["reference_gpu_searcher"] = {"unavailable": "oracle/_ref/dsearch_desert_gpu not built"}
+        if rows is not None and rows1 is not None:
+            out["plain_csv_identical"] = rows == rows1
+    return out
 
 
 def run_ours(args):
@@ -222,7 +277,7 @@ def run_ours(args):
 
     if args.flood_only:
         if rank == 0:
-            print(json.dumps({"flood": bench_floods(dsgpu, n_small=args.flood_small, rate=args.flood_rate, n_service=args.flood_requests,
+            print(json.dumps({"flood": bench_floods(dsgpu, n_small=args.flood_small, rates=args.flood_rates, n_service=args.flood_requests,
                                                     batch_only=args.flood_batch_only, n_large=args.flood_large)}), flush=True)
         return
     barrier()
@@ -281,6 +336,9 @@ def run_ours(args):
     }
     if world == 1:
         out["cpu_baseline"] = cpu_baseline()
+        if not args.no_extras:
+            out["pipeline"] = pipeline()
+            out["flood"] = bench_floods(dsgpu, n_small=1024, rates=args.flood_rates, n_service=args.flood_requests)
     print(json.dumps(out), flush=True)
     if pg:
         pg.destroy_process_group()
@@ -333,8 +391,9 @@ def main():
     ap.add_argument("--flood-small", type=int, default=4096)
     ap.add_argument("--flood-large", type=int, default=None, help="limit the large (verified-find) flood class")
     ap.add_argument("--flood-batch-only", action="store_true")
-    ap.add_argument("--flood-rate", type=float, default=500.0)
+    ap.add_argument("--flood-rates", type=float, nargs="+", default=[200.0, 1000.0, 3000.0])
     ap.add_argument("--flood-requests", type=int, default=1500)
+    ap.add_argument("--no-extras", action="store_true", help="skip the pipeline and flood measurements of the default run")
     args = ap.parse_args()
     global PER_STEP
     PER_STEP = 1 << args.per_step_log2

@@ -102,9 +102,11 @@ int run_batch(const dsg_flood_req *reqs, uint32_t n, dsg_area *out, size_t pool_
     k_tile_start<<<(n + 127) / 128, 128, 0, st>>>(g.d_ctl, nullptr, n, g.d_stat, g.d_dir, g.pool.T, ta, g.pool.n_list[0], g.d_cnt + 0,
                                                   0, nullptr, g.d_cnt + 10);
     DSG_CU(cudaGetLastError());
-    const int K = 4;                                   // rounds enqueued between completion checks
+    // rounds enqueued between completion checks: few at first (most batches of small floods end within a few
+    // rounds), doubling while work remains (a large flood runs hundreds of rounds)
+    int K = 2;
     uint32_t round = 0;
-    for (;;) {
+    for (;; K = std::min(2 * K, 64)) {
         for (int k = 0; k < K; k++, round++)
             launch_round(g.pool, round, g.d_cnt, nullptr, g.d_cnt + 10, g.d_evals, g.d_ctl, g.d_noise, g.d_dir, g.d_stat, ta, g.grid_eval, g.grid_conn, st);
         DSG_CU(cudaGetLastError());
