@@ -136,14 +136,14 @@ static __global__ void __launch_bounds__(EVAL_THREADS) k_tile_eval(const FloodCt
     __shared__ SeedNoise s_noise;
     __shared__ PendingState s_pend[EVAL_THREADS];
     __shared__ int8_t s_res[EVAL_THREADS];
-    __shared__ int s_n, s_seed;
+    __shared__ int s_n;
     __shared__ uint32_t s_run;
     const uint32_t items = *q.n_cnt;
     const uint32_t run = max(1u, min(16u, items / (4 * gridDim.x)));
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    if (threadIdx.x == 0) s_seed = -1;
+    int staged = -1;                                      // every thread walks the same items: no shared copy needed
     for (;;) {
-        __syncthreads();                                  // s_run of the previous run has been read
+        __syncthreads();                                  // the previous item is done with shared memory
         if (threadIdx.x == 0) s_run = atomicAdd(q.work, run);
         __syncthreads();
         const uint32_t begin = s_run;
@@ -154,14 +154,12 @@ static __global__ void __launch_bounds__(EVAL_THREADS) k_tile_eval(const FloodCt
             const uint32_t r = T.owner[t], pos = T.pos[t];
             const FloodCtl c = ctl[r];
             const int i = int(pos & 0xffff) * TILE + col, j = int(pos >> 16) * TILE + row;
-            __syncthreads();                              // the previous item is done with shared memory
-            const bool restage = s_seed != c.noise;
-            __syncthreads();
-            if (restage) {
+            if (item != begin) __syncthreads();           // the previous item is done with shared memory
+            if (staged != c.noise) {
                 const uint4 *src = reinterpret_cast<const uint4 *>(noise + c.noise);
                 uint4 *dst = reinterpret_cast<uint4 *>(&s_noise);
                 for (int k = threadIdx.x; k < int(sizeof(SeedNoise) / 16); k += blockDim.x) dst[k] = __ldg(src + k);
-                if (threadIdx.x == 0) s_seed = c.noise;
+                staged = c.noise;
             }
             if (threadIdx.x == 0) s_n = 0;
             __syncthreads();
@@ -185,9 +183,8 @@ static __global__ void __launch_bounds__(EVAL_THREADS) k_tile_eval(const FloodCt
                 b[h] = uint16_t(pm); b[h + 4] = uint16_t(pm >> 16);
                 b[4 * TILE + h] = uint16_t(dm); b[4 * TILE + h + 4] = uint16_t(dm >> 16);
             }
-            __syncthreads();
+            // the rows are read by the next launch (connect), so the mark needs no barrier after the stores
             if (threadIdx.x == 0) {
-                __threadfence();
                 atomicOr(&T.emask[t], 1u << sb);
                 if (atomicExch(&T.mark[t], q.round + 1) != q.round + 1) q.w_list[atomicAdd(q.w_cnt, 1u)] = t;
                 atomicAdd(q.evaluated, 1ull);

@@ -149,6 +149,88 @@ __global__ void __launch_bounds__(256) k_cand(const LeafBox *__restrict__ leaves
     }
     if (!off && threadIdx.x == 0) cnt[blockIdx.x] = base;
 }
+// Second pruning pass over each cell's list: leaf L also goes when a single leaf K of its depth interval is
+// nearer than L at every point of the cell, i.e. when the sum over the five axes of min over the cell's range
+// of (dist_L(v)^2 - dist_K(v)^2) is positive.  On one axis the difference is a piecewise polynomial of degree
+// at most two whose pieces meet at the intervals' ends, and on each piece it is linear, concave, or convex
+// with its vertex at a piece end, so the minimum over the integers of [A, B] is at A, B or an interval end
+// inside [A, B].  Each L is tested first against its class's leaf of least max-distance, then against all.
+// Lists longer than kPruneMax keep the first pass's result.  Survivors keep their order; cnt[cell] = kept.
+constexpr int kPruneMax = 2048;
+__device__ __forceinline__ int64_t axis_min_diff(const LeafBox &L, const LeafBox &K, int a, int64_t A, int64_t B) {
+    auto d2 = [](const LeafBox &X, int a2, int64_t v) { const int64_t d = max(max(int64_t(X.lo[a2]) - v, v - int64_t(X.hi[a2])), int64_t(0)); return d * d; };
+    const int64_t pts[6] = {A, B, L.lo[a], L.hi[a], K.lo[a], K.hi[a]};
+    int64_t m = INT64_MAX;
+    #pragma unroll
+    for (int k = 0; k < 6; k++) {
+        const int64_t v = pts[k];
+        if (v < A || v > B) continue;
+        m = min(m, d2(L, a, v) - d2(K, a, v));
+    }
+    return m;
+}
+__device__ __forceinline__ bool dominated_by(const LeafBox &L, const LeafBox &K, const int64_t *A, const int64_t *B) {
+    int64_t s = 0;
+    #pragma unroll
+    for (int a = 0; a < 5; a++) s += axis_min_diff(L, K, a, A[a], B[a]);
+    return s > 0;
+}
+__global__ void __launch_bounds__(256) k_cand_prune(const LeafBox *__restrict__ leaves, const uint16_t *__restrict__ leaf_of, WorldDev w,
+                                                    const uint32_t *__restrict__ off, uint16_t *__restrict__ cand, uint16_t *__restrict__ cnt) {
+    __shared__ uint16_t s_id[kPruneMax];
+    __shared__ uint8_t s_keep[kPruneMax];
+    __shared__ unsigned long long s_best[kMaxDepthClasses];
+    uint32_t r = blockIdx.x;
+    int64_t A[5], B[5];
+    for (int a = 4; a >= 0; a--) {
+        const uint32_t i = r % uint32_t(w.cdim[a]);
+        r /= uint32_t(w.cdim[a]);
+        A[a] = w.ccut[a][i]; B[a] = int64_t(w.ccut[a][i + 1]) - 1;
+    }
+    const uint32_t b = off[blockIdx.x], n = off[blockIdx.x + 1] - b;
+    if (n > uint32_t(kPruneMax)) { if (threadIdx.x == 0) cnt[blockIdx.x] = uint16_t(min(n, 65535u)); return; }
+    if (threadIdx.x < kMaxDepthClasses) s_best[threadIdx.x] = ~0ull;
+    __syncthreads();
+    for (uint32_t k = threadIdx.x; k < n; k += blockDim.x) {
+        const uint16_t id = leaf_of[cand[b + k]];
+        s_id[k] = id;
+        const LeafBox &l = leaves[id];
+        uint64_t mx = 0;
+        #pragma unroll
+        for (int a = 0; a < 5; a++) {
+            const int64_t da = max(max(int64_t(l.lo[a]) - A[a], A[a] - int64_t(l.hi[a])), int64_t(0));
+            const int64_t db = max(max(int64_t(l.lo[a]) - B[a], B[a] - int64_t(l.hi[a])), int64_t(0));
+            const int64_t d = max(da, db);
+            mx += uint64_t(d * d);
+        }
+        atomicMin(&s_best[l.cls], (mx << 16) | k);             // least max-distance, then list position
+    }
+    __syncthreads();
+    for (uint32_t k = threadIdx.x; k < n; k += blockDim.x) {
+        const LeafBox &L = leaves[s_id[k]];
+        const uint32_t kb = uint32_t(s_best[L.cls] & 0xffff);
+        bool dom = kb != k && dominated_by(L, leaves[s_id[kb]], A, B);
+        for (uint32_t j = 0; j < n && !dom; j++) {
+            if (j == k) continue;
+            const LeafBox &K = leaves[s_id[j]];
+            if (K.cls == L.cls && dominated_by(L, K, A, B)) dom = true;
+        }
+        s_keep[k] = !dom;
+    }
+    __syncthreads();
+    if (threadIdx.x < 32) {                                    // in-order compaction by the first warp
+        const int lane = threadIdx.x;
+        uint32_t kept = 0;
+        for (uint32_t k0 = 0; k0 < n; k0 += 32) {
+            const uint32_t k = k0 + lane;
+            const bool keep = k < n && s_keep[k];
+            const uint32_t m = __ballot_sync(0xffffffffu, keep);
+            if (keep) cand[b + kept + __popc(m & ((1u << lane) - 1))] = uint16_t(leaves[s_id[k]].node);
+            kept += __popc(m);
+        }
+        if (lane == 0) cnt[blockIdx.x] = uint16_t(kept);
+    }
+}
 void check_tree(const Blob &b) {
     const int n = int(b.tree.size());
     auto is_leaf = [&](int k) { return (b.tree[k] >> 56) == 255; };
@@ -214,7 +296,7 @@ void build_candidates(const Blob &b, WorldDev &w) {
     if (classes.size() > size_t(kMaxDepthClasses) || b.tree.size() > 0xffff) throw std::runtime_error("biome tree: too many depth intervals or nodes");
     uint32_t ncell = 1;
     for (int a = 0; a < 5; a++) ncell *= uint32_t(w.cdim[a]);
-    LeafBox *d_leaves = nullptr; uint32_t *d_cnt = nullptr, *d_off = nullptr; uint16_t *d_cand = nullptr;
+    LeafBox *d_leaves = nullptr; uint32_t *d_cnt = nullptr, *d_off = nullptr; uint16_t *d_cand = nullptr, *d_leaf_of = nullptr, *d_n = nullptr;
     try {
         DSG_CU(cudaMalloc(&d_leaves, leaves.size() * sizeof(LeafBox)));
         DSG_CU(cudaMemcpy(d_leaves, leaves.data(), leaves.size() * sizeof(LeafBox), cudaMemcpyHostToDevice));
@@ -234,10 +316,17 @@ void build_candidates(const Blob &b, WorldDev &w) {
         DSG_CU(cudaMalloc(&d_cand, size_t(off[ncell]) * 2 + 2));
         k_cand<<<ncell, 256>>>(d_leaves, int(leaves.size()), w, nullptr, d_off, d_cand);
         DSG_CU(cudaGetLastError());
+        std::vector<uint16_t> leaf_of(b.tree.size(), 0);
+        for (size_t k = 0; k < leaves.size(); k++) leaf_of[leaves[k].node] = uint16_t(k);
+        DSG_CU(cudaMalloc(&d_leaf_of, leaf_of.size() * 2));
+        DSG_CU(cudaMemcpy(d_leaf_of, leaf_of.data(), leaf_of.size() * 2, cudaMemcpyHostToDevice));
+        DSG_CU(cudaMalloc(&d_n, size_t(ncell) * 2));
+        k_cand_prune<<<ncell, 256>>>(d_leaves, d_leaf_of, w, d_off, d_cand, d_n);
+        DSG_CU(cudaGetLastError());
         DSG_CU(cudaDeviceSynchronize());
-    } catch (...) { cudaFree(d_leaves); cudaFree(d_cnt); cudaFree(d_off); cudaFree(d_cand); throw; }
-    cudaFree(d_leaves); cudaFree(d_cnt);
-    w.cand_off = d_off; w.cand = d_cand;
+    } catch (...) { cudaFree(d_leaves); cudaFree(d_cnt); cudaFree(d_off); cudaFree(d_cand); cudaFree(d_leaf_of); cudaFree(d_n); throw; }
+    cudaFree(d_leaves); cudaFree(d_cnt); cudaFree(d_leaf_of);
+    w.cand_off = d_off; w.cand = d_cand; w.cand_n = d_n;
 }
 template <class T> const T *upload(const std::vector<T> &v) {
     T *d = nullptr;

@@ -16,8 +16,9 @@ struct WorldDev {
     const int32_t *param;        // interval k = [param[2k], param[2k+1]]
     const SplineDev *spl;        // terrain-offset spline graph (node 0 is the root)
     const float *prob;           // 40 x 40 proxy desert probability (row = C bin, column = E bin)
-    const uint32_t *cand_off;    // candidate leaves of candidate-grid cell f: cand[cand_off[f] .. cand_off[f + 1])
+    const uint32_t *cand_off;    // candidate leaves of candidate-grid cell f: cand[cand_off[f] ..] (cand_n[f] of them)
     const uint16_t *cand;        // tree node indices, ascending within a cell
+    const uint16_t *cand_n;
     int32_t ntree, nspl, nparam;
     int32_t strides[8];
     int32_t dim[5];              // grid cells per axis (T, H, C, E, W)
@@ -128,7 +129,8 @@ __device__ __forceinline__ bool cand_locate(const WorldDev &w, const int64_t *q,
 // minimum over the candidate leaves of the point's candidate-grid cell.  Below the root every box contains
 // its children's boxes, so the pruned depth-first search returns exactly that minimum over all leaves; the
 // candidates of a cell are every leaf that can attain it for some point of the cell and any depth
-// (world_upload drops a leaf only when a leaf of the same depth interval is nearer everywhere in the cell).
+// (world_upload drops a leaf only when a leaf of the same depth interval is nearer everywhere in the cell, by
+// bounds of the whole cell and by pairwise comparison).
 // Points outside the candidate grid (rare: climate values beyond the surface boxes other than hot
 // temperatures) take the tree search itself.
 __device__ inline int classify_exact(const WorldDev &w, const int64_t *v) {
@@ -136,7 +138,7 @@ __device__ inline int classify_exact(const WorldDev &w, const int64_t *v) {
     if (!cand_locate(w, v, f)) return tree_classify(w, v);
     uint64_t bestd = ~0ull;
     int best = 0;
-    for (uint32_t k = __ldg(&w.cand_off[f]), e = __ldg(&w.cand_off[f + 1]); k < e; k++) {
+    for (uint32_t k = __ldg(&w.cand_off[f]), e = k + __ldg(&w.cand_n[f]); k < e; k++) {
         const int node = __ldg(&w.cand[k]);
         const uint64_t d = box_dist(w, node, v);
         if (d < bestd) { bestd = d; best = node; }

@@ -487,7 +487,9 @@ int main(int argc, char **argv) {
     fprintf(S.out, "seed,fyA,fyB,maxta,maxtb,rank,x,z,score,t0,c0,e0,proxy,s8,s4,edge,hot\n");
     fprintf(S.sout, "seed,fyA,fyB,maxta,maxtb,candidates,sites,best\n");
     signal(SIGINT, on_signal); signal(SIGTERM, on_signal);
+    const auto ti0 = Clock::now();
     ck(dsg_init(0, float(P.pcut)), "dsg_init");
+    const double t_init = std::chrono::duration<double>(Clock::now() - ti0).count(), t_before = std::chrono::duration<double>(ti0 - S.begin).count();
     {
         static TMap TMT(1024.0), TMC(512.0);
         hostcheck::blur_taps(P.sigma, S.kT, S.rT); hostcheck::blur_taps(P.sigmac, S.kC, S.rC);
@@ -576,7 +578,7 @@ int main(int argc, char **argv) {
             (unsigned long long)S.nsites.load(), sec, S.threads, P.max_phase, P.sigma, P.wc, P.we, P.t, P.ta, P.max_sites, P.nms, S.t_tab.load(), S.t_scan.load(), S.t_site.load());
     fclose(m);
     fprintf(stderr, "done: %llu seeds (%llu passed) in %.1fs\n", (unsigned long long)S.done.load(), (unsigned long long)S.passed.load(), sec);
-    fprintf(stderr, "startup %.3f s, gate done at %.3f s\n", t_ready, gate_end.load());
+    fprintf(stderr, "startup %.3f s (before dsg_init %.3f, dsg_init %.3f), gate done at %.3f s\n", t_ready, t_before, t_init, gate_end.load());
     fprintf(stderr, "stage seconds: tables %.3f scan %.3f sites %.3f (hot points %.3f; hot-zone floods %.3f: pre-floods %.3f [rounds %llu sub-blocks %llu touched %llu], %llu floods used, step-128 floods %.3f; proxy %.3f of which kernel %.3f; exact floods %.3f)\n",
             S.t_tab.load(), S.t_scan.load(), S.t_site.load(), S.t_hq.load(), S.t_hot.load(), S.t_pre.load(), (unsigned long long)S.pre_work[0].load(), (unsigned long long)S.pre_work[1].load(), (unsigned long long)S.pre_work[2].load(), (unsigned long long)S.nhot.load(), S.t_wave.load(), S.t_proxy.load(), S.t_gpu.load(), S.t_exact.load());
     std::fflush(nullptr);
