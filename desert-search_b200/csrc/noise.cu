@@ -65,7 +65,7 @@ __global__ void __launch_bounds__(64) k_seed_noise(const uint64_t *__restrict__ 
     o.iy = int(fl); o.fy = o.oy - fl; o.vy = fade_d(o.fy); o.pad = 0;
     S.oct[t] = o;
     #pragma unroll
-    for (int k = 0; k < 16; k++) reinterpret_cast<uint4 *>(S.perm[t])[k] = reinterpret_cast<const uint4 *>(perm)[k];
+    for (int k = 0; k < 32; k++) reinterpret_cast<uint4 *>(S.perm[t])[k] = reinterpret_cast<const uint4 *>(perm)[k & 15];   // stored twice
 }
 }  // namespace
 

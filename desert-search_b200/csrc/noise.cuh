@@ -14,10 +14,12 @@ enum { CH_T = 0, CH_H = 1, CH_C = 2, CH_E = 3, CH_S = 4, CH_W = 5 };
 constexpr int NOCT = 46;                     // nonzero octaves over all channels, both sides
 
 struct __align__(16) NOct { double ox, oy, oz, freq, amp, fy, vy; int32_t iy, pad; };
-// All noise of one seed: octave k of channel ch, side s is oct[off[ch] + s * cnt[ch] + k].
+// All noise of one seed: octave k of channel ch, side s is oct[off[ch] + s * cnt[ch] + k].  Each permutation
+// is stored twice over (perm[k][i] = perm[k][i & 255] for i < 512), so a lattice index masked once can be
+// offset by a hash and a corner step without masking again.
 struct __align__(16) SeedNoise {
     NOct oct[NOCT];
-    uint8_t perm[NOCT][256];
+    uint8_t perm[NOCT][512];
     double factor[6];
     int32_t off[6], cnt[6];
 };
@@ -25,29 +27,31 @@ struct __align__(16) SeedNoise {
 #ifdef __CUDACC__
 __device__ __forceinline__ double fade_d(double t) { return t * t * t * (t * (t * 6. - 15.) + 10.); }
 __device__ __forceinline__ double lerp_d(double t, double a, double b) { return a + t * (b - a); }
-// gx*x + gy*y + gz*z of Minecraft's 16 gradients (components 0/+-1): the two nonzero terms with signs.
+// gx*x + gy*y + gz*z of Minecraft's 16 gradients (components 0/+-1): the two nonzero terms with signs.  A
+// sign is applied by flipping the sign bit, which is what negation does.
+__device__ __forceinline__ double flip_sign(double v, int s) { return __hiloint2double(__double2hiint(v) ^ (s << 31), __double2loint(v)); }
 __device__ __forceinline__ double grad_d(int h, double x, double y, double z) {
     h &= 15;
     const double u = h < 8 ? x : y;
     const double v = h < 4 ? y : ((h == 12 || h == 14) ? x : z);
-    return ((h & 1) ? -u : u) + ((h & 2) ? -v : v);
+    return flip_sign(u, h & 1) + flip_sign(v, (h >> 1) & 1);
 }
-// One Perlin octave (standalone.hpp:62-83).
+// One Perlin octave (standalone.hpp:62-83); P is the doubled permutation of the octave.
 __device__ __forceinline__ double perlin(const NOct &o, const uint8_t *__restrict__ P, double x, double y, double z) {
     x += o.ox; z += o.oz;
     const double bx = floor(x), bz = floor(z);
-    const int ix = int(bx), iz = int(bz);
+    const int ix = int(bx) & 255, iz = int(bz) & 255;
     x -= bx; z -= bz;
     int jy = o.iy; double dy = o.fy, ty = o.vy;
-    if (y != 0) { y += o.oy; const double by = floor(y); jy = int(by); dy = y - by; ty = fade_d(dy); }
-    const int a0 = P[ix & 255], a1 = P[(ix + 1) & 255];
-    const int b00 = P[(a0 + jy) & 255], b01 = P[(a0 + jy + 1) & 255];
-    const int b10 = P[(a1 + jy) & 255], b11 = P[(a1 + jy + 1) & 255];
+    if (y != 0) { y += o.oy; const double by = floor(y); jy = int(by) & 255; dy = y - by; ty = fade_d(dy); }
+    const int a0 = P[ix], a1 = P[ix + 1];
+    const int b00 = P[a0 + jy], b01 = P[a0 + jy + 1];
+    const int b10 = P[a1 + jy], b11 = P[a1 + jy + 1];
     const double tx = fade_d(x), tz = fade_d(z);
-    const double lo = lerp_d(ty, lerp_d(tx, grad_d(P[(b00 + iz) & 255], x, dy, z), grad_d(P[(b10 + iz) & 255], x - 1, dy, z)),
-                                 lerp_d(tx, grad_d(P[(b01 + iz) & 255], x, dy - 1, z), grad_d(P[(b11 + iz) & 255], x - 1, dy - 1, z)));
-    const double hi = lerp_d(ty, lerp_d(tx, grad_d(P[(b00 + iz + 1) & 255], x, dy, z - 1), grad_d(P[(b10 + iz + 1) & 255], x - 1, dy, z - 1)),
-                                 lerp_d(tx, grad_d(P[(b01 + iz + 1) & 255], x, dy - 1, z - 1), grad_d(P[(b11 + iz + 1) & 255], x - 1, dy - 1, z - 1)));
+    const double lo = lerp_d(ty, lerp_d(tx, grad_d(P[b00 + iz], x, dy, z), grad_d(P[b10 + iz], x - 1, dy, z)),
+                                 lerp_d(tx, grad_d(P[b01 + iz], x, dy - 1, z), grad_d(P[b11 + iz], x - 1, dy - 1, z)));
+    const double hi = lerp_d(ty, lerp_d(tx, grad_d(P[b00 + iz + 1], x, dy, z - 1), grad_d(P[b10 + iz + 1], x - 1, dy, z - 1)),
+                                 lerp_d(tx, grad_d(P[b01 + iz + 1], x, dy - 1, z - 1), grad_d(P[b11 + iz + 1], x - 1, dy - 1, z - 1)));
     return lerp_d(tz, lo, hi);
 }
 // Two-sided channel value (standalone.hpp:140-151): per-side sums, side B at 337/331 scale.
