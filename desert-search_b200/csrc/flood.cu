@@ -13,6 +13,8 @@
 namespace dsg {
 namespace flood {
 
+constexpr uint32_t kEagerBatch = 32;                // batches up to this many requests run in eager mode
+
 struct Engine {
     std::mutex mu;
     bool ready = false;
@@ -76,6 +78,7 @@ int run_batch(const dsg_flood_req *reqs, uint32_t n, dsg_area *out, size_t pool_
         FloodCtl &c = ctl[r];
         c.qx = q.qx; c.qz = q.qz; c.step = q.step; c.half = q.half; c.n = 2 * q.half + 1; c.tpr = (c.n + TILE - 1) / TILE;
         c.conn8 = q.conn8 ? 1 : 0; c.pred = q.pred; c.pcut = q.pcut; c.noise = it->second; c.dir_off = int64_t(dir_total);
+        c.eager = n <= kEagerBatch ? 1 : 0;           // few requests: latency matters more than speculative work
         dir_total += size_t(c.tpr) * c.tpr;
         dir_max = std::max<int64_t>(dir_max, int64_t(c.tpr) * c.tpr);
     }

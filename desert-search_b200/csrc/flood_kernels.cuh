@@ -14,7 +14,9 @@
 //    warp, the diagonal step for 8-connectivity), seeded from the R edges of the neighbouring tiles; it
 //    requests the sub-blocks next to R (in this tile and across its edges) and queues evaluated neighbours
 //    whose shared edge changed.  R only grows, so the rounds reach the unique fixed point whatever the
-//    interleaving, and at that point every cell adjacent to R has been evaluated;
+//    interleaving, and at that point every cell adjacent to R has been evaluated.  In eager mode (for
+//    latency: the service, small batches) a tile whose R is already large requests whole tiles instead,
+//    so a large flood advances 64 cells per round at the cost of more speculative evaluation;
 //  * when a request has no queued work left, k_tile_finish derives DenseArea from R, D and the neighbours:
 //    cells = |R & D|, bbox over R & D, touched = start + R + neighbours of R, sampled = touched cells inside
 //    window and world, border = a touched cell outside the world, edge = an R cell on the window boundary.
@@ -27,8 +29,11 @@ namespace flood {
 
 struct FloodCtl {                      // one request
     int32_t qx, qz, step, half, n, tpr, conn8, pred;
-    float pcut; int32_t noise; int64_t dir_off;
+    float pcut; int32_t noise;
+    int32_t eager, pad;                // eager: tiles with >= 256 reached cells request whole neighbouring tiles
+    int64_t dir_off;
 };
+constexpr int kEagerCells = 256;
 struct FloodStat {
     unsigned long long cells, sampled;
     int32_t minx, maxx, minz, maxz, edge, border, overflow, pad;
@@ -386,6 +391,10 @@ static __global__ void __launch_bounds__(256) k_tile_connect(const FloodCtl *__r
             case 7: mask = c8 && (bot >> 63) ? 1u : 0; changed = (bot_new >> 63) != 0; dti = 1; dtj = 1; break;
             case 8: mask = self; break;
             default: break;
+        }
+        if (c.eager) {                                   // a large region: evaluate ahead by whole tiles (fewer rounds)
+            const int reached = __reduce_add_sync(0xffffffffu, __popcll(ra) + __popcll(rb));
+            if (reached >= kEagerCells) mask = lane == 8 ? (0xffffu & ~em) : (mask ? 0xffffu : 0u);
         }
         if (lane == 8) request_blocks(T, int32_t(t), mask, r, q.n_next, q.n_next_cnt, q.round + 1, q.active);
         const int nti = ti + dti, ntj = tj + dtj;

@@ -95,6 +95,7 @@ void engine_loop(Service &g) {
                 FloodCtl c{};
                 c.qx = q.qx; c.qz = q.qz; c.step = q.step; c.half = q.half; c.n = 2 * q.half + 1; c.tpr = (c.n + TILE - 1) / TILE;
                 c.conn8 = q.conn8 ? 1 : 0; c.pred = q.pred; c.pcut = q.pcut; c.noise = int32_t(si);
+                c.eager = 1;                                   // latency first: large floods take fewer rounds
                 const int64_t len = int64_t(c.tpr) * c.tpr;
                 int64_t off;
                 if (!dir_alloc(g, len, off)) break;
