@@ -98,11 +98,12 @@ def cpu_baseline(seconds_budget=20.0):
             "seeds_per_s": count / dt}
 
 
-def flood_sites(dsgpu, n_small, rng_seed=20261203):
+def flood_sites(dsgpu, n_small, rng_seed=20261203, candidates=()):
     """Synthetic flood sites.  Small class: random int64 seeds from a fixed RNG stream, each paired with the
     first of 64 uniform blocks in |X|, |Z| <= 3e7 whose bridged Y=256 state is desert.  Large class: the
-    220 MC-Measure-verified finds of the reference's results (72M-100M blocks^2) and the two `make check`
-    records (tests/golden/finds.json) -- the stand-in for the searcher's proxy >= 50M candidates."""
+    searcher's own proxy >= 50M candidates (CSV rows of the pipeline run, `candidates` = (seed, x, z) in
+    blocks, kept where the start's state is desert), then the 220 MC-Measure-verified finds of the
+    reference's results (72M-100M blocks^2) and the two `make check` records (tests/golden/finds.json)."""
     import numpy as np
     rng = np.random.default_rng(rng_seed)
     small = []
@@ -116,15 +117,22 @@ def flood_sites(dsgpu, n_small, rng_seed=20261203):
             if len(k):
                 small.append((int(seeds[i]), int(xz[i * 64 + k[0], 0]), int(xz[i * 64 + k[0], 1])))
     finds = json.load(open(os.path.join(ROOT, "tests", "golden", "finds.json")))
-    large = [(f["seed"] & ((1 << 64) - 1), f["x"] >> 2, f["z"] >> 2) for f in finds]
+    large = []
+    if candidates:
+        cs = np.array([c[0] for c in candidates], dtype=np.uint64)
+        xz = np.array([[c[1] >> 2, c[2] >> 2] for c in candidates], dtype=np.int32)
+        st = dsgpu.query(cs, np.arange(len(cs), dtype=np.uint32), 6, xz)
+        large = [(int(cs[k]), int(xz[k, 0]), int(xz[k, 1])) for k in range(len(cs)) if st[k] == 2]
+    large += [(f["seed"] & ((1 << 64) - 1), f["x"] >> 2, f["z"] >> 2) for f in finds]
     return small[:n_small], large
 
 
-def bench_floods(dsgpu, n_small=4096, rates=(200.0, 1000.0, 3000.0), n_service=1500, n_seq=120, batch_only=False, n_large=None):
+def bench_floods(dsgpu, n_small=4096, rates=(200.0, 1000.0, 3000.0), n_service=1500, n_seq=120, batch_only=False, n_large=None,
+                 candidates=()):
     """Exact step-1 floods: one batch of every site, and the flood service under Poisson arrivals."""
     import threading
     import numpy as np
-    small, large = flood_sites(dsgpu, n_small)
+    small, large = flood_sites(dsgpu, n_small, candidates=candidates)
     if n_large is not None:
         large = large[:n_large]
     req = lambda s: dsgpu.flood_req(s[0], s[1], s[2], 1, 20000)
@@ -136,7 +144,8 @@ def bench_floods(dsgpu, n_small=4096, rates=(200.0, 1000.0, 3000.0), n_service=1
     work = dsgpu.flood_last_stats()
     sampled = sum(a[1] for a in areas)
     cells = np.array([a[0] for a in areas], dtype=np.float64)
-    batch = {"floods": len(reqs), "small": len(small), "large": len(large), "seconds": t_batch, "floods_per_s": len(reqs) / t_batch,
+    batch = {"floods": len(reqs), "small": len(small), "large": len(large), "large_from_search": len(large) - 222 if candidates else 0,
+             "seconds": t_batch, "floods_per_s": len(reqs) / t_batch,
              "cells_per_s": float(cells.sum()) / t_batch, "evaluations_per_s": sampled / t_batch,
              "area_blocks2_min_median_max": [float(cells.min() * 16), float(np.median(cells) * 16), float(cells.max() * 16)],
              "rounds": work["rounds"], "subblocks": work["blocks"], "cells_evaluated_per_s": work["blocks"] * 256 / t_batch,
@@ -186,23 +195,28 @@ def bench_floods(dsgpu, n_small=4096, rates=(200.0, 1000.0, 3000.0), n_service=1
         return {"rate_req_per_s": rate, "requests": n_service, "floods_per_s": n_service / (done_t.max() - t_start),
                 "p50_ms": float(np.percentile(lat, 50) * 1e3), "p99_ms": float(np.percentile(lat, 99) * 1e3)}, arrive
     sweep = [serve(r) for r in rates]
-    arrive = sweep[0][1]
-    # sequential plain per-request launches: measured service times of a sample, FIFO queue on the same arrivals
+    # sequential plain per-request launches: measured service times of a sample of the same mix, then a FIFO
+    # queue on each rate's arrival times
     seq_t = []
     for i in range(n_seq):
         t1 = time.perf_counter(); dsgpu.flood(*mix[i][:3], 1, 20000); seq_t.append(time.perf_counter() - t1)
     mean_seq = float(np.mean(seq_t))
     svc_times = np.array([seq_t[i % n_seq] for i in range(n_service)])
-    fin = np.zeros(n_service); prev = 0.0
-    for i in range(n_service):
-        prev = max(prev, arrive[i]) + svc_times[i]; fin[i] = prev
-    seq_lat = fin - arrive
+    seq_rates = []
+    for rate in rates:
+        arrive = np.cumsum(gaps / rate)
+        fin = np.zeros(n_service); prev = 0.0
+        for i in range(n_service):
+            prev = max(prev, arrive[i]) + svc_times[i]; fin[i] = prev
+        lat = fin - arrive
+        seq_rates.append({"rate_req_per_s": rate, "floods_per_s": n_service / fin[-1] if fin[-1] > 0 else None,
+                          "p50_ms": float(np.percentile(lat, 50) * 1e3), "p99_ms": float(np.percentile(lat, 99) * 1e3)})
     return {
         "batch": batch,
-        "service": {"mix": "90% random desert sites, 10% verified finds (step 1, half 20000)", "rates": [r for r, _ in sweep]},
-        "sequential_plain": {"floods_per_s": 1.0 / mean_seq, "rate_req_per_s": rates[0], "p50_ms": float(np.percentile(seq_lat, 50) * 1e3),
-                             "p99_ms": float(np.percentile(seq_lat, 99) * 1e3),
-                             "how": f"dsg_flood per request, measured on {n_seq} requests of the same mix, FIFO queue on the first rate's arrival times"},
+        "service": {"mix": "90% random desert sites, 10% large (search candidates and verified finds); step 1, half 20000",
+                    "rates": [r for r, _ in sweep]},
+        "sequential_plain": {"floods_per_s": 1.0 / mean_seq, "rates": seq_rates,
+                             "how": f"dsg_flood per request, service times measured on {n_seq} requests of the same mix, FIFO queue on each rate's arrival times"},
     }
 
 
@@ -221,6 +235,7 @@ def pipeline(count=1 << 26):
     ours = os.path.join(ROOT, "desert-search_b200", "bin", "dsearch_desert")
     ref = os.path.join(ROOT, "oracle", "_ref", "dsearch_desert_gpu")
     out = {"seeds": count, "args": "START=2e13 gate=1 gpu=1 gscan=1", "host_cores": cores}
+    cands = []
 
     def run(exe, threads, td, tag):
         pre = os.path.join(td, tag)
@@ -238,6 +253,8 @@ def pipeline(count=1 << 26):
             res["gated_per_s_after_startup"] = gated / max(1e-9, wall - float(st.group(1)))
         rows = open(pre + ".csv").read().splitlines()[1:]
         seeds = {l.split(",")[0] for l in open(pre + ".seeds.csv").read().splitlines()[1:]}
+        if tag == "ours":                                   # proxy >= 50M rows: the flood batch's large class
+            cands.extend((int(l.split(",")[0]) & ((1 << 64) - 1), int(l.split(",")[6]), int(l.split(",")[7])) for l in rows)
         return res, (rows, seeds)
 
     def compare(a, b):
@@ -264,7 +281,7 @@ def pipeline(count=1 << 26):
                 out["ours_vs_reference"] = compare(a, b)
         else:
             out["reference_gpu_searcher"] = {"unavailable": "oracle/_ref/dsearch_desert_gpu not built"}
-    return out
+    return out, cands
 
 
 def run_ours(args):
@@ -354,8 +371,8 @@ def run_ours(args):
     if world == 1:
         out["cpu_baseline"] = cpu_baseline()
         if not args.no_extras:
-            out["pipeline"] = pipeline()
-            out["flood"] = bench_floods(dsgpu, n_small=1024, rates=args.flood_rates, n_service=args.flood_requests)
+            out["pipeline"], cands = pipeline()
+            out["flood"] = bench_floods(dsgpu, n_small=4096, rates=args.flood_rates, n_service=args.flood_requests, candidates=cands)
     print(json.dumps(out), flush=True)
     if pg:
         pg.destroy_process_group()

@@ -345,7 +345,14 @@ void Search::process(const std::vector<uint64_t> &seeds) {
                     for (int dzz = -1; ok && dzz <= 1; dzz++) for (int dxx = -1; dxx <= 1; dxx++) if (b[(z + dzz) * zn.nx + x + dxx] != 2) { ok = false; break; }
                     if (ok) inner.push_back({(x - cx) * (x - cx) + (z - cz) * (z - cz), c});
                 }
-                std::sort(inner.begin(), inner.end());
+                // only ranks 0, n/3 and 2n/3 of the (distance, cell) order are used; the keys are unique, so
+                // selecting them gives the elements a full sort would put there
+                const size_t ni = inner.size();
+                if (ni) {
+                    std::nth_element(inner.begin(), inner.begin() + 2 * ni / 3, inner.end());
+                    std::nth_element(inner.begin(), inner.begin() + ni / 3, inner.begin() + 2 * ni / 3);
+                    std::nth_element(inner.begin(), inner.begin(), inner.begin() + ni / 3);
+                }
                 auto cell_xy = [&](int c) { return std::pair<int, int>(zn.x0 + (c % zn.nx) * 32, zn.z0 + (c / zn.nx) * 32); };
                 const auto first = inner.empty() ? cell_xy(c0) : cell_xy(inner[0].second);
                 Eval e{zn.rank, first.first, first.second, area};
