@@ -81,6 +81,23 @@ int orc_noise(uint64_t seed, int ch, const double *xyz, int n, double *out) {
     for (int i = 0; i < n; i++) out[i] = S.nz[ch].sample(xyz[3 * i], xyz[3 * i + 1], xyz[3 * i + 2]);
     return 0;
 }
+// FP64 gate amplitudes (pre-gate and full gate, both sides) of n seeds, on `threads` threads: the yardstick
+// of the FP32 gate's error and pass set.
+int orc_gate_fp64(const uint64_t *seeds, int n, double *pre, double *full, int threads) {
+    std::atomic<int> next(0);
+    std::vector<std::thread> pool;
+    for (int t = 0; t < std::max(1, threads); t++)
+        pool.emplace_back([&] {
+            for (int i; (i = next++) < n;)
+                for (int s = 0; s < 2; s++) {
+                    const GateOctave p = gate_octave(seeds[i], s);
+                    pre[2 * i + s] = pregate_side64(p);
+                    full[2 * i + s] = fullgate_side64(p);
+                }
+        });
+    for (auto &t : pool) t.join();
+    return 0;
+}
 // Nearest-leaf node index two ways: the reference's pruned depth-first search (tree_nearest), and the
 // lexicographic minimum of (box distance, node index) over all leaves, the form the device's warp search
 // computes.  Test infrastructure: the two agree when every box below the root contains its children's.

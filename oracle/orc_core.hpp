@@ -518,6 +518,90 @@ inline float fullgate_side(const GateOctave &p, const float *k15) {
     }
     return blur_max(S, 512, 7, k15);
 }
+// The same two gate stages carried out entirely in double precision (corner tables, sums, taps, blur, norm):
+// the FP64 yardstick against which the FP32 gate's error and pass set are measured.  Not a restatement of a
+// reference function (the reference gate is FP32); same algorithm, wider arithmetic.
+inline double blur_max64(const std::vector<double> &S, int G, int R, double sig) {
+    std::vector<double> k(2 * R + 1), H(S.size());
+    double ks = 0;
+    for (int d = -R; d <= R; d++) { k[d + R] = std::exp(-0.5 * d * d / (sig * sig)); ks += k[d + R]; }
+    for (int r = 0; r < G; r++) for (int i = 0; i < G; i++) {
+        double s = 0;
+        for (int d = 0; d <= 2 * R; d++) s = std::fma(k[d], S[size_t(r) * G + ((i + d - R) & (G - 1))], s);
+        H[size_t(r) * G + i] = s;
+    }
+    double best = -1e300;
+    for (int o = 0; o < G; o++) for (int i = 0; i < G; i++) {
+        double s = 0;
+        for (int d = 0; d <= 2 * R; d++) s = std::fma(k[d], H[size_t((o - R + d) & (G - 1)) * G + i], s);
+        best = std::max(best, s / (ks * ks));
+    }
+    return best;
+}
+inline double gate_weight64() { return 1.25 * (32.0 / 63.0) * 1.5; }
+inline double pregate_side64(const GateOctave &p) {
+    double fr[2][2]; int sh[2][2];
+    for (int ax = 0; ax < 2; ax++) {
+        const double o = ax ? p.oz : p.ox;
+        for (int q = 0; q < 2; q++) { const double b = o + 0.5 * q; fr[ax][q] = b - std::floor(b); sh[ax][q] = int(std::floor(b) - std::floor(o)); }
+    }
+    double tab[288];
+    for (int e = 0; e < 288; e++) {
+        const int h = e & 15, dy = (e >> 4) & 1, uv = e >> 5, u = uv / 3, v = uv % 3;
+        double acc = 0;
+        for (int px = 0; px < 2; px++) for (int pz = 0; pz < 2; pz++) {
+            const int dx = u - sh[0][px], dz = v - sh[1][pz];
+            if (dx < 0 || dx > 1 || dz < 0 || dz > 1) continue;
+            const double fx = fr[0][px], fz = fr[1][pz], tx = fade_fused(fx), tz = fade_fused(fz);
+            const double wc = (dx ? tx : 1 - tx) * (dy ? p.vy : 1 - p.vy) * (dz ? tz : 1 - tz);
+            acc = std::fma(wc, grad(h, fx - dx, p.fy - dy, fz - dz), acc);
+        }
+        tab[e] = 0.25 * gate_weight64() * acc;
+    }
+    uint8_t col[2][256];
+    for (int c = 0; c < 256; c++) for (int dy = 0; dy < 2; dy++) col[dy][c] = p.perm[(p.perm[c] + p.iy + dy) & 255];
+    const int ix0 = int(std::floor(p.ox)), iz0 = int(std::floor(p.oz));
+    std::vector<double> S(256 * 256);
+    for (int r = 0; r < 256; r++) for (int i = 0; i < 256; i++) {
+        double acc = 0;
+        for (int v = 0; v < 3; v++) for (int dy = 0; dy < 2; dy++) for (int u = 0; u < 3; u++)
+            acc += tab[((u * 3 + v) * 2 + dy) * 16 + (p.perm[(col[dy][(i + u + ix0) & 255] + r + v + iz0) & 255] & 15)];
+        S[size_t(r) * 256 + i] = acc;
+    }
+    return blur_max64(S, 256, 4, 1.0);
+}
+inline double fullgate_side64(const GateOctave &p) {
+    double tab[4][8][16];
+    int ix0[2], iz0[2];
+    for (int par = 0; par < 2; par++) { ix0[par] = int(std::floor(par * 0.5 + p.ox)); iz0[par] = int(std::floor(par * 0.5 + p.oz)); }
+    for (int px = 0; px < 2; px++) for (int pz = 0; pz < 2; pz++) {
+        const double bx = px * 0.5 + p.ox, bz = pz * 0.5 + p.oz;
+        const double fx = bx - std::floor(bx), fz = bz - std::floor(bz);
+        const double tx = fade_fused(fx), tz = fade_fused(fz), ty = p.vy;
+        for (int c = 0; c < 8; c++) {
+            const int dx = c & 1, dy = (c >> 1) & 1, dz = c >> 2;
+            const double wc = (dx ? tx : 1 - tx) * (dy ? ty : 1 - ty) * (dz ? tz : 1 - tz);
+            for (int h = 0; h < 16; h++) tab[px * 2 + pz][c][h] = gate_weight64() * wc * grad(h, fx - dx, p.fy - dy, fz - dz);
+        }
+    }
+    uint8_t col[2][256];
+    for (int c = 0; c < 256; c++) for (int dy = 0; dy < 2; dy++) col[dy][c] = p.perm[(p.perm[c] + p.iy + dy) & 255];
+    std::vector<double> S(512 * 512);
+    for (int j = 0; j < 512; j++) {
+        const int pz = j & 1, iz = (j >> 1) + iz0[pz];
+        for (int i = 0; i < 512; i++) {
+            const int px = i & 1, ix = (i >> 1) + ix0[px];
+            double acc = 0;
+            for (int c = 0; c < 8; c++) {
+                const int dx = c & 1, dy = (c >> 1) & 1, dz = c >> 2;
+                acc += tab[px * 2 + pz][c][p.perm[(col[dy][(ix + dx) & 255] + iz + dz) & 255] & 15];
+            }
+            S[size_t(j) * 512 + i] = acc;
+        }
+    }
+    return blur_max64(S, 512, 7, 2.0);
+}
+
 struct GateResult { double phase; float pre[2], full[2], pre_amp, full_amp; };
 inline GateResult gate_eval(uint64_t seed, bool want_full, const float *k9 = nullptr, const float *k15 = nullptr) {
     float t9[9], t15[15];

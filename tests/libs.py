@@ -180,6 +180,15 @@ def ref_gpu_taps():
     return t[:9].copy(), t[9:].copy()
 
 
+def orc_gate_fp64(seeds, threads=8):
+    """Double-precision pre-gate and full-gate side amplitudes (n, 2) each: the FP64 yardstick."""
+    lib = orc().lib
+    s = np.ascontiguousarray(seeds, dtype=np.uint64)
+    pre = np.empty(2 * len(s)); full = np.empty(2 * len(s))
+    lib.orc_gate_fp64(ptr(s, u64p), C.c_int(len(s)), ptr(pre, f64p), ptr(full, f64p), C.c_int(threads))
+    return pre.reshape(-1, 2), full.reshape(-1, 2)
+
+
 def orc_gate_range(start, count, maxph=0.06, pthr=0.645, amp=0.70, threads=8, cap=1 << 16):
     """The whole gate over mix(start + k) on the CPU with the reference GPU gate's taps."""
     lib = orc().lib
