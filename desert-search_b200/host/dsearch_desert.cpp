@@ -48,6 +48,7 @@ struct Params {                                    // dsearch_desert.cpp:50-78 (
     int study = 0, gpu = 0, gpucheck = 0, gscan = 0, gscancheck = 0, gate = 0;
     double gate_phase = 0.06, gate_amp = 0.70, gate_pthr = 0.645;
     int from_stdin = 0;
+    int verified = 0;                              // this build only: verify CANDIDATEs in-process (PREFIX.verified)
 };
 
 // A cell i of a side-A table translated by t periods -> B table cell (dsearch_desert.cpp:98-113).
@@ -86,6 +87,13 @@ struct Search {
     std::atomic<double> t_tab{0}, t_scan{0}, t_site{0}, t_proxy{0}, t_hot{0}, t_gpu{0}, t_exact{0}, t_pre{0}, t_wave{0}, t_hq{0};
     Clock::time_point begin = Clock::now(), last = begin;
     std::atomic<int> gscan_checks{0};
+    // verified=1: every CANDIDATE's exact step-1 flood goes to the flood service as it is printed; a thread
+    // appends "TIME RUN LINE => RESULT" lines to PREFIX.verified in the format deploy/gpipe.sh:7-10 writes
+    // (RESULT as bin/mcmeasure prints it), which scripts/log_finds.py and deploy/status.py parse
+    struct Pending { uint64_t ticket; std::string line; int x, z; };
+    std::mutex vmu; std::condition_variable vcv; std::deque<Pending> vq; bool vdone = false;
+    FILE *vout = nullptr; std::string run;
+    void verify_loop();
     std::vector<float> kT, kC; int rT = 0, rC = 0;
     float prob[1600];
 
@@ -103,6 +111,29 @@ static uint64_t scan_order(const dsg_cand &c) {
     const int i = ((c.x % PERIOD) + PERIOD) % PERIOD / CELL, tx = int(std::floor(double(c.x) / PERIOD)) - KMIN;
     const int j = ((c.z % PERIOD) + PERIOD) % PERIOD / CELL, tz = int(std::floor(double(c.z) / PERIOD)) - KMIN;
     return (uint64_t(j) << 32) | (uint64_t(i) << 16) | (uint64_t(tz) << 8) | uint64_t(tx);
+}
+
+void Search::verify_loop() {
+    for (;;) {
+        Pending p;
+        {
+            std::unique_lock<std::mutex> l(vmu);
+            vcv.wait(l, [&] { return !vq.empty() || vdone; });
+            if (vq.empty()) return;
+            p = vq.front(); vq.pop_front();
+        }
+        dsg_area a{};
+        ck(dsg_service_wait(p.ticket, &a, -1), "verify wait");
+        char res[256];
+        if (a.cells == 0) snprintf(res, sizeof res, "Biome at (%d, 256, %d) is not Desert | 1:4 Size: 0 | Blocks^2 Size: 0", p.x, p.z);
+        else snprintf(res, sizeof res, "Biome: Desert at (%d, 256, %d) | 1:4 Size: %llu | Blocks^2 Size: %llu%s", p.x, p.z,
+                      (unsigned long long)a.cells, (unsigned long long)(a.cells * 16), a.edge ? " | window edge reached" : "");
+        char ts[32];
+        const time_t now = time(nullptr);
+        strftime(ts, sizeof ts, "%Y-%m-%dT%H:%M:%SZ", gmtime(&now));
+        fprintf(vout, "%s %s %s => %s \n", ts, run.c_str(), p.line.c_str(), res);
+        fflush(vout);
+    }
 }
 
 void Search::process(const std::vector<uint64_t> &seeds) {
@@ -430,8 +461,20 @@ void Search::process(const std::vector<uint64_t> &seeds) {
             if (e.nostart) continue;                       // no desert start near this component (:517)
             const double v = e.s4 > 0 ? e.s4 : e.s8;
             seed_best = std::max(seed_best, v);
-            if (e.s4 >= P.verify_mb)
-                fprintf(stderr, "CANDIDATE step4=%.2fM seed=%lld x=%d z=%d -> verify with exact flood (Y=256)\n", e.s4, seed, e.x * 4 + 2, e.z * 4 + 2);
+            if (e.s4 >= P.verify_mb) {
+                char line[256];
+                snprintf(line, sizeof line, "CANDIDATE step4=%.2fM seed=%lld x=%d z=%d -> verify with exact flood (Y=256)", e.s4, seed, e.x * 4 + 2, e.z * 4 + 2);
+                fprintf(stderr, "%s\n", line);
+                if (P.verified) {
+                    const int bx = e.x * 4 + 2, bz = e.z * 4 + 2;
+                    const dsg_flood_req q{seeds[s], bx >> 2, bz >> 2, 1, 20000, 0, DSG_PRED_DESERT, 0.f, 0};
+                    uint64_t ticket = 0;
+                    ck(dsg_service_submit(&q, &ticket), "verify submit");
+                    std::lock_guard<std::mutex> vl(vmu);
+                    vq.push_back({ticket, line, bx, bz});
+                    vcv.notify_all();
+                }
+            }
             if (v > best) {
                 best = v;
                 fprintf(stderr, "best %.2fM (step %d) seed=%lld x=%d z=%d proxy=%.1fM\n", v, e.s4 > 0 ? 4 : 8, seed, e.x * 4 + 2, e.z * 4 + 2, e.proxy);
@@ -478,6 +521,7 @@ int main(int argc, char **argv) {
         else if (k == "hot_pre") P.hot_pre = v; else if (k == "gate") P.gate = int(v); else if (k == "gscan") P.gscan = int(v);
         else if (k == "gscancheck") P.gscancheck = int(v); else if (k == "gate_phase") P.gate_phase = v; else if (k == "gate_amp") P.gate_amp = v;
         else if (k == "gate_pthr") P.gate_pthr = v; else if (k == "refine") P.refine_mb = v; else if (k == "verify") P.verify_mb = v;
+        else if (k == "verified") P.verified = int(v);
         else { fprintf(stderr, "unknown key %s\n", k.c_str()); return 2; }
     }
     if ((P.gscan || P.gscancheck) && !P.gpu) { fprintf(stderr, "gscan=1 needs gpu=1\n"); return 2; }
@@ -504,6 +548,16 @@ int main(int argc, char **argv) {
         hostcheck::scan_tmaps(&TMT.ib[0][0], TMT.lo, TMT.hi, &TMC.ib[0][0]);
     }
     ck(dsg_proxy_table(S.prob), "proxy table");
+    std::thread verifier;
+    if (P.verified) {
+        S.vout = fopen((prefix + ".verified").c_str(), "wx");
+        if (!S.vout) { fprintf(stderr, "cannot create %s.verified (exists?)\n", prefix.c_str()); return 2; }
+        const size_t slash = prefix.find_last_of('/');
+        S.run = slash == std::string::npos ? prefix : prefix.substr(slash + 1);
+        const dsg_service_cfg cfg{uint64_t(16) << 30, 1024, 4};
+        ck(dsg_service_open(&cfg), "flood service");
+        verifier = std::thread([&] { S.verify_loop(); });
+    }
     const double t_ready = std::chrono::duration<double>(Clock::now() - S.begin).count();
     S.gscan_checks = P.gscancheck;
     // ---- seed source: GPU gate thread, stdin reader, or the enumerated range through the GPU gate
@@ -577,6 +631,12 @@ int main(int argc, char **argv) {
     for (auto &t : pool) t.join();
     if (source.joinable()) { if (qdone) source.join(); else source.detach(); }
     fclose(S.out); fclose(S.sout);
+    if (verifier.joinable()) {                             // every candidate's line is written before the exit
+        { std::lock_guard<std::mutex> vl(S.vmu); S.vdone = true; S.vcv.notify_all(); }
+        verifier.join();
+        fclose(S.vout);
+        dsg_service_close();
+    }
     const double sec = std::chrono::duration<double>(Clock::now() - S.begin).count();
     FILE *m = fopen((prefix + ".json").c_str(), "w");
     fprintf(m, "{\"start\":%llu,\"done\":%llu,\"passed\":%llu,\"scanned\":%llu,\"amp\":%g,\"sites\":%llu,\"seconds\":%.3f,\"threads\":%d,\"phase\":%g,\"sigma\":%g,"

@@ -107,3 +107,27 @@ def test_dsearch_matches_reference_gpu_searcher(tmp_path):
             assert r["s4"] == q["s4"] and r["s8"] == q["s8"]
     cand = lambda s: sorted(re.findall(r"CANDIDATE step4=[\d.]+M seed=-?\d+ x=-?\d+ z=-?\d+", s))
     assert set(cand(a.stderr)) >= set(cand(b.stderr)) or set(cand(a.stderr)) <= set(cand(b.stderr))
+
+
+def test_searcher_verifies_candidates_in_process(tmp_path, dsg):
+    """verified=1: each CANDIDATE's exact step-1 flood runs on the flood service during the search, and
+    PREFIX.verified gets the line deploy/gpipe.sh would append after bin/mcmeasure, in the fields
+    scripts/log_finds.py parses; the areas equal dsg_flood's from the same starts."""
+    seeds = "".join(f"{f['seed']}\n" for f in finds()[:16])
+    pre = str(tmp_path / "v")
+    a = run([os.path.join(BIN, "dsearch_desert"), "0", "0", pre, "8", "stdin=1", "gpu=1", "gscan=1", "verified=1"], stdin=seeds)
+    assert a.returncode == 0, a.stderr[-2000:]
+    cands = [l for l in a.stderr.splitlines() if l.startswith("CANDIDATE")]
+    lines = open(pre + ".verified").read().splitlines()
+    assert cands and len(lines) == len(cands)
+    pat = re.compile(r'^(\S+) (\S+) CANDIDATE step4=([\d.]+)M seed=(-?\d+) x=(-?\d+) z=(-?\d+).*1:4 Size: (\d+) \| Blocks\^2 Size: (\d+)')
+    got = {}
+    for l in lines:
+        m = pat.search(l)
+        assert m, l
+        ts, run_name, s4, seed, x, z, cells, b2 = m.groups()
+        assert run_name == "v" and int(b2) == 16 * int(cells)
+        got[(int(seed), int(x), int(z))] = int(cells)
+    reqs = [dsg.flood_req(s & ((1 << 64) - 1), x >> 2, z >> 2, 1, 20000) for (s, x, z) in got]
+    for (k, cells), area in zip(got.items(), dsg.flood_batch(reqs)):
+        assert cells == area[0], k
