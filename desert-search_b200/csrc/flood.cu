@@ -101,7 +101,7 @@ int run_batch(const dsg_flood_req *reqs, uint32_t n, dsg_area *out, size_t pool_
     DSG_CU(cudaMemsetAsync(g.d_dir, 0xFF, dir_total * 4, st));
     DSG_CU(cudaMemsetAsync(g.d_cnt, 0, 16 * 4, st));
     DSG_CU(cudaMemsetAsync(g.d_evals, 0, 8, st));
-    const TileAlloc ta{nullptr, 0, g.pool.cap, g.pool.cap, g.d_cnt + 9, nullptr, 0};
+    const TileAlloc ta{nullptr, 0, g.pool.cap, g.pool.cap, g.d_cnt + 9, nullptr, nullptr};
     k_tile_start<<<(n + 127) / 128, 128, 0, st>>>(g.d_ctl, nullptr, n, g.d_stat, g.d_dir, g.pool.T, ta, g.pool.n_list[0], g.d_cnt + 0,
                                                   0, nullptr, g.d_cnt + 10);
     DSG_CU(cudaGetLastError());

@@ -48,9 +48,10 @@ constexpr int EVAL_THREADS = SUB * SUB;
 
 // Tiles come from a pool: the k-th tile taken since the last host update is ring[(head + k) % cap]
 // (ring == nullptr: tile k itself, a bump allocator).  Taking never waits; `avail` bounds it.
-// returned (service only): a tile taken by a thread that then lost the directory race goes back to the ring
-// at (tail + k) % cap, k counted by *returned (those ring positions are free while head..head+avail are not).
-struct TileAlloc { uint32_t *ring; uint32_t head, avail, cap; uint32_t *taken; uint32_t *returned; uint32_t tail; };
+// lost (service only): a tile taken by a thread that then lost the directory race is written to lost[k], k
+// counted by *returned; the host appends lost[0..k) to the ring at tail once the rounds have ended.  (Writing
+// it to the ring directly could overwrite a slot that another claim has been assigned but not yet read.)
+struct TileAlloc { uint32_t *ring; uint32_t head, avail, cap; uint32_t *taken; uint32_t *returned; uint32_t *lost; };
 // Per-tile storage, all zero while a tile is free.  bits: tile t holds P rows at [t*192, +64), D rows at +64,
 // R rows at +128 (bit c of row r = cell (64*ti + c, 64*tj + r) of the window).  emask / qmask: sub-blocks
 // evaluated / requested.  mark: 1 + the round the tile was last queued for connect.
@@ -90,7 +91,7 @@ __device__ inline int32_t claim_tile(const FloodCtl &c, uint32_t r, int ti, int 
     const int32_t nt = int32_t(ta.ring ? ta.ring[(ta.head + k) % ta.cap] : k);
     const int32_t old = atomicCAS(e, -1, nt);
     if (old != -1) {
-        if (ta.returned) ta.ring[(ta.tail + atomicAdd(ta.returned, 1u)) % ta.cap] = uint32_t(nt);
+        if (ta.returned) ta.lost[atomicAdd(ta.returned, 1u)] = uint32_t(nt);
         return old;
     }
     T.owner[nt] = r;

@@ -23,6 +23,10 @@ namespace flood {
 namespace {
 
 __global__ void k_iota(uint32_t *a, uint32_t n) { for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) a[i] = i; }
+// Tiles lost in directory races during the rounds go back to the free ring at tail, tail + 1, ...
+__global__ void k_ring_append(const uint32_t *__restrict__ lost, uint32_t n, uint32_t *__restrict__ ring, uint32_t cap, uint32_t tail) {
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) ring[(tail + i) % cap] = lost[i];
+}
 
 struct Ticket { dsg_area area{}; int status = 2; };        // 2 = pending
 
@@ -46,7 +50,7 @@ struct Service {
     uint32_t *d_active = nullptr, *h_active = nullptr;
     int32_t *d_dir = nullptr; int64_t dir_cap = 0;
     TilePool pool;
-    uint32_t *d_ring = nullptr; uint32_t head = 0, avail = 0;
+    uint32_t *d_ring = nullptr, *d_lost = nullptr; uint32_t head = 0, avail = 0;
     uint32_t *d_ctr = nullptr, *h_ctr = nullptr;               // [0] taken, [1] returned, [2..10] round counters (launch_round), [11] error flags
     unsigned long long *d_evals = nullptr;                     // sub-blocks evaluated since open
     uint32_t *d_slots = nullptr; uint64_t *d_seeds = nullptr;
@@ -109,7 +113,8 @@ void engine_loop(Service &g) {
         }
         try {
             cudaStream_t st = g.st;
-            const TileAlloc ta{g.d_ring, g.head, g.avail, cap, g.d_ctr + 0, g.d_ctr + 1, (g.head + g.avail) % cap};
+            const uint32_t tail = (g.head + g.avail) % cap;           // first empty ring slot; fixed until avail grows
+            const TileAlloc ta{g.d_ring, g.head, g.avail, cap, g.d_ctr + 0, g.d_ctr + 1, g.d_lost};
             if (!adm_slots.empty()) {
                 const uint32_t na = uint32_t(adm_slots.size());
                 DSG_CU(cudaMemcpyAsync(g.d_seeds, adm_seeds.data(), na * 8, cudaMemcpyHostToDevice, st));
@@ -135,6 +140,10 @@ void engine_loop(Service &g) {
             DSG_CU(cudaStreamSynchronize(st));
             const uint32_t taken = std::min(g.h_ctr[0], g.avail);
             uint32_t returned = g.h_ctr[1];
+            if (returned) {
+                k_ring_append<<<(returned + 255) / 256, 256, 0, st>>>(g.d_lost, returned, g.d_ring, cap, tail);
+                DSG_CU(cudaGetLastError());
+            }
             g.head = (g.head + taken) % cap;
             g.avail -= taken;
             // finished requests: nothing queued for the next round
@@ -149,7 +158,7 @@ void engine_loop(Service &g) {
                 // statistics, then release; the returned counter continues from the tiles lost in directory races
                 const dim3 grid(unsigned(fin.size()), dir_chunks(g.dir_max));
                 k_tile_finish<<<grid, 256, 0, st>>>(g.d_ctl, g.d_slots, g.d_dir, g.pool.T, g.d_stat);
-                k_tile_release<<<grid, 256, 0, st>>>(g.d_ctl, g.d_slots, g.d_dir, g.pool.T, g.d_ring, cap, (g.head + g.avail) % cap, g.d_ctr + 1);
+                k_tile_release<<<grid, 256, 0, st>>>(g.d_ctl, g.d_slots, g.d_dir, g.pool.T, g.d_ring, cap, tail, g.d_ctr + 1);
                 DSG_CU(cudaGetLastError());
                 for (size_t k = 0; k < fin.size(); k++) DSG_CU(cudaMemcpyAsync(&fs[k], g.d_stat + fin[k], sizeof(FloodStat), cudaMemcpyDeviceToHost, st));
                 DSG_CU(cudaMemcpyAsync(g.h_ctr + 1, g.d_ctr + 1, 4, cudaMemcpyDeviceToHost, st));
@@ -222,9 +231,10 @@ extern "C" int dsg_service_open(const dsg_service_cfg *cfg_in) {
         DSG_CU(cudaMalloc(&g.d_dir, size_t(g.dir_cap) * 4));
         g.dir_free = {{0, g.dir_cap}};
         g.dir_max = 0;
-        const uint32_t tiles = uint32_t(std::min<uint64_t>((c.budget_bytes - c.budget_bytes / 4) / (TilePool::kBytesPerTile + 4), 0x7fffffffu));
+        const uint32_t tiles = uint32_t(std::min<uint64_t>((c.budget_bytes - c.budget_bytes / 4) / (TilePool::kBytesPerTile + 8), 0x7fffffffu));
         g.pool.allocate(tiles);
         DSG_CU(cudaMalloc(&g.d_ring, size_t(tiles) * 4));
+        DSG_CU(cudaMalloc(&g.d_lost, size_t(tiles) * 4));
         k_iota<<<1024, 256>>>(g.d_ring, tiles);
         DSG_CU(cudaGetLastError());
         g.head = 0; g.avail = tiles;
@@ -317,7 +327,7 @@ extern "C" int dsg_service_close(void) {
         std::lock_guard<std::mutex> l(g.mu);
         cudaStreamSynchronize(g.st);
         cudaFree(g.d_ctl); cudaFree(g.d_stat); cudaFree(g.d_noise); cudaFree(g.d_noise_stage); cudaFree(g.d_active); cudaFreeHost(g.h_active);
-        cudaFree(g.d_slots); cudaFree(g.d_seeds); cudaFree(g.d_dir); cudaFree(g.d_ring); cudaFree(g.d_ctr);
+        cudaFree(g.d_slots); cudaFree(g.d_seeds); cudaFree(g.d_dir); cudaFree(g.d_ring); cudaFree(g.d_lost); cudaFree(g.d_ctr);
         cudaFreeHost(g.h_ctr); cudaFree(g.d_evals);
         g.pool.release();
         cudaStreamDestroy(g.st);

@@ -70,3 +70,32 @@ def test_service_reopen_and_poll(dsg):
         assert all(got[i] == (0, want[i]) for i in range(len(ts)))
     finally:
         svc.close()
+
+
+def test_service_overflow_reports_and_recovers(dsg):
+    """A request that outgrows the tile pool retires as DSG_OVERFLOW (not an error); its tiles go back to
+    the pool, and the same service then answers every fixture flood exactly.  Budget 2 MiB: 925 tiles of
+    64 x 64 cells (3.8M cells) against the 6.3M-cell step-1 find in a 16,001-quart window."""
+    reqs, want = fixture_reqs(dsg)
+    finds = json.load(open(os.path.join(G, "finds.json")))
+    f = max(finds, key=lambda x: x["cells"])
+    assert f["cells"] > 6_000_000
+    big = dsg.flood_req(f["seed"], f["x"] >> 2, f["z"] >> 2, 1, 8000)
+    svc = dsg.Service(budget_bytes=2 << 20, max_requests=64, rounds_per_check=4)
+    try:
+        rc, a = svc.wait(svc.submit(big), timeout_ms=120_000)
+        assert rc == dsg.DSG_OVERFLOW and 0 < a[0] < f["cells"]
+        # concurrently with a second overflowing request, small ones either finish exactly or overflow too
+        tb = svc.submit(big)
+        ts = [svc.submit(q) for q in reqs]
+        assert svc.wait(tb, timeout_ms=120_000)[0] == dsg.DSG_OVERFLOW
+        for t, w in zip(ts, want):
+            rc, a = svc.wait(t, timeout_ms=120_000)
+            assert rc == dsg.DSG_OVERFLOW or (rc == 0 and a == w)
+        # with the pool returned, all of them again, one at a time, exactly
+        for q, w in zip(reqs, want):
+            assert svc.wait(svc.submit(q), timeout_ms=120_000) == (0, w)
+        st = svc.stats()
+        assert st["inflight"] == 0 and st["queued"] == 0 and st["overflowed"] >= 2
+    finally:
+        svc.close()
