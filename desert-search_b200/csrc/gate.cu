@@ -2,9 +2,10 @@
 // amplitude gate.  Restates src/gpu/gate.cuh (k_phase, k_init, k_amp2) with the same per-cell arithmetic
 // (summation orders, fused multiply-adds of the blur chains, device expf taps), so amplitudes match the
 // reference's GPU gate bit for bit, on a different schedule:
-//  * pre-gate: one CTA per (seed, side) pair inside a 2-CTA cluster; each warp owns a 64-row band of its
+//  * pre-gate: one CTA per (seed, side) pair inside a 2-CTA cluster; each warp owns a 128-row band of its
 //    side's 256^2 grid and streams it with all state in registers (a lane holds 8 columns: hashes, samples,
 //    the horizontal blur through lane shuffles, and the vertical blur as 8 pending FMA chains per column).
+//    Hash rows come 4 at a time from a table of packed row words (one load per column per 4 rows).
 //    No block barrier inside a side; the two side maxima meet through distributed shared memory.
 //  * full gate: one 512-thread CTA per (seed, side) in a 2-CTA cluster, thread = column, row blocks of 8
 //    staged in shared memory; the vertical blur again accumulates in registers.
@@ -28,7 +29,7 @@ static_assert(sizeof(Oct) == 304, "Oct layout");
 // Blur taps and normalisers, passed by value (they live in the kernel-parameter constant bank).
 struct Taps { float k9[9], k15[15], norm9, norm15, w; };
 
-constexpr int PG_THREADS = 128, PG_BAND = 64;        // pre-gate: 4 warps x 64 rows = 256 rows per side
+constexpr int PG_THREADS = 64, PG_BAND = 256 / (PG_THREADS / 32);   // pre-gate: 2 warps x 128 rows per side
 constexpr int FG_THREADS = 128, FG_RB = 8;           // full gate: thread per 4 columns, 8-row blocks
 
 // ---------------------------------------------------------------- device math
@@ -111,20 +112,28 @@ __global__ void __launch_bounds__(128) k_octinit(const uint64_t *__restrict__ se
     }
 }
 
-// Hashes x4 (byte offsets into a 16-float table group) of one grid row for the lane's 10 lattice columns.
-// cv[dy][k] packs col[dy][c_t] for t = 4k..4k+3; columns t = 8, 9 come from the next lane (periodic).
-__device__ __forceinline__ void hash_row(const uint8_t *__restrict__ sP2, const uint32_t (&cv)[2][2], int mz, int lane, uint32_t (&h)[2][3]) {
+// Hashed rows of the pre-gate.  sW[i] packs the byte offsets (P[(i + b) & 255] & 15) * 4 for b = 0..3, so the
+// offsets of one lattice column for 4 consecutive rows come from one word: sW[c + m] (c = the column's hash
+// P[P[x] + y], m = the first row).  W[dy][t] holds such a word for the lane's column t; hash_row gathers byte
+// j (the row within the group) of the 4 columns of each word group into h[dy][0..1] and takes the next
+// lane's first group as h[dy][2] (columns 8..11, periodic in 256).
+constexpr int PG_SW = 528 + PG_BAND;         // > c + m0 + k for k <= PG_BAND + 9
+static_assert(PG_SW > 255 + 255 + 4 * ((PG_BAND + 9) / 4), "sW covers every group load");
+__device__ __forceinline__ void load_group(const uint32_t *__restrict__ sW, const uint32_t (&cv)[2][2], int base, uint32_t (&W)[2][8]) {
+    #pragma unroll
+    for (int dy = 0; dy < 2; dy++)
+        #pragma unroll
+        for (int t = 0; t < 8; t++) W[dy][t] = sW[((cv[dy][t >> 2] >> (8 * (t & 3))) & 255u) + base];
+}
+__device__ __forceinline__ void hash_row(const uint32_t (&W)[2][8], int j, int lane, uint32_t (&h)[2][3]) {
+    const uint32_t sel = uint32_t(j) * 0x11u + 0x40u;           // byte j of the first and of the second word
     #pragma unroll
     for (int dy = 0; dy < 2; dy++) {
         #pragma unroll
         for (int k = 0; k < 2; k++) {
-            uint32_t w = 0;
-            #pragma unroll
-            for (int b = 0; b < 4; b++) {
-                const uint32_t c = (cv[dy][k] >> (8 * b)) & 255u;
-                w |= uint32_t(sP2[c + mz] & 15) << (8 * b + 2);
-            }
-            h[dy][k] = w;
+            const uint32_t lo = __byte_perm(W[dy][4 * k], W[dy][4 * k + 1], sel);
+            const uint32_t hi = __byte_perm(W[dy][4 * k + 2], W[dy][4 * k + 3], sel);
+            h[dy][k] = __byte_perm(lo, hi, 0x5410u);
         }
         h[dy][2] = __shfl_sync(0xffffffffu, h[dy][0], (lane + 1) & 31);
     }
@@ -132,13 +141,14 @@ __device__ __forceinline__ void hash_row(const uint8_t *__restrict__ sP2, const 
 __device__ __forceinline__ uint32_t hbyte(const uint32_t (&h)[3], int t) { return (h[t >> 2] >> (8 * (t & 3))) & 255u; }
 
 // Anti-aliased pre-gate (gate.cuh stream_max<256,4,8,true>).  Cluster rank = noise side.
-__global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(PG_THREADS, 4)
+__global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(PG_THREADS, 6)
 k_pregate(const Oct *__restrict__ oct, const uint64_t *__restrict__ seeds, const uint32_t *__restrict__ n_in, uint32_t cap_in,
           float thr, Taps tp, uint64_t *__restrict__ out_seed, uint32_t *__restrict__ out_idx, uint32_t *__restrict__ n_out,
           uint32_t cap_out, float *__restrict__ side_amp) {
     __shared__ __align__(16) float sTc[288];
     __shared__ __align__(16) uint8_t sP2[512];
     __shared__ __align__(16) uint8_t sCol[2][256];
+    __shared__ __align__(16) uint32_t sW[PG_SW];
     __shared__ float sRed[PG_THREADS / 32];
     __shared__ float sPeer[2];
     cg::cluster_group cl = cg::this_cluster();
@@ -159,6 +169,12 @@ k_pregate(const Oct *__restrict__ oct, const uint64_t *__restrict__ seeds, const
             const int pc = sP2[c];
             sCol[0][c] = sP2[pc + (iy & 255)];
             sCol[1][c] = sP2[pc + ((iy + 1) & 255)];
+        }
+        for (int i = tid; i < PG_SW; i += PG_THREADS) {
+            uint32_t w = 0;
+            #pragma unroll
+            for (int b = 0; b < 4; b++) w |= uint32_t(sP2[(i + b) & 255] & 15) << (8 * b + 2);
+            sW[i] = w;
         }
         {   // 18 merged corner tables of 16 gradients: 4 half-lattice parities averaged (gate.cuh:218-235)
             double fr[2][2]; int sh[2][2];
@@ -196,12 +212,16 @@ k_pregate(const Oct *__restrict__ oct, const uint64_t *__restrict__ seeds, const
                 for (int b = 0; b < 4; b++) w |= uint32_t(sCol[dy][(8 * lane + ix0 + 4 * k + b) & 255]) << (8 * b);
                 cv[dy][k] = w;
             }
-        // ---- stream this warp's band: output rows [o0, o0 + 64) need sample rows o0-4 .. o0+67
+        // ---- stream this warp's band: output rows [o0, o0 + PG_BAND) need sample rows o0-4 .. o0+PG_BAND+3,
+        // i.e. hash rows k = 0 .. PG_BAND+9 from m0 = o0 - 4 + iz0 (mod 256), in word groups of 4
         const int o0 = warp * PG_BAND;
+        const int m0 = (o0 - 4 + iz0) & 255;
         float best = -1e9f;
+        uint32_t W[2][8];
         uint32_t hA[2][3], hB[2][3], hC[2][3];
-        hash_row(sP2, cv, (o0 - 4 + iz0) & 255, lane, hA);
-        hash_row(sP2, cv, (o0 - 3 + iz0) & 255, lane, hB);
+        load_group(sW, cv, m0, W);
+        hash_row(W, 0, lane, hA);
+        hash_row(W, 1, lane, hB);
         float pend[8][8];
         #pragma unroll
         for (int j = 0; j < 8; j++)
@@ -209,7 +229,9 @@ k_pregate(const Oct *__restrict__ oct, const uint64_t *__restrict__ seeds, const
             for (int e = 0; e < 8; e++) pend[j][e] = 0.f;
         const char *tcb = reinterpret_cast<const char *>(sTc);
         for (int r = o0 - 4; r < o0 + PG_BAND + 4; r++) {
-            hash_row(sP2, cv, (r + 2 + iz0) & 255, lane, hC);
+            const int k = r - o0 + 6;                            // hash row of sample row r + 2
+            if ((k & 3) == 0) load_group(sW, cv, m0 + k, W);
+            hash_row(W, k & 3, lane, hC);
             // samples: for each (v, dy) hash row, unpack its 10 bytes once, then add the three u terms of
             // all 8 cells; each cell still sums in the order v, dy, u (gate.cuh:274-281)
             float S[8];
