@@ -314,7 +314,8 @@ k_fullgate(const Oct *__restrict__ oct, const uint64_t *__restrict__ seeds, cons
     __shared__ __align__(16) float sTc[512];
     __shared__ __align__(16) uint8_t sP2[512];
     __shared__ __align__(16) uint8_t sCol[2][256];
-    __shared__ __align__(16) uint32_t sHk[FG_RB][256];     // byte q = dy*2 + dz: hash of corner (dy, dz)
+    __shared__ __align__(16) uint32_t sHk[FG_RB][256];     // byte q = dy*2 + dz: 4 x hash of corner (dy, dz)
+    __shared__ __align__(16) uint16_t sH2[512];            // 4 x (P[i & 255] & 15), 4 x (P[(i + 1) & 255] & 15)
     __shared__ __align__(16) float sV[FG_RB][512];
     __shared__ float sRed[FG_THREADS / 32];
     __shared__ float sPeer[2];
@@ -340,6 +341,11 @@ k_fullgate(const Oct *__restrict__ oct, const uint64_t *__restrict__ seeds, cons
             sCol[1][c] = sP2[pc + ((iy + 1) & 255)];
         }
         #pragma unroll
+        for (int h = 0; h < 4; h++) {
+            const int i = tid + 128 * h;
+            sH2[i] = uint16_t((sP2[i & 255] & 15) << 2 | (sP2[(i + 1) & 255] & 15) << 10);
+        }
+        #pragma unroll
         for (int m = 0; m < 4; m++) {   // corner tables per parity (gate.cuh:237-244): Tc[(px*2+pz)*128 + c*16 + h]
             const int e = tid + 128 * m, par = e >> 7, c = (e >> 4) & 7, h = e & 15, px = par >> 1, pz = par & 1;
             const double bx = px * 0.5 + ox, bz = pz * 0.5 + oz;
@@ -362,11 +368,9 @@ k_fullgate(const Oct *__restrict__ oct, const uint64_t *__restrict__ seeds, cons
             #pragma unroll
             for (int k = 0; k < FG_RB; k++) {
                 const int j = (r0 + k) & 511, iz = (j >> 1) + ((j & 1) ? iz0b : iz0a);
-                const int z0 = iz & 255, z1 = (iz + 1) & 255;
-                sHk[k][tid] = uint32_t(sP2[ca0 + z0] & 15) | uint32_t(sP2[ca0 + z1] & 15) << 8 |
-                              uint32_t(sP2[cb0 + z0] & 15) << 16 | uint32_t(sP2[cb0 + z1] & 15) << 24;
-                sHk[k][tid + 128] = uint32_t(sP2[ca1 + z0] & 15) | uint32_t(sP2[ca1 + z1] & 15) << 8 |
-                                    uint32_t(sP2[cb1 + z0] & 15) << 16 | uint32_t(sP2[cb1 + z1] & 15) << 24;
+                const int z0 = iz & 255;                     // corners z0 and z0 + 1 are one entry of sH2
+                sHk[k][tid] = __byte_perm(sH2[ca0 + z0], sH2[cb0 + z0], 0x5410u);
+                sHk[k][tid + 128] = __byte_perm(sH2[ca1 + z0], sH2[cb1 + z0], 0x5410u);
             }
             __syncthreads();
             #pragma unroll
@@ -385,7 +389,8 @@ k_fullgate(const Oct *__restrict__ oct, const uint64_t *__restrict__ seeds, cons
                     #pragma unroll
                     for (int c = 0; c < 8; c++) {
                         const int dx = c & 1, q = ((c >> 1) & 1) * 2 + (c >> 2);
-                        acc = __fadd_rn(acc, T[c * 16 + (((dx ? w1 : w0) >> (8 * q)) & 15)]);
+                        const uint32_t off = __byte_perm(dx ? w1 : w0, 0u, 0x4440u | uint32_t(q));   // byte q = 4 x hash
+                        acc = __fadd_rn(acc, *reinterpret_cast<const float *>(reinterpret_cast<const char *>(T + c * 16) + off));
                     }
                     S[e] = acc;
                 }
