@@ -5,7 +5,8 @@
 //  * pre-gate: one CTA per (seed, side) pair inside a 2-CTA cluster; each warp owns a 128-row band of its
 //    side's 256^2 grid and streams it with all state in registers (a lane holds 8 columns: hashes, samples,
 //    the horizontal blur through lane shuffles, and the vertical blur as 8 pending FMA chains per column).
-//    Hash rows come 4 at a time from a table of packed row words (one load per column per 4 rows).
+//    Hash rows come 4 at a time from a table of packed row words (one load per column per 4 rows); each is
+//    unpacked once and added to the three sample rows that use it.
 //    No block barrier inside a side; the two side maxima meet through distributed shared memory.
 //  * full gate: one 512-thread CTA per (seed, side) in a 2-CTA cluster, thread = column, row blocks of 8
 //    staged in shared memory; the vertical blur again accumulates in registers.
@@ -114,9 +115,8 @@ __global__ void __launch_bounds__(128) k_octinit(const uint64_t *__restrict__ se
 
 // Hashed rows of the pre-gate.  sW[i] packs the byte offsets (P[(i + b) & 255] & 15) * 4 for b = 0..3, so the
 // offsets of one lattice column for 4 consecutive rows come from one word: sW[c + m] (c = the column's hash
-// P[P[x] + y], m = the first row).  W[dy][t] holds such a word for the lane's column t; hash_row gathers byte
-// j (the row within the group) of the 4 columns of each word group into h[dy][0..1] and takes the next
-// lane's first group as h[dy][2] (columns 8..11, periodic in 256).
+// P[P[x] + y], m = the first row).  W[dy][t] holds such a word for the lane's column t; byte j of it is
+// the offset for row j of the group.
 constexpr int PG_SW = 528 + PG_BAND;         // > c + m0 + k for k <= PG_BAND + 9
 static_assert(PG_SW > 255 + 255 + 4 * ((PG_BAND + 9) / 4), "sW covers every group load");
 __device__ __forceinline__ void load_group(const uint32_t *__restrict__ sW, const uint32_t (&cv)[2][2], int base, uint32_t (&W)[2][8]) {
@@ -125,20 +125,30 @@ __device__ __forceinline__ void load_group(const uint32_t *__restrict__ sW, cons
         #pragma unroll
         for (int t = 0; t < 8; t++) W[dy][t] = sW[((cv[dy][t >> 2] >> (8 * (t & 3))) & 255u) + base];
 }
-__device__ __forceinline__ void hash_row(const uint32_t (&W)[2][8], int j, int lane, uint32_t (&h)[2][3]) {
-    const uint32_t sel = uint32_t(j) * 0x11u + 0x40u;           // byte j of the first and of the second word
+// Offsets of hash row j of the current word group for the lane's lattice columns t = 0..9 (8 and 9 are the
+// next lane's columns 0 and 1, periodic in 256).
+__device__ __forceinline__ void unpack_row(const uint32_t (&W)[2][8], int j, int lane, uint32_t (&hb)[2][10]) {
+    const uint32_t sel = 0x4440u | uint32_t(j);                 // byte j, upper bytes zero
     #pragma unroll
     for (int dy = 0; dy < 2; dy++) {
         #pragma unroll
-        for (int k = 0; k < 2; k++) {
-            const uint32_t lo = __byte_perm(W[dy][4 * k], W[dy][4 * k + 1], sel);
-            const uint32_t hi = __byte_perm(W[dy][4 * k + 2], W[dy][4 * k + 3], sel);
-            h[dy][k] = __byte_perm(lo, hi, 0x5410u);
-        }
-        h[dy][2] = __shfl_sync(0xffffffffu, h[dy][0], (lane + 1) & 31);
+        for (int t = 0; t < 8; t++) hb[dy][t] = __byte_perm(W[dy][t], 0u, sel);
+        hb[dy][8] = __byte_perm(__shfl_sync(0xffffffffu, W[dy][0], (lane + 1) & 31), 0u, sel);
+        hb[dy][9] = __byte_perm(__shfl_sync(0xffffffffu, W[dy][1], (lane + 1) & 31), 0u, sel);
     }
 }
-__device__ __forceinline__ uint32_t hbyte(const uint32_t (&h)[3], int t) { return (h[t >> 2] >> (8 * (t & 3))) & 255u; }
+// Terms of one hash row as row offset V of the 8 cells' samples, S[e] = S0[e] + ..., in the order dy, u.
+template <int V>
+__device__ __forceinline__ void add_row(const char *__restrict__ tcb, const uint32_t (&hb)[2][10], const float (&S0)[8], float (&S)[8]) {
+    #pragma unroll
+    for (int dy = 0; dy < 2; dy++)
+        #pragma unroll
+        for (int e = 0; e < 8; e++)
+            #pragma unroll
+            for (int u = 0; u < 3; u++)
+                S[e] = __fadd_rn(dy == 0 && u == 0 ? S0[e] : S[e],
+                                 *reinterpret_cast<const float *>(tcb + ((u * 3 + V) * 2 + dy) * 64 + hb[dy][e + u]));
+}
 
 // Anti-aliased pre-gate (gate.cuh stream_max<256,4,8,true>).  Cluster rank = noise side.
 __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(PG_THREADS, 6)
@@ -217,40 +227,30 @@ k_pregate(const Oct *__restrict__ oct, const uint64_t *__restrict__ seeds, const
         const int o0 = warp * PG_BAND;
         const int m0 = (o0 - 4 + iz0) & 255;
         float best = -1e9f;
-        uint32_t W[2][8];
-        uint32_t hA[2][3], hB[2][3], hC[2][3];
-        load_group(sW, cv, m0, W);
-        hash_row(W, 0, lane, hA);
-        hash_row(W, 1, lane, hB);
+        uint32_t W[2][8], hb[2][10];
         float pend[8][8];
         #pragma unroll
         for (int j = 0; j < 8; j++)
             #pragma unroll
             for (int e = 0; e < 8; e++) pend[j][e] = 0.f;
         const char *tcb = reinterpret_cast<const char *>(sTc);
-        for (int r = o0 - 4; r < o0 + PG_BAND + 4; r++) {
-            const int k = r - o0 + 6;                            // hash row of sample row r + 2
+        // Hash row k is unpacked once and added as row offset 2 of sample row k-2 (completing it), 1 of row
+        // k-1 (S2, then holding offsets 0 and 1) and 0 of row k (S1); every cell still sums in the order v,
+        // dy, u (gate.cuh:274-281).
+        float S1[8], S2[8];
+        const float Z[8] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
+        load_group(sW, cv, m0, W);
+        unpack_row(W, 0, lane, hb);
+        add_row<0>(tcb, hb, Z, S1);
+        unpack_row(W, 1, lane, hb);
+        add_row<1>(tcb, hb, S1, S2);
+        add_row<0>(tcb, hb, Z, S1);
+        for (int k = 2; k < PG_BAND + 10; k++) {
+            const int r = o0 + k - 6;                            // the sample row this hash row completes
             if ((k & 3) == 0) load_group(sW, cv, m0 + k, W);
-            hash_row(W, k & 3, lane, hC);
-            // samples: for each (v, dy) hash row, unpack its 10 bytes once, then add the three u terms of
-            // all 8 cells; each cell still sums in the order v, dy, u (gate.cuh:274-281)
+            unpack_row(W, k & 3, lane, hb);
             float S[8];
-            #pragma unroll
-            for (int e = 0; e < 8; e++) S[e] = 0.f;
-            #pragma unroll
-            for (int v = 0; v < 3; v++)
-                #pragma unroll
-                for (int dy = 0; dy < 2; dy++) {
-                    const uint32_t (&hw)[3] = v == 0 ? hA[dy] : v == 1 ? hB[dy] : hC[dy];
-                    uint32_t hb[10];
-                    #pragma unroll
-                    for (int t = 0; t < 10; t++) hb[t] = hbyte(hw, t);
-                    #pragma unroll
-                    for (int e = 0; e < 8; e++)
-                        #pragma unroll
-                        for (int u = 0; u < 3; u++)
-                            S[e] = __fadd_rn(S[e], *reinterpret_cast<const float *>(tcb + ((u * 3 + v) * 2 + dy) * 64 + hb[e + u]));
-                }
+            add_row<2>(tcb, hb, S2, S);
             // horizontal blur over columns i-4 .. i+4 (periodic in 256 = the warp's 32 lanes x 8)
             float X[16];
             #pragma unroll
@@ -272,10 +272,8 @@ k_pregate(const Oct *__restrict__ oct, const uint64_t *__restrict__ seeds, const
                 pend[7][e] = __fmaf_rn(tp.k9[0], hv, 0.f);
                 if (r - 4 >= o0) best = fmaxf(best, __fmul_rn(done, tp.norm9));
             }
-            #pragma unroll
-            for (int dy = 0; dy < 2; dy++)
-                #pragma unroll
-                for (int k = 0; k < 3; k++) { hA[dy][k] = hB[dy][k]; hB[dy][k] = hC[dy][k]; }
+            add_row<1>(tcb, hb, S1, S2);
+            add_row<0>(tcb, hb, Z, S1);
         }
         #pragma unroll
         for (int o = 16; o > 0; o >>= 1) best = fmaxf(best, __shfl_xor_sync(0xffffffffu, best, o));
