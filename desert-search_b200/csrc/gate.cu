@@ -2,14 +2,14 @@
 // amplitude gate.  Restates src/gpu/gate.cuh (k_phase, k_init, k_amp2) with the same per-cell arithmetic
 // (summation orders, fused multiply-adds of the blur chains, device expf taps), so amplitudes match the
 // reference's GPU gate bit for bit, on a different schedule:
-//  * pre-gate: one CTA per (seed, side) pair inside a 2-CTA cluster; each warp owns a 128-row band of its
-//    side's 256^2 grid and streams it with all state in registers (a lane holds 8 columns: hashes, samples,
-//    the horizontal blur through lane shuffles, and the vertical blur as 8 pending FMA chains per column).
+//  * pre-gate: one 64-thread CTA per seed, a warp per noise side; the warp streams all 256 rows of its
+//    side's 256^2 grid with all state in registers (a lane holds 8 columns: hashes, samples, the horizontal
+//    blur through lane shuffles, and the vertical blur as 8 pending FMA chains per column).
 //    Hash rows come 4 at a time from a table of packed row words (one load per column per 4 rows); each is
 //    unpacked once and added to the three sample rows that use it.
-//    No block barrier inside a side; the two side maxima meet through distributed shared memory.
-//  * full gate: one 512-thread CTA per (seed, side) in a 2-CTA cluster, thread = column, row blocks of 8
-//    staged in shared memory; the vertical blur again accumulates in registers.
+//    Only warp barriers inside a side; the two side maxima meet in shared memory.
+//  * full gate: one 128-thread CTA per (seed, side) in a 2-CTA cluster, thread = 4 columns, row blocks of
+//    8 staged in shared memory; the vertical blur again accumulates in registers.
 //  * the whole batch (phase -> init -> pre-gate -> full gate) runs from device-side counts: no host sync
 //    between stages, so a batch can be captured in a CUDA graph.
 #include "common.cuh"
@@ -30,7 +30,7 @@ static_assert(sizeof(Oct) == 304, "Oct layout");
 // Blur taps and normalisers, passed by value (they live in the kernel-parameter constant bank).
 struct Taps { float k9[9], k15[15], norm9, norm15, w; };
 
-constexpr int PG_THREADS = 64, PG_BAND = 256 / (PG_THREADS / 32);   // pre-gate: 2 warps x 128 rows per side
+constexpr int PG_THREADS = 64, PG_BAND = 256;      // pre-gate: a warp per side, 256 rows each
 constexpr int FG_THREADS = 128, FG_RB = 8;           // full gate: thread per 4 columns, 8-row blocks
 
 // ---------------------------------------------------------------- device math
@@ -150,37 +150,38 @@ __device__ __forceinline__ void add_row(const char *__restrict__ tcb, const uint
                                  *reinterpret_cast<const float *>(tcb + ((u * 3 + V) * 2 + dy) * 64 + hb[dy][e + u]));
 }
 
-// Anti-aliased pre-gate (gate.cuh stream_max<256,4,8,true>).  Cluster rank = noise side.
-__global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(PG_THREADS, 6)
+// Anti-aliased pre-gate (gate.cuh stream_max<256,4,8,true>).  Warp = noise side.
+__global__ void __launch_bounds__(PG_THREADS, 6)
 k_pregate(const Oct *__restrict__ oct, const uint64_t *__restrict__ seeds, const uint32_t *__restrict__ n_in, uint32_t cap_in,
           float thr, Taps tp, uint64_t *__restrict__ out_seed, uint32_t *__restrict__ out_idx, uint32_t *__restrict__ n_out,
           uint32_t cap_out, float *__restrict__ side_amp) {
-    __shared__ __align__(16) float sTc[288];
-    __shared__ __align__(16) uint8_t sP2[512];
-    __shared__ __align__(16) uint8_t sCol[2][256];
-    __shared__ __align__(16) uint32_t sW[PG_SW];
-    __shared__ float sRed[PG_THREADS / 32];
-    __shared__ float sPeer[2];
-    cg::cluster_group cl = cg::this_cluster();
-    const int side = int(cl.block_rank());
-    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-    const uint32_t n = min(*n_in, cap_in), ncl = gridDim.x / 2;
+    __shared__ __align__(16) float sTcA[2][288];
+    __shared__ __align__(16) uint8_t sP2A[2][512];
+    __shared__ __align__(16) uint8_t sColA[2][2][256];
+    __shared__ __align__(16) uint32_t sWA[2][PG_SW];
+    __shared__ float sRed[2][2];                        // [iteration parity][side]
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5, side = warp;
+    float *sTc = sTcA[side];
+    uint8_t *sP2 = sP2A[side];
+    uint8_t (*sCol)[256] = sColA[side];
+    uint32_t *sW = sWA[side];
+    const uint32_t n = min(*n_in, cap_in);
     int it = 0;
-    for (uint32_t s = blockIdx.x / 2; s < n; s += ncl, it++) {
+    for (uint32_t s = blockIdx.x; s < n; s += gridDim.x, it++) {
         const Oct &p = oct[2 * size_t(s) + side];
-        if (tid < 16) {
-            const uint4 v = reinterpret_cast<const uint4 *>(p.perm)[tid];
-            reinterpret_cast<uint4 *>(sP2)[tid] = v; reinterpret_cast<uint4 *>(sP2)[tid + 16] = v;
+        if (lane < 16) {
+            const uint4 v = reinterpret_cast<const uint4 *>(p.perm)[lane];
+            reinterpret_cast<uint4 *>(sP2)[lane] = v; reinterpret_cast<uint4 *>(sP2)[lane + 16] = v;
         }
         const double ox = p.ox, oz = p.oz, fy = p.fy, vy = p.vy;
         const int iy = p.iy;
-        __syncthreads();
-        for (int c = tid; c < 256; c += PG_THREADS) {
+        __syncwarp();
+        for (int c = lane; c < 256; c += 32) {
             const int pc = sP2[c];
             sCol[0][c] = sP2[pc + (iy & 255)];
             sCol[1][c] = sP2[pc + ((iy + 1) & 255)];
         }
-        for (int i = tid; i < PG_SW; i += PG_THREADS) {
+        for (int i = lane; i < PG_SW; i += 32) {
             uint32_t w = 0;
             #pragma unroll
             for (int b = 0; b < 4; b++) w |= uint32_t(sP2[(i + b) & 255] & 15) << (8 * b + 2);
@@ -194,7 +195,7 @@ k_pregate(const Oct *__restrict__ oct, const uint64_t *__restrict__ seeds, const
                 #pragma unroll
                 for (int q = 0; q < 2; q++) { const double b = o + 0.5 * q; fr[ax][q] = b - floor(b); sh[ax][q] = int(floor(b) - floor(o)); }
             }
-            for (int e = tid; e < 288; e += PG_THREADS) {
+            for (int e = lane; e < 288; e += 32) {
                 const int h = e & 15, dy = (e >> 4) & 1, uv = e >> 5, u = uv / 3, v = uv % 3;
                 double acc = 0;
                 #pragma unroll
@@ -210,7 +211,7 @@ k_pregate(const Oct *__restrict__ oct, const uint64_t *__restrict__ seeds, const
                 sTc[e] = float(0.25 * double(tp.w) * acc);
             }
         }
-        __syncthreads();
+        __syncwarp();
         const int ix0 = int(floor(ox)), iz0 = int(floor(oz));
         uint32_t cv[2][2];
         #pragma unroll
@@ -224,7 +225,7 @@ k_pregate(const Oct *__restrict__ oct, const uint64_t *__restrict__ seeds, const
             }
         // ---- stream this warp's band: output rows [o0, o0 + PG_BAND) need sample rows o0-4 .. o0+PG_BAND+3,
         // i.e. hash rows k = 0 .. PG_BAND+9 from m0 = o0 - 4 + iz0 (mod 256), in word groups of 4
-        const int o0 = warp * PG_BAND;
+        const int o0 = 0;
         const int m0 = (o0 - 4 + iz0) & 255;
         float best = -1e9f;
         uint32_t W[2][8], hb[2][10];
@@ -277,18 +278,10 @@ k_pregate(const Oct *__restrict__ oct, const uint64_t *__restrict__ seeds, const
         }
         #pragma unroll
         for (int o = 16; o > 0; o >>= 1) best = fmaxf(best, __shfl_xor_sync(0xffffffffu, best, o));
-        if (lane == 0) sRed[warp] = best;
+        if (lane == 0) sRed[it & 1][side] = best;
         __syncthreads();
-        float m = 0.f;
         if (tid == 0) {
-            m = sRed[0];
-            #pragma unroll
-            for (int w = 1; w < PG_THREADS / 32; w++) m = fmaxf(m, sRed[w]);
-            if (side == 1) *cl.map_shared_rank(&sPeer[it & 1], 0) = m;
-        }
-        cl.sync();
-        if (side == 0 && tid == 0) {
-            const float mb = sPeer[it & 1];
+            const float m = sRed[it & 1][0], mb = sRed[it & 1][1];
             const float amp = __fadd_rn(__fadd_rn(0.f, m), mb);
             if (side_amp) { side_amp[2 * size_t(s)] = m; side_amp[2 * size_t(s) + 1] = mb; }
             if (amp >= thr) {
