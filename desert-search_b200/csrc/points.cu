@@ -23,7 +23,8 @@ __global__ void k_noise(const SeedNoise *__restrict__ S, int ch, const double *_
     if (i < n) out[i] = channel(*S, ch, xyz[3 * i], xyz[3 * i + 1], xyz[3 * i + 2]);
 }
 // Multi-seed query: point k belongs to noise[pseed[k]]; kind 0..5 = channel noise at (x, 0, z) (unwarped),
-// DSG_Q_STATE = bridged desert state, DSG_Q_PROXY = proxy probability.
+// DSG_Q_STATE = bridged desert state, DSG_Q_PROXY = proxy probability, DSG_Q_CLOW / DSG_Q_ELOW = the proxy's
+// low-octave continentalness (octaves 0..2) and erosion (octaves 0..1).
 __global__ void k_query(const SeedNoise *__restrict__ noise, const uint32_t *__restrict__ pseed, WorldDev w, int kind,
                         const int32_t *__restrict__ xz, uint32_t n, double *__restrict__ out) {
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -33,6 +34,8 @@ __global__ void k_query(const SeedNoise *__restrict__ noise, const uint32_t *__r
     double v;
     if (kind < 6) v = channel(S, kind, x, 0, z);
     else if (kind == DSG_Q_STATE) v = desert_state(S, w, x, z);
+    else if (kind == DSG_Q_CLOW) v = channel_low(S, CH_C, x, z, 0, 3);
+    else if (kind == DSG_Q_ELOW) v = channel_low(S, CH_E, x, z, 0, 2);
     else v = proxy_prob(S, w, x, z);
     out[i] = v;
 }
@@ -112,7 +115,7 @@ extern "C" int dsg_query_batch(const uint64_t *seeds, uint32_t nseeds, const uin
                                double *out) {
     return guarded([&] {
         DSG_ARG(n == 0 || (seeds && pseed && xz && out), "dsg_query_batch: null pointer");
-        DSG_ARG((kind >= 0 && kind < 6) || kind == DSG_Q_STATE || kind == DSG_Q_PROXY, "dsg_query_batch: unknown kind");
+        DSG_ARG((kind >= 0 && kind < 6) || (kind >= DSG_Q_STATE && kind <= DSG_Q_ELOW), "dsg_query_batch: unknown kind");
         for (uint32_t k = 0; k < n; k++) DSG_ARG(pseed[k] < nseeds, "dsg_query_batch: seed index out of range");
         Engine &g = E(); std::lock_guard<std::mutex> l(g.mu);
         require_init();

@@ -9,8 +9,10 @@
 // reference's per-seed loop is sequential (a site is skipped if an earlier site's hot zone covers it; a
 // later exact-flood start is tried only if the earlier ones fell short) the GPU evaluates every candidate
 // speculatively and the host replays the reference's sequential decisions over the results, so the output
-// is what the reference's loop computes.  gpu=0 (the reference's CPU-only search) and study=1 are not part
-// of this build; gscan=0 runs the tables and scan on the GPU anyway (bit-identical to the CPU path).
+// is what the reference's loop computes.  hot_min <= 0 (proxy floods from per-site starts) and study=1 (the
+// per-component census in PREFIX.zones.csv) follow the reference's per-start loop the same way.  gpu=0 (the
+// reference's CPU-only search with its own CPU gate) is not part of this build; gscan=0 runs the tables and
+// scan on the GPU anyway (bit-identical to the CPU path).
 #include "dsgpu.h"
 #include "cpu_check.hpp"
 #include <algorithm>
@@ -70,6 +72,7 @@ struct TMap {
 
 struct Site { float s, t, c, e; int x, z; };
 struct Eval { size_t rank; int x, z; double proxy, s8 = -1, s4 = 0; bool edge = false; double hot = 0; std::vector<std::pair<int, int>> alt; bool nostart = false; };
+struct CensusReq { size_t s, rank; int bx, bz; double proxy; };   // study=1: a new proxy component and its start
 
 [[noreturn]] static void die(const char *what) { fprintf(stderr, "%s: %s\n", what, dsg_last_error()); fflush(nullptr); std::_Exit(3); }
 static void ck(int rc, const char *what) { if (rc < 0) die(what); }
@@ -78,7 +81,7 @@ struct Search {
     Params P;
     uint64_t start = 0, count = 0;
     int threads = 11;
-    FILE *out = nullptr, *sout = nullptr;
+    FILE *out = nullptr, *sout = nullptr, *zout = nullptr;
     std::mutex mu;                                 // output files, best, stderr lines
     double best = 0;
     std::atomic<uint64_t> done{0}, passed{0}, scanned{0}, nsites{0}, nhot{0}, nbig{0};
@@ -99,12 +102,32 @@ struct Search {
 
     // ---- per-batch stages
     void process(const std::vector<uint64_t> &seeds);
+    void start_loop(const std::vector<uint64_t> &seeds, const std::vector<std::vector<Site>> &sites, std::vector<std::vector<Eval>> &ev,
+                    std::vector<CensusReq> &census);
+    void study_census(const std::vector<uint64_t> &seeds, const std::vector<std::vector<Site>> &sites, const std::vector<std::array<double, 2>> &fy,
+                      const std::vector<float> &maxt, const std::vector<CensusReq> &census, std::vector<std::vector<std::string>> &zrows);
 };
 
 static uint64_t bucket_key(int x, int z, int nms) {
     return (uint64_t(uint32_t((x + 8000000) / nms)) << 32) | uint32_t((z + 8000000) / nms);
 }
 static uint64_t hotkey(int x, int z) { return (uint64_t(uint32_t((x + 8000000) >> 7)) << 32) | uint32_t((z + 8000000) >> 7); }
+// 32-quart block of a proxy-flood cell; starts inside a flooded component are skipped by it (:186-187)
+static uint64_t cellkey(int x, int z) { return (uint64_t(uint32_t((x + 8000000) >> 5)) << 32) | uint32_t((z + 8000000) >> 5); }
+
+// Cells (x, z) of a batch of floods into a buffer kept by the caller (grown, never value-initialised again);
+// an overflow reruns the batch with the exact size the library reported.
+static void flood_cells(const std::vector<dsg_flood_req> &q, std::vector<dsg_area> &a, std::vector<uint64_t> &off, std::vector<int32_t> &cells) {
+    a.resize(q.size()); off.assign(q.size() + 1, 0);
+    if (q.empty()) return;
+    if (cells.size() < 2 * q.size() * 256) cells.resize(2 * q.size() * 256);
+    for (;;) {
+        const int rc = dsg_flood_batch_cells(q.data(), uint32_t(q.size()), a.data(), off.data(), cells.data(), cells.size() / 2);
+        ck(rc, "flood cells");
+        if (rc == DSG_OK) return;
+        cells.resize(2 * (off.back() + 1));
+    }
+}
 
 // CPU loop order of a raw candidate (j, i, tz, tx): the order the reference's scan loop meets it.
 static uint64_t scan_order(const dsg_cand &c) {
@@ -196,7 +219,9 @@ void Search::process(const std::vector<uint64_t> &seeds) {
     // ---------------- S3: hot zones (dsearch_desert.cpp:326-372)
     struct Zone { size_t seed, rank; double hot; int x0, z0, nx, nz; };
     std::vector<Zone> zones;
-    {
+    std::vector<std::vector<Eval>> ev(n);
+    std::vector<CensusReq> census;
+    if (P.hot_min > 0) {
         // hottest of 7x7 points at 256-quart spacing around every site (first strict maximum in dz, dx order)
         const auto tq0 = Clock::now();
         std::vector<int32_t> xz; std::vector<uint32_t> ps;
@@ -258,19 +283,6 @@ void Search::process(const std::vector<uint64_t> &seeds) {
             }
             return false;
         };
-        // cells land in a buffer kept across batches (grown, never value-initialised again); an overflow reruns
-        // the batch with the exact size the library reported
-        auto flood_cells = [&](const std::vector<dsg_flood_req> &q, std::vector<dsg_area> &a, std::vector<uint64_t> &off, std::vector<int32_t> &cells) {
-            a.resize(q.size()); off.assign(q.size() + 1, 0);
-            if (q.empty()) return;
-            if (cells.size() < 2 * q.size() * 256) cells.resize(2 * q.size() * 256);
-            for (;;) {
-                const int rc = dsg_flood_batch_cells(q.data(), uint32_t(q.size()), a.data(), off.data(), cells.data(), cells.size() / 2);
-                ck(rc, "hot-zone flood");
-                if (rc == DSG_OK) return;
-                cells.resize(2 * (off.back() + 1));
-            }
-        };
         // Speculatively, all at once: the step-256 pre-flood of every hot site, then the step-128 flood of every
         // site whose pre-flood is large.  Each seed then replays its sites in rank order against the coverage
         // bitmaps and uses only the floods of the sites it does not skip, so the result is the reference's;
@@ -321,9 +333,10 @@ void Search::process(const std::vector<uint64_t> &seeds) {
                 zones.push_back({s2, r, hot_area, x0, z0, (hz.maxx + 128 - x0) / 32 + 1, (hz.maxz + 128 - z0) / 32 + 1});
             }
         t_hot += std::chrono::duration<double>(Clock::now() - th0).count();
+    } else {
+        start_loop(seeds, sites, ev, census);
     }
     // ---------------- S4: proxy bitmaps + components (dsearch_desert.cpp:425-492)
-    std::vector<std::vector<Eval>> ev(n);
     const auto tp0 = Clock::now();
     if (!zones.empty()) {
         std::vector<dsg_zone> dz; std::vector<uint32_t> zs; size_t total = 0;
@@ -393,6 +406,8 @@ void Search::process(const std::vector<uint64_t> &seeds) {
             }
         }
     }
+    std::vector<std::vector<std::string>> zrows(n);
+    if (!census.empty()) study_census(seeds, sites, fy, maxt, census, zrows);
     for (auto &e : ev) std::sort(e.begin(), e.end(), [](auto &a, auto &b) { return a.proxy > b.proxy; });
     t_proxy += std::chrono::duration<double>(Clock::now() - tp0).count();
     const auto te0 = Clock::now();
@@ -400,7 +415,7 @@ void Search::process(const std::vector<uint64_t> &seeds) {
     struct Try { size_t s, k2, t; int sx, sz; int bx = 0, bz = 0; bool found = false; };
     std::vector<Try> tries;
     for (size_t s = 0; s < n; s++)
-        for (size_t k2 = 0; k2 < ev[s].size() && int(k2) < P.exact_n && ev[s][k2].proxy >= P.exact_min; k2++) {
+        for (size_t k2 = 0; !P.study && k2 < ev[s].size() && int(k2) < P.exact_n && ev[s][k2].proxy >= P.exact_min; k2++) {
             const Eval &e = ev[s][k2];
             tries.push_back({s, k2, 0, e.x, e.z});
             for (size_t a = 0; a < e.alt.size(); a++) tries.push_back({s, k2, a + 1, e.alt[a].first, e.alt[a].second});
@@ -487,6 +502,7 @@ void Search::process(const std::vector<uint64_t> &seeds) {
                     e.rank, e.x * 4 + 2, e.z * 4 + 2, st.s, st.t, st.c, st.e, e.proxy, e.s8, e.s4, int(e.edge), e.hot);
         }
         fprintf(sout, "%lld,%.4f,%.4f,%.4f,%.4f,%zu,%zu,%.3f\n", seed, fy[s][0], fy[s][1], maxt[2 * s], maxt[2 * s + 1], ncand[s], sites[s].size(), seed_best);
+        for (const std::string &z : zrows[s]) fputs(z.c_str(), zout);
     }
     t_tab += std::chrono::duration<double>(t1 - t0).count();
     t_scan += std::chrono::duration<double>(t2 - t1).count();
@@ -498,6 +514,158 @@ void Search::process(const std::vector<uint64_t> &seeds) {
                 (unsigned long long)done.load(), (unsigned long long)passed.load(), (unsigned long long)scanned.load(), (unsigned long long)nsites.load(),
                 passed.load() / std::chrono::duration<double>(now - begin).count(), t_tab.load(), t_scan.load(), t_site.load(), t_proxy.load(), t_hot.load(), t_gpu.load(),
                 (unsigned long long)nhot.load(), (unsigned long long)nbig.load());
+    }
+}
+
+// Per-start proxy floods (dsearch_desert.cpp:367-423), used when hot_min <= 0: every site gets starts (the
+// most probable of 9 x 9 points at 64-quart spacing, first strict maximum in dz, dx order, if it reaches
+// pcut; or a (2 multi + 1)^2 grid at 512 quarts), and each start whose proxy state is 2 and that lies outside
+// the components flooded so far for the seed (32-quart blocks) floods its proxy component at step 32,
+// 8-connected, window 500.  Components already met (same (min x, min z)) are dropped.  All starts are flooded
+// speculatively in one batch and each seed replays the reference's sequence over the results.
+void Search::start_loop(const std::vector<uint64_t> &seeds, const std::vector<std::vector<Site>> &sites, std::vector<std::vector<Eval>> &ev,
+                        std::vector<CensusReq> &census) {
+    const size_t n = seeds.size();
+    const auto ts0 = Clock::now();
+    struct Start { size_t s, rank; int x, z; };
+    std::vector<Start> st;
+    for (size_t s = 0; s < n; s++) nsites += sites[s].size();
+    if (P.multi <= 1) {
+        std::vector<int32_t> xz; std::vector<uint32_t> ps;
+        for (size_t s = 0; s < n; s++)
+            for (const Site &t : sites[s])
+                for (int dz = -4; dz <= 4; dz++) for (int dx = -4; dx <= 4; dx++) { xz.push_back(t.x + dx * 64); xz.push_back(t.z + dz * 64); ps.push_back(uint32_t(s)); }
+        std::vector<double> pr(ps.size());
+        if (!ps.empty()) ck(dsg_query_batch(seeds.data(), uint32_t(n), ps.data(), DSG_Q_PROXY, xz.data(), uint32_t(ps.size()), pr.data()), "start points");
+        size_t k = 0;
+        for (size_t s = 0; s < n; s++)
+            for (size_t r = 0; r < sites[s].size(); r++) {
+                const Site &t = sites[s][r];
+                int bx = t.x, bz = t.z; float bp = -1;
+                for (int q = 0; q < 81; q++, k++) if (float(pr[k]) > bp) { bp = float(pr[k]); bx = t.x + (q % 9 - 4) * 64; bz = t.z + (q / 9 - 4) * 64; }
+                if (bp >= P.pcut) st.push_back({s, r, bx, bz});
+            }
+    } else {
+        for (size_t s = 0; s < n; s++)
+            for (size_t r = 0; r < sites[s].size(); r++)
+                for (int dz = -P.multi; dz <= P.multi; dz++) for (int dx = -P.multi; dx <= P.multi; dx++)
+                    st.push_back({s, r, sites[s][r].x + dx * 512, sites[s][r].z + dz * 512});
+    }
+    // PX(bx, bz) == 2: probability >= the float cut (desert_proxy.hpp:32)
+    std::vector<uint8_t> pass(st.size(), 0);
+    if (!st.empty()) {
+        std::vector<int32_t> xz; std::vector<uint32_t> ps;
+        for (const Start &t : st) { xz.push_back(t.x); xz.push_back(t.z); ps.push_back(uint32_t(t.s)); }
+        std::vector<double> pr(st.size());
+        ck(dsg_query_batch(seeds.data(), uint32_t(n), ps.data(), DSG_Q_PROXY, xz.data(), uint32_t(ps.size()), pr.data()), "start proxy");
+        for (size_t k = 0; k < st.size(); k++) pass[k] = float(pr[k]) >= float(P.pcut);
+    }
+    std::vector<dsg_flood_req> q; std::vector<long> f_of(st.size(), -1);
+    for (size_t k = 0; k < st.size(); k++)
+        if (pass[k]) { f_of[k] = long(q.size()); q.push_back({seeds[st[k].s], st[k].x, st[k].z, 32, 16000 / 32, 1, DSG_PRED_PROXY, float(P.pcut), 0}); }
+    std::vector<dsg_area> a; std::vector<uint64_t> off;
+    static thread_local std::vector<int32_t> cells;
+    flood_cells(q, a, off, cells);
+    for (size_t k = 0; k < st.size();) {
+        const size_t s = st[k].s;
+        std::unordered_set<uint64_t> covered;
+        std::vector<std::pair<int, int>> seen;
+        for (; k < st.size() && st[k].s == s; k++) {
+            if (!pass[k] || covered.count(cellkey(st[k].x, st[k].z))) continue;
+            const long f = f_of[k];
+            for (uint64_t c = off[f]; c < off[f + 1]; c++) covered.insert(cellkey(cells[2 * c], cells[2 * c + 1]));
+            const std::pair<int, int> sig(a[f].minx, a[f].minz);
+            if (std::find(seen.begin(), seen.end(), sig) != seen.end()) continue;
+            seen.push_back(sig);
+            const double proxy = a[f].cells * 32.0 * 32 * 16 / 1e6;
+            ev[s].push_back({st[k].rank, st[k].x, st[k].z, proxy});
+            if (P.study) census.push_back({s, st[k].rank, st[k].x, st[k].z, proxy});
+        }
+    }
+    t_proxy += std::chrono::duration<double>(Clock::now() - ts0).count();
+}
+
+// study=1 (dsearch_desert.cpp:401-421): for each new proxy component, the hot zone (T >= 0.55) at step 64
+// from its start (window 375, 4-connected) and a census of its cells: low-octave continentalness and
+// erosion, the ocean / badlands / mangrove-like fractions and the fraction the proxy table passes.  The sums
+// are FP64 in the order the reference's depth-first flood meets the cells: that order depends only on which
+// cells are hot, so it is replayed here over the flood's cell set, and the per-cell values come from the
+// device (bit-identical to the CPU sampler).
+void Search::study_census(const std::vector<uint64_t> &seeds, const std::vector<std::vector<Site>> &sites, const std::vector<std::array<double, 2>> &fy,
+                          const std::vector<float> &maxt, const std::vector<CensusReq> &census, std::vector<std::vector<std::string>> &zrows) {
+    const size_t n = seeds.size();
+    constexpr int half = 24000 / 64, nw = 2 * half + 1;
+    std::vector<dsg_flood_req> q;
+    for (const CensusReq &c : census) q.push_back({seeds[c.s], c.bx, c.bz, 64, half, 0, DSG_PRED_HOT, 0.f, 0});
+    std::vector<dsg_area> a; std::vector<uint64_t> off;
+    static thread_local std::vector<int32_t> cells;
+    flood_cells(q, a, off, cells);
+    const uint64_t total = off.back();
+    std::vector<double> cv(total), evv(total);
+    if (total) {
+        std::vector<uint32_t> ps(total);
+        for (size_t k = 0; k < census.size(); k++) for (uint64_t c = off[k]; c < off[k + 1]; c++) ps[c] = uint32_t(census[k].s);
+        ck(dsg_query_batch(seeds.data(), uint32_t(n), ps.data(), DSG_Q_CLOW, cells.data(), uint32_t(total), cv.data()), "census C");
+        ck(dsg_query_batch(seeds.data(), uint32_t(n), ps.data(), DSG_Q_ELOW, cells.data(), uint32_t(total), evv.data()), "census E");
+    }
+    // phases of the C and E octaves 0 and 1 (|fy - 0.5| summed over the two sides, :311-312)
+    std::vector<std::array<double, 4>> ph(n);
+    std::vector<uint8_t> have(n, 0);
+    static thread_local std::vector<int32_t> idx;          // window cell -> index in the flood's cell list
+    static thread_local std::vector<uint8_t> touched;
+    idx.assign(size_t(nw) * nw, -1); touched.assign(size_t(nw) * nw, 0);
+    std::vector<int> stack; std::vector<int32_t> order;
+    for (size_t k = 0; k < census.size(); k++) {
+        const CensusReq &c = census[k];
+        if (!have[c.s]) {
+            const hostcheck::Channel C(seeds[c.s], 2), E(seeds[c.s], 3);
+            auto phase_of = [](const hostcheck::Channel &N, int o) { return std::abs(N.o[0][o].fy - .5) + std::abs(N.o[1][o].fy - .5); };
+            ph[c.s] = {phase_of(E, 0), phase_of(E, 1), phase_of(C, 0), phase_of(C, 1)};
+            have[c.s] = 1;
+        }
+        const uint64_t c0 = off[k], c1 = off[k + 1];
+        for (uint64_t i = c0; i < c1; i++)
+            idx[size_t((cells[2 * i + 1] - c.bz) / 64 + half) * nw + size_t((cells[2 * i] - c.bx) / 64 + half)] = int32_t(i - c0);
+        // the reference's touch order (dense_flood.hpp:60-86): a hot cell is counted when first touched
+        order.clear(); stack.clear();
+        std::vector<int> visited;
+        auto touch = [&](int i, int j) {
+            if (i < 0 || j < 0 || i >= nw || j >= nw) return;
+            const int w = j * nw + i;
+            if (touched[w]) return;
+            touched[w] = 1; visited.push_back(w);
+            const int x = c.bx + (i - half) * 64, z = c.bz + (j - half) * 64;
+            if (x < -7499996 || x > 7499996 || z < -7499996 || z > 7499996) return;
+            if (idx[w] < 0) return;
+            order.push_back(idx[w]);
+            stack.push_back(w);
+        };
+        touch(half, half);
+        while (!stack.empty()) {
+            const int w = stack.back(); stack.pop_back();
+            const int i = w % nw, j = w / nw;
+            touch(i - 1, j); touch(i + 1, j); touch(i, j - 1); touch(i, j + 1);
+        }
+        for (int w : visited) touched[w] = 0;
+        for (uint64_t i = c0; i < c1; i++)
+            idx[size_t((cells[2 * i + 1] - c.bz) / 64 + half) * nw + size_t((cells[2 * i] - c.bx) / 64 + half)] = -1;
+        double sc = 0, se = 0, se2 = 0; long nh = 0, no = 0, nb = 0, nm = 0, ng = 0;
+        for (int32_t id : order) {
+            const double cc = cv[c0 + id], e = evv[c0 + id];
+            nh++; sc += cc; se += e; se2 += e * e;
+            no += cc < -0.19; nb += e < 0.05; nm += e > 0.55;
+            const int i = std::clamp(int(std::floor((cc + 0.8) / 0.05)), 0, 39), j = std::clamp(int(std::floor((e + 1.0) / 0.05)), 0, 39);
+            ng += prob[i * 40 + j] >= P.pcut;
+        }
+        const double d = double(std::max(1L, nh)), me = se / d;
+        const Site &t = sites[c.s][c.rank];
+        char line[512];
+        snprintf(line, sizeof line, "%lld,%.4f,%.4f,%.4f,%.4f,%.4f,%.4f,%zu,%d,%d,%.4f,%.4f,%.4f,%.2f,%.2f,%.4f,%.4f,%.4f,%.4f,%.4f,%.4f,%.4f\n",
+                 (long long)seeds[c.s], std::abs(fy[c.s][0] - .5) + std::abs(fy[c.s][1] - .5), maxt[2 * c.s] + maxt[2 * c.s + 1],
+                 ph[c.s][0], ph[c.s][1], ph[c.s][2], ph[c.s][3], c.rank, c.bx * 4, c.bz * 4, t.t, t.c, t.e,
+                 a[k].cells * 64.0 * 64 * 16 / 1e6, c.proxy, double(no) / d, double(nb) / d, double(nm) / d, double(ng) / d,
+                 sc / d, me, std::sqrt(std::max(0.0, se2 / d - me * me)));
+        zrows[c.s].push_back(line);
     }
 }
 
@@ -530,13 +698,16 @@ int main(int argc, char **argv) {
         P.from_stdin = 1;
     }
     if (!P.gpu) { fprintf(stderr, "gpu=0 selects the CPU-only search, which this B200 build does not provide: run with gpu=1 (gate=1 gscan=1)\n"); return 2; }
-    if (P.study) { fprintf(stderr, "study=1 is not provided by this build\n"); return 2; }
-    if (P.hot_min <= 0) { fprintf(stderr, "hot_min <= 0 (per-site proxy floods without hot zones) is not provided by this build\n"); return 2; }
     S.out = fopen((prefix + ".csv").c_str(), "wx");
     S.sout = fopen((prefix + ".seeds.csv").c_str(), "wx");
     if (!S.out || !S.sout) { fprintf(stderr, "cannot create %s outputs (exist?)\n", prefix.c_str()); return 2; }
     fprintf(S.out, "seed,fyA,fyB,maxta,maxtb,rank,x,z,score,t0,c0,e0,proxy,s8,s4,edge,hot\n");
     fprintf(S.sout, "seed,fyA,fyB,maxta,maxtb,candidates,sites,best\n");
+    if (P.study) {                                         // :147-150
+        S.zout = fopen((prefix + ".zones.csv").c_str(), "wx");
+        if (!S.zout) { fprintf(stderr, "cannot create %s outputs (exist?)\n", prefix.c_str()); return 2; }
+        fprintf(S.zout, "seed,phT,amp,phE0,phE1,phC0,phC1,rank,x,z,t0,c0,e0,hot,proxy,f_ocean,f_badl,f_mang,f_good,mean_c,mean_e,sd_e\n");
+    }
     signal(SIGINT, on_signal); signal(SIGTERM, on_signal);
     const auto ti0 = Clock::now();
     ck(dsg_init(0, float(P.pcut)), "dsg_init");
@@ -631,6 +802,7 @@ int main(int argc, char **argv) {
     for (auto &t : pool) t.join();
     if (source.joinable()) { if (qdone) source.join(); else source.detach(); }
     fclose(S.out); fclose(S.sout);
+    if (S.zout) fclose(S.zout);
     if (verifier.joinable()) {                             // every candidate's line is written before the exit
         { std::lock_guard<std::mutex> vl(S.vmu); S.vdone = true; S.vcv.notify_all(); }
         verifier.join();

@@ -153,9 +153,13 @@ int dsg_noise(uint64_t seed, int channel, const double *xyz, uint32_t n, double 
 
 /* Point queries over many seeds at once: point k (x = xz[2k], z = xz[2k+1]) belongs to seeds[pseed[k]].
  * kind 0..5: channel noise at the unwarped point (x, 0, z) (NormalNoise::sample, T.sample in
- * dsearch_desert.cpp:330); DSG_Q_STATE: bridged desert state (0/1/2); DSG_Q_PROXY: proxy probability. */
+ * dsearch_desert.cpp:330); DSG_Q_STATE: bridged desert state (0/1/2); DSG_Q_PROXY: proxy probability;
+ * DSG_Q_CLOW / DSG_Q_ELOW: continentalness octaves 0..2 / erosion octaves 0..1 of both sides in one sum
+ * (DesertProxy::octaves, desert_proxy.hpp:13-23, as the study census samples them, dsearch_desert.cpp:405). */
 #define DSG_Q_STATE 6
 #define DSG_Q_PROXY 7
+#define DSG_Q_CLOW  8
+#define DSG_Q_ELOW  9
 int dsg_query_batch(const uint64_t *seeds, uint32_t nseeds, const uint32_t *pseed, int kind, const int32_t *xz, uint32_t n, double *out);
 
 /* Flood a batch of requests concurrently (any mix of seeds, steps, windows, predicates).  Results are

@@ -81,6 +81,12 @@ int orc_noise(uint64_t seed, int ch, const double *xyz, int n, double *out) {
     for (int i = 0; i < n; i++) out[i] = S.nz[ch].sample(xyz[3 * i], xyz[3 * i + 1], xyz[3 * i + 2]);
     return 0;
 }
+// Octaves [lo, hi) of channel `ch`, both sides, at quart points (x, 0, z) (desert_proxy.hpp:13-23).
+int orc_noise_low(uint64_t seed, int ch, int lo, int hi, const int32_t *xz, int n, double *out) {
+    const Seed S(seed);
+    for (int i = 0; i < n; i++) out[i] = S.nz[ch].low(xz[2 * i], xz[2 * i + 1], lo, hi);
+    return 0;
+}
 // FP64 gate amplitudes (pre-gate and full gate, both sides) of n seeds, on `threads` threads: the yardstick
 // of the FP32 gate's error and pass set.
 int orc_gate_fp64(const uint64_t *seeds, int n, double *pre, double *full, int threads) {

@@ -39,7 +39,7 @@ def ptr(a, t):
 
 def _bind(lib, prefix):
     fns = {}
-    for name in ["phase", "noise", "points", "climate", "biome", "leaf_two_ways", "flood", "tabins", "tables", "tmap", "blur_taps"]:
+    for name in ["phase", "noise", "points", "climate", "biome", "leaf_two_ways", "flood", "tabins", "tables", "tmap", "blur_taps", "noise_low"]:
         f = getattr(lib, f"{prefix}_{name}", None)
         if f is not None:
             fns[name] = f
@@ -65,6 +65,12 @@ class CpuPath:
         xyz = np.ascontiguousarray(xyz, dtype=np.float64).reshape(-1, 3)
         out = np.empty(len(xyz))
         self.f["noise"](C.c_uint64(seed), C.c_int(ch), ptr(xyz, f64p), C.c_int(len(xyz)), ptr(out, f64p))
+        return out
+
+    def noise_low(self, seed, ch, lo, hi, xz):
+        xz = np.ascontiguousarray(xz, dtype=np.int32).reshape(-1, 2)
+        out = np.empty(len(xz))
+        self.f["noise_low"](C.c_uint64(seed), C.c_int(ch), C.c_int(lo), C.c_int(hi), ptr(xz, i32p), C.c_int(len(xz)), ptr(out, f64p))
         return out
 
     def points(self, seed, pred, xz, threads=1):

@@ -109,6 +109,31 @@ def test_dsearch_matches_reference_gpu_searcher(tmp_path):
     assert set(cand(a.stderr)) >= set(cand(b.stderr)) or set(cand(a.stderr)) <= set(cand(b.stderr))
 
 
+@pytest.mark.parametrize("opts", [["hot_min=0"], ["hot_min=0", "study=1"], ["hot_min=0", "study=1", "multi=2"]],
+                         ids=["per_start", "study", "study_multi2"])
+def test_dsearch_per_start_and_study_match_reference_cpu_searcher(tmp_path, opts):
+    """hot_min <= 0 (proxy floods from per-site starts: the best proxy point of 9 x 9, or a 5 x 5 grid with
+    multi=2) and study=1 (no exact floods; a census of every new proxy component in PREFIX.zones.csv) against
+    the reference's own CPU searcher on the same stdin seeds.  The reference's CPU proxy is FP64 like ours,
+    so every file is compared exactly, the census's FP64 sums included."""
+    seeds = "".join(f"{f['seed']}\n" for f in finds()[:8])
+    a = run([os.path.join(BIN, "dsearch_desert"), "0", "0", str(tmp_path / "ours"), "8", "stdin=1", "gpu=1", "gscan=1"] + opts, stdin=seeds)
+    b = run([ref("dsearch_desert"), "0", "0", str(tmp_path / "ref"), "8", "stdin=1"] + opts, stdin=seeds)
+    assert a.returncode == 0, a.stderr[-2000:]
+    assert b.returncode == 0, b.stderr[-2000:]
+    rd = lambda p: sorted(open(p).read().splitlines())
+    files = [".csv", ".seeds.csv"] + ([".zones.csv"] if "study=1" in opts else [])
+    for ext in files:
+        la, lb = rd(str(tmp_path / "ours") + ext), rd(str(tmp_path / "ref") + ext)
+        assert len(la) > 1, ext
+        assert la == lb, (ext, sorted(set(la) ^ set(lb))[:6])
+    if "study=1" in opts:
+        assert len(rd(str(tmp_path / "ours") + ".zones.csv")) > 100
+        assert "CANDIDATE" not in a.stderr and "best " not in a.stderr     # study mode runs no exact floods
+    cand = lambda s: sorted(re.findall(r"CANDIDATE step4=[\d.]+M seed=-?\d+ x=-?\d+ z=-?\d+", s))
+    assert cand(a.stderr) == cand(b.stderr)
+
+
 def test_searcher_verifies_candidates_in_process(tmp_path, dsg):
     """verified=1: each CANDIDATE's exact step-1 flood runs on the flood service during the search, and
     PREFIX.verified gets the line deploy/gpipe.sh would append after bin/mcmeasure, in the fields
