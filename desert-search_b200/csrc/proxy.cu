@@ -18,6 +18,9 @@ namespace {
 float g_cut = 0.35f;
 struct DZone { int32_t x0, z0, nx, nz; int64_t off; int32_t seed, pad; };
 constexpr int CHUNK = 2048;
+// Statistics of one 8-connected component of a zone bitmap.  sx, sz: sums of the cells' columns and rows
+// (exact integers); kid: index among the kept components or -1; seg, cur: its interior-key segment.
+struct CompStat { uint32_t zone, first, cells, inner; int32_t minx, minz, kid; uint32_t seg, cur, pad; uint64_t sx, sz; };
 
 __global__ void __launch_bounds__(256) k_proxy(const SeedNoise *__restrict__ noise, const DZone *__restrict__ zones, WorldDev w, float cut,
                                                uint8_t *__restrict__ out) {
@@ -31,6 +34,199 @@ __global__ void __launch_bounds__(256) k_proxy(const SeedNoise *__restrict__ noi
     }
 }
 
+// ---- component labelling of the bitmaps (the 8-connected components, centroids and interior starts of
+// dsearch_desert.cpp:451-490).  Union-find over zone-local cell indices; a union links the larger root to
+// the smaller one, so every component's root is its first cell in raster order, the order in which the
+// reference's scan meets it.  Loops on the parent links stop after kLinkLimit steps and raise the error flag.
+constexpr uint32_t kLinkLimit = 1u << 24;
+// Root of x, shortening the path on the way (each visited node is pointed two levels up); parents are
+// always smaller indices, so the stored value is still an ancestor whatever other threads do meanwhile.
+__device__ __forceinline__ int32_t uf_find(int32_t *par, int32_t x, uint32_t *err) {
+    int32_t cur = __ldcg(par + x);
+    if (cur == x) return x;
+    int32_t prev = x;
+    for (uint32_t it = 0; it < kLinkLimit; it++) {
+        const int32_t next = __ldcg(par + cur);
+        if (next == cur) return cur;
+        __stcg(par + prev, next);
+        prev = cur; cur = next;
+    }
+    atomicOr(err, 1u);
+    return cur;
+}
+__device__ __forceinline__ void uf_union(int32_t *par, int32_t a, int32_t b, uint32_t *err) {
+    for (uint32_t it = 0; it < kLinkLimit; it++) {
+        a = uf_find(par, a, err); b = uf_find(par, b, err);
+        if (a == b) return;
+        if (a < b) { const int32_t t = a; a = b; b = t; }
+        const int32_t old = atomicCAS(par + a, a, b);
+        if (old == a) return;
+        a = old;
+    }
+    atomicOr(err, 1u);
+}
+__device__ __forceinline__ bool zone_bit(const uint8_t *b, const DZone &z, int x, int y) {
+    return x >= 0 && y >= 0 && x < z.nx && y < z.nz && b[int64_t(y) * z.nx + x];
+}
+// All 8 neighbours set and the cell not on the zone's edge (the reference's interior test, :469-473).
+__device__ __forceinline__ bool interior(const uint8_t *b, const DZone &z, int x, int y) {
+    if (x <= 0 || y <= 0 || x >= z.nx - 1 || y >= z.nz - 1) return false;
+    for (int dy = -1; dy <= 1; dy++)
+        for (int dx = -1; dx <= 1; dx++) if (!b[int64_t(y + dy) * z.nx + x + dx]) return false;
+    return true;
+}
+__global__ void __launch_bounds__(256) k_cc_init(const DZone *__restrict__ zones, const uint8_t *__restrict__ bits, int32_t *__restrict__ par) {
+    const DZone z = zones[blockIdx.x];
+    const int64_t n = int64_t(z.nx) * z.nz, c0 = int64_t(blockIdx.y) * CHUNK, c1 = min(n, c0 + CHUNK);
+    for (int64_t c = c0 + threadIdx.x; c < c1; c += blockDim.x) par[z.off + c] = bits[z.off + c] ? int32_t(c) : -1;
+}
+__global__ void __launch_bounds__(256) k_cc_merge(const DZone *__restrict__ zones, const uint8_t *__restrict__ bits, int32_t *__restrict__ par,
+                                                  uint32_t *err) {
+    const DZone z = zones[blockIdx.x];
+    const int64_t n = int64_t(z.nx) * z.nz, c0 = int64_t(blockIdx.y) * CHUNK, c1 = min(n, c0 + CHUNK);
+    const uint8_t *b = bits + z.off;
+    int32_t *p = par + z.off;
+    for (int64_t c = c0 + threadIdx.x; c < c1; c += blockDim.x) {
+        if (!b[c]) continue;
+        const int x = int(c % z.nx), y = int(c / z.nx);
+        // the four neighbours that come earlier in raster order cover every 8-connected pair once
+        if (zone_bit(b, z, x - 1, y)) uf_union(p, int32_t(c), int32_t(c - 1), err);
+        if (zone_bit(b, z, x - 1, y - 1)) uf_union(p, int32_t(c), int32_t(c - z.nx - 1), err);
+        if (zone_bit(b, z, x, y - 1)) uf_union(p, int32_t(c), int32_t(c - z.nx), err);
+        if (zone_bit(b, z, x + 1, y - 1)) uf_union(p, int32_t(c), int32_t(c - z.nx + 1), err);
+    }
+}
+// Roots get a component id; every cell's parent becomes its root.
+__global__ void __launch_bounds__(256) k_cc_roots(const DZone *__restrict__ zones, int32_t *__restrict__ par, int32_t *__restrict__ rid,
+                                                  CompStat *__restrict__ cs, uint32_t *ctr) {
+    const DZone z = zones[blockIdx.x];
+    const int64_t n = int64_t(z.nx) * z.nz, c0 = int64_t(blockIdx.y) * CHUNK, c1 = min(n, c0 + CHUNK);
+    int32_t *p = par + z.off;
+    for (int64_t c = c0 + threadIdx.x; c < c1; c += blockDim.x) {
+        if (p[c] < 0) continue;
+        const int32_t r = uf_find(p, int32_t(c), ctr + 3);
+        if (r == int32_t(c)) {
+            const uint32_t id = atomicAdd(ctr, 1u);
+            rid[z.off + c] = int32_t(id);
+            CompStat &q = cs[id];
+            q.zone = blockIdx.x; q.first = uint32_t(c); q.cells = 0; q.inner = 0; q.minx = q.minz = 0x7fffffff; q.kid = -1;
+            q.seg = 0; q.cur = 0; q.sx = 0; q.sz = 0;
+        }
+    }
+}
+__global__ void __launch_bounds__(256) k_cc_flatten(const DZone *__restrict__ zones, int32_t *__restrict__ par, uint32_t *err) {
+    const DZone z = zones[blockIdx.x];
+    const int64_t n = int64_t(z.nx) * z.nz, c0 = int64_t(blockIdx.y) * CHUNK, c1 = min(n, c0 + CHUNK);
+    int32_t *p = par + z.off;
+    for (int64_t c = c0 + threadIdx.x; c < c1; c += blockDim.x)
+        if (p[c] >= 0) p[c] = uf_find(p, int32_t(c), err);
+}
+__global__ void __launch_bounds__(256) k_cc_stats(const DZone *__restrict__ zones, const uint8_t *__restrict__ bits, const int32_t *__restrict__ par,
+                                                  const int32_t *__restrict__ rid, CompStat *__restrict__ cs) {
+    const DZone z = zones[blockIdx.x];
+    const int64_t n = int64_t(z.nx) * z.nz, c0 = int64_t(blockIdx.y) * CHUNK, c1 = min(n, c0 + CHUNK);
+    const uint8_t *b = bits + z.off;
+    for (int64_t c = c0 + threadIdx.x; c < c1; c += blockDim.x) {
+        const int32_t r = par[z.off + c];
+        if (r < 0) continue;
+        CompStat &q = cs[rid[z.off + r]];
+        const int x = int(c % z.nx), y = int(c / z.nx);
+        atomicAdd(&q.cells, 1u);
+        atomicMin(&q.minx, x); atomicMin(&q.minz, y);
+        atomicAdd(reinterpret_cast<unsigned long long *>(&q.sx), (unsigned long long)x);
+        atomicAdd(reinterpret_cast<unsigned long long *>(&q.sz), (unsigned long long)y);
+        if (interior(b, z, x, y)) atomicAdd(&q.inner, 1u);
+    }
+}
+// Components of at least min_cells cells are kept; each gets a segment for its interior keys.
+__global__ void k_cc_keep(CompStat *__restrict__ cs, uint32_t min_cells, uint32_t *ctr) {
+    const uint32_t n = *ctr;
+    for (uint32_t id = blockIdx.x * blockDim.x + threadIdx.x; id < n; id += gridDim.x * blockDim.x) {
+        CompStat &q = cs[id];
+        if (q.cells < min_cells) continue;
+        q.kid = int32_t(atomicAdd(ctr + 1, 1u));
+        q.seg = atomicAdd(ctr + 2, q.inner);
+    }
+}
+// Interior cells of kept components as 96-bit keys (squared distance to the centroid, raster index), the
+// order of the reference's sorted `inner` list; the arithmetic is the host's, operation by operation.
+__global__ void __launch_bounds__(256) k_cc_keys(const DZone *__restrict__ zones, const uint8_t *__restrict__ bits, const int32_t *__restrict__ par,
+                                                 const int32_t *__restrict__ rid, CompStat *__restrict__ cs, uint64_t *__restrict__ khi,
+                                                 uint32_t *__restrict__ klo) {
+    const DZone z = zones[blockIdx.x];
+    const int64_t n = int64_t(z.nx) * z.nz, c0 = int64_t(blockIdx.y) * CHUNK, c1 = min(n, c0 + CHUNK);
+    const uint8_t *b = bits + z.off;
+    for (int64_t c = c0 + threadIdx.x; c < c1; c += blockDim.x) {
+        const int32_t r = par[z.off + c];
+        if (r < 0) continue;
+        CompStat &q = cs[rid[z.off + r]];
+        if (q.kid < 0) continue;
+        const int x = int(c % z.nx), y = int(c / z.nx);
+        if (!interior(b, z, x, y)) continue;
+        const double cx = double(q.sx) / double(q.cells), cz = double(q.sz) / double(q.cells);
+        const double d = __dadd_rn(__dmul_rn(x - cx, x - cx), __dmul_rn(y - cz, y - cz));
+        const uint32_t at = q.seg + atomicAdd(&q.cur, 1u);
+        khi[at] = uint64_t(__double_as_longlong(d));       // d >= 0: the bit pattern orders like the value
+        klo[at] = uint32_t(c);
+    }
+}
+// One block per kept component: the interior keys at ranks 0, n/3 and 2n/3, by an exact radix selection
+// over the 12 bytes of the key (all three ranks in each pass).
+__global__ void __launch_bounds__(256) k_cc_select(const CompStat *__restrict__ cs, const uint64_t *__restrict__ khi, const uint32_t *__restrict__ klo,
+                                                   const uint32_t *ctr, dsg_component *__restrict__ rec) {
+    __shared__ uint32_t hist[3][256];
+    __shared__ uint64_t pre_hi[3];
+    __shared__ uint32_t pre_lo[3], want[3];
+    const uint32_t ncomp = ctr[0];
+    for (uint32_t id = blockIdx.x; id < ncomp; id += gridDim.x) {
+        const CompStat q = cs[id];
+        if (q.kid < 0) continue;
+        dsg_component &o = rec[q.kid];
+        const uint32_t n = q.inner;
+        if (threadIdx.x == 0) {
+            o.zone = q.zone; o.first = int32_t(q.first); o.cells = q.cells; o.minx = q.minx; o.minz = q.minz; o.inner = n;
+            for (int k = 0; k < 3; k++) { o.pick[k] = -1; pre_hi[k] = 0; pre_lo[k] = 0; }
+            want[0] = 0; want[1] = n / 3; want[2] = 2 * (n / 3) + ((2 * (n % 3)) / 3);   // floor(2n/3)
+        }
+        __syncthreads();
+        if (n == 0) { __syncthreads(); continue; }
+        const uint64_t *kh = khi + q.seg;
+        const uint32_t *kl = klo + q.seg;
+        for (int d = 11; d >= 0; d--) {
+            for (int i = threadIdx.x; i < 3 * 256; i += blockDim.x) (&hist[0][0])[i] = 0;
+            __syncthreads();
+            for (uint32_t i = threadIdx.x; i < n; i += blockDim.x) {
+                const uint64_t h = kh[i];
+                const uint32_t l = kl[i];
+                const uint32_t dig = d >= 4 ? uint32_t(h >> (8 * (d - 4))) & 255u : (l >> (8 * d)) & 255u;
+                #pragma unroll
+                for (int k = 0; k < 3; k++) {
+                    bool match;
+                    if (d >= 4) match = d == 11 || (h >> (8 * (d - 4) + 8)) == (pre_hi[k] >> (8 * (d - 4) + 8));
+                    else match = h == pre_hi[k] && (d == 3 || (l >> (8 * d + 8)) == (pre_lo[k] >> (8 * d + 8)));
+                    if (match) atomicAdd(&hist[k][dig], 1u);
+                }
+            }
+            __syncthreads();
+            if (threadIdx.x < 3) {
+                const int k = threadIdx.x;
+                uint32_t below = 0, b = 0;
+                for (; b < 255; b++) {
+                    if (below + hist[k][b] > want[k]) break;
+                    below += hist[k][b];
+                }
+                want[k] -= below;
+                if (d >= 4) pre_hi[k] |= uint64_t(b) << (8 * (d - 4));
+                else pre_lo[k] |= b << (8 * d);
+            }
+            __syncthreads();
+        }
+        if (threadIdx.x == 0)
+            for (int k = 0; k < 3; k++) o.pick[k] = int32_t(pre_lo[k]);
+        __syncthreads();
+    }
+}
+
 struct State {
     std::mutex mu;
     cudaStream_t st = nullptr;
@@ -38,6 +234,12 @@ struct State {
     uint64_t *d_seeds = nullptr; size_t seeds_cap = 0;
     DZone *d_zones = nullptr; size_t zone_cap = 0;
     uint8_t *d_out = nullptr; size_t out_cap = 0;
+    // component labelling (dsg_proxy_components): per cell, per component, per interior key; counters
+    int32_t *d_par = nullptr, *d_rid = nullptr; size_t par_cap = 0, rid_cap = 0;
+    CompStat *d_cs = nullptr; size_t cs_cap = 0;
+    uint64_t *d_khi = nullptr; uint32_t *d_klo = nullptr; size_t khi_cap = 0, klo_cap = 0;
+    dsg_component *d_rec = nullptr; size_t rec_cap = 0;
+    uint32_t *d_ctr = nullptr, *h_ctr = nullptr;   // [0] components [1] kept [2] interior keys [3] error
 };
 State &S() { static State s; return s; }
 template <class T> void grow(T *&p, size_t &cap, size_t need) {
@@ -85,7 +287,86 @@ int proxy_eval(const uint64_t *seeds, uint32_t nseeds, const uint32_t *zone_seed
     DSG_CU(cudaStreamSynchronize(g.st));
     return DSG_OK;
 }
+
+// Proxy bitmaps and their components in one pass on the device; only the kept components come back.
+int proxy_components(const uint64_t *seeds, uint32_t nseeds, const uint32_t *zone_seed, const dsg_zone *zones, uint32_t nzones,
+                     uint32_t min_cells, dsg_component *out, uint32_t cap, uint32_t *n_out, uint8_t *bits) {
+    State &g = S();
+    std::lock_guard<std::mutex> l(g.mu);
+    require_init();
+    *n_out = 0;
+    if (!g.st) {
+        int lo, hi;
+        DSG_CU(cudaDeviceGetStreamPriorityRange(&lo, &hi));
+        DSG_CU(cudaStreamCreateWithPriority(&g.st, cudaStreamNonBlocking, hi));
+    }
+    if (!g.d_ctr) {
+        DSG_CU(cudaMalloc(&g.d_ctr, 4 * 4));
+        DSG_CU(cudaMallocHost(&g.h_ctr, 4 * 4));
+    }
+    std::vector<DZone> dz(nzones);
+    int64_t off = 0, maxc = 0;
+    for (uint32_t k = 0; k < nzones; k++) {
+        const dsg_zone &z = zones[k];
+        DSG_ARG(z.nx >= 0 && z.nz >= 0, "dsg_proxy_components: negative zone size");
+        DSG_ARG(int64_t(z.nx) * z.nz < (int64_t(1) << 31), "dsg_proxy_components: zone too large");
+        DSG_ARG(zone_seed[k] < nseeds, "dsg_proxy_components: zone seed index out of range");
+        dz[k] = {z.x0, z.z0, z.nx, z.nz, off, int32_t(zone_seed[k]), 0};
+        off += int64_t(z.nx) * z.nz;
+        maxc = std::max(maxc, int64_t(z.nx) * z.nz);
+    }
+    if (!off) return DSG_OK;
+    DSG_ARG(maxc / CHUNK < 65535, "dsg_proxy_components: zone too large");
+    grow(g.d_noise, g.seed_cap, nseeds);
+    grow(g.d_seeds, g.seeds_cap, nseeds);
+    grow(g.d_zones, g.zone_cap, nzones);
+    grow(g.d_out, g.out_cap, size_t(off));
+    grow(g.d_par, g.par_cap, size_t(off));
+    grow(g.d_rid, g.rid_cap, size_t(off));
+    grow(g.d_cs, g.cs_cap, size_t(off));             // at most one component per cell
+    grow(g.d_khi, g.khi_cap, size_t(off));           // at most one interior key per cell
+    grow(g.d_klo, g.klo_cap, size_t(off));
+    grow(g.d_rec, g.rec_cap, size_t(off));
+    cudaStream_t st = g.st;
+    DSG_CU(cudaMemcpyAsync(g.d_seeds, seeds, size_t(nseeds) * 8, cudaMemcpyHostToDevice, st));
+    seed_noise_build(g.d_seeds, nseeds, g.d_noise, st);
+    DSG_CU(cudaMemcpyAsync(g.d_zones, dz.data(), dz.size() * sizeof(DZone), cudaMemcpyHostToDevice, st));
+    DSG_CU(cudaMemsetAsync(g.d_ctr, 0, 4 * 4, st));
+    const dim3 grid(nzones, unsigned((maxc + CHUNK - 1) / CHUNK));
+    k_proxy<<<grid, 256, 0, st>>>(g.d_noise, g.d_zones, world_dev(), g_cut, g.d_out);
+    k_cc_init<<<grid, 256, 0, st>>>(g.d_zones, g.d_out, g.d_par);
+    k_cc_merge<<<grid, 256, 0, st>>>(g.d_zones, g.d_out, g.d_par, g.d_ctr + 3);
+    k_cc_roots<<<grid, 256, 0, st>>>(g.d_zones, g.d_par, g.d_rid, g.d_cs, g.d_ctr);
+    k_cc_flatten<<<grid, 256, 0, st>>>(g.d_zones, g.d_par, g.d_ctr + 3);
+    k_cc_stats<<<grid, 256, 0, st>>>(g.d_zones, g.d_out, g.d_par, g.d_rid, g.d_cs);
+    k_cc_keep<<<(std::min<int64_t>(off, 1 << 20) + 255) / 256, 256, 0, st>>>(g.d_cs, min_cells, g.d_ctr);
+    k_cc_keys<<<grid, 256, 0, st>>>(g.d_zones, g.d_out, g.d_par, g.d_rid, g.d_cs, g.d_khi, g.d_klo);
+    k_cc_select<<<unsigned(std::min<int64_t>(off, 4 * 148)), 256, 0, st>>>(g.d_cs, g.d_khi, g.d_klo, g.d_ctr, g.d_rec);
+    DSG_CU(cudaGetLastError());
+    if (bits) DSG_CU(cudaMemcpyAsync(bits, g.d_out, size_t(off), cudaMemcpyDeviceToHost, st));
+    DSG_CU(cudaMemcpyAsync(g.h_ctr, g.d_ctr, 4 * 4, cudaMemcpyDeviceToHost, st));
+    DSG_CU(cudaStreamSynchronize(st));
+    if (g.h_ctr[3]) { set_error("dsg_proxy_components: component labelling did not converge"); return DSG_E_CUDA; }
+    const uint32_t kept = g.h_ctr[1];
+    *n_out = kept;
+    std::vector<dsg_component> rec(kept);
+    if (kept) {
+        DSG_CU(cudaMemcpyAsync(rec.data(), g.d_rec, size_t(kept) * sizeof(dsg_component), cudaMemcpyDeviceToHost, st));
+        DSG_CU(cudaStreamSynchronize(st));
+    }
+    std::sort(rec.begin(), rec.end(), [](const dsg_component &a, const dsg_component &b) { return a.zone != b.zone ? a.zone < b.zone : a.first < b.first; });
+    std::copy(rec.begin(), rec.begin() + std::min(kept, cap), out);
+    return kept > cap ? DSG_OVERFLOW : DSG_OK;
+}
 }  // namespace dsg
+
+extern "C" int dsg_proxy_components(const uint64_t *seeds, uint32_t nseeds, const uint32_t *zone_seed, const dsg_zone *zones, uint32_t nzones,
+                                    uint32_t min_cells, dsg_component *out, uint32_t cap, uint32_t *n_out, uint8_t *bits) {
+    return dsg::guarded([&] {
+        DSG_ARG(n_out && (nzones == 0 || (seeds && zone_seed && zones)) && (cap == 0 || out), "dsg_proxy_components: null pointer");
+        return dsg::proxy_components(seeds, nseeds, zone_seed, zones, nzones, min_cells, out, cap, n_out, bits);
+    });
+}
 
 extern "C" int dsg_proxy(uint64_t seed, const dsg_zone *zones, uint32_t nzones, uint8_t *bits) {
     return dsg::guarded([&] {

@@ -205,6 +205,33 @@ def proxy(seed, zones):
     return out
 
 
+class Component(C.Structure):
+    _fields_ = [("zone", C.c_uint32), ("first", C.c_int32), ("cells", C.c_uint32), ("minx", C.c_int32), ("minz", C.c_int32),
+                ("inner", C.c_uint32), ("pick", C.c_int32 * 3)]
+
+
+def proxy_components(seeds, zone_seed, zones, min_cells=1, cap=1 << 16):
+    """Proxy bitmaps of zones of several seeds and their 8-connected components, labelled on the device
+    (dsg_proxy_components): (list of component dicts in zone / first-cell order, list of (nz, nx) bitmaps)."""
+    s = np.ascontiguousarray([x & ((1 << 64) - 1) for x in seeds], dtype=np.uint64)
+    zsd = np.ascontiguousarray(zone_seed, dtype=np.uint32)
+    zs = (Zone * len(zones))(*[Zone(*z) for z in zones])
+    total = sum(z[2] * z[3] for z in zones)
+    bits = np.zeros(max(total, 1), dtype=np.uint8)
+    out = (Component * cap)()
+    n = C.c_uint32()
+    rc = _ck(lib.dsg_proxy_components(ptr(s, u64p), C.c_uint32(len(s)), ptr(zsd, u32p), zs, C.c_uint32(len(zones)), C.c_uint32(min_cells),
+                                      out, C.c_uint32(cap), C.byref(n), bits.ctypes.data_as(C.c_void_p)), "dsg_proxy_components")
+    assert rc == DSG_OK, "component capacity exceeded"
+    comps = [{"zone": c.zone, "first": c.first, "cells": c.cells, "minx": c.minx, "minz": c.minz, "inner": c.inner,
+              "pick": tuple(c.pick)} for c in out[:n.value]]
+    maps, off = [], 0
+    for z in zones:
+        maps.append(bits[off: off + z[2] * z[3]].reshape(z[3], z[2]))
+        off += z[2] * z[3]
+    return comps, maps
+
+
 DSG_PENDING = 2
 
 

@@ -3,8 +3,9 @@
 // (PREFIX.csv, PREFIX.seeds.csv, PREFIX.json; exclusive create), stderr lines (progress, best, CANDIDATE,
 // gscancheck, gpucheck) and exit codes, so deploy/gpipe.sh runs it unchanged with gate=1 gpu=1 gscan=1.
 //
-// Stage placement: every stage runs on the GPU through libdsgpu's C ABI; the host keeps the bookkeeping
-// the reference keeps on the host (NMS, hot-zone coverage, component labelling, result lines).  Seeds are
+// Stage placement: every stage runs on the GPU through libdsgpu's C ABI, the proxy components' labelling
+// and start selection included; the host keeps the rest of the bookkeeping the reference keeps on the host
+// (NMS, hot-zone coverage, result lines).  Seeds are
 // processed in batches: each stage is one batched call for all seeds of the batch, and where the
 // reference's per-seed loop is sequential (a site is skipped if an earlier site's hot zone covers it; a
 // later exact-flood start is tried only if the earlier ones fell short) the GPU evaluates every candidate
@@ -341,69 +342,55 @@ void Search::process(const std::vector<uint64_t> &seeds) {
     if (!zones.empty()) {
         std::vector<dsg_zone> dz; std::vector<uint32_t> zs; size_t total = 0;
         for (auto &z : zones) { dz.push_back({z.x0, z.z0, z.nx, z.nz}); zs.push_back(uint32_t(z.seed)); total += size_t(z.nx) * z.nz; }
-        std::vector<uint8_t> bits(total);
+        // smallest component whose area reaches 1 M blocks^2 (the reference drops smaller ones, :462)
+        uint32_t min_cells = 1;
+        while (min_cells * 32.0 * 32 * 16 / 1e6 < 1) min_cells++;
+        const bool check = P.gpucheck > 0;                  // gpucheck also needs the bitmaps themselves
+        std::vector<uint8_t> bits(check ? total : 0);
+        static thread_local std::vector<dsg_component> comps(4096);
+        uint32_t nc = 0;
         const auto tg0 = Clock::now();
-        ck(dsg_proxy_batch(seeds.data(), uint32_t(n), zs.data(), dz.data(), uint32_t(dz.size()), bits.data()), "gproxy");
+        for (;;) {
+            const int rc = dsg_proxy_components(seeds.data(), uint32_t(n), zs.data(), dz.data(), uint32_t(dz.size()), min_cells, comps.data(),
+                                                uint32_t(comps.size()), &nc, check ? bits.data() : nullptr);
+            ck(rc, "gproxy");
+            if (rc == DSG_OK) break;
+            comps.resize(nc);                               // more components than room: rerun with room for all
+        }
         t_gpu += std::chrono::duration<double>(Clock::now() - tg0).count();
-        size_t off = 0;
-        std::vector<std::vector<std::pair<int, int>>> seen(n);
-        for (auto &zn : zones) {
-            uint8_t *b = &bits[off];
-            off += size_t(zn.nx) * zn.nz;
-            if (P.gpucheck > 0) {                           // spot-check every 7th cell against the CPU proxy (:445-450)
-                const hostcheck::Proxy PX(seeds[zn.seed], prob);
+        if (check) {
+            size_t off = 0;
+            for (auto &zn : zones) {
+                const uint8_t *b = &bits[off];
+                off += size_t(zn.nx) * zn.nz;
+                if (P.gpucheck <= 0) break;
+                const hostcheck::Proxy PX(seeds[zn.seed], prob);       // every 7th cell against the CPU proxy (:445-450)
                 long diff = 0, tot = 0;
                 for (int c = 0; c < zn.nx * zn.nz; c += 7) { tot++; diff += (PX.p(zn.x0 + (c % zn.nx) * 32, zn.z0 + (c / zn.nx) * 32) >= float(P.pcut)) != (b[c] != 0); }
                 std::lock_guard<std::mutex> g(mu);
                 fprintf(stderr, "gpucheck zone %dx%d: %ld/%ld cells differ\n", zn.nx, zn.nz, diff, tot);
                 P.gpucheck--;
             }
-            for (int c0 = 0; c0 < zn.nx * zn.nz; c0++) {       // 8-connected components
-                if (b[c0] != 1) continue;
-                long cells = 0; int mx = zn.nx, mz = zn.nz;
-                std::vector<int> stk{c0}, comp; b[c0] = 2;
-                while (!stk.empty()) {
-                    const int c = stk.back(); stk.pop_back(); cells++; comp.push_back(c);
-                    const int cx = c % zn.nx, cz = c / zn.nx;
-                    mx = std::min(mx, cx); mz = std::min(mz, cz);
-                    for (int dzz = -1; dzz <= 1; dzz++) for (int dxx = -1; dxx <= 1; dxx++) {
-                        const int nx2 = cx + dxx, nz2 = cz + dzz;
-                        if (nx2 < 0 || nz2 < 0 || nx2 >= zn.nx || nz2 >= zn.nz) continue;
-                        const int k2 = nz2 * zn.nx + nx2;
-                        if (b[k2] == 1) { b[k2] = 2; stk.push_back(k2); }
-                    }
-                }
-                const double area = cells * 32.0 * 32 * 16 / 1e6;
-                if (area < 1) continue;
-                const std::pair<int, int> sig(zn.x0 + mx * 32, zn.z0 + mz * 32);
-                auto &sn = seen[zn.seed];
-                if (std::find(sn.begin(), sn.end(), sig) != sn.end()) continue;
-                sn.push_back(sig);
-                double cx = 0, cz = 0;
-                for (int c : comp) { cx += c % zn.nx; cz += c / zn.nx; }
-                cx /= comp.size(); cz /= comp.size();
-                std::vector<std::pair<double, int>> inner;
-                for (int c : comp) {
-                    const int x = c % zn.nx, z = c / zn.nx;
-                    bool ok = x > 0 && z > 0 && x < zn.nx - 1 && z < zn.nz - 1;
-                    for (int dzz = -1; ok && dzz <= 1; dzz++) for (int dxx = -1; dxx <= 1; dxx++) if (b[(z + dzz) * zn.nx + x + dxx] != 2) { ok = false; break; }
-                    if (ok) inner.push_back({(x - cx) * (x - cx) + (z - cz) * (z - cz), c});
-                }
-                // only ranks 0, n/3 and 2n/3 of the (distance, cell) order are used; the keys are unique, so
-                // selecting them gives the elements a full sort would put there
-                const size_t ni = inner.size();
-                if (ni) {
-                    std::nth_element(inner.begin(), inner.begin() + 2 * ni / 3, inner.end());
-                    std::nth_element(inner.begin(), inner.begin() + ni / 3, inner.begin() + 2 * ni / 3);
-                    std::nth_element(inner.begin(), inner.begin(), inner.begin() + ni / 3);
-                }
-                auto cell_xy = [&](int c) { return std::pair<int, int>(zn.x0 + (c % zn.nx) * 32, zn.z0 + (c / zn.nx) * 32); };
-                const auto first = inner.empty() ? cell_xy(c0) : cell_xy(inner[0].second);
-                Eval e{zn.rank, first.first, first.second, area};
-                e.hot = zn.hot;
-                for (int t = 1; t < 3 && size_t(t) * inner.size() / 3 < inner.size() && !inner.empty(); t++) e.alt.push_back(cell_xy(inner[size_t(t) * inner.size() / 3].second));
-                ev[zn.seed].push_back(e);
-            }
+        }
+        // components in the reference's order (zone, then first cell): drop those under 1 M blocks^2 and those
+        // already met through another zone of the seed (same smallest column and row); the start is the interior
+        // cell nearest the centroid, with the cells at ranks n/3 and 2n/3 as alternatives (:451-490)
+        std::vector<std::vector<std::pair<int, int>>> seen(n);
+        for (uint32_t k = 0; k < nc; k++) {
+            const dsg_component &c = comps[k];
+            const Zone &zn = zones[c.zone];
+            const double area = c.cells * 32.0 * 32 * 16 / 1e6;
+            if (area < 1) continue;
+            const std::pair<int, int> sig(zn.x0 + c.minx * 32, zn.z0 + c.minz * 32);
+            auto &sn = seen[zn.seed];
+            if (std::find(sn.begin(), sn.end(), sig) != sn.end()) continue;
+            sn.push_back(sig);
+            auto cell_xy = [&](int cell) { return std::pair<int, int>(zn.x0 + (cell % zn.nx) * 32, zn.z0 + (cell / zn.nx) * 32); };
+            const auto first = c.inner ? cell_xy(c.pick[0]) : cell_xy(c.first);
+            Eval e{zn.rank, first.first, first.second, area};
+            e.hot = zn.hot;
+            if (c.inner) { e.alt.push_back(cell_xy(c.pick[1])); e.alt.push_back(cell_xy(c.pick[2])); }
+            ev[zn.seed].push_back(e);
         }
     }
     std::vector<std::vector<std::string>> zrows(n);

@@ -122,6 +122,25 @@ int dsg_proxy(uint64_t seed, const dsg_zone *zones, uint32_t nzones, uint8_t *bi
 int dsg_proxy_batch(const uint64_t *seeds, uint32_t nseeds, const uint32_t *zone_seed, const dsg_zone *zones, uint32_t nzones,
                     uint8_t *bits);
 
+/* An 8-connected component of a zone's proxy bitmap (cells in zone coordinates: column x, row z, raster
+ * index z * nx + x).  pick: the interior cells (all 8 neighbours in the component, not on the zone's edge)
+ * at ranks 0, inner/3 and 2*inner/3 when ordered by (squared distance to the component's centroid, raster
+ * index) -- the exact-flood start and its two alternatives of dsearch_desert.cpp:465-490; -1 if inner == 0. */
+typedef struct dsg_component {
+    uint32_t zone;          /* index into zones */
+    int32_t first;          /* raster index of the component's first cell (where the reference's scan meets it) */
+    uint32_t cells;         /* cells in the component */
+    int32_t minx, minz;     /* smallest column and row */
+    uint32_t inner;         /* interior cells */
+    int32_t pick[3];
+} dsg_component;
+/* Proxy bitmaps of zones (as dsg_proxy_batch) and their components, labelled on the device
+ * (dsearch_desert.cpp:451-490, the reference's host labelling): components of at least min_cells cells,
+ * ordered by zone, then by first cell.  bits (may be NULL) receives the bitmaps too.  At most cap records are
+ * written; *n_out gets the number of kept components; DSG_OVERFLOW if that exceeds cap. */
+int dsg_proxy_components(const uint64_t *seeds, uint32_t nseeds, const uint32_t *zone_seed, const dsg_zone *zones, uint32_t nzones,
+                         uint32_t min_cells, dsg_component *out, uint32_t cap, uint32_t *n_out, uint8_t *bits);
+
 /* ---------------------------------------------------------------- floods (S3 hot zones, S5 exact areas) */
 #define DSG_PRED_DESERT 0   /* bridged desert state at Y=256: desert counted, river to desert crossed (surface.hpp:98-124) */
 #define DSG_PRED_HOT    1   /* temperature >= 0.55, unwarped (dsearch_desert.cpp:334) */
