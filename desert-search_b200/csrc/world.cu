@@ -4,7 +4,10 @@
 #include "common.cuh"
 #include "world.cuh"
 #include <algorithm>
+#include <future>
+#include <memory>
 #include <stdexcept>
+#include <string>
 #include <vector>
 
 extern "C" const unsigned char dsw_worldgen_blob[];
@@ -276,7 +279,9 @@ void build_cand_grid(WorldDev &w) {
         std::copy(c.begin(), c.end(), w.ccut[a]);
     }
 }
-void build_candidates(const Blob &b, WorldDev &w) {
+// Runs on its own non-blocking stream, with stream-ordered temporaries, so that it overlaps whatever other
+// threads start on the device meanwhile (no device-wide synchronisation).
+void build_candidates(const Blob &b, WorldDev &w, cudaStream_t st) {
     static const int SLOT[5] = {0, 1, 2, 3, 5};
     build_cand_grid(w);
     std::vector<LeafBox> leaves;
@@ -298,13 +303,14 @@ void build_candidates(const Blob &b, WorldDev &w) {
     for (int a = 0; a < 5; a++) ncell *= uint32_t(w.cdim[a]);
     LeafBox *d_leaves = nullptr; uint32_t *d_cnt = nullptr, *d_off = nullptr; uint16_t *d_cand = nullptr, *d_leaf_of = nullptr, *d_n = nullptr;
     try {
-        DSG_CU(cudaMalloc(&d_leaves, leaves.size() * sizeof(LeafBox)));
-        DSG_CU(cudaMemcpy(d_leaves, leaves.data(), leaves.size() * sizeof(LeafBox), cudaMemcpyHostToDevice));
-        DSG_CU(cudaMalloc(&d_cnt, size_t(ncell) * 4));
-        k_cand<<<ncell, 256>>>(d_leaves, int(leaves.size()), w, d_cnt, nullptr, nullptr);
+        DSG_CU(cudaMallocAsync(reinterpret_cast<void **>(&d_leaves), leaves.size() * sizeof(LeafBox), st));
+        DSG_CU(cudaMemcpyAsync(d_leaves, leaves.data(), leaves.size() * sizeof(LeafBox), cudaMemcpyHostToDevice, st));
+        DSG_CU(cudaMallocAsync(reinterpret_cast<void **>(&d_cnt), size_t(ncell) * 4, st));
+        k_cand<<<ncell, 256, 0, st>>>(d_leaves, int(leaves.size()), w, d_cnt, nullptr, nullptr);
         DSG_CU(cudaGetLastError());
         std::vector<uint32_t> cnt(ncell), off(size_t(ncell) + 1, 0);
-        DSG_CU(cudaMemcpy(cnt.data(), d_cnt, size_t(ncell) * 4, cudaMemcpyDeviceToHost));
+        DSG_CU(cudaMemcpyAsync(cnt.data(), d_cnt, size_t(ncell) * 4, cudaMemcpyDeviceToHost, st));
+        DSG_CU(cudaStreamSynchronize(st));
         uint64_t total = 0;
         for (uint32_t c = 0; c < ncell; c++) {
             total += cnt[c];
@@ -312,20 +318,29 @@ void build_candidates(const Blob &b, WorldDev &w) {
             off[c + 1] = uint32_t(total);
         }
         DSG_CU(cudaMalloc(&d_off, off.size() * 4));
-        DSG_CU(cudaMemcpy(d_off, off.data(), off.size() * 4, cudaMemcpyHostToDevice));
+        DSG_CU(cudaMemcpyAsync(d_off, off.data(), off.size() * 4, cudaMemcpyHostToDevice, st));
         DSG_CU(cudaMalloc(&d_cand, size_t(off[ncell]) * 2 + 2));
-        k_cand<<<ncell, 256>>>(d_leaves, int(leaves.size()), w, nullptr, d_off, d_cand);
+        k_cand<<<ncell, 256, 0, st>>>(d_leaves, int(leaves.size()), w, nullptr, d_off, d_cand);
         DSG_CU(cudaGetLastError());
         std::vector<uint16_t> leaf_of(b.tree.size(), 0);
         for (size_t k = 0; k < leaves.size(); k++) leaf_of[leaves[k].node] = uint16_t(k);
-        DSG_CU(cudaMalloc(&d_leaf_of, leaf_of.size() * 2));
-        DSG_CU(cudaMemcpy(d_leaf_of, leaf_of.data(), leaf_of.size() * 2, cudaMemcpyHostToDevice));
+        DSG_CU(cudaMallocAsync(reinterpret_cast<void **>(&d_leaf_of), leaf_of.size() * 2, st));
+        DSG_CU(cudaMemcpyAsync(d_leaf_of, leaf_of.data(), leaf_of.size() * 2, cudaMemcpyHostToDevice, st));
         DSG_CU(cudaMalloc(&d_n, size_t(ncell) * 2));
-        k_cand_prune<<<ncell, 256>>>(d_leaves, d_leaf_of, w, d_off, d_cand, d_n);
+        k_cand_prune<<<ncell, 256, 0, st>>>(d_leaves, d_leaf_of, w, d_off, d_cand, d_n);
         DSG_CU(cudaGetLastError());
-        DSG_CU(cudaDeviceSynchronize());
-    } catch (...) { cudaFree(d_leaves); cudaFree(d_cnt); cudaFree(d_off); cudaFree(d_cand); cudaFree(d_leaf_of); cudaFree(d_n); throw; }
-    cudaFree(d_leaves); cudaFree(d_cnt); cudaFree(d_leaf_of);
+        DSG_CU(cudaFreeAsync(d_leaves, st)); d_leaves = nullptr;
+        DSG_CU(cudaFreeAsync(d_cnt, st)); d_cnt = nullptr;
+        DSG_CU(cudaFreeAsync(d_leaf_of, st)); d_leaf_of = nullptr;
+        DSG_CU(cudaStreamSynchronize(st));              // off, leaf_of: host vectors copied from above
+    } catch (...) {
+        cudaStreamSynchronize(st);
+        if (d_leaves) cudaFreeAsync(d_leaves, st);
+        if (d_cnt) cudaFreeAsync(d_cnt, st);
+        if (d_leaf_of) cudaFreeAsync(d_leaf_of, st);
+        cudaFree(d_off); cudaFree(d_cand); cudaFree(d_n);
+        throw;
+    }
     w.cand_off = d_off; w.cand = d_cand; w.cand_n = d_n;
 }
 template <class T> const T *upload(const std::vector<T> &v) {
@@ -336,11 +351,17 @@ template <class T> const T *upload(const std::vector<T> &v) {
 }
 }  // namespace
 
-const WorldDev &world_dev() { return g_world; }
+// Candidate lists under construction (dsg_init returns before they are done): every reader of the world
+// tables waits for them here; a failure of the build is reported to each caller.
+namespace { std::shared_future<void> g_cand_ready; }
+const WorldDev &world_dev() {
+    if (g_cand_ready.valid()) g_cand_ready.get();
+    return g_world;
+}
 namespace { std::vector<float> g_prob; }
 const std::vector<float> &proxy_table() { return g_prob; }
 
-void world_upload(int) {
+void world_upload(int device) {
     const Blob b = parse_blob();
     WorldDev w{};
     std::vector<int16_t> cells;
@@ -350,10 +371,35 @@ void world_upload(int) {
     w.ntree = int(b.tree.size()); w.nspl = int(b.spl.size()); w.nparam = int(b.param.size() / 2);
     if (b.param.size() > 2 * 256) throw std::runtime_error("worldgen blob: too many parameter intervals");
     check_tree(b);
-    build_candidates(b, w);
+    if (g_cand_ready.valid()) g_cand_ready.wait();       // a build for an earlier dsg_init finishes first
     w.cells = upload(cells); w.tree = upload(b.tree); w.param = upload(b.param); w.spl = upload(b.spl); w.prob = upload(b.prob);
-    g_world = w;
     g_prob = b.prob;
+    // The exact-classification candidate lists take a few hundred milliseconds of GPU work.  They are built on
+    // a worker thread while the caller goes on (the gate, tables and scan do not use them); the entry points
+    // that classify exactly wait for them in world_dev().
+    auto blob = std::make_shared<const Blob>(b);
+    g_world = w;
+    g_cand_ready = std::async(std::launch::async, [blob, device] {
+        cudaStream_t st = nullptr;
+        try {
+            DSG_CU(cudaSetDevice(device));
+            DSG_CU(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
+            WorldDev c = g_world;
+            build_candidates(*blob, c, st);
+            cudaStreamDestroy(st);
+            for (int a = 0; a < 5; a++) {
+                g_world.cdim[a] = c.cdim[a]; g_world.nccut[a] = c.nccut[a];
+                std::copy(c.ccut[a], c.ccut[a] + 48, g_world.ccut[a]);
+            }
+            g_world.cand_off = c.cand_off; g_world.cand = c.cand; g_world.cand_n = c.cand_n;
+        } catch (const std::exception &ex) {
+            if (st) cudaStreamDestroy(st);
+            throw std::runtime_error(std::string("exact-classification candidate lists: ") + ex.what());
+        } catch (...) {
+            if (st) cudaStreamDestroy(st);
+            throw std::runtime_error(std::string("exact-classification candidate lists: ") + dsg_last_error());
+        }
+    }).share();
 }
 }  // namespace dsg
 
