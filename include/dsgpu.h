@@ -27,7 +27,9 @@ const char *dsg_last_error(void);
 
 /* Select the device, upload the worldgen tables (biome tree, surface grid, splines, proxy table) and set
  * the proxy cut.  Replaces gproxy::init(device, cut) (src/gpu/gproxy.h:35, src/gpu/gproxy.cu:391-401).
- * Idempotent for the same device; cut may be changed by a later call. */
+ * Idempotent for the same device; cut may be changed by a later call.  The candidate lists of the exact
+ * biome classification are built on the device in the background after dsg_init returns (about 0.2 s of GPU
+ * work): the gate, tables and scan do not wait for them; the first flood, point, query or proxy call does. */
 int dsg_init(int device, float cut);
 
 /* ---------------------------------------------------------------- seed gate (S0) */
