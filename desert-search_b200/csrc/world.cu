@@ -4,6 +4,7 @@
 #include "common.cuh"
 #include "world.cuh"
 #include <algorithm>
+#include <cstdlib>
 #include <future>
 #include <memory>
 #include <stdexcept>
@@ -400,6 +401,13 @@ void world_upload(int device) {
             throw std::runtime_error(std::string("exact-classification candidate lists: ") + dsg_last_error());
         }
     }).share();
+    // A process that exits normally while the build still runs waits for it first: this handler is registered
+    // after the CUDA runtime's own (made at the first CUDA call above), so it runs before the runtime's teardown.
+    static bool waits_at_exit = false;
+    if (!waits_at_exit) {
+        waits_at_exit = true;
+        std::atexit([] { if (g_cand_ready.valid()) g_cand_ready.wait(); });
+    }
 }
 }  // namespace dsg
 

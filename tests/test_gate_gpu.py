@@ -112,3 +112,17 @@ def test_gate_deterministic(dsg):
     a = dsg.gate_amps(seeds)
     b = dsg.gate_amps(seeds)
     assert np.array_equal(a[0], b[0]) and np.array_equal(a[1], b[1])
+
+
+def test_process_exits_cleanly_right_after_init():
+    """dsg_init returns while the exact-classification candidate lists are still being built on a worker
+    thread; a process that exits at once waits for that build instead of tearing the CUDA runtime down
+    under it.  Also: a gate call right after dsg_init does not wait for the build."""
+    import subprocess
+    import sys
+    pkg = os.path.join(os.path.dirname(os.path.dirname(os.path.abspath(__file__))), "desert-search_b200")
+    code = ("import sys; sys.path.insert(0, %r); import dsgpu; dsgpu.init(0, 0.35); "
+            "p, f = dsgpu.phase([1, 2, 3]); print('ok', len(p))") % pkg
+    r = subprocess.run([sys.executable, "-c", code], capture_output=True, text=True, timeout=300)
+    assert r.returncode == 0, r.stderr[-2000:]
+    assert r.stdout.strip() == "ok 3"
