@@ -46,6 +46,38 @@ def dist():
     return rank, world, local
 
 
+def shard_start(rank):
+    """First seed index of a rank: per-GPU ranges 10^12 apart, as deploy/prun.sh:15 assigns them."""
+    return START + rank * RANK_STRIDE
+
+
+class Replicas:
+    """What the ranks of a multi-GPU run exchange: nothing on the data path, only the device times (max over
+    ranks) and the pass counts (summed), through the process group (NCCL between GPUs; gloo works the same
+    on CPU).  Every rank makes the same calls in the same order."""
+
+    def __init__(self, pg=None, device="cuda"):
+        self.pg, self.device = pg, device
+
+    def barrier(self):
+        if self.pg:
+            self.pg.barrier()
+
+    def reduce(self, vals, op):
+        if not self.pg:
+            return [float(v) for v in vals]
+        import torch
+        t = torch.tensor([float(v) for v in vals], dtype=torch.float64, device=self.device)
+        self.pg.all_reduce(t, op=getattr(self.pg.ReduceOp, op))
+        return t.tolist()
+
+    def combine(self, ms, counts):
+        """(max device ms, summed counts {seeds, phase-passed, pre-passed, gated}, whole-job gated seeds/s)."""
+        ms_max = self.reduce([ms], "MAX")[0]
+        tot = self.reduce(counts, "SUM")
+        return ms_max, tot, tot[3] / (ms_max / 1e3)
+
+
 class Clocks:
     """nvidia-smi samples of this GPU's clocks during the timed region."""
     Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
@@ -295,19 +327,9 @@ def run_ours(args):
         td.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=120))
         pg = td
     dsgpu.init(local, 0.35)
-    base = START + rank * RANK_STRIDE
-
-    def barrier():
-        if pg:
-            pg.barrier()
-
-    def reduce(vals, op):
-        if not pg:
-            return vals
-        import torch
-        t = torch.tensor(vals, dtype=torch.float64, device="cuda")
-        pg.all_reduce(t, op=op)
-        return t.tolist()
+    base = shard_start(rank)
+    rep = Replicas(pg, "cuda")
+    barrier = rep.barrier
 
     if args.flood_only:
         if rank == 0:
@@ -319,12 +341,7 @@ def run_ours(args):
     ms, mk, counts = dsgpu.gate_bench(base, PER_STEP, args.steps, args.warmup)
     clocks = clk.stop()
     barrier()
-    if pg:
-        ms_max = reduce([ms], pg.ReduceOp.MAX)[0]
-        tot = reduce([float(x) for x in counts], pg.ReduceOp.SUM)
-    else:
-        ms_max, tot = ms, [float(x) for x in counts]
-    value = tot[3] / (ms_max / 1e3)
+    ms_max, tot, value = rep.combine(ms, counts)
 
     if args.profile_run:
         if rank == 0:
@@ -336,11 +353,8 @@ def run_ours(args):
     s, a, c, rc = dsgpu.gate_run(base + (args.steps + args.warmup) * PER_STEP, args.steps * PER_STEP, batch=PER_STEP, cap=1 << 20)
     e2e_s = time.perf_counter() - t0
     barrier()
-    if pg:
-        e2e_s = reduce([e2e_s], pg.ReduceOp.MAX)[0]
-        e2e_n = reduce([float(c[3])], pg.ReduceOp.SUM)[0]
-    else:
-        e2e_n = float(c[3])
+    e2e_s = rep.reduce([e2e_s], "MAX")[0]
+    e2e_n = rep.reduce([c[3]], "SUM")[0]
     d2h = 16 + int(c[3]) * 12 // max(1, args.steps)      # counters + (seed, amp) of survivors per step
 
     # roofline of the dominant kernel (the anti-aliased pre-gate): corner-table gathers from shared memory
