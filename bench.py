@@ -39,6 +39,10 @@ RANK_STRIDE = 10**12            # per-GPU seed ranges, as deploy/prun.sh assigns
 # pre-gate: 2 sides x 256^2 cells x 18 corner-table gathers of 4 bytes per phase-passed seed
 PRE_BYTES_PER_SEED = 2 * 256 * 256 * 18 * 4
 SMEM_BYTES_PER_CLK_PER_SM = 128  # 32 banks x 4 bytes
+# k_pregate DRAM traffic per phase-passed seed from one ncu capture (dram__bytes_read.sum + write.sum =
+# 150.7 MB + 4.2 MB over 241,519 seeds on 2^25 seed indices): the seed's octave table read once; scaled to a
+# launch by the phase-passed seeds it processes
+PRE_DRAM_BYTES_PER_SEED = (150.7e6 + 4.2e6) / 241519
 
 
 def dist():
@@ -377,8 +381,10 @@ def run_ours(args):
         "kernel_ms": {"phase": float(mk[0]), "octave_init": float(mk[1]), "pregate": float(mk[2]), "fullgate": float(mk[3])},
         "e2e": {"value": e2e_n / e2e_s, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": d2h},
         "roofline": {"bound": "smem", "kernel": "k_pregate", "achieved": achieved, "peak": peak, "unit": "GB/s",
-                     "frac": achieved / peak, "traffic": None,
-                     "note": "shared-memory gather bytes (18 corner-table words per cell); peak = SMs x 128 B/clk at the median SM clock sampled during the run"},
+                     "frac": achieved / peak, "traffic": counts[1] / args.steps * PRE_DRAM_BYTES_PER_SEED,
+                     "note": "shared-memory gather bytes (18 corner-table words per cell); peak = SMs x 128 B/clk at the median SM clock "
+                             "sampled during the run; traffic = DRAM bytes per launch, scaled from an ncu capture on 2^25 seed indices "
+                             "by the phase-passed seeds of a launch"},
         "gpu_launches": 4 * args.steps,
         "clocks": clocks,
     }
