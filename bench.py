@@ -40,9 +40,9 @@ RANK_STRIDE = 10**12            # per-GPU seed ranges, as deploy/prun.sh assigns
 PRE_BYTES_PER_SEED = 2 * 256 * 256 * 18 * 4
 SMEM_BYTES_PER_CLK_PER_SM = 128  # 32 banks x 4 bytes
 # k_pregate DRAM traffic per phase-passed seed from one ncu capture (dram__bytes_read.sum + write.sum =
-# 150.7 MB + 4.2 MB over 241,519 seeds on 2^25 seed indices): the seed's octave table read once; scaled to a
+# 150.5 MB + 6.1 MB over 241,519 seeds on 2^25 seed indices): the seed's octave table read once; scaled to a
 # launch by the phase-passed seeds it processes
-PRE_DRAM_BYTES_PER_SEED = (150.7e6 + 4.2e6) / 241519
+PRE_DRAM_BYTES_PER_SEED = (150.5e6 + 6.1e6) / 241519
 
 
 def dist():
