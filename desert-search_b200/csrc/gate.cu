@@ -13,6 +13,7 @@
 //  * the whole batch (phase -> init -> pre-gate -> full gate) runs from device-side counts: no host sync
 //    between stages, so a batch can be captured in a CUDA graph.
 #include "common.cuh"
+#include "gate_tuned.h"
 #include <cooperative_groups.h>
 #include <algorithm>
 #include <mutex>
@@ -31,7 +32,7 @@ static_assert(sizeof(Oct) == 304, "Oct layout");
 struct Taps { float k9[9], k15[15], norm9, norm15, w; };
 
 constexpr int PG_THREADS = 64, PG_BAND = 256;      // pre-gate: a warp per side, 256 rows each
-constexpr int FG_THREADS = 128, FG_RB = 8;           // full gate: thread per 4 columns, 8-row blocks
+constexpr int FG_THREADS = 128, FG_RB = DSG_FG_ROWS; // full gate: thread per 4 columns, row blocks
 
 // ---------------------------------------------------------------- device math
 // fade as the reference's GPU gate evaluates it: nvcc contracts t*6-15 and t*(..)+10 (gate.cuh:51).
@@ -151,7 +152,7 @@ __device__ __forceinline__ void add_row(const char *__restrict__ tcb, const uint
 }
 
 // Anti-aliased pre-gate (gate.cuh stream_max<256,4,8,true>).  Warp = noise side.
-__global__ void __launch_bounds__(PG_THREADS, 6)
+__global__ void __launch_bounds__(PG_THREADS, DSG_PG_MINBLOCKS)
 k_pregate(const Oct *__restrict__ oct, const uint64_t *__restrict__ seeds, const uint32_t *__restrict__ n_in, uint32_t cap_in,
           float thr, Taps tp, uint64_t *__restrict__ out_seed, uint32_t *__restrict__ out_idx, uint32_t *__restrict__ n_out,
           uint32_t cap_out, float *__restrict__ side_amp) {
@@ -298,7 +299,7 @@ k_pregate(const Oct *__restrict__ oct, const uint64_t *__restrict__ seeds, const
 // them back as 128-bit vectors, and the vertical blur accumulates 14 pending FMA chains per column in
 // registers.
 constexpr int FG_COLS = 4;
-__global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(FG_THREADS, 4)
+__global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(FG_THREADS, DSG_FG_MINBLOCKS)
 k_fullgate(const Oct *__restrict__ oct, const uint64_t *__restrict__ seeds, const uint32_t *__restrict__ idx, const uint32_t *__restrict__ n_in,
            uint32_t cap_in, float thr, Taps tp, uint64_t *__restrict__ out_seed, float *__restrict__ out_amp, uint32_t *__restrict__ n_out,
            uint32_t cap_out, float *__restrict__ side_amp) {
