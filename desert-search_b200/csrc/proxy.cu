@@ -24,10 +24,13 @@ struct CompStat { uint32_t zone, first, cells, inner; int32_t minx, minz, kid; u
 
 __global__ void __launch_bounds__(256) k_proxy(const SeedNoise *__restrict__ noise, const DZone *__restrict__ zones, WorldDev w, float cut,
                                                uint8_t *__restrict__ out) {
+    __shared__ SeedNoise S;                               // the zone's seed: every Perlin lookup from shared memory
     const DZone z = zones[blockIdx.x];
     const int64_t n = int64_t(z.nx) * z.nz, c0 = int64_t(blockIdx.y) * CHUNK, c1 = min(n, c0 + CHUNK);
     if (c0 >= n) return;
-    const SeedNoise &S = noise[z.seed];
+    const uint4 *src = reinterpret_cast<const uint4 *>(noise + z.seed);
+    for (int k = threadIdx.x; k < int(sizeof(SeedNoise) / 16); k += blockDim.x) reinterpret_cast<uint4 *>(&S)[k] = __ldg(src + k);
+    __syncthreads();
     for (int64_t c = c0 + threadIdx.x; c < c1; c += blockDim.x) {
         const int ci = int(c % z.nx), cj = int(c / z.nx);
         out[z.off + c] = proxy_prob(S, w, z.x0 + 32 * ci, z.z0 + 32 * cj) >= cut;
