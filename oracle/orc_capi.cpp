@@ -81,6 +81,22 @@ int orc_noise(uint64_t seed, int ch, const double *xyz, int n, double *out) {
     for (int i = 0; i < n; i++) out[i] = S.nz[ch].sample(xyz[3 * i], xyz[3 * i + 1], xyz[3 * i + 2]);
     return 0;
 }
+// Sub-grid pre-gate estimates of both sides of n seeds (lowfield.hpp:60-102), out[2i + side], on `threads`.
+int orc_subgate(const uint64_t *seeds, int n, float *out, int threads) {
+    std::atomic<int> next(0);
+    auto work = [&] {
+        for (int i; (i = next++) < n;) {
+            const Seed S(seeds[i]);
+            const Noise &T = S.nz[0];
+            for (int side = 0; side < 2; side++) out[2 * i + side] = subgate_side(T.oct[side][0], T.factor * T.oct[side][0].amp);
+        }
+    };
+    std::vector<std::thread> pool;
+    for (int t = 1; t < std::max(1, threads); t++) pool.emplace_back(work);
+    work();
+    for (auto &t : pool) t.join();
+    return 0;
+}
 // Octaves [lo, hi) of channel `ch`, both sides, at quart points (x, 0, z) (desert_proxy.hpp:13-23).
 int orc_noise_low(uint64_t seed, int ch, int lo, int hi, const int32_t *xz, int n, double *out) {
     const Seed S(seed);

@@ -402,6 +402,58 @@ inline double phase(uint64_t seed, double *fy = nullptr) {
     }
     return s;
 }
+// The CPU search's sub-grid pre-gate estimate of one side (lowfield.hpp:60-102): the temperature octave -10
+// on its own integer lattice (256^2 cells, one parity, 8 corner tables), blurred horizontally then vertically
+// by 9 taps exp(-d^2/2) normalised by their double sum, then the maximum.  Float sums in the written order.
+inline void subgate_taps(float *k) {
+    double s = 0;
+    for (int d = -4; d <= 4; d++) s += k[d + 4] = float(std::exp(-0.5 * d * d));
+    for (int i = 0; i < 9; i++) k[i] = float(k[i] / s);
+}
+inline float subgate_side(const Octave &p, double w) {
+    const uint8_t *P = p.perm;
+    uint8_t col[2][256];
+    for (int x = 0; x < 256; x++)
+        for (int dy = 0; dy < 2; dy++) col[dy][x] = P[(P[x] + p.iy + dy) & 255];
+    const int i0 = int(std::floor(p.ox)), k0 = int(std::floor(p.oz));
+    const double fx = p.ox - i0, fz = p.oz - k0;
+    float T[8][16];
+    const double tx = fade(fx), tz = fade(fz), ty = p.vy;
+    for (int c = 0; c < 8; c++) {
+        const int dx = c & 1, dy = (c >> 1) & 1, dz = c >> 2;
+        const double wc = (dx ? tx : 1 - tx) * (dy ? ty : 1 - ty) * (dz ? tz : 1 - tz);
+        for (int h = 0; h < 16; h++) T[c][h] = float(w * wc * grad(unsigned(h), fx - dx, p.fy - dy, fz - dz));
+    }
+    std::vector<float> t(256 * 256), tmp(256 * 256);
+    for (int j = 0; j < 256; j++) {
+        const int iz = j + k0;
+        for (int i = 0; i < 256; i++) {
+            const int ix = i + i0;
+            float acc = 0;
+            for (int c = 0; c < 8; c++) {
+                const int dx = c & 1, dy = (c >> 1) & 1, dz = c >> 2;
+                acc += T[c][P[(col[dy][(ix + dx) & 255] + iz + dz) & 255] & 15];
+            }
+            t[j * 256 + i] = acc;
+        }
+    }
+    float k[9];
+    subgate_taps(k);
+    for (int j = 0; j < 256; j++)
+        for (int i = 0; i < 256; i++) {
+            float a = 0;
+            for (int d = -4; d <= 4; d++) a += k[d + 4] * t[j * 256 + ((i + d) & 255)];
+            tmp[j * 256 + i] = a;
+        }
+    float m = -9;
+    for (int j = 0; j < 256; j++)
+        for (int i = 0; i < 256; i++) {
+            float a = 0;
+            for (int d = -4; d <= 4; d++) a += k[d + 4] * tmp[((j + d) & 255) * 256 + i];
+            m = std::max(m, a);
+        }
+    return m;
+}
 // Temperature octave -10 of one side as the GPU gate derives it (gate.cuh:59-70): vy uses the fused fade.
 struct GateOctave { uint8_t perm[256]; double ox, oy, oz, fy, vy; int iy; };
 inline GateOctave gate_octave(uint64_t seed, int side) {

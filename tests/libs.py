@@ -151,6 +151,14 @@ def ref():
     return CpuPath(lib, "ref")
 
 
+def orc_subgate(seeds, threads=8):
+    """Oracle sub-grid pre-gate estimates (the CPU search's gate, lowfield.hpp:60-102), shape (n, 2)."""
+    s = np.ascontiguousarray(seeds, dtype=np.uint64)
+    out = np.empty(2 * len(s), dtype=np.float32)
+    orc().lib.orc_subgate(ptr(s, u64p), C.c_int(len(s)), ptr(out, f32p), C.c_int(threads))
+    return out.reshape(-1, 2)
+
+
 def orc_gate(seeds, want_full=True, k9=None, k15=None, threads=8):
     """Oracle pre-gate and full-gate side amplitudes, arrays of shape (n, 2); taps default to the
     reference GPU gate's."""

@@ -185,3 +185,17 @@ def test_reference_gpu_taps_vs_correctly_rounded():
     r9, r15 = libs.ref_gpu_taps()
     diff = np.r_[k9.view(np.int32) - r9.view(np.int32), k15.view(np.int32) - r15.view(np.int32)]
     assert set(np.unique(np.abs(diff))) <= {0, 1}
+
+
+def test_subgate_matches_reference_cpu_gate():
+    """The CPU search's sub-grid pre-gate (amplitude_sub, lowfield.hpp:60-102), restated by the oracle, equals
+    the reference's own function bit for bit on both sides of many seeds."""
+    import ctypes
+    r = libs.ref()
+    if r is None:
+        pytest.skip("oracle/_ref/libref_cpu.so not built")
+    seeds = [libs.mix(10**12 + k) for k in range(48)] + [libs.mix(7 * k + 3) for k in range(16)]
+    got = libs.orc_subgate(seeds)
+    want = np.array([[r.lib.ref_amplitude_sub(ctypes.c_uint64(s), side) for side in (0, 1)] for s in seeds], dtype=np.float32)
+    assert np.array_equal(got.view(np.uint32), want.view(np.uint32)), np.abs(got - want).max()
+    assert got.min() > 0 and got.max() < 1
