@@ -16,6 +16,7 @@
 #include "gate_tuned.h"
 #include <cooperative_groups.h>
 #include <algorithm>
+#include <cmath>
 #include <mutex>
 #include <vector>
 
@@ -288,6 +289,160 @@ k_pregate(const Oct *__restrict__ oct, const uint64_t *__restrict__ seeds, const
             if (amp >= thr) {
                 const uint32_t i = atomicAdd(n_out, 1u);
                 if (i < cap_out) { out_seed[i] = seeds[s]; out_idx[i] = s; }
+            }
+        }
+    }
+}
+
+// Sub-grid pre-gate of the CPU search (lowfield.hpp:60-102), the estimate dsearch_desert.cpp:216-223 tests when
+// it enumerates seeds itself: per side the temperature octave -10 on its own integer lattice (256^2 cells, one
+// parity), 8 corner tables of 16 gradient values (FP64 with the CPU's unfused fade, rounded to float), each cell
+// the float sum of its 8 corners in corner order, then a 9-tap blur along rows and along columns with separate
+// products and sums (the CPU code is built without contraction), and the maximum.  Same schedule as k_pregate:
+// one 64-thread CTA per seed, a warp per side streaming all 256 rows, hash-row words unpacked once and added
+// to the two sample rows that use them.
+struct SubTaps { float k[9]; double w; };
+__device__ __forceinline__ double fade_plain(double t) { return t * t * t * (t * (t * 6. - 15.) + 10.); }
+// Minecraft's 16 gradients, as gx*x + gy*y + gz*z with their 0/+-1 components (the CPU code's gradient)
+__constant__ signed char kGrad[16][3] = {{1, 1, 0}, {-1, 1, 0}, {1, -1, 0}, {-1, -1, 0}, {1, 0, 1}, {-1, 0, 1}, {1, 0, -1}, {-1, 0, -1},
+                                         {0, 1, 1}, {0, -1, 1}, {0, 1, -1}, {0, -1, -1}, {1, 1, 0}, {0, -1, 1}, {-1, 1, 0}, {0, -1, -1}};
+__device__ __forceinline__ double grad_products(int h, double x, double y, double z) {
+    h &= 15;
+    return double(kGrad[h][0]) * x + double(kGrad[h][1]) * y + double(kGrad[h][2]) * z;
+}
+// Offsets of hash row j of the current word group for the lane's lattice columns t = 0..8 (8 is the next
+// lane's column 0, periodic in 256).
+__device__ __forceinline__ void unpack_row9(const uint32_t (&W)[2][8], int j, int lane, uint32_t (&hb)[2][9]) {
+    const uint32_t sel = 0x4440u | uint32_t(j);
+    #pragma unroll
+    for (int dy = 0; dy < 2; dy++) {
+        #pragma unroll
+        for (int t = 0; t < 8; t++) hb[dy][t] = __byte_perm(W[dy][t], 0u, sel);
+        hb[dy][8] = __byte_perm(__shfl_sync(0xffffffffu, W[dy][0], (lane + 1) & 31), 0u, sel);
+    }
+}
+// The corner terms of one hash row as row offset V (dz) of the 8 cells' sums, S[e] = S0[e] + ..., in the
+// CPU's corner order c = dx + 2 dy + 4 dz.
+template <int V>
+__device__ __forceinline__ void add_row2(const char *__restrict__ tcb, const uint32_t (&hb)[2][9], const float (&S0)[8], float (&S)[8]) {
+    #pragma unroll
+    for (int dy = 0; dy < 2; dy++)
+        #pragma unroll
+        for (int e = 0; e < 8; e++)
+            #pragma unroll
+            for (int u = 0; u < 2; u++)
+                S[e] = __fadd_rn(dy == 0 && u == 0 ? S0[e] : S[e], *reinterpret_cast<const float *>(tcb + (u + 2 * dy + 4 * V) * 64 + hb[dy][e + u]));
+}
+__global__ void __launch_bounds__(64, 6) k_subgate(const Oct *__restrict__ oct, const uint64_t *__restrict__ seeds, const uint32_t *__restrict__ n_in,
+                                                   uint32_t cap_in, double thr, SubTaps tp, uint64_t *__restrict__ out_seed,
+                                                   uint32_t *__restrict__ n_out, uint32_t cap_out, float *__restrict__ side_amp) {
+    __shared__ __align__(16) float sTA[2][128];
+    __shared__ __align__(16) uint8_t sP2A[2][512];
+    __shared__ __align__(16) uint8_t sColA[2][2][256];
+    __shared__ __align__(16) uint32_t sWA[2][PG_SW];
+    __shared__ float sRed[2][2];                        // [iteration parity][side]
+    const int tid = threadIdx.x, lane = tid & 31, side = tid >> 5;
+    float *sT = sTA[side];
+    uint8_t *sP2 = sP2A[side];
+    uint8_t (*sCol)[256] = sColA[side];
+    uint32_t *sW = sWA[side];
+    const uint32_t n = min(*n_in, cap_in);
+    int it = 0;
+    for (uint32_t s = blockIdx.x; s < n; s += gridDim.x, it++) {
+        const Oct &p = oct[2 * size_t(s) + side];
+        if (lane < 16) {
+            const uint4 v = reinterpret_cast<const uint4 *>(p.perm)[lane];
+            reinterpret_cast<uint4 *>(sP2)[lane] = v; reinterpret_cast<uint4 *>(sP2)[lane + 16] = v;
+        }
+        const double ox = p.ox, oz = p.oz, fy = p.fy;
+        const int iy = p.iy;
+        __syncwarp();
+        for (int c = lane; c < 256; c += 32) {
+            const int pc = sP2[c];
+            sCol[0][c] = sP2[pc + (iy & 255)];
+            sCol[1][c] = sP2[pc + ((iy + 1) & 255)];
+        }
+        for (int i = lane; i < PG_SW; i += 32) {
+            uint32_t w = 0;
+            #pragma unroll
+            for (int b = 0; b < 4; b++) w |= uint32_t(sP2[(i + b) & 255] & 15) << (8 * b + 2);
+            sW[i] = w;
+        }
+        const int i0 = int(floor(ox)), k0 = int(floor(oz));
+        {   // corner tables T[c][h] (lowfield.hpp:65-73), c = dx + 2 dy + 4 dz
+            const double fx = ox - i0, fz = oz - k0, tx = fade_plain(fx), tz = fade_plain(fz), ty = fade_plain(fy);
+            for (int e = lane; e < 128; e += 32) {
+                const int c = e >> 4, h = e & 15, dx = c & 1, dy = (c >> 1) & 1, dz = c >> 2;
+                const double wc = (dx ? tx : 1 - tx) * (dy ? ty : 1 - ty) * (dz ? tz : 1 - tz);
+                sT[e] = float(tp.w * wc * grad_products(h, fx - dx, fy - dy, fz - dz));
+            }
+        }
+        __syncwarp();
+        uint32_t cv[2][2];                                // column hashes of the lane's lattice columns 8 lane + i0 + t
+        #pragma unroll
+        for (int dy = 0; dy < 2; dy++)
+            #pragma unroll
+            for (int k = 0; k < 2; k++) {
+                uint32_t w = 0;
+                #pragma unroll
+                for (int b = 0; b < 4; b++) w |= uint32_t(sCol[dy][(8 * lane + i0 + 4 * k + b) & 255]) << (8 * b);
+                cv[dy][k] = w;
+            }
+        // sample rows r = -4 .. 259 (output rows 0 .. 255 and the blur's halo); row r sums hash rows r + 4 (dz = 0)
+        // and r + 5 (dz = 1) of the lattice rows from m0 = k0 - 4 (mod 256)
+        const int m0 = (k0 - 4) & 255;
+        float best = -9.f;
+        uint32_t W[2][8], hb[2][9];
+        float pend[8][8];
+        #pragma unroll
+        for (int j = 0; j < 8; j++)
+            #pragma unroll
+            for (int e = 0; e < 8; e++) pend[j][e] = 0.f;
+        const char *tcb = reinterpret_cast<const char *>(sT);
+        float S1[8];
+        const float Z[8] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
+        load_group(sW, cv, m0, W);
+        unpack_row9(W, 0, lane, hb);
+        add_row2<0>(tcb, hb, Z, S1);
+        for (int k = 1; k < PG_BAND + 9; k++) {
+            const int r = k - 5;                              // the sample row this hash row completes
+            if ((k & 3) == 0) load_group(sW, cv, m0 + k, W);
+            unpack_row9(W, k & 3, lane, hb);
+            float S[8];
+            add_row2<1>(tcb, hb, S1, S);
+            float X[16];                                      // columns i-4 .. i+4 (periodic in 256)
+            #pragma unroll
+            for (int q = 0; q < 4; q++) {
+                X[q] = __shfl_sync(0xffffffffu, S[4 + q], (lane + 31) & 31);
+                X[12 + q] = __shfl_sync(0xffffffffu, S[q], (lane + 1) & 31);
+            }
+            #pragma unroll
+            for (int e = 0; e < 8; e++) X[4 + e] = S[e];
+            #pragma unroll
+            for (int e = 0; e < 8; e++) {
+                float hv = __fadd_rn(0.f, __fmul_rn(tp.k[0], X[e]));
+                #pragma unroll
+                for (int d = 1; d < 9; d++) hv = __fadd_rn(hv, __fmul_rn(tp.k[d], X[e + d]));
+                // along the column: this row is term 8-j of the pending output r-4+j
+                const float done = __fadd_rn(pend[0][e], __fmul_rn(tp.k[8], hv));
+                #pragma unroll
+                for (int j = 1; j < 8; j++) pend[j - 1][e] = __fadd_rn(pend[j][e], __fmul_rn(tp.k[8 - j], hv));
+                pend[7][e] = __fadd_rn(0.f, __fmul_rn(tp.k[0], hv));
+                if (r - 4 >= 0) best = fmaxf(best, done);
+            }
+            add_row2<0>(tcb, hb, Z, S1);
+        }
+        #pragma unroll
+        for (int o = 16; o > 0; o >>= 1) best = fmaxf(best, __shfl_xor_sync(0xffffffffu, best, o));
+        if (lane == 0) sRed[it & 1][side] = best;
+        __syncthreads();
+        if (tid == 0) {
+            const float ma = sRed[it & 1][0], mb = sRed[it & 1][1];
+            const float est = __fadd_rn(ma, mb);
+            if (side_amp) { side_amp[2 * size_t(s)] = ma; side_amp[2 * size_t(s) + 1] = mb; }
+            if (!(double(est) < thr)) {
+                const uint32_t i = atomicAdd(n_out, 1u);
+                if (i < cap_out) out_seed[i] = seeds[s];
             }
         }
     }
@@ -601,6 +756,92 @@ extern "C" int dsg_gate_run(uint64_t start, uint64_t count, const dsg_gate_cfg *
         *n_out = written;
         if (counts) std::memcpy(counts, tot, sizeof tot);
         return overflow ? DSG_OVERFLOW : DSG_OK;
+    });
+}
+
+// ---- the CPU search's gate: y-phase, then the sub-grid pre-gate estimate (dsearch_desert.cpp:201-223)
+namespace dsg { namespace gate {
+// taps exp(-d^2/2) rounded to float and normalised by their double sum, on the host as the CPU code computes
+// them (lowfield.hpp:86-89); w = factor x weight of the temperature octave -10 (1.25 x (32/63 x 1.5))
+SubTaps sub_taps() {
+    SubTaps t{};
+    double s = 0;
+    for (int d = -4; d <= 4; d++) s += t.k[d + 4] = float(std::exp(-0.5 * d * d));
+    for (float &v : t.k) v = float(v / s);
+    t.w = 1.25 * ((32.0 / 63.0) * 1.5);
+    return t;
+}
+int sub_blocks() { int occ = 0; cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_subgate, 64, 0); return std::max(1, occ) * device_info().sms; }
+}}  // namespace dsg::gate
+
+extern "C" int dsg_subgate_run(uint64_t start, uint64_t count, double maxph, double thr, uint64_t *out_seed, uint32_t cap, uint32_t *n_out,
+                               uint64_t counts[3]) {
+    return guarded([&] {
+        DSG_ARG(n_out && (cap == 0 || out_seed), "dsg_subgate_run: null pointer");
+        State &g = S(); std::lock_guard<std::mutex> l(g.mu); setup_locked(g);
+        const uint64_t B = 1ull << 26;
+        ensure_buffers(g, B);
+        const SubTaps tp = sub_taps();
+        const int blocks = sub_blocks();
+        uint64_t tot[3] = {0, 0, 0};
+        uint32_t written = 0;
+        bool overflow = false;
+        std::vector<uint64_t> found;
+        for (uint64_t base = 0; base < count; base += B) {
+            const uint64_t nb = std::min(B, count - base);
+            cudaStream_t st = g.st;
+            DSG_CU(cudaMemsetAsync(g.d_n, 0, 16, st));
+            const unsigned pb = unsigned(std::min<uint64_t>((nb + 255) / 256, uint64_t(device_info().sms) * 64));
+            k_phase<<<pb, 256, 0, st>>>(start + base, nb, maxph, g.d_s1, g.d_n, g.cap1);
+            k_octinit<<<unsigned(device_info().sms) * 16, 128, 0, st>>>(g.d_s1, g.d_n, g.cap1, g.d_oct);
+            k_subgate<<<blocks, 64, 0, st>>>(g.d_oct, g.d_s1, g.d_n, g.cap1, thr, tp, g.d_s2, g.d_n + 1, g.cap2, nullptr);
+            DSG_CU(cudaGetLastError());
+            DSG_CU(cudaMemcpyAsync(g.h_n, g.d_n, 16, cudaMemcpyDeviceToHost, st));
+            DSG_CU(cudaStreamSynchronize(st));
+            const uint32_t n1 = g.h_n[0], n2 = g.h_n[1];
+            overflow |= n1 > g.cap1 || n2 > g.cap2;
+            const uint32_t k2 = std::min(n2, g.cap2);
+            found.resize(k2);
+            if (k2) {
+                DSG_CU(cudaMemcpyAsync(found.data(), g.d_s2, size_t(k2) * 8, cudaMemcpyDeviceToHost, st));
+                DSG_CU(cudaStreamSynchronize(st));
+            }
+            std::sort(found.begin(), found.end());
+            for (uint64_t f : found) {
+                if (written < cap) out_seed[written++] = f;
+                else overflow = true;
+            }
+            tot[0] += nb; tot[1] += n1; tot[2] += n2;
+        }
+        *n_out = written;
+        if (counts) std::memcpy(counts, tot, sizeof tot);
+        return overflow ? DSG_OVERFLOW : DSG_OK;
+    });
+}
+
+extern "C" int dsg_subgate_amps(const uint64_t *seeds, uint32_t n, float *est) {
+    return guarded([&] {
+        DSG_ARG(n == 0 || (seeds && est), "dsg_subgate_amps: null pointer");
+        if (!n) return DSG_OK;
+        State &g = S(); std::lock_guard<std::mutex> l(g.mu); setup_locked(g);
+        uint64_t *d_s = nullptr; uint32_t *d_n = nullptr; Oct *d_oct = nullptr; float *d_e = nullptr; uint64_t *d_o = nullptr;
+        try {
+            DSG_CU(cudaMalloc(&d_s, size_t(n) * 8));
+            DSG_CU(cudaMalloc(&d_n, 16));
+            DSG_CU(cudaMalloc(&d_oct, size_t(n) * 2 * sizeof(Oct)));
+            DSG_CU(cudaMalloc(&d_e, size_t(n) * 8));
+            DSG_CU(cudaMalloc(&d_o, size_t(n) * 8));
+            DSG_CU(cudaMemcpyAsync(d_s, seeds, size_t(n) * 8, cudaMemcpyHostToDevice, g.st));
+            const uint32_t cnt[4] = {n, 0, 0, 0};
+            DSG_CU(cudaMemcpyAsync(d_n, cnt, 16, cudaMemcpyHostToDevice, g.st));
+            k_octinit<<<(2 * n + 127) / 128, 128, 0, g.st>>>(d_s, d_n, n, d_oct);
+            k_subgate<<<sub_blocks(), 64, 0, g.st>>>(d_oct, d_s, d_n, n, -1e30, sub_taps(), d_o, d_n + 1, n, d_e);
+            DSG_CU(cudaGetLastError());
+            DSG_CU(cudaMemcpyAsync(est, d_e, size_t(n) * 8, cudaMemcpyDeviceToHost, g.st));
+            DSG_CU(cudaStreamSynchronize(g.st));
+        } catch (...) { cudaFree(d_s); cudaFree(d_n); cudaFree(d_oct); cudaFree(d_e); cudaFree(d_o); throw; }
+        cudaFree(d_s); cudaFree(d_n); cudaFree(d_oct); cudaFree(d_e); cudaFree(d_o);
+        return DSG_OK;
     });
 }
 

@@ -60,6 +60,25 @@ def gate_taps():
     return t[:9].copy(), t[9:].copy()
 
 
+def subgate_amps(seeds):
+    """The CPU search's sub-grid pre-gate estimates of explicit seeds (dsg_subgate_amps), shape (n, 2)."""
+    s = np.ascontiguousarray(seeds, dtype=np.uint64)
+    est = np.empty(2 * len(s), dtype=np.float32)
+    _ck(lib.dsg_subgate_amps(ptr(s, u64p), C.c_uint32(len(s)), ptr(est, f32p)), "dsg_subgate_amps")
+    return est.reshape(-1, 2)
+
+
+def subgate_run(start, count, maxph=0.10, thr=0.69, cap=1 << 20):
+    """The CPU search's gate over seeds mix(start + k) (dsg_subgate_run): (survivors, counts)."""
+    out = np.empty(cap, dtype=np.uint64)
+    n = C.c_uint32()
+    cnt = np.zeros(3, dtype=np.uint64)
+    rc = _ck(lib.dsg_subgate_run(C.c_uint64(start), C.c_uint64(count), C.c_double(maxph), C.c_double(thr), ptr(out, u64p), C.c_uint32(cap),
+                                 C.byref(n), ptr(cnt, u64p)), "dsg_subgate_run")
+    assert rc == DSG_OK, "capacity exceeded"
+    return out[:n.value].copy(), [int(x) for x in cnt]
+
+
 def phase(seeds):
     s = np.ascontiguousarray(seeds, dtype=np.uint64)
     ph = np.empty(len(s)); fy = np.empty(2 * len(s))

@@ -50,6 +50,17 @@ typedef struct dsg_gate_cfg {
 int dsg_gate_run(uint64_t start, uint64_t count, const dsg_gate_cfg *cfg,
                  uint64_t *out_seed, float *out_amp, uint32_t cap, uint32_t *n_out, uint64_t counts[4]);
 
+/* The CPU search's own gate, for the enumerated seed ranges of dsearch_desert without gate=1
+ * (dsearch_desert.cpp:201-223): seeds mix(start + k), k < count, with y-phase <= maxph (phase_t, a double cut
+ * as Params.max_phase), then the sub-grid pre-gate estimate of lowfield.hpp:60-102 summed over the two sides
+ * (float) and kept when it is not below thr (the reference skips est < amp - amp_margin).  Survivors ascending
+ * per batch of 2^26 indices, at most cap; counts (may be NULL) = {seed indices, phase-passed, passed}.
+ * DSG_OVERFLOW if more than cap passed. */
+int dsg_subgate_run(uint64_t start, uint64_t count, double maxph, double thr, uint64_t *out_seed, uint32_t cap, uint32_t *n_out,
+                    uint64_t counts[3]);
+/* Sub-grid pre-gate estimates of explicit seeds: est[2i + side] = amplitude_sub of that side (lowfield.hpp:60-102). */
+int dsg_subgate_amps(const uint64_t *seeds, uint32_t n, float *est);
+
 /* Pre-gate and full-gate side amplitudes of explicit seeds (no thresholds): pre[2i+s], full[2i+s] for side
  * s of seed i.  The calibration view of the gate; replaces tgate's calib=N mode (src/gpu/tgate.cu:53-86). */
 int dsg_gate_amps(const uint64_t *seeds, uint32_t n, float *pre, float *full);

@@ -126,3 +126,28 @@ def test_process_exits_cleanly_right_after_init():
     r = subprocess.run([sys.executable, "-c", code], capture_output=True, text=True, timeout=300)
     assert r.returncode == 0, r.stderr[-2000:]
     assert r.stdout.strip() == "ok 3"
+
+
+def test_subgate_estimates_bit_exact(dsg):
+    """The CPU search's sub-grid pre-gate (amplitude_sub, lowfield.hpp:60-102) on the device equals the oracle's
+    (pinned to the reference's own function) bit for bit, both sides of every seed."""
+    seeds = np.array([libs.mix(5 * 10**11 + k) for k in range(600)], dtype=np.uint64)
+    got = dsg.subgate_amps(seeds)
+    want = libs.orc_subgate(seeds)
+    assert np.array_equal(got.view(np.uint32), want.view(np.uint32)), f"{np.sum(got != want)} differ"
+
+
+def test_subgate_run_equals_oracle_gate():
+    """dsg_subgate_run over an enumerated range: the phase count (phase_t <= 0.10, a double cut) and the
+    survivors (estimate summed over the sides, not below 0.69) equal the oracle's."""
+    import dsgpu
+    start, count = 3 * 10**12, 1 << 17
+    got, counts = dsgpu.subgate_run(start, count, 0.10, 0.69)
+    seeds = np.array([libs.mix(start + k) for k in range(count)], dtype=np.uint64)
+    ph, _ = libs.orc().phase(seeds)
+    passed = seeds[ph <= 0.10]
+    est = libs.orc_subgate(passed)
+    keep = ~((est[:, 0] + est[:, 1]).astype(np.float64) < 0.69)
+    assert counts == [count, len(passed), int(keep.sum())]
+    assert np.array_equal(np.sort(got), np.sort(passed[keep]))
+    assert 0 < keep.sum() < len(passed)
