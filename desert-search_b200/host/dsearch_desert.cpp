@@ -10,10 +10,11 @@
 // reference's per-seed loop is sequential (a site is skipped if an earlier site's hot zone covers it; a
 // later exact-flood start is tried only if the earlier ones fell short) the GPU evaluates every candidate
 // speculatively and the host replays the reference's sequential decisions over the results, so the output
-// is what the reference's loop computes.  hot_min <= 0 (proxy floods from per-site starts) and study=1 (the
-// per-component census in PREFIX.zones.csv) follow the reference's per-start loop the same way.  gpu=0 (the
-// reference's CPU-only search with its own CPU gate) is not part of this build; gscan=0 runs the tables and
-// scan on the GPU anyway (bit-identical to the CPU path).
+// is what the reference's loop computes.  hot_min <= 0 (proxy floods from per-site starts), gpu=0 (proxy floods
+// from the hot zones' lattice starts instead of zone bitmaps) and study=1 (the per-component census in
+// PREFIX.zones.csv) follow the reference's per-start loop the same way.  Enumerated ranges without gate=1 go
+// through the CPU search's own gate (y-phase, sub-grid estimate, period-table amplitude), on the device; gscan=0
+// runs the tables and scan on the GPU anyway (bit-identical to the CPU path).
 #include "dsgpu.h"
 #include "cpu_check.hpp"
 #include <algorithm>
@@ -74,6 +75,7 @@ struct TMap {
 struct Site { float s, t, c, e; int x, z; };
 struct Eval { size_t rank; int x, z; double proxy, s8 = -1, s4 = 0; bool edge = false; double hot = 0; std::vector<std::pair<int, int>> alt; bool nostart = false; };
 struct CensusReq { size_t s, rank; int bx, bz; double proxy; };   // study=1: a new proxy component and its start
+struct Start { size_t s, rank; int x, z; double hot; };            // a proxy-flood start of the per-start loop
 
 [[noreturn]] static void die(const char *what) { fprintf(stderr, "%s: %s\n", what, dsg_last_error()); fflush(nullptr); std::_Exit(3); }
 static void ck(int rc, const char *what) { if (rc < 0) die(what); }
@@ -103,7 +105,8 @@ struct Search {
 
     // ---- per-batch stages
     void process(const std::vector<uint64_t> &seeds);
-    void start_loop(const std::vector<uint64_t> &seeds, const std::vector<std::vector<Site>> &sites, std::vector<std::vector<Eval>> &ev,
+    std::vector<Start> site_starts(const std::vector<uint64_t> &seeds, const std::vector<std::vector<Site>> &sites);
+    void start_loop(const std::vector<uint64_t> &seeds, const std::vector<Start> &st, std::vector<std::vector<Eval>> &ev,
                     std::vector<CensusReq> &census);
     void study_census(const std::vector<uint64_t> &seeds, const std::vector<std::vector<Site>> &sites, const std::vector<std::array<double, 2>> &fy,
                       const std::vector<float> &maxt, const std::vector<CensusReq> &census, std::vector<std::vector<std::string>> &zrows);
@@ -179,9 +182,17 @@ void Search::process(const std::vector<uint64_t> &seeds) {
         cap *= 4;                                   // the reference falls back to the CPU here; the GPU simply retries larger
     }
     const auto t1 = Clock::now();
+    // enumerated seeds (no gate=1, no stdin) must also pass the period tables' amplitude; the others get a
+    // seeds.csv line with zero candidates and stop here (dsearch_desert.cpp:245-251)
+    std::vector<uint8_t> amp_fail(n, 0);
+    size_t nscan = n;
+    if (!P.from_stdin)
+        for (size_t s = 0; s < n; s++)
+            if (maxt[2 * s] + maxt[2 * s + 1] < P.amp) { amp_fail[s] = 1; nscan--; }
     std::vector<std::vector<Site>> sites(n);
     std::vector<size_t> ncand(n);
     for (size_t s = 0; s < n; s++) {
+        if (amp_fail[s]) continue;
         const uint64_t seed = seeds[s];
         std::vector<const dsg_cand *> rs(nraw[s]);
         for (uint32_t k = 0; k < nraw[s]; k++) rs[k] = &raw[size_t(s) * cap + k];
@@ -193,7 +204,7 @@ void Search::process(const std::vector<uint64_t> &seeds) {
             if (fresh) cand.push_back({r->s, r->t, r->c, r->e, r->x, r->z});
             else if (r->s > cand[it->second].s) cand[it->second] = {r->s, r->t, r->c, r->e, r->x, r->z};
         }
-        if (gscan_checks.fetch_sub(1) > 0) {                // gscancheck: the CPU path side by side (:292-296)
+        if (P.from_stdin && gscan_checks.fetch_sub(1) > 0) {   // gscancheck (stdin seeds): the CPU path side by side (:292-296)
             std::vector<float> tab[6];
             dsg_tabin tin[6];
             hostcheck::seed_tabins(seed, tin);
@@ -215,13 +226,14 @@ void Search::process(const std::vector<uint64_t> &seeds) {
             if ((int)sites[s].size() >= P.max_sites) break;
         }
     }
-    scanned += n;
+    scanned += nscan;
     const auto t2 = Clock::now();
     // ---------------- S3: hot zones (dsearch_desert.cpp:326-372)
     struct Zone { size_t seed, rank; double hot; int x0, z0, nx, nz; };
     std::vector<Zone> zones;
     std::vector<std::vector<Eval>> ev(n);
     std::vector<CensusReq> census;
+    std::vector<Start> hstarts;                         // proxy-flood starts of the per-start loop (gpu=0, hot_min <= 0)
     if (P.hot_min > 0) {
         // hottest of 7x7 points at 256-quart spacing around every site (first strict maximum in dz, dx order)
         const auto tq0 = Clock::now();
@@ -330,13 +342,27 @@ void Search::process(const std::vector<uint64_t> &seeds) {
                 const double hot_area = hz.cells * 128.0 * 128 * 16 / 1e6;
                 if (hot_area < P.hot_min) continue;
                 nbig++;
+                if (!P.gpu) {       // gpu=0: proxy floods from every fourth lattice cell of the zone, in row order (:355-362)
+                    const dsg_flood_req &fq = use2 ? q2[k2] : q1[k2];
+                    const std::vector<int32_t> &cc = use2 ? c2 : c1;
+                    const std::vector<uint64_t> &oo = use2 ? o2 : o1;
+                    std::vector<std::pair<int, int>> lat;
+                    for (uint64_t c = oo[k2]; c < oo[k2 + 1]; c++) {
+                        const int x = cc[2 * c], z = cc[2 * c + 1];
+                        if ((((x - fq.qx) / 128) & 3) == 0 && (((z - fq.qz) / 128) & 3) == 0) lat.push_back({z, x});
+                    }
+                    std::sort(lat.begin(), lat.end());
+                    for (const auto &[z, x] : lat) hstarts.push_back({s2, r, x, z, hot_area});
+                    continue;
+                }
                 const int x0 = int(std::floor((hz.minx - 128) / 32.0)) * 32, z0 = int(std::floor((hz.minz - 128) / 32.0)) * 32;
                 zones.push_back({s2, r, hot_area, x0, z0, (hz.maxx + 128 - x0) / 32 + 1, (hz.maxz + 128 - z0) / 32 + 1});
             }
         t_hot += std::chrono::duration<double>(Clock::now() - th0).count();
     } else {
-        start_loop(seeds, sites, ev, census);
+        hstarts = site_starts(seeds, sites);
     }
+    if (!hstarts.empty()) start_loop(seeds, hstarts, ev, census);
     // ---------------- S4: proxy bitmaps + components (dsearch_desert.cpp:425-492)
     const auto tp0 = Clock::now();
     if (!zones.empty()) {
@@ -457,6 +483,7 @@ void Search::process(const std::vector<uint64_t> &seeds) {
     std::lock_guard<std::mutex> g(mu);
     for (size_t s = 0; s < n; s++) {
         const long long seed = (long long)seeds[s];
+        if (amp_fail[s]) { fprintf(sout, "%lld,%.4f,%.4f,%.4f,%.4f,0,0,0\n", seed, fy[s][0], fy[s][1], maxt[2 * s], maxt[2 * s + 1]); continue; }
         double seed_best = 0;
         for (size_t k2 = 0; !P.study && k2 < ev[s].size() && int(k2) < P.exact_n && ev[s][k2].proxy >= P.exact_min; k2++) {
             const Eval &e = ev[s][k2];
@@ -510,11 +537,8 @@ void Search::process(const std::vector<uint64_t> &seeds) {
 // the components flooded so far for the seed (32-quart blocks) floods its proxy component at step 32,
 // 8-connected, window 500.  Components already met (same (min x, min z)) are dropped.  All starts are flooded
 // speculatively in one batch and each seed replays the reference's sequence over the results.
-void Search::start_loop(const std::vector<uint64_t> &seeds, const std::vector<std::vector<Site>> &sites, std::vector<std::vector<Eval>> &ev,
-                        std::vector<CensusReq> &census) {
+std::vector<Start> Search::site_starts(const std::vector<uint64_t> &seeds, const std::vector<std::vector<Site>> &sites) {
     const size_t n = seeds.size();
-    const auto ts0 = Clock::now();
-    struct Start { size_t s, rank; int x, z; };
     std::vector<Start> st;
     for (size_t s = 0; s < n; s++) nsites += sites[s].size();
     if (P.multi <= 1) {
@@ -530,14 +554,21 @@ void Search::start_loop(const std::vector<uint64_t> &seeds, const std::vector<st
                 const Site &t = sites[s][r];
                 int bx = t.x, bz = t.z; float bp = -1;
                 for (int q = 0; q < 81; q++, k++) if (float(pr[k]) > bp) { bp = float(pr[k]); bx = t.x + (q % 9 - 4) * 64; bz = t.z + (q / 9 - 4) * 64; }
-                if (bp >= P.pcut) st.push_back({s, r, bx, bz});
+                if (bp >= P.pcut) st.push_back({s, r, bx, bz, 0.});
             }
     } else {
         for (size_t s = 0; s < n; s++)
             for (size_t r = 0; r < sites[s].size(); r++)
                 for (int dz = -P.multi; dz <= P.multi; dz++) for (int dx = -P.multi; dx <= P.multi; dx++)
-                    st.push_back({s, r, sites[s][r].x + dx * 512, sites[s][r].z + dz * 512});
+                    st.push_back({s, r, sites[s][r].x + dx * 512, sites[s][r].z + dz * 512, 0.});
     }
+    return st;
+}
+
+void Search::start_loop(const std::vector<uint64_t> &seeds, const std::vector<Start> &st, std::vector<std::vector<Eval>> &ev,
+                        std::vector<CensusReq> &census) {
+    const size_t n = seeds.size();
+    const auto ts0 = Clock::now();
     // PX(bx, bz) == 2: probability >= the float cut (desert_proxy.hpp:32)
     std::vector<uint8_t> pass(st.size(), 0);
     if (!st.empty()) {
@@ -566,6 +597,7 @@ void Search::start_loop(const std::vector<uint64_t> &seeds, const std::vector<st
             seen.push_back(sig);
             const double proxy = a[f].cells * 32.0 * 32 * 16 / 1e6;
             ev[s].push_back({st[k].rank, st[k].x, st[k].z, proxy});
+            ev[s].back().hot = st[k].hot;
             if (P.study) census.push_back({s, st[k].rank, st[k].x, st[k].z, proxy});
         }
     }
@@ -684,7 +716,6 @@ int main(int argc, char **argv) {
         if (!P.gpu) { fprintf(stderr, "gate=1 needs gpu=1\n"); return 2; }
         P.from_stdin = 1;
     }
-    if (!P.gpu) { fprintf(stderr, "gpu=0 selects the CPU-only search, which this B200 build does not provide: run with gpu=1 (gate=1 gscan=1)\n"); return 2; }
     S.out = fopen((prefix + ".csv").c_str(), "wx");
     S.sout = fopen((prefix + ".seeds.csv").c_str(), "wx");
     if (!S.out || !S.sout) { fprintf(stderr, "cannot create %s outputs (exist?)\n", prefix.c_str()); return 2; }
@@ -735,11 +766,10 @@ int main(int argc, char **argv) {
             gate_end = std::chrono::duration<double>(Clock::now() - S.begin).count();
             std::lock_guard<std::mutex> l(qmu); qdone = true; qcv.notify_all();
         });
-    } else {
-        // gate=1: the production GPU gate; without gate/stdin the enumerated range goes through the same gate
-        // with the CPU mode's phase cut (its sub-grid pre-gate is replaced by the anti-aliased one)
-        dsg_gate_cfg g{float(P.gate ? P.gate_phase : P.max_phase), float(P.gate_pthr), float(P.gate ? P.gate_amp : P.amp), 0};
-        const uint64_t total = (P.gate && S.count == 0) ? 100000000000000ULL : S.count;
+    } else if (P.gate) {
+        // gate=1: the production GPU gate (gproxy::start_gate); its survivors are counted by the workers as taken
+        dsg_gate_cfg g{float(P.gate_phase), float(P.gate_pthr), float(P.gate_amp), 0};
+        const uint64_t total = S.count == 0 ? 100000000000000ULL : S.count;
         source = std::thread([&, g, total] {
             const uint64_t B = 1ull << 26;
             std::vector<uint64_t> sd(1u << 20); std::vector<float> am(1u << 20);
@@ -751,11 +781,26 @@ int main(int argc, char **argv) {
                 uint32_t nn = 0; uint64_t c[4];
                 ck(dsg_gate_run(S.start + base, nb, &gb, sd.data(), am.data(), uint32_t(sd.size()), &nn, c), "gate");
                 for (int k = 0; k < 4; k++) tot[k] += c[k];
-                S.done += P.gate ? 0 : nb;
                 const double sec = std::chrono::duration<double>(Clock::now() - tg).count();
                 fprintf(stderr, "gate: %llu seeds, %llu phase-passed, %llu pre-gate, %llu passed; %.0f seeds/s, %.1f passed/s\n",
                         (unsigned long long)(base + nb), (unsigned long long)tot[1], (unsigned long long)tot[2], (unsigned long long)tot[3],
                         (base + nb) / sec, tot[3] / sec);
+                for (uint32_t i = 0; i < nn && !interrupted; i++) push(sd[i]);
+            }
+            gate_end = std::chrono::duration<double>(Clock::now() - S.begin).count();
+            std::lock_guard<std::mutex> l(qmu); qdone = true; qcv.notify_all();
+        });
+    } else {
+        // the enumerated range through the CPU search's own gate (:201-223): y-phase <= max_phase, then the
+        // sub-grid estimate >= amp - amp_margin, on the device; done counts indices, passed the phase-passed
+        source = std::thread([&] {
+            const uint64_t B = 1ull << 26;
+            std::vector<uint64_t> sd(1u << 20);
+            for (uint64_t base = 0; base < S.count && !interrupted; base += B) {
+                const uint64_t nb = std::min(B, S.count - base);
+                uint32_t nn = 0; uint64_t c[3];
+                ck(dsg_subgate_run(S.start + base, nb, P.max_phase, P.amp - P.amp_margin, sd.data(), uint32_t(sd.size()), &nn, c), "gate");
+                S.done += nb; S.passed += c[1];
                 for (uint32_t i = 0; i < nn && !interrupted; i++) push(sd[i]);
             }
             gate_end = std::chrono::duration<double>(Clock::now() - S.begin).count();
@@ -778,8 +823,7 @@ int main(int argc, char **argv) {
                 if (batch.empty() && (qdone || interrupted)) return;
             }
             if (batch.empty()) continue;
-            S.passed += batch.size();
-            if (P.from_stdin) S.done += batch.size();
+            if (P.from_stdin) { S.passed += batch.size(); S.done += batch.size(); }
             S.process(batch);
             if (interrupted) return;
         }

@@ -134,6 +134,30 @@ def test_dsearch_per_start_and_study_match_reference_cpu_searcher(tmp_path, opts
     assert cand(a.stderr) == cand(b.stderr)
 
 
+@pytest.mark.parametrize("opts", [[], ["study=1"]], ids=["default", "study"])
+def test_dsearch_default_invocation_matches_reference_cpu_searcher(tmp_path, opts):
+    """The reference's default invocation, `dsearch_desert START COUNT PREFIX THREADS` (Params defaults: gpu=0,
+    gate=0): the enumerated range through the CPU search's gate (y-phase <= 0.10, sub-grid estimate >= 0.69,
+    period-table amplitude >= 0.70, with a zero-candidate seeds.csv line for seeds failing the last), then the
+    proxy floods from every fourth lattice cell of the hot zones.  Ours runs every stage on the device; the
+    files and the JSON counters equal the reference CPU searcher's."""
+    args = ["20000000000000", "262144"]
+    a = run([os.path.join(BIN, "dsearch_desert")] + args + [str(tmp_path / "ours"), "8"] + opts)
+    b = run([ref("dsearch_desert")] + args + [str(tmp_path / "ref"), "8"] + opts)
+    assert a.returncode == 0, a.stderr[-2000:]
+    assert b.returncode == 0, b.stderr[-2000:]
+    rd = lambda p: sorted(open(p).read().splitlines())
+    for ext in [".csv", ".seeds.csv"] + ([".zones.csv"] if opts else []):
+        la, lb = rd(str(tmp_path / "ours") + ext), rd(str(tmp_path / "ref") + ext)
+        assert la == lb, (ext, sorted(set(la) ^ set(lb))[:6])
+    ja, jb = json.load(open(str(tmp_path / "ours") + ".json")), json.load(open(str(tmp_path / "ref") + ".json"))
+    for k in ("done", "passed", "scanned", "sites"):
+        assert ja[k] == jb[k], (k, ja[k], jb[k])
+    assert jb["scanned"] > 10 and sum(l.endswith(",0,0,0") for l in rd(str(tmp_path / "ref") + ".seeds.csv")) > 100
+    cand = lambda s: sorted(re.findall(r"CANDIDATE step4=[\d.]+M seed=-?\d+ x=-?\d+ z=-?\d+", s))
+    assert cand(a.stderr) == cand(b.stderr)
+
+
 def test_searcher_verifies_candidates_in_process(tmp_path, dsg):
     """verified=1: each CANDIDATE's exact step-1 flood runs on the flood service during the search, and
     PREFIX.verified gets the line deploy/gpipe.sh would append after bin/mcmeasure, in the fields
