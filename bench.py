@@ -15,7 +15,8 @@ full tables) plus the tables+scan of every gated seed, with the hot-zone stage r
 
 Besides the gate line, the default run adds (single GPU): "pipeline", the whole per-seed search through the
 drop-in searcher (ours overlapped, ours plain, the reference's GPU searcher; wall clock; outputs compared),
-and "flood", exact step-1 floods of uneven size as one batch, through the flood service under Poisson
+"default_mode", the reference's default command line (gpu=0, gate=0) through ours and through the reference's
+own CPU searcher (wall clock; files compared), and "flood", exact step-1 floods of uneven size as one batch, through the flood service under Poisson
 arrivals, and as sequential per-request launches.
 """
 import argparse
@@ -320,6 +321,42 @@ def pipeline(count=1 << 26):
     return out, cands
 
 
+def default_mode(count=1 << 22):
+    """The reference's default command line, `dsearch_desert START COUNT PREFIX THREADS` (gpu=0, gate=0: its CPU
+    gate over the enumerated range, period tables and scan, hot zones, proxy floods from the zones' lattice
+    starts, exact floods), on seeds mix(2e13 + k), k < count: ours (every stage on the device) against the
+    reference's own CPU searcher on all host cores, wall clock around each process; the files are compared."""
+    import re
+    cores = os.cpu_count() or 1
+    ours = os.path.join(ROOT, "desert-search_b200", "bin", "dsearch_desert")
+    ref = os.path.join(ROOT, "oracle", "_ref", "dsearch_desert")
+    out = {"seeds": count, "args": "defaults (gpu=0 gate=0)", "host_cores": cores}
+    with tempfile.TemporaryDirectory() as td:
+        res = {}
+        for tag, exe in (("ours", ours), ("reference_cpu_searcher", ref)):
+            if not os.path.exists(exe):
+                out[tag] = {"unavailable": f"{os.path.relpath(exe, ROOT)} not built"}
+                continue
+            pre = os.path.join(td, tag)
+            t0 = time.perf_counter()
+            r = subprocess.run([exe, str(START), str(count), pre, str(cores)], capture_output=True, text=True)
+            wall = time.perf_counter() - t0
+            if r.returncode != 0:
+                out[tag] = {"error": r.stderr[-300:]}
+                continue
+            j = json.load(open(pre + ".json"))
+            out[tag] = {"threads": cores, "wall_s": wall, "passed": j["passed"], "scanned": j["scanned"], "seeds_per_s": count / wall}
+            st = re.search(r"startup ([\d.]+) s", r.stderr)
+            if st:
+                out[tag]["startup_s"] = float(st.group(1))
+            res[tag] = [sorted(open(pre + ext).read().splitlines()) for ext in (".csv", ".seeds.csv")]
+        if len(res) == 2:
+            out["files_identical"] = res["ours"] == res["reference_cpu_searcher"]
+            out["csv_rows"] = len(res["ours"][0]) - 1
+            out["seeds_csv_rows"] = len(res["ours"][1]) - 1
+    return out
+
+
 def run_ours(args):
     rank, world, local = dist()
     import dsgpu
@@ -392,6 +429,7 @@ def run_ours(args):
         out["cpu_baseline"] = cpu_baseline()
         if not args.no_extras:
             out["pipeline"], cands = pipeline()
+            out["default_mode"] = default_mode()
             out["flood"] = bench_floods(dsgpu, n_small=4096, rates=args.flood_rates, n_service=args.flood_requests, candidates=cands)
     print(json.dumps(out), flush=True)
     if pg:
