@@ -301,7 +301,9 @@ k_pregate(const Oct *__restrict__ oct, const uint64_t *__restrict__ seeds, const
 // products and sums (the CPU code is built without contraction), and the maximum.  Same schedule as k_pregate:
 // one 64-thread CTA per seed, a warp per side streaming all 256 rows, hash-row words unpacked once and added
 // to the two sample rows that use them.
-struct SubTaps { float k[9]; double w; };
+// CPU search: k = normalised host taps, w = the double weight.  Reference GPU one-parity pre-gate (tgate box=0,
+// gate.cuh k_amp2<256,4,16,false>): k = the device taps, wf = the float weight, norm = 1 / (sum k)^2.
+struct SubTaps { float k[9]; double w; float wf, norm; };
 __device__ __forceinline__ double fade_plain(double t) { return t * t * t * (t * (t * 6. - 15.) + 10.); }
 // Minecraft's 16 gradients, as gx*x + gy*y + gz*z with their 0/+-1 components (the CPU code's gradient)
 __constant__ signed char kGrad[16][3] = {{1, 1, 0}, {-1, 1, 0}, {1, -1, 0}, {-1, -1, 0}, {1, 0, 1}, {-1, 0, 1}, {1, 0, -1}, {-1, 0, -1},
@@ -333,9 +335,14 @@ __device__ __forceinline__ void add_row2(const char *__restrict__ tcb, const uin
             for (int u = 0; u < 2; u++)
                 S[e] = __fadd_rn(dy == 0 && u == 0 ? S0[e] : S[e], *reinterpret_cast<const float *>(tcb + (u + 2 * dy + 4 * V) * 64 + hb[dy][e + u]));
 }
+// CPU = false: the same grid with the reference GPU kernel's arithmetic instead (its one-parity pre-gate, tgate
+// box=0): fused fade, the corner tables as 1.0 x w x wc x gradient, fused multiply-add blur chains with the
+// device taps, the maximum of (sum x norm), sides summed from 0 (gate.cuh:236-244,256-313,340).
+template <bool CPU>
 __global__ void __launch_bounds__(64, 6) k_subgate(const Oct *__restrict__ oct, const uint64_t *__restrict__ seeds, const uint32_t *__restrict__ n_in,
                                                    uint32_t cap_in, double thr, SubTaps tp, uint64_t *__restrict__ out_seed,
-                                                   uint32_t *__restrict__ n_out, uint32_t cap_out, float *__restrict__ side_amp) {
+                                                   uint32_t *__restrict__ out_idx, uint32_t *__restrict__ n_out, uint32_t cap_out,
+                                                   float *__restrict__ side_amp) {
     __shared__ __align__(16) float sTA[2][128];
     __shared__ __align__(16) uint8_t sP2A[2][512];
     __shared__ __align__(16) uint8_t sColA[2][2][256];
@@ -369,12 +376,14 @@ __global__ void __launch_bounds__(64, 6) k_subgate(const Oct *__restrict__ oct, 
             sW[i] = w;
         }
         const int i0 = int(floor(ox)), k0 = int(floor(oz));
-        {   // corner tables T[c][h] (lowfield.hpp:65-73), c = dx + 2 dy + 4 dz
-            const double fx = ox - i0, fz = oz - k0, tx = fade_plain(fx), tz = fade_plain(fz), ty = fade_plain(fy);
+        {   // corner tables T[c][h] (lowfield.hpp:65-73; gate.cuh:238-244), c = dx + 2 dy + 4 dz
+            const double fx = ox - i0, fz = oz - k0;
+            const double tx = CPU ? fade_plain(fx) : fade_fused(fx), tz = CPU ? fade_plain(fz) : fade_fused(fz), ty = CPU ? fade_plain(fy) : p.vy;
             for (int e = lane; e < 128; e += 32) {
                 const int c = e >> 4, h = e & 15, dx = c & 1, dy = (c >> 1) & 1, dz = c >> 2;
                 const double wc = (dx ? tx : 1 - tx) * (dy ? ty : 1 - ty) * (dz ? tz : 1 - tz);
-                sT[e] = float(tp.w * wc * grad_products(h, fx - dx, fy - dy, fz - dz));
+                sT[e] = CPU ? float(tp.w * wc * grad_products(h, fx - dx, fy - dy, fz - dz))
+                            : float(1.0 * double(tp.wf) * wc * gradd(h, fx - dx, fy - dy, fz - dz));
             }
         }
         __syncwarp();
@@ -391,7 +400,7 @@ __global__ void __launch_bounds__(64, 6) k_subgate(const Oct *__restrict__ oct, 
         // sample rows r = -4 .. 259 (output rows 0 .. 255 and the blur's halo); row r sums hash rows r + 4 (dz = 0)
         // and r + 5 (dz = 1) of the lattice rows from m0 = k0 - 4 (mod 256)
         const int m0 = (k0 - 4) & 255;
-        float best = -9.f;
+        float best = CPU ? -9.f : -1e9f;
         uint32_t W[2][8], hb[2][9];
         float pend[8][8];
         #pragma unroll
@@ -420,15 +429,17 @@ __global__ void __launch_bounds__(64, 6) k_subgate(const Oct *__restrict__ oct, 
             for (int e = 0; e < 8; e++) X[4 + e] = S[e];
             #pragma unroll
             for (int e = 0; e < 8; e++) {
-                float hv = __fadd_rn(0.f, __fmul_rn(tp.k[0], X[e]));
+                // a += k x v: separate product and sum (CPU) or one fused multiply-add (reference GPU kernel)
+                auto acc = [](float a, float k, float v) { return CPU ? __fadd_rn(a, __fmul_rn(k, v)) : __fmaf_rn(k, v, a); };
+                float hv = acc(0.f, tp.k[0], X[e]);
                 #pragma unroll
-                for (int d = 1; d < 9; d++) hv = __fadd_rn(hv, __fmul_rn(tp.k[d], X[e + d]));
+                for (int d = 1; d < 9; d++) hv = acc(hv, tp.k[d], X[e + d]);
                 // along the column: this row is term 8-j of the pending output r-4+j
-                const float done = __fadd_rn(pend[0][e], __fmul_rn(tp.k[8], hv));
+                const float done = acc(pend[0][e], tp.k[8], hv);
                 #pragma unroll
-                for (int j = 1; j < 8; j++) pend[j - 1][e] = __fadd_rn(pend[j][e], __fmul_rn(tp.k[8 - j], hv));
-                pend[7][e] = __fadd_rn(0.f, __fmul_rn(tp.k[0], hv));
-                if (r - 4 >= 0) best = fmaxf(best, done);
+                for (int j = 1; j < 8; j++) pend[j - 1][e] = acc(pend[j][e], tp.k[8 - j], hv);
+                pend[7][e] = acc(0.f, tp.k[0], hv);
+                if (r - 4 >= 0) best = fmaxf(best, CPU ? done : __fmul_rn(done, tp.norm));
             }
             add_row2<0>(tcb, hb, Z, S1);
         }
@@ -438,11 +449,11 @@ __global__ void __launch_bounds__(64, 6) k_subgate(const Oct *__restrict__ oct, 
         __syncthreads();
         if (tid == 0) {
             const float ma = sRed[it & 1][0], mb = sRed[it & 1][1];
-            const float est = __fadd_rn(ma, mb);
+            const float est = CPU ? __fadd_rn(ma, mb) : __fadd_rn(__fadd_rn(0.f, ma), mb);
             if (side_amp) { side_amp[2 * size_t(s)] = ma; side_amp[2 * size_t(s) + 1] = mb; }
             if (!(double(est) < thr)) {
                 const uint32_t i = atomicAdd(n_out, 1u);
-                if (i < cap_out) out_seed[i] = seeds[s];
+                if (i < cap_out) { out_seed[i] = seeds[s]; if (out_idx) out_idx[i] = s; }
             }
         }
     }
@@ -771,7 +782,14 @@ SubTaps sub_taps() {
     t.w = 1.25 * ((32.0 / 63.0) * 1.5);
     return t;
 }
-int sub_blocks() { int occ = 0; cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_subgate, 64, 0); return std::max(1, occ) * device_info().sms; }
+int sub_blocks() { int occ = 0; cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_subgate<true>, 64, 0); return std::max(1, occ) * device_info().sms; }
+// the reference GPU one-parity pre-gate's constants: device taps (sigma 1), their norm, the float weight
+SubTaps onepar_taps(const Taps &t) {
+    SubTaps o{};
+    for (int i = 0; i < 9; i++) o.k[i] = t.k9[i];
+    o.wf = t.w; o.norm = t.norm9;
+    return o;
+}
 }}  // namespace dsg::gate
 
 extern "C" int dsg_subgate_run(uint64_t start, uint64_t count, double maxph, double thr, uint64_t *out_seed, uint32_t cap, uint32_t *n_out,
@@ -794,7 +812,7 @@ extern "C" int dsg_subgate_run(uint64_t start, uint64_t count, double maxph, dou
             const unsigned pb = unsigned(std::min<uint64_t>((nb + 255) / 256, uint64_t(device_info().sms) * 64));
             k_phase<<<pb, 256, 0, st>>>(start + base, nb, maxph, g.d_s1, g.d_n, g.cap1);
             k_octinit<<<unsigned(device_info().sms) * 16, 128, 0, st>>>(g.d_s1, g.d_n, g.cap1, g.d_oct);
-            k_subgate<<<blocks, 64, 0, st>>>(g.d_oct, g.d_s1, g.d_n, g.cap1, thr, tp, g.d_s2, g.d_n + 1, g.cap2, nullptr);
+            k_subgate<true><<<blocks, 64, 0, st>>>(g.d_oct, g.d_s1, g.d_n, g.cap1, thr, tp, g.d_s2, nullptr, g.d_n + 1, g.cap2, nullptr);
             DSG_CU(cudaGetLastError());
             DSG_CU(cudaMemcpyAsync(g.h_n, g.d_n, 16, cudaMemcpyDeviceToHost, st));
             DSG_CU(cudaStreamSynchronize(st));
@@ -819,6 +837,83 @@ extern "C" int dsg_subgate_run(uint64_t start, uint64_t count, double maxph, dou
     });
 }
 
+extern "C" int dsg_gate_onepar_run(uint64_t start, uint64_t count, const dsg_gate_cfg *cfg, float margin, uint64_t *out_seed, float *out_amp,
+                                   uint32_t cap, uint32_t *n_out, uint64_t counts[4]) {
+    return guarded([&] {
+        DSG_ARG(cfg && n_out, "dsg_gate_onepar_run: null pointer");
+        DSG_ARG(cap == 0 || (out_seed && out_amp), "dsg_gate_onepar_run: null output");
+        State &g = S(); std::lock_guard<std::mutex> l(g.mu); setup_locked(g);
+        const uint64_t B = cfg->batch ? cfg->batch : (1ull << 26);
+        ensure_buffers(g, B);
+        const SubTaps tp = onepar_taps(g.taps);
+        const double thr = double(cfg->amp - margin);         // float difference, as GateCfg.amp - GateCfg.margin
+        const int blocks = sub_blocks();
+        uint64_t tot[4] = {0, 0, 0, 0};
+        uint32_t written = 0;
+        bool overflow = false;
+        std::vector<std::pair<uint64_t, float>> found;
+        for (uint64_t base = 0; base < count; base += B) {
+            const uint64_t nb = std::min(B, count - base);
+            cudaStream_t st = g.st;
+            DSG_CU(cudaMemsetAsync(g.d_n, 0, 16, st));
+            const unsigned pb = unsigned(std::min<uint64_t>((nb + 255) / 256, uint64_t(device_info().sms) * 64));
+            k_phase<<<pb, 256, 0, st>>>(start + base, nb, double(cfg->maxph), g.d_s1, g.d_n, g.cap1);
+            k_octinit<<<unsigned(device_info().sms) * 16, 128, 0, st>>>(g.d_s1, g.d_n, g.cap1, g.d_oct);
+            k_subgate<false><<<blocks, 64, 0, st>>>(g.d_oct, g.d_s1, g.d_n, g.cap1, thr, tp, g.d_s2, g.d_idx2, g.d_n + 1, g.cap2, nullptr);
+            k_fullgate<<<g.fg_blocks, FG_THREADS, 0, st>>>(g.d_oct, g.d_s2, g.d_idx2, g.d_n + 1, g.cap2, cfg->amp, g.taps, g.d_s3, g.d_a3, g.d_n + 2,
+                                                          g.cap3, nullptr);
+            DSG_CU(cudaGetLastError());
+            DSG_CU(cudaMemcpyAsync(g.h_n, g.d_n, 16, cudaMemcpyDeviceToHost, st));
+            DSG_CU(cudaStreamSynchronize(st));
+            const uint32_t n1 = g.h_n[0], n2 = g.h_n[1], n3 = g.h_n[2];
+            overflow |= n1 > g.cap1 || n2 > g.cap2 || n3 > g.cap3;
+            const uint32_t k3 = std::min(n3, g.cap3);
+            if (k3) {
+                DSG_CU(cudaMemcpyAsync(g.h_s3, g.d_s3, size_t(k3) * 8, cudaMemcpyDeviceToHost, st));
+                DSG_CU(cudaMemcpyAsync(g.h_a3, g.d_a3, size_t(k3) * 4, cudaMemcpyDeviceToHost, st));
+                DSG_CU(cudaStreamSynchronize(st));
+            }
+            found.clear();
+            for (uint32_t i = 0; i < k3; i++) found.push_back({g.h_s3[i], g.h_a3[i]});
+            std::sort(found.begin(), found.end());
+            for (auto &f : found) {
+                if (written < cap) { out_seed[written] = f.first; out_amp[written] = f.second; written++; }
+                else overflow = true;
+            }
+            tot[0] += nb; tot[1] += n1; tot[2] += n2; tot[3] += n3;
+        }
+        *n_out = written;
+        if (counts) std::memcpy(counts, tot, sizeof tot);
+        return overflow ? DSG_OVERFLOW : DSG_OK;
+    });
+}
+
+extern "C" int dsg_gate_onepar_amps(const uint64_t *seeds, uint32_t n, float *pre) {
+    return guarded([&] {
+        DSG_ARG(n == 0 || (seeds && pre), "dsg_gate_onepar_amps: null pointer");
+        if (!n) return DSG_OK;
+        State &g = S(); std::lock_guard<std::mutex> l(g.mu); setup_locked(g);
+        uint64_t *d_s = nullptr; uint32_t *d_n = nullptr; Oct *d_oct = nullptr; float *d_e = nullptr; uint64_t *d_o = nullptr;
+        try {
+            DSG_CU(cudaMalloc(&d_s, size_t(n) * 8));
+            DSG_CU(cudaMalloc(&d_n, 16));
+            DSG_CU(cudaMalloc(&d_oct, size_t(n) * 2 * sizeof(Oct)));
+            DSG_CU(cudaMalloc(&d_e, size_t(n) * 8));
+            DSG_CU(cudaMalloc(&d_o, size_t(n) * 8));
+            DSG_CU(cudaMemcpyAsync(d_s, seeds, size_t(n) * 8, cudaMemcpyHostToDevice, g.st));
+            const uint32_t cnt[4] = {n, 0, 0, 0};
+            DSG_CU(cudaMemcpyAsync(d_n, cnt, 16, cudaMemcpyHostToDevice, g.st));
+            k_octinit<<<(2 * n + 127) / 128, 128, 0, g.st>>>(d_s, d_n, n, d_oct);
+            k_subgate<false><<<sub_blocks(), 64, 0, g.st>>>(d_oct, d_s, d_n, n, -1e30, onepar_taps(g.taps), d_o, nullptr, d_n + 1, n, d_e);
+            DSG_CU(cudaGetLastError());
+            DSG_CU(cudaMemcpyAsync(pre, d_e, size_t(n) * 8, cudaMemcpyDeviceToHost, g.st));
+            DSG_CU(cudaStreamSynchronize(g.st));
+        } catch (...) { cudaFree(d_s); cudaFree(d_n); cudaFree(d_oct); cudaFree(d_e); cudaFree(d_o); throw; }
+        cudaFree(d_s); cudaFree(d_n); cudaFree(d_oct); cudaFree(d_e); cudaFree(d_o);
+        return DSG_OK;
+    });
+}
+
 extern "C" int dsg_subgate_amps(const uint64_t *seeds, uint32_t n, float *est) {
     return guarded([&] {
         DSG_ARG(n == 0 || (seeds && est), "dsg_subgate_amps: null pointer");
@@ -835,7 +930,7 @@ extern "C" int dsg_subgate_amps(const uint64_t *seeds, uint32_t n, float *est) {
             const uint32_t cnt[4] = {n, 0, 0, 0};
             DSG_CU(cudaMemcpyAsync(d_n, cnt, 16, cudaMemcpyHostToDevice, g.st));
             k_octinit<<<(2 * n + 127) / 128, 128, 0, g.st>>>(d_s, d_n, n, d_oct);
-            k_subgate<<<sub_blocks(), 64, 0, g.st>>>(d_oct, d_s, d_n, n, -1e30, sub_taps(), d_o, d_n + 1, n, d_e);
+            k_subgate<true><<<sub_blocks(), 64, 0, g.st>>>(d_oct, d_s, d_n, n, -1e30, sub_taps(), d_o, nullptr, d_n + 1, n, d_e);
             DSG_CU(cudaGetLastError());
             DSG_CU(cudaMemcpyAsync(est, d_e, size_t(n) * 8, cudaMemcpyDeviceToHost, g.st));
             DSG_CU(cudaStreamSynchronize(g.st));

@@ -60,6 +60,14 @@ def gate_taps():
     return t[:9].copy(), t[9:].copy()
 
 
+def gate_onepar_amps(seeds):
+    """One-parity pre-gate side amplitudes of the reference's tgate box=0 (dsg_gate_onepar_amps), shape (n, 2)."""
+    s = np.ascontiguousarray(seeds, dtype=np.uint64)
+    pre = np.empty(2 * len(s), dtype=np.float32)
+    _ck(lib.dsg_gate_onepar_amps(ptr(s, u64p), C.c_uint32(len(s)), ptr(pre, f32p)), "dsg_gate_onepar_amps")
+    return pre.reshape(-1, 2)
+
+
 def subgate_amps(seeds):
     """The CPU search's sub-grid pre-gate estimates of explicit seeds (dsg_subgate_amps), shape (n, 2)."""
     s = np.ascontiguousarray(seeds, dtype=np.uint64)

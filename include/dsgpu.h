@@ -58,6 +58,13 @@ int dsg_gate_run(uint64_t start, uint64_t count, const dsg_gate_cfg *cfg,
  * DSG_OVERFLOW if more than cap passed. */
 int dsg_subgate_run(uint64_t start, uint64_t count, double maxph, double thr, uint64_t *out_seed, uint32_t cap, uint32_t *n_out,
                     uint64_t counts[3]);
+/* The gate with the reference's legacy one-parity pre-gate (tgate box=0, gate.cuh k_amp2<256,4,16,false> at
+ * amp - margin, then the full gate at amp; src/gpu/gate.cuh:393-394): arguments and outputs as dsg_gate_run
+ * (cfg->pthr unused), counts = {seed indices, phase-passed, pre-gate passed, full-gate passed}. */
+int dsg_gate_onepar_run(uint64_t start, uint64_t count, const dsg_gate_cfg *cfg, float margin, uint64_t *out_seed, float *out_amp,
+                        uint32_t cap, uint32_t *n_out, uint64_t counts[4]);
+/* One-parity pre-gate side amplitudes of explicit seeds, pre[2i + side] (tgate calib=N box=0). */
+int dsg_gate_onepar_amps(const uint64_t *seeds, uint32_t n, float *pre);
 /* Sub-grid pre-gate estimates of explicit seeds: est[2i + side] = amplitude_sub of that side (lowfield.hpp:60-102). */
 int dsg_subgate_amps(const uint64_t *seeds, uint32_t n, float *est);
 

@@ -49,6 +49,38 @@ done:
 #undef TRY
 }
 
+// Reference one-parity pre-gate amplitudes (tgate box=0: k_amp2<256,4,16,false>, sig 1) of n seeds, input order.
+int ref_gate_onepar_gpu(const uint64_t *seeds, int n, float *pre) {
+    uint64_t *d_s, *d_o; float *d_a; PerlinParams *d_p; unsigned *d_n;
+    cudaError_t e = cudaSuccess;
+#define TRY(x) do { e = (x); if (e != cudaSuccess) goto done; } while (0)
+    d_s = d_o = nullptr; d_a = nullptr; d_p = nullptr; d_n = nullptr;
+    TRY(cudaMalloc(&d_s, size_t(n) * 8)); TRY(cudaMalloc(&d_o, size_t(n) * 8)); TRY(cudaMalloc(&d_a, size_t(n) * 4));
+    TRY(cudaMalloc(&d_p, size_t(n) * 2 * sizeof(PerlinParams))); TRY(cudaMalloc(&d_n, 3 * 4));
+    TRY(cudaMemcpy(d_s, seeds, size_t(n) * 8, cudaMemcpyHostToDevice));
+    TRY(cudaMemset(d_n, 0, 12));
+    TRY(cudaFuncSetAttribute(k_amp2<256, 4, 16, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(dyn_bytes<256, 4, 16, false>())));
+    k_init<<<(2 * n + 255) / 256, 256>>>(d_s, unsigned(n), d_p);
+    k_amp2<256, 4, 16, false><<<n, 256, dyn_bytes<256, 4, 16, false>()>>>(d_s, d_p, unsigned(n), 1.0f, -1e9f, d_o, d_a, d_n + 1, unsigned(n));
+    TRY(cudaGetLastError());
+    TRY(cudaDeviceSynchronize());
+    {
+        std::vector<uint64_t> o(n); std::vector<float> a(n);
+        TRY(cudaMemcpy(o.data(), d_o, size_t(n) * 8, cudaMemcpyDeviceToHost)); TRY(cudaMemcpy(a.data(), d_a, size_t(n) * 4, cudaMemcpyDeviceToHost));
+        std::vector<std::pair<uint64_t, float>> m(n);
+        for (int i = 0; i < n; i++) m[i] = {o[i], a[i]};
+        std::sort(m.begin(), m.end());
+        for (int i = 0; i < n; i++) {
+            auto f = std::lower_bound(m.begin(), m.end(), std::make_pair(seeds[i], -1e30f));
+            pre[i] = f != m.end() && f->first == seeds[i] ? f->second : NAN;
+        }
+    }
+done:
+    cudaFree(d_s); cudaFree(d_o); cudaFree(d_a); cudaFree(d_p); cudaFree(d_n);
+    return int(e);
+#undef TRY
+}
+
 // Gate taps exactly as the reference kernels compute them (device expf), for the tap-equality check.
 __global__ void ref_k_taps(float *k, float sig1, float sig2) {
     const int t = threadIdx.x;

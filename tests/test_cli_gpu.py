@@ -75,6 +75,27 @@ def test_tgate_matches_reference_tool(dsg):
     assert re.search(r"gate: \d+ seeds, \d+ phase-passed, \d+ pre-gate, \d+ passed", a.stderr)
 
 
+def test_tgate_box0_matches_reference_tool(dsg):
+    """tgate box=0 (the legacy one-parity pre-gate at amp - margin, then the full gate): the same survivor lines
+    as the reference's tgate, up to seeds whose pre-gate sum lies within the reference kernel's run-to-run spread
+    of the threshold."""
+    import numpy as np
+    args = [str(10**12), str(1 << 22), "phase=0.06", "amp=0.70", "box=0", "margin=0.01"]
+    a = run([os.path.join(BIN, "tgate")] + args)
+    b = run([ref("tgate")] + args)
+    assert a.returncode == b.returncode == 0, (a.stderr[-500:], b.stderr[-500:])
+    la, lb = sorted(a.stdout.split("\n")), sorted(b.stdout.split("\n"))
+    assert len(la) > 10
+    diff = (set(la) ^ set(lb)) - {""}
+    assert len(diff) <= 4, diff
+    if diff:
+        seeds = np.array([int(l.split()[0]) for l in diff], dtype=np.uint64)
+        pre = dsg.gate_onepar_amps(seeds).sum(1)
+        _, full = dsg.gate_amps(seeds)
+        near = (np.abs(pre - 0.69) < 4e-3) | (np.abs(full.sum(1) - 0.70) < 4e-3)
+        assert near.all(), (diff, pre, full.sum(1))
+
+
 def test_dsearch_matches_reference_gpu_searcher(tmp_path):
     seeds = "".join(f"{f['seed']}\n" for f in finds()[:8])
     opts = ["stdin=1", "gpu=1", "gscan=1"]

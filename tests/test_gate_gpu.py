@@ -151,3 +151,24 @@ def test_subgate_run_equals_oracle_gate():
     assert counts == [count, len(passed), int(keep.sum())]
     assert np.array_equal(np.sort(got), np.sort(passed[keep]))
     assert 0 < keep.sum() < len(passed)
+
+
+def test_onepar_pregate_matches_reference_kernel(dsg):
+    """The legacy one-parity pre-gate (tgate box=0) against the reference's own kernel (gate.cuh
+    k_amp2<256,4,16,false>) run live on this GPU, on the gate microbench's phase-passed seeds: equal bit for bit,
+    except on seeds where repeated reference runs disagree with each other."""
+    p = os.path.join(libs.REF_DIR, "libref_gate.so")
+    if not os.path.exists(p):
+        pytest.skip("oracle/_ref/libref_gate.so not built")
+    g = C.CDLL(p)
+    seeds = phase_passed(10**12, 65536)
+    runs = []
+    for _ in range(3):
+        pre = np.empty(len(seeds), dtype=np.float32)
+        assert g.ref_gate_onepar_gpu(seeds.ctypes.data_as(C.POINTER(C.c_uint64)), C.c_int(len(seeds)), pre.ctypes.data_as(C.POINTER(C.c_float))) == 0
+        runs.append(pre)
+    m = dsg.gate_onepar_amps(seeds)
+    ours = libs.side_sum(m)
+    stable = np.all(np.stack([r.view(np.uint32) for r in runs]) == runs[0].view(np.uint32), axis=0)
+    assert stable.mean() > 0.95
+    assert np.array_equal(ours.view(np.uint32)[stable], runs[0].view(np.uint32)[stable]), np.abs(ours - runs[0])[stable].max()
