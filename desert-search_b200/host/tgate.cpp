@@ -27,7 +27,8 @@ int main(int argc, char **argv) {
         if (k == "phase") g.maxph = float(v); else if (k == "amp") g.amp = float(v); else if (k == "pthr") g.pthr = float(v);
         else if (k == "check") check = int(v); else if (k == "calib") calib = int(v); else if (k == "box") box = int(v);
         else if (k == "margin") margin = float(v);
-        // tpb_pre, tpb_full, perseed, sig: launch-shape knobs of the reference kernels; ignored here
+        // tpb_pre, tpb_full, perseed: launch-shape knobs of the reference kernels, ignored here; sig: the reference's
+        // calibration blur width for the anti-aliased pre-gate, which this build keeps at the gate's 1.0
     }
     if (dsg_init(0, 0.35f) != DSG_OK) { fprintf(stderr, "tgate: %s\n", dsg_last_error()); return 3; }
     const uint64_t B = 1ull << 26;
