@@ -5,16 +5,18 @@
 // Every value is bit-identical to the CPU path: the corner sums, the blur (multiply and add rounded
 // separately, taps in order) and the scan's score arithmetic follow the CPU expressions exactly.
 // Kernels:
-//  * k_tab_h: one CTA per 8-row block of one table; thread = column.  Tabulates the rows into shared memory
-//    and writes them horizontally blurred (the row never round-trips through HBM unblurred).
-//  * k_blur_v: one CTA per 32-row block; thread = column; a register ring holds the 15 rows the vertical
-//    blur needs, so each blurred row is read once per block.  T tables also reduce their maximum.
+//  * k_tables<R>: the period tables and their blur (radius R taps each way) in one pass; one 512-thread CTA
+//    per band of rows of one table.  Rows are produced FCH at a time: corner sums (thread = column) into
+//    shared memory, the horizontal blur of those rows (thread = 4 columns of a row) into a ring of blurred
+//    rows, and the vertical blur of FCH output rows (thread = column) from the ring.  Only the finished
+//    table reaches HBM; the T tables also reduce their maximum.
 //  * k_scan: CTAs loop over the active side-A cells (TA >= ta), threads over the (tz, tx) translation pairs.
 //  * k_tabins: the table inputs of a seed (tab_setup, lowfield.hpp:14-33) from its device noise tables, for
 //    dsg_scan_seeds.
 #include "noise.cuh"
 #include <algorithm>
 #include <mutex>
+#include <utility>
 #include <vector>
 
 namespace dsg {
@@ -30,68 +32,159 @@ struct ScanConst {                                  // dsg_scan_init parameters 
     int32_t rT, rC, nt, cell, period, kmin;
 };
 
-__global__ void __launch_bounds__(TN) k_tab_h(const TabIn *__restrict__ tin, float *__restrict__ hout, ScanConst sc) {
-    __shared__ uint8_t P[256], col[2][256];
-    __shared__ float Tc[2][2][8][16];
-    __shared__ int i0[2], k0[2];
-    __shared__ float row[8][TN];
-    const int tb = blockIdx.z * 6 + blockIdx.y, t = threadIdx.x;
-    const TabIn &in = tin[tb];
-    if (t < 256) { P[t] = in.perm[t]; col[0][t] = in.col[0][t]; col[1][t] = in.col[1][t]; }
-    (&Tc[0][0][0][0])[t] = (&in.T[0][0][0][0])[t];
-    if (t < 2) { i0[t] = in.i0[t]; k0[t] = in.k0[t]; }
-    __syncthreads();
-    const int px = t & 1, ix = (t >> 1) + i0[px];
-    #pragma unroll
-    for (int r = 0; r < 8; r++) {
-        const int j = blockIdx.x * 8 + r, pz = j & 1, iz = (j >> 1) + k0[pz];
-        float acc = 0.f;
-        #pragma unroll
-        for (int c = 0; c < 8; c++) {
-            const int dx = c & 1, dy = (c >> 1) & 1, dz = c >> 2;
-            acc = __fadd_rn(acc, Tc[px][pz][c][P[(col[dy][(ix + dx) & 255] + iz + dz) & 255] & 15]);
-        }
-        row[r][t] = acc;
-    }
-    __syncthreads();
-    const bool isT = blockIdx.y < 2;
-    const int rr = isT ? sc.rT : sc.rC;
-    const float *k = isT ? sc.kT : sc.kC;
-    float *o = hout + size_t(tb) * TN * TN + size_t(blockIdx.x) * 8 * TN;
-    #pragma unroll
-    for (int r = 0; r < 8; r++) {
-        float s = 0.f;
-        for (int d = 0; d <= 2 * rr; d++) s = __fadd_rn(s, __fmul_rn(k[d], row[r][(t + d - rr) & (TN - 1)]));
-        o[r * TN + t] = s;
-    }
-}
-
 __device__ __forceinline__ void atomic_max_float(float *a, float v) {
     if (v >= 0.f) atomicMax(reinterpret_cast<int *>(a), __float_as_int(v));
     else atomicMin(reinterpret_cast<unsigned *>(a), __float_as_uint(v));
 }
 
-constexpr int VB = 32;                              // output rows per k_blur_v block
-__global__ void __launch_bounds__(TN) k_blur_v(const float *__restrict__ hin, float *__restrict__ out, float *__restrict__ mx, ScanConst sc) {
-    const int tb = blockIdx.z * 6 + blockIdx.y, t = threadIdx.x;
-    const bool isT = blockIdx.y < 2;
-    const int rr = isT ? sc.rT : sc.rC;
-    const float *k = isT ? sc.kT : sc.kC;
-    const float *h = hin + size_t(tb) * TN * TN;
-    float *o = out + size_t(tb) * TN * TN;
-    const int j0 = blockIdx.x * VB;
-    float best = -1e30f;
-    for (int jj = 0; jj < VB; jj++) {
-        const int j = j0 + jj;
-        float s = 0.f;
-        for (int d = 0; d <= 2 * rr; d++) s = __fadd_rn(s, __fmul_rn(k[d], __ldg(&h[size_t((j + d - rr) & (TN - 1)) * TN + t])));
-        o[size_t(j) * TN + t] = s;
-        best = fmaxf(best, s);
+// Geometry of k_tables for blur radius R.  A band of NR output rows starting at row r0 needs the blurred rows
+// r0 - R .. r0 + NR - 1 + R (periodic in 512).  The CTA generates rows from g0 = r0 - E (E = R rounded up to
+// even, so that every chunk starts on an even row and its rows' parities are known at compile time), FCH per
+// chunk; output block b (rows r0 + b FCH ..) needs chunks up to b + A.  Chunk k + 1 is blurred into the ring
+// only after every thread has finished output block k + 1 - A, so the ring needs NEED rows.
+constexpr int FCH = 8;
+template <int R> struct Band {
+    static constexpr int E = 2 * ((R + 1) / 2);
+    static constexpr int A = (E + R + FCH - 1) / FCH;
+    static constexpr int NEED = (A + 1) * FCH - (E - R);
+    static constexpr int RING = NEED <= 32 ? 32 : 64;
+    static constexpr int NQ = (R + 3) / 4;                 // 4-column groups read on each side by the row blur
+    static constexpr int BLOCKS = RING == 32 ? 2 : 1;      // CTAs per SM (shared memory)
+    static constexpr size_t SMEM = size_t(FCH + RING) * TN * 4;
+};
+struct TableTaps { float k[2][2 * RMAX + 1]; };            // [0]: T tables, [1]: C and E tables
+
+// Corner sums of the FCH rows of one chunk for this thread's column (tabulate, lowfield.hpp:35-55): row g of
+// the chunk, parity pz = g & 1, z lattice iz = (g >> 1) + k0[pz]; corner c = dx + 2 dy + 4 dz adds
+// Tc[px][pz][c][P[(col[dy][ix + dx] + iz + dz) & 255] & 15] in corner order.  The hash of each (dx, dy, m)
+// is looked up once per chunk: even rows use m = me + q + dz (q = row / 2); odd rows m = me + D + q + dz when
+// D = k0[1] - k0[0] is 0 or 1, else (D == 2) their own lookups from mo.  A hash is kept as the byte offset of
+// its entry in the [pz][c][px][h] table, so each corner is one shared load with a constant offset.  (Lookups
+// from a pre-shifted copy of P, repeated to 520 entries per column parity so that they need no mask, issued
+// 11% fewer instructions but took 6% longer: the larger table's byte gathers conflict more in the banks.)
+template <int D>
+__device__ __forceinline__ void tab_chunk(const uint8_t *__restrict__ P, const char *__restrict__ tcb, const int (&cv)[4], int pxo, int me,
+                                          int mo, float *__restrict__ rawc) {
+    constexpr int NE = FCH / 2 + 1 + (D == 1), NO = D == 2 ? FCH / 2 + 1 : 1;
+    int ae[4][NE], ao[4][NO];
+    #pragma unroll
+    for (int q = 0; q < 4; q++) {
+        #pragma unroll
+        for (int i = 0; i < NE; i++) ae[q][i] = pxo + ((P[(cv[q] + me + i) & 255] & 15) << 2);
+        #pragma unroll
+        for (int i = 0; i < NO; i++) ao[q][i] = D == 2 ? pxo + ((P[(cv[q] + mo + i) & 255] & 15) << 2) : 0;
     }
-    if (isT) {
+    #pragma unroll
+    for (int r = 0; r < FCH; r++) {
+        const int pz = r & 1, q = r >> 1;
+        float acc = 0.f;
+        #pragma unroll
+        for (int c = 0; c < 8; c++) {
+            const int xy = c & 3, dz = c >> 2;
+            const int off = pz == 0 ? ae[xy][q + dz] : D == 2 ? ao[xy][q + dz] : ae[xy][q + dz + D];
+            acc = __fadd_rn(acc, *reinterpret_cast<const float *>(tcb + off + (pz * 8 + c) * 128));
+        }
+        rawc[r * TN] = acc;
+    }
+}
+
+// Vertical blur of output block rows (thread = column): output o adds k[d] * row(o + d - R) for d = 0..2R in
+// that order (the blur's rounding order), streaming the window's rows from the ring once each.  PH = the
+// block's position in the ring (its slot offsets are then constants).
+template <int R, int PH>
+__device__ __forceinline__ void vblur_block(const float *__restrict__ ringc, const float (&kk)[2 * R + 1], float *__restrict__ outc, float &best) {
+    using B = Band<R>;
+    constexpr int W0 = PH * FCH + B::E - R;
+    float s[FCH];
+    #pragma unroll
+    for (int o = 0; o < FCH; o++) s[o] = 0.f;
+    #pragma unroll
+    for (int i = 0; i < FCH + 2 * R; i++) {
+        const float v = ringc[((W0 + i) & (B::RING - 1)) * TN];
+        #pragma unroll
+        for (int o = 0; o < FCH; o++)
+            if (i - o >= 0 && i - o <= 2 * R) s[o] = __fadd_rn(s[o], __fmul_rn(kk[i - o], v));
+    }
+    #pragma unroll
+    for (int o = 0; o < FCH; o++) { outc[o * TN] = s[o]; best = fmaxf(best, s[o]); }
+}
+
+template <int R, int... PH>
+__device__ __forceinline__ void vblur_any(int ph, const float *ringc, const float (&kk)[2 * R + 1], float *outc, float &best,
+                                          std::integer_sequence<int, PH...>) {
+    ((ph == PH ? vblur_block<R, PH>(ringc, kk, outc, best) : void()), ...);
+}
+
+// Tables tab0 .. tab0 + gridDim.y - 1 of seed blockIdx.z, band blockIdx.x of gridDim.x; out = the blurred
+// tables [seed][6][512][512]; mx[seed][2] = the maxima of the two T tables (atomic, preset by the caller).
+template <int R>
+__global__ void __launch_bounds__(TN, Band<R>::BLOCKS) k_tables(const TabIn *__restrict__ tin, float *__restrict__ out, float *__restrict__ mx,
+                                                              TableTaps taps, int tab0) {
+    using B = Band<R>;
+    extern __shared__ __align__(16) float dsm[];
+    __shared__ uint8_t P[256];
+    __shared__ __align__(16) float Tc[2][8][2][16];                // [pz][c][px][h]
+    float *raw = dsm, *ring = dsm + FCH * TN;
+    const int t = threadIdx.x, tb = tab0 + blockIdx.y, sd = blockIdx.z;
+    const TabIn &in = tin[sd * 6 + tb];
+    if (t < 256) P[t] = in.perm[t];
+    {
+        const int h = t & 15, c = (t >> 4) & 7, pz = (t >> 7) & 1, px = t >> 8;
+        Tc[pz][c][px][h] = in.T[px][pz][c][h];
+    }
+    const int px = t & 1, ix = (t >> 1) + in.i0[px];
+    int cv[4];
+    #pragma unroll
+    for (int q = 0; q < 4; q++) cv[q] = in.col[q >> 1][(ix + (q & 1)) & 255];
+    const int k00 = in.k0[0], k01 = in.k0[1], dk = k01 - k00;
+    float kk[2 * R + 1];
+    #pragma unroll
+    for (int d = 0; d <= 2 * R; d++) kk[d] = tb < 2 ? taps.k[0][d] : taps.k[1][d];
+    __syncthreads();
+
+    const int NR = TN / gridDim.x, r0 = blockIdx.x * NR, NB = NR / FCH, g0 = r0 - B::E;
+    const char *tcb = reinterpret_cast<const char *>(&Tc[0][0][0][0]);
+    const int pxo = px * 64, hq = t & 127, hr = t >> 7;
+    float *const otab = out + (size_t(sd) * 6 + tb) * TN * TN;
+    float best = -1e30f;
+    for (int k = 0; k < NB + B::A; k++) {
+        const int gb = (g0 + k * FCH) & (TN - 1), me = (gb >> 1) + k00, mo = (gb >> 1) + k01;
+        if (dk == 0) tab_chunk<0>(P, tcb, cv, pxo, me, mo, raw + t);
+        else if (dk == 1) tab_chunk<1>(P, tcb, cv, pxo, me, mo, raw + t);
+        else tab_chunk<2>(P, tcb, cv, pxo, me, mo, raw + t);
+        __syncthreads();
+        // row blur (thread = columns 4 hq .. 4 hq + 3 of rows hr, hr + 4): column i adds k[d] * raw[i + d - R]
+        #pragma unroll
+        for (int h = 0; h < FCH / 4; h++) {
+            const int r = hr + 4 * h;
+            const float *row = raw + r * TN;
+            float x[4 * (2 * B::NQ + 1)];
+            #pragma unroll
+            for (int j = 0; j <= 2 * B::NQ; j++) {
+                const float4 v = *reinterpret_cast<const float4 *>(row + ((4 * (hq + j - B::NQ)) & (TN - 1)));
+                x[4 * j] = v.x; x[4 * j + 1] = v.y; x[4 * j + 2] = v.z; x[4 * j + 3] = v.w;
+            }
+            float o[4];
+            #pragma unroll
+            for (int u = 0; u < 4; u++) {
+                float a = 0.f;
+                #pragma unroll
+                for (int d = 0; d <= 2 * R; d++) a = __fadd_rn(a, __fmul_rn(kk[d], x[u + d - R + 4 * B::NQ]));
+                o[u] = a;
+            }
+            *reinterpret_cast<float4 *>(ring + (((k * FCH) & (B::RING - 1)) + r) * TN + 4 * hq) = make_float4(o[0], o[1], o[2], o[3]);
+        }
+        __syncthreads();
+        if (k >= B::A) {
+            const int b = k - B::A;
+            vblur_any<R>(b & (B::RING / FCH - 1), ring + t, kk, otab + size_t(r0 + b * FCH) * TN + t, best,
+                         std::make_integer_sequence<int, B::RING / FCH>{});
+        }
+    }
+    if (tb < 2) {
         #pragma unroll
         for (int q = 16; q > 0; q >>= 1) best = fmaxf(best, __shfl_xor_sync(0xffffffffu, best, q));
-        if ((t & 31) == 0) atomic_max_float(&mx[blockIdx.z * 2 + blockIdx.y], best);
+        if ((t & 31) == 0) atomic_max_float(&mx[sd * 2 + tb], best);
     }
 }
 
@@ -177,7 +270,7 @@ struct State {
     int16_t *d_ibT = nullptr, *d_ibC = nullptr; int8_t *d_loT = nullptr, *d_hiT = nullptr;
     cudaStream_t st = nullptr;
     uint32_t cap_seeds = 0;
-    TabIn *d_in = nullptr; float *d_tab = nullptr, *d_h = nullptr, *d_mx = nullptr;
+    TabIn *d_in = nullptr; float *d_tab = nullptr, *d_mx = nullptr;
     int32_t *d_act = nullptr; uint32_t *d_nact = nullptr, *d_ncand = nullptr;
     Cand *d_out = nullptr; uint32_t cap_cand = 0;
     uint64_t *d_seeds = nullptr; SeedNoise *d_noise = nullptr;   // dsg_scan_seeds
@@ -187,13 +280,12 @@ State &S() { static State s; return s; }
 void ensure(State &g, uint32_t seeds, uint32_t cap) {
     if (seeds <= g.cap_seeds && cap <= g.cap_cand) return;
     const uint32_t ns = std::max(seeds, g.cap_seeds), nc = std::max(cap, g.cap_cand);
-    cudaFree(g.d_in); cudaFree(g.d_tab); cudaFree(g.d_h); cudaFree(g.d_mx); cudaFree(g.d_act); cudaFree(g.d_nact);
+    cudaFree(g.d_in); cudaFree(g.d_tab); cudaFree(g.d_mx); cudaFree(g.d_act); cudaFree(g.d_nact);
     cudaFree(g.d_ncand); cudaFree(g.d_out); cudaFree(g.d_seeds); cudaFree(g.d_noise);
     DSG_CU(cudaMalloc(&g.d_seeds, size_t(ns) * 8));
     DSG_CU(cudaMalloc(&g.d_noise, size_t(ns) * sizeof(SeedNoise)));
     DSG_CU(cudaMalloc(&g.d_in, size_t(ns) * 6 * sizeof(TabIn)));
     DSG_CU(cudaMalloc(&g.d_tab, size_t(ns) * 6 * TN * TN * 4));
-    DSG_CU(cudaMalloc(&g.d_h, size_t(ns) * 6 * TN * TN * 4));
     DSG_CU(cudaMalloc(&g.d_mx, size_t(ns) * 2 * 4));
     DSG_CU(cudaMalloc(&g.d_act, size_t(ns) * TN * TN * 4));
     DSG_CU(cudaMalloc(&g.d_nact, size_t(ns) * 4));
@@ -202,13 +294,41 @@ void ensure(State &g, uint32_t seeds, uint32_t cap) {
     g.cap_seeds = ns; g.cap_cand = nc;
 }
 
+// k_tables for radius R over tables tab0 .. tab0 + ntab - 1 of S seeds.  Bands per table: the fewest (1 to 8)
+// that give at least four waves of CTAs, so that the tail of the grid stays short.
+template <int R>
+void tables_radius(State &g, uint32_t S, int tab0, int ntab) {
+    using B = Band<R>;
+    static const int slots = [] {
+        DSG_CU(cudaFuncSetAttribute(k_tables<R>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(B::SMEM)));
+        int occ = 0;
+        DSG_CU(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_tables<R>, TN, B::SMEM));
+        return std::max(1, occ) * device_info().sms;
+    }();
+    int split = 1;
+    while (split < 8 && uint64_t(S) * ntab * split < uint64_t(4) * slots) split *= 2;
+    TableTaps tp{};
+    std::copy(g.sc.kT, g.sc.kT + 2 * RMAX + 1, tp.k[0]);
+    std::copy(g.sc.kC, g.sc.kC + 2 * RMAX + 1, tp.k[1]);
+    k_tables<R><<<dim3(split, ntab, S), TN, B::SMEM, g.st>>>(g.d_in, g.d_tab, g.d_mx, tp, tab0);
+}
+template <int... R>
+void tables_any(int r, State &g, uint32_t S, int tab0, int ntab, std::integer_sequence<int, R...>) {
+    ((r == R ? tables_radius<R>(g, S, tab0, ntab) : void()), ...);
+}
+// All six tables of S seeds: one launch when the T and C/E blurs have the same radius, else one per radius.
+void launch_tables(State &g, uint32_t S) {
+    constexpr auto radii = std::make_integer_sequence<int, RMAX + 1>{};
+    if (g.sc.rT == g.sc.rC) tables_any(g.sc.rT, g, S, 0, 6, radii);
+    else { tables_any(g.sc.rT, g, S, 0, 2, radii); tables_any(g.sc.rC, g, S, 2, 4, radii); }
+}
+
 // Tables + blur + max (+ active list and scan if want_scan) for S seeds already in g.d_in; on g.st.
 void enqueue(State &g, uint32_t S, const dsg_scan_params *sp, uint32_t cap, bool want_scan) {
     const std::vector<float> ninf(size_t(S) * 2, -1e30f);
     DSG_CU(cudaMemcpyAsync(g.d_mx, ninf.data(), size_t(S) * 8, cudaMemcpyHostToDevice, g.st));
     DSG_CU(cudaStreamSynchronize(g.st));                 // ninf is a host temporary
-    k_tab_h<<<dim3(TN / 8, 6, S), TN, 0, g.st>>>(g.d_in, g.d_h, g.sc);
-    k_blur_v<<<dim3(TN / VB, 6, S), TN, 0, g.st>>>(g.d_h, g.d_tab, g.d_mx, g.sc);
+    launch_tables(g, S);
     if (want_scan) {
         DSG_CU(cudaMemsetAsync(g.d_nact, 0, size_t(S) * 4, g.st));
         DSG_CU(cudaMemsetAsync(g.d_ncand, 0, size_t(S) * 4, g.st));

@@ -189,6 +189,13 @@ int orc_tables(uint64_t seed, double sigma, double sigmac, float *out, float *mx
     for (int s = 0; s < 2; s++) mx[s] = *std::max_element(out + size_t(s) * TN * TN, out + size_t(s + 1) * TN * TN);
     return 0;
 }
+// The same six tables from given table inputs (any lattice offsets, e.g. k0[1] - k0[0] outside {0, 1}).
+int orc_tables_in(const TabIn *t, double sigma, double sigmac, float *out, float *mx) {
+    const BlurTaps bt = blur_taps(sigma), bc = blur_taps(sigmac);
+    for (int k = 0; k < 6; k++) { tabulate(t[k], out + size_t(k) * TN * TN); blur(out + size_t(k) * TN * TN, k < 2 ? bt : bc); }
+    for (int s = 0; s < 2; s++) mx[s] = *std::max_element(out + size_t(s) * TN * TN, out + size_t(s + 1) * TN * TN);
+    return 0;
+}
 int orc_tmap(double lat, int16_t *ib, int8_t *lo, int8_t *hi) {
     const TMap m = tmap(lat);
     std::memcpy(ib, m.ib, sizeof m.ib); std::memcpy(lo, m.lo, TN); std::memcpy(hi, m.hi, TN);

@@ -38,6 +38,53 @@ def test_tables_bit_exact(scan_ready):
         assert np.array_equal(mx[k], m)
 
 
+def _init(dsg, sigma, sigmac):
+    o = libs.orc()
+    ibT, loT, hiT = o.tmap(1024.0)
+    ibC, _, _ = o.tmap(512.0)
+    dsg.scan_init(ibT, loT, hiT, ibC, o.blur_taps(sigma)[0], o.blur_taps(sigmac)[0])
+
+
+@pytest.mark.parametrize("sigma,sigmac", [(2.0, 2.0), (0.3, 4.9), (3.6, 3.6), (4.9, 1.0)])
+def test_tables_radii_and_batch_sizes(scan_ready, sigma, sigmac):
+    """Blur radii 1 to 15 (equal radii: one launch over six tables; different: one per radius) and batches of
+    1 to 200 seeds (every band split of the tables kernel) against the oracle, bit for bit; three seeds of
+    each batch are checked."""
+    o = libs.orc()
+    rng = np.random.default_rng(int(sigma * 10 + sigmac))
+    _init(scan_ready, sigma, sigmac)
+    try:
+        for n in ([1, 50, 100, 200] if sigma == sigmac == 2.0 else [1, 60]):
+            ss = [libs.mix(int(v)) for v in rng.integers(0, 1 << 40, n)]
+            tabs, mx = scan_ready.tables(np.concatenate([o.tabins(s) for s in ss]))
+            for k in sorted({0, n // 2, n - 1}):
+                t, m = o.tables(ss[k], sigma, sigmac)
+                assert np.array_equal(tabs[k], t), f"n={n} seed {ss[k]}: {np.sum(tabs[k] != t)} cells differ"
+                assert np.array_equal(mx[k], m)
+    finally:
+        _init(scan_ready, 2.0, 2.0)
+
+
+def test_tables_any_lattice_offsets(scan_ready):
+    """Table inputs whose z (or x) lattice offsets of the two parities differ by other than 0 or 1 take the
+    kernel's general hash path; results equal the oracle's tabulation of the same inputs."""
+    o = libs.orc()
+    base = o.tabins(seeds()[0]).copy()
+    recs = []
+    for di, dk in [(0, 0), (1, 1), (0, -3), (7, 200), (-40, 2)]:
+        t = base.copy().view(np.uint8)
+        off = libs.TABIN_BYTES - 16                       # int i0[2], k0[2] close each record
+        for k in range(6):
+            v = t[k * libs.TABIN_BYTES + off: (k + 1) * libs.TABIN_BYTES].view(np.int32)
+            v[1] = v[0] + di; v[3] = v[2] + dk
+        recs.append(t)
+    tabs, mx = scan_ready.tables(np.concatenate(recs))
+    for k, t in enumerate(recs):
+        want, m = o.tables_in(t)
+        assert np.array_equal(tabs[k], want), f"record {k}: {np.sum(tabs[k] != want)} cells differ"
+        assert np.array_equal(mx[k], m)
+
+
 def test_scan_candidates_match_oracle(scan_ready):
     o = libs.orc()
     ss = seeds()
