@@ -59,20 +59,23 @@ struct TableTaps { float k[2][2 * RMAX + 1]; };            // [0]: T tables, [1]
 // Tc[px][pz][c][P[(col[dy][ix + dx] + iz + dz) & 255] & 15] in corner order.  The hash of each (dx, dy, m)
 // is looked up once per chunk: even rows use m = me + q + dz (q = row / 2); odd rows m = me + D + q + dz when
 // D = k0[1] - k0[0] is 0 or 1, else (D == 2) their own lookups from mo.  A hash is kept as the byte offset of
-// its entry in the [pz][c][px][h] table, so each corner is one shared load with a constant offset.  (Lookups
-// from a pre-shifted copy of P, repeated to 520 entries per column parity so that they need no mask, issued
-// 11% fewer instructions but took 6% longer: the larger table's byte gathers conflict more in the banks.)
+// its entry in the [pz][c][px][h] table, so each corner is one shared load with a constant offset.  PO holds
+// 4 (P[x & 255] & 15) for x = 0 .. PL - 1: masking cv + m once per chunk, the chunk's lookups are byte loads
+// at constant offsets, plus the column parity's offset pxo.  (Tables with pxo folded in, one per parity,
+// measured 6% slower: alternate lanes then gather from two tables, and the banks conflict more.)
+constexpr int PL = 264;                                    // >= 256 + FCH / 2 + 2, multiple of 4
 template <int D>
-__device__ __forceinline__ void tab_chunk(const uint8_t *__restrict__ P, const char *__restrict__ tcb, const int (&cv)[4], int pxo, int me,
+__device__ __forceinline__ void tab_chunk(const uint8_t *__restrict__ PO, const char *__restrict__ tcb, const int (&cv)[4], int pxo, int me,
                                           int mo, float *__restrict__ rawc) {
     constexpr int NE = FCH / 2 + 1 + (D == 1), NO = D == 2 ? FCH / 2 + 1 : 1;
     int ae[4][NE], ao[4][NO];
     #pragma unroll
     for (int q = 0; q < 4; q++) {
+        const uint8_t *pe = PO + ((cv[q] + me) & 255), *po = PO + ((cv[q] + mo) & 255);
         #pragma unroll
-        for (int i = 0; i < NE; i++) ae[q][i] = pxo + ((P[(cv[q] + me + i) & 255] & 15) << 2);
+        for (int i = 0; i < NE; i++) ae[q][i] = pxo + pe[i];
         #pragma unroll
-        for (int i = 0; i < NO; i++) ao[q][i] = D == 2 ? pxo + ((P[(cv[q] + mo + i) & 255] & 15) << 2) : 0;
+        for (int i = 0; i < NO; i++) ao[q][i] = D == 2 ? pxo + po[i] : 0;
     }
     #pragma unroll
     for (int r = 0; r < FCH; r++) {
@@ -122,12 +125,12 @@ __global__ void __launch_bounds__(TN, Band<R>::BLOCKS) k_tables(const TabIn *__r
                                                               TableTaps taps, int tab0) {
     using B = Band<R>;
     extern __shared__ __align__(16) float dsm[];
-    __shared__ uint8_t P[256];
+    __shared__ uint8_t PO[PL];                                      // see tab_chunk
     __shared__ __align__(16) float Tc[2][8][2][16];                // [pz][c][px][h]
     float *raw = dsm, *ring = dsm + FCH * TN;
     const int t = threadIdx.x, tb = tab0 + blockIdx.y, sd = blockIdx.z;
     const TabIn &in = tin[sd * 6 + tb];
-    if (t < 256) P[t] = in.perm[t];
+    for (int x = t; x < PL; x += TN) PO[x] = uint8_t((in.perm[x & 255] & 15) << 2);
     {
         const int h = t & 15, c = (t >> 4) & 7, pz = (t >> 7) & 1, px = t >> 8;
         Tc[pz][c][px][h] = in.T[px][pz][c][h];
@@ -149,9 +152,9 @@ __global__ void __launch_bounds__(TN, Band<R>::BLOCKS) k_tables(const TabIn *__r
     float best = -1e30f;
     for (int k = 0; k < NB + B::A; k++) {
         const int gb = (g0 + k * FCH) & (TN - 1), me = (gb >> 1) + k00, mo = (gb >> 1) + k01;
-        if (dk == 0) tab_chunk<0>(P, tcb, cv, pxo, me, mo, raw + t);
-        else if (dk == 1) tab_chunk<1>(P, tcb, cv, pxo, me, mo, raw + t);
-        else tab_chunk<2>(P, tcb, cv, pxo, me, mo, raw + t);
+        if (dk == 0) tab_chunk<0>(PO, tcb, cv, pxo, me, mo, raw + t);
+        else if (dk == 1) tab_chunk<1>(PO, tcb, cv, pxo, me, mo, raw + t);
+        else tab_chunk<2>(PO, tcb, cv, pxo, me, mo, raw + t);
         __syncthreads();
         // row blur (thread = columns 4 hq .. 4 hq + 3 of rows hr, hr + 4): column i adds k[d] * raw[i + d - R]
         #pragma unroll

@@ -55,21 +55,29 @@ def test_mcmeasure_step1_golden():
 
 def test_tgate_matches_reference_tool(dsg):
     """Same survivor lines as the reference's tgate.  The reference's pre-gate kernel is not deterministic on
-    this GPU (a few seeds per run move by up to 3e-3), so a seed may differ only when one of its gate sums
-    lies that close to its threshold."""
+    this GPU (a few seeds per run move, most by up to 3e-3), so a seed may differ only when one of its gate
+    sums lies that close to its threshold, or when the reference disagrees with itself on it (a second run
+    of the reference tool, made only in that case)."""
     import numpy as np
     args = [str(10**12), str(1 << 22), "phase=0.06", "amp=0.70", "pthr=0.645"]
     a = run([os.path.join(BIN, "tgate")] + args + ["check=1"])
     b = run([ref("tgate")] + args)
     assert a.returncode == b.returncode == 0
-    la, lb = sorted(a.stdout.split("\n")), sorted(b.stdout.split("\n"))
-    diff = (set(la) ^ set(lb)) - {""}
+    la, lb = set(a.stdout.split("\n")) - {""}, set(b.stdout.split("\n")) - {""}
+    diff = la ^ lb
     assert len(diff) <= 4, diff
     if diff:
-        seeds = np.array([int(l.split()[0]) for l in diff], dtype=np.uint64)
+        lines = sorted(diff)
+        seeds = np.array([int(l.split()[0]) for l in lines], dtype=np.uint64)
         pre, full = dsg.gate_amps(seeds)
         near = (np.abs(pre.sum(1) - 0.645) < 4e-3) | (np.abs(full.sum(1) - 0.70) < 4e-3)
-        assert near.all(), (diff, pre.sum(1), full.sum(1))
+        if not near.all():
+            b2 = run([ref("tgate")] + args)
+            assert b2.returncode == 0
+            lb2 = set(b2.stdout.split("\n")) - {""}
+            unstable = {l for l in lines if (l in lb) != (l in lb2)}
+            near |= np.array([l in unstable for l in lines])
+        assert near.all(), (lines, pre.sum(1), full.sum(1))
     checks = re.findall(r"check seed \d+: gpu amp ([\d.]+) cpu amp ([\d.]+)", a.stderr)
     assert checks and all(abs(float(g) - float(c)) < 2e-5 for g, c in checks)
     assert re.search(r"gate: \d+ seeds, \d+ phase-passed, \d+ pre-gate, \d+ passed", a.stderr)
