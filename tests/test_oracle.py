@@ -121,6 +121,21 @@ def test_tables_match_reference_fixture():
     assert hashlib.sha256(t.tobytes()).digest() == d["sha0"].tobytes() and np.array_equal(mx, d["max0"])
 
 
+@pytest.mark.parametrize("sigma,sigmac", [(0.3, 4.9), (3.6, 3.6), (4.9, 1.0)])
+def test_tables_other_blur_widths_match_reference_live(ref_cpu, sigma, sigmac):
+    """The oracle's six tables at the blur widths the GPU tests use besides sigma 2 (radii 1, 4, 11, 15) equal
+    the reference's own code's (lowfield.hpp tabulate_octave + Blur), bit for bit."""
+    o = libs.orc()
+    rng = np.random.default_rng(7)
+    for s in [libs.mix(int(v)) for v in rng.integers(0, 1 << 40, 2)]:
+        a, ma = o.tables(s, sigma, sigmac)
+        b, mb = ref_cpu.tables(s, sigma, sigmac)
+        assert np.array_equal(a, b), f"seed {s}: {np.sum(a != b)} cells differ"
+        assert np.array_equal(ma, mb)
+    for sg in (sigma, sigmac):
+        assert np.array_equal(o.blur_taps(sg)[0], ref_cpu.blur_taps(sg)[0])
+
+
 def test_scan_buckets_match_reference_cli():
     """Scan candidates bucketed by 5,000 quarts and NMS'd as the searcher does give the reference CLI's
     bucket and site counts and its maxta/maxtb (printed to 4 decimals)."""
