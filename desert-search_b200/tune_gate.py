@@ -79,6 +79,33 @@ def child(lib_path, steps, warmup):
     print(json.dumps({"ms": ms.value, "kernel_ms": list(mk), "counts": list(cnt), "amps": amps}))
 
 
+def choose(rows):
+    """The pre-gate and full-gate shapes to keep, from the measured rows (the first row is the default build).
+    Only candidates whose amplitudes are bit-identical to the default's count; a shape replaces the default
+    only when it is at least MIN_GAIN faster (run-to-run noise is ~0.5%)."""
+    ok = [r for r in rows if r.get("bit_identical")]
+    default = ok[0]
+    best_pg = min((r for r in ok if (r["fullgate_blocks_per_sm"], r["fullgate_rows"]) == FULLGATE[0]), key=lambda r: r["pregate_ms"])
+    best_fg = min((r for r in ok if r["pregate_blocks_per_sm"] == PREGATE[0]), key=lambda r: r["fullgate_ms"])
+    if best_pg["pregate_ms"] > (1 - MIN_GAIN) * default["pregate_ms"]:
+        best_pg = default
+    if best_fg["fullgate_ms"] > (1 - MIN_GAIN) * default["fullgate_ms"]:
+        best_fg = default
+    return best_pg, best_fg
+
+
+def header_text(best_pg, best_fg):
+    """gate_tuned.h for the chosen shapes."""
+    out = ("// Launch shapes of the gate kernels, as chosen by desert-search_b200/tune_gate.py on a B200 (each candidate\n"
+           "// built, checked bit for bit against the default build, and timed with dsg_gate_bench).  A -D on the\n"
+           "// compiler command line overrides them; that is how the tuner builds its candidates.\n#pragma once\n")
+    for name, val, what in (("DSG_PG_MINBLOCKS", best_pg["pregate_blocks_per_sm"], "k_pregate blocks per SM (register cap 65536 / (64 x this))"),
+                            ("DSG_FG_MINBLOCKS", best_fg["fullgate_blocks_per_sm"], "k_fullgate blocks per SM (register cap 65536 / (128 x this))"),
+                            ("DSG_FG_ROWS", best_fg["fullgate_rows"], "k_fullgate rows staged in shared memory per block step")):
+        out += f"#ifndef {name}\n" + f"#define {name} {val}".ljust(32) + f"// {what}\n#endif\n"
+    return out
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--child", nargs=3)
@@ -109,23 +136,9 @@ def main():
             row.update({"pregate_ms": m["kernel_ms"][2], "fullgate_ms": m["kernel_ms"][3], "total_ms": m["ms"],
                         "gated": m["counts"][3], "bit_identical": m["amps"] == base})
             rows.append(row); print(json.dumps(row), flush=True)
-    # a shape replaces the default only when it is at least MIN_GAIN faster (run-to-run noise is ~0.5%)
-    ok = [r for r in rows if r.get("bit_identical")]
-    default = ok[0]
-    best_pg = min((r for r in ok if (r["fullgate_blocks_per_sm"], r["fullgate_rows"]) == FULLGATE[0]), key=lambda r: r["pregate_ms"])
-    best_fg = min((r for r in ok if r["pregate_blocks_per_sm"] == PREGATE[0]), key=lambda r: r["fullgate_ms"])
-    if best_pg["pregate_ms"] > (1 - MIN_GAIN) * default["pregate_ms"]:
-        best_pg = default
-    if best_fg["fullgate_ms"] > (1 - MIN_GAIN) * default["fullgate_ms"]:
-        best_fg = default
+    best_pg, best_fg = choose(rows)
     with open(a.out, "w") as f:
-        f.write("// Launch shapes of the gate kernels, as chosen by desert-search_b200/tune_gate.py on a B200 (each candidate\n"
-                "// built, checked bit for bit against the default build, and timed with dsg_gate_bench).  A -D on the\n"
-                "// compiler command line overrides them; that is how the tuner builds its candidates.\n#pragma once\n")
-        for name, val, what in (("DSG_PG_MINBLOCKS", best_pg["pregate_blocks_per_sm"], "k_pregate blocks per SM (register cap 65536 / (64 x this))"),
-                                ("DSG_FG_MINBLOCKS", best_fg["fullgate_blocks_per_sm"], "k_fullgate blocks per SM (register cap 65536 / (128 x this))"),
-                                ("DSG_FG_ROWS", best_fg["fullgate_rows"], "k_fullgate rows staged in shared memory per block step")):
-            f.write(f"#ifndef {name}\n#define {name} {val:<8}// {what}\n#endif\n")
+        f.write(header_text(best_pg, best_fg))
     if a.report:
         with open(a.report, "w") as f:
             f.write("\n".join(json.dumps(r) for r in rows) + "\n")
