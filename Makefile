@@ -1,10 +1,9 @@
 # desert-search-b200 build.  `make` builds the CUDA library (sm_100a), the host tools and the test
 # oracle; `make ref` additionally compiles the reference's own sources in place into oracle/_ref
-# (needs the reference checkout, REF).
+# (needs the reference checkout: oracle/ref.mk holds its default location, REF=... overrides it).
 NVCC     ?= nvcc
 CXX      ?= g++
 PY       ?= python3
-REF      ?= /root/reference
 PKG      := desert-search_b200
 B        := _build
 GPUARCH  := -gencode arch=compute_100a,code=sm_100a
@@ -25,7 +24,7 @@ all: $(LIB) $(HOST_BIN) $(ORC_LIB)
 lib: $(LIB)
 oracle: $(ORC_LIB)
 ref:
-	$(MAKE) -f oracle/ref.mk REF=$(REF)
+	$(MAKE) -f oracle/ref.mk $(if $(REF),REF=$(REF))
 
 $(B) $(PKG)/lib $(PKG)/bin:
 	mkdir -p $@

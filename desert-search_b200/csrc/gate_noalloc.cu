@@ -14,7 +14,8 @@
 // code the array's name is only a host-side stand-in, never a device address) and computes the blur taps
 // into it with one synchronous copy back; make that first call before any stream capture.  Every call
 // shares the one array and leaves the previous call's contents in it; this file resets the counters that
-// must start at zero on each call.  Calls whose work overlaps on the GPU (different streams, or several
+// must start at zero on each call.  The set-up is kept for the life of the process: a cudaDeviceReset of a
+// device after the first call there is not supported (the array's contents and address are not restored).  Calls whose work overlaps on the GPU (different streams, or several
 // host threads at once) race on the array and must be serialised by the caller.
 #include "common.cuh"
 #include <mutex>
@@ -63,6 +64,7 @@ extern "C" int dsg_gate_amps_noalloc(const uint64_t *seeds, uint32_t n, float *p
             e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
             if (e != cudaSuccess) { set_error("dsg_gate_amps_noalloc: cudaGetSymbolAddress: %s", cudaGetErrorString(e)); return DSG_E_CUDA; }
             unsigned char *s = static_cast<unsigned char *>(p);
+            (void)cudaGetLastError();                    // an error the caller left pending is not this set-up's
             gate::gate_taps_into(reinterpret_cast<float *>(s + OFF_TAPS), nullptr);
             e = cudaGetLastError();
             if (e == cudaSuccess) e = cudaMemcpy(d.taps, s + OFF_TAPS, sizeof d.taps, cudaMemcpyDeviceToHost);
@@ -80,6 +82,7 @@ extern "C" int dsg_gate_amps_noalloc(const uint64_t *seeds, uint32_t n, float *p
     cudaStream_t st = static_cast<cudaStream_t>(stream);
     unsigned char *s = d.scratch;
     uint32_t *cnt = reinterpret_cast<uint32_t *>(s + OFF_CNT);
+    (void)cudaGetLastError();                            // report only this call's launch errors below
     k_reset_counters<<<1, 1, 0, st>>>(cnt, n);
     gate::launch_amps_on(seeds, n, s + OFF_OCT, cnt, reinterpret_cast<uint64_t *>(s + OFF_SEEDS), reinterpret_cast<uint32_t *>(s + OFF_IDX),
                          reinterpret_cast<float *>(s + OFF_AMP), pre, full, d.taps, d.pg_blocks, d.fg_blocks, st);

@@ -64,6 +64,7 @@ struct TableTaps { float k[2][2 * RMAX + 1]; };            // [0]: T tables, [1]
 // at constant offsets, plus the column parity's offset pxo.  (Tables with pxo folded in, one per parity,
 // measured 6% slower: alternate lanes then gather from two tables, and the banks conflict more.)
 constexpr int PL = 264;                                    // >= 256 + FCH / 2 + 2, multiple of 4
+static_assert(PL >= 256 + FCH / 2 + 2 && PL % 4 == 0, "PO must cover the largest offset a chunk reads");
 template <int D>
 __device__ __forceinline__ void tab_chunk(const uint8_t *__restrict__ PO, const char *__restrict__ tcb, const int (&cv)[4], int pxo, int me,
                                           int mo, float *__restrict__ rawc) {

@@ -56,7 +56,9 @@ int main() {
 
 
 def main():
-    ref = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
+    ref = sys.argv[1] if len(sys.argv) > 1 else os.environ.get("REF")
+    if not ref:
+        sys.exit("usage: extract_worldgen.py REFERENCE_CHECKOUT [OUT] (or REF=... in the environment)")
     out = sys.argv[2] if len(sys.argv) > 2 else os.path.join(os.path.dirname(os.path.abspath(__file__)), "worldgen.bin")
     with tempfile.TemporaryDirectory() as td:
         src = os.path.join(td, "dump.cpp")

@@ -5,8 +5,9 @@ For each candidate it compiles csrc/gate.cu with the shape given as -D overrides
 other objects of `make`'s build folder, and in a fresh process (one library per process) times the gate with
 dsg_gate_bench (CUDA events, 2^26 seed indices per step) and takes the side amplitudes of fixed seeds with
 dsg_gate_amps.  A candidate whose amplitudes are not bit-identical to the default build's is rejected.  The
-pre-gate and full-gate shapes are chosen independently (their kernel times are measured separately), and
-the winners are written as a gate_tuned.h.
+pre-gate and full-gate shapes are chosen independently (their kernel times are measured separately); when both
+winners differ from the default, their combination is built, checked and timed as well, and kept only if it is
+bit-identical and faster than the default.  The result is written as a gate_tuned.h.
 
     make && python desert-search_b200/tune_gate.py --out gate_tuned.h [--report tuning.txt]
 
@@ -94,6 +95,23 @@ def choose(rows):
     return best_pg, best_fg
 
 
+def confirm_combined(rows, best_pg, best_fg, measure_pair):
+    """The two winners were each measured with the other kernel at its default shape.  When both differ from
+    the default, the combined build is measured too (measure_pair(pg, fg) -> row) and kept only if its
+    amplitudes are bit-identical to the default's and it beats the default's total time by MIN_GAIN; else the
+    single change with the larger gain is kept.  Returns (best_pg, best_fg, combined row or None)."""
+    default = next(r for r in rows if r.get("bit_identical"))
+    if best_pg is default or best_fg is default:
+        return best_pg, best_fg, None
+    combo = measure_pair(best_pg["pregate_blocks_per_sm"], (best_fg["fullgate_blocks_per_sm"], best_fg["fullgate_rows"]))
+    ok = combo.get("bit_identical") and combo.get("total_ms", float("inf")) <= (1 - MIN_GAIN) * default["total_ms"]
+    if ok:
+        return best_pg, best_fg, combo
+    gain_pg = default["pregate_ms"] - best_pg["pregate_ms"]
+    gain_fg = default["fullgate_ms"] - best_fg["fullgate_ms"]
+    return (best_pg, default, combo) if gain_pg >= gain_fg else (default, best_fg, combo)
+
+
 def header_text(best_pg, best_fg):
     """gate_tuned.h for the chosen shapes."""
     out = ("// Launch shapes of the gate kernels, as chosen by desert-search_b200/tune_gate.py on a B200 (each candidate\n"
@@ -119,24 +137,29 @@ def main():
         return
     # the default, then one kernel's shape varied at a time (the two kernels are timed separately)
     pairs = [(PREGATE[0], FULLGATE[0])] + [(pg, FULLGATE[0]) for pg in PREGATE[1:]] + [(PREGATE[0], fg) for fg in FULLGATE[1:]]
-    rows, base = [], None
+    rows, base = [], []
     with tempfile.TemporaryDirectory() as tmp:
-        for i, (pg, fg) in enumerate(pairs):
+        def measure_pair(pg, fg):
             row = {"pregate_blocks_per_sm": pg, "fullgate_blocks_per_sm": fg[0], "fullgate_rows": fg[1]}
             try:
-                m = measure(build(tmp, f"c{i}", pg, fg), a.steps, a.warmup)
+                m = measure(build(tmp, f"c{len(rows)}", pg, fg), a.steps, a.warmup)
             except RuntimeError as ex:
-                if base is None:
+                if not base:
                     raise
                 row["failed"] = str(ex).strip().splitlines()[-1][:200]
-                rows.append(row); print(json.dumps(row), flush=True)
-                continue
-            if base is None:
-                base = m["amps"]
+                return row
+            if not base:
+                base.append(m["amps"])
             row.update({"pregate_ms": m["kernel_ms"][2], "fullgate_ms": m["kernel_ms"][3], "total_ms": m["ms"],
-                        "gated": m["counts"][3], "bit_identical": m["amps"] == base})
-            rows.append(row); print(json.dumps(row), flush=True)
-    best_pg, best_fg = choose(rows)
+                        "gated": m["counts"][3], "bit_identical": m["amps"] == base[0]})
+            return row
+        for pg, fg in pairs:
+            rows.append(measure_pair(pg, fg)); print(json.dumps(rows[-1]), flush=True)
+        best_pg, best_fg = choose(rows)
+        best_pg, best_fg, combo = confirm_combined(rows, best_pg, best_fg, measure_pair)
+        if combo is not None:
+            combo["combined"] = True
+            rows.append(combo); print(json.dumps(combo), flush=True)
     with open(a.out, "w") as f:
         f.write(header_text(best_pg, best_fg))
     if a.report:

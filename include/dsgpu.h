@@ -80,7 +80,8 @@ int dsg_gate_amps(const uint64_t *seeds, uint32_t n, float *pre, float *full);
  * enqueued on `stream` (a cudaStream_t, NULL = default stream) and the call returns without waiting.
  * Does not need dsg_init; uses the current device.  The first call on each device sets up the array
  * (address lookup, blur taps, one synchronous copy): make it before any stream capture.  All calls share
- * the array: calls whose work overlaps on the GPU race and must be serialised by the caller. */
+ * the array: calls whose work overlaps on the GPU race and must be serialised by the caller.  Resetting a
+ * device (cudaDeviceReset) after the first call on it is not supported: the set-up is not redone. */
 #define DSG_NOALLOC_MAX_SEEDS 4096
 int dsg_gate_amps_noalloc(const uint64_t *seeds, uint32_t n, float *pre, float *full, void *stream);
 

@@ -2,7 +2,9 @@
 # Test infrastructure only: the outputs pin the oracle and serve as the timed CPU reference arm.
 # Flags follow the reference Makefile (-ffp-contract=off is what makes its sampler round like Java);
 # -march=x86-64-v3 (its `bundle` target's host flags) instead of -march=native so the binaries run on
-# any AVX2 host the build is copied to.
+# any AVX2 host the build is copied to.  This recipe is the one place that knows where the reference checkout
+# lies by default; `make ref REF=...` (or REF in the environment) points it elsewhere.  Without a checkout
+# it builds nothing (the GPU machines use the binaries built here).
 REF      ?= /root/reference
 OUT      := oracle/_ref
 CXXFLAGS := -O3 -march=x86-64-v3 -ffp-contract=off -std=c++20 -pthread -I$(REF)/src
@@ -11,6 +13,10 @@ GPUARCH  := -gencode arch=compute_100a,code=sm_100a
 
 REFHDR := $(wildcard $(REF)/src/*.hpp) $(REF)/src/dsearch_desert.cpp
 
+ifeq ($(wildcard $(REF)/src/dsearch_desert.cpp),)
+all:
+	@echo "oracle/ref.mk: no reference checkout at REF=$(REF); oracle/_ref not rebuilt"
+else
 all: $(OUT)/dsearch_desert $(OUT)/dflood $(OUT)/libref_cpu.so $(OUT)/libref_gate.so $(OUT)/tgate $(OUT)/dsearch_desert_gpu
 
 $(OUT):
@@ -34,3 +40,4 @@ $(OUT)/gproxy.o: $(REF)/src/gpu/gproxy.cu $(REF)/src/gpu/gate.cuh $(REF)/src/gpu
 	$(NVCC) -O3 -std=c++20 $(GPUARCH) -c $< -o $@
 $(OUT)/dsearch_desert_gpu: $(REF)/src/dsearch_desert.cpp $(REFHDR) $(OUT)/gproxy.o | $(OUT)
 	g++ $(CXXFLAGS) -DDRIP_GPU -I/usr/local/cuda/include $< $(OUT)/gproxy.o -L/usr/local/cuda/lib64 -lcudart_static -ldl -lrt -o $@
+endif

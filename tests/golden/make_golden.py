@@ -11,7 +11,7 @@ Runs where the reference checkout is present and oracle/_ref has been built (`ma
   ref_tables.npz    tab_setup inputs, translation maps, blur taps, and a checksum of the six blurred tables
   ref_cli.json      the reference CLI's per-seed scan summary (maxta, maxtb, NMS buckets, sites) for
                     gated seeds fed through stdin=1, with the hot-zone stage switched off (hot_min=1e9)
-Usage: python tests/golden/make_golden.py [REFERENCE_ROOT]
+Usage: python tests/golden/make_golden.py REFERENCE_ROOT   (or REF=REFERENCE_ROOT in the environment)
 """
 import hashlib
 import json
@@ -31,7 +31,9 @@ M64 = (1 << 64) - 1
 
 
 def main():
-    refroot = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
+    refroot = sys.argv[1] if len(sys.argv) > 1 else os.environ.get("REF")
+    if not refroot:
+        sys.exit("usage: make_golden.py REFERENCE_CHECKOUT (or REF=... in the environment)")
     r = libs.ref()
     assert r is not None, "build oracle/_ref first (make ref)"
     rows = [json.loads(l) for l in open(os.path.join(refroot, "results", "desert_finds.jsonl"))]

@@ -51,3 +51,41 @@ def test_default_choice_writes_the_committed_header():
     pg, fg = tg.choose(rows(100.0, 50.0))
     with open(os.path.join(PKG, "csrc", "gate_tuned.h")) as f:
         assert tg.header_text(pg, fg) == f.read()
+
+
+def _combo_rows():
+    r = rows(97.0, 48.0)
+    for x in r:
+        x["total_ms"] = x["pregate_ms"] + x["fullgate_ms"]
+    return r
+
+
+def test_combined_shape_measured_and_kept_when_identical_and_faster():
+    r = _combo_rows()
+    pg, fg = tg.choose(r)
+    seen = []
+
+    def measure_pair(p, f):
+        seen.append((p, f))
+        return row(p, f, 97.0, 48.0) | {"total_ms": 145.0}
+    pg2, fg2, combo = tg.confirm_combined(r, pg, fg, measure_pair)
+    assert seen == [(tg.PREGATE[1], tg.FULLGATE[1])]
+    assert (pg2, fg2) == (pg, fg) and combo["total_ms"] == 145.0
+
+
+def test_combined_shape_rejected_keeps_the_larger_single_gain():
+    r = _combo_rows()
+    pg, fg = tg.choose(r)
+    for bad in (row(0, (0, 0), 97.0, 48.0, same=False) | {"total_ms": 100.0}, row(0, (0, 0), 99.0, 52.0) | {"total_ms": 151.0},
+                {"failed": "ptxas error"}):
+        pg2, fg2, _ = tg.confirm_combined(r, pg, fg, lambda p, f, b=bad: b)
+        # the pre-gate change saves 3 ms, the full-gate change 2 ms: the pre-gate one alone is kept
+        assert pg2["pregate_blocks_per_sm"] == tg.PREGATE[1]
+        assert (fg2["fullgate_blocks_per_sm"], fg2["fullgate_rows"]) == tg.FULLGATE[0]
+
+
+def test_no_combined_measurement_when_one_winner_is_the_default():
+    r = rows(97.0, 50.0)
+    pg, fg = tg.choose(r)
+    _, _, combo = tg.confirm_combined(r, pg, fg, lambda p, f: (_ for _ in ()).throw(AssertionError("measured")))
+    assert combo is None
