@@ -59,7 +59,7 @@ struct Tiles { uint64_t *bits; uint32_t *owner, *pos, *emask, *qmask, *mark; };
 // Queues of one round: n (sub-blocks to evaluate, entries tile * 16 + sub-block), w (tiles to connect);
 // *_next are the next round's.
 struct Round {
-    uint32_t round;
+    uint32_t round;                    // this round's number, plus *round_base when round_base is set
     const uint32_t *n_list; const uint32_t *n_cnt;
     uint32_t *w_list; uint32_t *w_cnt;
     uint32_t *n_next; uint32_t *n_next_cnt;
@@ -69,7 +69,9 @@ struct Round {
     uint32_t *active;                  // per request: the last round it has queued work for (service)
     uint32_t *err;                     // bit 0: tile pool exhausted
     unsigned long long *evaluated;     // sub-blocks evaluated (statistics)
+    const uint32_t *round_base;        // device-side round offset (rounds launched from a device-driven loop), or null
 };
+__device__ __forceinline__ uint32_t round_of(const Round &q) { return q.round + (q.round_base ? *q.round_base : 0u); }
 
 // Predicate value of request c at quart (x, z): 2 counted, 1 crossed (bridged river), 0 boundary; -1 with `p`
 // filled when a desert point needs desert_state_finish.
@@ -145,6 +147,7 @@ static __global__ void __launch_bounds__(EVAL_THREADS) k_tile_eval(const FloodCt
     __shared__ int s_n;
     __shared__ uint32_t s_run;
     const uint32_t items = *q.n_cnt;
+    const uint32_t round = round_of(q);
     const uint32_t run = max(1u, min(16u, items / (4 * gridDim.x)));
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     int staged = -1;                                      // every thread walks the same items: no shared copy needed
@@ -192,7 +195,7 @@ static __global__ void __launch_bounds__(EVAL_THREADS) k_tile_eval(const FloodCt
             // the rows are read by the next launch (connect), so the mark needs no barrier after the stores
             if (threadIdx.x == 0) {
                 atomicOr(&T.emask[t], 1u << sb);
-                if (atomicExch(&T.mark[t], q.round + 1) != q.round + 1) q.w_list[atomicAdd(q.w_cnt, 1u)] = t;
+                if (atomicExch(&T.mark[t], round + 1) != round + 1) q.w_list[atomicAdd(q.w_cnt, 1u)] = t;
                 atomicAdd(q.evaluated, 1ull);
             }
         }
@@ -337,6 +340,7 @@ static __global__ void __launch_bounds__(256) k_tile_connect(const FloodCtl *__r
                                                              TileAlloc ta, FloodStat *__restrict__ st, Round q) {
     if (blockIdx.x == 0 && threadIdx.x == 0) { *q.zero_a = 0; *q.zero_b = 0; *q.zero_c = 0; }
     const uint32_t n = *q.w_cnt;
+    const uint32_t round = round_of(q);
     const int lane = threadIdx.x & 31;
     const uint32_t nw = gridDim.x * (blockDim.x >> 5);
     for (uint32_t idx = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5); idx < n; idx += nw) {
@@ -397,15 +401,15 @@ static __global__ void __launch_bounds__(256) k_tile_connect(const FloodCtl *__r
             const int reached = __reduce_add_sync(0xffffffffu, __popcll(ra) + __popcll(rb));
             if (reached >= kEagerCells) mask = lane == 8 ? (0xffffu & ~em) : (mask ? 0xffffu : 0u);
         }
-        if (lane == 8) request_blocks(T, int32_t(t), mask, r, q.n_next, q.n_next_cnt, q.round + 1, q.active);
+        if (lane == 8) request_blocks(T, int32_t(t), mask, r, q.n_next, q.n_next_cnt, round + 1, q.active);
         const int nti = ti + dti, ntj = tj + dtj;
         if (lane < 8 && mask && nti >= 0 && ntj >= 0 && nti < c.tpr && ntj < c.tpr) {
             const int32_t d = claim_tile(c, r, nti, ntj, dir, T, ta, st, q.err);
-            request_blocks(T, d, mask, r, q.n_next, q.n_next_cnt, q.round + 1, q.active);
+            request_blocks(T, d, mask, r, q.n_next, q.n_next_cnt, round + 1, q.active);
             if (d >= 0 && changed && (__ldcg(&T.emask[d]) & mask)) {      // evaluated cells next to new R: reconnect
-                if (atomicExch(&T.mark[d], q.round + 2) != q.round + 2) {
+                if (atomicExch(&T.mark[d], round + 2) != round + 2) {
                     q.w_next[atomicAdd(q.w_next_cnt, 1u)] = uint32_t(d);
-                    if (q.active) q.active[r] = q.round + 1;
+                    if (q.active) q.active[r] = round + 1;
                 }
             }
         }
@@ -478,7 +482,9 @@ inline unsigned dir_chunks(int64_t max_entries) { return unsigned((max_entries +
 // Finished requests (slots, or 0..gridDim.x-1; blockIdx.y = directory chunk): statistics of every tile.
 // Releasing the tiles is a separate launch (k_tile_release), since the statistics read neighbouring tiles.
 static __global__ void __launch_bounds__(256) k_tile_finish(const FloodCtl *__restrict__ ctl, const uint32_t *__restrict__ slots,
-                                                            const int32_t *__restrict__ dir, Tiles T, FloodStat *__restrict__ st) {
+                                                            const int32_t *__restrict__ dir, Tiles T, FloodStat *__restrict__ st,
+                                                            const uint32_t *__restrict__ n_dev = nullptr) {
+    if (n_dev && blockIdx.x >= *n_dev) return;           // requests counted on the device (grid sized for the capacity)
     const uint32_t r = slots ? slots[blockIdx.x] : blockIdx.x;
     const FloodCtl c = ctl[r];
     const int lane = threadIdx.x & 31;
@@ -607,12 +613,15 @@ struct TilePool {
 };
 // Launch one round: evaluate the sub-blocks requested last round, then connect.  cnt[0..2] are the rotating
 // evaluation-queue counters, cnt[3..5] the connect-queue ones, cnt[6..8] the evaluation work counters.
+// round_base (may be null): a device counter added to `round` (a multiple of 6, so the queues and counters
+// chosen by round & 1 and round % 3 are those of round + *round_base).
 inline void launch_round(const TilePool &p, uint32_t round, uint32_t *cnt, uint32_t *active, uint32_t *err, unsigned long long *evaluated,
                          const FloodCtl *ctl, const SeedNoise *noise, int32_t *dir, FloodStat *st, const TileAlloc &ta, int grid_eval,
-                         int grid_conn, cudaStream_t s) {
+                         int grid_conn, cudaStream_t s, const uint32_t *round_base = nullptr) {
     const Round q{round, p.n_list[round & 1], cnt + round % 3, p.w_list[round & 1], cnt + 3 + round % 3,
                   p.n_list[(round + 1) & 1], cnt + (round + 1) % 3, p.w_list[(round + 1) & 1], cnt + 3 + (round + 1) % 3,
-                  cnt + 6 + round % 3, cnt + (round + 2) % 3, cnt + 3 + (round + 2) % 3, cnt + 6 + (round + 2) % 3, active, err, evaluated};
+                  cnt + 6 + round % 3, cnt + (round + 2) % 3, cnt + 3 + (round + 2) % 3, cnt + 6 + (round + 2) % 3, active, err, evaluated,
+                  round_base};
     k_tile_eval<<<grid_eval, EVAL_THREADS, 0, s>>>(ctl, noise, world_dev(), p.T, q);
     k_tile_connect<<<grid_conn, 256, 0, s>>>(ctl, dir, p.T, ta, st, q);
 }

@@ -676,6 +676,20 @@ void enqueue_batch(State &g, cudaStream_t st, uint64_t start, uint64_t nb, const
     k_fullgate<<<g.fg_blocks, FG_THREADS, 0, st>>>(g.d_oct, g.d_s2, g.d_idx2, g.d_n + 1, g.cap2, c.amp, g.taps, g.d_s3, g.d_a3, g.d_n + 2, g.cap3, nullptr);
     DSG_CU(cudaGetLastError());
 }
+// A gate with buffers of its own, for the device-resident searcher: batches of up to `batch` indices enqueued
+// on the caller's stream.  survivors / counts point at its full-gate list and its counters {phase-passed,
+// pre-gate passed, full-gate passed} (counts above the list capacities mean an overflow).
+struct Lane { State g; };
+Lane *lane_create(uint64_t batch) {
+    Lane *l = new Lane;
+    setup_locked(l->g);
+    ensure_buffers(l->g, batch);
+    return l;
+}
+void lane_enqueue(Lane *l, cudaStream_t st, uint64_t start, uint64_t nb, const dsg_gate_cfg &c) { enqueue_batch(l->g, st, start, nb, c); }
+const uint64_t *lane_survivors(const Lane *l) { return l->g.d_s3; }
+uint32_t *lane_counts(Lane *l) { return l->g.d_n; }
+void lane_caps(const Lane *l, uint32_t caps[3]) { caps[0] = l->g.cap1; caps[1] = l->g.cap2; caps[2] = l->g.cap3; }
 }  // namespace gate
 }  // namespace dsg
 

@@ -21,7 +21,9 @@ __constant__ uint64_t c_salt[11][2] = {
     {0xbd90d5377ba1b762ULL, 0xc07317d419a7548dULL}, {0x53d39c6752dac858ULL, 0xbcd1c5a80ab65b3eULL},
     {0xb4a24d7a84e7677bULL, 0x023ff9668e89b5c4ULL}, {0xdffa22b534c5f608ULL, 0xb9b67517d3665ca9ULL},
     {0xd50708086cef4d7cULL, 0x6e1651ecc7f43309ULL}};
-__global__ void __launch_bounds__(64) k_seed_noise(const uint64_t *__restrict__ seeds, uint32_t n, SeedNoise *__restrict__ out) {
+__global__ void __launch_bounds__(64) k_seed_noise(const uint64_t *__restrict__ seeds, uint32_t n, SeedNoise *__restrict__ out,
+                                                   const uint32_t *__restrict__ n_dev) {
+    if (n_dev) n = min(n, *n_dev);
     // nonzero octave counts per channel (T 2, H 2, C 9, E 4, shift 3, W 3) and their offsets in SeedNoise
     constexpr int kCnt[6] = {2, 2, 9, 4, 3, 3};
     constexpr int kOff[6] = {0, 4, 8, 26, 34, 40};
@@ -71,7 +73,13 @@ __global__ void __launch_bounds__(64) k_seed_noise(const uint64_t *__restrict__ 
 
 void seed_noise_build(const uint64_t *d_seeds, uint32_t n, SeedNoise *d_out, cudaStream_t st) {
     if (!n) return;
-    k_seed_noise<<<n, 64, 0, st>>>(d_seeds, n, d_out);
+    k_seed_noise<<<n, 64, 0, st>>>(d_seeds, n, d_out, nullptr);
+    DSG_CU(cudaGetLastError());
+}
+// The same for seeds counted on the device: blocks for seeds at or beyond *n_dev (at most cap) return at once.
+void seed_noise_build_dev(const uint64_t *d_seeds, const uint32_t *n_dev, uint32_t cap, SeedNoise *d_out, cudaStream_t st) {
+    if (!cap) return;
+    k_seed_noise<<<cap, 64, 0, st>>>(d_seeds, cap, d_out, n_dev);
     DSG_CU(cudaGetLastError());
 }
 }  // namespace dsg

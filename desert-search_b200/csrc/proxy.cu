@@ -8,6 +8,7 @@
 // 40 x 40 probability table, passable iff prob >= cut.  One thread per step-32 cell; a zone's cells
 // spread over many blocks so that a single large zone fills the GPU (gproxy.cu:91-93).
 #include "noise.cuh"
+#include "zones.cuh"
 #include <algorithm>
 #include <map>
 #include <mutex>
@@ -16,25 +17,46 @@
 namespace dsg {
 namespace {
 float g_cut = 0.35f;
-struct DZone { int32_t x0, z0, nx, nz; int64_t off; int32_t seed, pad; };
-constexpr int CHUNK = 2048;
-// Statistics of one 8-connected component of a zone bitmap.  sx, sz: sums of the cells' columns and rows
-// (exact integers); kid: index among the kept components or -1; seg, cur: its interior-key segment.
-struct CompStat { uint32_t zone, first, cells, inner; int32_t minx, minz, kid; uint32_t seg, cur, pad; uint64_t sx, sz; };
+using zones::DZone;
+using zones::CHUNK;
+using zones::ZoneWork;
+using zones::CompStat;
+// The chunks of CHUNK cells a block handles: (zone blockIdx.x, chunk blockIdx.y) when the host knows the zones
+// (w.chunk == null), else chunks w.chunk[k] for k = blockIdx.x, blockIdx.x + gridDim.x, ... < *w.nchunk (zones and
+// their cell offsets built on the device).  f(zone index, zone, first cell, end cell) runs for each.
+template <class F> __device__ __forceinline__ void each_chunk(const DZone *__restrict__ zones, const ZoneWork &w, F &&f) {
+    if (!w.chunk) {
+        const DZone z = zones[blockIdx.x];
+        const int64_t n = int64_t(z.nx) * z.nz, c0 = int64_t(blockIdx.y) * CHUNK;
+        if (c0 < n) f(blockIdx.x, z, c0, min(n, c0 + CHUNK));
+        return;
+    }
+    const uint32_t nch = *w.nchunk;
+    for (uint32_t k = blockIdx.x; k < nch; k += gridDim.x) {
+        const uint2 zc = w.chunk[k];
+        const DZone z = zones[zc.x];
+        const int64_t n = int64_t(z.nx) * z.nz, c0 = int64_t(zc.y) * CHUNK;
+        f(zc.x, z, c0, min(n, c0 + CHUNK));
+    }
+}
 
 __global__ void __launch_bounds__(256) k_proxy(const SeedNoise *__restrict__ noise, const DZone *__restrict__ zones, WorldDev w, float cut,
-                                               uint8_t *__restrict__ out) {
+                                               uint8_t *__restrict__ out, ZoneWork wk) {
     __shared__ SeedNoise S;                               // the zone's seed: every Perlin lookup from shared memory
-    const DZone z = zones[blockIdx.x];
-    const int64_t n = int64_t(z.nx) * z.nz, c0 = int64_t(blockIdx.y) * CHUNK, c1 = min(n, c0 + CHUNK);
-    if (c0 >= n) return;
-    const uint4 *src = reinterpret_cast<const uint4 *>(noise + z.seed);
-    for (int k = threadIdx.x; k < int(sizeof(SeedNoise) / 16); k += blockDim.x) reinterpret_cast<uint4 *>(&S)[k] = __ldg(src + k);
-    __syncthreads();
-    for (int64_t c = c0 + threadIdx.x; c < c1; c += blockDim.x) {
-        const int ci = int(c % z.nx), cj = int(c / z.nx);
-        out[z.off + c] = proxy_prob(S, w, z.x0 + 32 * ci, z.z0 + 32 * cj) >= cut;
-    }
+    int staged = -1;
+    each_chunk(zones, wk, [&](uint32_t, const DZone &z, int64_t c0, int64_t c1) {
+        if (z.seed != staged) {                           // block-uniform: every thread walks the same chunks
+            __syncthreads();
+            const uint4 *src = reinterpret_cast<const uint4 *>(noise + z.seed);
+            for (int k = threadIdx.x; k < int(sizeof(SeedNoise) / 16); k += blockDim.x) reinterpret_cast<uint4 *>(&S)[k] = __ldg(src + k);
+            __syncthreads();
+            staged = z.seed;
+        }
+        for (int64_t c = c0 + threadIdx.x; c < c1; c += blockDim.x) {
+            const int ci = int(c % z.nx), cj = int(c / z.nx);
+            out[z.off + c] = proxy_prob(S, w, z.x0 + 32 * ci, z.z0 + 32 * cj) >= cut;
+        }
+    });
 }
 
 // ---- component labelling of the bitmaps (the 8-connected components, centroids and interior starts of
@@ -78,68 +100,69 @@ __device__ __forceinline__ bool interior(const uint8_t *b, const DZone &z, int x
         for (int dx = -1; dx <= 1; dx++) if (!b[int64_t(y + dy) * z.nx + x + dx]) return false;
     return true;
 }
-__global__ void __launch_bounds__(256) k_cc_init(const DZone *__restrict__ zones, const uint8_t *__restrict__ bits, int32_t *__restrict__ par) {
-    const DZone z = zones[blockIdx.x];
-    const int64_t n = int64_t(z.nx) * z.nz, c0 = int64_t(blockIdx.y) * CHUNK, c1 = min(n, c0 + CHUNK);
-    for (int64_t c = c0 + threadIdx.x; c < c1; c += blockDim.x) par[z.off + c] = bits[z.off + c] ? int32_t(c) : -1;
+__global__ void __launch_bounds__(256) k_cc_init(const DZone *__restrict__ zones, const uint8_t *__restrict__ bits, int32_t *__restrict__ par,
+                                                 ZoneWork wk) {
+    each_chunk(zones, wk, [&](uint32_t, const DZone &z, int64_t c0, int64_t c1) {
+        for (int64_t c = c0 + threadIdx.x; c < c1; c += blockDim.x) par[z.off + c] = bits[z.off + c] ? int32_t(c) : -1;
+    });
 }
 __global__ void __launch_bounds__(256) k_cc_merge(const DZone *__restrict__ zones, const uint8_t *__restrict__ bits, int32_t *__restrict__ par,
-                                                  uint32_t *err) {
-    const DZone z = zones[blockIdx.x];
-    const int64_t n = int64_t(z.nx) * z.nz, c0 = int64_t(blockIdx.y) * CHUNK, c1 = min(n, c0 + CHUNK);
-    const uint8_t *b = bits + z.off;
-    int32_t *p = par + z.off;
-    for (int64_t c = c0 + threadIdx.x; c < c1; c += blockDim.x) {
-        if (!b[c]) continue;
-        const int x = int(c % z.nx), y = int(c / z.nx);
-        // the four neighbours that come earlier in raster order cover every 8-connected pair once
-        if (zone_bit(b, z, x - 1, y)) uf_union(p, int32_t(c), int32_t(c - 1), err);
-        if (zone_bit(b, z, x - 1, y - 1)) uf_union(p, int32_t(c), int32_t(c - z.nx - 1), err);
-        if (zone_bit(b, z, x, y - 1)) uf_union(p, int32_t(c), int32_t(c - z.nx), err);
-        if (zone_bit(b, z, x + 1, y - 1)) uf_union(p, int32_t(c), int32_t(c - z.nx + 1), err);
-    }
+                                                  uint32_t *err, ZoneWork wk) {
+    each_chunk(zones, wk, [&](uint32_t, const DZone &z, int64_t c0, int64_t c1) {
+        const uint8_t *b = bits + z.off;
+        int32_t *p = par + z.off;
+        for (int64_t c = c0 + threadIdx.x; c < c1; c += blockDim.x) {
+            if (!b[c]) continue;
+            const int x = int(c % z.nx), y = int(c / z.nx);
+            // the four neighbours that come earlier in raster order cover every 8-connected pair once
+            if (zone_bit(b, z, x - 1, y)) uf_union(p, int32_t(c), int32_t(c - 1), err);
+            if (zone_bit(b, z, x - 1, y - 1)) uf_union(p, int32_t(c), int32_t(c - z.nx - 1), err);
+            if (zone_bit(b, z, x, y - 1)) uf_union(p, int32_t(c), int32_t(c - z.nx), err);
+            if (zone_bit(b, z, x + 1, y - 1)) uf_union(p, int32_t(c), int32_t(c - z.nx + 1), err);
+        }
+    });
 }
 // Roots get a component id; every cell's parent becomes its root.
 __global__ void __launch_bounds__(256) k_cc_roots(const DZone *__restrict__ zones, int32_t *__restrict__ par, int32_t *__restrict__ rid,
-                                                  CompStat *__restrict__ cs, uint32_t *ctr) {
-    const DZone z = zones[blockIdx.x];
-    const int64_t n = int64_t(z.nx) * z.nz, c0 = int64_t(blockIdx.y) * CHUNK, c1 = min(n, c0 + CHUNK);
-    int32_t *p = par + z.off;
-    for (int64_t c = c0 + threadIdx.x; c < c1; c += blockDim.x) {
-        if (p[c] < 0) continue;
-        const int32_t r = uf_find(p, int32_t(c), ctr + 3);
-        if (r == int32_t(c)) {
-            const uint32_t id = atomicAdd(ctr, 1u);
-            rid[z.off + c] = int32_t(id);
-            CompStat &q = cs[id];
-            q.zone = blockIdx.x; q.first = uint32_t(c); q.cells = 0; q.inner = 0; q.minx = q.minz = 0x7fffffff; q.kid = -1;
-            q.seg = 0; q.cur = 0; q.sx = 0; q.sz = 0;
+                                                  CompStat *__restrict__ cs, uint32_t *ctr, ZoneWork wk) {
+    each_chunk(zones, wk, [&](uint32_t zi, const DZone &z, int64_t c0, int64_t c1) {
+        int32_t *p = par + z.off;
+        for (int64_t c = c0 + threadIdx.x; c < c1; c += blockDim.x) {
+            if (p[c] < 0) continue;
+            const int32_t r = uf_find(p, int32_t(c), ctr + 3);
+            if (r == int32_t(c)) {
+                const uint32_t id = atomicAdd(ctr, 1u);
+                rid[z.off + c] = int32_t(id);
+                CompStat &q = cs[id];
+                q.zone = zi; q.first = uint32_t(c); q.cells = 0; q.inner = 0; q.minx = q.minz = 0x7fffffff; q.kid = -1;
+                q.seg = 0; q.cur = 0; q.sx = 0; q.sz = 0;
+            }
         }
-    }
+    });
 }
-__global__ void __launch_bounds__(256) k_cc_flatten(const DZone *__restrict__ zones, int32_t *__restrict__ par, uint32_t *err) {
-    const DZone z = zones[blockIdx.x];
-    const int64_t n = int64_t(z.nx) * z.nz, c0 = int64_t(blockIdx.y) * CHUNK, c1 = min(n, c0 + CHUNK);
-    int32_t *p = par + z.off;
-    for (int64_t c = c0 + threadIdx.x; c < c1; c += blockDim.x)
-        if (p[c] >= 0) p[c] = uf_find(p, int32_t(c), err);
+__global__ void __launch_bounds__(256) k_cc_flatten(const DZone *__restrict__ zones, int32_t *__restrict__ par, uint32_t *err, ZoneWork wk) {
+    each_chunk(zones, wk, [&](uint32_t, const DZone &z, int64_t c0, int64_t c1) {
+        int32_t *p = par + z.off;
+        for (int64_t c = c0 + threadIdx.x; c < c1; c += blockDim.x)
+            if (p[c] >= 0) p[c] = uf_find(p, int32_t(c), err);
+    });
 }
 __global__ void __launch_bounds__(256) k_cc_stats(const DZone *__restrict__ zones, const uint8_t *__restrict__ bits, const int32_t *__restrict__ par,
-                                                  const int32_t *__restrict__ rid, CompStat *__restrict__ cs) {
-    const DZone z = zones[blockIdx.x];
-    const int64_t n = int64_t(z.nx) * z.nz, c0 = int64_t(blockIdx.y) * CHUNK, c1 = min(n, c0 + CHUNK);
-    const uint8_t *b = bits + z.off;
-    for (int64_t c = c0 + threadIdx.x; c < c1; c += blockDim.x) {
-        const int32_t r = par[z.off + c];
-        if (r < 0) continue;
-        CompStat &q = cs[rid[z.off + r]];
-        const int x = int(c % z.nx), y = int(c / z.nx);
-        atomicAdd(&q.cells, 1u);
-        atomicMin(&q.minx, x); atomicMin(&q.minz, y);
-        atomicAdd(reinterpret_cast<unsigned long long *>(&q.sx), (unsigned long long)x);
-        atomicAdd(reinterpret_cast<unsigned long long *>(&q.sz), (unsigned long long)y);
-        if (interior(b, z, x, y)) atomicAdd(&q.inner, 1u);
-    }
+                                                  const int32_t *__restrict__ rid, CompStat *__restrict__ cs, ZoneWork wk) {
+    each_chunk(zones, wk, [&](uint32_t, const DZone &z, int64_t c0, int64_t c1) {
+        const uint8_t *b = bits + z.off;
+        for (int64_t c = c0 + threadIdx.x; c < c1; c += blockDim.x) {
+            const int32_t r = par[z.off + c];
+            if (r < 0) continue;
+            CompStat &q = cs[rid[z.off + r]];
+            const int x = int(c % z.nx), y = int(c / z.nx);
+            atomicAdd(&q.cells, 1u);
+            atomicMin(&q.minx, x); atomicMin(&q.minz, y);
+            atomicAdd(reinterpret_cast<unsigned long long *>(&q.sx), (unsigned long long)x);
+            atomicAdd(reinterpret_cast<unsigned long long *>(&q.sz), (unsigned long long)y);
+            if (interior(b, z, x, y)) atomicAdd(&q.inner, 1u);
+        }
+    });
 }
 // Components of at least min_cells cells are kept; each gets a segment for its interior keys.
 __global__ void k_cc_keep(CompStat *__restrict__ cs, uint32_t min_cells, uint32_t *ctr) {
@@ -155,23 +178,23 @@ __global__ void k_cc_keep(CompStat *__restrict__ cs, uint32_t min_cells, uint32_
 // order of the reference's sorted `inner` list; the arithmetic is the host's, operation by operation.
 __global__ void __launch_bounds__(256) k_cc_keys(const DZone *__restrict__ zones, const uint8_t *__restrict__ bits, const int32_t *__restrict__ par,
                                                  const int32_t *__restrict__ rid, CompStat *__restrict__ cs, uint64_t *__restrict__ khi,
-                                                 uint32_t *__restrict__ klo) {
-    const DZone z = zones[blockIdx.x];
-    const int64_t n = int64_t(z.nx) * z.nz, c0 = int64_t(blockIdx.y) * CHUNK, c1 = min(n, c0 + CHUNK);
-    const uint8_t *b = bits + z.off;
-    for (int64_t c = c0 + threadIdx.x; c < c1; c += blockDim.x) {
-        const int32_t r = par[z.off + c];
-        if (r < 0) continue;
-        CompStat &q = cs[rid[z.off + r]];
-        if (q.kid < 0) continue;
-        const int x = int(c % z.nx), y = int(c / z.nx);
-        if (!interior(b, z, x, y)) continue;
-        const double cx = double(q.sx) / double(q.cells), cz = double(q.sz) / double(q.cells);
-        const double d = __dadd_rn(__dmul_rn(x - cx, x - cx), __dmul_rn(y - cz, y - cz));
-        const uint32_t at = q.seg + atomicAdd(&q.cur, 1u);
-        khi[at] = uint64_t(__double_as_longlong(d));       // d >= 0: the bit pattern orders like the value
-        klo[at] = uint32_t(c);
-    }
+                                                 uint32_t *__restrict__ klo, ZoneWork wk) {
+    each_chunk(zones, wk, [&](uint32_t, const DZone &z, int64_t c0, int64_t c1) {
+        const uint8_t *b = bits + z.off;
+        for (int64_t c = c0 + threadIdx.x; c < c1; c += blockDim.x) {
+            const int32_t r = par[z.off + c];
+            if (r < 0) continue;
+            CompStat &q = cs[rid[z.off + r]];
+            if (q.kid < 0) continue;
+            const int x = int(c % z.nx), y = int(c / z.nx);
+            if (!interior(b, z, x, y)) continue;
+            const double cx = double(q.sx) / double(q.cells), cz = double(q.sz) / double(q.cells);
+            const double d = __dadd_rn(__dmul_rn(x - cx, x - cx), __dmul_rn(y - cz, y - cz));
+            const uint32_t at = q.seg + atomicAdd(&q.cur, 1u);
+            khi[at] = uint64_t(__double_as_longlong(d));       // d >= 0: the bit pattern orders like the value
+            klo[at] = uint32_t(c);
+        }
+    });
 }
 // One block per kept component: the interior keys at ranks 0, n/3 and 2n/3, by an exact radix selection
 // over the 12 bytes of the key (all three ranks in each pass).
@@ -230,6 +253,22 @@ __global__ void __launch_bounds__(256) k_cc_select(const CompStat *__restrict__ 
     }
 }
 
+// Component labelling of bitmaps already in `bits` (k_proxy's output): union-find, statistics, kept components
+// (at least min_cells cells), interior keys and the three interior starts of each kept component into rec[kid].
+// ctr = {components, kept, interior keys, error}, zeroed by the caller.
+void label_components(const DZone *zones, dim3 grid, const ZoneWork &wk, const uint8_t *bits, int32_t *par, int32_t *rid, CompStat *cs,
+                      uint64_t *khi, uint32_t *klo, dsg_component *rec, uint32_t *ctr, uint32_t min_cells, unsigned keep_blocks,
+                      unsigned select_blocks, cudaStream_t st) {
+    k_cc_init<<<grid, 256, 0, st>>>(zones, bits, par, wk);
+    k_cc_merge<<<grid, 256, 0, st>>>(zones, bits, par, ctr + 3, wk);
+    k_cc_roots<<<grid, 256, 0, st>>>(zones, par, rid, cs, ctr, wk);
+    k_cc_flatten<<<grid, 256, 0, st>>>(zones, par, ctr + 3, wk);
+    k_cc_stats<<<grid, 256, 0, st>>>(zones, bits, par, rid, cs, wk);
+    k_cc_keep<<<(keep_blocks + 255) / 256, 256, 0, st>>>(cs, min_cells, ctr);
+    k_cc_keys<<<grid, 256, 0, st>>>(zones, bits, par, rid, cs, khi, klo, wk);
+    k_cc_select<<<select_blocks, 256, 0, st>>>(cs, khi, klo, ctr, rec);
+}
+
 struct State {
     std::mutex mu;
     cudaStream_t st = nullptr;
@@ -284,7 +323,7 @@ int proxy_eval(const uint64_t *seeds, uint32_t nseeds, const uint32_t *zone_seed
     DSG_CU(cudaMemcpyAsync(g.d_seeds, seeds, size_t(nseeds) * 8, cudaMemcpyHostToDevice, g.st));
     seed_noise_build(g.d_seeds, nseeds, g.d_noise, g.st);
     DSG_CU(cudaMemcpyAsync(g.d_zones, dz.data(), dz.size() * sizeof(DZone), cudaMemcpyHostToDevice, g.st));
-    k_proxy<<<dim3(nzones, unsigned((maxc + CHUNK - 1) / CHUNK)), 256, 0, g.st>>>(g.d_noise, g.d_zones, world_dev(), g_cut, g.d_out);
+    k_proxy<<<dim3(nzones, unsigned((maxc + CHUNK - 1) / CHUNK)), 256, 0, g.st>>>(g.d_noise, g.d_zones, world_dev(), g_cut, g.d_out, ZoneWork{});
     DSG_CU(cudaGetLastError());
     DSG_CU(cudaMemcpyAsync(bits, g.d_out, size_t(off), cudaMemcpyDeviceToHost, g.st));
     DSG_CU(cudaStreamSynchronize(g.st));
@@ -336,15 +375,9 @@ int proxy_components(const uint64_t *seeds, uint32_t nseeds, const uint32_t *zon
     DSG_CU(cudaMemcpyAsync(g.d_zones, dz.data(), dz.size() * sizeof(DZone), cudaMemcpyHostToDevice, st));
     DSG_CU(cudaMemsetAsync(g.d_ctr, 0, 4 * 4, st));
     const dim3 grid(nzones, unsigned((maxc + CHUNK - 1) / CHUNK));
-    k_proxy<<<grid, 256, 0, st>>>(g.d_noise, g.d_zones, world_dev(), g_cut, g.d_out);
-    k_cc_init<<<grid, 256, 0, st>>>(g.d_zones, g.d_out, g.d_par);
-    k_cc_merge<<<grid, 256, 0, st>>>(g.d_zones, g.d_out, g.d_par, g.d_ctr + 3);
-    k_cc_roots<<<grid, 256, 0, st>>>(g.d_zones, g.d_par, g.d_rid, g.d_cs, g.d_ctr);
-    k_cc_flatten<<<grid, 256, 0, st>>>(g.d_zones, g.d_par, g.d_ctr + 3);
-    k_cc_stats<<<grid, 256, 0, st>>>(g.d_zones, g.d_out, g.d_par, g.d_rid, g.d_cs);
-    k_cc_keep<<<(std::min<int64_t>(off, 1 << 20) + 255) / 256, 256, 0, st>>>(g.d_cs, min_cells, g.d_ctr);
-    k_cc_keys<<<grid, 256, 0, st>>>(g.d_zones, g.d_out, g.d_par, g.d_rid, g.d_cs, g.d_khi, g.d_klo);
-    k_cc_select<<<unsigned(std::min<int64_t>(off, 4 * 148)), 256, 0, st>>>(g.d_cs, g.d_khi, g.d_klo, g.d_ctr, g.d_rec);
+    k_proxy<<<grid, 256, 0, st>>>(g.d_noise, g.d_zones, world_dev(), g_cut, g.d_out, ZoneWork{});
+    label_components(g.d_zones, grid, ZoneWork{}, g.d_out, g.d_par, g.d_rid, g.d_cs, g.d_khi, g.d_klo, g.d_rec, g.d_ctr, min_cells,
+                     unsigned(std::min<int64_t>(off, 1 << 20)), unsigned(std::min<int64_t>(off, 4 * 148)), st);
     DSG_CU(cudaGetLastError());
     if (bits) DSG_CU(cudaMemcpyAsync(bits, g.d_out, size_t(off), cudaMemcpyDeviceToHost, st));
     DSG_CU(cudaMemcpyAsync(g.h_ctr, g.d_ctr, 4 * 4, cudaMemcpyDeviceToHost, st));
@@ -360,6 +393,17 @@ int proxy_components(const uint64_t *seeds, uint32_t nseeds, const uint32_t *zon
     std::sort(rec.begin(), rec.end(), [](const dsg_component &a, const dsg_component &b) { return a.zone != b.zone ? a.zone < b.zone : a.first < b.first; });
     std::copy(rec.begin(), rec.begin() + std::min(kept, cap), out);
     return kept > cap ? DSG_OVERFLOW : DSG_OK;
+}
+// Proxy bitmaps and components of zones built on the device (the device-resident searcher): zones[0, *nzones)
+// with their cell offsets, and the chunk list chunk[0, *nchunk) over them; buffers sized for the capacities by
+// the caller (par, rid, cs, khi, klo, rec: one entry per cell).  Enqueued on st; ctr as label_components.
+void proxy_components_device(const SeedNoise *noise, const zones::DZone *zones, const ZoneWork &wk, uint32_t grid_blocks, uint8_t *bits,
+                             int32_t *par, int32_t *rid, CompStat *cs, uint64_t *khi, uint32_t *klo, dsg_component *rec, uint32_t *ctr,
+                             uint32_t min_cells, cudaStream_t st) {
+    DSG_CU(cudaMemsetAsync(ctr, 0, 4 * 4, st));
+    k_proxy<<<grid_blocks, 256, 0, st>>>(noise, zones, world_dev(), g_cut, bits, wk);
+    label_components(zones, dim3(grid_blocks), wk, bits, par, rid, cs, khi, klo, rec, ctr, min_cells, 1u << 20, 4 * 148, st);
+    DSG_CU(cudaGetLastError());
 }
 }  // namespace dsg
 

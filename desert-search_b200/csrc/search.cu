@@ -1,0 +1,995 @@
+// The device-resident searcher: gate -> period tables/blur -> translation scan -> bucket suppression -> hot-zone
+// floods -> proxy components -> exact floods, for a range of seed indices, with every stage on the GPU and the
+// survivors of one stage handed to the next through device queues (counts and index lists in device memory).
+//
+// Reference: the production GPU search, `dsearch_desert_gpu START COUNT PREFIX THREADS gate=1 gpu=1 gscan=1`
+// (deploy/gpipe.sh:5): src/dsearch_desert.cpp:173-557 (per-seed stages S1-S5 on worker threads), its GPU engine
+// src/gpu/gproxy.cu (scan_loop, gpu_loop) and gate src/gpu/gate.cuh:361-419.  The reference moves every gated
+// seed through host threads and synchronises the host with the GPU several times per seed and stage
+// (gate.cuh:386-407, gproxy.cu:254-264, :375).  Here one wave of seed indices is a gate launch followed by one
+// CUDA graph: every stage is a kernel whose grid covers the wave's capacity and reads its work count from the
+// queue the previous stage filled; the floods' round loops are conditional WHILE nodes whose bodies end in a
+// kernel that ends the loop when no work is queued (or a round limit is reached), so the host is not involved
+// until the wave's result records are copied back.
+//
+// The per-seed decisions the reference makes sequentially (a site is skipped when an earlier site's hot zone
+// covers it; a later exact-flood start is tried only if the earlier ones fell short) are replayed per seed
+// on the device over speculatively computed floods, exactly as the host searcher does; the element orders of
+// std::sort (candidates by score, components by size) come from the same algorithm (stl_sort.h).  Results are
+// therefore the host searcher's, line for line.  A wave that exceeds one of the fixed capacities below is
+// reported back (its gated seeds) for the caller to run through the per-stage entry points.
+#include "flood_kernels.cuh"
+#include "zones.cuh"
+#include "stl_sort.h"
+#include <cub/block/block_scan.cuh>
+#include <algorithm>
+#include <climits>
+#include <mutex>
+#include <vector>
+
+namespace dsg {
+namespace gate {
+struct Lane;
+Lane *lane_create(uint64_t batch);
+void lane_enqueue(Lane *l, cudaStream_t st, uint64_t start, uint64_t nb, const dsg_gate_cfg &c);
+const uint64_t *lane_survivors(const Lane *l);
+uint32_t *lane_counts(Lane *l);
+void lane_caps(const Lane *l, uint32_t caps[3]);
+}  // namespace gate
+void scan_seeds_device(const SeedNoise *noise, const uint32_t *n_dev, uint32_t cap_seeds, void *tabin, float *tab, float *mx, int32_t *act,
+                       uint32_t *nact, dsg_cand *cand, uint32_t *ncand, uint32_t cap, const dsg_scan_params &sp, cudaStream_t st);
+size_t tabin_bytes();
+void proxy_components_device(const SeedNoise *noise, const zones::DZone *zones, const zones::ZoneWork &wk, uint32_t grid_blocks, uint8_t *bits,
+                             int32_t *par, int32_t *rid, zones::CompStat *cs, uint64_t *khi, uint32_t *klo, dsg_component *rec, uint32_t *ctr,
+                             uint32_t min_cells, cudaStream_t st);
+void seed_noise_build_dev(const uint64_t *d_seeds, const uint32_t *n_dev, uint32_t cap, SeedNoise *d_out, cudaStream_t st);
+
+namespace search {
+using namespace flood;
+using zones::DZone;
+using zones::CHUNK;
+
+constexpr int PERIOD = 262144, CELL = 512, KMIN = -30;
+// capacities of one wave
+constexpr uint32_t SC = 1024;                // gated seeds
+constexpr uint32_t RAWCAP = 1u << 16;        // raw scan candidates per seed (the reference's per-seed buffer, gproxy.cu:209)
+constexpr int HT = 4096;                     // bucket hash slots per seed (shared memory)
+constexpr uint32_t MS = 300;                 // sites per seed (Params.max_sites at most this)
+constexpr uint32_t ZPS = 64;                 // big hot zones per seed
+constexpr uint32_t ZCAP = 8192;              // zones per wave
+constexpr uint32_t CELLCAP = 1u << 25;       // proxy cells per wave
+constexpr uint32_t CHCAP = CELLCAP / CHUNK + ZCAP;
+constexpr uint32_t EVC = 128;                // proxy components kept per seed
+constexpr int EXN = 2;                       // exact floods per seed (Params.exact_n at most this)
+constexpr uint32_t TRIES = SC * EXN * 3;     // exact-flood starts: the start and two alternatives
+constexpr uint32_t ROWCAP = 1u << 16;        // CSV rows per wave
+constexpr uint32_t LOOP_LIMIT = 2048;        // flood loop iterations (6 rounds each) before a wave gives up
+constexpr uint32_t POOL_TILES = 3u << 20;    // flood tiles (1.7 KB each)
+constexpr int RING = 289;                    // exact-start search points: rings 0..8 of 16 quarts
+
+// wave flags (ctr[C_FLAGS]): a set bit means the wave's results are incomplete
+enum : uint32_t { F_GATE = 1, F_RAW = 2, F_HASH = 4, F_ZONES = 8, F_CELLS = 16, F_EVALS = 32, F_POOL = 64, F_LOOP = 128, F_LABEL = 256,
+                  F_ROWS = 512 };
+// device counters
+enum { C_NS = 0, C_NREQ = 1 /* 4 flood phases */, C_ZONES = 5, C_CHUNKS = 6, C_ROWS = 7, C_FLAGS = 8, C_NHOT = 9, C_NBIG = 10, C_SITES = 11,
+       C_ROUND = 16 /* 9 round counters */, C_TAKEN = 25, C_FERR = 26, C_BASE = 27, C_LOOPS = 28, C_PROXY = 32 /* 4 */, C_KEPT = 33,
+       C_N = 48 };
+
+struct Params {
+    dsg_scan_params sp;
+    int32_t max_sites, nms, exact_n;
+    double hot_min, hot_pre, exact_min, refine_mb, csv_min;
+};
+struct Site { float s, t, c, e; int32_t x, z; };           // dsg_cand layout
+struct Hot { int32_t hx, hz; double bt; };
+struct ZoneMeta { uint32_t seed, rank; double hot; };
+struct Eval {
+    uint32_t rank; int32_t x, z; double proxy, s8, s4, hot;
+    int32_t ax[2], az[2];
+    int32_t nalt, edge, nostart, exact;
+};
+struct Try { int32_t sx, sz; int32_t q; int32_t valid; };
+
+__constant__ int8_t c_ring[RING][2];                       // (dx, dz) of the exact-start search, in the reference's order
+
+// ---------------------------------------------------------------- wave set-up
+__global__ void k_begin(const uint32_t *gcount, uint32_t cap1, uint32_t cap2, uint32_t cap3, const uint64_t *surv, uint64_t *seeds, uint32_t *ctr) {
+    const uint32_t n3 = gcount[2], nS = min(n3, SC);
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+        for (int k = 0; k < C_N; k++) if (k != C_TAKEN && k != C_BASE) ctr[k] = 0;
+        ctr[C_NS] = nS;
+        if (gcount[0] > cap1 || gcount[1] > cap2 || n3 > cap3 || n3 > SC) ctr[C_FLAGS] |= F_GATE;
+    }
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < nS; i += gridDim.x * blockDim.x) seeds[i] = surv[i];
+}
+
+// ---------------------------------------------------------------- bucket best + suppression (dsearch_desert.cpp:285-308)
+__device__ __forceinline__ uint32_t scan_order(int32_t x, int32_t z) {      // the CPU scan loop's (j, i, tz, tx) order
+    const int i = ((x % PERIOD) + PERIOD) % PERIOD / CELL, tx = int(floor(double(x) / PERIOD)) - KMIN;
+    const int j = ((z % PERIOD) + PERIOD) % PERIOD / CELL, tz = int(floor(double(z) / PERIOD)) - KMIN;
+    return (uint32_t(j) << 21) | (uint32_t(i) << 12) | (uint32_t(tz) << 6) | uint32_t(tx);
+}
+__device__ __forceinline__ uint64_t bucket_key(int32_t x, int32_t z, int nms) {
+    return (uint64_t(uint32_t((x + 8000000) / nms)) << 32) | uint32_t((z + 8000000) / nms);
+}
+__device__ __forceinline__ uint32_t float_order(float f) {               // unsigned order of floats
+    const uint32_t b = __float_as_uint(f);
+    return (b & 0x80000000u) ? ~b : (b | 0x80000000u);
+}
+__device__ __forceinline__ uint32_t hash_slot(uint64_t k) { return uint32_t((k * 0x9E3779B97F4A7C15ull) >> 52) & (HT - 1); }
+
+// One block per seed.  For each NMS bucket: the candidate with the highest score (first in CPU loop order on
+// equal scores) and the loop order of the bucket's first candidate; buckets in that first-seen order, sorted
+// by score with std::sort's algorithm, then kept greedily unless within nms of an earlier kept site, up to
+// max_sites.  Mirrors host/dsearch_desert.cpp (and the reference's S2 loop).
+constexpr int NMS_THREADS = 512;
+constexpr size_t NMS_SMEM = size_t(HT) * (8 + 8 + 4 + 4 + 4 + 2) + size_t(MS) * 8;
+__global__ void __launch_bounds__(NMS_THREADS) k_nms(const dsg_cand *__restrict__ raw, const uint32_t *__restrict__ nraw, Params P,
+                                                     Site *__restrict__ sites, uint32_t *__restrict__ nsites, uint32_t *__restrict__ nbuck,
+                                                     uint32_t *ctr) {
+    extern __shared__ __align__(16) unsigned char nms_smem[];
+    unsigned long long *key = reinterpret_cast<unsigned long long *>(nms_smem);
+    unsigned long long *best = key + HT;           // (score order << 32) | ~loop order
+    uint32_t *first = reinterpret_cast<uint32_t *>(best + HT);
+    uint32_t *bidx = first + HT;                   // raw index of the bucket's best candidate
+    float *sv = reinterpret_cast<float *>(bidx + HT);
+    int32_t *kx = reinterpret_cast<int32_t *>(sv + HT), *kz = kx + MS;
+    uint16_t *order = reinterpret_cast<uint16_t *>(kz + MS);   // bucket positions, then sorted by score
+    __shared__ uint32_t s_m, s_flag;
+    const uint32_t s = blockIdx.x;
+    if (s >= ctr[C_NS]) return;
+    const uint32_t nr = nraw[s];
+    if (threadIdx.x == 0) { s_m = 0; s_flag = 0; }
+    if (nr > RAWCAP) {                            // the scan overflowed: this seed cannot be finished here
+        if (threadIdx.x == 0) { atomicOr(ctr + C_FLAGS, F_RAW); nsites[s] = 0; nbuck[s] = 0; }
+        return;
+    }
+    for (int k = threadIdx.x; k < HT; k += blockDim.x) { key[k] = ~0ull; best[k] = 0; first[k] = 0xffffffffu; bidx[k] = 0xffffffffu; }
+    __syncthreads();
+    const dsg_cand *rc = raw + size_t(s) * RAWCAP;
+    for (uint32_t i = threadIdx.x; i < nr; i += blockDim.x) {
+        const dsg_cand c = rc[i];
+        const uint64_t k = bucket_key(c.x, c.z, P.nms);
+        const uint32_t o = scan_order(c.x, c.z);
+        uint32_t h = hash_slot(k);
+        int probe = 0;
+        for (; probe < HT; probe++, h = (h + 1) & (HT - 1)) {
+            const unsigned long long old = atomicCAS(&key[h], ~0ull, k);
+            if (old == ~0ull || old == k) break;
+        }
+        if (probe == HT) { s_flag = 1; continue; }
+        atomicMin(&first[h], o);
+        atomicMax(&best[h], (uint64_t(float_order(c.s)) << 32) | uint64_t(0xffffffffu - o));
+    }
+    __syncthreads();
+    if (s_flag) {
+        if (threadIdx.x == 0) { atomicOr(ctr + C_FLAGS, F_HASH); nsites[s] = 0; nbuck[s] = 0; }
+        return;
+    }
+    for (uint32_t i = threadIdx.x; i < nr; i += blockDim.x) {            // which raw candidate is each bucket's best
+        const dsg_cand c = rc[i];
+        const uint64_t k = bucket_key(c.x, c.z, P.nms);
+        uint32_t h = hash_slot(k);
+        while (key[h] != k) h = (h + 1) & (HT - 1);
+        if (0xffffffffu - uint32_t(best[h]) == scan_order(c.x, c.z)) bidx[h] = i;
+    }
+    // occupied slots, sorted by first-seen order (bitonic over (first, slot) keys in `best`, now free)
+    __syncthreads();
+    for (int k = threadIdx.x; k < HT; k += blockDim.x) best[k] = key[k] != ~0ull ? (uint64_t(first[k]) << 32) | uint32_t(k) : ~0ull;
+    __syncthreads();
+    for (int size = 2; size <= HT; size <<= 1)
+        for (int stride = size >> 1; stride > 0; stride >>= 1) {
+            for (int i = threadIdx.x; i < HT / 2; i += blockDim.x) {
+                const int lo = 2 * i - (i & (stride - 1)), hi = lo + stride;
+                const bool up = (lo & size) == 0;
+                const unsigned long long a = best[lo], b = best[hi];
+                if ((a > b) == up) { best[lo] = b; best[hi] = a; }
+            }
+            __syncthreads();
+        }
+    for (int k = threadIdx.x; k < HT; k += blockDim.x)
+        if (best[k] != ~0ull && bidx[uint32_t(best[k])] == 0xffffffffu) s_flag = 1;     // cannot happen: each best is a candidate
+    __syncthreads();
+    if (s_flag) {
+        if (threadIdx.x == 0) { atomicOr(ctr + C_FLAGS, F_HASH); nsites[s] = 0; nbuck[s] = 0; }
+        return;
+    }
+    for (int k = threadIdx.x; k < HT; k += blockDim.x)
+        if (best[k] != ~0ull) {
+            const uint32_t slot = uint32_t(best[k]);
+            order[k] = uint16_t(k);
+            sv[k] = rc[bidx[slot]].s;
+            first[k] = bidx[slot];                 // position k (first-seen order) -> raw index
+            atomicAdd(&s_m, 1u);
+        }
+    __syncthreads();
+    const uint32_t m = s_m;
+    // std::sort(cand, score descending) over the buckets in first-seen order
+    if (threadIdx.x == 0) dsg::stl::sort(order, int64_t(m), [&](uint16_t a, uint16_t b) { return sv[a] > sv[b]; });
+    __syncthreads();
+    // greedy suppression: warp 0 walks the sorted buckets, the lanes test the kept sites
+    if (threadIdx.x < 32) {
+        const int lane = threadIdx.x;
+        uint32_t kept = 0;
+        const int nms = P.nms;
+        for (uint32_t k = 0; k < m && int(kept) < P.max_sites; k++) {
+            const dsg_cand c = rc[first[order[k]]];
+            bool near = false;
+            for (uint32_t q = lane; q < kept; q += 32) near |= abs(kx[q] - c.x) < nms && abs(kz[q] - c.z) < nms;
+            near = __any_sync(0xffffffffu, near);
+            if (!near) {
+                if (lane == 0) {
+                    kx[kept] = c.x; kz[kept] = c.z;
+                    sites[size_t(s) * MS + kept] = {c.s, c.t, c.c, c.e, c.x, c.z};
+                }
+                kept++;
+                __syncwarp();
+            }
+        }
+        if (lane == 0) { nsites[s] = kept; nbuck[s] = m; atomicAdd(ctr + C_SITES, kept); }
+    }
+}
+
+// ---------------------------------------------------------------- hot points (dsearch_desert.cpp:328-332)
+// Warp per site: T at 7 x 7 points 256 quarts apart around it; the hottest, first in (dz, dx) order on ties.
+__global__ void __launch_bounds__(256) k_hot(const SeedNoise *__restrict__ noise, const Site *__restrict__ sites, const uint32_t *__restrict__ nsites,
+                                             const uint32_t *ctr, Hot *__restrict__ hot) {
+    const int lane = threadIdx.x & 31;
+    const uint32_t nS = ctr[C_NS];
+    const uint32_t warps = gridDim.x * (blockDim.x >> 5);
+    for (uint32_t w = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5); w < nS * MS; w += warps) {
+        const uint32_t s = w / MS, r = w % MS;
+        if (r >= nsites[s]) continue;
+        const Site st = sites[w];
+        const SeedNoise &S = noise[s];
+        double bv = -9; int bq = 64;
+        for (int q = lane; q < 49; q += 32) {
+            const int x = st.x + (q % 7 - 3) * 256, z = st.z + (q / 7 - 3) * 256;
+            const double v = channel(S, CH_T, x, 0, z);
+            if (v > bv) { bv = v; bq = q; }
+        }
+        #pragma unroll
+        for (int o = 16; o; o >>= 1) {
+            const double ov = __shfl_xor_sync(0xffffffffu, bv, o);
+            const int oq = __shfl_xor_sync(0xffffffffu, bq, o);
+            if (ov > bv || (ov == bv && oq < bq)) { bv = ov; bq = oq; }
+        }
+        if (lane == 0) {
+            Hot h{st.x, st.z, -9};
+            if (bq < 49) { h.hx = st.x + (bq % 7 - 3) * 256; h.hz = st.z + (bq / 7 - 3) * 256; h.bt = bv; }
+            hot[w] = h;
+        }
+    }
+}
+
+// ---------------------------------------------------------------- flood requests
+__device__ __forceinline__ FloodCtl make_ctl(int32_t qx, int32_t qz, int step, int half, int conn8, int pred, int32_t noise, uint32_t k) {
+    FloodCtl c{};
+    c.qx = qx; c.qz = qz; c.step = step; c.half = half; c.n = 2 * half + 1; c.tpr = (c.n + TILE - 1) / TILE;
+    c.conn8 = conn8; c.pred = pred; c.pcut = 0.f; c.noise = noise; c.eager = 0; c.pad = 0;
+    c.dir_off = int64_t(k) * c.tpr * c.tpr;
+    return c;
+}
+// Step-256 pre-flood of every hot site (T >= 0.55 at its hottest point), speculatively (dsearch_desert.cpp:334-345).
+__global__ void k_req_pre(const Hot *__restrict__ hot, const uint32_t *__restrict__ nsites, uint32_t *ctr, FloodCtl *__restrict__ ctl,
+                          uint32_t *__restrict__ meta, int32_t *__restrict__ f1, int32_t *__restrict__ f2) {
+    const uint32_t nS = ctr[C_NS];
+    for (uint32_t w = blockIdx.x * blockDim.x + threadIdx.x; w < nS * MS; w += gridDim.x * blockDim.x) {
+        const uint32_t s = w / MS, r = w % MS;
+        f1[w] = -1; f2[w] = -1;
+        if (r >= nsites[s] || hot[w].bt < 0.55) continue;
+        const uint32_t k = atomicAdd(ctr + C_NREQ + 0, 1u);
+        f1[w] = int32_t(k);
+        ctl[k] = make_ctl(hot[w].hx, hot[w].hz, 256, 32000 / 256, 0, DSG_PRED_HOT, int32_t(s), k);
+        meta[k] = w;
+    }
+}
+__device__ __forceinline__ bool small_zone(const FloodStat &a, const Params &P) {
+    return double(a.cells) * 256.0 * 256 * 16 / 1e6 < P.hot_pre * P.hot_min;
+}
+// Step-128 flood of every hot site whose pre-flood is not small (dsearch_desert.cpp:346-352), speculatively.
+__global__ void k_req_128(const FloodStat *__restrict__ st1, const FloodCtl *__restrict__ ctl1, const uint32_t *__restrict__ meta1, Params P,
+                          uint32_t *ctr, FloodCtl *__restrict__ ctl, uint32_t *__restrict__ meta, int32_t *__restrict__ f2) {
+    const uint32_t n1 = ctr[C_NREQ + 0];
+    for (uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < n1; k += gridDim.x * blockDim.x) {
+        if (small_zone(st1[k], P)) continue;
+        const uint32_t w = meta1[k], j = atomicAdd(ctr + C_NREQ + 1, 1u);
+        f2[w] = int32_t(j);
+        ctl[j] = make_ctl(ctl1[k].qx, ctl1[k].qz, 128, 32000 / 128, 0, DSG_PRED_HOT, ctl1[k].noise, j);
+        meta[j] = w;
+    }
+}
+
+// ---------------------------------------------------------------- device-driven flood rounds
+__global__ void k_dir_fill(int32_t *__restrict__ dir, const uint32_t *nreq, uint32_t per_req) {
+    const uint64_t n = uint64_t(*nreq) * per_req;
+    for (uint64_t i = uint64_t(blockIdx.x) * blockDim.x + threadIdx.x; i < n; i += uint64_t(gridDim.x) * blockDim.x) dir[i] = -1;
+}
+// Phase start: round counters cleared, the loop entered only if there are requests.
+__global__ void k_phase_begin(uint32_t *ctr, const uint32_t *nreq, cudaGraphConditionalHandle h) {
+    for (int k = 0; k < 9; k++) ctr[C_ROUND + k] = 0;
+    cudaGraphSetConditional(h, *nreq > 0 ? 1u : 0u);
+}
+// Start of every request: statistics reset, start tile claimed, start sub-block queued for round *base.
+__global__ void k_req_start(const FloodCtl *__restrict__ ctl, const uint32_t *nreq, FloodStat *__restrict__ st, int32_t *__restrict__ dir, Tiles T,
+                            TileAlloc ta, uint32_t *n_list, uint32_t *ctr) {
+    const uint32_t n = *nreq;
+    for (uint32_t r = blockIdx.x * blockDim.x + threadIdx.x; r < n; r += gridDim.x * blockDim.x) {
+        const FloodCtl c = ctl[r];
+        FloodStat &s = st[r];
+        s.cells = 0; s.sampled = 0; s.minx = s.maxx = c.qx; s.minz = s.maxz = c.qz; s.edge = s.border = s.overflow = 0;
+        const int32_t t = claim_tile(c, r, c.half >> 6, c.half >> 6, dir, T, ta, st, ctr + C_FERR);
+        const int sb = (((c.half & 63) >> 4) << 2) | ((c.half & 63) >> 4);
+        request_blocks(T, t, 1u << sb, r, n_list, ctr + C_ROUND, 0, nullptr);
+    }
+}
+// End of a loop iteration (6 rounds): advance the round base; stop when the next round has no work, or at the
+// iteration limit (the wave is then flagged).
+__global__ void k_loop_ctl(uint32_t *ctr, cudaGraphConditionalHandle h) {
+    ctr[C_BASE] += 6;
+    const uint32_t it = ++ctr[C_LOOPS];
+    const bool more = ctr[C_ROUND + 0] != 0 || ctr[C_ROUND + 3] != 0;
+    if (more && it >= LOOP_LIMIT) ctr[C_FLAGS] |= F_LOOP;
+    cudaGraphSetConditional(h, more && it < LOOP_LIMIT ? 1u : 0u);
+}
+__global__ void k_phase_end(uint32_t *ctr) {
+    ctr[C_LOOPS] = 0;
+    if (ctr[C_FERR]) ctr[C_FLAGS] |= F_POOL;
+}
+
+// ---------------------------------------------------------------- hot-zone coverage replay (dsearch_desert.cpp:326-372)
+struct FloodView { const FloodCtl *ctl; const int32_t *dir; };
+// Is window cell (i, j) of request k in its reached set R?
+__device__ __forceinline__ bool reached(const FloodView &f, const Tiles &T, uint32_t k, int64_t i, int64_t j) {
+    const FloodCtl &c = f.ctl[k];
+    if (i < 0 || j < 0 || i >= c.n || j >= c.n) return false;
+    const int32_t t = f.dir[c.dir_off + (j >> 6) * c.tpr + (i >> 6)];
+    if (t < 0) return false;
+    return (T.bits[size_t(t) * TILE_U64 + 2 * TILE + (j & 63)] >> (i & 63)) & 1;
+}
+__device__ __forceinline__ int64_t ceil_div(int64_t a, int64_t b) { return a >= 0 ? (a + b - 1) / b : -((-a) / b); }
+// hotcovered.count(hotkey(hx, hz)) against the floods a seed has used: a step-128 flood covers the 128-quart
+// key block of each of its cells, a step-256 one the key blocks of its cells offset by 0 or 128 on each axis.
+__device__ bool covered(int hx, int hz, const uint32_t *cov, int ncov, const FloodView &f1, const FloodView &f2, const Tiles &T) {
+    const int64_t bx = int64_t((hx + 8000000) >> 7) * 128 - 8000000, bz = int64_t((hz + 8000000) >> 7) * 128 - 8000000;
+    for (int k = 0; k < ncov; k++) {
+        const bool pre = (cov[k] >> 31) == 0;
+        const uint32_t r = cov[k] & 0x7fffffffu;
+        const FloodView &f = pre ? f1 : f2;
+        const FloodCtl &c = f.ctl[r];
+        const int offs = pre ? 2 : 1;
+        for (int dz = 0; dz < offs; dz++)
+            for (int dx = 0; dx < offs; dx++) {
+                const int64_t lox = bx - dx * 128, loz = bz - dz * 128;
+                const int64_t ix = ceil_div(lox - c.qx, c.step), iz = ceil_div(loz - c.qz, c.step);
+                if (c.qx + ix * c.step > lox + 127 || c.qz + iz * c.step > loz + 127) continue;
+                if (reached(f, T, r, ix + c.half, iz + c.half)) return true;
+            }
+    }
+    return false;
+}
+// Thread per seed: the reference's walk over its sites in rank order, using only the floods of the sites it
+// does not skip; big zones (hot area >= hot_min) become proxy zones of 32-quart cells around the flood's bbox.
+__global__ void k_cover(const Hot *__restrict__ hot, const uint32_t *__restrict__ nsites, const int32_t *__restrict__ f1, const int32_t *__restrict__ f2,
+                        FloodView v1, FloodView v2, const FloodStat *__restrict__ st1, const FloodStat *__restrict__ st2, Tiles T, Params P,
+                        uint32_t *__restrict__ cov_buf, uint32_t *__restrict__ nzone, DZone *__restrict__ zslot, ZoneMeta *__restrict__ zmeta,
+                        uint32_t *ctr) {
+    const uint32_t s = blockIdx.x * blockDim.x + threadIdx.x;
+    if (s >= ctr[C_NS]) return;
+    uint32_t *cov = cov_buf + size_t(s) * MS;
+    int ncov = 0;
+    uint32_t nz = 0, nhot = 0, nbig = 0;
+    for (uint32_t r = 0; r < nsites[s]; r++) {
+        const uint32_t w = s * MS + r;
+        const Hot h = hot[w];
+        if (h.bt < 0.55 || covered(h.hx, h.hz, cov, ncov, v1, v2, T)) continue;
+        const int32_t k1 = f1[w];
+        if (small_zone(st1[k1], P)) { cov[ncov++] = uint32_t(k1); nhot++; continue; }
+        const int32_t k2 = f2[w];
+        cov[ncov++] = 0x80000000u | uint32_t(k2);
+        nhot++;
+        const FloodStat a = st2[k2];
+        const double hot_area = double(a.cells) * 128.0 * 128 * 16 / 1e6;
+        if (hot_area < P.hot_min) continue;
+        nbig++;
+        if (nz == ZPS) { atomicOr(ctr + C_FLAGS, F_ZONES); continue; }
+        DZone z{};
+        z.x0 = int(floor((a.minx - 128) / 32.0)) * 32; z.z0 = int(floor((a.minz - 128) / 32.0)) * 32;
+        z.nx = (a.maxx + 128 - z.x0) / 32 + 1; z.nz = (a.maxz + 128 - z.z0) / 32 + 1;
+        z.seed = int32_t(s);
+        zslot[size_t(s) * ZPS + nz] = z;
+        zmeta[size_t(s) * ZPS + nz] = {s, r, hot_area};
+        nz++;
+    }
+    nzone[s] = nz;
+    atomicAdd(ctr + C_NHOT, nhot); atomicAdd(ctr + C_NBIG, nbig);
+}
+// One block: the seeds' zones concatenated in seed order (zfirst[s] = first zone of seed s), their cell offsets
+// and the chunk list over them.  Flags the wave when the zones or cells exceed the capacities.
+constexpr int LIST_THREADS = 1024;
+__global__ void __launch_bounds__(LIST_THREADS) k_zone_list(const uint32_t *__restrict__ nzone, const DZone *__restrict__ zslot,
+                                                            const ZoneMeta *__restrict__ zmeta, uint32_t *__restrict__ zfirst, DZone *__restrict__ zones,
+                                                            ZoneMeta *__restrict__ meta, uint2 *__restrict__ chunks, uint32_t *ctr) {
+    using Scan = cub::BlockScan<uint64_t, LIST_THREADS>;
+    __shared__ typename Scan::TempStorage tmp;
+    __shared__ uint64_t s_base[2];
+    const uint32_t nS = ctr[C_NS];
+    // zone offsets per seed (one seed per thread, SC <= LIST_THREADS)
+    const uint32_t s = threadIdx.x;
+    uint64_t cnt = s < nS ? nzone[s] : 0, off = 0, total = 0;
+    Scan(tmp).ExclusiveSum(cnt, off, total);
+    __syncthreads();
+    if (s < nS) zfirst[s] = uint32_t(off);
+    if (s == 0) zfirst[nS] = uint32_t(total);
+    const uint32_t nz = uint32_t(total < ZCAP ? total : ZCAP);
+    if (total > ZCAP && threadIdx.x == 0) ctr[C_FLAGS] |= F_ZONES;
+    if (s < nS)
+        for (uint32_t k = 0; k < cnt && off + k < ZCAP; k++) { zones[off + k] = zslot[size_t(s) * ZPS + k]; meta[off + k] = zmeta[size_t(s) * ZPS + k]; }
+    __syncthreads();
+    // cell offsets and chunk counts, LIST_THREADS zones at a time
+    if (threadIdx.x == 0) { s_base[0] = 0; s_base[1] = 0; }
+    __syncthreads();
+    for (uint32_t z0 = 0; z0 < nz; z0 += LIST_THREADS) {
+        const uint32_t z = z0 + threadIdx.x;
+        const uint64_t cells = z < nz ? uint64_t(zones[z].nx) * uint64_t(zones[z].nz) : 0;
+        const uint64_t nch = (cells + CHUNK - 1) / CHUNK;
+        uint64_t coff, ctot, choff, chtot;
+        Scan(tmp).ExclusiveSum(cells, coff, ctot);
+        __syncthreads();
+        Scan(tmp).ExclusiveSum(nch, choff, chtot);
+        __syncthreads();
+        const uint64_t cb = s_base[0] + coff, hb = s_base[1] + choff;
+        if (z < nz) {
+            zones[z].off = int64_t(cb);
+            if (cb + cells <= CELLCAP && hb + nch <= CHCAP)
+                for (uint64_t k = 0; k < nch; k++) chunks[hb + k] = make_uint2(z, uint32_t(k));
+        }
+        __syncthreads();
+        if (threadIdx.x == 0) { s_base[0] += ctot; s_base[1] += chtot; }
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) {
+        ctr[C_ZONES] = nz;
+        if (s_base[0] > CELLCAP || s_base[1] > CHCAP) { ctr[C_FLAGS] |= F_CELLS; ctr[C_CHUNKS] = 0; }
+        else ctr[C_CHUNKS] = uint32_t(s_base[1]);
+    }
+}
+
+// ---------------------------------------------------------------- components per zone, evaluations (dsearch_desert.cpp:451-496)
+__global__ void k_comp_count(const dsg_component *__restrict__ rec, const uint32_t *ctr, uint32_t *__restrict__ zcnt) {
+    const uint32_t kept = ctr[C_KEPT];
+    for (uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < kept; k += gridDim.x * blockDim.x) atomicAdd(&zcnt[rec[k].zone], 1u);
+}
+__global__ void __launch_bounds__(LIST_THREADS) k_comp_offsets(const uint32_t *__restrict__ zcnt, uint32_t *__restrict__ zoff, const uint32_t *ctr) {
+    using Scan = cub::BlockScan<uint32_t, LIST_THREADS>;
+    __shared__ typename Scan::TempStorage tmp;
+    __shared__ uint32_t base;
+    const uint32_t nz = ctr[C_ZONES];
+    if (threadIdx.x == 0) base = 0;
+    __syncthreads();
+    for (uint32_t z0 = 0; z0 < nz; z0 += LIST_THREADS) {
+        const uint32_t z = z0 + threadIdx.x;
+        uint32_t c = z < nz ? zcnt[z] : 0, o, t;
+        Scan(tmp).ExclusiveSum(c, o, t);
+        if (z < nz) zoff[z] = base + o;
+        __syncthreads();
+        if (threadIdx.x == 0) base += t;
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) zoff[nz] = base;
+}
+__global__ void k_comp_scatter(const dsg_component *__restrict__ rec, const uint32_t *ctr, const uint32_t *__restrict__ zoff,
+                               uint32_t *__restrict__ zfill, uint32_t *__restrict__ zcomp) {
+    const uint32_t kept = ctr[C_KEPT];
+    for (uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < kept; k += gridDim.x * blockDim.x) {
+        const uint32_t z = rec[k].zone;
+        zcomp[zoff[z] + atomicAdd(&zfill[z], 1u)] = k;
+    }
+}
+// Thread per seed: components of its zones in (zone, first cell) order, each new one (by its smallest column and
+// row) an evaluation whose start is the interior cell nearest the centroid (alternatives at ranks n/3, 2n/3);
+// evaluations sorted by proxy size with std::sort's algorithm; exact-flood starts of the first exact_n.
+__global__ void k_evals(const uint32_t *__restrict__ zfirst, const DZone *__restrict__ zones, const ZoneMeta *__restrict__ zmeta,
+                        const uint32_t *__restrict__ zoff, uint32_t *__restrict__ zcomp, const dsg_component *__restrict__ rec, Params P,
+                        Eval *__restrict__ evu, Eval *__restrict__ ev, uint32_t *__restrict__ nev, int64_t *__restrict__ sig, Try *__restrict__ tries,
+                        uint32_t *ctr) {
+    const uint32_t s = blockIdx.x * blockDim.x + threadIdx.x;
+    if (s >= ctr[C_NS]) return;
+    Eval *U = evu + size_t(s) * EVC, *E = ev + size_t(s) * EVC;
+    int64_t *seen = sig + size_t(s) * EVC;
+    uint32_t ne = 0, nseen = 0;
+    bool full = false;
+    const uint32_t nzw = ctr[C_ZONES];
+    for (uint32_t zi = zfirst[s]; zi < zfirst[s + 1] && zi < nzw; zi++) {
+        const DZone z = zones[zi];
+        const ZoneMeta m = zmeta[zi];
+        uint32_t *L = zcomp + zoff[zi];
+        const uint32_t nc = zoff[zi + 1] - zoff[zi];
+        for (uint32_t i = 1; i < nc; i++) {                 // by first cell (unique within a zone)
+            const uint32_t v = L[i];
+            int32_t j = int32_t(i) - 1;
+            while (j >= 0 && rec[L[j]].first > rec[v].first) { L[j + 1] = L[j]; j--; }
+            L[j + 1] = v;
+        }
+        for (uint32_t i = 0; i < nc; i++) {
+            const dsg_component c = rec[L[i]];
+            const double area = c.cells * 32.0 * 32 * 16 / 1e6;
+            if (area < 1) continue;
+            const int64_t sg = (int64_t(z.x0 + c.minx * 32) << 32) | uint32_t(z.z0 + c.minz * 32);
+            bool dup = false;
+            for (uint32_t k = 0; k < nseen; k++) dup |= seen[k] == sg;
+            if (dup) continue;
+            if (nseen == EVC) { full = true; continue; }
+            seen[nseen++] = sg;
+            const int32_t cell = c.inner ? c.pick[0] : c.first;
+            Eval e{};
+            e.rank = m.rank; e.x = z.x0 + (cell % z.nx) * 32; e.z = z.z0 + (cell / z.nx) * 32;
+            e.proxy = area; e.s8 = -1; e.s4 = 0; e.hot = m.hot;
+            e.nalt = c.inner ? 2 : 0;
+            for (int a = 0; a < e.nalt; a++) { e.ax[a] = z.x0 + (c.pick[a + 1] % z.nx) * 32; e.az[a] = z.z0 + (c.pick[a + 1] / z.nx) * 32; }
+            U[ne++] = e;
+        }
+    }
+    if (full) atomicOr(ctr + C_FLAGS, F_EVALS);
+    // std::sort(ev, proxy descending): the permutation from the sort, the records copied out in its order
+    uint8_t idx[EVC];
+    for (uint32_t k = 0; k < ne; k++) idx[k] = uint8_t(k);
+    dsg::stl::sort(idx, int64_t(ne), [&](uint8_t a, uint8_t b) { return U[a].proxy > U[b].proxy; });
+    for (uint32_t k = 0; k < ne; k++) E[k] = U[idx[k]];
+    if (s == 0 && ctr[C_PROXY + 3]) atomicOr(ctr + C_FLAGS, F_LABEL);
+    nev[s] = ne;
+    for (int k2 = 0; k2 < EXN; k2++)
+        for (int t = 0; t < 3; t++) {
+            Try &tr = tries[(size_t(s) * EXN + k2) * 3 + t];
+            tr.valid = 0; tr.q = INT_MAX;
+            if (k2 >= P.exact_n || uint32_t(k2) >= ne || E[k2].proxy < P.exact_min) continue;
+            if (t > E[k2].nalt) continue;
+            tr.valid = 1;
+            tr.sx = t == 0 ? E[k2].x : E[k2].ax[t - 1];
+            tr.sz = t == 0 ? E[k2].z : E[k2].az[t - 1];
+        }
+}
+// Nearest desert point of every exact-flood start: first of rings 0..8 (16 quarts apart) in (r, dz, dx) order
+// with state 2 (dsearch_desert.cpp:505-510).
+__global__ void __launch_bounds__(128) k_ring(const SeedNoise *__restrict__ noise, WorldDev w, Try *__restrict__ tries, const uint32_t *ctr) {
+    const uint64_t n = uint64_t(ctr[C_NS]) * EXN * 3 * RING;
+    for (uint64_t i = uint64_t(blockIdx.x) * blockDim.x + threadIdx.x; i < n; i += uint64_t(gridDim.x) * blockDim.x) {
+        const uint32_t slot = uint32_t(i / RING), q = uint32_t(i % RING);
+        const Try t = tries[slot];
+        if (!t.valid || int(q) >= __ldcg(&tries[slot].q)) continue;
+        const uint32_t s = slot / (EXN * 3);
+        if (desert_state(noise[s], w, t.sx + c_ring[q][0] * 16, t.sz + c_ring[q][1] * 16) == 2) atomicMin(&tries[slot].q, int(q));
+    }
+}
+__global__ void k_req_8(const Try *__restrict__ tries, uint32_t *ctr, FloodCtl *__restrict__ ctl, int32_t *__restrict__ f8) {
+    const uint32_t n = ctr[C_NS] * EXN * 3;
+    for (uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x) {
+        const Try t = tries[k];
+        f8[k] = -1;
+        if (!t.valid || t.q == INT_MAX) continue;
+        const uint32_t j = atomicAdd(ctr + C_NREQ + 2, 1u);
+        f8[k] = int32_t(j);
+        ctl[j] = make_ctl(t.sx + c_ring[t.q][0] * 16, t.sz + c_ring[t.q][1] * 16, 8, 16000 / 8, 1, DSG_PRED_DESERT, int32_t(k / (EXN * 3)), j);
+    }
+}
+// Thread per (seed, exact slot): the reference's retry loop (stop once a start reaches 0.6 x proxy) over the
+// step-8 floods, then a step-4 refinement request (dsearch_desert.cpp:511-523).
+__global__ void k_retry(const Try *__restrict__ tries, const int32_t *__restrict__ f8, const FloodStat *__restrict__ st8,
+                        const FloodCtl *__restrict__ ctl8, Eval *__restrict__ ev, const uint32_t *__restrict__ nev, Params P, uint32_t *ctr,
+                        FloodCtl *__restrict__ ctl4, int32_t *__restrict__ f4) {
+    const uint32_t n = ctr[C_NS] * EXN;
+    for (uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x) {
+        const uint32_t s = k / EXN, k2 = k % EXN;
+        f4[k] = -1;
+        if (!tries[k * 3].valid) continue;
+        Eval &e = ev[size_t(s) * EVC + k2];
+        double best8 = -1; int bx = e.x, bz = e.z; bool bedge = false;
+        for (int t = 0; t < 3; t++) {
+            const uint32_t slot = k * 3 + t;
+            if (!tries[slot].valid) continue;
+            if (best8 >= 0.6 * e.proxy) continue;
+            if (f8[slot] < 0) continue;
+            const FloodStat a = st8[f8[slot]];
+            const double v8 = a.cells * 64.0 * 16 / 1e6;
+            if (v8 > best8) { best8 = v8; bx = ctl8[f8[slot]].qx; bz = ctl8[f8[slot]].qz; bedge = a.edge != 0; }
+        }
+        e.exact = 1;
+        if (best8 < 0) { e.s8 = 0; e.nostart = 1; continue; }
+        e.x = bx; e.z = bz; e.s8 = best8; e.edge = bedge;
+        if (e.s8 >= P.refine_mb) {
+            const uint32_t j = atomicAdd(ctr + C_NREQ + 3, 1u);
+            f4[k] = int32_t(j);
+            ctl4[j] = make_ctl(bx, bz, 4, 16000 / 4, 0, DSG_PRED_DESERT, int32_t(s), j);
+        }
+    }
+}
+// Thread per seed: step-4 areas, the seed's best exact area, its seeds.csv record and its CSV rows.
+__global__ void k_results(const uint64_t *__restrict__ seeds, const SeedNoise *__restrict__ noise, const float *__restrict__ mx,
+                          const uint32_t *__restrict__ nbuck, const uint32_t *__restrict__ nsites, const Site *__restrict__ sites,
+                          Eval *__restrict__ ev, const uint32_t *__restrict__ nev, const int32_t *__restrict__ f4, const FloodStat *__restrict__ st4,
+                          Params P, dsg_search_seed *__restrict__ out, dsg_search_row *__restrict__ rows, uint32_t *ctr) {
+    const uint32_t s = blockIdx.x * blockDim.x + threadIdx.x;
+    if (s >= ctr[C_NS]) return;
+    Eval *E = ev + size_t(s) * EVC;
+    const uint32_t ne = nev[s];
+    double best = 0;
+    for (int k2 = 0; k2 < EXN && uint32_t(k2) < ne; k2++) {
+        Eval &e = E[k2];
+        const int32_t j = f4[s * EXN + k2];
+        if (j >= 0) { e.s4 = st4[j].cells * 16.0 * 16 / 1e6; e.edge |= st4[j].edge != 0; }
+        if (!e.exact || e.nostart) continue;
+        best = fmax(best, e.s4 > 0 ? e.s4 : e.s8);
+    }
+    uint32_t nr = 0;
+    for (uint32_t k = 0; k < ne; k++) nr += !(E[k].proxy < P.csv_min && E[k].s8 <= 0 && E[k].s4 <= 0);
+    uint32_t at = nr ? atomicAdd(ctr + C_ROWS, nr) : 0;
+    if (at + nr > ROWCAP) { atomicOr(ctr + C_FLAGS, F_ROWS); nr = 0; }
+    dsg_search_seed &o = out[s];
+    o.seed = seeds[s];
+    o.fya = noise[s].oct[0].fy; o.fyb = noise[s].oct[2].fy;       // octave -10 of the temperature, sides A and B
+    o.maxta = mx[2 * s]; o.maxtb = mx[2 * s + 1];
+    o.candidates = nbuck[s]; o.sites = nsites[s]; o.best = best; o.row0 = at; o.nrows = nr;
+    if (!nr) return;
+    for (uint32_t k = 0; k < ne; k++) {
+        const Eval &e = E[k];
+        if (e.proxy < P.csv_min && e.s8 <= 0 && e.s4 <= 0) continue;
+        const Site &st = sites[size_t(s) * MS + e.rank];
+        dsg_search_row &r = rows[at++];
+        r.seed = seeds[s]; r.rank = e.rank; r.x = e.x; r.z = e.z;
+        r.score = st.s; r.t0 = st.t; r.c0 = st.c; r.e0 = st.e;
+        r.proxy = e.proxy; r.s8 = e.s8; r.s4 = e.s4; r.hot = e.hot;
+        r.edge = e.edge; r.exact = e.exact && !e.nostart && k < uint32_t(P.exact_n) ? 1 : 0;
+    }
+}
+// Tiles taken in this wave back to zero (the next wave allocates from tile 0 again).
+__global__ void k_pool_zero(Tiles T, uint32_t *ctr, uint32_t cap) {
+    const uint32_t n = min(ctr[C_TAKEN], cap);
+    for (uint64_t i = uint64_t(blockIdx.x) * blockDim.x + threadIdx.x; i < uint64_t(n) * TILE_U64; i += uint64_t(gridDim.x) * blockDim.x) T.bits[i] = 0;
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) { T.emask[i] = 0; T.qmask[i] = 0; T.mark[i] = 0; }
+}
+__global__ void k_wave_end(uint32_t *ctr) { ctr[C_TAKEN] = 0; ctr[C_BASE] = 0; }
+
+// ---------------------------------------------------------------- host side
+template <class T> T *dalloc(size_t n) {
+    T *p = nullptr;
+    DSG_CU(cudaMalloc(&p, std::max<size_t>(n, 1) * sizeof(T)));
+    return p;
+}
+
+struct Phase { FloodCtl *ctl; FloodStat *st; int32_t *dir; uint32_t per_req; uint32_t cap; };
+
+struct Pipeline {
+    std::mutex mu;
+    bool open = false;
+    Params P{};
+    dsg_gate_cfg gcfg{};
+    uint64_t wave = 0;
+    uint32_t min_cells = 1;
+    cudaStream_t st = nullptr, body_st = nullptr;
+    gate::Lane *lane = nullptr;
+    uint32_t gcaps[3] = {0, 0, 0};
+    // device buffers
+    uint32_t *ctr = nullptr;
+    uint64_t *seeds = nullptr; SeedNoise *noise = nullptr;
+    void *tabin = nullptr; float *tab = nullptr, *mx = nullptr; int32_t *act = nullptr; uint32_t *nact = nullptr;
+    dsg_cand *raw = nullptr; uint32_t *nraw = nullptr;
+    Site *sites = nullptr; uint32_t *nsites = nullptr, *nbuck = nullptr; Hot *hot = nullptr;
+    int32_t *f1 = nullptr, *f2 = nullptr, *f8 = nullptr, *f4 = nullptr;
+    uint32_t *meta1 = nullptr, *meta2 = nullptr;
+    Phase ph[4]{};
+    TilePool pool;
+    unsigned long long *evals = nullptr;
+    uint32_t *cov = nullptr, *nzone = nullptr, *zfirst = nullptr;
+    DZone *zslot = nullptr, *zones = nullptr; ZoneMeta *zmslot = nullptr, *zmeta = nullptr; uint2 *chunks = nullptr;
+    uint8_t *bits = nullptr; int32_t *par = nullptr, *rid = nullptr; zones::CompStat *cs = nullptr; uint64_t *khi = nullptr; uint32_t *klo = nullptr;
+    dsg_component *rec = nullptr; uint32_t *zcnt = nullptr, *zoff = nullptr, *zfill = nullptr, *zcomp = nullptr;
+    Eval *evu = nullptr, *ev = nullptr; uint32_t *nev = nullptr; int64_t *sig = nullptr; Try *tries = nullptr;
+    dsg_search_seed *out = nullptr; dsg_search_row *rows = nullptr;
+    int grid_eval = 0, grid_conn = 0;
+    cudaGraphExec_t exec = nullptr;
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    // pinned host copies
+    uint32_t *h_ctr = nullptr, *h_gcnt = nullptr; dsg_search_seed *h_out = nullptr; dsg_search_row *h_rows = nullptr; uint64_t *h_seeds = nullptr;
+};
+Pipeline &PL() { static Pipeline p; return p; }
+
+// One flood phase into the graph being captured on p.st: directory, round counters, request starts, the round
+// loop as a conditional WHILE node (body: 6 rounds and the loop control, captured on p.body_st), statistics.
+void capture_phase(Pipeline &p, int k) {
+    Phase &f = p.ph[k];
+    uint32_t *nreq = p.ctr + C_NREQ + k;
+    const TileAlloc ta{nullptr, 0, p.pool.cap, p.pool.cap, p.ctr + C_TAKEN, nullptr, nullptr};
+    k_dir_fill<<<4 * 148, 256, 0, p.st>>>(f.dir, nreq, f.per_req);
+    cudaStreamCaptureStatus cs;
+    cudaGraph_t g;
+    const cudaGraphNode_t *deps = nullptr;
+    size_t ndeps = 0;
+    DSG_CU(cudaStreamGetCaptureInfo(p.st, &cs, nullptr, &g, &deps, &ndeps));
+    cudaGraphConditionalHandle h;
+    DSG_CU(cudaGraphConditionalHandleCreate(&h, g, 0, cudaGraphCondAssignDefault));
+    k_phase_begin<<<1, 1, 0, p.st>>>(p.ctr, nreq, h);
+    k_req_start<<<64, 128, 0, p.st>>>(f.ctl, nreq, f.st, f.dir, p.pool.T, ta, p.pool.n_list[0], p.ctr);
+    DSG_CU(cudaGetLastError());
+    DSG_CU(cudaStreamGetCaptureInfo(p.st, &cs, nullptr, &g, &deps, &ndeps));
+    cudaGraphNodeParams np{};
+    np.type = cudaGraphNodeTypeConditional;
+    np.conditional.handle = h;
+    np.conditional.type = cudaGraphCondTypeWhile;
+    np.conditional.size = 1;
+    cudaGraphNode_t node;
+    DSG_CU(cudaGraphAddNode(&node, g, deps, ndeps, &np));
+    cudaGraph_t body = np.conditional.phGraph_out[0];
+    DSG_CU(cudaStreamUpdateCaptureDependencies(p.st, &node, 1, cudaStreamSetCaptureDependencies));
+    DSG_CU(cudaStreamBeginCaptureToGraph(p.body_st, body, nullptr, nullptr, 0, cudaStreamCaptureModeRelaxed));
+    for (uint32_t r = 0; r < 6; r++)
+        launch_round(p.pool, r, p.ctr + C_ROUND, nullptr, p.ctr + C_FERR, p.evals, f.ctl, p.noise, f.dir, f.st, ta, p.grid_eval, p.grid_conn,
+                     p.body_st, p.ctr + C_BASE);
+    k_loop_ctl<<<1, 1, 0, p.body_st>>>(p.ctr, h);
+    DSG_CU(cudaGetLastError());
+    cudaGraph_t body_out = nullptr;
+    DSG_CU(cudaStreamEndCapture(p.body_st, &body_out));
+    k_tile_finish<<<dim3(f.cap, dir_chunks(f.per_req)), 256, 0, p.st>>>(f.ctl, nullptr, f.dir, p.pool.T, f.st, nreq);
+    k_phase_end<<<1, 1, 0, p.st>>>(p.ctr);
+    DSG_CU(cudaGetLastError());
+}
+
+// Everything of a wave after the gate, as one graph.
+void capture_wave(Pipeline &p) {
+    DSG_CU(cudaStreamBeginCapture(p.st, cudaStreamCaptureModeRelaxed));
+    uint32_t caps[3];
+    gate::lane_caps(p.lane, caps);
+    k_begin<<<8, 128, 0, p.st>>>(gate::lane_counts(p.lane), caps[0], caps[1], caps[2], gate::lane_survivors(p.lane), p.seeds, p.ctr);
+    seed_noise_build_dev(p.seeds, p.ctr + C_NS, SC, p.noise, p.st);
+    scan_seeds_device(p.noise, p.ctr + C_NS, SC, p.tabin, p.tab, p.mx, p.act, p.nact, p.raw, p.nraw, RAWCAP, p.P.sp, p.st);
+    DSG_CU(cudaFuncSetAttribute(k_nms, cudaFuncAttributeMaxDynamicSharedMemorySize, int(NMS_SMEM)));
+    k_nms<<<SC, NMS_THREADS, NMS_SMEM, p.st>>>(p.raw, p.nraw, p.P, p.sites, p.nsites, p.nbuck, p.ctr);
+    k_hot<<<4 * 148, 256, 0, p.st>>>(p.noise, p.sites, p.nsites, p.ctr, p.hot);
+    k_req_pre<<<4 * 148, 256, 0, p.st>>>(p.hot, p.nsites, p.ctr, p.ph[0].ctl, p.meta1, p.f1, p.f2);
+    DSG_CU(cudaGetLastError());
+    capture_phase(p, 0);
+    k_req_128<<<4 * 148, 256, 0, p.st>>>(p.ph[0].st, p.ph[0].ctl, p.meta1, p.P, p.ctr, p.ph[1].ctl, p.meta2, p.f2);
+    capture_phase(p, 1);
+    k_cover<<<(SC + 63) / 64, 64, 0, p.st>>>(p.hot, p.nsites, p.f1, p.f2, FloodView{p.ph[0].ctl, p.ph[0].dir}, FloodView{p.ph[1].ctl, p.ph[1].dir},
+                                               p.ph[0].st, p.ph[1].st, p.pool.T, p.P, p.cov, p.nzone, p.zslot, p.zmslot, p.ctr);
+    k_zone_list<<<1, LIST_THREADS, 0, p.st>>>(p.nzone, p.zslot, p.zmslot, p.zfirst, p.zones, p.zmeta, p.chunks, p.ctr);
+    DSG_CU(cudaGetLastError());
+    proxy_components_device(p.noise, p.zones, zones::ZoneWork{p.chunks, p.ctr + C_CHUNKS}, 8 * 148, p.bits, p.par, p.rid, p.cs, p.khi, p.klo,
+                            p.rec, p.ctr + C_PROXY, p.min_cells, p.st);
+    DSG_CU(cudaMemsetAsync(p.zcnt, 0, size_t(ZCAP + 1) * 4, p.st));
+    DSG_CU(cudaMemsetAsync(p.zfill, 0, size_t(ZCAP + 1) * 4, p.st));
+    k_comp_count<<<64, 256, 0, p.st>>>(p.rec, p.ctr, p.zcnt);
+    k_comp_offsets<<<1, LIST_THREADS, 0, p.st>>>(p.zcnt, p.zoff, p.ctr);
+    k_comp_scatter<<<64, 256, 0, p.st>>>(p.rec, p.ctr, p.zoff, p.zfill, p.zcomp);
+    k_evals<<<(SC + 63) / 64, 64, 0, p.st>>>(p.zfirst, p.zones, p.zmeta, p.zoff, p.zcomp, p.rec, p.P, p.evu, p.ev, p.nev, p.sig, p.tries,
+                                              p.ctr);
+    k_ring<<<8 * 148, 128, 0, p.st>>>(p.noise, world_dev(), p.tries, p.ctr);
+    k_req_8<<<32, 256, 0, p.st>>>(p.tries, p.ctr, p.ph[2].ctl, p.f8);
+    DSG_CU(cudaGetLastError());
+    capture_phase(p, 2);
+    k_retry<<<16, 256, 0, p.st>>>(p.tries, p.f8, p.ph[2].st, p.ph[2].ctl, p.ev, p.nev, p.P, p.ctr, p.ph[3].ctl, p.f4);
+    capture_phase(p, 3);
+    k_results<<<(SC + 127) / 128, 128, 0, p.st>>>(p.seeds, p.noise, p.mx, p.nbuck, p.nsites, p.sites, p.ev, p.nev, p.f4, p.ph[3].st, p.P, p.out,
+                                                   p.rows, p.ctr);
+    k_pool_zero<<<8 * 148, 256, 0, p.st>>>(p.pool.T, p.ctr, p.pool.cap);
+    k_wave_end<<<1, 1, 0, p.st>>>(p.ctr);
+    DSG_CU(cudaGetLastError());
+    cudaGraph_t g = nullptr;
+    DSG_CU(cudaStreamEndCapture(p.st, &g));
+    DSG_CU(cudaGraphInstantiate(&p.exec, g, 0));
+    DSG_CU(cudaGraphDestroy(g));
+}
+}  // namespace search
+}  // namespace dsg
+
+using namespace dsg;
+using namespace dsg::search;
+
+extern "C" int dsg_search_open(const dsg_search_params *q) {
+    return guarded([&] {
+        DSG_ARG(q, "dsg_search_open: null pointer");
+        DSG_ARG(q->max_sites > 0 && uint32_t(q->max_sites) <= MS, "dsg_search_open: max_sites must be 1..300");
+        DSG_ARG(q->exact_n >= 0 && q->exact_n <= EXN, "dsg_search_open: exact_n must be 0..2");
+        DSG_ARG(q->nms > 0 && q->hot_min > 0 && q->hot_pre > 0, "dsg_search_open: needs nms > 0, hot_min > 0 and hot_pre > 0");
+        Pipeline &p = PL();
+        std::lock_guard<std::mutex> l(p.mu);
+        require_init();
+        DSG_ARG(!p.open, "dsg_search_open: already open");
+        Params &P = p.P;
+        P.sp = {q->ta, q->t, q->wc, q->we};
+        P.max_sites = q->max_sites; P.nms = q->nms; P.exact_n = q->exact_n;
+        P.hot_min = q->hot_min; P.hot_pre = q->hot_pre; P.exact_min = q->exact_min; P.refine_mb = q->refine_mb; P.csv_min = q->csv_min;
+        p.gcfg = {q->gate_phase, q->gate_pthr, q->gate_amp, 0};
+        p.wave = q->wave ? q->wave : (uint64_t(1) << 22);
+        DSG_ARG(p.wave <= (uint64_t(1) << 26), "dsg_search_open: wave above 2^26 seed indices");
+        p.min_cells = 1;
+        while (p.min_cells * 32.0 * 32 * 16 / 1e6 < 1) p.min_cells++;
+        // exact-start rings r = 0..8 in (r, dz, dx) order
+        int8_t ring[RING][2]; int n = 0;
+        for (int r = 0; r <= 8; r++)
+            for (int dz = -r; dz <= r; dz++)
+                for (int dx = -r; dx <= r; dx++)
+                    if (std::max(std::abs(dx), std::abs(dz)) == r) { ring[n][0] = int8_t(dx); ring[n][1] = int8_t(dz); n++; }
+        DSG_CU(cudaMemcpyToSymbol(c_ring, ring, sizeof ring));
+        int lo, hi;
+        DSG_CU(cudaDeviceGetStreamPriorityRange(&lo, &hi));
+        DSG_CU(cudaStreamCreateWithPriority(&p.st, cudaStreamNonBlocking, hi));
+        DSG_CU(cudaStreamCreateWithFlags(&p.body_st, cudaStreamNonBlocking));
+        p.lane = gate::lane_create(p.wave);
+        gate::lane_caps(p.lane, p.gcaps);
+        p.ctr = dalloc<uint32_t>(C_N);
+        DSG_CU(cudaMemset(p.ctr, 0, C_N * 4));
+        p.seeds = dalloc<uint64_t>(SC); p.noise = dalloc<SeedNoise>(SC);
+        p.tabin = dalloc<char>(size_t(SC) * 6 * tabin_bytes());
+        p.tab = dalloc<float>(size_t(SC) * 6 * 512 * 512); p.mx = dalloc<float>(2 * SC);
+        p.act = dalloc<int32_t>(size_t(SC) * 512 * 512); p.nact = dalloc<uint32_t>(SC);
+        p.raw = dalloc<dsg_cand>(size_t(SC) * RAWCAP); p.nraw = dalloc<uint32_t>(SC);
+        p.sites = dalloc<Site>(size_t(SC) * MS); p.nsites = dalloc<uint32_t>(SC); p.nbuck = dalloc<uint32_t>(SC); p.hot = dalloc<Hot>(size_t(SC) * MS);
+        p.f1 = dalloc<int32_t>(size_t(SC) * MS); p.f2 = dalloc<int32_t>(size_t(SC) * MS);
+        p.meta1 = dalloc<uint32_t>(size_t(SC) * MS); p.meta2 = dalloc<uint32_t>(size_t(SC) * MS);
+        p.f8 = dalloc<int32_t>(TRIES); p.f4 = dalloc<int32_t>(SC * EXN);
+        const uint32_t caps[4] = {SC * MS, SC * MS, TRIES, SC * EXN};
+        const int steps[4] = {256, 128, 8, 4};
+        for (int k = 0; k < 4; k++) {
+            const int half = (k < 2 ? 32000 : 16000) / steps[k], tpr = (2 * half + 1 + TILE - 1) / TILE;
+            p.ph[k].per_req = uint32_t(tpr * tpr);
+            p.ph[k].cap = caps[k];
+            p.ph[k].ctl = dalloc<FloodCtl>(caps[k]); p.ph[k].st = dalloc<FloodStat>(caps[k]);
+            p.ph[k].dir = dalloc<int32_t>(size_t(caps[k]) * p.ph[k].per_req);
+        }
+        p.pool.allocate(POOL_TILES);
+        p.evals = dalloc<unsigned long long>(1);
+        round_grids(p.grid_eval, p.grid_conn);
+        p.cov = dalloc<uint32_t>(size_t(SC) * MS); p.nzone = dalloc<uint32_t>(SC); p.zfirst = dalloc<uint32_t>(SC + 1);
+        p.zslot = dalloc<DZone>(size_t(SC) * ZPS); p.zmslot = dalloc<ZoneMeta>(size_t(SC) * ZPS);
+        p.zones = dalloc<DZone>(ZCAP); p.zmeta = dalloc<ZoneMeta>(ZCAP); p.chunks = dalloc<uint2>(CHCAP);
+        p.bits = dalloc<uint8_t>(CELLCAP); p.par = dalloc<int32_t>(CELLCAP); p.rid = dalloc<int32_t>(CELLCAP);
+        p.cs = dalloc<zones::CompStat>(CELLCAP); p.khi = dalloc<uint64_t>(CELLCAP); p.klo = dalloc<uint32_t>(CELLCAP);
+        p.rec = dalloc<dsg_component>(CELLCAP);
+        p.zcnt = dalloc<uint32_t>(ZCAP + 1); p.zoff = dalloc<uint32_t>(ZCAP + 1); p.zfill = dalloc<uint32_t>(ZCAP + 1);
+        p.zcomp = dalloc<uint32_t>(CELLCAP);
+        p.evu = dalloc<Eval>(size_t(SC) * EVC); p.ev = dalloc<Eval>(size_t(SC) * EVC); p.nev = dalloc<uint32_t>(SC); p.sig = dalloc<int64_t>(size_t(SC) * EVC);
+        p.tries = dalloc<Try>(TRIES);
+        p.out = dalloc<dsg_search_seed>(SC); p.rows = dalloc<dsg_search_row>(ROWCAP);
+        DSG_CU(cudaMallocHost(&p.h_ctr, C_N * 4)); DSG_CU(cudaMallocHost(&p.h_gcnt, 16));
+        DSG_CU(cudaMallocHost(&p.h_out, SC * sizeof(dsg_search_seed))); DSG_CU(cudaMallocHost(&p.h_rows, ROWCAP * sizeof(dsg_search_row)));
+        DSG_CU(cudaMallocHost(&p.h_seeds, SC * 8));
+        DSG_CU(cudaEventCreate(&p.ev0)); DSG_CU(cudaEventCreate(&p.ev1));
+        DSG_CU(cudaDeviceSynchronize());
+        capture_wave(p);
+        p.open = true;
+        return DSG_OK;
+    });
+}
+
+namespace dsg {
+namespace search {
+// Output cursor of one run call.
+struct Out {
+    dsg_search_seed *seeds; uint32_t seed_cap, ns = 0;
+    dsg_search_row *rows; uint32_t row_cap, nr = 0;
+    uint64_t *unf; uint32_t unf_cap, nu = 0;
+    uint64_t tot[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+    bool over = false;
+    float ms = 0;
+};
+// The wave whose gated seeds are in the gate lane's survivor list (just enqueued on p.st): its graph, then its
+// records; a flagged wave hands its gated seeds back instead.
+void finish_wave(Pipeline &p, Out &o, uint64_t indices) {
+    DSG_CU(cudaGraphLaunch(p.exec, p.st));
+    DSG_CU(cudaMemcpyAsync(p.h_ctr, p.ctr, C_N * 4, cudaMemcpyDeviceToHost, p.st));
+    DSG_CU(cudaMemcpyAsync(p.h_gcnt, gate::lane_counts(p.lane), 16, cudaMemcpyDeviceToHost, p.st));
+    DSG_CU(cudaMemcpyAsync(p.h_out, p.out, SC * sizeof(dsg_search_seed), cudaMemcpyDeviceToHost, p.st));
+    DSG_CU(cudaStreamSynchronize(p.st));
+    const uint32_t wrows = std::min(p.h_ctr[C_ROWS], ROWCAP);
+    if (wrows) DSG_CU(cudaMemcpyAsync(p.h_rows, p.rows, size_t(wrows) * sizeof(dsg_search_row), cudaMemcpyDeviceToHost, p.st));
+    DSG_CU(cudaEventRecord(p.ev1, p.st));
+    DSG_CU(cudaStreamSynchronize(p.st));
+    float ms = 0;
+    DSG_CU(cudaEventElapsedTime(&ms, p.ev0, p.ev1));
+    o.ms += ms;
+    const uint32_t wS = p.h_ctr[C_NS];
+    o.tot[0] += indices; o.tot[1] += p.h_gcnt[0]; o.tot[2] += p.h_gcnt[1]; o.tot[3] += p.h_gcnt[2];
+    if (p.h_ctr[C_FLAGS]) {
+        o.tot[7] |= p.h_ctr[C_FLAGS];
+        if (p.h_ctr[C_FLAGS] & F_GATE) { set_error("device search: gate survivors exceed the wave's capacity"); throw ArgFail{}; }
+        DSG_CU(cudaMemcpy(p.h_seeds, p.seeds, size_t(wS) * 8, cudaMemcpyDeviceToHost));
+        for (uint32_t i = 0; i < wS; i++) {
+            if (o.nu < o.unf_cap) o.unf[o.nu] = p.h_seeds[i];
+            else o.over = true;
+            o.nu++;
+        }
+        return;
+    }
+    o.tot[4] += p.h_ctr[C_SITES]; o.tot[5] += p.h_ctr[C_NHOT]; o.tot[6] += p.h_ctr[C_NBIG];
+    for (uint32_t i = 0; i < wS; i++) {
+        dsg_search_seed rec = p.h_out[i];
+        const uint32_t r0 = rec.row0;
+        rec.row0 = o.nr;
+        for (uint32_t k = 0; k < rec.nrows; k++) {
+            if (o.nr < o.row_cap) o.rows[o.nr] = p.h_rows[r0 + k];
+            else o.over = true;
+            o.nr++;
+        }
+        if (o.ns < o.seed_cap) o.seeds[o.ns] = rec;
+        else o.over = true;
+        o.ns++;
+    }
+}
+int report(const Out &o, uint32_t *n_seeds, uint32_t *n_rows, uint32_t *n_unfinished, uint64_t counts[8], float *device_ms) {
+    *n_seeds = o.ns; *n_rows = o.nr; *n_unfinished = o.nu;
+    if (counts) std::memcpy(counts, o.tot, sizeof o.tot);
+    if (device_ms) *device_ms = o.ms;
+    if (o.over) { set_error("device search: output capacity exceeded"); return DSG_OVERFLOW; }
+    return DSG_OK;
+}
+}  // namespace search
+}  // namespace dsg
+
+extern "C" int dsg_search_run(uint64_t start, uint64_t count, dsg_search_seed *seeds_out, uint32_t seed_cap, uint32_t *n_seeds,
+                              dsg_search_row *rows_out, uint32_t row_cap, uint32_t *n_rows, uint64_t *unfinished, uint32_t unfinished_cap,
+                              uint32_t *n_unfinished, uint64_t counts[8], float *device_ms) {
+    return guarded([&] {
+        DSG_ARG(n_seeds && n_rows && n_unfinished, "dsg_search_run: null pointer");
+        DSG_ARG((seed_cap == 0 || seeds_out) && (row_cap == 0 || rows_out) && (unfinished_cap == 0 || unfinished), "dsg_search_run: null output");
+        Pipeline &p = PL();
+        std::lock_guard<std::mutex> l(p.mu);
+        DSG_ARG(p.open, "dsg_search_run: dsg_search_open has not been called");
+        require_init();
+        Out o{seeds_out, seed_cap, 0, rows_out, row_cap, 0, unfinished, unfinished_cap, 0};
+        for (uint64_t base = 0; base < count; base += p.wave) {
+            const uint64_t nb = std::min(p.wave, count - base);
+            DSG_CU(cudaEventRecord(p.ev0, p.st));
+            gate::lane_enqueue(p.lane, p.st, start + base, nb, p.gcfg);
+            finish_wave(p, o, nb);
+        }
+        return report(o, n_seeds, n_rows, n_unfinished, counts, device_ms);
+    });
+}
+
+extern "C" int dsg_search_seeds(const uint64_t *seeds, uint32_t n, dsg_search_seed *seeds_out, uint32_t seed_cap, uint32_t *n_seeds,
+                                dsg_search_row *rows_out, uint32_t row_cap, uint32_t *n_rows, uint64_t *unfinished, uint32_t unfinished_cap,
+                                uint32_t *n_unfinished, uint64_t counts[8], float *device_ms) {
+    return guarded([&] {
+        DSG_ARG(n_seeds && n_rows && n_unfinished && (n == 0 || seeds), "dsg_search_seeds: null pointer");
+        DSG_ARG((seed_cap == 0 || seeds_out) && (row_cap == 0 || rows_out) && (unfinished_cap == 0 || unfinished), "dsg_search_seeds: null output");
+        Pipeline &p = PL();
+        std::lock_guard<std::mutex> l(p.mu);
+        DSG_ARG(p.open, "dsg_search_seeds: dsg_search_open has not been called");
+        require_init();
+        Out o{seeds_out, seed_cap, 0, rows_out, row_cap, 0, unfinished, unfinished_cap, 0};
+        uint64_t *surv = const_cast<uint64_t *>(gate::lane_survivors(p.lane));
+        for (uint32_t base = 0; base < n; base += SC) {
+            const uint32_t nb = std::min<uint32_t>(SC, n - base);
+            DSG_CU(cudaEventRecord(p.ev0, p.st));
+            // the seeds take the place of the gate's survivors: counts {0, 0, nb}
+            std::memcpy(p.h_seeds, seeds + base, size_t(nb) * 8);
+            p.h_gcnt[0] = 0; p.h_gcnt[1] = 0; p.h_gcnt[2] = nb; p.h_gcnt[3] = 0;
+            DSG_CU(cudaMemcpyAsync(surv, p.h_seeds, size_t(nb) * 8, cudaMemcpyHostToDevice, p.st));
+            DSG_CU(cudaMemcpyAsync(gate::lane_counts(p.lane), p.h_gcnt, 16, cudaMemcpyHostToDevice, p.st));
+            finish_wave(p, o, nb);
+        }
+        return report(o, n_seeds, n_rows, n_unfinished, counts, device_ms);
+    });
+}
+
+extern "C" int dsg_search_close(void) {
+    return guarded([&] {
+        Pipeline &p = PL();
+        std::lock_guard<std::mutex> l(p.mu);
+        if (!p.open) return DSG_OK;
+        DSG_CU(cudaStreamSynchronize(p.st));
+        cudaGraphExecDestroy(p.exec); p.exec = nullptr;
+        void *bufs[] = {p.ctr, p.seeds, p.noise, p.tabin, p.tab, p.mx, p.act, p.nact, p.raw, p.nraw, p.sites, p.nsites, p.nbuck, p.hot,
+                        p.f1, p.f2, p.f8, p.f4, p.meta1, p.meta2, p.evals, p.cov, p.nzone, p.zfirst, p.zslot, p.zmslot, p.zones, p.zmeta,
+                        p.chunks, p.bits, p.par, p.rid, p.cs, p.khi, p.klo, p.rec, p.zcnt, p.zoff, p.zfill, p.zcomp, p.evu, p.ev, p.nev,
+                        p.sig, p.tries, p.out, p.rows};
+        for (void *b : bufs) cudaFree(b);
+        for (Phase &f : p.ph) { cudaFree(f.ctl); cudaFree(f.st); cudaFree(f.dir); f = Phase{}; }
+        p.pool.release();
+        cudaFreeHost(p.h_ctr); cudaFreeHost(p.h_gcnt); cudaFreeHost(p.h_out); cudaFreeHost(p.h_rows); cudaFreeHost(p.h_seeds);
+        cudaEventDestroy(p.ev0); cudaEventDestroy(p.ev1);
+        cudaStreamDestroy(p.st); cudaStreamDestroy(p.body_st);
+        p.open = false;
+        return DSG_OK;
+    });
+}

@@ -121,9 +121,11 @@ __device__ __forceinline__ void vblur_any(int ph, const float *ringc, const floa
 
 // Tables tab0 .. tab0 + gridDim.y - 1 of seed blockIdx.z, band blockIdx.x of gridDim.x; out = the blurred
 // tables [seed][6][512][512]; mx[seed][2] = the maxima of the two T tables (atomic, preset by the caller).
+// n_dev (may be null): the number of seeds, counted on the device; the grid covers a capacity.
 template <int R>
 __global__ void __launch_bounds__(TN, Band<R>::BLOCKS) k_tables(const TabIn *__restrict__ tin, float *__restrict__ out, float *__restrict__ mx,
-                                                              TableTaps taps, int tab0) {
+                                                              TableTaps taps, int tab0, const uint32_t *__restrict__ n_dev) {
+    if (n_dev && blockIdx.z >= *n_dev) return;
     using B = Band<R>;
     extern __shared__ __align__(16) float dsm[];
     __shared__ uint8_t PO[PL];                                      // see tab_chunk
@@ -193,7 +195,9 @@ __global__ void __launch_bounds__(TN, Band<R>::BLOCKS) k_tables(const TabIn *__r
 }
 
 // Active side-A T cells (TA >= ta), compacted per seed in row-major order of discovery.
-__global__ void k_active(const float *__restrict__ tabs, float ta, int32_t *__restrict__ act, uint32_t *__restrict__ nact) {
+__global__ void k_active(const float *__restrict__ tabs, float ta, int32_t *__restrict__ act, uint32_t *__restrict__ nact,
+                         const uint32_t *__restrict__ n_dev) {
+    if (n_dev && blockIdx.y >= *n_dev) return;
     const int cell = blockIdx.x * blockDim.x + threadIdx.x, sd = blockIdx.y;
     const bool on = tabs[size_t(sd) * 6 * TN * TN + cell] >= ta;
     const uint32_t m = __ballot_sync(0xffffffffu, on);
@@ -208,7 +212,9 @@ __global__ void k_active(const float *__restrict__ tabs, float ta, int32_t *__re
 // Translation scan of one active cell (dsearch_desert.cpp:257-280): thread = (tz, tx) pair.
 __global__ void __launch_bounds__(256) k_scan(const float *__restrict__ tabs, const int32_t *__restrict__ act, const uint32_t *__restrict__ nact,
         const int16_t *__restrict__ ibT, const int16_t *__restrict__ ibC, const int8_t *__restrict__ loT, const int8_t *__restrict__ hiT,
-        dsg_scan_params sp, ScanConst sc, Cand *__restrict__ out, uint32_t *__restrict__ ncand, uint32_t cap) {
+        dsg_scan_params sp, ScanConst sc, Cand *__restrict__ out, uint32_t *__restrict__ ncand, uint32_t cap,
+        const uint32_t *__restrict__ n_dev) {
+    if (n_dev && blockIdx.y >= *n_dev) return;
     const int sd = blockIdx.y;
     const uint32_t na = nact[sd];
     for (uint32_t a = blockIdx.x; a < na; a += gridDim.x) {
@@ -240,9 +246,10 @@ constexpr int SCAN_BLOCKS = 512;                    // CTAs per seed of k_scan
 // host (lowfield.hpp:14-33; octave 0 of each side of channels T, C, E, weight factor * amplitude).  Block =
 // (seed, table); thread x = permutation entry x, column-hash entries x of both y offsets, and corner terms
 // x and x + 256 in [px][pz][c][h] order.  The double-precision expressions are the host's, in its order.
-__global__ void __launch_bounds__(256) k_tabins(const SeedNoise *__restrict__ noise, TabIn *__restrict__ out) {
+__global__ void __launch_bounds__(256) k_tabins(const SeedNoise *__restrict__ noise, TabIn *__restrict__ out, const uint32_t *__restrict__ n_dev) {
     constexpr int CH[3] = {CH_T, CH_C, CH_E};
     const uint32_t s = blockIdx.x / 6, k = blockIdx.x % 6;
+    if (n_dev && s >= *n_dev) return;
     const SeedNoise &S = noise[s];
     const int ch = CH[k / 2], idx = S.off[ch] + int(k & 1) * S.cnt[ch];
     const NOct &p = S.oct[idx];
@@ -298,10 +305,14 @@ void ensure(State &g, uint32_t seeds, uint32_t cap) {
     g.cap_seeds = ns; g.cap_cand = nc;
 }
 
+// Where one launch of the tables reads and writes: inputs, tables, maxima, stream, and the seed count when it
+// lives on the device (null: the grid's seed count is exact).
+struct TabJob { const ScanConst &sc; const TabIn *in; float *tab, *mx; cudaStream_t st; const uint32_t *n_dev; };
+
 // k_tables for radius R over tables tab0 .. tab0 + ntab - 1 of S seeds.  Bands per table: the fewest (1 to 8)
 // that give at least four waves of CTAs, so that the tail of the grid stays short.
 template <int R>
-void tables_radius(State &g, uint32_t S, int tab0, int ntab) {
+void tables_radius(const TabJob &j, uint32_t S, int tab0, int ntab) {
     using B = Band<R>;
     static const int slots = [] {
         DSG_CU(cudaFuncSetAttribute(k_tables<R>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(B::SMEM)));
@@ -312,20 +323,21 @@ void tables_radius(State &g, uint32_t S, int tab0, int ntab) {
     int split = 1;
     while (split < 8 && uint64_t(S) * ntab * split < uint64_t(4) * slots) split *= 2;
     TableTaps tp{};
-    std::copy(g.sc.kT, g.sc.kT + 2 * RMAX + 1, tp.k[0]);
-    std::copy(g.sc.kC, g.sc.kC + 2 * RMAX + 1, tp.k[1]);
-    k_tables<R><<<dim3(split, ntab, S), TN, B::SMEM, g.st>>>(g.d_in, g.d_tab, g.d_mx, tp, tab0);
+    std::copy(j.sc.kT, j.sc.kT + 2 * RMAX + 1, tp.k[0]);
+    std::copy(j.sc.kC, j.sc.kC + 2 * RMAX + 1, tp.k[1]);
+    k_tables<R><<<dim3(split, ntab, S), TN, B::SMEM, j.st>>>(j.in, j.tab, j.mx, tp, tab0, j.n_dev);
 }
 template <int... R>
-void tables_any(int r, State &g, uint32_t S, int tab0, int ntab, std::integer_sequence<int, R...>) {
-    ((r == R ? tables_radius<R>(g, S, tab0, ntab) : void()), ...);
+void tables_any(int r, const TabJob &j, uint32_t S, int tab0, int ntab, std::integer_sequence<int, R...>) {
+    ((r == R ? tables_radius<R>(j, S, tab0, ntab) : void()), ...);
 }
 // All six tables of S seeds: one launch when the T and C/E blurs have the same radius, else one per radius.
-void launch_tables(State &g, uint32_t S) {
+void launch_tables(const TabJob &j, uint32_t S) {
     constexpr auto radii = std::make_integer_sequence<int, RMAX + 1>{};
-    if (g.sc.rT == g.sc.rC) tables_any(g.sc.rT, g, S, 0, 6, radii);
-    else { tables_any(g.sc.rT, g, S, 0, 2, radii); tables_any(g.sc.rC, g, S, 2, 4, radii); }
+    if (j.sc.rT == j.sc.rC) tables_any(j.sc.rT, j, S, 0, 6, radii);
+    else { tables_any(j.sc.rT, j, S, 0, 2, radii); tables_any(j.sc.rC, j, S, 2, 4, radii); }
 }
+void launch_tables(State &g, uint32_t S) { launch_tables(TabJob{g.sc, g.d_in, g.d_tab, g.d_mx, g.st, nullptr}, S); }
 
 // Tables + blur + max (+ active list and scan if want_scan) for S seeds already in g.d_in; on g.st.
 void enqueue(State &g, uint32_t S, const dsg_scan_params *sp, uint32_t cap, bool want_scan) {
@@ -336,12 +348,38 @@ void enqueue(State &g, uint32_t S, const dsg_scan_params *sp, uint32_t cap, bool
     if (want_scan) {
         DSG_CU(cudaMemsetAsync(g.d_nact, 0, size_t(S) * 4, g.st));
         DSG_CU(cudaMemsetAsync(g.d_ncand, 0, size_t(S) * 4, g.st));
-        k_active<<<dim3(TN * TN / 256, S), 256, 0, g.st>>>(g.d_tab, sp->ta, g.d_act, g.d_nact);
-        k_scan<<<dim3(SCAN_BLOCKS, S), 256, 0, g.st>>>(g.d_tab, g.d_act, g.d_nact, g.d_ibT, g.d_ibC, g.d_loT, g.d_hiT, *sp, g.sc, g.d_out, g.d_ncand, cap);
+        k_active<<<dim3(TN * TN / 256, S), 256, 0, g.st>>>(g.d_tab, sp->ta, g.d_act, g.d_nact, nullptr);
+        k_scan<<<dim3(SCAN_BLOCKS, S), 256, 0, g.st>>>(g.d_tab, g.d_act, g.d_nact, g.d_ibT, g.d_ibC, g.d_loT, g.d_hiT, *sp, g.sc, g.d_out, g.d_ncand, cap,
+                                                       nullptr);
     }
     DSG_CU(cudaGetLastError());
 }
+__global__ void k_fill_f32(float *__restrict__ p, float v, uint32_t n) {
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) p[i] = v;
+}
 }  // namespace tables
+
+// Tables, blur, maxima, active cells and the translation scan for seeds whose noise tables and count are on the
+// device (the device-resident searcher): grids cover cap_seeds, blocks of seeds at or beyond *n_dev return at
+// once.  Needs dsg_scan_init.  cand holds cap candidates per seed (dsg_cand layout), ncand the counts (a count
+// above cap means the seed overflowed).  Everything is enqueued on st.
+void scan_seeds_device(const SeedNoise *noise, const uint32_t *n_dev, uint32_t cap_seeds, void *tabin, float *tab, float *mx, int32_t *act,
+                       uint32_t *nact, dsg_cand *cand, uint32_t *ncand, uint32_t cap, const dsg_scan_params &sp, cudaStream_t st) {
+    using namespace tables;
+    State &g = S();
+    if (!g.init) { set_error("device searcher: dsg_scan_init has not been called"); throw ArgFail{}; }
+    TabIn *in = static_cast<TabIn *>(tabin);
+    k_tabins<<<6 * cap_seeds, 256, 0, st>>>(noise, in, n_dev);
+    k_fill_f32<<<64, 256, 0, st>>>(mx, -1e30f, 2 * cap_seeds);
+    launch_tables(TabJob{g.sc, in, tab, mx, st, n_dev}, cap_seeds);
+    DSG_CU(cudaMemsetAsync(nact, 0, size_t(cap_seeds) * 4, st));
+    DSG_CU(cudaMemsetAsync(ncand, 0, size_t(cap_seeds) * 4, st));
+    k_active<<<dim3(TN * TN / 256, cap_seeds), 256, 0, st>>>(tab, sp.ta, act, nact, n_dev);
+    k_scan<<<dim3(SCAN_BLOCKS, cap_seeds), 256, 0, st>>>(tab, act, nact, g.d_ibT, g.d_ibC, g.d_loT, g.d_hiT, sp, g.sc,
+                                                         reinterpret_cast<Cand *>(cand), ncand, cap, n_dev);
+    DSG_CU(cudaGetLastError());
+}
+size_t tabin_bytes() { return sizeof(tables::TabIn); }
 }  // namespace dsg
 
 using namespace dsg;
@@ -437,7 +475,7 @@ extern "C" int dsg_scan_seeds(const uint64_t *seeds, uint32_t nseeds, const dsg_
         ensure(g, nseeds, dcap);
         DSG_CU(cudaMemcpyAsync(g.d_seeds, seeds, size_t(nseeds) * 8, cudaMemcpyHostToDevice, g.st));
         seed_noise_build(g.d_seeds, nseeds, g.d_noise, g.st);
-        k_tabins<<<6 * nseeds, 256, 0, g.st>>>(g.d_noise, g.d_in);
+        k_tabins<<<6 * nseeds, 256, 0, g.st>>>(g.d_noise, g.d_in, nullptr);
         DSG_CU(cudaGetLastError());
         enqueue(g, nseeds, sp, dcap, true);
         return collect(g, nseeds, maxt, out, cap, dcap, n);

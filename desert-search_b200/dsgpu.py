@@ -305,3 +305,53 @@ def query(seeds, pseed, kind, xz):
     _ck(lib.dsg_query_batch(ptr(s, u64p), C.c_uint32(len(s)), ptr(p, u32p), C.c_int(kind), ptr(xz, i32p), C.c_uint32(len(xz)),
                             ptr(out, f64p)), "dsg_query_batch")
     return out
+
+
+# ---------------------------------------------------------------- device-resident search (dsg_search_*)
+class SearchParams(C.Structure):
+    _fields_ = [("gate_phase", C.c_float), ("gate_pthr", C.c_float), ("gate_amp", C.c_float),
+                ("ta", C.c_float), ("t", C.c_float), ("wc", C.c_float), ("we", C.c_float),
+                ("max_sites", C.c_int32), ("nms", C.c_int32), ("exact_n", C.c_int32),
+                ("hot_min", C.c_double), ("hot_pre", C.c_double), ("exact_min", C.c_double), ("refine_mb", C.c_double),
+                ("csv_min", C.c_double), ("wave", C.c_uint64)]
+
+
+SEARCH_SEED = np.dtype([("seed", "<u8"), ("fya", "<f8"), ("fyb", "<f8"), ("maxta", "<f4"), ("maxtb", "<f4"), ("candidates", "<u4"),
+                        ("sites", "<u4"), ("best", "<f8"), ("row0", "<u4"), ("nrows", "<u4")], align=True)
+SEARCH_ROW = np.dtype([("seed", "<u8"), ("rank", "<u4"), ("x", "<i4"), ("z", "<i4"), ("score", "<f4"), ("t0", "<f4"), ("c0", "<f4"),
+                       ("e0", "<f4"), ("proxy", "<f8"), ("s8", "<f8"), ("s4", "<f8"), ("hot", "<f8"), ("edge", "<i4"), ("exact", "<i4")],
+                      align=True)
+# the searcher's Params defaults (dsearch_desert.cpp:50-78) for the production command line gate=1 gpu=1 gscan=1
+SEARCH_DEFAULTS = dict(gate_phase=0.06, gate_pthr=0.645, gate_amp=0.70, ta=0.25, t=0.55, wc=0.25, we=0.41, max_sites=300, nms=5000,
+                       exact_n=2, hot_min=180.0, hot_pre=0.8, exact_min=75.0, refine_mb=70.0, csv_min=50.0, wave=0)
+
+
+def search_open(**kw):
+    """Open the device-resident pipeline (dsg_search_open) with the searcher's defaults overridden by kw."""
+    p = dict(SEARCH_DEFAULTS, **kw)
+    _ck(lib.dsg_search_open(C.byref(SearchParams(**p))), "dsg_search_open")
+
+
+def search_close():
+    _ck(lib.dsg_search_close(), "dsg_search_close")
+
+
+def _search_call(fn, args, seed_cap, row_cap):
+    recs = np.zeros(seed_cap, dtype=SEARCH_SEED); rows = np.zeros(row_cap, dtype=SEARCH_ROW); unf = np.zeros(seed_cap, dtype=np.uint64)
+    ns, nr, nu = C.c_uint32(), C.c_uint32(), C.c_uint32()
+    counts = np.zeros(8, dtype=np.uint64); ms = C.c_float()
+    rc = _ck(fn(*args, recs.ctypes.data_as(C.c_void_p), C.c_uint32(seed_cap), C.byref(ns), rows.ctypes.data_as(C.c_void_p), C.c_uint32(row_cap),
+                C.byref(nr), ptr(unf, u64p), C.c_uint32(seed_cap), C.byref(nu), ptr(counts, u64p), C.byref(ms)), fn.__name__)
+    assert rc == DSG_OK, "output capacity exceeded"
+    return recs[:ns.value].copy(), rows[:nr.value].copy(), unf[:nu.value].copy(), [int(x) for x in counts], ms.value
+
+
+def search_run(start, count, seed_cap=1 << 16, row_cap=1 << 18):
+    """Seeds mix(start + k), k < count, through the device pipeline: (seed records, rows, unfinished seeds, counts, device ms)."""
+    return _search_call(lib.dsg_search_run, (C.c_uint64(start), C.c_uint64(count)), seed_cap, row_cap)
+
+
+def search_seeds(seeds, row_cap=1 << 18):
+    """Explicit gated seeds through the device pipeline (dsg_search_seeds); returns as search_run."""
+    s = np.ascontiguousarray(seeds, dtype=np.uint64)
+    return _search_call(lib.dsg_search_seeds, (ptr(s, u64p), C.c_uint32(len(s))), max(1, len(s)), row_cap)

@@ -53,6 +53,7 @@ struct Params {                                    // dsearch_desert.cpp:50-78 (
     double gate_phase = 0.06, gate_amp = 0.70, gate_pthr = 0.645;
     int from_stdin = 0;
     int verified = 0;                              // this build only: verify CANDIDATEs in-process (PREFIX.verified)
+    int fused = 1;                                 // this build only: gate=1 runs on the device-resident pipeline (0: per-stage path)
 };
 
 // A cell i of a side-A table translated by t periods -> B table cell (dsearch_desert.cpp:98-113).
@@ -105,6 +106,8 @@ struct Search {
 
     // ---- per-batch stages
     void process(const std::vector<uint64_t> &seeds);
+    void candidate(long long seed, double s4, int x, int z, uint64_t sd);
+    void emit_device(const dsg_search_seed &r, const dsg_search_row *rows);
     std::vector<Start> site_starts(const std::vector<uint64_t> &seeds, const std::vector<std::vector<Site>> &sites);
     void start_loop(const std::vector<uint64_t> &seeds, const std::vector<Start> &st, std::vector<std::vector<Eval>> &ev,
                     std::vector<CensusReq> &census);
@@ -490,20 +493,7 @@ void Search::process(const std::vector<uint64_t> &seeds) {
             if (e.nostart) continue;                       // no desert start near this component (:517)
             const double v = e.s4 > 0 ? e.s4 : e.s8;
             seed_best = std::max(seed_best, v);
-            if (e.s4 >= P.verify_mb) {
-                char line[256];
-                snprintf(line, sizeof line, "CANDIDATE step4=%.2fM seed=%lld x=%d z=%d -> verify with exact flood (Y=256)", e.s4, seed, e.x * 4 + 2, e.z * 4 + 2);
-                fprintf(stderr, "%s\n", line);
-                if (P.verified) {
-                    const int bx = e.x * 4 + 2, bz = e.z * 4 + 2;
-                    const dsg_flood_req q{seeds[s], bx >> 2, bz >> 2, 1, 20000, 0, DSG_PRED_DESERT, 0.f, 0};
-                    uint64_t ticket = 0;
-                    ck(dsg_service_submit(&q, &ticket), "verify submit");
-                    std::lock_guard<std::mutex> vl(vmu);
-                    vq.push_back({ticket, line, bx, bz});
-                    vcv.notify_all();
-                }
-            }
+            if (e.s4 >= P.verify_mb) candidate(seed, e.s4, e.x, e.z, seeds[s]);
             if (v > best) {
                 best = v;
                 fprintf(stderr, "best %.2fM (step %d) seed=%lld x=%d z=%d proxy=%.1fM\n", v, e.s4 > 0 ? 4 : 8, seed, e.x * 4 + 2, e.z * 4 + 2, e.proxy);
@@ -529,6 +519,44 @@ void Search::process(const std::vector<uint64_t> &seeds) {
                 passed.load() / std::chrono::duration<double>(now - begin).count(), t_tab.load(), t_scan.load(), t_site.load(), t_proxy.load(), t_hot.load(), t_gpu.load(),
                 (unsigned long long)nhot.load(), (unsigned long long)nbig.load());
     }
+}
+
+// A CANDIDATE line (dsearch_desert.cpp:528), and with verified=1 its exact flood on the flood service.  Called
+// with mu held.
+void Search::candidate(long long seed, double s4, int x, int z, uint64_t sd) {
+    char line[256];
+    snprintf(line, sizeof line, "CANDIDATE step4=%.2fM seed=%lld x=%d z=%d -> verify with exact flood (Y=256)", s4, seed, x * 4 + 2, z * 4 + 2);
+    fprintf(stderr, "%s\n", line);
+    if (!P.verified) return;
+    const int bx = x * 4 + 2, bz = z * 4 + 2;
+    const dsg_flood_req q{sd, bx >> 2, bz >> 2, 1, 20000, 0, DSG_PRED_DESERT, 0.f, 0};
+    uint64_t ticket = 0;
+    ck(dsg_service_submit(&q, &ticket), "verify submit");
+    std::lock_guard<std::mutex> vl(vmu);
+    vq.push_back({ticket, line, bx, bz});
+    vcv.notify_all();
+}
+
+// One seed finished by the device-resident pipeline: the same lines process() writes for it.
+void Search::emit_device(const dsg_search_seed &r, const dsg_search_row *rows) {
+    std::lock_guard<std::mutex> g(mu);
+    const long long seed = (long long)r.seed;
+    for (uint32_t k = 0; k < r.nrows; k++) {
+        const dsg_search_row &e = rows[k];
+        if (!e.exact) continue;
+        const double v = e.s4 > 0 ? e.s4 : e.s8;
+        if (e.s4 >= P.verify_mb) candidate(seed, e.s4, e.x, e.z, r.seed);
+        if (v > best) {
+            best = v;
+            fprintf(stderr, "best %.2fM (step %d) seed=%lld x=%d z=%d proxy=%.1fM\n", v, e.s4 > 0 ? 4 : 8, seed, e.x * 4 + 2, e.z * 4 + 2, e.proxy);
+        }
+    }
+    for (uint32_t k = 0; k < r.nrows; k++) {
+        const dsg_search_row &e = rows[k];
+        fprintf(out, "%lld,%.4f,%.4f,%.4f,%.4f,%u,%d,%d,%.4f,%.4f,%.4f,%.4f,%.3f,%.3f,%.3f,%d,%.1f\n", seed, r.fya, r.fyb, r.maxta, r.maxtb,
+                e.rank, e.x * 4 + 2, e.z * 4 + 2, e.score, e.t0, e.c0, e.e0, e.proxy, e.s8, e.s4, e.edge, e.hot);
+    }
+    fprintf(sout, "%lld,%.4f,%.4f,%.4f,%.4f,%u,%u,%.3f\n", seed, r.fya, r.fyb, r.maxta, r.maxtb, r.candidates, r.sites, r.best);
 }
 
 // Per-start proxy floods (dsearch_desert.cpp:367-423), used when hot_min <= 0: every site gets starts (the
@@ -708,7 +736,7 @@ int main(int argc, char **argv) {
         else if (k == "hot_pre") P.hot_pre = v; else if (k == "gate") P.gate = int(v); else if (k == "gscan") P.gscan = int(v);
         else if (k == "gscancheck") P.gscancheck = int(v); else if (k == "gate_phase") P.gate_phase = v; else if (k == "gate_amp") P.gate_amp = v;
         else if (k == "gate_pthr") P.gate_pthr = v; else if (k == "refine") P.refine_mb = v; else if (k == "verify") P.verify_mb = v;
-        else if (k == "verified") P.verified = int(v);
+        else if (k == "verified") P.verified = int(v); else if (k == "fused") P.fused = int(v);
         else { fprintf(stderr, "unknown key %s\n", k.c_str()); return 2; }
     }
     if ((P.gscan || P.gscancheck) && !P.gpu) { fprintf(stderr, "gscan=1 needs gpu=1\n"); return 2; }
@@ -759,10 +787,67 @@ int main(int argc, char **argv) {
     };
     std::thread source;
     std::atomic<double> gate_end{0};
-    if (P.from_stdin && !P.gate) {
+    // the device-resident pipeline covers the production configuration (hot zones with pre-floods, exact
+    // floods, no study census, no CPU cross-checks); other settings take the per-stage path
+    const bool fused = P.gpu && P.gscan && P.fused && (P.gate || P.from_stdin) && P.hot_min > 0 && P.hot_pre > 0 && !P.study &&
+                       !P.gscancheck && !P.gpucheck && P.max_sites >= 1 && P.max_sites <= 300 && P.exact_n >= 0 && P.exact_n <= 2 && P.nms > 0;
+    if (P.from_stdin && !P.gate && !fused) {
         source = std::thread([&] {
             char line[256];
             while (!interrupted && fgets(line, sizeof line, stdin)) push(std::strtoull(line, nullptr, 10));
+            gate_end = std::chrono::duration<double>(Clock::now() - S.begin).count();
+            std::lock_guard<std::mutex> l(qmu); qdone = true; qcv.notify_all();
+        });
+    } else if (fused) {
+        // the device-resident pipeline: every stage of every gated seed on the GPU, wave by wave; only the result
+        // records come back.  With gate=1 the waves are ranges of seed indices through the GPU gate; with stdin=1
+        // they are the seeds read (up to 1,024 at a time).  Seeds of a wave that exceeded the pipeline's
+        // capacities come back too and go to the workers (the per-stage path), which write their lines as usual.
+        const uint64_t total = S.count == 0 ? 100000000000000ULL : S.count;
+        source = std::thread([&, total] {
+            dsg_search_params sp{};
+            sp.gate_phase = float(P.gate_phase); sp.gate_pthr = float(P.gate_pthr); sp.gate_amp = float(P.gate_amp);
+            sp.ta = float(P.ta); sp.t = float(P.t); sp.wc = float(P.wc); sp.we = float(P.we);
+            sp.max_sites = P.max_sites; sp.nms = P.nms; sp.exact_n = P.exact_n;
+            sp.hot_min = P.hot_min; sp.hot_pre = P.hot_pre; sp.exact_min = P.exact_min; sp.refine_mb = P.refine_mb; sp.csv_min = P.csv_min;
+            ck(dsg_search_open(&sp), "device search");
+            std::vector<dsg_search_seed> recs(1u << 16); std::vector<dsg_search_row> rows(1u << 18); std::vector<uint64_t> unf(1u << 16);
+            uint64_t tot[4] = {0, 0, 0, 0};
+            const auto tg = Clock::now();
+            auto take = [&](uint32_t ns, uint32_t nu, const uint64_t *c) {
+                for (int k = 0; k < 4; k++) tot[k] += c[k];
+                S.done += ns; S.passed += ns; S.scanned += ns; S.nsites += c[4]; S.nhot += c[5]; S.nbig += c[6];
+                for (uint32_t i = 0; i < ns; i++) S.emit_device(recs[i], rows.data() + recs[i].row0);
+                for (uint32_t i = 0; i < nu && !interrupted; i++) push(unf[i]);
+            };
+            if (P.gate) {
+                const uint64_t B = 1ull << 24;
+                for (uint64_t base = 0; base < total && !interrupted; base += B) {
+                    const uint64_t nb = std::min(B, total - base);
+                    uint32_t ns = 0, nr = 0, nu = 0; uint64_t c[8]; float ms = 0;
+                    ck(dsg_search_run(S.start + base, nb, recs.data(), uint32_t(recs.size()), &ns, rows.data(), uint32_t(rows.size()), &nr,
+                                      unf.data(), uint32_t(unf.size()), &nu, c, &ms), "device search");
+                    take(ns, nu, c);
+                    const double sec = std::chrono::duration<double>(Clock::now() - tg).count();
+                    fprintf(stderr, "gate: %llu seeds, %llu phase-passed, %llu pre-gate, %llu passed; %.0f seeds/s, %.1f passed/s\n",
+                            (unsigned long long)(base + nb), (unsigned long long)tot[1], (unsigned long long)tot[2], (unsigned long long)tot[3],
+                            (base + nb) / sec, tot[3] / sec);
+                }
+            } else {
+                char line[256];
+                std::vector<uint64_t> in;
+                bool eof = false;
+                while (!eof && !interrupted) {
+                    in.clear();
+                    while (in.size() < 1024 && !(eof = !fgets(line, sizeof line, stdin))) in.push_back(std::strtoull(line, nullptr, 10));
+                    if (in.empty()) break;
+                    uint32_t ns = 0, nr = 0, nu = 0; uint64_t c[8]; float ms = 0;
+                    ck(dsg_search_seeds(in.data(), uint32_t(in.size()), recs.data(), uint32_t(recs.size()), &ns, rows.data(), uint32_t(rows.size()),
+                                        &nr, unf.data(), uint32_t(unf.size()), &nu, c, &ms), "device search");
+                    take(ns, nu, c);
+                }
+            }
+            ck(dsg_search_close(), "device search");
             gate_end = std::chrono::duration<double>(Clock::now() - S.begin).count();
             std::lock_guard<std::mutex> l(qmu); qdone = true; qcv.notify_all();
         });

@@ -239,6 +239,57 @@ int dsg_flood(const dsg_flood_req *req, dsg_area *out);
  * exactly the touched cells); sub-blocks * 256 / touched is the speculative-evaluation overhead. */
 int dsg_flood_last_stats(uint64_t stats[3]);
 
+/* ---------------------------------------------------------------- device-resident search (fused pipeline) */
+/* The production search (dsearch_desert START COUNT PREFIX THREADS gate=1 gpu=1 gscan=1: src/dsearch_desert.cpp:173-557
+ * with its GPU engine src/gpu/gproxy.cu and gate src/gpu/gate.cuh) with every stage on the device and no host
+ * round trip between stages: per wave of seed indices, the gate, then one CUDA graph (tables/blur, scan, bucket
+ * suppression, hot-point search, hot-zone floods with the reference's coverage replay, proxy bitmaps and
+ * components, exact-start search, step-8 and step-4 floods with the retry replay); only the result records come
+ * back.  Results equal the per-stage entry points' (and the reference CPU searcher's semantics) line for line. */
+typedef struct dsg_search_params {
+    float gate_phase, gate_pthr, gate_amp;     /* the GPU gate (Params.gate_phase, gate_pthr, gate_amp) */
+    float ta, t, wc, we;                       /* scan prune, score threshold and weights (Params.ta, t, wc, we) */
+    int32_t max_sites, nms, exact_n;           /* sites per seed (<= 300), suppression distance, exact floods per seed (<= 2) */
+    double hot_min, hot_pre;                   /* big hot-zone area (M blocks^2, > 0) and pre-flood fraction (> 0) */
+    double exact_min, refine_mb, csv_min;      /* proxy area for exact floods, step-8 area for step 4, CSV row cut */
+    uint64_t wave;                             /* seed indices per wave (0 = 2^22, at most 2^26) */
+} dsg_search_params;
+/* One gated seed: its PREFIX.seeds.csv line (dsearch_desert.cpp:548), rows[row0 .. row0 + nrows) its CSV rows. */
+typedef struct dsg_search_seed {
+    uint64_t seed;
+    double fya, fyb;                           /* fractional y offsets of temperature octave -10, sides A and B */
+    float maxta, maxtb;                        /* maxima of the blurred octave-0 temperature tables */
+    uint32_t candidates, sites;                /* NMS buckets, kept sites */
+    double best;                               /* best exact area (M blocks^2), 0 if none */
+    uint32_t row0, nrows;
+} dsg_search_seed;
+/* One PREFIX.csv row (dsearch_desert.cpp:539-540); x, z in quarts (the file prints x * 4 + 2). exact: one of the
+ * seed's exact-flood evaluations with a start (its CANDIDATE / best lines, :524-531). */
+typedef struct dsg_search_row {
+    uint64_t seed;
+    uint32_t rank; int32_t x, z;
+    float score, t0, c0, e0;
+    double proxy, s8, s4, hot;
+    int32_t edge, exact;
+} dsg_search_row;
+/* Allocate the pipeline (about 20 GB of device memory) and capture its graph; needs dsg_init and dsg_scan_init. */
+int dsg_search_open(const dsg_search_params *p);
+/* Search seeds mix(start + k), k < count, wave by wave.  Gated seeds' records go to seeds_out (their rows to
+ * rows_out, row0 re-based), in no particular order.  A wave that exceeds a fixed capacity of the pipeline
+ * returns its gated seeds in `unfinished` instead: run them through the per-stage entry points.  counts =
+ * {indices, phase-passed, pre-gate passed, gated, sites, hot zones used, big zones, OR of wave flags};
+ * device_ms (may be NULL) = CUDA-event time of the waves on the pipeline's stream.  DSG_OVERFLOW if an output
+ * capacity was too small (outputs hold the first items). */
+int dsg_search_run(uint64_t start, uint64_t count, dsg_search_seed *seeds_out, uint32_t seed_cap, uint32_t *n_seeds,
+                   dsg_search_row *rows_out, uint32_t row_cap, uint32_t *n_rows, uint64_t *unfinished, uint32_t unfinished_cap,
+                   uint32_t *n_unfinished, uint64_t counts[8], float *device_ms);
+/* The same for explicit gated seeds (the searcher's stdin=1 input, dsearch_desert.cpp:571-581: seeds already
+ * gated elsewhere): no gate, every seed goes through the stages; counts[0..2] = 0, counts[3] = n. */
+int dsg_search_seeds(const uint64_t *seeds, uint32_t n, dsg_search_seed *seeds_out, uint32_t seed_cap, uint32_t *n_seeds,
+                     dsg_search_row *rows_out, uint32_t row_cap, uint32_t *n_rows, uint64_t *unfinished, uint32_t unfinished_cap,
+                     uint32_t *n_unfinished, uint64_t counts[8], float *device_ms);
+int dsg_search_close(void);
+
 #ifdef __cplusplus
 }
 #endif
