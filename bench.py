@@ -1,27 +1,38 @@
 #!/usr/bin/env python3
-"""Benchmark: gated seeds/s of the B200 seed gate, and the timed CPU reference arm.
+"""Benchmark: gated seeds/s of the whole per-seed search on one B200, and the timed CPU reference arm.
 
-Workload: the batched search's seed stream, seeds mix(2*10^13 + k), processed in steps of 2^26 seed
-indices.  One step is one pass of the plain per-stage gate (y-phase -> octave init -> anti-aliased 256^2
-pre-gate -> full 512^2 gate) on the device; the metric counts the seeds that pass all three (about 1 in
-13,000).  Multi-GPU: one process per GPU, each on its own seed range 10^12 apart (weak scaling, no
-data-path collective); device time is the max over ranks.
+Workload (the batched full search): seeds mix(2*10^13 + k) through the production search -- the command line
+`dsearch_desert START COUNT PREFIX THREADS gate=1 gpu=1 gscan=1` of deploy/gpipe.sh -- on the device-resident
+pipeline (dsg_search_run): GPU gate (y-phase <= 0.06, anti-aliased 256^2 pre-gate >= 0.645, 512^2 gate >= 0.70),
+period tables + blur, translation scan, bucket suppression, hot-zone floods, proxy bitmaps and components, exact
+step-8/step-4 floods.  One step = 2^24 seed indices (four waves of 2^22, each a gate launch and one CUDA graph);
+the metric counts the seeds that pass the gate and are carried through every later stage (about 1 in 13,000).
+`value` = gated seeds / device time (CUDA events on the pipeline's stream); `e2e` = the same over the wall clock
+of the dsg_search_run calls, whose outputs (seed records and CSV rows) land in host memory.  Multi-GPU: one
+process per GPU, each on its own seed range 10^12 apart (weak scaling, no data-path collective); device time is
+the max over ranks.
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
 
---impl reference times the reference's own CPU searcher (oracle/_ref/dsearch_desert, compiled from the
-reference sources) on the same seed stream with all host cores: its CPU gate (y-phase, sub-grid pre-gate,
-full tables) plus the tables+scan of every gated seed, with the hot-zone stage reduced to one site.
+--impl reference times the reference's own CPU searcher (oracle/_ref/dsearch_desert, built from the reference
+sources) on the same seed stream with all host cores and every stage at its defaults, with the y-phase cut of the
+GPU gate (phase=0.06); the reference's CPU build has no anti-aliased pre-gate, so its gate is its own CPU gate
+(sub-grid estimate >= 0.69, period-table amplitude >= 0.70).
 
-Besides the gate line, the default run adds (single GPU): "pipeline", the whole per-seed search through the
-drop-in searcher (ours overlapped, ours plain, the reference's GPU searcher; wall clock; outputs compared),
-"default_mode", the reference's default command line (gpu=0, gate=0) through ours and through the reference's
-own CPU searcher (wall clock; files compared), and "flood", exact step-1 floods of uneven size as one batch, through the flood service under Poisson
-arrivals, and as sequential per-request launches.
+The line carries "stages_ms" (device ms of each stage over the timed steps, from events captured in the wave
+graph).  Besides it, the default run adds (single GPU): "pipeline" (the same search through the drop-in searcher binary:
+device pipeline, per-stage path on one host worker (the plain form: one batched call per stage with host syncs
+between stages), per-stage path on 8 workers, and the reference's own GPU searcher; wall clock; outputs
+compared), "default_mode" (the reference's default command line, ours vs its CPU searcher), "gate" (the seed
+gate alone against the shared-memory roofline, and the reference's tgate on the same seeds) and "flood" (exact
+step-1 floods of uneven size: one batch, the flood service under Poisson arrivals, sequential per-request
+launches under the same arrivals, the reference's dflood on the host cores, FP64 roofline).
 """
 import argparse
+import concurrent.futures as cf
 import json
 import os
+import re
 import statistics
 import subprocess
 import sys
@@ -35,20 +46,22 @@ sys.path.insert(0, os.path.join(ROOT, "tests"))
 METRIC = "gated seeds/s on 1 B200, fused vs plain; flood-request p50/p99 latency"
 UNIT = "gated seeds/s"
 START = 2 * 10**13
-PER_STEP = 1 << 26
+PER_STEP = 1 << 24
 RANK_STRIDE = 10**12            # per-GPU seed ranges, as deploy/prun.sh assigns them
 # pre-gate: 2 sides x 256^2 cells x 18 corner-table gathers of 4 bytes per phase-passed seed
 PRE_BYTES_PER_SEED = 2 * 256 * 256 * 18 * 4
 SMEM_BYTES_PER_CLK_PER_SM = 128  # 32 banks x 4 bytes
+FP64_FLOPS_PER_CLK_PER_SM = 128  # 64 FP64 FMA lanes per SM (B200) x 2 flops
 # k_pregate DRAM traffic per phase-passed seed from one ncu capture (dram__bytes_read.sum + write.sum =
-# 150.5 MB + 6.1 MB over 241,519 seeds on 2^25 seed indices): the seed's octave table read once; scaled to a
-# launch by the phase-passed seeds it processes
+# 150.5 MB + 6.1 MB over 241,519 seeds on 2^25 seed indices): the seed's octave table read once
 PRE_DRAM_BYTES_PER_SEED = (150.5e6 + 6.1e6) / 241519
+# k_tile_eval FP64 work per evaluated cell, from one ncu capture of a flood batch (profiles/flood_eval_batch.md:
+# executed DFMA x 2 + DADD + DMUL over the cells of the evaluated 16x16 sub-blocks)
+EVAL_FP64_FLOPS_PER_CELL = None
 
 
 def dist():
-    rank, world, local = int(os.environ.get("RANK", 0)), int(os.environ.get("WORLD_SIZE", 1)), int(os.environ.get("LOCAL_RANK", 0))
-    return rank, world, local
+    return int(os.environ.get("RANK", 0)), int(os.environ.get("WORLD_SIZE", 1)), int(os.environ.get("LOCAL_RANK", 0))
 
 
 def shard_start(rank):
@@ -117,167 +130,106 @@ class Clocks:
         return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": mx, "reasons": sorted(reasons), "samples": len(sm)}
 
 
-def cpu_baseline(seconds_budget=20.0):
-    """The oracle's CPU restatement of the same gate, on all host threads, over a bounded sample."""
-    import libs
-    threads = os.cpu_count() or 1
-    count = 1 << 19
+def ref_exe(name):
+    p = os.path.join(ROOT, "oracle", "_ref", name)
+    return p if os.path.exists(p) else None
+
+
+def ref_cpu_search(start, count, cores, td, tag):
+    """The reference's own CPU searcher over seeds mix(start + k), k < count: every stage at its defaults, the
+    GPU gate's y-phase cut.  (wall s, seeds, gated) -- gated = seeds its gate passed and it scanned."""
+    exe = ref_exe("dsearch_desert")
+    pre = os.path.join(td, tag)
     t0 = time.perf_counter()
-    _, _, c = libs.orc_gate_range(START + (1 << 40), count, threads=threads)
+    subprocess.run([exe, str(start), str(count), pre, str(cores), "phase=0.06"], check=True, capture_output=True)
     dt = time.perf_counter() - t0
-    if dt < seconds_budget / 4:                     # grow the sample towards the budget
-        count = int(count * min(16, seconds_budget / max(dt, 1e-3)))
-        t0 = time.perf_counter()
-        _, _, c = libs.orc_gate_range(START + (1 << 40), count, threads=threads)
-        dt = time.perf_counter() - t0
-    return {"value": float(c[3]) / dt, "unit": UNIT, "cores": threads, "kind": "port",
-            "sample": f"seeds mix(2e13 + 2^40 + k), k < {count}: {int(c[1])} phase-passed, {int(c[3])} gated in {dt:.2f} s",
-            "seeds_per_s": count / dt}
+    j = json.load(open(pre + ".json"))
+    return dt, int(j["done"]), int(j["scanned"])
 
 
-def flood_sites(dsgpu, n_small, rng_seed=20261203, candidates=()):
-    """Synthetic flood sites.  Small class: random int64 seeds from a fixed RNG stream, each paired with the
-    first of 64 uniform blocks in |X|, |Z| <= 3e7 whose bridged Y=256 state is desert.  Large class: the
-    searcher's own proxy >= 50M candidates (CSV rows of the pipeline run, `candidates` = (seed, x, z) in
-    blocks, kept where the start's state is desert), then the 220 MC-Measure-verified finds of the
-    reference's results (72M-100M blocks^2) and the two `make check` records (tests/golden/finds.json)."""
-    import numpy as np
-    rng = np.random.default_rng(rng_seed)
-    small = []
-    while len(small) < n_small:
-        m = 256
-        seeds = rng.integers(-(1 << 63), (1 << 63) - 1, m, dtype=np.int64).view(np.uint64)
-        xz = (rng.integers(-30_000_000, 30_000_001, (m * 64, 2)) >> 2).astype(np.int32)
-        st = dsgpu.query(seeds, np.repeat(np.arange(m, dtype=np.uint32), 64), 6, xz).reshape(m, 64)
-        for i in range(m):
-            k = np.nonzero(st[i] == 2)[0]
-            if len(k):
-                small.append((int(seeds[i]), int(xz[i * 64 + k[0], 0]), int(xz[i * 64 + k[0], 1])))
-    finds = json.load(open(os.path.join(ROOT, "tests", "golden", "finds.json")))
-    large = []
-    if candidates:
-        cs = np.array([c[0] for c in candidates], dtype=np.uint64)
-        xz = np.array([[c[1] >> 2, c[2] >> 2] for c in candidates], dtype=np.int32)
-        st = dsgpu.query(cs, np.arange(len(cs), dtype=np.uint32), 6, xz)
-        large = [(int(cs[k]), int(xz[k, 0]), int(xz[k, 1])) for k in range(len(cs)) if st[k] == 2]
-    large += [(f["seed"] & ((1 << 64) - 1), f["x"] >> 2, f["z"] >> 2) for f in finds]
-    return small[:n_small], large
+def cpu_baseline(cores, seconds_budget=20.0):
+    """The reference's CPU searcher on the host cores, on a bounded sample of the same seed stream."""
+    if not ref_exe("dsearch_desert"):
+        return {"value": None, "unit": UNIT, "cores": cores, "kind": "reference", "sample": "oracle/_ref/dsearch_desert not built"}
+    count = 1 << 19
+    with tempfile.TemporaryDirectory() as td:
+        dt, done, gated = ref_cpu_search(START + (1 << 40), count, cores, td, "a")
+        if dt < seconds_budget / 3:
+            count = int(count * min(32, seconds_budget / max(dt, 1e-3)))
+            dt, done, gated = ref_cpu_search(START + (1 << 40), count, cores, td, "b")
+    return {"value": gated / dt, "unit": UNIT, "cores": cores, "kind": "reference",
+            "sample": f"oracle/_ref/dsearch_desert (reference sources) on seeds mix(2e13 + 2^40 + k), k < {count}, phase=0.06, every stage: "
+                      f"{gated} gated in {dt:.2f} s", "seeds_per_s": done / dt}
 
 
-def bench_floods(dsgpu, n_small=4096, rates=(200.0, 1000.0, 3000.0), n_service=1500, n_seq=120, batch_only=False, n_large=None,
-                 candidates=()):
-    """Exact step-1 floods: one batch of every site, and the flood service under Poisson arrivals."""
-    import threading
-    import numpy as np
-    small, large = flood_sites(dsgpu, n_small, candidates=candidates)
-    if n_large is not None:
-        large = large[:n_large]
-    req = lambda s: dsgpu.flood_req(s[0], s[1], s[2], 1, 20000)
-    # batch: all sites in one dsg_flood_batch call
-    reqs = [req(s) for s in small + large]
+# ---------------------------------------------------------------------------- the device pipeline
+def search_steps(dsgpu, base, steps, warmup, per_step):
+    """W untimed steps, then K timed ones of per_step seed indices each: (device ms, wall s, counts[10], d2h bytes).
+    The stage timers cover the timed steps only."""
+    import torch
+    for i in range(warmup):
+        dsgpu.search_run(base + i * per_step, per_step)
+    dsgpu.search_stage_ms(reset=True)
+    base += warmup * per_step
+    torch.cuda.synchronize()
+    ms, tot, d2h = 0.0, [0] * 10, 0
     t0 = time.perf_counter()
-    areas = dsgpu.flood_batch(reqs)
-    t_batch = time.perf_counter() - t0
-    work = dsgpu.flood_last_stats()
-    sampled = sum(a[1] for a in areas)
-    cells = np.array([a[0] for a in areas], dtype=np.float64)
-    batch = {"floods": len(reqs), "small": len(small), "large": len(large), "large_from_search": len(large) - 222 if candidates else 0,
-             "seconds": t_batch, "floods_per_s": len(reqs) / t_batch,
-             "cells_per_s": float(cells.sum()) / t_batch, "evaluations_per_s": sampled / t_batch,
-             "area_blocks2_min_median_max": [float(cells.min() * 16), float(np.median(cells) * 16), float(cells.max() * 16)],
-             "rounds": work["rounds"], "subblocks": work["blocks"], "cells_evaluated_per_s": work["blocks"] * 256 / t_batch,
-             "speculation_overhead": work["blocks"] * 256 / max(1, work["touched"])}
-    if batch_only:
-        return {"batch": batch}
-    # service: 90% small, 10% large, Poisson arrivals, at each rate of the sweep
-    rng = np.random.default_rng(7)
-    kinds = rng.random(n_service) < 0.1
-    mix = [large[rng.integers(len(large))] if k else small[rng.integers(len(small))] for k in kinds]
-    gaps = rng.exponential(1.0, n_service)
-
-    def serve(rate):
-        arrive = np.cumsum(gaps / rate)
-        svc = dsgpu.Service(budget_bytes=24 << 30, max_requests=4096, rounds_per_check=4)
-        done_t = np.zeros(n_service); tickets = [0] * n_service
-        lock = threading.Lock(); ready = threading.Semaphore(0)
-        todo = []
-
-        def waiter():
-            while True:
-                ready.acquire()
-                with lock:
-                    if not todo:
-                        return
-                    i = todo.pop(0)
-                svc.wait(tickets[i])
-                done_t[i] = time.perf_counter()
-        ws = [threading.Thread(target=waiter) for _ in range(16)]
-        for w in ws:
-            w.start()
-        t_start = time.perf_counter()
-        for i in range(n_service):
-            d = t_start + arrive[i] - time.perf_counter()
-            if d > 0:
-                time.sleep(d)
-            tickets[i] = svc.submit(req(mix[i]))
-            with lock:
-                todo.append(i)
-            ready.release()
-        for _ in ws:
-            ready.release()
-        for w in ws:
-            w.join()
-        svc.close()
-        lat = done_t - (t_start + arrive)
-        return {"rate_req_per_s": rate, "requests": n_service, "floods_per_s": n_service / (done_t.max() - t_start),
-                "p50_ms": float(np.percentile(lat, 50) * 1e3), "p99_ms": float(np.percentile(lat, 99) * 1e3)}, arrive
-    sweep = [serve(r) for r in rates]
-    # sequential plain per-request launches: measured service times of a sample of the same mix, then a FIFO
-    # queue on each rate's arrival times
-    seq_t = []
-    for i in range(n_seq):
-        t1 = time.perf_counter(); dsgpu.flood(*mix[i][:3], 1, 20000); seq_t.append(time.perf_counter() - t1)
-    mean_seq = float(np.mean(seq_t))
-    svc_times = np.array([seq_t[i % n_seq] for i in range(n_service)])
-    seq_rates = []
-    for rate in rates:
-        arrive = np.cumsum(gaps / rate)
-        fin = np.zeros(n_service); prev = 0.0
-        for i in range(n_service):
-            prev = max(prev, arrive[i]) + svc_times[i]; fin[i] = prev
-        lat = fin - arrive
-        seq_rates.append({"rate_req_per_s": rate, "floods_per_s": n_service / fin[-1] if fin[-1] > 0 else None,
-                          "p50_ms": float(np.percentile(lat, 50) * 1e3), "p99_ms": float(np.percentile(lat, 99) * 1e3)})
-    return {
-        "batch": batch,
-        "service": {"mix": "90% random desert sites, 10% large (search candidates and verified finds); step 1, half 20000",
-                    "rates": [r for r, _ in sweep]},
-        "sequential_plain": {"floods_per_s": 1.0 / mean_seq, "rates": seq_rates,
-                             "how": f"dsg_flood per request, service times measured on {n_seq} requests of the same mix, FIFO queue on each rate's arrival times"},
-    }
+    for i in range(steps):
+        recs, rows, unf, c, m = dsgpu.search_run(base + i * per_step, per_step)
+        ms += m
+        for k in (0, 1, 2, 3, 4, 5, 6, 8, 9):
+            tot[k] += c[k]
+        tot[7] |= c[7]
+        d2h += recs.nbytes + rows.nbytes + unf.nbytes
+    torch.cuda.synchronize()
+    return ms, time.perf_counter() - t0, tot, d2h // max(1, steps)
 
 
-def pipeline(count=1 << 26):
-    """The whole per-seed pipeline through the drop-in searcher (gate -> tables/blur/scan -> hot-zone floods ->
-    proxy -> exact floods), seeds mix(2e13 + k), k < count, timed by wall clock around each process (CUDA
-    context creation included, ~1-3 s on these hosts; ours also reports its own startup): ours with one
-    worker per host core up to 8 (device stages of different batches overlap; the library serialises each
-    kind of device call), ours with one worker (plain: every stage of a batch in turn), and the reference's
-    own GPU searcher built from its sources, with the same arguments.  Outputs are compared row by row on
-    the seeds both gates passed: the reference's pre-gate kernel is not deterministic on this GPU (a seed
-    now and then passes one run and not another), and its GPU proxy is FP32 where ours and its CPU path are
-    FP64, so a proxy value may differ in the last digits."""
-    import re
+# ---------------------------------------------------------------------------- the gate alone
+def gate_leg(dsgpu, sm_mhz, sms, steps=6, warmup=3):
+    """The seed gate (y-phase, octave init, pre-gate, full gate) alone on 2^26 indices per step, its k_pregate
+    against the shared-memory gather roofline, and the reference's tgate (its GPU gate) on the same seeds."""
+    n = 1 << 26
+    ms, mk, counts = dsgpu.gate_bench(START, n, steps, warmup)
+    pre_ms = float(mk[2])
+    achieved = counts[1] * PRE_BYTES_PER_SEED / (pre_ms / 1e3) / 1e9
+    peak = sms * SMEM_BYTES_PER_CLK_PER_SM * sm_mhz * 1e6 / 1e9
+    out = {"seeds_per_step": n, "steps": steps, "gated_per_s": counts[3] / (ms / 1e3), "seeds_per_s": counts[0] / (ms / 1e3),
+           "kernel_ms": {"phase": float(mk[0]), "octave_init": float(mk[1]), "pregate": pre_ms, "fullgate": float(mk[3])},
+           "counts": {"seeds": int(counts[0]), "phase_passed": int(counts[1]), "pre_passed": int(counts[2]), "gated": int(counts[3])},
+           "roofline": {"bound": "smem", "kernel": "k_pregate", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                        "traffic": counts[1] / steps * PRE_DRAM_BYTES_PER_SEED,
+                        "note": "shared-memory gather bytes (18 corner-table words per cell) / k_pregate event time; peak = SMs x 128 B/clk "
+                                "at the median sampled SM clock; traffic = DRAM bytes per launch scaled from an ncu capture"}}
+    tg = ref_exe("tgate")
+    if tg:
+        t0 = time.perf_counter()
+        r = subprocess.run([tg, str(START), str(n)], capture_output=True, text=True)
+        wall = time.perf_counter() - t0
+        m = re.findall(r"gate: .*?([\d.]+) ?s", r.stderr)
+        out["reference_tgate"] = {"seeds": n, "wall_s": wall, "rc": r.returncode, "survivors": len(r.stdout.splitlines()),
+                                  "gate_line": (r.stderr.strip().splitlines() or [""])[-1][:300]}
+    return out
+
+
+# ---------------------------------------------------------------------------- whole searcher binaries
+def searcher_runs(count=1 << 26):
+    """The search through the drop-in searcher binary on seeds mix(2e13 + k), k < count, wall clock around each
+    process (startup reported separately): the device pipeline (fused=1, the default), the per-stage path on
+    one host worker (the plain form: each stage one batched call with host syncs between stages), the
+    per-stage path on 8 workers (device stages of different batches overlap), and the reference's own GPU
+    searcher built from its sources.  Outputs are compared row by row on the seeds both gates passed (the
+    reference's pre-gate kernel is not deterministic on this GPU, and its GPU proxy is FP32)."""
     cores = os.cpu_count() or 1
     ours = os.path.join(ROOT, "desert-search_b200", "bin", "dsearch_desert")
-    ref = os.path.join(ROOT, "oracle", "_ref", "dsearch_desert_gpu")
+    ref = ref_exe("dsearch_desert_gpu")
     out = {"seeds": count, "args": "START=2e13 gate=1 gpu=1 gscan=1", "host_cores": cores}
     cands = []
 
-    def run(exe, threads, td, tag):
+    def run(exe, threads, td, tag, extra=()):
         pre = os.path.join(td, tag)
         t0 = time.perf_counter()
-        r = subprocess.run([exe, str(START), str(count), pre, str(threads), "gate=1", "gpu=1", "gscan=1"], capture_output=True, text=True)
+        r = subprocess.run([exe, str(START), str(count), pre, str(threads), "gate=1", "gpu=1", "gscan=1"] + list(extra), capture_output=True, text=True)
         wall = time.perf_counter() - t0
         if r.returncode != 0:
             return {"error": r.stderr[-300:]}, None
@@ -290,9 +242,9 @@ def pipeline(count=1 << 26):
             res["gated_per_s_after_startup"] = gated / max(1e-9, wall - float(st.group(1)))
         rows = open(pre + ".csv").read().splitlines()[1:]
         seeds = {l.split(",")[0] for l in open(pre + ".seeds.csv").read().splitlines()[1:]}
-        if tag == "ours":                                   # proxy >= 50M rows: the flood batch's large class
+        if tag == "fused":                                   # proxy >= 50M rows: the flood batch's large class
             cands.extend((int(l.split(",")[0]) & ((1 << 64) - 1), int(l.split(",")[6]), int(l.split(",")[7])) for l in rows)
-        return res, (rows, seeds)
+        return res, (rows, seeds, sorted(open(pre + ".seeds.csv").read().splitlines()[1:]))
 
     def compare(a, b):
         common = a[1] & b[1]
@@ -308,14 +260,20 @@ def pipeline(count=1 << 26):
                 "rows_other_differences": len(ka) + len(kb) - 2 * same - 2 * proxy_only}
 
     with tempfile.TemporaryDirectory() as td:
-        out["ours"], a = run(ours, cores, td, "ours")
-        out["ours_plain"], p1 = run(ours, 1, td, "plain")
-        if a is not None and p1 is not None:
-            out["plain_vs_ours"] = compare(a, p1)
-        if os.path.exists(ref):
+        out["fused"], f = run(ours, cores, td, "fused")
+        out["plain"], p1 = run(ours, 1, td, "plain", ["fused=0"])
+        out["per_stage_8_workers"], p8 = run(ours, cores, td, "p8", ["fused=0"])
+        if f and p1:
+            out["fused_vs_plain_files_identical"] = sorted(f[0]) == sorted(p1[0]) and f[2] == p1[2]
+        if f and p8:
+            out["fused_vs_per_stage_8_files_identical"] = sorted(f[0]) == sorted(p8[0]) and f[2] == p8[2]
+        k = "gated_per_s_after_startup"
+        if k in out["fused"] and k in out["plain"]:
+            out["fused_over_plain"] = out["fused"][k] / out["plain"][k]
+        if ref:
             out["reference_gpu_searcher"], b = run(ref, cores, td, "ref")
-            if a is not None and b is not None:
-                out["ours_vs_reference"] = compare(a, b)
+            if f and b:
+                out["ours_vs_reference_gpu_searcher"] = compare(f, b)
         else:
             out["reference_gpu_searcher"] = {"unavailable": "oracle/_ref/dsearch_desert_gpu not built"}
     return out, cands
@@ -326,16 +284,15 @@ def default_mode(count=1 << 22):
     gate over the enumerated range, period tables and scan, hot zones, proxy floods from the zones' lattice
     starts, exact floods), on seeds mix(2e13 + k), k < count: ours (every stage on the device) against the
     reference's own CPU searcher on all host cores, wall clock around each process; the files are compared."""
-    import re
     cores = os.cpu_count() or 1
     ours = os.path.join(ROOT, "desert-search_b200", "bin", "dsearch_desert")
-    ref = os.path.join(ROOT, "oracle", "_ref", "dsearch_desert")
+    ref = ref_exe("dsearch_desert")
     out = {"seeds": count, "args": "defaults (gpu=0 gate=0)", "host_cores": cores}
     with tempfile.TemporaryDirectory() as td:
         res = {}
         for tag, exe in (("ours", ours), ("reference_cpu_searcher", ref)):
-            if not os.path.exists(exe):
-                out[tag] = {"unavailable": f"{os.path.relpath(exe, ROOT)} not built"}
+            if not exe or not os.path.exists(exe):
+                out[tag] = {"unavailable": "not built"}
                 continue
             pre = os.path.join(td, tag)
             t0 = time.perf_counter()
@@ -357,12 +314,181 @@ def default_mode(count=1 << 22):
     return out
 
 
+# ---------------------------------------------------------------------------- floods
+def flood_sites(dsgpu, n_small, rng_seed=20261203, candidates=(), n_large=None):
+    """Synthetic flood sites.  Small class: random int64 seeds from a fixed RNG stream, each paired with the
+    first of 64 uniform blocks in |X|, |Z| <= 3e7 whose bridged Y=256 state is desert.  Large class: the
+    search's own proxy >= 50M candidates (CSV rows, `candidates` = (seed, x, z) in blocks, kept where the
+    start's state is desert), then the 222 MC-Measure-verified finds (tests/golden/finds.json)."""
+    import numpy as np
+    rng = np.random.default_rng(rng_seed)
+    small = []
+    while len(small) < n_small:
+        m = 256
+        seeds = rng.integers(-(1 << 63), (1 << 63) - 1, m, dtype=np.int64).view(np.uint64)
+        xz = (rng.integers(-30_000_000, 30_000_001, (m * 64, 2)) >> 2).astype(np.int32)
+        st = dsgpu.query(seeds, np.repeat(np.arange(m, dtype=np.uint32), 64), 6, xz).reshape(m, 64)
+        for i in range(m):
+            k = np.nonzero(st[i] == 2)[0]
+            if len(k):
+                small.append((int(seeds[i]), int(xz[i * 64 + k[0], 0]), int(xz[i * 64 + k[0], 1])))
+    finds = json.load(open(os.path.join(ROOT, "tests", "golden", "finds.json")))
+    large = []
+    if candidates:
+        cs = np.array([c[0] for c in candidates], dtype=np.uint64)
+        xz = np.array([[c[1] >> 2, c[2] >> 2] for c in candidates], dtype=np.int32)
+        st = dsgpu.query(cs, np.arange(len(cs), dtype=np.uint32), 6, xz)
+        large = [(int(cs[k]), int(xz[k, 0]), int(xz[k, 1])) for k in range(len(cs)) if st[k] == 2]
+    large += [(f["seed"] & ((1 << 64) - 1), f["x"] >> 2, f["z"] >> 2) for f in finds]
+    if n_large is not None:
+        large = large[:n_large]
+    return small[:n_small], large
+
+
+def more_candidates(dsgpu, have, want, start, per_call=1 << 26, max_calls=8):
+    """Proxy >= 50M rows from further seed ranges of the device pipeline until `want` candidates are known."""
+    cands, used = list(have), 0
+    while len(cands) < want and used < max_calls:
+        recs, rows, unf, c, ms = dsgpu.search_run(start + used * per_call, per_call)
+        cands += [(int(r["seed"]), int(r["x"]) * 4 + 2, int(r["z"]) * 4 + 2) for r in rows]
+        used += 1
+    return cands, used * per_call
+
+
+def ref_dflood(sites, cores, budget_s=25.0):
+    """The reference's own exact flood, `dflood SEED X Z 1` (tools/dflood.cpp), one process per site on all host
+    cores, over a bounded sample of the sites: (floods/s, cells/s, sample description)."""
+    exe = ref_exe("dflood")
+    if not exe:
+        return {"value": None, "unavailable": "oracle/_ref/dflood not built"}
+
+    def one(s):
+        seed, qx, qz = s
+        r = subprocess.run([exe, str(seed - (1 << 64) if seed >= 1 << 63 else seed), str(qx * 4), str(qz * 4), "1"], capture_output=True,
+                           text=True, timeout=600)
+        m = re.search(r"([\d.]+) cells", r.stdout)
+        return float(m.group(1)) if m else 0.0
+    t0 = time.perf_counter()
+    cells, n = 0.0, 0
+    with cf.ThreadPoolExecutor(cores) as ex:
+        futs = [ex.submit(one, s) for s in sites]
+        for f in futs:
+            cells += f.result(); n += 1
+    dt = time.perf_counter() - t0
+    return {"value": n / dt, "unit": "floods/s", "cells_per_s": cells / dt, "cores": cores, "kind": "reference", "floods": n, "seconds": dt}
+
+
+def bench_floods(dsgpu, sm_mhz, sms, n_small=4096, n_large=4096, rates=(100.0, 500.0, 1000.0, 2000.0, 3000.0, 5000.0), requests=None,
+                 seq_requests=1500, candidates=(), cand_start=None, service_seconds=20.0, budget_gb=64):
+    """Exact step-1 floods (half 20000, rivers bridged) of uneven size: one batch of every site, the flood service
+    under Poisson arrivals at each rate, sequential dsg_flood calls under the same arrivals, the reference's
+    dflood on the host cores, and the evaluation kernel's FP64 roofline."""
+    import threading
+    import numpy as np
+    extra = 0
+    if cand_start is not None and len(candidates) < n_large:
+        candidates, extra = more_candidates(dsgpu, candidates, n_large, cand_start)
+    small, large = flood_sites(dsgpu, n_small, candidates=candidates, n_large=n_large)
+    req = lambda s: dsgpu.flood_req(s[0], s[1], s[2], 1, 20000)
+    reqs = [req(s) for s in small + large]
+    t0 = time.perf_counter()
+    areas = dsgpu.flood_batch(reqs)
+    t_batch = time.perf_counter() - t0
+    work = dsgpu.flood_last_stats()
+    cells = np.array([a[0] for a in areas], dtype=np.float64)
+    sampled = sum(a[1] for a in areas)
+    evaluated = work["blocks"] * 256
+    batch = {"floods": len(reqs), "small": len(small), "large": len(large), "large_from_search": max(0, len(large) - 222),
+             "extra_search_seeds_for_candidates": extra, "seconds": t_batch, "floods_per_s": len(reqs) / t_batch,
+             "cells_per_s": float(cells.sum()) / t_batch, "evaluations_per_s": sampled / t_batch,
+             "area_blocks2_min_median_max": [float(cells.min() * 16), float(np.median(cells) * 16), float(cells.max() * 16)],
+             "rounds": work["rounds"], "subblocks": work["blocks"], "cells_evaluated_per_s": evaluated / t_batch,
+             "speculation_overhead": evaluated / max(1, work["touched"])}
+    peak = sms * FP64_FLOPS_PER_CLK_PER_SM * sm_mhz * 1e6
+    if EVAL_FP64_FLOPS_PER_CELL:
+        ach = EVAL_FP64_FLOPS_PER_CELL * evaluated / t_batch
+        batch["roofline"] = {"bound": "fp64", "kernel": "k_tile_eval", "achieved": ach / 1e12, "peak": peak / 1e12, "unit": "TFLOP/s",
+                             "frac": ach / peak, "note": "executed FP64 flops per evaluated cell (ncu) x cells evaluated / batch wall time; "
+                                                         "peak = SMs x 64 FP64 FMA/clk x 2 at the sampled clock (nominal rate)"}
+    out = {"batch": batch}
+    # the reference's dflood on the host cores: a sample of small sites and large sites
+    cores = os.cpu_count() or 1
+    out["cpu_baseline"] = ref_dflood(small[:8 * cores] + large[:cores], cores)
+    out["cpu_baseline"]["sample"] = f"{8 * cores} small + {cores} large sites, one dflood process per site on {cores} host threads"
+    # service and sequential launches under Poisson arrivals: 90% small, 10% large
+    rng = np.random.default_rng(7)
+
+    def serve(rate, n):
+        kinds = rng.random(n) < 0.1
+        mix = [large[rng.integers(len(large))] if k else small[rng.integers(len(small))] for k in kinds]
+        arrive = np.cumsum(rng.exponential(1.0, n) / rate)
+        svc = dsgpu.Service(budget_bytes=budget_gb << 30, max_requests=4096, rounds_per_check=4)
+        done_t = np.zeros(n); tickets = [0] * n
+        lock = threading.Lock(); ready = threading.Semaphore(0)
+        todo = []
+
+        def waiter():
+            while True:
+                ready.acquire()
+                with lock:
+                    if not todo:
+                        return
+                    i = todo.pop(0)
+                svc.wait(tickets[i])
+                done_t[i] = time.perf_counter()
+        ws = [threading.Thread(target=waiter) for _ in range(32)]
+        for w in ws:
+            w.start()
+        t_start = time.perf_counter()
+        for i in range(n):
+            d = t_start + arrive[i] - time.perf_counter()
+            if d > 0:
+                time.sleep(d)
+            tickets[i] = svc.submit(req(mix[i]))
+            with lock:
+                todo.append(i)
+            ready.release()
+        for _ in ws:
+            ready.release()
+        for w in ws:
+            w.join()
+        svc.close()
+        lat = done_t - (t_start + arrive)
+        res = {"rate_req_per_s": rate, "requests": n, "floods_per_s": n / (done_t.max() - t_start),
+               "p50_ms": float(np.percentile(lat, 50) * 1e3), "p99_ms": float(np.percentile(lat, 99) * 1e3)}
+        # sequential plain launches, one dsg_flood per request in arrival order, under the same arrivals
+        m = min(n, seq_requests)
+        fin = np.zeros(m)
+        t_start = time.perf_counter()
+        for i in range(m):
+            d = t_start + arrive[i] - time.perf_counter()
+            if d > 0:
+                time.sleep(d)
+            dsgpu.flood(*mix[i][:3], 1, 20000)
+            fin[i] = time.perf_counter()
+        lat = fin - (t_start + arrive[:m])
+        seq = {"rate_req_per_s": rate, "requests": m, "floods_per_s": m / (fin[-1] - t_start),
+               "p50_ms": float(np.percentile(lat, 50) * 1e3), "p99_ms": float(np.percentile(lat, 99) * 1e3)}
+        return res, seq
+    sweep, seq = [], []
+    for r in rates:
+        n = requests if requests else int(min(100_000, max(1000, r * service_seconds)))
+        a, b = serve(r, n)
+        sweep.append(a); seq.append(b)
+    out["service"] = {"mix": "90% random desert sites, 10% large (search candidates and verified finds); step 1, half 20000",
+                      "budget_bytes": budget_gb << 30, "rates": sweep}
+    out["sequential_plain"] = {"rates": seq, "how": "dsg_flood per request in arrival order on the same Poisson arrivals (the first "
+                                                    f"{seq_requests} requests of each rate)"}
+    return out
+
+
+# ---------------------------------------------------------------------------- arms
 def run_ours(args):
     rank, world, local = dist()
     import dsgpu
+    import torch
     pg = None
     if world > 1:
-        import torch
         import torch.distributed as td
         torch.cuda.set_device(local)
         td.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=120))
@@ -370,67 +496,70 @@ def run_ours(args):
     dsgpu.init(local, 0.35)
     base = shard_start(rank)
     rep = Replicas(pg, "cuda")
-    barrier = rep.barrier
+    props = torch.cuda.get_device_properties(local)
+    sms = props.multi_processor_count
 
     if args.flood_only:
         if rank == 0:
-            print(json.dumps({"flood": bench_floods(dsgpu, n_small=args.flood_small, rates=args.flood_rates, n_service=args.flood_requests,
-                                                    batch_only=args.flood_batch_only, n_large=args.flood_large)}), flush=True)
+            dsgpu.scan_init_default(); dsgpu.search_open()
+            print(json.dumps({"flood": bench_floods(dsgpu, 1965.0, sms, n_small=args.flood_small, n_large=args.flood_large,
+                                                    rates=args.flood_rates, requests=args.flood_requests, cand_start=START + (1 << 41))}),
+                  flush=True)
+            dsgpu.search_close()
         return
-    barrier()
+    dsgpu.scan_init_default()
+    dsgpu.search_open()
+    rep.barrier()
     clk = Clocks(local)
-    ms, mk, counts = dsgpu.gate_bench(base, PER_STEP, args.steps, args.warmup)
+    ms, wall, tot, d2h = search_steps(dsgpu, base, args.steps, args.warmup, PER_STEP)
+    stages = dsgpu.search_stage_ms()
     clocks = clk.stop()
-    barrier()
-    ms_max, tot, value = rep.combine(ms, counts)
-
+    rep.barrier()
+    ms_max, summed, value = rep.combine(ms, tot[:4])
+    wall_max = rep.reduce([wall], "MAX")[0]
+    extra_tot = rep.reduce(tot[4:7], "SUM")
     if args.profile_run:
         if rank == 0:
-            print(json.dumps({"profile_run": True, "ms": ms_max, "kernel_ms": [float(x) for x in mk], "counts": [int(x) for x in tot]}))
+            print(json.dumps({"profile_run": True, "ms": ms_max, "counts": [int(x) for x in summed]}))
+        dsgpu.search_close()
         return
-    # end to end through the C ABI: host output buffers, device->host copies inside the timed region
-    barrier()
-    t0 = time.perf_counter()
-    s, a, c, rc = dsgpu.gate_run(base + (args.steps + args.warmup) * PER_STEP, args.steps * PER_STEP, batch=PER_STEP, cap=1 << 20)
-    e2e_s = time.perf_counter() - t0
-    barrier()
-    e2e_s = rep.reduce([e2e_s], "MAX")[0]
-    e2e_n = rep.reduce([c[3]], "SUM")[0]
-    d2h = 16 + int(c[3]) * 12 // max(1, args.steps)      # counters + (seed, amp) of survivors per step
-
-    # roofline of the dominant kernel (the anti-aliased pre-gate): corner-table gathers from shared memory
-    pre_ms = float(mk[2])
-    achieved = counts[1] * PRE_BYTES_PER_SEED / (pre_ms / 1e3) / 1e9
     sm_mhz = clocks.get("sm_mhz") or 1965.0
-    props = __import__("torch").cuda.get_device_properties(local)
-    peak = props.multi_processor_count * SMEM_BYTES_PER_CLK_PER_SM * sm_mhz * 1e6 / 1e9
     if rank != 0:
+        dsgpu.search_close()
+        if pg:
+            pg.destroy_process_group()
         return
     out = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": ms_max / args.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
-        "dtype": "fp32", "data": "synthetic",
-        "config": {"workload": "seed gate (y-phase <= 0.06, AA pre-gate >= 0.645, full gate >= 0.70) over seeds mix(2e13 + k)",
-                   "seeds_per_step": PER_STEP, "global_seeds": PER_STEP * args.steps * world, "parallelism": f"replicas{world}",
-                   "l2": "no input data: seeds are generated on the device; the per-step octave table (~0.6 KB per phase-passed seed, ~290 MB) exceeds L2"},
-        "counts": {"seeds": int(tot[0]), "phase_passed": int(tot[1]), "pre_passed": int(tot[2]), "gated": int(tot[3])},
-        "seeds_per_s": tot[0] / (ms_max / 1e3),
-        "kernel_ms": {"phase": float(mk[0]), "octave_init": float(mk[1]), "pregate": float(mk[2]), "fullgate": float(mk[3])},
-        "e2e": {"value": e2e_n / e2e_s, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": d2h},
-        "roofline": {"bound": "smem", "kernel": "k_pregate", "achieved": achieved, "peak": peak, "unit": "GB/s",
-                     "frac": achieved / peak, "traffic": counts[1] / args.steps * PRE_DRAM_BYTES_PER_SEED,
-                     "note": "shared-memory gather bytes (18 corner-table words per cell); peak = SMs x 128 B/clk at the median SM clock "
-                             "sampled during the run; traffic = DRAM bytes per launch, scaled from an ncu capture on 2^25 seed indices "
-                             "by the phase-passed seeds of a launch"},
-        "gpu_launches": 4 * args.steps,
+        "dtype": "fp32 gate/tables/scan, fp64 floods/proxy", "data": "synthetic",
+        "config": {"workload": "batched full search (production command line gate=1 gpu=1 gscan=1) over seeds mix(2e13 + k) on the "
+                               "device-resident pipeline: gate, tables/blur, scan, suppression, hot-zone floods, proxy components, exact floods",
+                   "seeds_per_step": PER_STEP, "global_seeds": PER_STEP * args.steps * world, "waves_per_step": PER_STEP >> 22,
+                   "parallelism": f"replicas{world}",
+                   "l2": "no input data (seeds generated on the device); each wave writes ~6 MiB of tables per gated seed (GBs per wave), "
+                         "larger than L2"},
+        "counts": {"seeds": int(summed[0]), "phase_passed": int(summed[1]), "pre_passed": int(summed[2]), "gated": int(summed[3]),
+                   "sites": int(extra_tot[0]), "hot_zones": int(extra_tot[1]), "big_zones": int(extra_tot[2]), "wave_flags": int(tot[7])},
+        "seeds_per_s": summed[0] / (ms_max / 1e3),
+        "e2e": {"value": summed[3] / wall_max, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": d2h,
+                "how": "wall clock of the dsg_search_run calls (C ABI) with the seed records and CSV rows copied to host memory"},
+        "gpu_launches": int(tot[9]),
+        "stages_ms": stages,
         "clocks": clocks,
     }
     if world == 1:
-        out["cpu_baseline"] = cpu_baseline()
+        gate = gate_leg(dsgpu, sm_mhz, sms)
+        out["gate"] = gate
+        out["roofline"] = dict(gate["roofline"])
+        out["roofline"]["scope"] = "k_pregate, the gate's dominant kernel, timed in the gate leg on the same seed stream"
+        out["cpu_baseline"] = cpu_baseline(os.cpu_count() or 1)
         if not args.no_extras:
-            out["pipeline"], cands = pipeline()
+            out["pipeline"], cands = searcher_runs()
             out["default_mode"] = default_mode()
-            out["flood"] = bench_floods(dsgpu, n_small=4096, rates=args.flood_rates, n_service=args.flood_requests, candidates=cands)
+            out["flood"] = bench_floods(dsgpu, sm_mhz, sms, candidates=cands, cand_start=START + (1 << 41), rates=args.flood_rates,
+                                        requests=args.flood_requests)
+    dsgpu.search_close()
     print(json.dumps(out), flush=True)
     if pg:
         pg.destroy_process_group()
@@ -440,31 +569,27 @@ def run_reference(args):
     rank, world, local = dist()
     if rank != 0:
         return
-    exe = os.path.join(ROOT, "oracle", "_ref", "dsearch_desert")
-    if not os.path.exists(exe):
+    if not ref_exe("dsearch_desert"):
         print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref/dsearch_desert not built (make ref needs the reference checkout)"}))
         return
     cores = os.cpu_count() or 1
-    per_step = max(100_000, 50_000 * cores)          # ~2.6 core-s per 50k seeds: a few seconds per step
-    total_s, scanned, done = 0.0, 0, 0
+    per_step = max(1 << 18, 65536 * cores)           # a few seconds of every stage on all host cores per step
+    total_s, gated, done = 0.0, 0, 0
     with tempfile.TemporaryDirectory() as td:
-        for it in range(args.warmup + args.steps):
-            pre = os.path.join(td, f"s{it}")
-            t0 = time.perf_counter()
-            subprocess.run([exe, str(START + it * per_step), str(per_step), pre, str(cores), "phase=0.06", "hot_min=1e9", "sites=1",
-                            "exact_n=0"], check=True, capture_output=True)
-            dt = time.perf_counter() - t0
-            if it >= args.warmup:
-                j = json.load(open(pre + ".json"))
-                total_s += dt; scanned += j["scanned"]; done += j["done"]
-    value = scanned / total_s
+        for it in range(args.warmup):                # untimed, short
+            ref_cpu_search(START + (1 << 42) + it * per_step, per_step // 16, cores, td, f"w{it}")
+        for it in range(args.steps):
+            dt, d, g = ref_cpu_search(START + it * per_step, per_step, cores, td, f"s{it}")
+            total_s += dt; gated += g; done += d
+    value = gated / total_s
     print(json.dumps({
         "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": total_s * 1e3 / args.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "fp64/fp32",
         "data": "synthetic",
-        "config": {"workload": "seed gate over seeds mix(2e13 + k): reference CPU gate (y-phase <= 0.06, sub-grid pre-gate, full tables) "
-                               "plus tables+scan of each gated seed", "seeds_per_step": per_step, "parallelism": f"{cores} host threads"},
-        "counts": {"seeds": done, "gated": scanned},
+        "config": {"workload": "batched full search over seeds mix(2e13 + k): the reference's CPU searcher, every stage at its defaults "
+                               "(its CPU gate with phase=0.06: sub-grid estimate >= 0.69, period-table amplitude >= 0.70; tables, scan, "
+                               "hot zones, proxy floods, exact floods)", "seeds_per_step": per_step, "parallelism": f"{cores} host threads"},
+        "counts": {"seeds": done, "gated": gated},
         "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": "reference",
                          "sample": f"{args.steps} x {per_step} seeds through oracle/_ref/dsearch_desert (reference sources)"},
         "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
@@ -477,15 +602,14 @@ def main():
     ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--per-step-log2", type=int, default=26, help="seed indices per step = 2^N")
-    ap.add_argument("--profile-run", action="store_true", help="device steps only (no e2e pass, no CPU baseline): for ncu captures")
-    ap.add_argument("--flood-only", action="store_true", help="only the flood measurements (batch + service)")
+    ap.add_argument("--per-step-log2", type=int, default=24, help="seed indices per step = 2^N")
+    ap.add_argument("--profile-run", action="store_true", help="device steps only (no e2e legs, no CPU baseline): for ncu captures")
+    ap.add_argument("--flood-only", action="store_true", help="only the flood measurements")
     ap.add_argument("--flood-small", type=int, default=4096)
-    ap.add_argument("--flood-large", type=int, default=None, help="limit the large (verified-find) flood class")
-    ap.add_argument("--flood-batch-only", action="store_true")
-    ap.add_argument("--flood-rates", type=float, nargs="+", default=[200.0, 1000.0, 3000.0])
-    ap.add_argument("--flood-requests", type=int, default=1500)
-    ap.add_argument("--no-extras", action="store_true", help="skip the pipeline and flood measurements of the default run")
+    ap.add_argument("--flood-large", type=int, default=4096)
+    ap.add_argument("--flood-rates", type=float, nargs="+", default=[100.0, 500.0, 1000.0, 2000.0, 3000.0, 5000.0])
+    ap.add_argument("--flood-requests", type=int, default=None, help="requests per rate (default: 20 s of arrivals, at most 10^5)")
+    ap.add_argument("--no-extras", action="store_true", help="skip the pipeline, default-mode and flood measurements")
     args = ap.parse_args()
     global PER_STEP
     PER_STEP = 1 << args.per_step_log2

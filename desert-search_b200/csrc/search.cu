@@ -72,8 +72,9 @@ enum : uint32_t { F_GATE = 1, F_RAW = 2, F_HASH = 4, F_ZONES = 8, F_CELLS = 16, 
                   F_ROWS = 512 };
 // device counters
 enum { C_NS = 0, C_NREQ = 1 /* 4 flood phases */, C_ZONES = 5, C_CHUNKS = 6, C_ROWS = 7, C_FLAGS = 8, C_NHOT = 9, C_NBIG = 10, C_SITES = 11,
-       C_ROUND = 16 /* 9 round counters */, C_TAKEN = 25, C_FERR = 26, C_BASE = 27, C_LOOPS = 28, C_PROXY = 32 /* 4 */, C_KEPT = 33,
-       C_N = 48 };
+       C_ROUND = 16 /* 9 round counters */, C_TAKEN = 25, C_FERR = 26, C_BASE = 27, C_LOOPS = 28, C_ITERS = 29, C_PROXY = 32 /* 4 */,
+       C_KEPT = 33, C_N = 48 };
+constexpr int BODY_KERNELS = 13;             // kernels of one flood-loop iteration: 6 rounds of eval + connect, the loop control
 
 struct Params {
     dsg_scan_params sp;
@@ -327,6 +328,7 @@ __global__ void k_req_start(const FloodCtl *__restrict__ ctl, const uint32_t *nr
 // iteration limit (the wave is then flagged).
 __global__ void k_loop_ctl(uint32_t *ctr, cudaGraphConditionalHandle h) {
     ctr[C_BASE] += 6;
+    ctr[C_ITERS]++;
     const uint32_t it = ++ctr[C_LOOPS];
     const bool more = ctr[C_ROUND + 0] != 0 || ctr[C_ROUND + 3] != 0;
     if (more && it >= LOOP_LIMIT) ctr[C_FLAGS] |= F_LOOP;
@@ -687,7 +689,11 @@ struct Pipeline {
     dsg_search_seed *out = nullptr; dsg_search_row *rows = nullptr;
     int grid_eval = 0, grid_conn = 0;
     cudaGraphExec_t exec = nullptr;
+    uint32_t graph_kernels = 0;                  // kernel nodes of the wave graph outside the loop bodies
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    static constexpr int NSTAGE = 8;             // gate | tables+scan | suppression+hot points | pre-floods | step-128 floods+coverage |
+    cudaEvent_t sev[NSTAGE] = {};                // proxy+components+exact starts | step-8 floods | step-4 floods+results
+    double stage_ms[NSTAGE] = {};
     // pinned host copies
     uint32_t *h_ctr = nullptr, *h_gcnt = nullptr; dsg_search_seed *h_out = nullptr; dsg_search_row *h_rows = nullptr; uint64_t *h_seeds = nullptr;
 };
@@ -738,19 +744,24 @@ void capture_wave(Pipeline &p) {
     DSG_CU(cudaStreamBeginCapture(p.st, cudaStreamCaptureModeRelaxed));
     uint32_t caps[3];
     gate::lane_caps(p.lane, caps);
+    DSG_CU(cudaEventRecord(p.sev[0], p.st));
     k_begin<<<8, 128, 0, p.st>>>(gate::lane_counts(p.lane), caps[0], caps[1], caps[2], gate::lane_survivors(p.lane), p.seeds, p.ctr);
     seed_noise_build_dev(p.seeds, p.ctr + C_NS, SC, p.noise, p.st);
     scan_seeds_device(p.noise, p.ctr + C_NS, SC, p.tabin, p.tab, p.mx, p.act, p.nact, p.raw, p.nraw, RAWCAP, p.P.sp, p.st);
+    DSG_CU(cudaEventRecord(p.sev[1], p.st));
     DSG_CU(cudaFuncSetAttribute(k_nms, cudaFuncAttributeMaxDynamicSharedMemorySize, int(NMS_SMEM)));
     k_nms<<<SC, NMS_THREADS, NMS_SMEM, p.st>>>(p.raw, p.nraw, p.P, p.sites, p.nsites, p.nbuck, p.ctr);
     k_hot<<<4 * 148, 256, 0, p.st>>>(p.noise, p.sites, p.nsites, p.ctr, p.hot);
     k_req_pre<<<4 * 148, 256, 0, p.st>>>(p.hot, p.nsites, p.ctr, p.ph[0].ctl, p.meta1, p.f1, p.f2);
     DSG_CU(cudaGetLastError());
+    DSG_CU(cudaEventRecord(p.sev[2], p.st));
     capture_phase(p, 0);
+    DSG_CU(cudaEventRecord(p.sev[3], p.st));
     k_req_128<<<4 * 148, 256, 0, p.st>>>(p.ph[0].st, p.ph[0].ctl, p.meta1, p.P, p.ctr, p.ph[1].ctl, p.meta2, p.f2);
     capture_phase(p, 1);
     k_cover<<<(SC + 63) / 64, 64, 0, p.st>>>(p.hot, p.nsites, p.f1, p.f2, FloodView{p.ph[0].ctl, p.ph[0].dir}, FloodView{p.ph[1].ctl, p.ph[1].dir},
                                                p.ph[0].st, p.ph[1].st, p.pool.T, p.P, p.cov, p.nzone, p.zslot, p.zmslot, p.ctr);
+    DSG_CU(cudaEventRecord(p.sev[4], p.st));
     k_zone_list<<<1, LIST_THREADS, 0, p.st>>>(p.nzone, p.zslot, p.zmslot, p.zfirst, p.zones, p.zmeta, p.chunks, p.ctr);
     DSG_CU(cudaGetLastError());
     proxy_components_device(p.noise, p.zones, zones::ZoneWork{p.chunks, p.ctr + C_CHUNKS}, 8 * 148, p.bits, p.par, p.rid, p.cs, p.khi, p.klo,
@@ -765,7 +776,9 @@ void capture_wave(Pipeline &p) {
     k_ring<<<8 * 148, 128, 0, p.st>>>(p.noise, world_dev(), p.tries, p.ctr);
     k_req_8<<<32, 256, 0, p.st>>>(p.tries, p.ctr, p.ph[2].ctl, p.f8);
     DSG_CU(cudaGetLastError());
+    DSG_CU(cudaEventRecord(p.sev[5], p.st));
     capture_phase(p, 2);
+    DSG_CU(cudaEventRecord(p.sev[6], p.st));
     k_retry<<<16, 256, 0, p.st>>>(p.tries, p.f8, p.ph[2].st, p.ph[2].ctl, p.ev, p.nev, p.P, p.ctr, p.ph[3].ctl, p.f4);
     capture_phase(p, 3);
     k_results<<<(SC + 127) / 128, 128, 0, p.st>>>(p.seeds, p.noise, p.mx, p.nbuck, p.nsites, p.sites, p.ev, p.nev, p.f4, p.ph[3].st, p.P, p.out,
@@ -773,8 +786,19 @@ void capture_wave(Pipeline &p) {
     k_pool_zero<<<8 * 148, 256, 0, p.st>>>(p.pool.T, p.ctr, p.pool.cap);
     k_wave_end<<<1, 1, 0, p.st>>>(p.ctr);
     DSG_CU(cudaGetLastError());
+    DSG_CU(cudaEventRecord(p.sev[7], p.st));
     cudaGraph_t g = nullptr;
     DSG_CU(cudaStreamEndCapture(p.st, &g));
+    size_t nn = 0;
+    DSG_CU(cudaGraphGetNodes(g, nullptr, &nn));
+    std::vector<cudaGraphNode_t> nodes(nn);
+    DSG_CU(cudaGraphGetNodes(g, nodes.data(), &nn));
+    p.graph_kernels = 0;
+    for (cudaGraphNode_t n : nodes) {
+        cudaGraphNodeType t;
+        DSG_CU(cudaGraphNodeGetType(n, &t));
+        p.graph_kernels += t == cudaGraphNodeTypeKernel;
+    }
     DSG_CU(cudaGraphInstantiate(&p.exec, g, 0));
     DSG_CU(cudaGraphDestroy(g));
 }
@@ -854,6 +878,7 @@ extern "C" int dsg_search_open(const dsg_search_params *q) {
         DSG_CU(cudaMallocHost(&p.h_out, SC * sizeof(dsg_search_seed))); DSG_CU(cudaMallocHost(&p.h_rows, ROWCAP * sizeof(dsg_search_row)));
         DSG_CU(cudaMallocHost(&p.h_seeds, SC * 8));
         DSG_CU(cudaEventCreate(&p.ev0)); DSG_CU(cudaEventCreate(&p.ev1));
+        for (cudaEvent_t &e : p.sev) DSG_CU(cudaEventCreate(&e));
         DSG_CU(cudaDeviceSynchronize());
         capture_wave(p);
         p.open = true;
@@ -868,13 +893,13 @@ struct Out {
     dsg_search_seed *seeds; uint32_t seed_cap, ns = 0;
     dsg_search_row *rows; uint32_t row_cap, nr = 0;
     uint64_t *unf; uint32_t unf_cap, nu = 0;
-    uint64_t tot[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+    uint64_t tot[10] = {0, 0, 0, 0, 0, 0, 0, 0, 0, 0};
     bool over = false;
     float ms = 0;
 };
 // The wave whose gated seeds are in the gate lane's survivor list (just enqueued on p.st): its graph, then its
 // records; a flagged wave hands its gated seeds back instead.
-void finish_wave(Pipeline &p, Out &o, uint64_t indices) {
+void finish_wave(Pipeline &p, Out &o, uint64_t indices, bool gated_by_lane) {
     DSG_CU(cudaGraphLaunch(p.exec, p.st));
     DSG_CU(cudaMemcpyAsync(p.h_ctr, p.ctr, C_N * 4, cudaMemcpyDeviceToHost, p.st));
     DSG_CU(cudaMemcpyAsync(p.h_gcnt, gate::lane_counts(p.lane), 16, cudaMemcpyDeviceToHost, p.st));
@@ -887,8 +912,17 @@ void finish_wave(Pipeline &p, Out &o, uint64_t indices) {
     float ms = 0;
     DSG_CU(cudaEventElapsedTime(&ms, p.ev0, p.ev1));
     o.ms += ms;
+    float st = 0;
+    DSG_CU(cudaEventElapsedTime(&st, p.ev0, p.sev[0]));
+    p.stage_ms[0] += st;
+    for (int k = 1; k < Pipeline::NSTAGE; k++) {
+        DSG_CU(cudaEventElapsedTime(&st, p.sev[k - 1], p.sev[k]));
+        p.stage_ms[k] += st;
+    }
     const uint32_t wS = p.h_ctr[C_NS];
     o.tot[0] += indices; o.tot[1] += p.h_gcnt[0]; o.tot[2] += p.h_gcnt[1]; o.tot[3] += p.h_gcnt[2];
+    o.tot[8] += p.h_ctr[C_ITERS];
+    o.tot[9] += uint64_t(p.graph_kernels) + uint64_t(BODY_KERNELS) * p.h_ctr[C_ITERS] + (gated_by_lane ? 4 : 0);
     if (p.h_ctr[C_FLAGS]) {
         o.tot[7] |= p.h_ctr[C_FLAGS];
         if (p.h_ctr[C_FLAGS] & F_GATE) { set_error("device search: gate survivors exceed the wave's capacity"); throw ArgFail{}; }
@@ -915,7 +949,7 @@ void finish_wave(Pipeline &p, Out &o, uint64_t indices) {
         o.ns++;
     }
 }
-int report(const Out &o, uint32_t *n_seeds, uint32_t *n_rows, uint32_t *n_unfinished, uint64_t counts[8], float *device_ms) {
+int report(const Out &o, uint32_t *n_seeds, uint32_t *n_rows, uint32_t *n_unfinished, uint64_t counts[10], float *device_ms) {
     *n_seeds = o.ns; *n_rows = o.nr; *n_unfinished = o.nu;
     if (counts) std::memcpy(counts, o.tot, sizeof o.tot);
     if (device_ms) *device_ms = o.ms;
@@ -927,7 +961,7 @@ int report(const Out &o, uint32_t *n_seeds, uint32_t *n_rows, uint32_t *n_unfini
 
 extern "C" int dsg_search_run(uint64_t start, uint64_t count, dsg_search_seed *seeds_out, uint32_t seed_cap, uint32_t *n_seeds,
                               dsg_search_row *rows_out, uint32_t row_cap, uint32_t *n_rows, uint64_t *unfinished, uint32_t unfinished_cap,
-                              uint32_t *n_unfinished, uint64_t counts[8], float *device_ms) {
+                              uint32_t *n_unfinished, uint64_t counts[10], float *device_ms) {
     return guarded([&] {
         DSG_ARG(n_seeds && n_rows && n_unfinished, "dsg_search_run: null pointer");
         DSG_ARG((seed_cap == 0 || seeds_out) && (row_cap == 0 || rows_out) && (unfinished_cap == 0 || unfinished), "dsg_search_run: null output");
@@ -940,7 +974,7 @@ extern "C" int dsg_search_run(uint64_t start, uint64_t count, dsg_search_seed *s
             const uint64_t nb = std::min(p.wave, count - base);
             DSG_CU(cudaEventRecord(p.ev0, p.st));
             gate::lane_enqueue(p.lane, p.st, start + base, nb, p.gcfg);
-            finish_wave(p, o, nb);
+            finish_wave(p, o, nb, true);
         }
         return report(o, n_seeds, n_rows, n_unfinished, counts, device_ms);
     });
@@ -948,7 +982,7 @@ extern "C" int dsg_search_run(uint64_t start, uint64_t count, dsg_search_seed *s
 
 extern "C" int dsg_search_seeds(const uint64_t *seeds, uint32_t n, dsg_search_seed *seeds_out, uint32_t seed_cap, uint32_t *n_seeds,
                                 dsg_search_row *rows_out, uint32_t row_cap, uint32_t *n_rows, uint64_t *unfinished, uint32_t unfinished_cap,
-                                uint32_t *n_unfinished, uint64_t counts[8], float *device_ms) {
+                                uint32_t *n_unfinished, uint64_t counts[10], float *device_ms) {
     return guarded([&] {
         DSG_ARG(n_seeds && n_rows && n_unfinished && (n == 0 || seeds), "dsg_search_seeds: null pointer");
         DSG_ARG((seed_cap == 0 || seeds_out) && (row_cap == 0 || rows_out) && (unfinished_cap == 0 || unfinished), "dsg_search_seeds: null output");
@@ -966,9 +1000,20 @@ extern "C" int dsg_search_seeds(const uint64_t *seeds, uint32_t n, dsg_search_se
             p.h_gcnt[0] = 0; p.h_gcnt[1] = 0; p.h_gcnt[2] = nb; p.h_gcnt[3] = 0;
             DSG_CU(cudaMemcpyAsync(surv, p.h_seeds, size_t(nb) * 8, cudaMemcpyHostToDevice, p.st));
             DSG_CU(cudaMemcpyAsync(gate::lane_counts(p.lane), p.h_gcnt, 16, cudaMemcpyHostToDevice, p.st));
-            finish_wave(p, o, nb);
+            finish_wave(p, o, nb, false);
         }
         return report(o, n_seeds, n_rows, n_unfinished, counts, device_ms);
+    });
+}
+
+extern "C" int dsg_search_stage_ms(double ms[8], int reset) {
+    return guarded([&] {
+        DSG_ARG(ms, "dsg_search_stage_ms: null pointer");
+        Pipeline &p = PL();
+        std::lock_guard<std::mutex> l(p.mu);
+        std::copy(p.stage_ms, p.stage_ms + Pipeline::NSTAGE, ms);
+        if (reset) std::fill(p.stage_ms, p.stage_ms + Pipeline::NSTAGE, 0.0);
+        return DSG_OK;
     });
 }
 
@@ -988,6 +1033,7 @@ extern "C" int dsg_search_close(void) {
         p.pool.release();
         cudaFreeHost(p.h_ctr); cudaFreeHost(p.h_gcnt); cudaFreeHost(p.h_out); cudaFreeHost(p.h_rows); cudaFreeHost(p.h_seeds);
         cudaEventDestroy(p.ev0); cudaEventDestroy(p.ev1);
+        for (cudaEvent_t &e : p.sev) cudaEventDestroy(e);
         cudaStreamDestroy(p.st); cudaStreamDestroy(p.body_st);
         p.open = false;
         return DSG_OK;

@@ -332,6 +332,16 @@ def search_open(**kw):
     _ck(lib.dsg_search_open(C.byref(SearchParams(**p))), "dsg_search_open")
 
 
+SEARCH_STAGES = ["gate", "tables_scan", "suppression_hot_points", "hot_pre_floods", "step128_floods_coverage", "proxy_components_starts",
+                 "step8_floods", "step4_floods_results"]
+
+
+def search_stage_ms(reset=False):
+    ms = np.zeros(8)
+    _ck(lib.dsg_search_stage_ms(ptr(ms, f64p), C.c_int(1 if reset else 0)), "dsg_search_stage_ms")
+    return dict(zip(SEARCH_STAGES, ms.tolist()))
+
+
 def search_close():
     _ck(lib.dsg_search_close(), "dsg_search_close")
 
@@ -339,7 +349,7 @@ def search_close():
 def _search_call(fn, args, seed_cap, row_cap):
     recs = np.zeros(seed_cap, dtype=SEARCH_SEED); rows = np.zeros(row_cap, dtype=SEARCH_ROW); unf = np.zeros(seed_cap, dtype=np.uint64)
     ns, nr, nu = C.c_uint32(), C.c_uint32(), C.c_uint32()
-    counts = np.zeros(8, dtype=np.uint64); ms = C.c_float()
+    counts = np.zeros(10, dtype=np.uint64); ms = C.c_float()
     rc = _ck(fn(*args, recs.ctypes.data_as(C.c_void_p), C.c_uint32(seed_cap), C.byref(ns), rows.ctypes.data_as(C.c_void_p), C.c_uint32(row_cap),
                 C.byref(nr), ptr(unf, u64p), C.c_uint32(seed_cap), C.byref(nu), ptr(counts, u64p), C.byref(ms)), fn.__name__)
     assert rc == DSG_OK, "output capacity exceeded"
@@ -355,3 +365,38 @@ def search_seeds(seeds, row_cap=1 << 18):
     """Explicit gated seeds through the device pipeline (dsg_search_seeds); returns as search_run."""
     s = np.ascontiguousarray(seeds, dtype=np.uint64)
     return _search_call(lib.dsg_search_seeds, (ptr(s, u64p), C.c_uint32(len(s))), max(1, len(s)), row_cap)
+
+
+def translation_map(lat, cell=512, period=262144, nt=60, kmin=-30, world=7499996, tn=512):
+    """The searcher's translation map of a side-A table cell (dsearch_desert.cpp:98-113) in double precision,
+    as host/dsearch_desert.cpp's TMap computes it: ib (tn, nt) int16, lo/hi (tn,) int8."""
+    import math
+    ib = np.empty((tn, nt), dtype=np.int16); lo = np.full(tn, nt, dtype=np.int8); hi = np.full(tn, -1, dtype=np.int8)
+    bs = 337.0 / 331.0
+    for i in range(tn):
+        for t in range(nt):
+            x = i * cell + (t + kmin) * period
+            u = x * bs / lat
+            u -= math.floor(u / 256.0) * 256.0
+            ib[i, t] = int(u * (tn / 256.0) + 0.5) & (tn - 1)
+            if -world + 6000 <= x <= world - 6000:
+                lo[i] = min(lo[i], t); hi[i] = max(hi[i], t)
+    return ib, lo, hi
+
+
+def blur_taps(sigma):
+    """The searcher's blur taps (lowfield.hpp:106-113): exp(-d^2 / (2 sigma^2)) in double, normalised, as float."""
+    import math
+    r = int(3 * sigma + 1)
+    kd = [math.exp(-0.5 * i * i / (sigma * sigma)) for i in range(-r, r + 1)]
+    s = 0.0
+    for v in kd:
+        s += v
+    return np.array([v / s for v in kd], dtype=np.float32)
+
+
+def scan_init_default(sigma=2.0, sigmac=2.0):
+    """dsg_scan_init with the searcher's own maps and taps (what bin/dsearch_desert passes)."""
+    ibT, loT, hiT = translation_map(1024.0)
+    ibC, _, _ = translation_map(512.0)
+    scan_init(ibT, loT, hiT, ibC, blur_taps(sigma), blur_taps(sigmac))

@@ -824,7 +824,7 @@ int main(int argc, char **argv) {
                 const uint64_t B = 1ull << 24;
                 for (uint64_t base = 0; base < total && !interrupted; base += B) {
                     const uint64_t nb = std::min(B, total - base);
-                    uint32_t ns = 0, nr = 0, nu = 0; uint64_t c[8]; float ms = 0;
+                    uint32_t ns = 0, nr = 0, nu = 0; uint64_t c[10]; float ms = 0;
                     ck(dsg_search_run(S.start + base, nb, recs.data(), uint32_t(recs.size()), &ns, rows.data(), uint32_t(rows.size()), &nr,
                                       unf.data(), uint32_t(unf.size()), &nu, c, &ms), "device search");
                     take(ns, nu, c);
@@ -841,7 +841,7 @@ int main(int argc, char **argv) {
                     in.clear();
                     while (in.size() < 1024 && !(eof = !fgets(line, sizeof line, stdin))) in.push_back(std::strtoull(line, nullptr, 10));
                     if (in.empty()) break;
-                    uint32_t ns = 0, nr = 0, nu = 0; uint64_t c[8]; float ms = 0;
+                    uint32_t ns = 0, nr = 0, nu = 0; uint64_t c[10]; float ms = 0;
                     ck(dsg_search_seeds(in.data(), uint32_t(in.size()), recs.data(), uint32_t(recs.size()), &ns, rows.data(), uint32_t(rows.size()),
                                         &nr, unf.data(), uint32_t(unf.size()), &nu, c, &ms), "device search");
                     take(ns, nu, c);

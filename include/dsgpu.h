@@ -277,17 +277,23 @@ int dsg_search_open(const dsg_search_params *p);
 /* Search seeds mix(start + k), k < count, wave by wave.  Gated seeds' records go to seeds_out (their rows to
  * rows_out, row0 re-based), in no particular order.  A wave that exceeds a fixed capacity of the pipeline
  * returns its gated seeds in `unfinished` instead: run them through the per-stage entry points.  counts =
- * {indices, phase-passed, pre-gate passed, gated, sites, hot zones used, big zones, OR of wave flags};
+ * {indices, phase-passed, pre-gate passed, gated, sites, hot zones used, big zones, OR of wave flags, flood-loop
+ * iterations, kernel launches (gate, graph nodes, loop bodies)};
  * device_ms (may be NULL) = CUDA-event time of the waves on the pipeline's stream.  DSG_OVERFLOW if an output
  * capacity was too small (outputs hold the first items). */
 int dsg_search_run(uint64_t start, uint64_t count, dsg_search_seed *seeds_out, uint32_t seed_cap, uint32_t *n_seeds,
                    dsg_search_row *rows_out, uint32_t row_cap, uint32_t *n_rows, uint64_t *unfinished, uint32_t unfinished_cap,
-                   uint32_t *n_unfinished, uint64_t counts[8], float *device_ms);
+                   uint32_t *n_unfinished, uint64_t counts[10], float *device_ms);
 /* The same for explicit gated seeds (the searcher's stdin=1 input, dsearch_desert.cpp:571-581: seeds already
  * gated elsewhere): no gate, every seed goes through the stages; counts[0..2] = 0, counts[3] = n. */
 int dsg_search_seeds(const uint64_t *seeds, uint32_t n, dsg_search_seed *seeds_out, uint32_t seed_cap, uint32_t *n_seeds,
                      dsg_search_row *rows_out, uint32_t row_cap, uint32_t *n_rows, uint64_t *unfinished, uint32_t unfinished_cap,
-                     uint32_t *n_unfinished, uint64_t counts[8], float *device_ms);
+                     uint32_t *n_unfinished, uint64_t counts[10], float *device_ms);
+/* Device ms per stage summed over the waves run since dsg_search_open (or the last reset), from events captured
+ * in the wave graph: {gate, tables + scan, suppression + hot points, hot pre-floods, step-128 floods + coverage
+ * replay, proxy components + exact-start search, step-8 floods, step-4 floods + results}.  No reference
+ * counterpart (the reference prints core-seconds per stage on its progress line, dsearch_desert.cpp:552). */
+int dsg_search_stage_ms(double ms[8], int reset);
 int dsg_search_close(void);
 
 #ifdef __cplusplus

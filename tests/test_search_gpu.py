@@ -56,6 +56,7 @@ def test_fused_equals_per_stage_on_gate_range(tmp_path):
 def test_search_run_covers_exactly_the_gate_survivors(dsg):
     """Every seed the GPU gate passes comes back once, finished or handed back, and no other seed does."""
     start, count = 7 * 10**12, 1 << 23
+    dsg.scan_init_default()
     dsg.search_open()
     try:
         recs, rows, unf, counts, ms = dsg.search_run(start, count)
