@@ -39,9 +39,12 @@ $(B)/orc_blob.o: $(B)/orc_blob.c
 	gcc -O1 -fPIC -c $< -o $@
 
 # ---- CUDA library (C ABI in include/dsgpu.h)
-# taps.cu alone keeps nvcc's default contraction: it evaluates expf exactly as the reference kernels do.
+# taps.cu keeps nvcc's default contraction: it evaluates expf exactly as the reference kernels do.
 $(B)/taps.o: $(PKG)/csrc/taps.cu $(CU_HDR) | $(B)
 	$(NVCC) $(filter-out -fmad=false,$(NVFLAGS)) -c $< -o $@ 2> $(B)/taps.ptxas.txt || (cat $(B)/taps.ptxas.txt; false)
+# proxy_f32.cu likewise: the FP32 proxy of the reference's GPU engine, with the engine's contraction.
+$(B)/proxy_f32.o: $(PKG)/csrc/proxy_f32.cu $(CU_HDR) | $(B)
+	$(NVCC) $(filter-out -fmad=false,$(NVFLAGS)) -c $< -o $@ 2> $(B)/proxy_f32.ptxas.txt || (cat $(B)/proxy_f32.ptxas.txt; false)
 $(B)/%.o: $(PKG)/csrc/%.cu $(CU_HDR) | $(B)
 	$(NVCC) $(NVFLAGS) -c $< -o $@ 2> $(B)/$*.ptxas.txt || (cat $(B)/$*.ptxas.txt; false)
 $(B)/host_%.o: $(PKG)/csrc/%.cpp $(CU_HDR) | $(B)

@@ -22,6 +22,7 @@ void require_init() {
 }
 void world_upload(int device);        // world.cpp
 void proxy_set_cut(float cut);        // proxy.cu
+void proxy32_set_cut(float cut);      // proxy_f32.cu
 }  // namespace dsg
 
 extern "C" const char *dsg_last_error(void) { return dsg::g_err; }
@@ -43,6 +44,7 @@ extern "C" int dsg_init(int device, float cut) {
             dsg::g_dev.device = device;
         }
         dsg::proxy_set_cut(cut);
+        dsg::proxy32_set_cut(cut);
         return DSG_OK;
     });
 }

@@ -139,6 +139,21 @@ int dsg_proxy_table(float prob[1600]);
  * proxy DesertProxy::prob (src/desert_proxy.hpp:24-32); replaces gproxy::evaluate (src/gpu/gproxy.h:37,
  * FP32 there).  The seed itself is passed: the device derives its noise octaves. */
 int dsg_proxy(uint64_t seed, const dsg_zone *zones, uint32_t nzones, uint8_t *bits);
+/* One Perlin octave of one noise side as the reference's GPU engine receives it: gproxy::Octave
+ * (src/gpu/gproxy.h:11-19), same layout -- permutation, frequency 2^-k, side (0 = A, 1 = B with the 337/331
+ * scale), integer and fractional offsets, the y slice (iy, fy, fade(fy)) and the weight in final units. */
+typedef struct dsg_octave {
+    uint8_t perm[256];
+    int32_t k, side, ox_i, oz_i;
+    float ox_f, oz_f;
+    int32_t iy;
+    float fy, vy, w;
+} dsg_octave;
+/* Proxy bitmaps of zones from a seed's 14 octave records in gproxy::SeedNoise order (T 0-1, C 0-2, E 0-1, sides
+ * A then B in each: t[4], c[6], e[4]), in FP32 exactly as the reference's GPU engine computes them
+ * (src/gpu/gproxy.cu:21-120); bits as dsg_proxy.  What gproxy::evaluate (gproxy.h:37) maps to for a caller that
+ * holds octave records instead of the seed; dsg_proxy (FP64) equals the CPU proxy instead. */
+int dsg_proxy_f32(const dsg_octave oct[14], const dsg_zone *zones, uint32_t nzones, uint8_t *bits);
 /* Zones of several seeds in one launch: zone k belongs to seeds[zone_seed[k]]. */
 int dsg_proxy_batch(const uint64_t *seeds, uint32_t nseeds, const uint32_t *zone_seed, const dsg_zone *zones, uint32_t nzones,
                     uint8_t *bits);

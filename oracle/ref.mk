@@ -17,7 +17,7 @@ ifeq ($(wildcard $(REF)/src/dsearch_desert.cpp),)
 all:
 	@echo "oracle/ref.mk: no reference checkout at REF=$(REF); oracle/_ref not rebuilt"
 else
-all: $(OUT)/dsearch_desert $(OUT)/dflood $(OUT)/libref_cpu.so $(OUT)/libref_gate.so $(OUT)/tgate $(OUT)/dsearch_desert_gpu
+all: $(OUT)/dsearch_desert $(OUT)/dflood $(OUT)/libref_cpu.so $(OUT)/libref_gate.so $(OUT)/tgate $(OUT)/dsearch_desert_gpu $(OUT)/dsearch_desert_shim
 
 $(OUT):
 	mkdir -p $@
@@ -34,6 +34,14 @@ $(OUT)/tgate: $(REF)/src/gpu/tgate.cu $(REF)/src/gpu/gate.cuh | $(OUT)
 	$(NVCC) -O3 -std=c++20 $(GPUARCH) $< -o $@
 
 .PHONY: all
+
+# The reference's unmodified searcher with -DDRIP_GPU linked against this repository's engine instead of its own:
+# the gproxy interface (its header) implemented over libdsgpu's C ABI (desert-search_b200/shim/gproxy_dsgpu.cpp).
+SHIM := desert-search_b200/shim/gproxy_dsgpu.cpp
+DSGLIB := desert-search_b200/lib/libdsgpu.so
+$(OUT)/dsearch_desert_shim: $(REF)/src/dsearch_desert.cpp $(REFHDR) $(REF)/src/gpu/gproxy.h $(SHIM) include/dsgpu.h $(DSGLIB) | $(OUT)
+	g++ $(CXXFLAGS) -DDRIP_GPU -I$(REF)/src/gpu -Iinclude $(REF)/src/dsearch_desert.cpp $(SHIM) -L$(dir $(DSGLIB)) -ldsgpu \
+	    -Wl,-rpath,'$$ORIGIN/../../desert-search_b200/lib' -o $@
 
 # The reference's GPU searcher (Makefile:43-46): its engine gproxy.cu for sm_100a, the searcher with -DDRIP_GPU.
 $(OUT)/gproxy.o: $(REF)/src/gpu/gproxy.cu $(REF)/src/gpu/gate.cuh $(REF)/src/gpu/gproxy.h | $(OUT)

@@ -209,3 +209,36 @@ def test_searcher_verifies_candidates_in_process(tmp_path, dsg):
     reqs = [dsg.flood_req(s & ((1 << 64) - 1), x >> 2, z >> 2, 1, 20000) for (s, x, z) in got]
     for (k, cells), area in zip(got.items(), dsg.flood_batch(reqs)):
         assert cells == area[0], k
+
+
+def test_reference_searcher_links_against_the_library(tmp_path):
+    """The reference's own searcher, src/dsearch_desert.cpp unmodified, built with -DDRIP_GPU against this
+    library through the gproxy shim (desert-search_b200/shim/gproxy_dsgpu.cpp) instead of its own engine:
+    its output equals the reference GPU searcher's.  stdin seeds (scan, FP32 proxy through dsg_proxy_f32, exact
+    floods: every file line for line) and the GPU gate over a seed range (start_gate through dsg_gate_run:
+    every seeds.csv line on the seeds both gates pass; the reference's own pre-gate is not deterministic on this
+    GPU, so a seed near a cut may be passed by one run and not the other)."""
+    shim = ref("dsearch_desert_shim")
+    seeds = "".join(f"{f['seed']}\n" for f in finds()[:24])
+    opts = ["stdin=1", "gpu=1", "gscan=1"]
+    a = run([shim, "0", "0", str(tmp_path / "shim"), "8"] + opts, stdin=seeds)
+    b = run([ref("dsearch_desert_gpu"), "0", "0", str(tmp_path / "ref"), "8"] + opts, stdin=seeds)
+    assert a.returncode == 0, a.stderr[-2000:]
+    assert b.returncode == 0, b.stderr[-2000:]
+    rd = lambda p: sorted(open(p).read().splitlines())
+    for ext in (".csv", ".seeds.csv"):
+        la, lb = rd(str(tmp_path / "shim") + ext), rd(str(tmp_path / "ref") + ext)
+        assert len(la) > 10, ext
+        assert la == lb, (ext, sorted(set(la) ^ set(lb))[:6])
+    cand = lambda s: sorted(re.findall(r"CANDIDATE step4=[\d.]+M seed=-?\d+ x=-?\d+ z=-?\d+", s))
+    assert cand(a.stderr) == cand(b.stderr) and cand(a.stderr)
+    args = ["20000000000000", str(1 << 24), "8", "gate=1", "gpu=1", "gscan=1"]
+    a = run([shim] + args[:2] + [str(tmp_path / "gs")] + args[2:])
+    b = run([ref("dsearch_desert_gpu")] + args[:2] + [str(tmp_path / "gr")] + args[2:])
+    assert a.returncode == 0, a.stderr[-2000:]
+    assert b.returncode == 0, b.stderr[-2000:]
+    sa = {l.split(",")[0]: l for l in rd(str(tmp_path / "gs.seeds.csv"))[:-1]}
+    sb = {l.split(",")[0]: l for l in rd(str(tmp_path / "gr.seeds.csv"))[:-1]}
+    common = set(sa) & set(sb)
+    assert len(common) > 0.99 * max(len(sa), len(sb)) and len(common) > 1000
+    assert all(sa[k] == sb[k] for k in common)
