@@ -1037,3 +1037,229 @@ size_t oct_bytes() { return sizeof(Oct); }
 int pregate_blocks_per_sm() { int occ = 0; cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_pregate, PG_THREADS, 0); return occ; }
 int fullgate_blocks_per_sm() { int occ = 0; cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_fullgate, FG_THREADS, 0); return occ; }
 }}
+
+// ---------------------------------------------------------------- the gate in double precision
+// The same two amplitude stages with every step in double: corner tables without the rounding to float, cell
+// sums, blur taps exp(-d^2 / (2 sigma^2)) and their sum, the two fused multiply-add blur passes, the division
+// by the squared tap sum, the maximum.  The FP64 yardstick of the FP32 gate (the reference's gate is FP32;
+// this is the same algorithm at double width), used where a seed's FP32 amplitude lies within the proven
+// error margin of a threshold.  Few seeds take this path, so it favours plainness over speed: one block per
+// (seed, side) and row, the grids in global scratch.
+namespace dsg { namespace gate {
+constexpr int G64_PRE = 256, G64_FULL = 512;
+__device__ __forceinline__ double weight64() { return 1.25 * (32.0 / 63.0) * 1.5; }
+// Corner tables of one (seed, side): tpre[288] (merged parity terms of the anti-aliased grid, gate.cuh:218-235)
+// and tfull[512] ([px*2+pz][corner][hash], gate.cuh:236-244).
+__global__ void __launch_bounds__(512) k_g64_tables(const Oct *__restrict__ oct, double *__restrict__ tpre, double *__restrict__ tfull) {
+    const Oct &p = oct[blockIdx.x];
+    const int e = threadIdx.x;
+    if (e < 288) {
+        const int h = e & 15, dy = (e >> 4) & 1, uv = e >> 5, u = uv / 3, v = uv % 3;
+        double fr[2][2]; int sh[2][2];
+        for (int ax = 0; ax < 2; ax++) {
+            const double o = ax ? p.oz : p.ox;
+            for (int q = 0; q < 2; q++) { const double b = o + 0.5 * q; fr[ax][q] = b - floor(b); sh[ax][q] = int(floor(b) - floor(o)); }
+        }
+        double acc = 0;
+        for (int px = 0; px < 2; px++)
+            for (int pz = 0; pz < 2; pz++) {
+                const int dx = u - sh[0][px], dz = v - sh[1][pz];
+                if (dx < 0 || dx > 1 || dz < 0 || dz > 1) continue;
+                const double fx = fr[0][px], fz = fr[1][pz], tx = fade_fused(fx), tz = fade_fused(fz);
+                const double wc = __dmul_rn(__dmul_rn(dx ? tx : 1 - tx, dy ? p.vy : 1 - p.vy), dz ? tz : 1 - tz);
+                acc = __fma_rn(wc, gradd(h, fx - dx, p.fy - dy, fz - dz), acc);
+            }
+        tpre[size_t(blockIdx.x) * 288 + e] = __dmul_rn(__dmul_rn(0.25, weight64()), acc);
+    }
+    {
+        const int h = e & 15, c = (e >> 4) & 7, pp = e >> 7, px = pp >> 1, pz = pp & 1;
+        const double bx = px * 0.5 + p.ox, bz = pz * 0.5 + p.oz;
+        const double fx = bx - floor(bx), fz = bz - floor(bz);
+        const double tx = fade_fused(fx), tz = fade_fused(fz), ty = p.vy;
+        const int dx = c & 1, dy = (c >> 1) & 1, dz = c >> 2;
+        const double wc = __dmul_rn(__dmul_rn(dx ? tx : 1 - tx, dy ? ty : 1 - ty), dz ? tz : 1 - tz);
+        tfull[size_t(blockIdx.x) * 512 + e] = __dmul_rn(__dmul_rn(weight64(), wc), gradd(h, fx - dx, p.fy - dy, fz - dz));
+    }
+}
+// Cell sums of row blockIdx.x of (seed, side) blockIdx.y: G = 256 (pre-gate) or 512 (full gate).
+template <int G>
+__global__ void __launch_bounds__(256) k_g64_cells(const Oct *__restrict__ oct, const double *__restrict__ tab, double *__restrict__ S) {
+    const Oct &p = oct[blockIdx.y];
+    const int r = blockIdx.x;
+    const double *T = tab + size_t(blockIdx.y) * (G == G64_PRE ? 288 : 512);
+    double *row = S + (size_t(blockIdx.y) * G + r) * G;
+    for (int i = threadIdx.x; i < G; i += blockDim.x) {
+        double acc = 0;
+        if (G == G64_PRE) {
+            const int ix0 = int(floor(p.ox)), iz0 = int(floor(p.oz));
+            for (int v = 0; v < 3; v++)
+                for (int dy = 0; dy < 2; dy++)
+                    for (int u = 0; u < 3; u++) {
+                        const int col = p.perm[(p.perm[(i + u + ix0) & 255] + p.iy + dy) & 255];
+                        acc = __dadd_rn(acc, T[((u * 3 + v) * 2 + dy) * 16 + (p.perm[(col + r + v + iz0) & 255] & 15)]);
+                    }
+        } else {
+            const int pz = r & 1, iz = (r >> 1) + int(floor(pz * 0.5 + p.oz));
+            const int px = i & 1, ix = (i >> 1) + int(floor(px * 0.5 + p.ox));
+            for (int c = 0; c < 8; c++) {
+                const int dx = c & 1, dy = (c >> 1) & 1, dz = c >> 2;
+                const int col = p.perm[(p.perm[(ix + dx) & 255] + p.iy + dy) & 255];
+                acc = __dadd_rn(acc, T[((px * 2 + pz) * 8 + c) * 16 + (p.perm[(col + iz + dz) & 255] & 15)]);
+            }
+        }
+        row[i] = acc;
+    }
+}
+// Blur taps in double and their sum (lowfield-style Gaussian, unnormalised as the gate's).
+template <int R>
+__device__ __forceinline__ double taps64(double sig, double (&k)[2 * R + 1]) {
+    double ks = 0;
+    for (int d = -R; d <= R; d++) { k[d + R] = exp(-0.5 * d * d / (sig * sig)); ks += k[d + R]; }
+    return ks;
+}
+template <int G, int R>
+__global__ void __launch_bounds__(256) k_g64_hblur(const double *__restrict__ S, double *__restrict__ H, double sig) {
+    double k[2 * R + 1];
+    taps64<R>(sig, k);
+    const size_t base = (size_t(blockIdx.y) * G + blockIdx.x) * G;
+    for (int i = threadIdx.x; i < G; i += blockDim.x) {
+        double s = 0;
+        for (int d = 0; d <= 2 * R; d++) s = __fma_rn(k[d], S[base + ((i + d - R) & (G - 1))], s);
+        H[base + i] = s;
+    }
+}
+__device__ __forceinline__ unsigned long long order64(double v) {    // unsigned order of doubles
+    const unsigned long long b = (unsigned long long)__double_as_longlong(v);
+    return (b >> 63) ? ~b : (b | 0x8000000000000000ull);
+}
+__device__ __forceinline__ double unorder64(unsigned long long o) {
+    return __longlong_as_double((long long)((o >> 63) ? (o & 0x7fffffffffffffffull) : ~o));
+}
+template <int G, int R>
+__global__ void __launch_bounds__(256) k_g64_vmax(const double *__restrict__ H, double sig, unsigned long long *__restrict__ best) {
+    __shared__ unsigned long long bm;
+    double k[2 * R + 1];
+    const double ks = taps64<R>(sig, k);
+    if (threadIdx.x == 0) bm = 0;
+    __syncthreads();
+    const int o = blockIdx.x;
+    const size_t base = size_t(blockIdx.y) * G * G;
+    unsigned long long m = 0;
+    for (int i = threadIdx.x; i < G; i += blockDim.x) {
+        double s = 0;
+        for (int d = 0; d <= 2 * R; d++) s = __fma_rn(k[d], H[base + size_t((o - R + d) & (G - 1)) * G + i], s);
+        m = max(m, order64(__ddiv_rn(s, __dmul_rn(ks, ks))));
+    }
+    atomicMax(&bm, m);
+    __syncthreads();
+    if (threadIdx.x == 0) atomicMax(&best[blockIdx.y], bm);
+}
+__global__ void k_g64_out(const unsigned long long *__restrict__ best, uint32_t n2, double *__restrict__ out) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n2) out[i] = unorder64(best[i]);
+}
+
+// FP64 side amplitudes pre[2i + s], full[2i + s] of n seeds (device pointers), on st, with scratch it allocates.
+void amps_fp64(const uint64_t *d_seeds, uint32_t n, double *d_pre, double *d_full, cudaStream_t st) {
+    constexpr uint32_t CH = 32;                              // seeds per chunk: ~300 MB of grids
+    Oct *oct; uint32_t *cnt; double *tpre, *tfull, *S, *H; unsigned long long *best;
+    DSG_CU(cudaMalloc(&oct, size_t(CH) * 2 * sizeof(Oct)));
+    DSG_CU(cudaMalloc(&cnt, 4));
+    DSG_CU(cudaMalloc(&tpre, size_t(CH) * 2 * 288 * 8)); DSG_CU(cudaMalloc(&tfull, size_t(CH) * 2 * 512 * 8));
+    DSG_CU(cudaMalloc(&S, size_t(CH) * 2 * G64_FULL * G64_FULL * 8)); DSG_CU(cudaMalloc(&H, size_t(CH) * 2 * G64_FULL * G64_FULL * 8));
+    DSG_CU(cudaMalloc(&best, size_t(CH) * 2 * 8));
+    for (uint32_t b = 0; b < n; b += CH) {
+        const uint32_t m = std::min(CH, n - b);
+        DSG_CU(cudaMemcpyAsync(cnt, &m, 4, cudaMemcpyHostToDevice, st));
+        k_octinit<<<(2 * m + 127) / 128, 128, 0, st>>>(d_seeds + b, cnt, m, oct);
+        k_g64_tables<<<2 * m, 512, 0, st>>>(oct, tpre, tfull);
+        DSG_CU(cudaMemsetAsync(best, 0, size_t(2 * m) * 8, st));
+        k_g64_cells<G64_PRE><<<dim3(G64_PRE, 2 * m), 256, 0, st>>>(oct, tpre, S);
+        k_g64_hblur<G64_PRE, 4><<<dim3(G64_PRE, 2 * m), 256, 0, st>>>(S, H, 1.0);
+        k_g64_vmax<G64_PRE, 4><<<dim3(G64_PRE, 2 * m), 256, 0, st>>>(H, 1.0, best);
+        k_g64_out<<<(2 * m + 127) / 128, 128, 0, st>>>(best, 2 * m, d_pre + 2 * size_t(b));
+        DSG_CU(cudaMemsetAsync(best, 0, size_t(2 * m) * 8, st));
+        k_g64_cells<G64_FULL><<<dim3(G64_FULL, 2 * m), 256, 0, st>>>(oct, tfull, S);
+        k_g64_hblur<G64_FULL, 7><<<dim3(G64_FULL, 2 * m), 256, 0, st>>>(S, H, 2.0);
+        k_g64_vmax<G64_FULL, 7><<<dim3(G64_FULL, 2 * m), 256, 0, st>>>(H, 2.0, best);
+        k_g64_out<<<(2 * m + 127) / 128, 128, 0, st>>>(best, 2 * m, d_full + 2 * size_t(b));
+        DSG_CU(cudaGetLastError());
+        DSG_CU(cudaStreamSynchronize(st));                   // the chunk's scratch is reused by the next
+    }
+    cudaFree(oct); cudaFree(cnt); cudaFree(tpre); cudaFree(tfull); cudaFree(S); cudaFree(H); cudaFree(best);
+}
+}}  // namespace dsg::gate
+
+extern "C" int dsg_gate_amps_fp64(const uint64_t *seeds, uint32_t n, double *pre, double *full) {
+    return guarded([&] {
+        DSG_ARG(n == 0 || (seeds && pre && full), "dsg_gate_amps_fp64: null pointer");
+        require_init();
+        if (!n) return DSG_OK;
+        uint64_t *d_s; double *d_p, *d_f;
+        cudaStream_t st;
+        DSG_CU(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
+        DSG_CU(cudaMalloc(&d_s, size_t(n) * 8)); DSG_CU(cudaMalloc(&d_p, size_t(n) * 16)); DSG_CU(cudaMalloc(&d_f, size_t(n) * 16));
+        DSG_CU(cudaMemcpyAsync(d_s, seeds, size_t(n) * 8, cudaMemcpyHostToDevice, st));
+        gate::amps_fp64(d_s, n, d_p, d_f, st);
+        DSG_CU(cudaMemcpyAsync(pre, d_p, size_t(n) * 16, cudaMemcpyDeviceToHost, st));
+        DSG_CU(cudaMemcpyAsync(full, d_f, size_t(n) * 16, cudaMemcpyDeviceToHost, st));
+        DSG_CU(cudaStreamSynchronize(st));
+        cudaFree(d_s); cudaFree(d_p); cudaFree(d_f); cudaStreamDestroy(st);
+        return DSG_OK;
+    });
+}
+
+// The gate decided in double precision at the price of the FP32 gate: the FP32 gate screens at thresholds
+// lowered by `margin`, so every seed the FP64 gate passes survives the screen as long as the FP32 amplitudes
+// are within `margin` of the FP64 ones; survivors whose FP32 amplitudes clear both thresholds by the margin
+// pass as they are, and the rest are decided by the FP64 amplitudes.
+extern "C" int dsg_gate_run_fp64(uint64_t start, uint64_t count, double maxph, double pthr, double amp, double margin, uint64_t *out_seed,
+                                 uint32_t cap, uint32_t *n_out, uint64_t counts[6]) {
+    uint64_t tot[6] = {0, 0, 0, 0, 0, 0};
+    const int rc0 = guarded([&] {
+        DSG_ARG(n_out && (cap == 0 || out_seed), "dsg_gate_run_fp64: null pointer");
+        DSG_ARG(margin >= 0 && margin < 0.1, "dsg_gate_run_fp64: margin must be in [0, 0.1)");
+        return DSG_OK;
+    });
+    if (rc0 != DSG_OK) return rc0;
+    *n_out = 0;
+    const dsg_gate_cfg screen{float(maxph), float(pthr - margin), float(amp - margin), 0};
+    const uint64_t B = 1ull << 26;
+    std::vector<uint64_t> s(1u << 20); std::vector<float> a(1u << 20);
+    bool over = false;
+    for (uint64_t base = 0; base < count; base += B) {
+        const uint64_t nb = std::min(B, count - base);
+        uint32_t n = 0; uint64_t c[4];
+        const int rc = dsg_gate_run(start + base, nb, &screen, s.data(), a.data(), uint32_t(s.size()), &n, c);
+        if (rc < 0) return rc;
+        if (rc == DSG_OVERFLOW) over = true;
+        tot[0] += c[0]; tot[1] += c[1]; tot[2] += n;
+        if (!n) continue;
+        std::vector<float> pre(2 * size_t(n)), full(2 * size_t(n));
+        int rc2 = dsg_gate_amps(s.data(), n, pre.data(), full.data());
+        if (rc2 < 0) return rc2;
+        std::vector<uint64_t> unsure;
+        std::vector<char> keep(n, 0);
+        for (uint32_t i = 0; i < n; i++) {
+            const double p32 = double(0.f + pre[2 * i] + pre[2 * i + 1]), f32 = double(0.f + full[2 * i] + full[2 * i + 1]);
+            if (p32 >= pthr + margin && f32 >= amp + margin) keep[i] = 1;
+            else unsure.push_back(s[i]);
+        }
+        tot[3] += n - unsure.size(); tot[4] += unsure.size();
+        std::vector<double> p64(2 * unsure.size()), f64(2 * unsure.size());
+        if (!unsure.empty()) {
+            rc2 = dsg_gate_amps_fp64(unsure.data(), uint32_t(unsure.size()), p64.data(), f64.data());
+            if (rc2 < 0) return rc2;
+        }
+        for (uint32_t i = 0, u = 0; i < n; i++) {
+            if (!keep[i]) { keep[i] = p64[2 * u] + p64[2 * u + 1] >= pthr && f64[2 * u] + f64[2 * u + 1] >= amp; u++; }
+            if (!keep[i]) continue;
+            tot[5]++;
+            if (*n_out < cap) out_seed[(*n_out)++] = s[i];
+            else over = true;
+        }
+    }
+    if (counts) std::memcpy(counts, tot, sizeof tot);
+    if (over) { dsg::set_error("dsg_gate_run_fp64: more survivors than capacity"); return DSG_OVERFLOW; }
+    return DSG_OK;
+}

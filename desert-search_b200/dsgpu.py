@@ -400,3 +400,21 @@ def scan_init_default(sigma=2.0, sigmac=2.0):
     ibT, loT, hiT = translation_map(1024.0)
     ibC, _, _ = translation_map(512.0)
     scan_init(ibT, loT, hiT, ibC, blur_taps(sigma), blur_taps(sigmac))
+
+
+def gate_amps_fp64(seeds):
+    """The gate's side amplitudes in double precision (dsg_gate_amps_fp64): (pre, full), arrays (n, 2) float64."""
+    s = np.ascontiguousarray(seeds, dtype=np.uint64)
+    pre = np.empty(2 * len(s)); full = np.empty(2 * len(s))
+    _ck(lib.dsg_gate_amps_fp64(ptr(s, u64p), C.c_uint32(len(s)), ptr(pre, f64p), ptr(full, f64p)), "dsg_gate_amps_fp64")
+    return pre.reshape(-1, 2), full.reshape(-1, 2)
+
+
+def gate_run_fp64(start, count, maxph=0.06, pthr=0.645, amp=0.70, margin=5e-5, cap=1 << 16):
+    """The FP64 gate's survivors by the margin-screened FP32 gate (dsg_gate_run_fp64): (seeds, counts[6])."""
+    out = np.empty(cap, dtype=np.uint64)
+    n = C.c_uint32(); counts = np.zeros(6, dtype=np.uint64)
+    rc = _ck(lib.dsg_gate_run_fp64(C.c_uint64(start), C.c_uint64(count), C.c_double(maxph), C.c_double(pthr), C.c_double(amp),
+                                   C.c_double(margin), ptr(out, u64p), C.c_uint32(cap), C.byref(n), ptr(counts, u64p)), "dsg_gate_run_fp64")
+    assert rc == DSG_OK, "capacity exceeded"
+    return out[:n.value].copy(), [int(x) for x in counts]

@@ -85,6 +85,18 @@ int dsg_gate_amps(const uint64_t *seeds, uint32_t n, float *pre, float *full);
 #define DSG_NOALLOC_MAX_SEEDS 4096
 int dsg_gate_amps_noalloc(const uint64_t *seeds, uint32_t n, float *pre, float *full, void *stream);
 
+/* The gate in double precision (no reference counterpart: the reference's gate is FP32, gate.cuh:198-346; this is
+ * the same algorithm at double width, the yardstick of the FP32 gate's error): pre-gate and full-gate side
+ * amplitudes pre[2i+s], full[2i+s] of explicit seeds, every step in double. */
+int dsg_gate_amps_fp64(const uint64_t *seeds, uint32_t n, double *pre, double *full);
+/* The FP64 gate's decision at the FP32 gate's speed: seeds mix(start + k), k < count, with y-phase <= maxph
+ * screened by the FP32 gate at pthr - margin and amp - margin (a superset of the FP64 pass set whenever the FP32
+ * amplitudes are within margin of the FP64 ones); screen survivors clearing both thresholds by the margin pass,
+ * the others are decided by dsg_gate_amps_fp64.  out_seed: the FP64 gate's survivors, ascending per 2^26 batch;
+ * counts = {indices, phase-passed, screen survivors, passed on FP32 amplitudes, decided in FP64, passed}. */
+int dsg_gate_run_fp64(uint64_t start, uint64_t count, double maxph, double pthr, double amp, double margin, uint64_t *out_seed,
+                      uint32_t cap, uint32_t *n_out, uint64_t counts[6]);
+
 /* y-phase of explicit seeds and the two fractional y offsets (fy[2i], fy[2i+1]); phase_t
  * (src/dsearch_desert.cpp:80-94). */
 int dsg_phase(const uint64_t *seeds, uint32_t n, double *phase, double *fy);
