@@ -196,6 +196,63 @@ int orc_tables_in(const TabIn *t, double sigma, double sigmac, float *out, float
     for (int s = 0; s < 2; s++) mx[s] = *std::max_element(out + size_t(s) * TN * TN, out + size_t(s + 1) * TN * TN);
     return 0;
 }
+// The same six blurred tables with every step in double (corner terms unrounded, sums, normalised taps, blur): the
+// FP64 yardstick of the FP32 period tables (not a reference function: the reference tabulates in float).
+int orc_tables_fp64(uint64_t seed, double sigma, double sigmac, double *out) {
+    const Seed S(seed);
+    const int ch[3] = {TEMP, CONT, EROS};
+    for (int k = 0; k < 6; k++) {
+        const Noise &nn = S.nz[ch[k / 2]];
+        const Octave &p = nn.oct[k & 1][0];
+        const double w = nn.factor * p.amp;
+        uint8_t col[2][256];
+        for (int x = 0; x < 256; x++) for (int dy = 0; dy < 2; dy++) col[dy][x] = p.perm[(p.perm[x] + p.iy + dy) & 255];
+        double fx[2], fz[2], T[2][2][8][16]; int i0[2], k0[2];
+        for (int par = 0; par < 2; par++) {
+            const double bx = par * 0.5 + p.ox, bz = par * 0.5 + p.oz;
+            i0[par] = int(std::floor(bx)); fx[par] = bx - std::floor(bx);
+            k0[par] = int(std::floor(bz)); fz[par] = bz - std::floor(bz);
+        }
+        for (int px = 0; px < 2; px++) for (int pz = 0; pz < 2; pz++) {
+            const double tx = fade(fx[px]), tz = fade(fz[pz]), ty = p.vy;
+            for (int c = 0; c < 8; c++) {
+                const int dx = c & 1, dy = (c >> 1) & 1, dz = c >> 2;
+                const double wc = (dx ? tx : 1 - tx) * (dy ? ty : 1 - ty) * (dz ? tz : 1 - tz);
+                for (int h = 0; h < 16; h++) T[px][pz][c][h] = w * wc * grad(h, fx[px] - dx, p.fy - dy, fz[pz] - dz);
+            }
+        }
+        double *o = out + size_t(k) * TN * TN;
+        for (int j = 0; j < TN; j++) {
+            const int pz = j & 1, iz = (j >> 1) + k0[pz];
+            for (int i = 0; i < TN; i++) {
+                const int px = i & 1, ix = (i >> 1) + i0[px];
+                double acc = 0;
+                for (int c = 0; c < 8; c++) {
+                    const int dx = c & 1, dy = (c >> 1) & 1, dz = c >> 2;
+                    acc += T[px][pz][c][p.perm[(col[dy][(ix + dx) & 255] + iz + dz) & 255] & 15];
+                }
+                o[size_t(j) * TN + i] = acc;
+            }
+        }
+        const double sg = k < 2 ? sigma : sigmac;
+        const int r = int(3 * sg + 1);
+        std::vector<double> kd(2 * r + 1), h(size_t(TN) * TN);
+        double ks = 0;
+        for (int d = -r; d <= r; d++) ks += kd[d + r] = std::exp(-0.5 * d * d / (sg * sg));
+        for (double &v : kd) v /= ks;
+        for (int j = 0; j < TN; j++) for (int i = 0; i < TN; i++) {
+            double a = 0;
+            for (int d = 0; d <= 2 * r; d++) a += kd[d] * o[size_t(j) * TN + ((i + d - r) & (TN - 1))];
+            h[size_t(j) * TN + i] = a;
+        }
+        for (int j = 0; j < TN; j++) for (int i = 0; i < TN; i++) {
+            double a = 0;
+            for (int d = 0; d <= 2 * r; d++) a += kd[d] * h[size_t((j + d - r) & (TN - 1)) * TN + i];
+            o[size_t(j) * TN + i] = a;
+        }
+    }
+    return 0;
+}
 int orc_tmap(double lat, int16_t *ib, int8_t *lo, int8_t *hi) {
     const TMap m = tmap(lat);
     std::memcpy(ib, m.ib, sizeof m.ib); std::memcpy(lo, m.lo, TN); std::memcpy(hi, m.hi, TN);

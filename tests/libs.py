@@ -39,7 +39,8 @@ def ptr(a, t):
 
 def _bind(lib, prefix):
     fns = {}
-    for name in ["phase", "noise", "points", "climate", "biome", "leaf_two_ways", "flood", "tabins", "tables", "tables_in", "tmap", "blur_taps", "noise_low"]:
+    for name in ["phase", "noise", "points", "climate", "biome", "leaf_two_ways", "flood", "tabins", "tables", "tables_in", "tmap", "blur_taps", "noise_low",
+                 "tables_fp64"]:
         f = getattr(lib, f"{prefix}_{name}", None)
         if f is not None:
             fns[name] = f
@@ -116,6 +117,12 @@ class CpuPath:
         out = np.empty(6 * 512 * 512, dtype=np.float32); mx = np.empty(2, dtype=np.float32)
         self.f["tables"](C.c_uint64(seed), C.c_double(sigma), C.c_double(sigmac), ptr(out, f32p), ptr(mx, f32p))
         return out.reshape(6, 512, 512), mx
+
+    def tables_fp64(self, seed, sigma=2.0, sigmac=2.0):
+        """The six blurred period tables in double precision (the FP64 yardstick), (6, 512, 512) float64."""
+        out = np.empty(6 * 512 * 512, dtype=np.float64)
+        self.f["tables_fp64"](C.c_uint64(seed), C.c_double(sigma), C.c_double(sigmac), ptr(out, f64p))
+        return out.reshape(6, 512, 512)
 
     def tables_in(self, tabins, sigma=2.0, sigmac=2.0):
         t = np.ascontiguousarray(tabins, dtype=np.uint8)
