@@ -28,6 +28,21 @@ __global__ void k_ring_append(const uint32_t *__restrict__ lost, uint32_t n, uin
     for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) ring[(tail + i) % cap] = lost[i];
 }
 
+// Admitted requests into their slots: block k copies staged request k's noise tables and control block to slot
+// slots[k] and clears its tile directory.
+__global__ void __launch_bounds__(256) k_admit(const uint32_t *__restrict__ slots, const FloodCtl *__restrict__ ctl_stage,
+                                               const SeedNoise *__restrict__ noise_stage, SeedNoise *__restrict__ noise, FloodCtl *__restrict__ ctl,
+                                               int32_t *__restrict__ dir) {
+    const uint32_t slot = slots[blockIdx.x];
+    const FloodCtl c = ctl_stage[blockIdx.x];
+    const uint4 *src = reinterpret_cast<const uint4 *>(noise_stage + blockIdx.x);
+    uint4 *dst = reinterpret_cast<uint4 *>(noise + slot);
+    for (int k = threadIdx.x; k < int(sizeof(SeedNoise) / 16); k += blockDim.x) dst[k] = src[k];
+    if (threadIdx.x == 0) ctl[slot] = c;
+    const int64_t len = int64_t(c.tpr) * c.tpr;
+    for (int64_t e = threadIdx.x; e < len; e += blockDim.x) dir[c.dir_off + e] = -1;
+}
+
 struct Ticket { dsg_area area{}; int status = 2; };        // 2 = pending
 
 struct Service {
@@ -54,6 +69,9 @@ struct Service {
     uint32_t *d_ctr = nullptr, *h_ctr = nullptr;               // [0] taken, [1] returned, [2..10] round counters (launch_round), [11] error flags
     unsigned long long *d_evals = nullptr;                     // sub-blocks evaluated since open
     uint32_t *d_slots = nullptr; uint64_t *d_seeds = nullptr;
+    // admission staging in pinned memory: written by the engine between rounds, read by the stream's copies,
+    // which finish before the engine's next synchronisation (every iteration synchronises after its rounds)
+    uint64_t *h_adm_seeds = nullptr; FloodCtl *h_adm_ctl = nullptr, *d_adm_ctl = nullptr; uint32_t *h_adm_slots = nullptr, *d_adm_slots = nullptr;
     int grid_eval = 0, grid_conn = 0;
     int64_t dir_max = 0;                                       // largest directory of an admitted request
 };
@@ -77,10 +95,8 @@ void engine_loop(Service &g) {
     const uint32_t S = g.cfg.max_requests, K = std::max<uint32_t>(1, g.cfg.rounds_per_check);
     const uint32_t cap = g.pool.cap, reserve = std::max<uint32_t>(64, cap / 64);
     uint32_t round = 0;                                        // the next round to run
-    std::vector<uint32_t> adm_slots; std::vector<uint64_t> adm_seeds;
     for (;;) {
-        adm_slots.clear(); adm_seeds.clear();
-        std::vector<FloodCtl> adm_ctl;
+        uint32_t na = 0;                                       // requests admitted in this iteration (pinned staging)
         {
             std::unique_lock<std::mutex> l(g.mu);
             g.cv_engine.wait(l, [&] {
@@ -107,7 +123,7 @@ void engine_loop(Service &g) {
                 g.slots[si] = {true, g.pending.front().first, off, len};
                 g.pending.pop_front();
                 g.dir_max = std::max(g.dir_max, len);
-                adm_slots.push_back(si); adm_seeds.push_back(q.seed); adm_ctl.push_back(c);
+                g.h_adm_slots[na] = si; g.h_adm_seeds[na] = q.seed; g.h_adm_ctl[na] = c; na++;
                 inflight++; g.admitted++;
             }
         }
@@ -115,21 +131,15 @@ void engine_loop(Service &g) {
             cudaStream_t st = g.st;
             const uint32_t tail = (g.head + g.avail) % cap;           // first empty ring slot; fixed until avail grows
             const TileAlloc ta{g.d_ring, g.head, g.avail, cap, g.d_ctr + 0, g.d_ctr + 1, g.d_lost};
-            if (!adm_slots.empty()) {
-                const uint32_t na = uint32_t(adm_slots.size());
-                DSG_CU(cudaMemcpyAsync(g.d_seeds, adm_seeds.data(), na * 8, cudaMemcpyHostToDevice, st));
+            if (na) {
+                DSG_CU(cudaMemcpyAsync(g.d_seeds, g.h_adm_seeds, na * 8, cudaMemcpyHostToDevice, st));
+                DSG_CU(cudaMemcpyAsync(g.d_adm_ctl, g.h_adm_ctl, na * sizeof(FloodCtl), cudaMemcpyHostToDevice, st));
+                DSG_CU(cudaMemcpyAsync(g.d_adm_slots, g.h_adm_slots, na * 4, cudaMemcpyHostToDevice, st));
                 seed_noise_build(g.d_seeds, na, g.d_noise_stage, st);
-                for (uint32_t k = 0; k < na; k++) {
-                    DSG_CU(cudaMemcpyAsync(g.d_noise + adm_slots[k], g.d_noise_stage + k, sizeof(SeedNoise), cudaMemcpyDeviceToDevice, st));
-                    DSG_CU(cudaMemcpyAsync(g.d_ctl + adm_slots[k], &adm_ctl[k], sizeof(FloodCtl), cudaMemcpyHostToDevice, st));
-                    DSG_CU(cudaMemsetAsync(g.d_dir + adm_ctl[k].dir_off, 0xFF, size_t(g.slots[adm_slots[k]].dir_len) * 4, st));
-                }
-                DSG_CU(cudaMemcpyAsync(g.d_slots, adm_slots.data(), na * 4, cudaMemcpyHostToDevice, st));
-                k_tile_start<<<(na + 127) / 128, 128, 0, st>>>(g.d_ctl, g.d_slots, na, g.d_stat, g.d_dir, g.pool.T, ta,
+                k_admit<<<na, 256, 0, st>>>(g.d_adm_slots, g.d_adm_ctl, g.d_noise_stage, g.d_noise, g.d_ctl, g.d_dir);
+                k_tile_start<<<(na + 127) / 128, 128, 0, st>>>(g.d_ctl, g.d_adm_slots, na, g.d_stat, g.d_dir, g.pool.T, ta,
                                                                g.pool.n_list[round & 1], g.d_ctr + 2 + round % 3, round, g.d_active, g.d_ctr + 11);
                 DSG_CU(cudaGetLastError());
-                // ctl/slots are host vectors: finish these copies before they go out of scope
-                DSG_CU(cudaStreamSynchronize(st));
             }
             for (uint32_t k = 0; k < K; k++, round++)
                 launch_round(g.pool, round, g.d_ctr + 2, g.d_active, g.d_ctr + 11, g.d_evals, g.d_ctl, g.d_noise, g.d_dir, g.d_stat, ta,
@@ -226,6 +236,11 @@ extern "C" int dsg_service_open(const dsg_service_cfg *cfg_in) {
         DSG_CU(cudaMallocHost(&g.h_active, size_t(S) * 4));
         DSG_CU(cudaMalloc(&g.d_slots, size_t(S) * 4));
         DSG_CU(cudaMalloc(&g.d_seeds, size_t(S) * 8));
+        DSG_CU(cudaMallocHost(&g.h_adm_seeds, size_t(S) * 8));
+        DSG_CU(cudaMallocHost(&g.h_adm_ctl, size_t(S) * sizeof(FloodCtl)));
+        DSG_CU(cudaMallocHost(&g.h_adm_slots, size_t(S) * 4));
+        DSG_CU(cudaMalloc(&g.d_adm_ctl, size_t(S) * sizeof(FloodCtl)));
+        DSG_CU(cudaMalloc(&g.d_adm_slots, size_t(S) * 4));
         // budget: a quarter for tile directories, the rest for tiles, their queues and their free ring
         g.dir_cap = int64_t(c.budget_bytes / 4 / 4);
         DSG_CU(cudaMalloc(&g.d_dir, size_t(g.dir_cap) * 4));
@@ -327,7 +342,8 @@ extern "C" int dsg_service_close(void) {
         std::lock_guard<std::mutex> l(g.mu);
         cudaStreamSynchronize(g.st);
         cudaFree(g.d_ctl); cudaFree(g.d_stat); cudaFree(g.d_noise); cudaFree(g.d_noise_stage); cudaFree(g.d_active); cudaFreeHost(g.h_active);
-        cudaFree(g.d_slots); cudaFree(g.d_seeds); cudaFree(g.d_dir); cudaFree(g.d_ring); cudaFree(g.d_lost); cudaFree(g.d_ctr);
+        cudaFree(g.d_slots); cudaFree(g.d_seeds); cudaFree(g.d_dir);
+        cudaFreeHost(g.h_adm_seeds); cudaFreeHost(g.h_adm_ctl); cudaFreeHost(g.h_adm_slots); cudaFree(g.d_adm_ctl); cudaFree(g.d_adm_slots); cudaFree(g.d_ring); cudaFree(g.d_lost); cudaFree(g.d_ctr);
         cudaFreeHost(g.h_ctr); cudaFree(g.d_evals);
         g.pool.release();
         cudaStreamDestroy(g.st);
