@@ -22,6 +22,7 @@
 //    window and world, border = a touched cell outside the world, edge = an R cell on the window boundary.
 #pragma once
 #include "noise.cuh"
+#include "kernels_tuned.h"
 #include <algorithm>
 
 namespace dsg {
@@ -148,7 +149,7 @@ static __global__ void __launch_bounds__(EVAL_THREADS) k_tile_eval(const FloodCt
     __shared__ uint32_t s_run;
     const uint32_t items = *q.n_cnt;
     const uint32_t round = round_of(q);
-    const uint32_t run = max(1u, min(16u, items / (4 * gridDim.x)));
+    const uint32_t run = max(1u, min(uint32_t(DSG_EVAL_RUN), items / (4 * gridDim.x)));
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     int staged = -1;                                      // every thread walks the same items: no shared copy needed
     for (;;) {
@@ -628,6 +629,7 @@ inline void launch_round(const TilePool &p, uint32_t round, uint32_t *cnt, uint3
 inline void round_grids(int &grid_eval, int &grid_conn) {
     int occ = 0;
     DSG_CU(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_tile_eval, EVAL_THREADS, 0));
+    if (DSG_EVAL_BLOCKS > 0) occ = std::min(occ, DSG_EVAL_BLOCKS);
     grid_eval = std::max(1, occ) * device_info().sms;
     DSG_CU(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_tile_connect, 256, 0));
     grid_conn = std::max(1, occ) * device_info().sms;

@@ -14,6 +14,7 @@
 //  * k_tabins: the table inputs of a seed (tab_setup, lowfield.hpp:14-33) from its device noise tables, for
 //    dsg_scan_seeds.
 #include "noise.cuh"
+#include "kernels_tuned.h"
 #include <algorithm>
 #include <mutex>
 #include <utility>
@@ -321,7 +322,7 @@ void tables_radius(const TabJob &j, uint32_t S, int tab0, int ntab) {
         return std::max(1, occ) * device_info().sms;
     }();
     int split = 1;
-    while (split < 8 && uint64_t(S) * ntab * split < uint64_t(4) * slots) split *= 2;
+    while (split < 8 && uint64_t(S) * ntab * split < uint64_t(DSG_TAB_WAVES) * slots) split *= 2;
     TableTaps tp{};
     std::copy(j.sc.kT, j.sc.kT + 2 * RMAX + 1, tp.k[0]);
     std::copy(j.sc.kC, j.sc.kC + 2 * RMAX + 1, tp.k[1]);

@@ -2,13 +2,14 @@
 // device-resident searcher that builds zones on the device.
 #pragma once
 #include <cstdint>
+#include "kernels_tuned.h"
 
 namespace dsg {
 namespace zones {
 // One zone: origin in quarts, step-32 cells nx x nz (row-major, z outer), its first cell in the concatenated
 // bitmap, and the index of its seed's noise tables.
 struct DZone { int32_t x0, z0, nx, nz; int64_t off; int32_t seed, pad; };
-constexpr int CHUNK = 2048;                 // cells per block step of the zone kernels
+constexpr int CHUNK = DSG_ZONE_CHUNK;       // cells per block step of the zone kernels
 // Chunk list of zones built on the device: chunk k covers cells [chunk[k].y * CHUNK, + CHUNK) of zone chunk[k].x.
 // A null chunk list means the host-known layout: zone blockIdx.x, chunk blockIdx.y.
 struct ZoneWork { const uint2 *chunk; const uint32_t *nchunk; };

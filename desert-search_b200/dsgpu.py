@@ -10,7 +10,7 @@ import os
 import numpy as np
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-LIB_PATH = os.path.join(HERE, "lib", "libdsgpu.so")
+LIB_PATH = os.environ.get("DSGPU_LIB") or os.path.join(HERE, "lib", "libdsgpu.so")   # DSGPU_LIB: another build (the tuners)
 
 DSG_OK, DSG_OVERFLOW = 0, 1
 
