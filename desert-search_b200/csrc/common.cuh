@@ -19,7 +19,7 @@ struct ArgFail {};
 #define DSG_ARG(cond, msg) do { if (!(cond)) { ::dsg::set_error("%s", msg); throw ::dsg::ArgFail{}; } } while (0)
 template <class F> int guarded(F &&f) {
     try { return f(); }
-    catch (const CudaFail &) { return DSG_E_CUDA; }
+    catch (const CudaFail &) { (void)cudaGetLastError(); return DSG_E_CUDA; }   // the failure is reported here, not again by a later call
     catch (const ArgFail &) { return DSG_E_ARG; }
     catch (const std::exception &ex) { set_error("%s", ex.what()); return DSG_E_STATE; }
 }

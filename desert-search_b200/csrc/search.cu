@@ -36,8 +36,8 @@ const uint64_t *lane_survivors(const Lane *l);
 uint32_t *lane_counts(Lane *l);
 void lane_caps(const Lane *l, uint32_t caps[3]);
 }  // namespace gate
-void scan_seeds_device(const SeedNoise *noise, const uint32_t *n_dev, uint32_t cap_seeds, void *tabin, float *tab, float *mx, int32_t *act,
-                       uint32_t *nact, dsg_cand *cand, uint32_t *ncand, uint32_t cap, const dsg_scan_params &sp, cudaStream_t st);
+int scan_seeds_device(const SeedNoise *noise, const uint32_t *n_dev, uint32_t cap_seeds, void *tabin, float *tab, float *mx, int32_t *act,
+                      uint32_t *nact, dsg_cand *cand, uint32_t *ncand, uint32_t cap, const dsg_scan_params &sp, cudaStream_t st);
 size_t tabin_bytes();
 void proxy_components_device(const SeedNoise *noise, const zones::DZone *zones, const zones::ZoneWork &wk, uint32_t grid_blocks, uint8_t *bits,
                              int32_t *par, int32_t *rid, zones::CompStat *cs, uint64_t *khi, uint32_t *klo, dsg_component *rec, uint32_t *ctr,
@@ -174,37 +174,40 @@ __global__ void __launch_bounds__(NMS_THREADS) k_nms(const dsg_cand *__restrict_
         while (key[h] != k) h = (h + 1) & (HT - 1);
         if (0xffffffffu - uint32_t(best[h]) == scan_order(c.x, c.z)) bidx[h] = i;
     }
-    // occupied slots, sorted by first-seen order (bitonic over (first, slot) keys in `best`, now free)
+    // occupied slots compacted into `best` (now free) as (first, slot) keys, sorted into first-seen order by a
+    // bitonic sort over the next power of two
     __syncthreads();
-    for (int k = threadIdx.x; k < HT; k += blockDim.x) best[k] = key[k] != ~0ull ? (uint64_t(first[k]) << 32) | uint32_t(k) : ~0ull;
+    for (int k = threadIdx.x; k < HT; k += blockDim.x)
+        if (key[k] != ~0ull) best[atomicAdd(&s_m, 1u)] = (uint64_t(first[k]) << 32) | uint32_t(k);
     __syncthreads();
-    for (int size = 2; size <= HT; size <<= 1)
-        for (int stride = size >> 1; stride > 0; stride >>= 1) {
-            for (int i = threadIdx.x; i < HT / 2; i += blockDim.x) {
-                const int lo = 2 * i - (i & (stride - 1)), hi = lo + stride;
+    const uint32_t m = s_m;
+    uint32_t p2 = 2;
+    while (p2 < m) p2 <<= 1;
+    for (uint32_t k = m + threadIdx.x; k < p2; k += blockDim.x) best[k] = ~0ull;
+    __syncthreads();
+    for (uint32_t size = 2; size <= p2; size <<= 1)
+        for (uint32_t stride = size >> 1; stride > 0; stride >>= 1) {
+            for (uint32_t i = threadIdx.x; i < p2 / 2; i += blockDim.x) {
+                const uint32_t lo = 2 * i - (i & (stride - 1)), hi = lo + stride;
                 const bool up = (lo & size) == 0;
                 const unsigned long long a = best[lo], b = best[hi];
                 if ((a > b) == up) { best[lo] = b; best[hi] = a; }
             }
             __syncthreads();
         }
-    for (int k = threadIdx.x; k < HT; k += blockDim.x)
-        if (best[k] != ~0ull && bidx[uint32_t(best[k])] == 0xffffffffu) s_flag = 1;     // cannot happen: each best is a candidate
+    for (uint32_t k = threadIdx.x; k < m; k += blockDim.x)
+        if (bidx[uint32_t(best[k])] == 0xffffffffu) s_flag = 1;     // cannot happen: each best is a candidate
     __syncthreads();
     if (s_flag) {
         if (threadIdx.x == 0) { atomicOr(ctr + C_FLAGS, F_HASH); nsites[s] = 0; nbuck[s] = 0; }
         return;
     }
-    for (int k = threadIdx.x; k < HT; k += blockDim.x)
-        if (best[k] != ~0ull) {
-            const uint32_t slot = uint32_t(best[k]);
-            order[k] = uint16_t(k);
-            sv[k] = rc[bidx[slot]].s;
-            first[k] = bidx[slot];                 // position k (first-seen order) -> raw index
-            atomicAdd(&s_m, 1u);
-        }
-    __syncthreads();
-    const uint32_t m = s_m;
+    for (uint32_t k = threadIdx.x; k < m; k += blockDim.x) {
+        const uint32_t slot = uint32_t(best[k]);
+        order[k] = uint16_t(k);
+        sv[k] = rc[bidx[slot]].s;
+        first[k] = bidx[slot];                     // position k (first-seen order) -> raw index
+    }
     // std::sort(cand, score descending) over the buckets in first-seen order
     if (threadIdx.x == 0) dsg::stl::sort(order, int64_t(m), [&](uint16_t a, uint16_t b) { return sv[a] > sv[b]; });
     __syncthreads();
@@ -747,7 +750,7 @@ void capture_wave(Pipeline &p) {
     DSG_CU(cudaEventRecord(p.sev[0], p.st));
     k_begin<<<8, 128, 0, p.st>>>(gate::lane_counts(p.lane), caps[0], caps[1], caps[2], gate::lane_survivors(p.lane), p.seeds, p.ctr);
     seed_noise_build_dev(p.seeds, p.ctr + C_NS, SC, p.noise, p.st);
-    scan_seeds_device(p.noise, p.ctr + C_NS, SC, p.tabin, p.tab, p.mx, p.act, p.nact, p.raw, p.nraw, RAWCAP, p.P.sp, p.st);
+    const int table_launches = scan_seeds_device(p.noise, p.ctr + C_NS, SC, p.tabin, p.tab, p.mx, p.act, p.nact, p.raw, p.nraw, RAWCAP, p.P.sp, p.st);
     DSG_CU(cudaEventRecord(p.sev[1], p.st));
     DSG_CU(cudaFuncSetAttribute(k_nms, cudaFuncAttributeMaxDynamicSharedMemorySize, int(NMS_SMEM)));
     k_nms<<<SC, NMS_THREADS, NMS_SMEM, p.st>>>(p.raw, p.nraw, p.P, p.sites, p.nsites, p.nbuck, p.ctr);
@@ -789,16 +792,10 @@ void capture_wave(Pipeline &p) {
     DSG_CU(cudaEventRecord(p.sev[7], p.st));
     cudaGraph_t g = nullptr;
     DSG_CU(cudaStreamEndCapture(p.st, &g));
-    size_t nn = 0;
-    DSG_CU(cudaGraphGetNodes(g, nullptr, &nn));
-    std::vector<cudaGraphNode_t> nodes(nn);
-    DSG_CU(cudaGraphGetNodes(g, nodes.data(), &nn));
-    p.graph_kernels = 0;
-    for (cudaGraphNode_t n : nodes) {
-        cudaGraphNodeType t;
-        DSG_CU(cudaGraphNodeGetType(n, &t));
-        p.graph_kernels += t == cudaGraphNodeTypeKernel;
-    }
+    // kernel nodes outside the loop bodies: 6 set-up/scan kernels and the table launches, 6 for suppression, hot
+    // points, requests, coverage and zones, 9 for the proxy bitmaps and labelling, 10 for components, exact starts,
+    // retries, results and the wave's end, and 5 per flood phase
+    p.graph_kernels = 6 + table_launches + 6 + 9 + 10 + 4 * 5;
     DSG_CU(cudaGraphInstantiate(&p.exec, g, 0));
     DSG_CU(cudaGraphDestroy(g));
 }

@@ -363,8 +363,8 @@ __global__ void k_fill_f32(float *__restrict__ p, float v, uint32_t n) {
 // Tables, blur, maxima, active cells and the translation scan for seeds whose noise tables and count are on the
 // device (the device-resident searcher): grids cover cap_seeds, blocks of seeds at or beyond *n_dev return at
 // once.  Needs dsg_scan_init.  cand holds cap candidates per seed (dsg_cand layout), ncand the counts (a count
-// above cap means the seed overflowed).  Everything is enqueued on st.
-void scan_seeds_device(const SeedNoise *noise, const uint32_t *n_dev, uint32_t cap_seeds, void *tabin, float *tab, float *mx, int32_t *act,
+// above cap means the seed overflowed).  Everything is enqueued on st; returns the number of k_tables launches.
+int scan_seeds_device(const SeedNoise *noise, const uint32_t *n_dev, uint32_t cap_seeds, void *tabin, float *tab, float *mx, int32_t *act,
                        uint32_t *nact, dsg_cand *cand, uint32_t *ncand, uint32_t cap, const dsg_scan_params &sp, cudaStream_t st) {
     using namespace tables;
     State &g = S();
@@ -379,6 +379,7 @@ void scan_seeds_device(const SeedNoise *noise, const uint32_t *n_dev, uint32_t c
     k_scan<<<dim3(SCAN_BLOCKS, cap_seeds), 256, 0, st>>>(tab, act, nact, g.d_ibT, g.d_ibC, g.d_loT, g.d_hiT, sp, g.sc,
                                                          reinterpret_cast<Cand *>(cand), ncand, cap, n_dev);
     DSG_CU(cudaGetLastError());
+    return g.sc.rT == g.sc.rC ? 1 : 2;
 }
 size_t tabin_bytes() { return sizeof(tables::TabIn); }
 }  // namespace dsg

@@ -54,19 +54,18 @@ def build(outdir):
         if os.path.exists(os.path.join(d, "lib", "libdsgpu.so")):
             continue
         bdir = os.path.join(d, "_build")
+        os.makedirs(os.path.join(d, "lib"), exist_ok=True)
         flags = " ".join(f"-D{k}={v}" for k, v in defs.items())
+        # the candidate's objects and library in its own folder: the default build is not touched
         r = subprocess.run(["make", "-C", ROOT, "-j", str(os.cpu_count() or 4), "lib", f"B={os.path.relpath(bdir, ROOT)}",
-                            f"NVCC=nvcc {flags}"], capture_output=True, text=True)
+                            f"LIB={os.path.relpath(os.path.join(d, 'lib', 'libdsgpu.so'), ROOT)}", f"NVCC=nvcc {flags}"],
+                           capture_output=True, text=True)
         if r.returncode:
             raise RuntimeError(r.stderr[-2000:])
-        os.makedirs(os.path.join(d, "lib"), exist_ok=True)
-        shutil.copy(os.path.join(ROOT, "desert-search_b200", "lib", "libdsgpu.so"), os.path.join(d, "lib", "libdsgpu.so"))
         shutil.rmtree(bdir, ignore_errors=True)
         with open(os.path.join(d, "defines.json"), "w") as f:
             json.dump(defs, f)
         print(name, "built", flush=True)
-    os.remove(os.path.join(ROOT, "desert-search_b200", "lib", "libdsgpu.so"))           # relink the default build
-    subprocess.check_call(["make", "-C", ROOT, "-j", str(os.cpu_count() or 4), "lib"], stdout=subprocess.DEVNULL)
 
 
 def child(lib_path, reps):
