@@ -51,20 +51,16 @@ using zones::CHUNK;
 
 constexpr int PERIOD = 262144, CELL = 512, KMIN = -30;
 // capacities of one wave
-constexpr uint32_t SC = 1024;                // gated seeds
+constexpr uint32_t SC_MAX = 1024;            // gated seeds per wave (at most; dsg_search_params.seeds_cap)
 constexpr uint32_t RAWCAP = 1u << 16;        // raw scan candidates per seed (the reference's per-seed buffer, gproxy.cu:209)
 constexpr int HT = 4096;                     // bucket hash slots per seed (shared memory)
 constexpr uint32_t MS = 300;                 // sites per seed (Params.max_sites at most this)
 constexpr uint32_t ZPS = 64;                 // big hot zones per seed
-constexpr uint32_t ZCAP = 8192;              // zones per wave
-constexpr uint32_t CELLCAP = 1u << 25;       // proxy cells per wave
-constexpr uint32_t CHCAP = CELLCAP / CHUNK + ZCAP;
+// zones, proxy cells and flood tiles per wave are set for SC_MAX seeds and scale with seeds_cap (Pipeline::caps)
 constexpr uint32_t EVC = 128;                // proxy components kept per seed
 constexpr int EXN = 2;                       // exact floods per seed (Params.exact_n at most this)
-constexpr uint32_t TRIES = SC * EXN * 3;     // exact-flood starts: the start and two alternatives
 constexpr uint32_t ROWCAP = 1u << 16;        // CSV rows per wave
 constexpr uint32_t LOOP_LIMIT = 2048;        // flood loop iterations (6 rounds each) before a wave gives up
-constexpr uint32_t POOL_TILES = 3u << 20;    // flood tiles (1.7 KB each)
 constexpr int RING = 289;                    // exact-start search points: rings 0..8 of 16 quarts
 
 // wave flags (ctr[C_FLAGS]): a set bit means the wave's results are incomplete
@@ -94,12 +90,13 @@ struct Try { int32_t sx, sz; int32_t q; int32_t valid; };
 __constant__ int8_t c_ring[RING][2];                       // (dx, dz) of the exact-start search, in the reference's order
 
 // ---------------------------------------------------------------- wave set-up
-__global__ void k_begin(const uint32_t *gcount, uint32_t cap1, uint32_t cap2, uint32_t cap3, const uint64_t *surv, uint64_t *seeds, uint32_t *ctr) {
-    const uint32_t n3 = gcount[2], nS = min(n3, SC);
+__global__ void k_begin(const uint32_t *gcount, uint32_t cap1, uint32_t cap2, uint32_t cap3, uint32_t sc, const uint64_t *surv, uint64_t *seeds,
+                        uint32_t *ctr) {
+    const uint32_t n3 = gcount[2], nS = min(n3, sc);
     if (blockIdx.x == 0 && threadIdx.x == 0) {
         for (int k = 0; k < C_N; k++) if (k != C_TAKEN && k != C_BASE) ctr[k] = 0;
         ctr[C_NS] = nS;
-        if (gcount[0] > cap1 || gcount[1] > cap2 || n3 > cap3 || n3 > SC) ctr[C_FLAGS] |= F_GATE;
+        if (gcount[0] > cap1 || gcount[1] > cap2 || n3 > cap3 || n3 > sc) ctr[C_FLAGS] |= F_GATE;
     }
     for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < nS; i += gridDim.x * blockDim.x) seeds[i] = surv[i];
 }
@@ -414,12 +411,13 @@ __global__ void k_cover(const Hot *__restrict__ hot, const uint32_t *__restrict_
 constexpr int LIST_THREADS = 1024;
 __global__ void __launch_bounds__(LIST_THREADS) k_zone_list(const uint32_t *__restrict__ nzone, const DZone *__restrict__ zslot,
                                                             const ZoneMeta *__restrict__ zmeta, uint32_t *__restrict__ zfirst, DZone *__restrict__ zones,
-                                                            ZoneMeta *__restrict__ meta, uint2 *__restrict__ chunks, uint32_t *ctr) {
+                                                            ZoneMeta *__restrict__ meta, uint2 *__restrict__ chunks, uint32_t *ctr, uint32_t ZCAP,
+                                                            uint64_t CELLCAP, uint64_t CHCAP) {
     using Scan = cub::BlockScan<uint64_t, LIST_THREADS>;
     __shared__ typename Scan::TempStorage tmp;
     __shared__ uint64_t s_base[2];
     const uint32_t nS = ctr[C_NS];
-    // zone offsets per seed (one seed per thread, SC <= LIST_THREADS)
+    // zone offsets per seed (one seed per thread, seeds per wave <= LIST_THREADS)
     const uint32_t s = threadIdx.x;
     uint64_t cnt = s < nS ? nzone[s] : 0, off = 0, total = 0;
     Scan(tmp).ExclusiveSum(cnt, off, total);
@@ -663,9 +661,25 @@ template <class T> T *dalloc(size_t n) {
 
 struct Phase { FloodCtl *ctl; FloodStat *st; int32_t *dir; uint32_t per_req; uint32_t cap; };
 
+struct Caps {
+    uint32_t sc, zcap, tries;
+    uint64_t cellcap, chcap;
+    uint32_t pool_tiles;
+    explicit Caps(uint32_t seeds = SC_MAX) {
+        sc = seeds;
+        const double f = double(seeds) / SC_MAX;
+        zcap = std::max<uint32_t>(256, uint32_t(8192 * f));
+        cellcap = std::max<uint64_t>(1u << 20, uint64_t(double(1u << 25) * f));
+        chcap = cellcap / CHUNK + zcap;
+        tries = seeds * EXN * 3;
+        pool_tiles = std::max<uint32_t>(1u << 16, uint32_t(double(3u << 20) * f));
+    }
+};
+
 struct Pipeline {
     std::mutex mu;
     bool open = false;
+    Caps c{};
     Params P{};
     dsg_gate_cfg gcfg{};
     uint64_t wave = 0;
@@ -748,7 +762,8 @@ void capture_wave(Pipeline &p) {
     uint32_t caps[3];
     gate::lane_caps(p.lane, caps);
     DSG_CU(cudaEventRecord(p.sev[0], p.st));
-    k_begin<<<8, 128, 0, p.st>>>(gate::lane_counts(p.lane), caps[0], caps[1], caps[2], gate::lane_survivors(p.lane), p.seeds, p.ctr);
+    const uint32_t SC = p.c.sc;
+    k_begin<<<8, 128, 0, p.st>>>(gate::lane_counts(p.lane), caps[0], caps[1], caps[2], SC, gate::lane_survivors(p.lane), p.seeds, p.ctr);
     seed_noise_build_dev(p.seeds, p.ctr + C_NS, SC, p.noise, p.st);
     const int table_launches = scan_seeds_device(p.noise, p.ctr + C_NS, SC, p.tabin, p.tab, p.mx, p.act, p.nact, p.raw, p.nraw, RAWCAP, p.P.sp, p.st);
     DSG_CU(cudaEventRecord(p.sev[1], p.st));
@@ -765,12 +780,12 @@ void capture_wave(Pipeline &p) {
     k_cover<<<(SC + 63) / 64, 64, 0, p.st>>>(p.hot, p.nsites, p.f1, p.f2, FloodView{p.ph[0].ctl, p.ph[0].dir}, FloodView{p.ph[1].ctl, p.ph[1].dir},
                                                p.ph[0].st, p.ph[1].st, p.pool.T, p.P, p.cov, p.nzone, p.zslot, p.zmslot, p.ctr);
     DSG_CU(cudaEventRecord(p.sev[4], p.st));
-    k_zone_list<<<1, LIST_THREADS, 0, p.st>>>(p.nzone, p.zslot, p.zmslot, p.zfirst, p.zones, p.zmeta, p.chunks, p.ctr);
+    k_zone_list<<<1, LIST_THREADS, 0, p.st>>>(p.nzone, p.zslot, p.zmslot, p.zfirst, p.zones, p.zmeta, p.chunks, p.ctr, p.c.zcap, p.c.cellcap, p.c.chcap);
     DSG_CU(cudaGetLastError());
     proxy_components_device(p.noise, p.zones, zones::ZoneWork{p.chunks, p.ctr + C_CHUNKS}, 8 * 148, p.bits, p.par, p.rid, p.cs, p.khi, p.klo,
                             p.rec, p.ctr + C_PROXY, p.min_cells, p.st);
-    DSG_CU(cudaMemsetAsync(p.zcnt, 0, size_t(ZCAP + 1) * 4, p.st));
-    DSG_CU(cudaMemsetAsync(p.zfill, 0, size_t(ZCAP + 1) * 4, p.st));
+    DSG_CU(cudaMemsetAsync(p.zcnt, 0, size_t(p.c.zcap + 1) * 4, p.st));
+    DSG_CU(cudaMemsetAsync(p.zfill, 0, size_t(p.c.zcap + 1) * 4, p.st));
     k_comp_count<<<64, 256, 0, p.st>>>(p.rec, p.ctr, p.zcnt);
     k_comp_offsets<<<1, LIST_THREADS, 0, p.st>>>(p.zcnt, p.zoff, p.ctr);
     k_comp_scatter<<<64, 256, 0, p.st>>>(p.rec, p.ctr, p.zoff, p.zfill, p.zcomp);
@@ -810,6 +825,7 @@ extern "C" int dsg_search_open(const dsg_search_params *q) {
         DSG_ARG(q, "dsg_search_open: null pointer");
         DSG_ARG(q->max_sites > 0 && uint32_t(q->max_sites) <= MS, "dsg_search_open: max_sites must be 1..300");
         DSG_ARG(q->exact_n >= 0 && q->exact_n <= EXN, "dsg_search_open: exact_n must be 0..2");
+        DSG_ARG(q->seeds_cap <= SC_MAX, "dsg_search_open: seeds_cap above 1024");
         DSG_ARG(q->nms > 0 && q->hot_min > 0 && q->hot_pre > 0, "dsg_search_open: needs nms > 0, hot_min > 0 and hot_pre > 0");
         Pipeline &p = PL();
         std::lock_guard<std::mutex> l(p.mu);
@@ -839,6 +855,8 @@ extern "C" int dsg_search_open(const dsg_search_params *q) {
         gate::lane_caps(p.lane, p.gcaps);
         p.ctr = dalloc<uint32_t>(C_N);
         DSG_CU(cudaMemset(p.ctr, 0, C_N * 4));
+        p.c = Caps(q->seeds_cap ? q->seeds_cap : SC_MAX);
+        const uint32_t SC = p.c.sc;
         p.seeds = dalloc<uint64_t>(SC); p.noise = dalloc<SeedNoise>(SC);
         p.tabin = dalloc<char>(size_t(SC) * 6 * tabin_bytes());
         p.tab = dalloc<float>(size_t(SC) * 6 * 512 * 512); p.mx = dalloc<float>(2 * SC);
@@ -847,8 +865,8 @@ extern "C" int dsg_search_open(const dsg_search_params *q) {
         p.sites = dalloc<Site>(size_t(SC) * MS); p.nsites = dalloc<uint32_t>(SC); p.nbuck = dalloc<uint32_t>(SC); p.hot = dalloc<Hot>(size_t(SC) * MS);
         p.f1 = dalloc<int32_t>(size_t(SC) * MS); p.f2 = dalloc<int32_t>(size_t(SC) * MS);
         p.meta1 = dalloc<uint32_t>(size_t(SC) * MS); p.meta2 = dalloc<uint32_t>(size_t(SC) * MS);
-        p.f8 = dalloc<int32_t>(TRIES); p.f4 = dalloc<int32_t>(SC * EXN);
-        const uint32_t caps[4] = {SC * MS, SC * MS, TRIES, SC * EXN};
+        p.f8 = dalloc<int32_t>(p.c.tries); p.f4 = dalloc<int32_t>(SC * EXN);
+        const uint32_t caps[4] = {SC * MS, SC * MS, p.c.tries, SC * EXN};
         const int steps[4] = {256, 128, 8, 4};
         for (int k = 0; k < 4; k++) {
             const int half = (k < 2 ? 32000 : 16000) / steps[k], tpr = (2 * half + 1 + TILE - 1) / TILE;
@@ -857,19 +875,19 @@ extern "C" int dsg_search_open(const dsg_search_params *q) {
             p.ph[k].ctl = dalloc<FloodCtl>(caps[k]); p.ph[k].st = dalloc<FloodStat>(caps[k]);
             p.ph[k].dir = dalloc<int32_t>(size_t(caps[k]) * p.ph[k].per_req);
         }
-        p.pool.allocate(POOL_TILES);
+        p.pool.allocate(p.c.pool_tiles);
         p.evals = dalloc<unsigned long long>(1);
         round_grids(p.grid_eval, p.grid_conn);
         p.cov = dalloc<uint32_t>(size_t(SC) * MS); p.nzone = dalloc<uint32_t>(SC); p.zfirst = dalloc<uint32_t>(SC + 1);
         p.zslot = dalloc<DZone>(size_t(SC) * ZPS); p.zmslot = dalloc<ZoneMeta>(size_t(SC) * ZPS);
-        p.zones = dalloc<DZone>(ZCAP); p.zmeta = dalloc<ZoneMeta>(ZCAP); p.chunks = dalloc<uint2>(CHCAP);
-        p.bits = dalloc<uint8_t>(CELLCAP); p.par = dalloc<int32_t>(CELLCAP); p.rid = dalloc<int32_t>(CELLCAP);
-        p.cs = dalloc<zones::CompStat>(CELLCAP); p.khi = dalloc<uint64_t>(CELLCAP); p.klo = dalloc<uint32_t>(CELLCAP);
-        p.rec = dalloc<dsg_component>(CELLCAP);
-        p.zcnt = dalloc<uint32_t>(ZCAP + 1); p.zoff = dalloc<uint32_t>(ZCAP + 1); p.zfill = dalloc<uint32_t>(ZCAP + 1);
-        p.zcomp = dalloc<uint32_t>(CELLCAP);
+        p.zones = dalloc<DZone>(p.c.zcap); p.zmeta = dalloc<ZoneMeta>(p.c.zcap); p.chunks = dalloc<uint2>(p.c.chcap);
+        p.bits = dalloc<uint8_t>(p.c.cellcap); p.par = dalloc<int32_t>(p.c.cellcap); p.rid = dalloc<int32_t>(p.c.cellcap);
+        p.cs = dalloc<zones::CompStat>(p.c.cellcap); p.khi = dalloc<uint64_t>(p.c.cellcap); p.klo = dalloc<uint32_t>(p.c.cellcap);
+        p.rec = dalloc<dsg_component>(p.c.cellcap);
+        p.zcnt = dalloc<uint32_t>(p.c.zcap + 1); p.zoff = dalloc<uint32_t>(p.c.zcap + 1); p.zfill = dalloc<uint32_t>(p.c.zcap + 1);
+        p.zcomp = dalloc<uint32_t>(p.c.cellcap);
         p.evu = dalloc<Eval>(size_t(SC) * EVC); p.ev = dalloc<Eval>(size_t(SC) * EVC); p.nev = dalloc<uint32_t>(SC); p.sig = dalloc<int64_t>(size_t(SC) * EVC);
-        p.tries = dalloc<Try>(TRIES);
+        p.tries = dalloc<Try>(p.c.tries);
         p.out = dalloc<dsg_search_seed>(SC); p.rows = dalloc<dsg_search_row>(ROWCAP);
         DSG_CU(cudaMallocHost(&p.h_ctr, C_N * 4)); DSG_CU(cudaMallocHost(&p.h_gcnt, 16));
         DSG_CU(cudaMallocHost(&p.h_out, SC * sizeof(dsg_search_seed))); DSG_CU(cudaMallocHost(&p.h_rows, ROWCAP * sizeof(dsg_search_row)));
@@ -900,7 +918,7 @@ void finish_wave(Pipeline &p, Out &o, uint64_t indices, bool gated_by_lane) {
     DSG_CU(cudaGraphLaunch(p.exec, p.st));
     DSG_CU(cudaMemcpyAsync(p.h_ctr, p.ctr, C_N * 4, cudaMemcpyDeviceToHost, p.st));
     DSG_CU(cudaMemcpyAsync(p.h_gcnt, gate::lane_counts(p.lane), 16, cudaMemcpyDeviceToHost, p.st));
-    DSG_CU(cudaMemcpyAsync(p.h_out, p.out, SC * sizeof(dsg_search_seed), cudaMemcpyDeviceToHost, p.st));
+    DSG_CU(cudaMemcpyAsync(p.h_out, p.out, p.c.sc * sizeof(dsg_search_seed), cudaMemcpyDeviceToHost, p.st));
     DSG_CU(cudaStreamSynchronize(p.st));
     const uint32_t wrows = std::min(p.h_ctr[C_ROWS], ROWCAP);
     if (wrows) DSG_CU(cudaMemcpyAsync(p.h_rows, p.rows, size_t(wrows) * sizeof(dsg_search_row), cudaMemcpyDeviceToHost, p.st));
@@ -989,8 +1007,8 @@ extern "C" int dsg_search_seeds(const uint64_t *seeds, uint32_t n, dsg_search_se
         require_init();
         Out o{seeds_out, seed_cap, 0, rows_out, row_cap, 0, unfinished, unfinished_cap, 0};
         uint64_t *surv = const_cast<uint64_t *>(gate::lane_survivors(p.lane));
-        for (uint32_t base = 0; base < n; base += SC) {
-            const uint32_t nb = std::min<uint32_t>(SC, n - base);
+        for (uint32_t base = 0; base < n; base += p.c.sc) {
+            const uint32_t nb = std::min<uint32_t>(p.c.sc, n - base);
             DSG_CU(cudaEventRecord(p.ev0, p.st));
             // the seeds take the place of the gate's survivors: counts {0, 0, nb}
             std::memcpy(p.h_seeds, seeds + base, size_t(nb) * 8);

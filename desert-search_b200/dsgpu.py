@@ -313,7 +313,7 @@ class SearchParams(C.Structure):
                 ("ta", C.c_float), ("t", C.c_float), ("wc", C.c_float), ("we", C.c_float),
                 ("max_sites", C.c_int32), ("nms", C.c_int32), ("exact_n", C.c_int32),
                 ("hot_min", C.c_double), ("hot_pre", C.c_double), ("exact_min", C.c_double), ("refine_mb", C.c_double),
-                ("csv_min", C.c_double), ("wave", C.c_uint64)]
+                ("csv_min", C.c_double), ("wave", C.c_uint64), ("seeds_cap", C.c_uint32), ("reserved", C.c_uint32)]
 
 
 SEARCH_SEED = np.dtype([("seed", "<u8"), ("fya", "<f8"), ("fyb", "<f8"), ("maxta", "<f4"), ("maxtb", "<f4"), ("candidates", "<u4"),
@@ -323,7 +323,8 @@ SEARCH_ROW = np.dtype([("seed", "<u8"), ("rank", "<u4"), ("x", "<i4"), ("z", "<i
                       align=True)
 # the searcher's Params defaults (dsearch_desert.cpp:50-78) for the production command line gate=1 gpu=1 gscan=1
 SEARCH_DEFAULTS = dict(gate_phase=0.06, gate_pthr=0.645, gate_amp=0.70, ta=0.25, t=0.55, wc=0.25, we=0.41, max_sites=300, nms=5000,
-                       exact_n=2, hot_min=180.0, hot_pre=0.8, exact_min=75.0, refine_mb=70.0, csv_min=50.0, wave=0)
+                       exact_n=2, hot_min=180.0, hot_pre=0.8, exact_min=75.0, refine_mb=70.0, csv_min=50.0, wave=0,
+                       seeds_cap=0)
 
 
 def search_open(**kw):

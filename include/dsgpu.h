@@ -280,6 +280,9 @@ typedef struct dsg_search_params {
     double hot_min, hot_pre;                   /* big hot-zone area (M blocks^2, > 0) and pre-flood fraction (> 0) */
     double exact_min, refine_mb, csv_min;      /* proxy area for exact floods, step-8 area for step 4, CSV row cut */
     uint64_t wave;                             /* seed indices per wave (0 = 2^22, at most 2^26) */
+    uint32_t seeds_cap;                        /* gated seeds per wave (0 = 1,024, the most); the wave's zone, cell and
+                                                  flood-tile capacities scale with it (about 20 GB of device memory at 1,024) */
+    uint32_t reserved;
 } dsg_search_params;
 /* One gated seed: its PREFIX.seeds.csv line (dsearch_desert.cpp:548), rows[row0 .. row0 + nrows) its CSV rows. */
 typedef struct dsg_search_seed {
@@ -299,7 +302,8 @@ typedef struct dsg_search_row {
     double proxy, s8, s4, hot;
     int32_t edge, exact;
 } dsg_search_row;
-/* Allocate the pipeline (about 20 GB of device memory) and capture its graph; needs dsg_init and dsg_scan_init. */
+/* Allocate the pipeline (about 20 GB of device memory at the default capacity) and capture its graph; needs
+ * dsg_init and dsg_scan_init. */
 int dsg_search_open(const dsg_search_params *p);
 /* Search seeds mix(start + k), k < count, wave by wave.  Gated seeds' records go to seeds_out (their rows to
  * rows_out, row0 re-based), in no particular order.  A wave that exceeds a fixed capacity of the pipeline
