@@ -19,8 +19,8 @@ sources) on the same seed stream with all host cores and every stage at its defa
 GPU gate (phase=0.06); the reference's CPU build has no anti-aliased pre-gate, so its gate is its own CPU gate
 (sub-grid estimate >= 0.69, period-table amplitude >= 0.70).
 
-The line carries "stages_ms" (device ms of each stage over the timed steps, from events captured in the wave
-graph).  Besides it, the default run adds (single GPU): "pipeline" (the same search through the drop-in searcher binary:
+The line carries "stages_ms" (device ms of each stage over the timed steps, from global-timer stamps at the
+stage boundaries of the wave graph).  Besides it, the default run adds (single GPU): "pipeline" (the same search through the drop-in searcher binary:
 device pipeline, per-stage path on one host worker (the plain form: one batched call per stage with host syncs
 between stages), per-stage path on 8 workers, and the reference's own GPU searcher; wall clock; outputs
 compared), "default_mode" (the reference's default command line, ours vs its CPU searcher), "gate" (the seed

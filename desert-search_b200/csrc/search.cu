@@ -651,6 +651,12 @@ __global__ void k_pool_zero(Tiles T, uint32_t *ctr, uint32_t cap) {
     for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) { T.emask[i] = 0; T.qmask[i] = 0; T.mark[i] = 0; }
 }
 __global__ void k_wave_end(uint32_t *ctr) { ctr[C_TAKEN] = 0; ctr[C_BASE] = 0; }
+// Stage boundary k of the wave: the device's global timer (ns).  One thread; its cost is a launch.
+__global__ void k_stamp(unsigned long long *ts, int k) {
+    unsigned long long t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    ts[k] = t;
+}
 
 // ---------------------------------------------------------------- host side
 template <class T> T *dalloc(size_t n) {
@@ -709,8 +715,8 @@ struct Pipeline {
     uint32_t graph_kernels = 0;                  // kernel nodes of the wave graph outside the loop bodies
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
     static constexpr int NSTAGE = 8;             // gate | tables+scan | suppression+hot points | pre-floods | step-128 floods+coverage |
-    cudaEvent_t sev[NSTAGE] = {};                // proxy+components+exact starts | step-8 floods | step-4 floods+results
-    double stage_ms[NSTAGE] = {};
+    double stage_ms[NSTAGE] = {};                // proxy+components+exact starts | step-8 floods | step-4 floods+results
+    unsigned long long *d_ts = nullptr, *h_ts = nullptr;   // stage boundary stamps of the last wave (device global timer, ns)
     // pinned host copies
     uint32_t *h_ctr = nullptr, *h_gcnt = nullptr; dsg_search_seed *h_out = nullptr; dsg_search_row *h_rows = nullptr; uint64_t *h_seeds = nullptr;
 };
@@ -761,25 +767,25 @@ void capture_wave(Pipeline &p) {
     DSG_CU(cudaStreamBeginCapture(p.st, cudaStreamCaptureModeRelaxed));
     uint32_t caps[3];
     gate::lane_caps(p.lane, caps);
-    DSG_CU(cudaEventRecord(p.sev[0], p.st));
+    k_stamp<<<1, 1, 0, p.st>>>(p.d_ts, 1);
     const uint32_t SC = p.c.sc;
     k_begin<<<8, 128, 0, p.st>>>(gate::lane_counts(p.lane), caps[0], caps[1], caps[2], SC, gate::lane_survivors(p.lane), p.seeds, p.ctr);
     seed_noise_build_dev(p.seeds, p.ctr + C_NS, SC, p.noise, p.st);
     const int table_launches = scan_seeds_device(p.noise, p.ctr + C_NS, SC, p.tabin, p.tab, p.mx, p.act, p.nact, p.raw, p.nraw, RAWCAP, p.P.sp, p.st);
-    DSG_CU(cudaEventRecord(p.sev[1], p.st));
+    k_stamp<<<1, 1, 0, p.st>>>(p.d_ts, 2);
     DSG_CU(cudaFuncSetAttribute(k_nms, cudaFuncAttributeMaxDynamicSharedMemorySize, int(NMS_SMEM)));
     k_nms<<<SC, NMS_THREADS, NMS_SMEM, p.st>>>(p.raw, p.nraw, p.P, p.sites, p.nsites, p.nbuck, p.ctr);
     k_hot<<<4 * 148, 256, 0, p.st>>>(p.noise, p.sites, p.nsites, p.ctr, p.hot);
     k_req_pre<<<4 * 148, 256, 0, p.st>>>(p.hot, p.nsites, p.ctr, p.ph[0].ctl, p.meta1, p.f1, p.f2);
     DSG_CU(cudaGetLastError());
-    DSG_CU(cudaEventRecord(p.sev[2], p.st));
+    k_stamp<<<1, 1, 0, p.st>>>(p.d_ts, 3);
     capture_phase(p, 0);
-    DSG_CU(cudaEventRecord(p.sev[3], p.st));
+    k_stamp<<<1, 1, 0, p.st>>>(p.d_ts, 4);
     k_req_128<<<4 * 148, 256, 0, p.st>>>(p.ph[0].st, p.ph[0].ctl, p.meta1, p.P, p.ctr, p.ph[1].ctl, p.meta2, p.f2);
     capture_phase(p, 1);
     k_cover<<<(SC + 63) / 64, 64, 0, p.st>>>(p.hot, p.nsites, p.f1, p.f2, FloodView{p.ph[0].ctl, p.ph[0].dir}, FloodView{p.ph[1].ctl, p.ph[1].dir},
                                                p.ph[0].st, p.ph[1].st, p.pool.T, p.P, p.cov, p.nzone, p.zslot, p.zmslot, p.ctr);
-    DSG_CU(cudaEventRecord(p.sev[4], p.st));
+    k_stamp<<<1, 1, 0, p.st>>>(p.d_ts, 5);
     k_zone_list<<<1, LIST_THREADS, 0, p.st>>>(p.nzone, p.zslot, p.zmslot, p.zfirst, p.zones, p.zmeta, p.chunks, p.ctr, p.c.zcap, p.c.cellcap, p.c.chcap);
     DSG_CU(cudaGetLastError());
     proxy_components_device(p.noise, p.zones, zones::ZoneWork{p.chunks, p.ctr + C_CHUNKS}, 8 * 148, p.bits, p.par, p.rid, p.cs, p.khi, p.klo,
@@ -794,9 +800,9 @@ void capture_wave(Pipeline &p) {
     k_ring<<<8 * 148, 128, 0, p.st>>>(p.noise, world_dev(), p.tries, p.ctr);
     k_req_8<<<32, 256, 0, p.st>>>(p.tries, p.ctr, p.ph[2].ctl, p.f8);
     DSG_CU(cudaGetLastError());
-    DSG_CU(cudaEventRecord(p.sev[5], p.st));
+    k_stamp<<<1, 1, 0, p.st>>>(p.d_ts, 6);
     capture_phase(p, 2);
-    DSG_CU(cudaEventRecord(p.sev[6], p.st));
+    k_stamp<<<1, 1, 0, p.st>>>(p.d_ts, 7);
     k_retry<<<16, 256, 0, p.st>>>(p.tries, p.f8, p.ph[2].st, p.ph[2].ctl, p.ev, p.nev, p.P, p.ctr, p.ph[3].ctl, p.f4);
     capture_phase(p, 3);
     k_results<<<(SC + 127) / 128, 128, 0, p.st>>>(p.seeds, p.noise, p.mx, p.nbuck, p.nsites, p.sites, p.ev, p.nev, p.f4, p.ph[3].st, p.P, p.out,
@@ -804,13 +810,13 @@ void capture_wave(Pipeline &p) {
     k_pool_zero<<<8 * 148, 256, 0, p.st>>>(p.pool.T, p.ctr, p.pool.cap);
     k_wave_end<<<1, 1, 0, p.st>>>(p.ctr);
     DSG_CU(cudaGetLastError());
-    DSG_CU(cudaEventRecord(p.sev[7], p.st));
+    k_stamp<<<1, 1, 0, p.st>>>(p.d_ts, 8);
     cudaGraph_t g = nullptr;
     DSG_CU(cudaStreamEndCapture(p.st, &g));
     // kernel nodes outside the loop bodies: 6 set-up/scan kernels and the table launches, 6 for suppression, hot
     // points, requests, coverage and zones, 9 for the proxy bitmaps and labelling, 10 for components, exact starts,
     // retries, results and the wave's end, and 5 per flood phase
-    p.graph_kernels = 6 + table_launches + 6 + 9 + 10 + 4 * 5;
+    p.graph_kernels = 6 + table_launches + 6 + 9 + 10 + 4 * 5 + 8;      // + 8 stage stamps
     DSG_CU(cudaGraphInstantiate(&p.exec, g, 0));
     DSG_CU(cudaGraphDestroy(g));
 }
@@ -893,7 +899,8 @@ extern "C" int dsg_search_open(const dsg_search_params *q) {
         DSG_CU(cudaMallocHost(&p.h_out, SC * sizeof(dsg_search_seed))); DSG_CU(cudaMallocHost(&p.h_rows, ROWCAP * sizeof(dsg_search_row)));
         DSG_CU(cudaMallocHost(&p.h_seeds, SC * 8));
         DSG_CU(cudaEventCreate(&p.ev0)); DSG_CU(cudaEventCreate(&p.ev1));
-        for (cudaEvent_t &e : p.sev) DSG_CU(cudaEventCreate(&e));
+        p.d_ts = dalloc<unsigned long long>(16);
+        DSG_CU(cudaMallocHost(&p.h_ts, 16 * 8));
         DSG_CU(cudaDeviceSynchronize());
         capture_wave(p);
         p.open = true;
@@ -916,6 +923,7 @@ struct Out {
 // records; a flagged wave hands its gated seeds back instead.
 void finish_wave(Pipeline &p, Out &o, uint64_t indices, bool gated_by_lane) {
     DSG_CU(cudaGraphLaunch(p.exec, p.st));
+    DSG_CU(cudaMemcpyAsync(p.h_ts, p.d_ts, 16 * 8, cudaMemcpyDeviceToHost, p.st));
     DSG_CU(cudaMemcpyAsync(p.h_ctr, p.ctr, C_N * 4, cudaMemcpyDeviceToHost, p.st));
     DSG_CU(cudaMemcpyAsync(p.h_gcnt, gate::lane_counts(p.lane), 16, cudaMemcpyDeviceToHost, p.st));
     DSG_CU(cudaMemcpyAsync(p.h_out, p.out, p.c.sc * sizeof(dsg_search_seed), cudaMemcpyDeviceToHost, p.st));
@@ -927,17 +935,11 @@ void finish_wave(Pipeline &p, Out &o, uint64_t indices, bool gated_by_lane) {
     float ms = 0;
     DSG_CU(cudaEventElapsedTime(&ms, p.ev0, p.ev1));
     o.ms += ms;
-    float st = 0;
-    DSG_CU(cudaEventElapsedTime(&st, p.ev0, p.sev[0]));
-    p.stage_ms[0] += st;
-    for (int k = 1; k < Pipeline::NSTAGE; k++) {
-        DSG_CU(cudaEventElapsedTime(&st, p.sev[k - 1], p.sev[k]));
-        p.stage_ms[k] += st;
-    }
+    for (int k = 0; k < Pipeline::NSTAGE; k++) p.stage_ms[k] += double(p.h_ts[k + 1] - p.h_ts[k]) * 1e-6;
     const uint32_t wS = p.h_ctr[C_NS];
     o.tot[0] += indices; o.tot[1] += p.h_gcnt[0]; o.tot[2] += p.h_gcnt[1]; o.tot[3] += p.h_gcnt[2];
     o.tot[8] += p.h_ctr[C_ITERS];
-    o.tot[9] += uint64_t(p.graph_kernels) + uint64_t(BODY_KERNELS) * p.h_ctr[C_ITERS] + (gated_by_lane ? 4 : 0);
+    o.tot[9] += uint64_t(p.graph_kernels) + uint64_t(BODY_KERNELS) * p.h_ctr[C_ITERS] + (gated_by_lane ? 4 : 0) + 1;   // + the first stamp
     if (p.h_ctr[C_FLAGS]) {
         o.tot[7] |= p.h_ctr[C_FLAGS];
         if (p.h_ctr[C_FLAGS] & F_GATE) { set_error("device search: gate survivors exceed the wave's capacity"); throw ArgFail{}; }
@@ -988,6 +990,7 @@ extern "C" int dsg_search_run(uint64_t start, uint64_t count, dsg_search_seed *s
         for (uint64_t base = 0; base < count; base += p.wave) {
             const uint64_t nb = std::min(p.wave, count - base);
             DSG_CU(cudaEventRecord(p.ev0, p.st));
+            k_stamp<<<1, 1, 0, p.st>>>(p.d_ts, 0);
             gate::lane_enqueue(p.lane, p.st, start + base, nb, p.gcfg);
             finish_wave(p, o, nb, true);
         }
@@ -1010,6 +1013,7 @@ extern "C" int dsg_search_seeds(const uint64_t *seeds, uint32_t n, dsg_search_se
         for (uint32_t base = 0; base < n; base += p.c.sc) {
             const uint32_t nb = std::min<uint32_t>(p.c.sc, n - base);
             DSG_CU(cudaEventRecord(p.ev0, p.st));
+            k_stamp<<<1, 1, 0, p.st>>>(p.d_ts, 0);
             // the seeds take the place of the gate's survivors: counts {0, 0, nb}
             std::memcpy(p.h_seeds, seeds + base, size_t(nb) * 8);
             p.h_gcnt[0] = 0; p.h_gcnt[1] = 0; p.h_gcnt[2] = nb; p.h_gcnt[3] = 0;
@@ -1048,7 +1052,7 @@ extern "C" int dsg_search_close(void) {
         p.pool.release();
         cudaFreeHost(p.h_ctr); cudaFreeHost(p.h_gcnt); cudaFreeHost(p.h_out); cudaFreeHost(p.h_rows); cudaFreeHost(p.h_seeds);
         cudaEventDestroy(p.ev0); cudaEventDestroy(p.ev1);
-        for (cudaEvent_t &e : p.sev) cudaEventDestroy(e);
+        cudaFree(p.d_ts); cudaFreeHost(p.h_ts);
         cudaStreamDestroy(p.st); cudaStreamDestroy(p.body_st);
         p.open = false;
         return DSG_OK;

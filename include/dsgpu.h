@@ -320,8 +320,8 @@ int dsg_search_run(uint64_t start, uint64_t count, dsg_search_seed *seeds_out, u
 int dsg_search_seeds(const uint64_t *seeds, uint32_t n, dsg_search_seed *seeds_out, uint32_t seed_cap, uint32_t *n_seeds,
                      dsg_search_row *rows_out, uint32_t row_cap, uint32_t *n_rows, uint64_t *unfinished, uint32_t unfinished_cap,
                      uint32_t *n_unfinished, uint64_t counts[10], float *device_ms);
-/* Device ms per stage summed over the waves run since dsg_search_open (or the last reset), from events captured
- * in the wave graph: {gate, tables + scan, suppression + hot points, hot pre-floods, step-128 floods + coverage
+/* Device ms per stage summed over the waves run since dsg_search_open (or the last reset), from the device's
+ * global timer stamped by one-thread kernels at the stage boundaries of the wave graph: {gate, tables + scan, suppression + hot points, hot pre-floods, step-128 floods + coverage
  * replay, proxy components + exact-start search, step-8 floods, step-4 floods + results}.  No reference
  * counterpart (the reference prints core-seconds per stage on its progress line, dsearch_desert.cpp:552). */
 int dsg_search_stage_ms(double ms[8], int reset);
