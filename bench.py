@@ -508,8 +508,10 @@ def run_ours(args):
             dsgpu.search_close()
         return
     dsgpu.scan_init_default()
-    if args.small:                                   # a few GB on the device: for ncu captures of single launches
-        dsgpu.search_open(seeds_cap=128, wave=1 << 20)
+    if args.small:                                   # a few GB on the device, stages launched on a stream: for ncu captures
+        dsgpu.search_open(seeds_cap=128, wave=1 << 20, flags=dsgpu.SEARCH_EAGER)
+    elif args.eager:
+        dsgpu.search_open(flags=dsgpu.SEARCH_EAGER)
     else:
         dsgpu.search_open()
     rep.barrier()
@@ -607,8 +609,10 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--per-step-log2", type=int, default=24, help="seed indices per step = 2^N")
     ap.add_argument("--profile-run", action="store_true", help="device steps only (no e2e legs, no CPU baseline): for ncu captures")
-    ap.add_argument("--small", action="store_true", help="pipeline opened with 128 seeds and 2^20 indices per wave (a few GB): "
-                                                         "for ncu captures; use with --per-step-log2 20")
+    ap.add_argument("--small", action="store_true", help="pipeline opened with 128 seeds and 2^20 indices per wave (a few GB), stages "
+                                                         "launched on a stream: for ncu captures; use with --per-step-log2 20")
+    ap.add_argument("--eager", action="store_true", help="stages launched on a stream (no graph): for launch lists under ncu, which does "
+                                                         "not profile kernels of graphs with conditional nodes")
     ap.add_argument("--flood-only", action="store_true", help="only the flood measurements")
     ap.add_argument("--flood-small", type=int, default=4096)
     ap.add_argument("--flood-large", type=int, default=4096)

@@ -124,7 +124,7 @@ __global__ void __launch_bounds__(256) k_cc_merge(const DZone *__restrict__ zone
 }
 // Roots get a component id; every cell's parent becomes its root.
 __global__ void __launch_bounds__(256) k_cc_roots(const DZone *__restrict__ zones, int32_t *__restrict__ par, int32_t *__restrict__ rid,
-                                                  CompStat *__restrict__ cs, uint32_t *ctr, ZoneWork wk) {
+                                                  CompStat *__restrict__ cs, uint32_t *ctr, ZoneWork wk, uint32_t comp_cap) {
     each_chunk(zones, wk, [&](uint32_t zi, const DZone &z, int64_t c0, int64_t c1) {
         int32_t *p = par + z.off;
         for (int64_t c = c0 + threadIdx.x; c < c1; c += blockDim.x) {
@@ -132,6 +132,7 @@ __global__ void __launch_bounds__(256) k_cc_roots(const DZone *__restrict__ zone
             const int32_t r = uf_find(p, int32_t(c), ctr + 3);
             if (r == int32_t(c)) {
                 const uint32_t id = atomicAdd(ctr, 1u);
+                if (id >= comp_cap) { rid[z.off + c] = -1; atomicOr(ctr + 3, 2u); continue; }   // out of component records
                 rid[z.off + c] = int32_t(id);
                 CompStat &q = cs[id];
                 q.zone = zi; q.first = uint32_t(c); q.cells = 0; q.inner = 0; q.minx = q.minz = 0x7fffffff; q.kid = -1;
@@ -153,7 +154,7 @@ __global__ void __launch_bounds__(256) k_cc_stats(const DZone *__restrict__ zone
         const uint8_t *b = bits + z.off;
         for (int64_t c = c0 + threadIdx.x; c < c1; c += blockDim.x) {
             const int32_t r = par[z.off + c];
-            if (r < 0) continue;
+            if (r < 0 || rid[z.off + r] < 0) continue;
             CompStat &q = cs[rid[z.off + r]];
             const int x = int(c % z.nx), y = int(c / z.nx);
             atomicAdd(&q.cells, 1u);
@@ -165,8 +166,8 @@ __global__ void __launch_bounds__(256) k_cc_stats(const DZone *__restrict__ zone
     });
 }
 // Components of at least min_cells cells are kept; each gets a segment for its interior keys.
-__global__ void k_cc_keep(CompStat *__restrict__ cs, uint32_t min_cells, uint32_t *ctr) {
-    const uint32_t n = *ctr;
+__global__ void k_cc_keep(CompStat *__restrict__ cs, uint32_t min_cells, uint32_t *ctr, uint32_t comp_cap) {
+    const uint32_t n = min(*ctr, comp_cap);
     for (uint32_t id = blockIdx.x * blockDim.x + threadIdx.x; id < n; id += gridDim.x * blockDim.x) {
         CompStat &q = cs[id];
         if (q.cells < min_cells) continue;
@@ -183,7 +184,7 @@ __global__ void __launch_bounds__(256) k_cc_keys(const DZone *__restrict__ zones
         const uint8_t *b = bits + z.off;
         for (int64_t c = c0 + threadIdx.x; c < c1; c += blockDim.x) {
             const int32_t r = par[z.off + c];
-            if (r < 0) continue;
+            if (r < 0 || rid[z.off + r] < 0) continue;
             CompStat &q = cs[rid[z.off + r]];
             if (q.kid < 0) continue;
             const int x = int(c % z.nx), y = int(c / z.nx);
@@ -199,11 +200,11 @@ __global__ void __launch_bounds__(256) k_cc_keys(const DZone *__restrict__ zones
 // One block per kept component: the interior keys at ranks 0, n/3 and 2n/3, by an exact radix selection
 // over the 12 bytes of the key (all three ranks in each pass).
 __global__ void __launch_bounds__(256) k_cc_select(const CompStat *__restrict__ cs, const uint64_t *__restrict__ khi, const uint32_t *__restrict__ klo,
-                                                   const uint32_t *ctr, dsg_component *__restrict__ rec) {
+                                                   const uint32_t *ctr, dsg_component *__restrict__ rec, uint32_t comp_cap) {
     __shared__ uint32_t hist[3][256];
     __shared__ uint64_t pre_hi[3];
     __shared__ uint32_t pre_lo[3], want[3];
-    const uint32_t ncomp = ctr[0];
+    const uint32_t ncomp = min(ctr[0], comp_cap);
     for (uint32_t id = blockIdx.x; id < ncomp; id += gridDim.x) {
         const CompStat q = cs[id];
         if (q.kid < 0) continue;
@@ -256,17 +257,18 @@ __global__ void __launch_bounds__(256) k_cc_select(const CompStat *__restrict__ 
 // Component labelling of bitmaps already in `bits` (k_proxy's output): union-find, statistics, kept components
 // (at least min_cells cells), interior keys and the three interior starts of each kept component into rec[kid].
 // ctr = {components, kept, interior keys, error}, zeroed by the caller.
+// comp_cap: records in cs and rec; more components raise bit 1 of the error flag (their cells are left out).
 void label_components(const DZone *zones, dim3 grid, const ZoneWork &wk, const uint8_t *bits, int32_t *par, int32_t *rid, CompStat *cs,
                       uint64_t *khi, uint32_t *klo, dsg_component *rec, uint32_t *ctr, uint32_t min_cells, unsigned keep_blocks,
-                      unsigned select_blocks, cudaStream_t st) {
+                      unsigned select_blocks, uint32_t comp_cap, cudaStream_t st) {
     k_cc_init<<<grid, 256, 0, st>>>(zones, bits, par, wk);
     k_cc_merge<<<grid, 256, 0, st>>>(zones, bits, par, ctr + 3, wk);
-    k_cc_roots<<<grid, 256, 0, st>>>(zones, par, rid, cs, ctr, wk);
+    k_cc_roots<<<grid, 256, 0, st>>>(zones, par, rid, cs, ctr, wk, comp_cap);
     k_cc_flatten<<<grid, 256, 0, st>>>(zones, par, ctr + 3, wk);
     k_cc_stats<<<grid, 256, 0, st>>>(zones, bits, par, rid, cs, wk);
-    k_cc_keep<<<(keep_blocks + 255) / 256, 256, 0, st>>>(cs, min_cells, ctr);
+    k_cc_keep<<<(keep_blocks + 255) / 256, 256, 0, st>>>(cs, min_cells, ctr, comp_cap);
     k_cc_keys<<<grid, 256, 0, st>>>(zones, bits, par, rid, cs, khi, klo, wk);
-    k_cc_select<<<select_blocks, 256, 0, st>>>(cs, khi, klo, ctr, rec);
+    k_cc_select<<<select_blocks, 256, 0, st>>>(cs, khi, klo, ctr, rec, comp_cap);
 }
 
 struct State {
@@ -377,7 +379,7 @@ int proxy_components(const uint64_t *seeds, uint32_t nseeds, const uint32_t *zon
     const dim3 grid(nzones, unsigned((maxc + CHUNK - 1) / CHUNK));
     k_proxy<<<grid, 256, 0, st>>>(g.d_noise, g.d_zones, world_dev(), g_cut, g.d_out, ZoneWork{});
     label_components(g.d_zones, grid, ZoneWork{}, g.d_out, g.d_par, g.d_rid, g.d_cs, g.d_khi, g.d_klo, g.d_rec, g.d_ctr, min_cells,
-                     unsigned(std::min<int64_t>(off, 1 << 20)), unsigned(std::min<int64_t>(off, 4 * 148)), st);
+                     unsigned(std::min<int64_t>(off, 1 << 20)), unsigned(std::min<int64_t>(off, 4 * 148)), uint32_t(std::min<int64_t>(off, 0x7fffffff)), st);
     DSG_CU(cudaGetLastError());
     if (bits) DSG_CU(cudaMemcpyAsync(bits, g.d_out, size_t(off), cudaMemcpyDeviceToHost, st));
     DSG_CU(cudaMemcpyAsync(g.h_ctr, g.d_ctr, 4 * 4, cudaMemcpyDeviceToHost, st));
@@ -399,10 +401,10 @@ int proxy_components(const uint64_t *seeds, uint32_t nseeds, const uint32_t *zon
 // the caller (par, rid, cs, khi, klo, rec: one entry per cell).  Enqueued on st; ctr as label_components.
 void proxy_components_device(const SeedNoise *noise, const zones::DZone *zones, const ZoneWork &wk, uint32_t grid_blocks, uint8_t *bits,
                              int32_t *par, int32_t *rid, CompStat *cs, uint64_t *khi, uint32_t *klo, dsg_component *rec, uint32_t *ctr,
-                             uint32_t min_cells, cudaStream_t st) {
+                             uint32_t min_cells, uint32_t comp_cap, cudaStream_t st) {
     DSG_CU(cudaMemsetAsync(ctr, 0, 4 * 4, st));
     k_proxy<<<grid_blocks, 256, 0, st>>>(noise, zones, world_dev(), g_cut, bits, wk);
-    label_components(zones, dim3(grid_blocks), wk, bits, par, rid, cs, khi, klo, rec, ctr, min_cells, 1u << 20, 4 * 148, st);
+    label_components(zones, dim3(grid_blocks), wk, bits, par, rid, cs, khi, klo, rec, ctr, min_cells, 1u << 20, 4 * 148, comp_cap, st);
     DSG_CU(cudaGetLastError());
 }
 }  // namespace dsg

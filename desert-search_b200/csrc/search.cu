@@ -41,7 +41,7 @@ int scan_seeds_device(const SeedNoise *noise, const uint32_t *n_dev, uint32_t ca
 size_t tabin_bytes();
 void proxy_components_device(const SeedNoise *noise, const zones::DZone *zones, const zones::ZoneWork &wk, uint32_t grid_blocks, uint8_t *bits,
                              int32_t *par, int32_t *rid, zones::CompStat *cs, uint64_t *khi, uint32_t *klo, dsg_component *rec, uint32_t *ctr,
-                             uint32_t min_cells, cudaStream_t st);
+                             uint32_t min_cells, uint32_t comp_cap, cudaStream_t st);
 void seed_noise_build_dev(const uint64_t *d_seeds, const uint32_t *n_dev, uint32_t cap, SeedNoise *d_out, cudaStream_t st);
 
 namespace search {
@@ -55,9 +55,9 @@ constexpr uint32_t SC_MAX = 1024;            // gated seeds per wave (at most; d
 constexpr uint32_t RAWCAP = 1u << 16;        // raw scan candidates per seed (the reference's per-seed buffer, gproxy.cu:209)
 constexpr int HT = 4096;                     // bucket hash slots per seed (shared memory)
 constexpr uint32_t MS = 300;                 // sites per seed (Params.max_sites at most this)
-constexpr uint32_t ZPS = 64;                 // big hot zones per seed
+constexpr uint32_t ZPS = 256;                // big hot zones per seed
 // zones, proxy cells and flood tiles per wave are set for SC_MAX seeds and scale with seeds_cap (Pipeline::caps)
-constexpr uint32_t EVC = 128;                // proxy components kept per seed
+constexpr uint32_t EVC = 512;                // proxy components kept per seed
 constexpr int EXN = 2;                       // exact floods per seed (Params.exact_n at most this)
 constexpr uint32_t ROWCAP = 1u << 16;        // CSV rows per wave
 constexpr uint32_t LOOP_LIMIT = 2048;        // flood loop iterations (6 rounds each) before a wave gives up
@@ -69,7 +69,8 @@ enum : uint32_t { F_GATE = 1, F_RAW = 2, F_HASH = 4, F_ZONES = 8, F_CELLS = 16, 
 // device counters
 enum { C_NS = 0, C_NREQ = 1 /* 4 flood phases */, C_ZONES = 5, C_CHUNKS = 6, C_ROWS = 7, C_FLAGS = 8, C_NHOT = 9, C_NBIG = 10, C_SITES = 11,
        C_ROUND = 16 /* 9 round counters */, C_TAKEN = 25, C_FERR = 26, C_BASE = 27, C_LOOPS = 28, C_ITERS = 29, C_PROXY = 32 /* 4 */,
-       C_KEPT = 33, C_N = 48 };
+       C_KEPT = 33, C_MAXZ = 36 /* most big zones of a seed */, C_CELLS = 37 /* proxy cells (saturating) */, C_MAXEV = 38 /* most evaluations of a
+       seed */, C_N = 48 };
 constexpr int BODY_KERNELS = 13;             // kernels of one flood-loop iteration: 6 rounds of eval + connect, the loop control
 
 struct Params {
@@ -307,9 +308,10 @@ __global__ void k_dir_fill(int32_t *__restrict__ dir, const uint32_t *nreq, uint
     for (uint64_t i = uint64_t(blockIdx.x) * blockDim.x + threadIdx.x; i < n; i += uint64_t(gridDim.x) * blockDim.x) dir[i] = -1;
 }
 // Phase start: round counters cleared, the loop entered only if there are requests.
-__global__ void k_phase_begin(uint32_t *ctr, const uint32_t *nreq, cudaGraphConditionalHandle h) {
+// (in_graph = false: launched on a stream, where there is no handle to set; the host drives the loop)
+__global__ void k_phase_begin(uint32_t *ctr, const uint32_t *nreq, cudaGraphConditionalHandle h, bool in_graph) {
     for (int k = 0; k < 9; k++) ctr[C_ROUND + k] = 0;
-    cudaGraphSetConditional(h, *nreq > 0 ? 1u : 0u);
+    if (in_graph) cudaGraphSetConditional(h, *nreq > 0 ? 1u : 0u);
 }
 // Start of every request: statistics reset, start tile claimed, start sub-block queued for round *base.
 __global__ void k_req_start(const FloodCtl *__restrict__ ctl, const uint32_t *nreq, FloodStat *__restrict__ st, int32_t *__restrict__ dir, Tiles T,
@@ -326,13 +328,13 @@ __global__ void k_req_start(const FloodCtl *__restrict__ ctl, const uint32_t *nr
 }
 // End of a loop iteration (6 rounds): advance the round base; stop when the next round has no work, or at the
 // iteration limit (the wave is then flagged).
-__global__ void k_loop_ctl(uint32_t *ctr, cudaGraphConditionalHandle h) {
+__global__ void k_loop_ctl(uint32_t *ctr, cudaGraphConditionalHandle h, bool in_graph) {
     ctr[C_BASE] += 6;
     ctr[C_ITERS]++;
     const uint32_t it = ++ctr[C_LOOPS];
     const bool more = ctr[C_ROUND + 0] != 0 || ctr[C_ROUND + 3] != 0;
     if (more && it >= LOOP_LIMIT) ctr[C_FLAGS] |= F_LOOP;
-    cudaGraphSetConditional(h, more && it < LOOP_LIMIT ? 1u : 0u);
+    if (in_graph) cudaGraphSetConditional(h, more && it < LOOP_LIMIT ? 1u : 0u);
 }
 __global__ void k_phase_end(uint32_t *ctr) {
     ctr[C_LOOPS] = 0;
@@ -352,59 +354,78 @@ __device__ __forceinline__ bool reached(const FloodView &f, const Tiles &T, uint
 __device__ __forceinline__ int64_t ceil_div(int64_t a, int64_t b) { return a >= 0 ? (a + b - 1) / b : -((-a) / b); }
 // hotcovered.count(hotkey(hx, hz)) against the floods a seed has used: a step-128 flood covers the 128-quart
 // key block of each of its cells, a step-256 one the key blocks of its cells offset by 0 or 128 on each axis.
-__device__ bool covered(int hx, int hz, const uint32_t *cov, int ncov, const FloodView &f1, const FloodView &f2, const Tiles &T) {
-    const int64_t bx = int64_t((hx + 8000000) >> 7) * 128 - 8000000, bz = int64_t((hz + 8000000) >> 7) * 128 - 8000000;
-    for (int k = 0; k < ncov; k++) {
-        const bool pre = (cov[k] >> 31) == 0;
-        const uint32_t r = cov[k] & 0x7fffffffu;
-        const FloodView &f = pre ? f1 : f2;
-        const FloodCtl &c = f.ctl[r];
-        const int offs = pre ? 2 : 1;
-        for (int dz = 0; dz < offs; dz++)
-            for (int dx = 0; dx < offs; dx++) {
-                const int64_t lox = bx - dx * 128, loz = bz - dz * 128;
-                const int64_t ix = ceil_div(lox - c.qx, c.step), iz = ceil_div(loz - c.qz, c.step);
-                if (c.qx + ix * c.step > lox + 127 || c.qz + iz * c.step > loz + 127) continue;
-                if (reached(f, T, r, ix + c.half, iz + c.half)) return true;
-            }
-    }
+// One used flood: does it cover the key block of (hx, hz)?  A step-128 flood covers the 128-quart key block of each
+// of its cells, a step-256 one the key blocks of its cells offset by 0 or 128 on each axis (hotcovered.count, the
+// reference's set of keys, dsearch_desert.cpp:341-345,357-361): the key block holds at most one lattice point of
+// the flood per offset, and that point covers it when it is in the flood's reached set.
+__device__ __forceinline__ bool covers(uint32_t cv, int64_t bx, int64_t bz, const FloodView &f1, const FloodView &f2, const Tiles &T) {
+    const bool pre = (cv >> 31) == 0;
+    const uint32_t r = cv & 0x7fffffffu;
+    const FloodView &f = pre ? f1 : f2;
+    const FloodCtl &c = f.ctl[r];
+    const int offs = pre ? 2 : 1;
+    for (int dz = 0; dz < offs; dz++)
+        for (int dx = 0; dx < offs; dx++) {
+            const int64_t lox = bx - dx * 128, loz = bz - dz * 128;
+            const int64_t ix = ceil_div(lox - c.qx, c.step), iz = ceil_div(loz - c.qz, c.step);
+            if (c.qx + ix * c.step > lox + 127 || c.qz + iz * c.step > loz + 127) continue;
+            if (reached(f, T, r, ix + c.half, iz + c.half)) return true;
+        }
     return false;
 }
-// Thread per seed: the reference's walk over its sites in rank order, using only the floods of the sites it
-// does not skip; big zones (hot area >= hot_min) become proxy zones of 32-quart cells around the flood's bbox.
-__global__ void k_cover(const Hot *__restrict__ hot, const uint32_t *__restrict__ nsites, const int32_t *__restrict__ f1, const int32_t *__restrict__ f2,
-                        FloodView v1, FloodView v2, const FloodStat *__restrict__ st1, const FloodStat *__restrict__ st2, Tiles T, Params P,
-                        uint32_t *__restrict__ cov_buf, uint32_t *__restrict__ nzone, DZone *__restrict__ zslot, ZoneMeta *__restrict__ zmeta,
-                        uint32_t *ctr) {
-    const uint32_t s = blockIdx.x * blockDim.x + threadIdx.x;
+// Warp per seed: the reference's walk over its sites in rank order, using only the floods of the sites it does
+// not skip (the lanes test the floods used so far in parallel); big zones (hot area >= hot_min) become proxy zones
+// of 32-quart cells around the step-128 flood's bbox.
+__global__ void __launch_bounds__(256) k_cover(const Hot *__restrict__ hot, const uint32_t *__restrict__ nsites, const int32_t *__restrict__ f1,
+                                               const int32_t *__restrict__ f2, FloodView v1, FloodView v2, const FloodStat *__restrict__ st1,
+                                               const FloodStat *__restrict__ st2, Tiles T, Params P, uint32_t *__restrict__ cov_buf,
+                                               uint32_t *__restrict__ nzone, DZone *__restrict__ zslot, ZoneMeta *__restrict__ zmeta, uint32_t *ctr) {
+    const int lane = threadIdx.x & 31;
+    const uint32_t s = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
     if (s >= ctr[C_NS]) return;
     uint32_t *cov = cov_buf + size_t(s) * MS;
-    int ncov = 0;
-    uint32_t nz = 0, nhot = 0, nbig = 0;
-    for (uint32_t r = 0; r < nsites[s]; r++) {
+    uint32_t ncov = 0, nz = 0, nhot = 0, nbig = 0;
+    const uint32_t ns = nsites[s];
+    for (uint32_t r = 0; r < ns; r++) {
         const uint32_t w = s * MS + r;
         const Hot h = hot[w];
-        if (h.bt < 0.55 || covered(h.hx, h.hz, cov, ncov, v1, v2, T)) continue;
+        if (h.bt < 0.55) continue;
+        const int64_t bx = int64_t((h.hx + 8000000) >> 7) * 128 - 8000000, bz = int64_t((h.hz + 8000000) >> 7) * 128 - 8000000;
+        bool hit = false;
+        for (uint32_t k = lane; k < ncov; k += 32) hit |= covers(__ldcg(cov + k), bx, bz, v1, v2, T);
+        if (__any_sync(0xffffffffu, hit)) continue;
         const int32_t k1 = f1[w];
-        if (small_zone(st1[k1], P)) { cov[ncov++] = uint32_t(k1); nhot++; continue; }
-        const int32_t k2 = f2[w];
-        cov[ncov++] = 0x80000000u | uint32_t(k2);
         nhot++;
+        if (small_zone(st1[k1], P)) {
+            if (lane == 0) __stcg(cov + ncov, uint32_t(k1));
+            ncov++;
+            __syncwarp();
+            continue;
+        }
+        const int32_t k2 = f2[w];
+        if (lane == 0) __stcg(cov + ncov, 0x80000000u | uint32_t(k2));
+        ncov++;
+        __syncwarp();
         const FloodStat a = st2[k2];
         const double hot_area = double(a.cells) * 128.0 * 128 * 16 / 1e6;
         if (hot_area < P.hot_min) continue;
         nbig++;
-        if (nz == ZPS) { atomicOr(ctr + C_FLAGS, F_ZONES); continue; }
-        DZone z{};
-        z.x0 = int(floor((a.minx - 128) / 32.0)) * 32; z.z0 = int(floor((a.minz - 128) / 32.0)) * 32;
-        z.nx = (a.maxx + 128 - z.x0) / 32 + 1; z.nz = (a.maxz + 128 - z.z0) / 32 + 1;
-        z.seed = int32_t(s);
-        zslot[size_t(s) * ZPS + nz] = z;
-        zmeta[size_t(s) * ZPS + nz] = {s, r, hot_area};
+        if (nz == ZPS) { if (lane == 0) atomicOr(ctr + C_FLAGS, F_ZONES); continue; }
+        if (lane == 0) {
+            DZone z{};
+            z.x0 = int(floor((a.minx - 128) / 32.0)) * 32; z.z0 = int(floor((a.minz - 128) / 32.0)) * 32;
+            z.nx = (a.maxx + 128 - z.x0) / 32 + 1; z.nz = (a.maxz + 128 - z.z0) / 32 + 1;
+            z.seed = int32_t(s);
+            zslot[size_t(s) * ZPS + nz] = z;
+            zmeta[size_t(s) * ZPS + nz] = {s, r, hot_area};
+        }
         nz++;
     }
-    nzone[s] = nz;
-    atomicAdd(ctr + C_NHOT, nhot); atomicAdd(ctr + C_NBIG, nbig);
+    if (lane == 0) {
+        nzone[s] = nz;
+        atomicAdd(ctr + C_NHOT, nhot); atomicAdd(ctr + C_NBIG, nbig);
+        atomicMax(ctr + C_MAXZ, nbig);
+    }
 }
 // One block: the seeds' zones concatenated in seed order (zfirst[s] = first zone of seed s), their cell offsets
 // and the chunk list over them.  Flags the wave when the zones or cells exceed the capacities.
@@ -453,6 +474,7 @@ __global__ void __launch_bounds__(LIST_THREADS) k_zone_list(const uint32_t *__re
     }
     if (threadIdx.x == 0) {
         ctr[C_ZONES] = nz;
+        ctr[C_CELLS] = uint32_t(s_base[0] < 0xffffffffull ? s_base[0] : 0xffffffffull);
         if (s_base[0] > CELLCAP || s_base[1] > CHCAP) { ctr[C_FLAGS] |= F_CELLS; ctr[C_CHUNKS] = 0; }
         else ctr[C_CHUNKS] = uint32_t(s_base[1]);
     }
@@ -534,10 +556,11 @@ __global__ void k_evals(const uint32_t *__restrict__ zfirst, const DZone *__rest
         }
     }
     if (full) atomicOr(ctr + C_FLAGS, F_EVALS);
+    atomicMax(ctr + C_MAXEV, nseen + (full ? 1 : 0));
     // std::sort(ev, proxy descending): the permutation from the sort, the records copied out in its order
-    uint8_t idx[EVC];
-    for (uint32_t k = 0; k < ne; k++) idx[k] = uint8_t(k);
-    dsg::stl::sort(idx, int64_t(ne), [&](uint8_t a, uint8_t b) { return U[a].proxy > U[b].proxy; });
+    uint16_t idx[EVC];
+    for (uint32_t k = 0; k < ne; k++) idx[k] = uint16_t(k);
+    dsg::stl::sort(idx, int64_t(ne), [&](uint16_t a, uint16_t b) { return U[a].proxy > U[b].proxy; });
     for (uint32_t k = 0; k < ne; k++) E[k] = U[idx[k]];
     if (s == 0 && ctr[C_PROXY + 3]) atomicOr(ctr + C_FLAGS, F_LABEL);
     nev[s] = ne;
@@ -670,12 +693,14 @@ struct Phase { FloodCtl *ctl; FloodStat *st; int32_t *dir; uint32_t per_req; uin
 struct Caps {
     uint32_t sc, zcap, tries;
     uint64_t cellcap, chcap;
+    uint32_t compcap;
     uint32_t pool_tiles;
     explicit Caps(uint32_t seeds = SC_MAX) {
         sc = seeds;
         const double f = double(seeds) / SC_MAX;
-        zcap = std::max<uint32_t>(256, uint32_t(8192 * f));
-        cellcap = std::max<uint64_t>(1u << 20, uint64_t(double(1u << 25) * f));
+        zcap = std::max<uint32_t>(1024, uint32_t(32768 * f));
+        cellcap = std::max<uint64_t>(1u << 22, uint64_t(double(1u << 27) * f));
+        compcap = std::max<uint32_t>(1u << 16, uint32_t(double(1u << 22) * f));
         chcap = cellcap / CHUNK + zcap;
         tries = seeds * EXN * 3;
         pool_tiles = std::max<uint32_t>(1u << 16, uint32_t(double(3u << 20) * f));
@@ -712,6 +737,7 @@ struct Pipeline {
     dsg_search_seed *out = nullptr; dsg_search_row *rows = nullptr;
     int grid_eval = 0, grid_conn = 0;
     cudaGraphExec_t exec = nullptr;
+    bool eager = false;                          // no graph: every wave launches the stages on the stream (for profilers)
     uint32_t graph_kernels = 0;                  // kernel nodes of the wave graph outside the loop bodies
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
     static constexpr int NSTAGE = 8;             // gate | tables+scan | suppression+hot points | pre-floods | step-128 floods+coverage |
@@ -729,42 +755,59 @@ void capture_phase(Pipeline &p, int k) {
     uint32_t *nreq = p.ctr + C_NREQ + k;
     const TileAlloc ta{nullptr, 0, p.pool.cap, p.pool.cap, p.ctr + C_TAKEN, nullptr, nullptr};
     k_dir_fill<<<4 * 148, 256, 0, p.st>>>(f.dir, nreq, f.per_req);
-    cudaStreamCaptureStatus cs;
-    cudaGraph_t g;
-    const cudaGraphNode_t *deps = nullptr;
-    size_t ndeps = 0;
-    DSG_CU(cudaStreamGetCaptureInfo(p.st, &cs, nullptr, &g, &deps, &ndeps));
-    cudaGraphConditionalHandle h;
-    DSG_CU(cudaGraphConditionalHandleCreate(&h, g, 0, cudaGraphCondAssignDefault));
-    k_phase_begin<<<1, 1, 0, p.st>>>(p.ctr, nreq, h);
-    k_req_start<<<64, 128, 0, p.st>>>(f.ctl, nreq, f.st, f.dir, p.pool.T, ta, p.pool.n_list[0], p.ctr);
-    DSG_CU(cudaGetLastError());
-    DSG_CU(cudaStreamGetCaptureInfo(p.st, &cs, nullptr, &g, &deps, &ndeps));
-    cudaGraphNodeParams np{};
-    np.type = cudaGraphNodeTypeConditional;
-    np.conditional.handle = h;
-    np.conditional.type = cudaGraphCondTypeWhile;
-    np.conditional.size = 1;
-    cudaGraphNode_t node;
-    DSG_CU(cudaGraphAddNode(&node, g, deps, ndeps, &np));
-    cudaGraph_t body = np.conditional.phGraph_out[0];
-    DSG_CU(cudaStreamUpdateCaptureDependencies(p.st, &node, 1, cudaStreamSetCaptureDependencies));
-    DSG_CU(cudaStreamBeginCaptureToGraph(p.body_st, body, nullptr, nullptr, 0, cudaStreamCaptureModeRelaxed));
-    for (uint32_t r = 0; r < 6; r++)
-        launch_round(p.pool, r, p.ctr + C_ROUND, nullptr, p.ctr + C_FERR, p.evals, f.ctl, p.noise, f.dir, f.st, ta, p.grid_eval, p.grid_conn,
-                     p.body_st, p.ctr + C_BASE);
-    k_loop_ctl<<<1, 1, 0, p.body_st>>>(p.ctr, h);
-    DSG_CU(cudaGetLastError());
-    cudaGraph_t body_out = nullptr;
-    DSG_CU(cudaStreamEndCapture(p.body_st, &body_out));
+    if (p.eager) {
+        // the same kernels launched on the stream, the loop driven by the host after every 6 rounds
+        k_phase_begin<<<1, 1, 0, p.st>>>(p.ctr, nreq, 0, false);
+        k_req_start<<<64, 128, 0, p.st>>>(f.ctl, nreq, f.st, f.dir, p.pool.T, ta, p.pool.n_list[0], p.ctr);
+        for (uint32_t it = 0; it < LOOP_LIMIT; it++) {
+            for (uint32_t r = 0; r < 6; r++)
+                launch_round(p.pool, r, p.ctr + C_ROUND, nullptr, p.ctr + C_FERR, p.evals, f.ctl, p.noise, f.dir, f.st, ta, p.grid_eval, p.grid_conn,
+                             p.st, p.ctr + C_BASE);
+            k_loop_ctl<<<1, 1, 0, p.st>>>(p.ctr, 0, false);
+            DSG_CU(cudaGetLastError());
+            DSG_CU(cudaMemcpyAsync(p.h_ctr, p.ctr, C_N * 4, cudaMemcpyDeviceToHost, p.st));
+            DSG_CU(cudaStreamSynchronize(p.st));
+            if (p.h_ctr[C_ROUND + 0] == 0 && p.h_ctr[C_ROUND + 3] == 0) break;
+        }
+    } else {
+        cudaStreamCaptureStatus cs;
+        cudaGraph_t g;
+        const cudaGraphNode_t *deps = nullptr;
+        size_t ndeps = 0;
+        DSG_CU(cudaStreamGetCaptureInfo(p.st, &cs, nullptr, &g, &deps, &ndeps));
+        cudaGraphConditionalHandle h;
+        DSG_CU(cudaGraphConditionalHandleCreate(&h, g, 0, cudaGraphCondAssignDefault));
+        k_phase_begin<<<1, 1, 0, p.st>>>(p.ctr, nreq, h, true);
+        k_req_start<<<64, 128, 0, p.st>>>(f.ctl, nreq, f.st, f.dir, p.pool.T, ta, p.pool.n_list[0], p.ctr);
+        DSG_CU(cudaGetLastError());
+        DSG_CU(cudaStreamGetCaptureInfo(p.st, &cs, nullptr, &g, &deps, &ndeps));
+        cudaGraphNodeParams np{};
+        np.type = cudaGraphNodeTypeConditional;
+        np.conditional.handle = h;
+        np.conditional.type = cudaGraphCondTypeWhile;
+        np.conditional.size = 1;
+        cudaGraphNode_t node;
+        DSG_CU(cudaGraphAddNode(&node, g, deps, ndeps, &np));
+        cudaGraph_t body = np.conditional.phGraph_out[0];
+        DSG_CU(cudaStreamUpdateCaptureDependencies(p.st, &node, 1, cudaStreamSetCaptureDependencies));
+        DSG_CU(cudaStreamBeginCaptureToGraph(p.body_st, body, nullptr, nullptr, 0, cudaStreamCaptureModeRelaxed));
+        for (uint32_t r = 0; r < 6; r++)
+            launch_round(p.pool, r, p.ctr + C_ROUND, nullptr, p.ctr + C_FERR, p.evals, f.ctl, p.noise, f.dir, f.st, ta, p.grid_eval, p.grid_conn,
+                         p.body_st, p.ctr + C_BASE);
+        k_loop_ctl<<<1, 1, 0, p.body_st>>>(p.ctr, h, true);
+        DSG_CU(cudaGetLastError());
+        cudaGraph_t body_out = nullptr;
+        DSG_CU(cudaStreamEndCapture(p.body_st, &body_out));
+    }
     k_tile_finish<<<dim3(f.cap, dir_chunks(f.per_req)), 256, 0, p.st>>>(f.ctl, nullptr, f.dir, p.pool.T, f.st, nreq);
     k_phase_end<<<1, 1, 0, p.st>>>(p.ctr);
     DSG_CU(cudaGetLastError());
 }
 
 // Everything of a wave after the gate, as one graph.
+// In eager mode (profiling) the same sequence is launched on the stream for every wave instead.
 void capture_wave(Pipeline &p) {
-    DSG_CU(cudaStreamBeginCapture(p.st, cudaStreamCaptureModeRelaxed));
+    if (!p.eager) DSG_CU(cudaStreamBeginCapture(p.st, cudaStreamCaptureModeRelaxed));
     uint32_t caps[3];
     gate::lane_caps(p.lane, caps);
     k_stamp<<<1, 1, 0, p.st>>>(p.d_ts, 1);
@@ -783,13 +826,13 @@ void capture_wave(Pipeline &p) {
     k_stamp<<<1, 1, 0, p.st>>>(p.d_ts, 4);
     k_req_128<<<4 * 148, 256, 0, p.st>>>(p.ph[0].st, p.ph[0].ctl, p.meta1, p.P, p.ctr, p.ph[1].ctl, p.meta2, p.f2);
     capture_phase(p, 1);
-    k_cover<<<(SC + 63) / 64, 64, 0, p.st>>>(p.hot, p.nsites, p.f1, p.f2, FloodView{p.ph[0].ctl, p.ph[0].dir}, FloodView{p.ph[1].ctl, p.ph[1].dir},
+    k_cover<<<(SC + 7) / 8, 256, 0, p.st>>>(p.hot, p.nsites, p.f1, p.f2, FloodView{p.ph[0].ctl, p.ph[0].dir}, FloodView{p.ph[1].ctl, p.ph[1].dir},
                                                p.ph[0].st, p.ph[1].st, p.pool.T, p.P, p.cov, p.nzone, p.zslot, p.zmslot, p.ctr);
     k_stamp<<<1, 1, 0, p.st>>>(p.d_ts, 5);
     k_zone_list<<<1, LIST_THREADS, 0, p.st>>>(p.nzone, p.zslot, p.zmslot, p.zfirst, p.zones, p.zmeta, p.chunks, p.ctr, p.c.zcap, p.c.cellcap, p.c.chcap);
     DSG_CU(cudaGetLastError());
     proxy_components_device(p.noise, p.zones, zones::ZoneWork{p.chunks, p.ctr + C_CHUNKS}, 8 * 148, p.bits, p.par, p.rid, p.cs, p.khi, p.klo,
-                            p.rec, p.ctr + C_PROXY, p.min_cells, p.st);
+                            p.rec, p.ctr + C_PROXY, p.min_cells, p.c.compcap, p.st);
     DSG_CU(cudaMemsetAsync(p.zcnt, 0, size_t(p.c.zcap + 1) * 4, p.st));
     DSG_CU(cudaMemsetAsync(p.zfill, 0, size_t(p.c.zcap + 1) * 4, p.st));
     k_comp_count<<<64, 256, 0, p.st>>>(p.rec, p.ctr, p.zcnt);
@@ -811,12 +854,13 @@ void capture_wave(Pipeline &p) {
     k_wave_end<<<1, 1, 0, p.st>>>(p.ctr);
     DSG_CU(cudaGetLastError());
     k_stamp<<<1, 1, 0, p.st>>>(p.d_ts, 8);
+    // kernels outside the loop bodies: 6 set-up/scan kernels and the table launches, 6 for suppression, hot points,
+    // requests, coverage and zones, 9 for the proxy bitmaps and labelling, 10 for components, exact starts, retries,
+    // results and the wave's end, 5 per flood phase, 8 stage stamps
+    p.graph_kernels = 6 + table_launches + 6 + 9 + 10 + 4 * 5 + 8;
+    if (p.eager) return;
     cudaGraph_t g = nullptr;
     DSG_CU(cudaStreamEndCapture(p.st, &g));
-    // kernel nodes outside the loop bodies: 6 set-up/scan kernels and the table launches, 6 for suppression, hot
-    // points, requests, coverage and zones, 9 for the proxy bitmaps and labelling, 10 for components, exact starts,
-    // retries, results and the wave's end, and 5 per flood phase
-    p.graph_kernels = 6 + table_launches + 6 + 9 + 10 + 4 * 5 + 8;      // + 8 stage stamps
     DSG_CU(cudaGraphInstantiate(&p.exec, g, 0));
     DSG_CU(cudaGraphDestroy(g));
 }
@@ -888,10 +932,10 @@ extern "C" int dsg_search_open(const dsg_search_params *q) {
         p.zslot = dalloc<DZone>(size_t(SC) * ZPS); p.zmslot = dalloc<ZoneMeta>(size_t(SC) * ZPS);
         p.zones = dalloc<DZone>(p.c.zcap); p.zmeta = dalloc<ZoneMeta>(p.c.zcap); p.chunks = dalloc<uint2>(p.c.chcap);
         p.bits = dalloc<uint8_t>(p.c.cellcap); p.par = dalloc<int32_t>(p.c.cellcap); p.rid = dalloc<int32_t>(p.c.cellcap);
-        p.cs = dalloc<zones::CompStat>(p.c.cellcap); p.khi = dalloc<uint64_t>(p.c.cellcap); p.klo = dalloc<uint32_t>(p.c.cellcap);
-        p.rec = dalloc<dsg_component>(p.c.cellcap);
+        p.cs = dalloc<zones::CompStat>(p.c.compcap); p.khi = dalloc<uint64_t>(p.c.cellcap); p.klo = dalloc<uint32_t>(p.c.cellcap);
+        p.rec = dalloc<dsg_component>(p.c.compcap);
         p.zcnt = dalloc<uint32_t>(p.c.zcap + 1); p.zoff = dalloc<uint32_t>(p.c.zcap + 1); p.zfill = dalloc<uint32_t>(p.c.zcap + 1);
-        p.zcomp = dalloc<uint32_t>(p.c.cellcap);
+        p.zcomp = dalloc<uint32_t>(p.c.compcap);
         p.evu = dalloc<Eval>(size_t(SC) * EVC); p.ev = dalloc<Eval>(size_t(SC) * EVC); p.nev = dalloc<uint32_t>(SC); p.sig = dalloc<int64_t>(size_t(SC) * EVC);
         p.tries = dalloc<Try>(p.c.tries);
         p.out = dalloc<dsg_search_seed>(SC); p.rows = dalloc<dsg_search_row>(ROWCAP);
@@ -902,7 +946,8 @@ extern "C" int dsg_search_open(const dsg_search_params *q) {
         p.d_ts = dalloc<unsigned long long>(16);
         DSG_CU(cudaMallocHost(&p.h_ts, 16 * 8));
         DSG_CU(cudaDeviceSynchronize());
-        capture_wave(p);
+        p.eager = (q->flags & DSG_SEARCH_EAGER) != 0;
+        if (!p.eager) capture_wave(p);
         p.open = true;
         return DSG_OK;
     });
@@ -922,7 +967,8 @@ struct Out {
 // The wave whose gated seeds are in the gate lane's survivor list (just enqueued on p.st): its graph, then its
 // records; a flagged wave hands its gated seeds back instead.
 void finish_wave(Pipeline &p, Out &o, uint64_t indices, bool gated_by_lane) {
-    DSG_CU(cudaGraphLaunch(p.exec, p.st));
+    if (p.eager) capture_wave(p);
+    else DSG_CU(cudaGraphLaunch(p.exec, p.st));
     DSG_CU(cudaMemcpyAsync(p.h_ts, p.d_ts, 16 * 8, cudaMemcpyDeviceToHost, p.st));
     DSG_CU(cudaMemcpyAsync(p.h_ctr, p.ctr, C_N * 4, cudaMemcpyDeviceToHost, p.st));
     DSG_CU(cudaMemcpyAsync(p.h_gcnt, gate::lane_counts(p.lane), 16, cudaMemcpyDeviceToHost, p.st));
@@ -1025,6 +1071,19 @@ extern "C" int dsg_search_seeds(const uint64_t *seeds, uint32_t n, dsg_search_se
     });
 }
 
+extern "C" int dsg_search_last_wave(uint64_t info[10]) {
+    return guarded([&] {
+        DSG_ARG(info, "dsg_search_last_wave: null pointer");
+        Pipeline &p = PL();
+        std::lock_guard<std::mutex> l(p.mu);
+        DSG_ARG(p.open, "dsg_search_last_wave: dsg_search_open has not been called");
+        const uint32_t *c = p.h_ctr;
+        const uint64_t v[10] = {c[C_FLAGS], c[C_NS], c[C_SITES], c[C_NHOT], c[C_NBIG], c[C_MAXZ], c[C_ZONES], c[C_CELLS], c[C_KEPT], c[C_MAXEV]};
+        std::copy(v, v + 10, info);
+        return DSG_OK;
+    });
+}
+
 extern "C" int dsg_search_stage_ms(double ms[8], int reset) {
     return guarded([&] {
         DSG_ARG(ms, "dsg_search_stage_ms: null pointer");
@@ -1042,7 +1101,8 @@ extern "C" int dsg_search_close(void) {
         std::lock_guard<std::mutex> l(p.mu);
         if (!p.open) return DSG_OK;
         DSG_CU(cudaStreamSynchronize(p.st));
-        cudaGraphExecDestroy(p.exec); p.exec = nullptr;
+        if (p.exec) cudaGraphExecDestroy(p.exec);
+        p.exec = nullptr;
         void *bufs[] = {p.ctr, p.seeds, p.noise, p.tabin, p.tab, p.mx, p.act, p.nact, p.raw, p.nraw, p.sites, p.nsites, p.nbuck, p.hot,
                         p.f1, p.f2, p.f8, p.f4, p.meta1, p.meta2, p.evals, p.cov, p.nzone, p.zfirst, p.zslot, p.zmslot, p.zones, p.zmeta,
                         p.chunks, p.bits, p.par, p.rid, p.cs, p.khi, p.klo, p.rec, p.zcnt, p.zoff, p.zfill, p.zcomp, p.evu, p.ev, p.nev,

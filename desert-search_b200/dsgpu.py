@@ -313,7 +313,7 @@ class SearchParams(C.Structure):
                 ("ta", C.c_float), ("t", C.c_float), ("wc", C.c_float), ("we", C.c_float),
                 ("max_sites", C.c_int32), ("nms", C.c_int32), ("exact_n", C.c_int32),
                 ("hot_min", C.c_double), ("hot_pre", C.c_double), ("exact_min", C.c_double), ("refine_mb", C.c_double),
-                ("csv_min", C.c_double), ("wave", C.c_uint64), ("seeds_cap", C.c_uint32), ("reserved", C.c_uint32)]
+                ("csv_min", C.c_double), ("wave", C.c_uint64), ("seeds_cap", C.c_uint32), ("flags", C.c_uint32)]
 
 
 SEARCH_SEED = np.dtype([("seed", "<u8"), ("fya", "<f8"), ("fyb", "<f8"), ("maxta", "<f4"), ("maxtb", "<f4"), ("candidates", "<u4"),
@@ -324,7 +324,8 @@ SEARCH_ROW = np.dtype([("seed", "<u8"), ("rank", "<u4"), ("x", "<i4"), ("z", "<i
 # the searcher's Params defaults (dsearch_desert.cpp:50-78) for the production command line gate=1 gpu=1 gscan=1
 SEARCH_DEFAULTS = dict(gate_phase=0.06, gate_pthr=0.645, gate_amp=0.70, ta=0.25, t=0.55, wc=0.25, we=0.41, max_sites=300, nms=5000,
                        exact_n=2, hot_min=180.0, hot_pre=0.8, exact_min=75.0, refine_mb=70.0, csv_min=50.0, wave=0,
-                       seeds_cap=0)
+                       seeds_cap=0, flags=0)
+SEARCH_EAGER = 1
 
 
 def search_open(**kw):
@@ -341,6 +342,17 @@ def search_stage_ms(reset=False):
     ms = np.zeros(8)
     _ck(lib.dsg_search_stage_ms(ptr(ms, f64p), C.c_int(1 if reset else 0)), "dsg_search_stage_ms")
     return dict(zip(SEARCH_STAGES, ms.tolist()))
+
+
+SEARCH_WAVE_INFO = ["flags", "gated", "sites", "hot_floods_used", "big_zones", "max_zones_per_seed", "zones", "proxy_cells", "components",
+                    "max_evals_per_seed"]
+
+
+def search_last_wave():
+    """Counters of the last wave (dsg_search_last_wave) as a dict."""
+    v = np.zeros(10, dtype=np.uint64)
+    _ck(lib.dsg_search_last_wave(ptr(v, u64p)), "dsg_search_last_wave")
+    return dict(zip(SEARCH_WAVE_INFO, (int(x) for x in v)))
 
 
 def search_close():

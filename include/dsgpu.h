@@ -282,8 +282,11 @@ typedef struct dsg_search_params {
     uint64_t wave;                             /* seed indices per wave (0 = 2^22, at most 2^26) */
     uint32_t seeds_cap;                        /* gated seeds per wave (0 = 1,024, the most); the wave's zone, cell and
                                                   flood-tile capacities scale with it (about 20 GB of device memory at 1,024) */
-    uint32_t reserved;
+    uint32_t flags;                            /* DSG_SEARCH_EAGER: no graph, the stages launched on a stream per wave
+                                                  and the flood loops driven by the host (for profilers that cannot
+                                                  see the kernels of graphs with conditional nodes) */
 } dsg_search_params;
+#define DSG_SEARCH_EAGER 1u
 /* One gated seed: its PREFIX.seeds.csv line (dsearch_desert.cpp:548), rows[row0 .. row0 + nrows) its CSV rows. */
 typedef struct dsg_search_seed {
     uint64_t seed;
@@ -325,6 +328,10 @@ int dsg_search_seeds(const uint64_t *seeds, uint32_t n, dsg_search_seed *seeds_o
  * replay, proxy components + exact-start search, step-8 floods, step-4 floods + results}.  No reference
  * counterpart (the reference prints core-seconds per stage on its progress line, dsearch_desert.cpp:552). */
 int dsg_search_stage_ms(double ms[8], int reset);
+/* Counters of the last wave, for capacity planning: {wave flags, gated seeds, sites, hot-zone floods used, big
+ * zones, most big zones of one seed, zones, proxy cells (saturating at 2^32 - 1), components kept, most
+ * evaluations of one seed}. */
+int dsg_search_last_wave(uint64_t info[10]);
 int dsg_search_close(void);
 
 #ifdef __cplusplus

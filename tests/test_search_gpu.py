@@ -60,6 +60,8 @@ def test_search_run_covers_exactly_the_gate_survivors(dsg):
     dsg.search_open()
     try:
         recs, rows, unf, counts, ms = dsg.search_run(start, count)
+        info = dsg.search_last_wave()
+        print("\nlast wave:", info, "flags of all waves:", counts[7])
     finally:
         dsg.search_close()
     surv, _, gc, rc = dsg.gate_run(start, count, batch=1 << 22)
@@ -67,5 +69,23 @@ def test_search_run_covers_exactly_the_gate_survivors(dsg):
     got = np.sort(np.concatenate([recs["seed"], unf]))
     assert np.array_equal(got, np.sort(surv))
     assert counts[:4] == [int(x) for x in gc]
-    assert ms > 0 and len(unf) == 0
+    assert ms > 0 and len(unf) == 0, (counts, info)
     assert all(r["row0"] + r["nrows"] <= len(rows) for r in recs)
+
+
+def test_graph_and_stream_launched_waves_agree(dsg):
+    """The wave graph (conditional WHILE nodes for the flood loops) and the same stages launched on a stream with
+    the loops driven by the host (the profiling mode) give the same records and rows."""
+    dsg.scan_init_default()
+    out = []
+    for flags in (0, dsg.SEARCH_EAGER):
+        dsg.search_open(flags=flags)
+        try:
+            recs, rows, unf, counts, ms = dsg.search_run(9 * 10**12, 1 << 22)
+        finally:
+            dsg.search_close()
+        r = sorted(tuple(x[:8]) + (x[9],) for x in recs.tolist())          # all but row0 (output position)
+        w = sorted(rows.tolist())
+        out.append((r, w, sorted(unf.tolist()), counts[:8]))
+    assert out[0] == out[1]
+    assert len(out[0][0]) > 100
