@@ -55,9 +55,9 @@ constexpr uint32_t SC_MAX = 1024;            // gated seeds per wave (at most; d
 constexpr uint32_t RAWCAP = 1u << 16;        // raw scan candidates per seed (the reference's per-seed buffer, gproxy.cu:209)
 constexpr int HT = 4096;                     // bucket hash slots per seed (shared memory)
 constexpr uint32_t MS = 300;                 // sites per seed (Params.max_sites at most this)
-constexpr uint32_t ZPS = 256;                // big hot zones per seed
+constexpr uint32_t ZPS = MS;                 // big hot zones per seed (at most one per site)
 // zones, proxy cells and flood tiles per wave are set for SC_MAX seeds and scale with seeds_cap (Pipeline::caps)
-constexpr uint32_t EVC = 512;                // proxy components kept per seed
+constexpr uint32_t EVC = 2048;               // proxy components kept per seed
 constexpr int EXN = 2;                       // exact floods per seed (Params.exact_n at most this)
 constexpr uint32_t ROWCAP = 1u << 16;        // CSV rows per wave
 constexpr uint32_t LOOP_LIMIT = 2048;        // flood loop iterations (6 rounds each) before a wave gives up
@@ -699,7 +699,7 @@ struct Caps {
         sc = seeds;
         const double f = double(seeds) / SC_MAX;
         zcap = std::max<uint32_t>(1024, uint32_t(32768 * f));
-        cellcap = std::max<uint64_t>(1u << 22, uint64_t(double(1u << 27) * f));
+        cellcap = std::max<uint64_t>(1u << 22, uint64_t(double(1u << 28) * f));
         compcap = std::max<uint32_t>(1u << 16, uint32_t(double(1u << 22) * f));
         chcap = cellcap / CHUNK + zcap;
         tries = seeds * EXN * 3;
