@@ -164,7 +164,8 @@ def cpu_baseline(cores, seconds_budget=20.0):
 
 # ---------------------------------------------------------------------------- the device pipeline
 def search_steps(dsgpu, base, steps, warmup, per_step):
-    """W untimed steps, then K timed ones of per_step seed indices each: (device ms, wall s, counts[10], d2h bytes).
+    """W untimed steps, then K timed ones of per_step seed indices each: (device ms, wall s, counts[10] + [handed back],
+    d2h bytes).
     The stage timers cover the timed steps only."""
     import torch
     for i in range(warmup):
@@ -172,7 +173,7 @@ def search_steps(dsgpu, base, steps, warmup, per_step):
     dsgpu.search_stage_ms(reset=True)
     base += warmup * per_step
     torch.cuda.synchronize()
-    ms, tot, d2h = 0.0, [0] * 10, 0
+    ms, tot, d2h = 0.0, [0] * 11, 0
     t0 = time.perf_counter()
     for i in range(steps):
         recs, rows, unf, c, m = dsgpu.search_run(base + i * per_step, per_step)
@@ -180,6 +181,7 @@ def search_steps(dsgpu, base, steps, warmup, per_step):
         for k in (0, 1, 2, 3, 4, 5, 6, 8, 9):
             tot[k] += c[k]
         tot[7] |= c[7]
+        tot[10] += len(unf)                          # gated seeds of waves over a capacity: handed back, not finished
         d2h += recs.nbytes + rows.nbytes + unf.nbytes
     torch.cuda.synchronize()
     return ms, time.perf_counter() - t0, tot, d2h // max(1, steps)
@@ -520,7 +522,9 @@ def run_ours(args):
     stages = dsgpu.search_stage_ms()
     clocks = clk.stop()
     rep.barrier()
-    ms_max, summed, value = rep.combine(ms, tot[:4])
+    # the metric counts gated seeds carried through every stage: seeds handed back by an over-capacity wave are not
+    ms_max, summed, value = rep.combine(ms, tot[:3] + [tot[3] - tot[10]])
+    handed_back = int(rep.reduce([tot[10]], "SUM")[0])
     wall_max = rep.reduce([wall], "MAX")[0]
     extra_tot = rep.reduce(tot[4:7], "SUM")
     if args.profile_run:
@@ -545,7 +549,8 @@ def run_ours(args):
                    "l2": "no input data (seeds generated on the device); each wave writes ~6 MiB of tables per gated seed (GBs per wave), "
                          "larger than L2"},
         "counts": {"seeds": int(summed[0]), "phase_passed": int(summed[1]), "pre_passed": int(summed[2]), "gated": int(summed[3]),
-                   "sites": int(extra_tot[0]), "hot_zones": int(extra_tot[1]), "big_zones": int(extra_tot[2]), "wave_flags": int(tot[7])},
+                   "sites": int(extra_tot[0]), "hot_zones": int(extra_tot[1]), "big_zones": int(extra_tot[2]), "wave_flags": int(tot[7]),
+                   "handed_back": handed_back},
         "seeds_per_s": summed[0] / (ms_max / 1e3),
         "e2e": {"value": summed[3] / wall_max, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": d2h,
                 "how": "wall clock of the dsg_search_run calls (C ABI) with the seed records and CSV rows copied to host memory"},

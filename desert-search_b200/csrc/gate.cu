@@ -687,6 +687,14 @@ Lane *lane_create(uint64_t batch) {
     return l;
 }
 void lane_enqueue(Lane *l, cudaStream_t st, uint64_t start, uint64_t nb, const dsg_gate_cfg &c) { enqueue_batch(l->g, st, start, nb, c); }
+void lane_destroy(Lane *l) {
+    if (!l) return;
+    State &g = l->g;
+    cudaFree(g.d_s1); cudaFree(g.d_s2); cudaFree(g.d_s3); cudaFree(g.d_idx2); cudaFree(g.d_a3); cudaFree(g.d_oct); cudaFree(g.d_n);
+    cudaFreeHost(g.h_n); cudaFreeHost(g.h_s3); cudaFreeHost(g.h_a3);
+    if (g.st) cudaStreamDestroy(g.st);
+    delete l;
+}
 const uint64_t *lane_survivors(const Lane *l) { return l->g.d_s3; }
 uint32_t *lane_counts(Lane *l) { return l->g.d_n; }
 void lane_caps(const Lane *l, uint32_t caps[3]) { caps[0] = l->g.cap1; caps[1] = l->g.cap2; caps[2] = l->g.cap3; }

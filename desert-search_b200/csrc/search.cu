@@ -32,6 +32,7 @@ namespace gate {
 struct Lane;
 Lane *lane_create(uint64_t batch);
 void lane_enqueue(Lane *l, cudaStream_t st, uint64_t start, uint64_t nb, const dsg_gate_cfg &c);
+void lane_destroy(Lane *l);
 const uint64_t *lane_survivors(const Lane *l);
 uint32_t *lane_counts(Lane *l);
 void lane_caps(const Lane *l, uint32_t caps[3]);
@@ -265,10 +266,11 @@ __global__ void __launch_bounds__(256) k_hot(const SeedNoise *__restrict__ noise
 }
 
 // ---------------------------------------------------------------- flood requests
-__device__ __forceinline__ FloodCtl make_ctl(int32_t qx, int32_t qz, int step, int half, int conn8, int pred, int32_t noise, uint32_t k) {
+__device__ __forceinline__ FloodCtl make_ctl(int32_t qx, int32_t qz, int step, int half, int conn8, int pred, int32_t noise, uint32_t k,
+                                             int eager = 0) {
     FloodCtl c{};
     c.qx = qx; c.qz = qz; c.step = step; c.half = half; c.n = 2 * half + 1; c.tpr = (c.n + TILE - 1) / TILE;
-    c.conn8 = conn8; c.pred = pred; c.pcut = 0.f; c.noise = noise; c.eager = 0; c.pad = 0;
+    c.conn8 = conn8; c.pred = pred; c.pcut = 0.f; c.noise = noise; c.eager = eager; c.pad = 0;
     c.dir_off = int64_t(k) * c.tpr * c.tpr;
     return c;
 }
@@ -373,44 +375,64 @@ __device__ __forceinline__ bool covers(uint32_t cv, int64_t bx, int64_t bz, cons
         }
     return false;
 }
-// Warp per seed: the reference's walk over its sites in rank order, using only the floods of the sites it does
-// not skip (the lanes test the floods used so far in parallel); big zones (hot area >= hot_min) become proxy zones
-// of 32-quart cells around the step-128 flood's bbox.
+constexpr uint32_t CW = (MS + 31) / 32;      // words of a per-site bit set over the seed's sites
+// The flood a hot site uses when the walk does not skip it: its pre-flood when small, else its step-128 flood.
+__device__ __forceinline__ uint32_t used_flood(const int32_t *f1, const int32_t *f2, const FloodStat *st1, uint32_t w, const Params &P) {
+    const int32_t k1 = f1[w];
+    return small_zone(st1[k1], P) ? uint32_t(k1) : 0x80000000u | uint32_t(f2[w]);
+}
+// Warp per (seed, site r): bit r' of cvm[r] = site r' < r is hot and the flood it would use covers r's key block.
+// Every pair at once, so that the sequential walk below only combines bit sets.
+__global__ void __launch_bounds__(256) k_cover_pairs(const Hot *__restrict__ hot, const uint32_t *__restrict__ nsites, const int32_t *__restrict__ f1,
+                                                     const int32_t *__restrict__ f2, FloodView v1, FloodView v2, const FloodStat *__restrict__ st1,
+                                                     Tiles T, Params P, uint32_t *__restrict__ cvm, const uint32_t *ctr) {
+    const int lane = threadIdx.x & 31;
+    const uint32_t nS = ctr[C_NS];
+    const uint32_t warps = gridDim.x * (blockDim.x >> 5);
+    for (uint32_t w = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5); w < nS * MS; w += warps) {
+        const uint32_t s = w / MS, r = w % MS;
+        if (r >= nsites[s]) continue;
+        const Hot h = hot[w];
+        uint32_t *row = cvm + size_t(w) * CW;
+        if (h.bt < 0.55) continue;                       // never tested (the walk skips it first)
+        const int64_t bx = int64_t((h.hx + 8000000) >> 7) * 128 - 8000000, bz = int64_t((h.hz + 8000000) >> 7) * 128 - 8000000;
+        for (uint32_t base = 0; base < r; base += 32) {
+            const uint32_t r2 = base + lane;
+            bool hit = false;
+            if (r2 < r && hot[s * MS + r2].bt >= 0.55) hit = covers(used_flood(f1, f2, st1, s * MS + r2, P), bx, bz, v1, v2, T);
+            const uint32_t m = __ballot_sync(0xffffffffu, hit);
+            if (lane == 0) row[base >> 5] = m;
+        }
+    }
+}
+// Warp per seed: the reference's walk over its sites in rank order (dsearch_desert.cpp:326-372): a hot site is
+// skipped when a flood used so far covers it (lane j < CW holds word j of the used set); else its flood is used,
+// and a big one (hot area >= hot_min) becomes a proxy zone of 32-quart cells around the step-128 flood's bbox.
 __global__ void __launch_bounds__(256) k_cover(const Hot *__restrict__ hot, const uint32_t *__restrict__ nsites, const int32_t *__restrict__ f1,
-                                               const int32_t *__restrict__ f2, FloodView v1, FloodView v2, const FloodStat *__restrict__ st1,
-                                               const FloodStat *__restrict__ st2, Tiles T, Params P, uint32_t *__restrict__ cov_buf,
-                                               uint32_t *__restrict__ nzone, DZone *__restrict__ zslot, ZoneMeta *__restrict__ zmeta, uint32_t *ctr) {
+                                               const int32_t *__restrict__ f2, const FloodStat *__restrict__ st1, const FloodStat *__restrict__ st2,
+                                               Params P, const uint32_t *__restrict__ cvm, uint32_t *__restrict__ nzone, DZone *__restrict__ zslot,
+                                               ZoneMeta *__restrict__ zmeta, uint32_t *ctr) {
     const int lane = threadIdx.x & 31;
     const uint32_t s = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
     if (s >= ctr[C_NS]) return;
-    uint32_t *cov = cov_buf + size_t(s) * MS;
-    uint32_t ncov = 0, nz = 0, nhot = 0, nbig = 0;
+    uint32_t used = 0;                                   // word `lane` of the used set (lanes < CW)
+    uint32_t nz = 0, nhot = 0, nbig = 0;
     const uint32_t ns = nsites[s];
     for (uint32_t r = 0; r < ns; r++) {
         const uint32_t w = s * MS + r;
         const Hot h = hot[w];
         if (h.bt < 0.55) continue;
-        const int64_t bx = int64_t((h.hx + 8000000) >> 7) * 128 - 8000000, bz = int64_t((h.hz + 8000000) >> 7) * 128 - 8000000;
-        bool hit = false;
-        for (uint32_t k = lane; k < ncov; k += 32) hit |= covers(__ldcg(cov + k), bx, bz, v1, v2, T);
+        const uint32_t words = (r + 31) >> 5;            // bits of sites before r
+        const bool hit = uint32_t(lane) < words && (used & cvm[size_t(w) * CW + lane]) != 0;
         if (__any_sync(0xffffffffu, hit)) continue;
-        const int32_t k1 = f1[w];
+        if (uint32_t(lane) == (r >> 5)) used |= 1u << (r & 31);
         nhot++;
-        if (small_zone(st1[k1], P)) {
-            if (lane == 0) __stcg(cov + ncov, uint32_t(k1));
-            ncov++;
-            __syncwarp();
-            continue;
-        }
-        const int32_t k2 = f2[w];
-        if (lane == 0) __stcg(cov + ncov, 0x80000000u | uint32_t(k2));
-        ncov++;
-        __syncwarp();
-        const FloodStat a = st2[k2];
+        const int32_t k1 = f1[w];
+        if (small_zone(st1[k1], P)) continue;
+        const FloodStat a = st2[f2[w]];
         const double hot_area = double(a.cells) * 128.0 * 128 * 16 / 1e6;
         if (hot_area < P.hot_min) continue;
         nbig++;
-        if (nz == ZPS) { if (lane == 0) atomicOr(ctr + C_FLAGS, F_ZONES); continue; }
         if (lane == 0) {
             DZone z{};
             z.x0 = int(floor((a.minx - 128) / 32.0)) * 32; z.z0 = int(floor((a.minz - 128) / 32.0)) * 32;
@@ -514,15 +536,18 @@ __global__ void k_comp_scatter(const dsg_component *__restrict__ rec, const uint
 // Thread per seed: components of its zones in (zone, first cell) order, each new one (by its smallest column and
 // row) an evaluation whose start is the interior cell nearest the centroid (alternatives at ranks n/3, 2n/3);
 // evaluations sorted by proxy size with std::sort's algorithm; exact-flood starts of the first exact_n.
-__global__ void k_evals(const uint32_t *__restrict__ zfirst, const DZone *__restrict__ zones, const ZoneMeta *__restrict__ zmeta,
-                        const uint32_t *__restrict__ zoff, uint32_t *__restrict__ zcomp, const dsg_component *__restrict__ rec, Params P,
-                        Eval *__restrict__ evu, Eval *__restrict__ ev, uint32_t *__restrict__ nev, int64_t *__restrict__ sig, Try *__restrict__ tries,
-                        uint32_t *ctr) {
-    const uint32_t s = blockIdx.x * blockDim.x + threadIdx.x;
+__global__ void __launch_bounds__(256) k_evals(const uint32_t *__restrict__ zfirst, const DZone *__restrict__ zones,
+                                               const ZoneMeta *__restrict__ zmeta, const uint32_t *__restrict__ zoff, uint32_t *__restrict__ zcomp,
+                                               const dsg_component *__restrict__ rec, Params P, Eval *__restrict__ evu, Eval *__restrict__ ev,
+                                               uint32_t *__restrict__ nev, int64_t *__restrict__ sig, uint16_t *__restrict__ sidx,
+                                               Try *__restrict__ tries, uint32_t *ctr) {
+    const int lane = threadIdx.x & 31;
+    const uint32_t s = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
     if (s >= ctr[C_NS]) return;
     Eval *U = evu + size_t(s) * EVC, *E = ev + size_t(s) * EVC;
     int64_t *seen = sig + size_t(s) * EVC;
-    uint32_t ne = 0, nseen = 0;
+    uint16_t *idx = sidx + size_t(s) * EVC;
+    uint32_t ne = 0;                                     // evaluations so far (= signatures seen), uniform across the warp
     bool full = false;
     const uint32_t nzw = ctr[C_ZONES];
     for (uint32_t zi = zfirst[s]; zi < zfirst[s + 1] && zi < nzw; zi++) {
@@ -530,50 +555,59 @@ __global__ void k_evals(const uint32_t *__restrict__ zfirst, const DZone *__rest
         const ZoneMeta m = zmeta[zi];
         uint32_t *L = zcomp + zoff[zi];
         const uint32_t nc = zoff[zi + 1] - zoff[zi];
-        for (uint32_t i = 1; i < nc; i++) {                 // by first cell (unique within a zone)
-            const uint32_t v = L[i];
-            int32_t j = int32_t(i) - 1;
-            while (j >= 0 && rec[L[j]].first > rec[v].first) { L[j + 1] = L[j]; j--; }
-            L[j + 1] = v;
-        }
+        if (lane == 0)
+            for (uint32_t i = 1; i < nc; i++) {             // by first cell (unique within a zone)
+                const uint32_t v = L[i];
+                int32_t j = int32_t(i) - 1;
+                while (j >= 0 && rec[L[j]].first > rec[v].first) { L[j + 1] = L[j]; j--; }
+                L[j + 1] = v;
+            }
+        __syncwarp();
         for (uint32_t i = 0; i < nc; i++) {
-            const dsg_component c = rec[L[i]];
+            const dsg_component c = rec[__ldcg(L + i)];
             const double area = c.cells * 32.0 * 32 * 16 / 1e6;
             if (area < 1) continue;
             const int64_t sg = (int64_t(z.x0 + c.minx * 32) << 32) | uint32_t(z.z0 + c.minz * 32);
             bool dup = false;
-            for (uint32_t k = 0; k < nseen; k++) dup |= seen[k] == sg;
-            if (dup) continue;
-            if (nseen == EVC) { full = true; continue; }
-            seen[nseen++] = sg;
-            const int32_t cell = c.inner ? c.pick[0] : c.first;
-            Eval e{};
-            e.rank = m.rank; e.x = z.x0 + (cell % z.nx) * 32; e.z = z.z0 + (cell / z.nx) * 32;
-            e.proxy = area; e.s8 = -1; e.s4 = 0; e.hot = m.hot;
-            e.nalt = c.inner ? 2 : 0;
-            for (int a = 0; a < e.nalt; a++) { e.ax[a] = z.x0 + (c.pick[a + 1] % z.nx) * 32; e.az[a] = z.z0 + (c.pick[a + 1] / z.nx) * 32; }
-            U[ne++] = e;
+            for (uint32_t k = lane; k < ne; k += 32) dup |= __ldcg(seen + k) == sg;
+            if (__any_sync(0xffffffffu, dup)) continue;
+            if (ne == EVC) { full = true; continue; }
+            if (lane == 0) {
+                __stcg(seen + ne, sg);
+                const int32_t cell = c.inner ? c.pick[0] : c.first;
+                Eval e{};
+                e.rank = m.rank; e.x = z.x0 + (cell % z.nx) * 32; e.z = z.z0 + (cell / z.nx) * 32;
+                e.proxy = area; e.s8 = -1; e.s4 = 0; e.hot = m.hot;
+                e.nalt = c.inner ? 2 : 0;
+                for (int a = 0; a < e.nalt; a++) { e.ax[a] = z.x0 + (c.pick[a + 1] % z.nx) * 32; e.az[a] = z.z0 + (c.pick[a + 1] / z.nx) * 32; }
+                U[ne] = e;
+            }
+            ne++;
+            __syncwarp();
         }
     }
-    if (full) atomicOr(ctr + C_FLAGS, F_EVALS);
-    atomicMax(ctr + C_MAXEV, nseen + (full ? 1 : 0));
-    // std::sort(ev, proxy descending): the permutation from the sort, the records copied out in its order
-    uint16_t idx[EVC];
-    for (uint32_t k = 0; k < ne; k++) idx[k] = uint16_t(k);
-    dsg::stl::sort(idx, int64_t(ne), [&](uint16_t a, uint16_t b) { return U[a].proxy > U[b].proxy; });
-    for (uint32_t k = 0; k < ne; k++) E[k] = U[idx[k]];
-    if (s == 0 && ctr[C_PROXY + 3]) atomicOr(ctr + C_FLAGS, F_LABEL);
-    nev[s] = ne;
-    for (int k2 = 0; k2 < EXN; k2++)
-        for (int t = 0; t < 3; t++) {
-            Try &tr = tries[(size_t(s) * EXN + k2) * 3 + t];
-            tr.valid = 0; tr.q = INT_MAX;
-            if (k2 >= P.exact_n || uint32_t(k2) >= ne || E[k2].proxy < P.exact_min) continue;
-            if (t > E[k2].nalt) continue;
+    if (lane == 0) {
+        if (full) atomicOr(ctr + C_FLAGS, F_EVALS);
+        atomicMax(ctr + C_MAXEV, ne + (full ? 1 : 0));
+        if (s == 0 && ctr[C_PROXY + 3]) atomicOr(ctr + C_FLAGS, F_LABEL);
+        // std::sort(ev, proxy descending): the permutation from the sort, then the records copied out in its order
+        for (uint32_t k = 0; k < ne; k++) idx[k] = uint16_t(k);
+        dsg::stl::sort(idx, int64_t(ne), [&](uint16_t a, uint16_t b) { return U[a].proxy > U[b].proxy; });
+        nev[s] = ne;
+    }
+    __syncwarp();
+    for (uint32_t k = lane; k < ne; k += 32) E[k] = U[idx[k]];
+    __syncwarp();
+    if (lane < EXN * 3) {
+        const int k2 = lane / 3, t = lane % 3;
+        Try &tr = tries[(size_t(s) * EXN + k2) * 3 + t];
+        tr.valid = 0; tr.q = INT_MAX;
+        if (k2 < P.exact_n && uint32_t(k2) < ne && E[k2].proxy >= P.exact_min && t <= E[k2].nalt) {
             tr.valid = 1;
             tr.sx = t == 0 ? E[k2].x : E[k2].ax[t - 1];
             tr.sz = t == 0 ? E[k2].z : E[k2].az[t - 1];
         }
+    }
 }
 // Nearest desert point of every exact-flood start: first of rings 0..8 (16 quarts apart) in (r, dz, dx) order
 // with state 2 (dsearch_desert.cpp:505-510).
@@ -595,7 +629,9 @@ __global__ void k_req_8(const Try *__restrict__ tries, uint32_t *ctr, FloodCtl *
         if (!t.valid || t.q == INT_MAX) continue;
         const uint32_t j = atomicAdd(ctr + C_NREQ + 2, 1u);
         f8[k] = int32_t(j);
-        ctl[j] = make_ctl(t.sx + c_ring[t.q][0] * 16, t.sz + c_ring[t.q][1] * 16, 8, 16000 / 8, 1, DSG_PRED_DESERT, int32_t(k / (EXN * 3)), j);
+        // exact floods are few and large: eager tiles (whole neighbouring tiles once a tile's region is large) take
+        // fewer rounds; the result does not depend on it
+        ctl[j] = make_ctl(t.sx + c_ring[t.q][0] * 16, t.sz + c_ring[t.q][1] * 16, 8, 16000 / 8, 1, DSG_PRED_DESERT, int32_t(k / (EXN * 3)), j, 1);
     }
 }
 // Thread per (seed, exact slot): the reference's retry loop (stop once a start reaches 0.6 x proxy) over the
@@ -625,7 +661,7 @@ __global__ void k_retry(const Try *__restrict__ tries, const int32_t *__restrict
         if (e.s8 >= P.refine_mb) {
             const uint32_t j = atomicAdd(ctr + C_NREQ + 3, 1u);
             f4[k] = int32_t(j);
-            ctl4[j] = make_ctl(bx, bz, 4, 16000 / 4, 0, DSG_PRED_DESERT, int32_t(s), j);
+            ctl4[j] = make_ctl(bx, bz, 4, 16000 / 4, 0, DSG_PRED_DESERT, int32_t(s), j, 1);
         }
     }
 }
@@ -716,7 +752,9 @@ struct Pipeline {
     uint64_t wave = 0;
     uint32_t min_cells = 1;
     cudaStream_t st = nullptr, body_st = nullptr;
-    gate::Lane *lane = nullptr;
+    gate::Lane *lane[2] = {nullptr, nullptr};    // two gate lanes: the gate of wave k + 1 runs while wave k's graph does
+    cudaStream_t gst = nullptr;                  // the gates' stream (low priority)
+    cudaEvent_t ev_gate[2] = {}, ev_done[2] = {}, ev_start = nullptr, ev_end = nullptr;
     uint32_t gcaps[3] = {0, 0, 0};
     // device buffers
     uint32_t *ctr = nullptr;
@@ -729,20 +767,20 @@ struct Pipeline {
     Phase ph[4]{};
     TilePool pool;
     unsigned long long *evals = nullptr;
-    uint32_t *cov = nullptr, *nzone = nullptr, *zfirst = nullptr;
+    uint32_t *cvm = nullptr, *nzone = nullptr, *zfirst = nullptr;
     DZone *zslot = nullptr, *zones = nullptr; ZoneMeta *zmslot = nullptr, *zmeta = nullptr; uint2 *chunks = nullptr;
     uint8_t *bits = nullptr; int32_t *par = nullptr, *rid = nullptr; zones::CompStat *cs = nullptr; uint64_t *khi = nullptr; uint32_t *klo = nullptr;
     dsg_component *rec = nullptr; uint32_t *zcnt = nullptr, *zoff = nullptr, *zfill = nullptr, *zcomp = nullptr;
-    Eval *evu = nullptr, *ev = nullptr; uint32_t *nev = nullptr; int64_t *sig = nullptr; Try *tries = nullptr;
+    Eval *evu = nullptr, *ev = nullptr; uint32_t *nev = nullptr; uint16_t *sidx = nullptr; int64_t *sig = nullptr; Try *tries = nullptr;
     dsg_search_seed *out = nullptr; dsg_search_row *rows = nullptr;
     int grid_eval = 0, grid_conn = 0;
-    cudaGraphExec_t exec = nullptr;
+    cudaGraphExec_t exec[2] = {nullptr, nullptr};   // one graph per gate lane (the lane's buffers are baked in)
     bool eager = false;                          // no graph: every wave launches the stages on the stream (for profilers)
     uint32_t graph_kernels = 0;                  // kernel nodes of the wave graph outside the loop bodies
-    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
     static constexpr int NSTAGE = 8;             // gate | tables+scan | suppression+hot points | pre-floods | step-128 floods+coverage |
     double stage_ms[NSTAGE] = {};                // proxy+components+exact starts | step-8 floods | step-4 floods+results
-    unsigned long long *d_ts = nullptr, *h_ts = nullptr;   // stage boundary stamps of the last wave (device global timer, ns)
+    unsigned long long *d_ts = nullptr, *h_ts = nullptr;   // stage boundary stamps per lane: [0] gate start, [1..8] graph stages,
+                                                           // [9] gate end (device global timer, ns)
     // pinned host copies
     uint32_t *h_ctr = nullptr, *h_gcnt = nullptr; dsg_search_seed *h_out = nullptr; dsg_search_row *h_rows = nullptr; uint64_t *h_seeds = nullptr;
 };
@@ -806,29 +844,31 @@ void capture_phase(Pipeline &p, int k) {
 
 // Everything of a wave after the gate, as one graph.
 // In eager mode (profiling) the same sequence is launched on the stream for every wave instead.
-void capture_wave(Pipeline &p) {
+void capture_wave(Pipeline &p, int L) {
     if (!p.eager) DSG_CU(cudaStreamBeginCapture(p.st, cudaStreamCaptureModeRelaxed));
     uint32_t caps[3];
-    gate::lane_caps(p.lane, caps);
-    k_stamp<<<1, 1, 0, p.st>>>(p.d_ts, 1);
+    gate::lane_caps(p.lane[L], caps);
+    unsigned long long *ts = p.d_ts + 16 * L;
+    k_stamp<<<1, 1, 0, p.st>>>(ts, 1);
     const uint32_t SC = p.c.sc;
-    k_begin<<<8, 128, 0, p.st>>>(gate::lane_counts(p.lane), caps[0], caps[1], caps[2], SC, gate::lane_survivors(p.lane), p.seeds, p.ctr);
+    k_begin<<<8, 128, 0, p.st>>>(gate::lane_counts(p.lane[L]), caps[0], caps[1], caps[2], SC, gate::lane_survivors(p.lane[L]), p.seeds, p.ctr);
     seed_noise_build_dev(p.seeds, p.ctr + C_NS, SC, p.noise, p.st);
     const int table_launches = scan_seeds_device(p.noise, p.ctr + C_NS, SC, p.tabin, p.tab, p.mx, p.act, p.nact, p.raw, p.nraw, RAWCAP, p.P.sp, p.st);
-    k_stamp<<<1, 1, 0, p.st>>>(p.d_ts, 2);
+    k_stamp<<<1, 1, 0, p.st>>>(ts, 2);
     DSG_CU(cudaFuncSetAttribute(k_nms, cudaFuncAttributeMaxDynamicSharedMemorySize, int(NMS_SMEM)));
     k_nms<<<SC, NMS_THREADS, NMS_SMEM, p.st>>>(p.raw, p.nraw, p.P, p.sites, p.nsites, p.nbuck, p.ctr);
     k_hot<<<4 * 148, 256, 0, p.st>>>(p.noise, p.sites, p.nsites, p.ctr, p.hot);
     k_req_pre<<<4 * 148, 256, 0, p.st>>>(p.hot, p.nsites, p.ctr, p.ph[0].ctl, p.meta1, p.f1, p.f2);
     DSG_CU(cudaGetLastError());
-    k_stamp<<<1, 1, 0, p.st>>>(p.d_ts, 3);
+    k_stamp<<<1, 1, 0, p.st>>>(ts, 3);
     capture_phase(p, 0);
-    k_stamp<<<1, 1, 0, p.st>>>(p.d_ts, 4);
+    k_stamp<<<1, 1, 0, p.st>>>(ts, 4);
     k_req_128<<<4 * 148, 256, 0, p.st>>>(p.ph[0].st, p.ph[0].ctl, p.meta1, p.P, p.ctr, p.ph[1].ctl, p.meta2, p.f2);
     capture_phase(p, 1);
-    k_cover<<<(SC + 7) / 8, 256, 0, p.st>>>(p.hot, p.nsites, p.f1, p.f2, FloodView{p.ph[0].ctl, p.ph[0].dir}, FloodView{p.ph[1].ctl, p.ph[1].dir},
-                                               p.ph[0].st, p.ph[1].st, p.pool.T, p.P, p.cov, p.nzone, p.zslot, p.zmslot, p.ctr);
-    k_stamp<<<1, 1, 0, p.st>>>(p.d_ts, 5);
+    k_cover_pairs<<<8 * 148, 256, 0, p.st>>>(p.hot, p.nsites, p.f1, p.f2, FloodView{p.ph[0].ctl, p.ph[0].dir}, FloodView{p.ph[1].ctl, p.ph[1].dir},
+                                              p.ph[0].st, p.pool.T, p.P, p.cvm, p.ctr);
+    k_cover<<<(SC + 7) / 8, 256, 0, p.st>>>(p.hot, p.nsites, p.f1, p.f2, p.ph[0].st, p.ph[1].st, p.P, p.cvm, p.nzone, p.zslot, p.zmslot, p.ctr);
+    k_stamp<<<1, 1, 0, p.st>>>(ts, 5);
     k_zone_list<<<1, LIST_THREADS, 0, p.st>>>(p.nzone, p.zslot, p.zmslot, p.zfirst, p.zones, p.zmeta, p.chunks, p.ctr, p.c.zcap, p.c.cellcap, p.c.chcap);
     DSG_CU(cudaGetLastError());
     proxy_components_device(p.noise, p.zones, zones::ZoneWork{p.chunks, p.ctr + C_CHUNKS}, 8 * 148, p.bits, p.par, p.rid, p.cs, p.khi, p.klo,
@@ -838,14 +878,14 @@ void capture_wave(Pipeline &p) {
     k_comp_count<<<64, 256, 0, p.st>>>(p.rec, p.ctr, p.zcnt);
     k_comp_offsets<<<1, LIST_THREADS, 0, p.st>>>(p.zcnt, p.zoff, p.ctr);
     k_comp_scatter<<<64, 256, 0, p.st>>>(p.rec, p.ctr, p.zoff, p.zfill, p.zcomp);
-    k_evals<<<(SC + 63) / 64, 64, 0, p.st>>>(p.zfirst, p.zones, p.zmeta, p.zoff, p.zcomp, p.rec, p.P, p.evu, p.ev, p.nev, p.sig, p.tries,
-                                              p.ctr);
+    k_evals<<<(SC + 7) / 8, 256, 0, p.st>>>(p.zfirst, p.zones, p.zmeta, p.zoff, p.zcomp, p.rec, p.P, p.evu, p.ev, p.nev, p.sig, p.sidx, p.tries,
+                                             p.ctr);
     k_ring<<<8 * 148, 128, 0, p.st>>>(p.noise, world_dev(), p.tries, p.ctr);
     k_req_8<<<32, 256, 0, p.st>>>(p.tries, p.ctr, p.ph[2].ctl, p.f8);
     DSG_CU(cudaGetLastError());
-    k_stamp<<<1, 1, 0, p.st>>>(p.d_ts, 6);
+    k_stamp<<<1, 1, 0, p.st>>>(ts, 6);
     capture_phase(p, 2);
-    k_stamp<<<1, 1, 0, p.st>>>(p.d_ts, 7);
+    k_stamp<<<1, 1, 0, p.st>>>(ts, 7);
     k_retry<<<16, 256, 0, p.st>>>(p.tries, p.f8, p.ph[2].st, p.ph[2].ctl, p.ev, p.nev, p.P, p.ctr, p.ph[3].ctl, p.f4);
     capture_phase(p, 3);
     k_results<<<(SC + 127) / 128, 128, 0, p.st>>>(p.seeds, p.noise, p.mx, p.nbuck, p.nsites, p.sites, p.ev, p.nev, p.f4, p.ph[3].st, p.P, p.out,
@@ -853,15 +893,15 @@ void capture_wave(Pipeline &p) {
     k_pool_zero<<<8 * 148, 256, 0, p.st>>>(p.pool.T, p.ctr, p.pool.cap);
     k_wave_end<<<1, 1, 0, p.st>>>(p.ctr);
     DSG_CU(cudaGetLastError());
-    k_stamp<<<1, 1, 0, p.st>>>(p.d_ts, 8);
-    // kernels outside the loop bodies: 6 set-up/scan kernels and the table launches, 6 for suppression, hot points,
+    k_stamp<<<1, 1, 0, p.st>>>(ts, 8);
+    // kernels outside the loop bodies: 6 set-up/scan kernels and the table launches, 7 for suppression, hot points,
     // requests, coverage and zones, 9 for the proxy bitmaps and labelling, 10 for components, exact starts, retries,
     // results and the wave's end, 5 per flood phase, 8 stage stamps
-    p.graph_kernels = 6 + table_launches + 6 + 9 + 10 + 4 * 5 + 8;
+    p.graph_kernels = 6 + table_launches + 7 + 9 + 10 + 4 * 5 + 8;
     if (p.eager) return;
     cudaGraph_t g = nullptr;
     DSG_CU(cudaStreamEndCapture(p.st, &g));
-    DSG_CU(cudaGraphInstantiate(&p.exec, g, 0));
+    DSG_CU(cudaGraphInstantiate(&p.exec[L], g, 0));
     DSG_CU(cudaGraphDestroy(g));
 }
 }  // namespace search
@@ -901,8 +941,9 @@ extern "C" int dsg_search_open(const dsg_search_params *q) {
         DSG_CU(cudaDeviceGetStreamPriorityRange(&lo, &hi));
         DSG_CU(cudaStreamCreateWithPriority(&p.st, cudaStreamNonBlocking, hi));
         DSG_CU(cudaStreamCreateWithFlags(&p.body_st, cudaStreamNonBlocking));
-        p.lane = gate::lane_create(p.wave);
-        gate::lane_caps(p.lane, p.gcaps);
+        for (auto &ln : p.lane) ln = gate::lane_create(p.wave);
+        gate::lane_caps(p.lane[0], p.gcaps);
+        DSG_CU(cudaStreamCreateWithPriority(&p.gst, cudaStreamNonBlocking, lo));
         p.ctr = dalloc<uint32_t>(C_N);
         DSG_CU(cudaMemset(p.ctr, 0, C_N * 4));
         p.c = Caps(q->seeds_cap ? q->seeds_cap : SC_MAX);
@@ -928,7 +969,7 @@ extern "C" int dsg_search_open(const dsg_search_params *q) {
         p.pool.allocate(p.c.pool_tiles);
         p.evals = dalloc<unsigned long long>(1);
         round_grids(p.grid_eval, p.grid_conn);
-        p.cov = dalloc<uint32_t>(size_t(SC) * MS); p.nzone = dalloc<uint32_t>(SC); p.zfirst = dalloc<uint32_t>(SC + 1);
+        p.cvm = dalloc<uint32_t>(size_t(SC) * MS * CW); p.nzone = dalloc<uint32_t>(SC); p.zfirst = dalloc<uint32_t>(SC + 1);
         p.zslot = dalloc<DZone>(size_t(SC) * ZPS); p.zmslot = dalloc<ZoneMeta>(size_t(SC) * ZPS);
         p.zones = dalloc<DZone>(p.c.zcap); p.zmeta = dalloc<ZoneMeta>(p.c.zcap); p.chunks = dalloc<uint2>(p.c.chcap);
         p.bits = dalloc<uint8_t>(p.c.cellcap); p.par = dalloc<int32_t>(p.c.cellcap); p.rid = dalloc<int32_t>(p.c.cellcap);
@@ -937,17 +978,23 @@ extern "C" int dsg_search_open(const dsg_search_params *q) {
         p.zcnt = dalloc<uint32_t>(p.c.zcap + 1); p.zoff = dalloc<uint32_t>(p.c.zcap + 1); p.zfill = dalloc<uint32_t>(p.c.zcap + 1);
         p.zcomp = dalloc<uint32_t>(p.c.compcap);
         p.evu = dalloc<Eval>(size_t(SC) * EVC); p.ev = dalloc<Eval>(size_t(SC) * EVC); p.nev = dalloc<uint32_t>(SC); p.sig = dalloc<int64_t>(size_t(SC) * EVC);
+        p.sidx = dalloc<uint16_t>(size_t(SC) * EVC);
         p.tries = dalloc<Try>(p.c.tries);
         p.out = dalloc<dsg_search_seed>(SC); p.rows = dalloc<dsg_search_row>(ROWCAP);
         DSG_CU(cudaMallocHost(&p.h_ctr, C_N * 4)); DSG_CU(cudaMallocHost(&p.h_gcnt, 16));
         DSG_CU(cudaMallocHost(&p.h_out, SC * sizeof(dsg_search_seed))); DSG_CU(cudaMallocHost(&p.h_rows, ROWCAP * sizeof(dsg_search_row)));
         DSG_CU(cudaMallocHost(&p.h_seeds, SC * 8));
-        DSG_CU(cudaEventCreate(&p.ev0)); DSG_CU(cudaEventCreate(&p.ev1));
-        p.d_ts = dalloc<unsigned long long>(16);
-        DSG_CU(cudaMallocHost(&p.h_ts, 16 * 8));
+        DSG_CU(cudaEventCreate(&p.ev_start)); DSG_CU(cudaEventCreate(&p.ev_end));
+        for (int L = 0; L < 2; L++) {
+            DSG_CU(cudaEventCreateWithFlags(&p.ev_gate[L], cudaEventDisableTiming));
+            DSG_CU(cudaEventCreateWithFlags(&p.ev_done[L], cudaEventDisableTiming));
+        }
+        p.d_ts = dalloc<unsigned long long>(32);
+        DSG_CU(cudaMemset(p.d_ts, 0, 32 * 8));
+        DSG_CU(cudaMallocHost(&p.h_ts, 32 * 8));
         DSG_CU(cudaDeviceSynchronize());
         p.eager = (q->flags & DSG_SEARCH_EAGER) != 0;
-        if (!p.eager) capture_wave(p);
+        if (!p.eager) { capture_wave(p, 0); capture_wave(p, 1); }
         p.open = true;
         return DSG_OK;
     });
@@ -964,28 +1011,27 @@ struct Out {
     bool over = false;
     float ms = 0;
 };
-// The wave whose gated seeds are in the gate lane's survivor list (just enqueued on p.st): its graph, then its
+// The wave whose gated seeds are in gate lane L's survivor list (on p.st, after the gate): its graph, then its
 // records; a flagged wave hands its gated seeds back instead.
-void finish_wave(Pipeline &p, Out &o, uint64_t indices, bool gated_by_lane) {
-    if (p.eager) capture_wave(p);
-    else DSG_CU(cudaGraphLaunch(p.exec, p.st));
-    DSG_CU(cudaMemcpyAsync(p.h_ts, p.d_ts, 16 * 8, cudaMemcpyDeviceToHost, p.st));
+void finish_wave(Pipeline &p, Out &o, uint64_t indices, bool gated_by_lane, int L) {
+    if (p.eager) capture_wave(p, L);
+    else DSG_CU(cudaGraphLaunch(p.exec[L], p.st));
+    DSG_CU(cudaMemcpyAsync(p.h_ts + 16 * L, p.d_ts + 16 * L, 16 * 8, cudaMemcpyDeviceToHost, p.st));
     DSG_CU(cudaMemcpyAsync(p.h_ctr, p.ctr, C_N * 4, cudaMemcpyDeviceToHost, p.st));
-    DSG_CU(cudaMemcpyAsync(p.h_gcnt, gate::lane_counts(p.lane), 16, cudaMemcpyDeviceToHost, p.st));
+    DSG_CU(cudaMemcpyAsync(p.h_gcnt, gate::lane_counts(p.lane[L]), 16, cudaMemcpyDeviceToHost, p.st));
     DSG_CU(cudaMemcpyAsync(p.h_out, p.out, p.c.sc * sizeof(dsg_search_seed), cudaMemcpyDeviceToHost, p.st));
+    DSG_CU(cudaEventRecord(p.ev_done[L], p.st));         // lane L may take the next gate once its graph and copies are done
     DSG_CU(cudaStreamSynchronize(p.st));
     const uint32_t wrows = std::min(p.h_ctr[C_ROWS], ROWCAP);
     if (wrows) DSG_CU(cudaMemcpyAsync(p.h_rows, p.rows, size_t(wrows) * sizeof(dsg_search_row), cudaMemcpyDeviceToHost, p.st));
-    DSG_CU(cudaEventRecord(p.ev1, p.st));
     DSG_CU(cudaStreamSynchronize(p.st));
-    float ms = 0;
-    DSG_CU(cudaEventElapsedTime(&ms, p.ev0, p.ev1));
-    o.ms += ms;
-    for (int k = 0; k < Pipeline::NSTAGE; k++) p.stage_ms[k] += double(p.h_ts[k + 1] - p.h_ts[k]) * 1e-6;
+    const unsigned long long *t = p.h_ts + 16 * L;
+    if (gated_by_lane) p.stage_ms[0] += double(t[9] - t[0]) * 1e-6;
+    for (int k = 1; k < Pipeline::NSTAGE; k++) p.stage_ms[k] += double(t[k + 1] - t[k]) * 1e-6;
     const uint32_t wS = p.h_ctr[C_NS];
     o.tot[0] += indices; o.tot[1] += p.h_gcnt[0]; o.tot[2] += p.h_gcnt[1]; o.tot[3] += p.h_gcnt[2];
     o.tot[8] += p.h_ctr[C_ITERS];
-    o.tot[9] += uint64_t(p.graph_kernels) + uint64_t(BODY_KERNELS) * p.h_ctr[C_ITERS] + (gated_by_lane ? 4 : 0) + 1;   // + the first stamp
+    o.tot[9] += uint64_t(p.graph_kernels) + uint64_t(BODY_KERNELS) * p.h_ctr[C_ITERS] + (gated_by_lane ? 4 + 2 : 0);   // + gate stamps
     if (p.h_ctr[C_FLAGS]) {
         o.tot[7] |= p.h_ctr[C_FLAGS];
         if (p.h_ctr[C_FLAGS] & F_GATE) { set_error("device search: gate survivors exceed the wave's capacity"); throw ArgFail{}; }
@@ -1033,12 +1079,30 @@ extern "C" int dsg_search_run(uint64_t start, uint64_t count, dsg_search_seed *s
         DSG_ARG(p.open, "dsg_search_run: dsg_search_open has not been called");
         require_init();
         Out o{seeds_out, seed_cap, 0, rows_out, row_cap, 0, unfinished, unfinished_cap, 0};
-        for (uint64_t base = 0; base < count; base += p.wave) {
-            const uint64_t nb = std::min(p.wave, count - base);
-            DSG_CU(cudaEventRecord(p.ev0, p.st));
-            k_stamp<<<1, 1, 0, p.st>>>(p.d_ts, 0);
-            gate::lane_enqueue(p.lane, p.st, start + base, nb, p.gcfg);
-            finish_wave(p, o, nb, true);
+        const uint64_t waves = (count + p.wave - 1) / p.wave;
+        // the gate of wave k on lane k & 1 and the gates' stream, after lane k & 1's previous graph is done
+        auto gate = [&](uint64_t k) {
+            const int L = int(k & 1);
+            const uint64_t nb = std::min(p.wave, count - k * p.wave);
+            DSG_CU(cudaStreamWaitEvent(p.gst, p.ev_done[L], 0));
+            k_stamp<<<1, 1, 0, p.gst>>>(p.d_ts + 16 * L, 0);
+            gate::lane_enqueue(p.lane[L], p.gst, start + k * p.wave, nb, p.gcfg);
+            k_stamp<<<1, 1, 0, p.gst>>>(p.d_ts + 16 * L, 9);
+            DSG_CU(cudaEventRecord(p.ev_gate[L], p.gst));
+        };
+        if (waves) {
+            DSG_CU(cudaEventRecord(p.ev_start, p.gst));
+            gate(0);
+        }
+        for (uint64_t k = 0; k < waves; k++) {
+            if (k + 1 < waves) gate(k + 1);                  // overlaps this wave's graph
+            DSG_CU(cudaStreamWaitEvent(p.st, p.ev_gate[k & 1], 0));
+            finish_wave(p, o, std::min(p.wave, count - k * p.wave), true, int(k & 1));
+        }
+        if (waves) {
+            DSG_CU(cudaEventRecord(p.ev_end, p.st));
+            DSG_CU(cudaEventSynchronize(p.ev_end));
+            DSG_CU(cudaEventElapsedTime(&o.ms, p.ev_start, p.ev_end));
         }
         return report(o, n_seeds, n_rows, n_unfinished, counts, device_ms);
     });
@@ -1055,18 +1119,21 @@ extern "C" int dsg_search_seeds(const uint64_t *seeds, uint32_t n, dsg_search_se
         DSG_ARG(p.open, "dsg_search_seeds: dsg_search_open has not been called");
         require_init();
         Out o{seeds_out, seed_cap, 0, rows_out, row_cap, 0, unfinished, unfinished_cap, 0};
-        uint64_t *surv = const_cast<uint64_t *>(gate::lane_survivors(p.lane));
+        uint64_t *surv = const_cast<uint64_t *>(gate::lane_survivors(p.lane[0]));
+        DSG_CU(cudaEventRecord(p.ev_start, p.st));
         for (uint32_t base = 0; base < n; base += p.c.sc) {
             const uint32_t nb = std::min<uint32_t>(p.c.sc, n - base);
-            DSG_CU(cudaEventRecord(p.ev0, p.st));
-            k_stamp<<<1, 1, 0, p.st>>>(p.d_ts, 0);
-            // the seeds take the place of the gate's survivors: counts {0, 0, nb}
+            // the seeds take the place of lane 0's gate survivors: counts {0, 0, nb}
             std::memcpy(p.h_seeds, seeds + base, size_t(nb) * 8);
             p.h_gcnt[0] = 0; p.h_gcnt[1] = 0; p.h_gcnt[2] = nb; p.h_gcnt[3] = 0;
             DSG_CU(cudaMemcpyAsync(surv, p.h_seeds, size_t(nb) * 8, cudaMemcpyHostToDevice, p.st));
-            DSG_CU(cudaMemcpyAsync(gate::lane_counts(p.lane), p.h_gcnt, 16, cudaMemcpyHostToDevice, p.st));
-            finish_wave(p, o, nb, false);
+            DSG_CU(cudaMemcpyAsync(gate::lane_counts(p.lane[0]), p.h_gcnt, 16, cudaMemcpyHostToDevice, p.st));
+            k_stamp<<<1, 1, 0, p.st>>>(p.d_ts, 0);
+            finish_wave(p, o, nb, false, 0);
         }
+        DSG_CU(cudaEventRecord(p.ev_end, p.st));
+        DSG_CU(cudaEventSynchronize(p.ev_end));
+        DSG_CU(cudaEventElapsedTime(&o.ms, p.ev_start, p.ev_end));
         return report(o, n_seeds, n_rows, n_unfinished, counts, device_ms);
     });
 }
@@ -1101,17 +1168,20 @@ extern "C" int dsg_search_close(void) {
         std::lock_guard<std::mutex> l(p.mu);
         if (!p.open) return DSG_OK;
         DSG_CU(cudaStreamSynchronize(p.st));
-        if (p.exec) cudaGraphExecDestroy(p.exec);
-        p.exec = nullptr;
+        DSG_CU(cudaStreamSynchronize(p.gst));
+        for (auto &e : p.exec) { if (e) cudaGraphExecDestroy(e); e = nullptr; }
         void *bufs[] = {p.ctr, p.seeds, p.noise, p.tabin, p.tab, p.mx, p.act, p.nact, p.raw, p.nraw, p.sites, p.nsites, p.nbuck, p.hot,
-                        p.f1, p.f2, p.f8, p.f4, p.meta1, p.meta2, p.evals, p.cov, p.nzone, p.zfirst, p.zslot, p.zmslot, p.zones, p.zmeta,
+                        p.f1, p.f2, p.f8, p.f4, p.meta1, p.meta2, p.evals, p.cvm, p.nzone, p.zfirst, p.zslot, p.zmslot, p.zones, p.zmeta,
                         p.chunks, p.bits, p.par, p.rid, p.cs, p.khi, p.klo, p.rec, p.zcnt, p.zoff, p.zfill, p.zcomp, p.evu, p.ev, p.nev,
-                        p.sig, p.tries, p.out, p.rows};
+                        p.sidx, p.sig, p.tries, p.out, p.rows};
         for (void *b : bufs) cudaFree(b);
         for (Phase &f : p.ph) { cudaFree(f.ctl); cudaFree(f.st); cudaFree(f.dir); f = Phase{}; }
         p.pool.release();
         cudaFreeHost(p.h_ctr); cudaFreeHost(p.h_gcnt); cudaFreeHost(p.h_out); cudaFreeHost(p.h_rows); cudaFreeHost(p.h_seeds);
-        cudaEventDestroy(p.ev0); cudaEventDestroy(p.ev1);
+        cudaEventDestroy(p.ev_start); cudaEventDestroy(p.ev_end);
+        for (int L = 0; L < 2; L++) { cudaEventDestroy(p.ev_gate[L]); cudaEventDestroy(p.ev_done[L]); }
+        cudaStreamDestroy(p.gst);
+        for (auto &ln : p.lane) { gate::lane_destroy(ln); ln = nullptr; }
         cudaFree(p.d_ts); cudaFreeHost(p.h_ts);
         cudaStreamDestroy(p.st); cudaStreamDestroy(p.body_st);
         p.open = false;
