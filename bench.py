@@ -529,7 +529,8 @@ def run_ours(args):
     extra_tot = rep.reduce(tot[4:7], "SUM")
     if args.profile_run:
         if rank == 0:
-            print(json.dumps({"profile_run": True, "ms": ms_max, "counts": [int(x) for x in summed]}))
+            print(json.dumps({"profile_run": True, "ms": ms_max, "counts": [int(x) for x in summed], "last_wave": dsgpu.search_last_wave(),
+                              "stages_ms": stages}))
         dsgpu.search_close()
         return
     sm_mhz = clocks.get("sm_mhz") or 1965.0
@@ -556,6 +557,7 @@ def run_ours(args):
                 "how": "wall clock of the dsg_search_run calls (C ABI) with the seed records and CSV rows copied to host memory"},
         "gpu_launches": int(tot[9]),
         "stages_ms": stages,
+        "last_wave": dsgpu.search_last_wave(),
         "clocks": clocks,
     }
     if world == 1:

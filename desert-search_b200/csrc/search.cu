@@ -71,7 +71,7 @@ enum : uint32_t { F_GATE = 1, F_RAW = 2, F_HASH = 4, F_ZONES = 8, F_CELLS = 16, 
 enum { C_NS = 0, C_NREQ = 1 /* 4 flood phases */, C_ZONES = 5, C_CHUNKS = 6, C_ROWS = 7, C_FLAGS = 8, C_NHOT = 9, C_NBIG = 10, C_SITES = 11,
        C_ROUND = 16 /* 9 round counters */, C_TAKEN = 25, C_FERR = 26, C_BASE = 27, C_LOOPS = 28, C_ITERS = 29, C_PROXY = 32 /* 4 */,
        C_KEPT = 33, C_MAXZ = 36 /* most big zones of a seed */, C_CELLS = 37 /* proxy cells (saturating) */, C_MAXEV = 38 /* most evaluations of a
-       seed */, C_N = 48 };
+       seed */, C_PHEV = 40 /* 4: sub-blocks evaluated per flood phase */, C_PHIT = 44 /* 4: loop iterations per flood phase */, C_N = 48 };
 constexpr int BODY_KERNELS = 13;             // kernels of one flood-loop iteration: 6 rounds of eval + connect, the loop control
 
 struct Params {
@@ -207,8 +207,41 @@ __global__ void __launch_bounds__(NMS_THREADS) k_nms(const dsg_cand *__restrict_
         sv[k] = rc[bidx[slot]].s;
         first[k] = bidx[slot];                     // position k (first-seen order) -> raw index
     }
-    // std::sort(cand, score descending) over the buckets in first-seen order
-    if (threadIdx.x == 0) dsg::stl::sort(order, int64_t(m), [&](uint16_t a, uint16_t b) { return sv[a] > sv[b]; });
+    __syncthreads();
+    // std::sort(cand, score descending) over the buckets in first-seen order.  Without equal scores the sorted
+    // order is unique, so a bitonic sort of (score descending, position) gives std::sort's order; with equal
+    // scores std::sort's own algorithm decides their order.
+    for (uint32_t k = threadIdx.x; k < p2; k += blockDim.x) {
+        const float v = k < m ? sv[k] : 0.0f;
+        if (v != v) s_flag = 2;                    // NaN: no strict order, std::sort's algorithm decides
+        best[k] = k < m ? (uint64_t(~float_order(v == 0.0f ? 0.0f : v)) << 32) | k : ~0ull;   // -0 = +0, a tie
+    }
+    __syncthreads();
+    for (uint32_t size = 2; size <= p2; size <<= 1)
+        for (uint32_t stride = size >> 1; stride > 0; stride >>= 1) {
+            for (uint32_t i = threadIdx.x; i < p2 / 2; i += blockDim.x) {
+                const uint32_t lo = 2 * i - (i & (stride - 1)), hi = lo + stride;
+                const bool up = (lo & size) == 0;
+                const unsigned long long a = best[lo], b = best[hi];
+                if ((a > b) == up) { best[lo] = b; best[hi] = a; }
+            }
+            __syncthreads();
+        }
+    for (uint32_t k = 1 + threadIdx.x; k < m; k += blockDim.x)
+        if ((best[k] >> 32) == (best[k - 1] >> 32)) s_flag = 2;
+    __syncthreads();
+    if (s_flag) {
+        if (threadIdx.x == 0) dsg::stl::sort(order, int64_t(m), [&](uint16_t a, uint16_t b) { return sv[a] > sv[b]; });
+    } else {
+        for (uint32_t k = threadIdx.x; k < m; k += blockDim.x) order[k] = uint16_t(best[k]);
+    }
+    __syncthreads();
+    // the sorted buckets' positions, staged for the walk (the hash keys are no longer needed)
+    int2 *pos = reinterpret_cast<int2 *>(key);
+    for (uint32_t k = threadIdx.x; k < m; k += blockDim.x) {
+        const dsg_cand c = rc[first[order[k]]];
+        pos[k] = make_int2(c.x, c.z);
+    }
     __syncthreads();
     // greedy suppression: warp 0 walks the sorted buckets, the lanes test the kept sites
     if (threadIdx.x < 32) {
@@ -216,14 +249,15 @@ __global__ void __launch_bounds__(NMS_THREADS) k_nms(const dsg_cand *__restrict_
         uint32_t kept = 0;
         const int nms = P.nms;
         for (uint32_t k = 0; k < m && int(kept) < P.max_sites; k++) {
-            const dsg_cand c = rc[first[order[k]]];
+            const int2 c = pos[k];
             bool near = false;
-            for (uint32_t q = lane; q < kept; q += 32) near |= abs(kx[q] - c.x) < nms && abs(kz[q] - c.z) < nms;
+            for (uint32_t q = lane; q < kept; q += 32) near |= abs(kx[q] - c.x) < nms && abs(kz[q] - c.y) < nms;
             near = __any_sync(0xffffffffu, near);
             if (!near) {
                 if (lane == 0) {
-                    kx[kept] = c.x; kz[kept] = c.z;
-                    sites[size_t(s) * MS + kept] = {c.s, c.t, c.c, c.e, c.x, c.z};
+                    kx[kept] = c.x; kz[kept] = c.y;
+                    const dsg_cand d = rc[first[order[k]]];
+                    sites[size_t(s) * MS + kept] = {d.s, d.t, d.c, d.e, d.x, d.z};
                 }
                 kept++;
                 __syncwarp();
@@ -311,8 +345,10 @@ __global__ void k_dir_fill(int32_t *__restrict__ dir, const uint32_t *nreq, uint
 }
 // Phase start: round counters cleared, the loop entered only if there are requests.
 // (in_graph = false: launched on a stream, where there is no handle to set; the host drives the loop)
-__global__ void k_phase_begin(uint32_t *ctr, const uint32_t *nreq, cudaGraphConditionalHandle h, bool in_graph) {
+__global__ void k_phase_begin(uint32_t *ctr, const uint32_t *nreq, cudaGraphConditionalHandle h, bool in_graph, int phase,
+                              const unsigned long long *evals) {
     for (int k = 0; k < 9; k++) ctr[C_ROUND + k] = 0;
+    ctr[C_PHEV + phase] = uint32_t(*evals);              // the phase's sub-block count is taken against this at its end
     if (in_graph) cudaGraphSetConditional(h, *nreq > 0 ? 1u : 0u);
 }
 // Start of every request: statistics reset, start tile claimed, start sub-block queued for round *base.
@@ -338,7 +374,9 @@ __global__ void k_loop_ctl(uint32_t *ctr, cudaGraphConditionalHandle h, bool in_
     if (more && it >= LOOP_LIMIT) ctr[C_FLAGS] |= F_LOOP;
     if (in_graph) cudaGraphSetConditional(h, more && it < LOOP_LIMIT ? 1u : 0u);
 }
-__global__ void k_phase_end(uint32_t *ctr) {
+__global__ void k_phase_end(uint32_t *ctr, int phase, const unsigned long long *evals) {
+    ctr[C_PHEV + phase] = uint32_t(*evals) - ctr[C_PHEV + phase];
+    ctr[C_PHIT + phase] = ctr[C_LOOPS];
     ctr[C_LOOPS] = 0;
     if (ctr[C_FERR]) ctr[C_FLAGS] |= F_POOL;
 }
@@ -533,66 +571,100 @@ __global__ void k_comp_scatter(const dsg_component *__restrict__ rec, const uint
         zcomp[zoff[z] + atomicAdd(&zfill[z], 1u)] = k;
     }
 }
-// Thread per seed: components of its zones in (zone, first cell) order, each new one (by its smallest column and
+// Block per zone: its components (scattered in any order) put in first-cell order, the order in which the
+// reference's raster scan meets them.  First cells are unique within a zone, so a component's position is the
+// number of the zone's components with a smaller first cell.
+__global__ void __launch_bounds__(256) k_comp_order(const dsg_component *__restrict__ rec, const uint32_t *ctr, const uint32_t *__restrict__ zoff,
+                                                    const uint32_t *__restrict__ zin, uint32_t *__restrict__ zout) {
+    __shared__ int32_t f[1024];
+    const uint32_t nz = ctr[C_ZONES];
+    for (uint32_t z = blockIdx.x; z < nz; z += gridDim.x) {
+        const uint32_t o = zoff[z], nc = zoff[z + 1] - o;
+        for (uint32_t i0 = 0; i0 < nc; i0 += blockDim.x) {
+            const uint32_t i = i0 + threadIdx.x;
+            const int32_t mine = i < nc ? rec[zin[o + i]].first : 0;
+            uint32_t rank = 0;
+            for (uint32_t j0 = 0; j0 < nc; j0 += 1024) {
+                const uint32_t m = min(1024u, nc - j0);
+                __syncthreads();
+                for (uint32_t j = threadIdx.x; j < m; j += blockDim.x) f[j] = rec[zin[o + j0 + j]].first;
+                __syncthreads();
+                if (i < nc)
+                    for (uint32_t j = 0; j < m; j++) rank += f[j] < mine;
+            }
+            if (i < nc) zout[o + rank] = zin[o + i];
+        }
+    }
+}
+// Warp per seed: components of its zones in (zone, first cell) order, each new one (by its smallest column and
 // row) an evaluation whose start is the interior cell nearest the centroid (alternatives at ranks n/3, 2n/3);
-// evaluations sorted by proxy size with std::sort's algorithm; exact-flood starts of the first exact_n.
-__global__ void __launch_bounds__(256) k_evals(const uint32_t *__restrict__ zfirst, const DZone *__restrict__ zones,
-                                               const ZoneMeta *__restrict__ zmeta, const uint32_t *__restrict__ zoff, uint32_t *__restrict__ zcomp,
-                                               const dsg_component *__restrict__ rec, Params P, Eval *__restrict__ evu, Eval *__restrict__ ev,
-                                               uint32_t *__restrict__ nev, int64_t *__restrict__ sig, uint16_t *__restrict__ sidx,
-                                               Try *__restrict__ tries, uint32_t *ctr) {
-    const int lane = threadIdx.x & 31;
-    const uint32_t s = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+// evaluations sorted by proxy size with std::sort's algorithm; exact-flood starts of the first exact_n.  The
+// lanes load 32 components at a time; the signatures seen and the sort keys live in shared memory.
+constexpr int EV_WARPS = 4;
+constexpr size_t EV_SMEM = size_t(EV_WARPS) * EVC * (8 + 4 + 2);
+__global__ void __launch_bounds__(EV_WARPS * 32) k_evals(const uint32_t *__restrict__ zfirst, const DZone *__restrict__ zones,
+                                                         const ZoneMeta *__restrict__ zmeta, const uint32_t *__restrict__ zoff,
+                                                         const uint32_t *__restrict__ zcomp, const dsg_component *__restrict__ rec, Params P,
+                                                         Eval *__restrict__ evu, Eval *__restrict__ ev, uint32_t *__restrict__ nev,
+                                                         Try *__restrict__ tries, uint32_t *ctr) {
+    extern __shared__ __align__(16) unsigned char ev_smem[];
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    int64_t *seen = reinterpret_cast<int64_t *>(ev_smem) + size_t(w) * EVC;
+    uint32_t *cellk = reinterpret_cast<uint32_t *>(ev_smem + size_t(EV_WARPS) * EVC * 8) + size_t(w) * EVC;
+    uint16_t *idx = reinterpret_cast<uint16_t *>(ev_smem + size_t(EV_WARPS) * EVC * 12) + size_t(w) * EVC;
+    const uint32_t s = blockIdx.x * EV_WARPS + w;
     if (s >= ctr[C_NS]) return;
     Eval *U = evu + size_t(s) * EVC, *E = ev + size_t(s) * EVC;
-    int64_t *seen = sig + size_t(s) * EVC;
-    uint16_t *idx = sidx + size_t(s) * EVC;
     uint32_t ne = 0;                                     // evaluations so far (= signatures seen), uniform across the warp
     bool full = false;
     const uint32_t nzw = ctr[C_ZONES];
     for (uint32_t zi = zfirst[s]; zi < zfirst[s + 1] && zi < nzw; zi++) {
         const DZone z = zones[zi];
         const ZoneMeta m = zmeta[zi];
-        uint32_t *L = zcomp + zoff[zi];
+        const uint32_t *L = zcomp + zoff[zi];
         const uint32_t nc = zoff[zi + 1] - zoff[zi];
-        if (lane == 0)
-            for (uint32_t i = 1; i < nc; i++) {             // by first cell (unique within a zone)
-                const uint32_t v = L[i];
-                int32_t j = int32_t(i) - 1;
-                while (j >= 0 && rec[L[j]].first > rec[v].first) { L[j + 1] = L[j]; j--; }
-                L[j + 1] = v;
+        for (uint32_t i0 = 0; i0 < nc; i0 += 32) {
+            dsg_component c{};
+            int elig = 0;
+            int64_t sg = 0;
+            if (i0 + lane < nc) {
+                c = rec[L[i0 + lane]];
+                elig = c.cells * 32.0 * 32 * 16 / 1e6 >= 1;
+                sg = (int64_t(z.x0 + c.minx * 32) << 32) | uint32_t(z.z0 + c.minz * 32);
             }
-        __syncwarp();
-        for (uint32_t i = 0; i < nc; i++) {
-            const dsg_component c = rec[__ldcg(L + i)];
-            const double area = c.cells * 32.0 * 32 * 16 / 1e6;
-            if (area < 1) continue;
-            const int64_t sg = (int64_t(z.x0 + c.minx * 32) << 32) | uint32_t(z.z0 + c.minz * 32);
-            bool dup = false;
-            for (uint32_t k = lane; k < ne; k += 32) dup |= __ldcg(seen + k) == sg;
-            if (__any_sync(0xffffffffu, dup)) continue;
-            if (ne == EVC) { full = true; continue; }
-            if (lane == 0) {
-                __stcg(seen + ne, sg);
-                const int32_t cell = c.inner ? c.pick[0] : c.first;
-                Eval e{};
-                e.rank = m.rank; e.x = z.x0 + (cell % z.nx) * 32; e.z = z.z0 + (cell / z.nx) * 32;
-                e.proxy = area; e.s8 = -1; e.s4 = 0; e.hot = m.hot;
-                e.nalt = c.inner ? 2 : 0;
-                for (int a = 0; a < e.nalt; a++) { e.ax[a] = z.x0 + (c.pick[a + 1] % z.nx) * 32; e.az[a] = z.z0 + (c.pick[a + 1] / z.nx) * 32; }
-                U[ne] = e;
+            const uint32_t cnt = min(32u, nc - i0);
+            for (uint32_t j = 0; j < cnt; j++) {
+                if (!__shfl_sync(0xffffffffu, elig, j)) continue;
+                const int64_t sj = __shfl_sync(0xffffffffu, sg, j);
+                bool dup = false;
+                for (uint32_t k = lane; k < ne; k += 32) dup |= seen[k] == sj;
+                if (__any_sync(0xffffffffu, dup)) continue;
+                if (ne == EVC) { full = true; continue; }
+                if (uint32_t(lane) == j) {                   // the component's own lane writes its evaluation
+                    seen[ne] = sj;
+                    cellk[ne] = c.cells;
+                    const int32_t cell = c.inner ? c.pick[0] : c.first;
+                    Eval e{};
+                    e.rank = m.rank; e.x = z.x0 + (cell % z.nx) * 32; e.z = z.z0 + (cell / z.nx) * 32;
+                    e.proxy = c.cells * 32.0 * 32 * 16 / 1e6; e.s8 = -1; e.s4 = 0; e.hot = m.hot;
+                    e.nalt = c.inner ? 2 : 0;
+                    for (int a = 0; a < e.nalt; a++) { e.ax[a] = z.x0 + (c.pick[a + 1] % z.nx) * 32; e.az[a] = z.z0 + (c.pick[a + 1] / z.nx) * 32; }
+                    U[ne] = e;
+                }
+                ne++;
+                __syncwarp();
             }
-            ne++;
-            __syncwarp();
         }
     }
     if (lane == 0) {
         if (full) atomicOr(ctr + C_FLAGS, F_EVALS);
         atomicMax(ctr + C_MAXEV, ne + (full ? 1 : 0));
         if (s == 0 && ctr[C_PROXY + 3]) atomicOr(ctr + C_FLAGS, F_LABEL);
-        // std::sort(ev, proxy descending): the permutation from the sort, then the records copied out in its order
+        // std::sort(ev, proxy descending): the permutation from the sort, then the records copied out in its order.
+        // The proxy is cells x 16384 / 10^6, strictly increasing in cells, so comparing cells gives the same
+        // comparison results and hence the same permutation.
         for (uint32_t k = 0; k < ne; k++) idx[k] = uint16_t(k);
-        dsg::stl::sort(idx, int64_t(ne), [&](uint16_t a, uint16_t b) { return U[a].proxy > U[b].proxy; });
+        dsg::stl::sort(idx, int64_t(ne), [&](uint16_t a, uint16_t b) { return cellk[a] > cellk[b]; });
         nev[s] = ne;
     }
     __syncwarp();
@@ -743,6 +815,38 @@ struct Caps {
     }
 };
 
+// One wave in flight: its streams, gate lane, device buffers (about 20 GB at 1,024 seeds), graph, stage stamps and
+// pinned host copies.  Consecutive waves alternate between two slots that run concurrently, so the
+// latency-bound flood rounds of one wave overlap the throughput-bound stages of the other (gate, tables, proxy).
+struct Slot {
+    cudaStream_t st = nullptr, body_st = nullptr;
+    gate::Lane *lane = nullptr;
+    uint32_t *ctr = nullptr;
+    uint64_t *seeds = nullptr; SeedNoise *noise = nullptr;
+    void *tabin = nullptr; float *tab = nullptr, *mx = nullptr; int32_t *act = nullptr; uint32_t *nact = nullptr;
+    dsg_cand *raw = nullptr; uint32_t *nraw = nullptr;
+    Site *sites = nullptr; uint32_t *nsites = nullptr, *nbuck = nullptr; Hot *hot = nullptr;
+    int32_t *f1 = nullptr, *f2 = nullptr, *f8 = nullptr, *f4 = nullptr;
+    uint32_t *meta1 = nullptr, *meta2 = nullptr;
+    Phase ph[4]{};                               // pre-floods, step 128, step 8, step 4
+    TilePool pool;
+    unsigned long long *evals = nullptr;
+    uint32_t *cvm = nullptr, *nzone = nullptr, *zfirst = nullptr;
+    DZone *zslot = nullptr, *zones = nullptr; ZoneMeta *zmslot = nullptr, *zmeta = nullptr; uint2 *chunks = nullptr;
+    uint8_t *bits = nullptr; int32_t *par = nullptr, *rid = nullptr; zones::CompStat *cs = nullptr; uint64_t *khi = nullptr; uint32_t *klo = nullptr;
+    dsg_component *rec = nullptr; uint32_t *zcnt = nullptr, *zoff = nullptr, *zfill = nullptr, *zcomp = nullptr, *zcomp2 = nullptr;
+    Eval *evu = nullptr, *ev = nullptr; uint32_t *nev = nullptr; Try *tries = nullptr;
+    dsg_search_seed *out = nullptr; dsg_search_row *rows = nullptr;
+    cudaGraphExec_t exec = nullptr;
+    cudaEvent_t ev_done = nullptr;
+    unsigned long long *d_ts = nullptr, *h_ts = nullptr;   // [0] gate start, [1..8] graph stages, [9] gate end (global timer, ns)
+    // pinned host copies
+    uint32_t *h_ctr = nullptr, *h_gcnt = nullptr; dsg_search_seed *h_out = nullptr; dsg_search_row *h_rows = nullptr; uint64_t *h_seeds = nullptr;
+    // the wave in flight
+    uint64_t indices = 0;
+    bool gated = false;
+};
+
 struct Pipeline {
     std::mutex mu;
     bool open = false;
@@ -751,74 +855,52 @@ struct Pipeline {
     dsg_gate_cfg gcfg{};
     uint64_t wave = 0;
     uint32_t min_cells = 1;
-    cudaStream_t st = nullptr, body_st = nullptr;
-    gate::Lane *lane[2] = {nullptr, nullptr};    // two gate lanes: the gate of wave k + 1 runs while wave k's graph does
-    cudaStream_t gst = nullptr;                  // the gates' stream (low priority)
-    cudaEvent_t ev_gate[2] = {}, ev_done[2] = {}, ev_start = nullptr, ev_end = nullptr;
-    uint32_t gcaps[3] = {0, 0, 0};
-    // device buffers
-    uint32_t *ctr = nullptr;
-    uint64_t *seeds = nullptr; SeedNoise *noise = nullptr;
-    void *tabin = nullptr; float *tab = nullptr, *mx = nullptr; int32_t *act = nullptr; uint32_t *nact = nullptr;
-    dsg_cand *raw = nullptr; uint32_t *nraw = nullptr;
-    Site *sites = nullptr; uint32_t *nsites = nullptr, *nbuck = nullptr; Hot *hot = nullptr;
-    int32_t *f1 = nullptr, *f2 = nullptr, *f8 = nullptr, *f4 = nullptr;
-    uint32_t *meta1 = nullptr, *meta2 = nullptr;
-    Phase ph[4]{};
-    TilePool pool;
-    unsigned long long *evals = nullptr;
-    uint32_t *cvm = nullptr, *nzone = nullptr, *zfirst = nullptr;
-    DZone *zslot = nullptr, *zones = nullptr; ZoneMeta *zmslot = nullptr, *zmeta = nullptr; uint2 *chunks = nullptr;
-    uint8_t *bits = nullptr; int32_t *par = nullptr, *rid = nullptr; zones::CompStat *cs = nullptr; uint64_t *khi = nullptr; uint32_t *klo = nullptr;
-    dsg_component *rec = nullptr; uint32_t *zcnt = nullptr, *zoff = nullptr, *zfill = nullptr, *zcomp = nullptr;
-    Eval *evu = nullptr, *ev = nullptr; uint32_t *nev = nullptr; uint16_t *sidx = nullptr; int64_t *sig = nullptr; Try *tries = nullptr;
-    dsg_search_seed *out = nullptr; dsg_search_row *rows = nullptr;
     int grid_eval = 0, grid_conn = 0;
-    cudaGraphExec_t exec[2] = {nullptr, nullptr};   // one graph per gate lane (the lane's buffers are baked in)
     bool eager = false;                          // no graph: every wave launches the stages on the stream (for profilers)
     uint32_t graph_kernels = 0;                  // kernel nodes of the wave graph outside the loop bodies
+    static constexpr int NSLOT = 2;
+    int nslot = NSLOT;                           // 1 in eager mode (its flood loops synchronise with the host)
+    Slot sl[NSLOT];
+    cudaEvent_t ev_start = nullptr, ev_end = nullptr;
     static constexpr int NSTAGE = 8;             // gate | tables+scan | suppression+hot points | pre-floods | step-128 floods+coverage |
     double stage_ms[NSTAGE] = {};                // proxy+components+exact starts | step-8 floods | step-4 floods+results
-    unsigned long long *d_ts = nullptr, *h_ts = nullptr;   // stage boundary stamps per lane: [0] gate start, [1..8] graph stages,
-                                                           // [9] gate end (device global timer, ns)
-    // pinned host copies
-    uint32_t *h_ctr = nullptr, *h_gcnt = nullptr; dsg_search_seed *h_out = nullptr; dsg_search_row *h_rows = nullptr; uint64_t *h_seeds = nullptr;
+    uint32_t last_ctr[C_N] = {};                 // counters of the last wave collected
 };
 Pipeline &PL() { static Pipeline p; return p; }
 
-// One flood phase into the graph being captured on p.st: directory, round counters, request starts, the round
-// loop as a conditional WHILE node (body: 6 rounds and the loop control, captured on p.body_st), statistics.
-void capture_phase(Pipeline &p, int k) {
-    Phase &f = p.ph[k];
-    uint32_t *nreq = p.ctr + C_NREQ + k;
-    const TileAlloc ta{nullptr, 0, p.pool.cap, p.pool.cap, p.ctr + C_TAKEN, nullptr, nullptr};
-    k_dir_fill<<<4 * 148, 256, 0, p.st>>>(f.dir, nreq, f.per_req);
+// One flood phase into the graph being captured on S.st: directory, round counters, request starts, the round
+// loop as a conditional WHILE node (body: 6 rounds and the loop control, captured on S.body_st), statistics.
+void capture_phase(Pipeline &p, Slot &S, int k) {
+    Phase &f = S.ph[k];
+    uint32_t *nreq = S.ctr + C_NREQ + k;
+    const TileAlloc ta{nullptr, 0, S.pool.cap, S.pool.cap, S.ctr + C_TAKEN, nullptr, nullptr};
+    k_dir_fill<<<4 * 148, 256, 0, S.st>>>(f.dir, nreq, f.per_req);
     if (p.eager) {
         // the same kernels launched on the stream, the loop driven by the host after every 6 rounds
-        k_phase_begin<<<1, 1, 0, p.st>>>(p.ctr, nreq, 0, false);
-        k_req_start<<<64, 128, 0, p.st>>>(f.ctl, nreq, f.st, f.dir, p.pool.T, ta, p.pool.n_list[0], p.ctr);
+        k_phase_begin<<<1, 1, 0, S.st>>>(S.ctr, nreq, 0, false, k, S.evals);
+        k_req_start<<<64, 128, 0, S.st>>>(f.ctl, nreq, f.st, f.dir, S.pool.T, ta, S.pool.n_list[0], S.ctr);
         for (uint32_t it = 0; it < LOOP_LIMIT; it++) {
             for (uint32_t r = 0; r < 6; r++)
-                launch_round(p.pool, r, p.ctr + C_ROUND, nullptr, p.ctr + C_FERR, p.evals, f.ctl, p.noise, f.dir, f.st, ta, p.grid_eval, p.grid_conn,
-                             p.st, p.ctr + C_BASE);
-            k_loop_ctl<<<1, 1, 0, p.st>>>(p.ctr, 0, false);
+                launch_round(S.pool, r, S.ctr + C_ROUND, nullptr, S.ctr + C_FERR, S.evals, f.ctl, S.noise, f.dir, f.st, ta, p.grid_eval, p.grid_conn,
+                             S.st, S.ctr + C_BASE);
+            k_loop_ctl<<<1, 1, 0, S.st>>>(S.ctr, 0, false);
             DSG_CU(cudaGetLastError());
-            DSG_CU(cudaMemcpyAsync(p.h_ctr, p.ctr, C_N * 4, cudaMemcpyDeviceToHost, p.st));
-            DSG_CU(cudaStreamSynchronize(p.st));
-            if (p.h_ctr[C_ROUND + 0] == 0 && p.h_ctr[C_ROUND + 3] == 0) break;
+            DSG_CU(cudaMemcpyAsync(S.h_ctr, S.ctr, C_N * 4, cudaMemcpyDeviceToHost, S.st));
+            DSG_CU(cudaStreamSynchronize(S.st));
+            if (S.h_ctr[C_ROUND + 0] == 0 && S.h_ctr[C_ROUND + 3] == 0) break;
         }
     } else {
         cudaStreamCaptureStatus cs;
         cudaGraph_t g;
         const cudaGraphNode_t *deps = nullptr;
         size_t ndeps = 0;
-        DSG_CU(cudaStreamGetCaptureInfo(p.st, &cs, nullptr, &g, &deps, &ndeps));
+        DSG_CU(cudaStreamGetCaptureInfo(S.st, &cs, nullptr, &g, &deps, &ndeps));
         cudaGraphConditionalHandle h;
         DSG_CU(cudaGraphConditionalHandleCreate(&h, g, 0, cudaGraphCondAssignDefault));
-        k_phase_begin<<<1, 1, 0, p.st>>>(p.ctr, nreq, h, true);
-        k_req_start<<<64, 128, 0, p.st>>>(f.ctl, nreq, f.st, f.dir, p.pool.T, ta, p.pool.n_list[0], p.ctr);
+        k_phase_begin<<<1, 1, 0, S.st>>>(S.ctr, nreq, h, true, k, S.evals);
+        k_req_start<<<64, 128, 0, S.st>>>(f.ctl, nreq, f.st, f.dir, S.pool.T, ta, S.pool.n_list[0], S.ctr);
         DSG_CU(cudaGetLastError());
-        DSG_CU(cudaStreamGetCaptureInfo(p.st, &cs, nullptr, &g, &deps, &ndeps));
+        DSG_CU(cudaStreamGetCaptureInfo(S.st, &cs, nullptr, &g, &deps, &ndeps));
         cudaGraphNodeParams np{};
         np.type = cudaGraphNodeTypeConditional;
         np.conditional.handle = h;
@@ -827,83 +909,89 @@ void capture_phase(Pipeline &p, int k) {
         cudaGraphNode_t node;
         DSG_CU(cudaGraphAddNode(&node, g, deps, ndeps, &np));
         cudaGraph_t body = np.conditional.phGraph_out[0];
-        DSG_CU(cudaStreamUpdateCaptureDependencies(p.st, &node, 1, cudaStreamSetCaptureDependencies));
-        DSG_CU(cudaStreamBeginCaptureToGraph(p.body_st, body, nullptr, nullptr, 0, cudaStreamCaptureModeRelaxed));
+        DSG_CU(cudaStreamUpdateCaptureDependencies(S.st, &node, 1, cudaStreamSetCaptureDependencies));
+        DSG_CU(cudaStreamBeginCaptureToGraph(S.body_st, body, nullptr, nullptr, 0, cudaStreamCaptureModeRelaxed));
         for (uint32_t r = 0; r < 6; r++)
-            launch_round(p.pool, r, p.ctr + C_ROUND, nullptr, p.ctr + C_FERR, p.evals, f.ctl, p.noise, f.dir, f.st, ta, p.grid_eval, p.grid_conn,
-                         p.body_st, p.ctr + C_BASE);
-        k_loop_ctl<<<1, 1, 0, p.body_st>>>(p.ctr, h, true);
+            launch_round(S.pool, r, S.ctr + C_ROUND, nullptr, S.ctr + C_FERR, S.evals, f.ctl, S.noise, f.dir, f.st, ta, p.grid_eval, p.grid_conn,
+                         S.body_st, S.ctr + C_BASE);
+        k_loop_ctl<<<1, 1, 0, S.body_st>>>(S.ctr, h, true);
         DSG_CU(cudaGetLastError());
         cudaGraph_t body_out = nullptr;
-        DSG_CU(cudaStreamEndCapture(p.body_st, &body_out));
+        DSG_CU(cudaStreamEndCapture(S.body_st, &body_out));
     }
-    k_tile_finish<<<dim3(f.cap, dir_chunks(f.per_req)), 256, 0, p.st>>>(f.ctl, nullptr, f.dir, p.pool.T, f.st, nreq);
-    k_phase_end<<<1, 1, 0, p.st>>>(p.ctr);
+    k_tile_finish<<<dim3(f.cap, dir_chunks(f.per_req)), 256, 0, S.st>>>(f.ctl, nullptr, f.dir, S.pool.T, f.st, nreq);
+    k_phase_end<<<1, 1, 0, S.st>>>(S.ctr, k, S.evals);
     DSG_CU(cudaGetLastError());
 }
 
 // Everything of a wave after the gate, as one graph.
 // In eager mode (profiling) the same sequence is launched on the stream for every wave instead.
-void capture_wave(Pipeline &p, int L) {
-    if (!p.eager) DSG_CU(cudaStreamBeginCapture(p.st, cudaStreamCaptureModeRelaxed));
+void capture_wave(Pipeline &p, Slot &S) {
+    if (!p.eager) DSG_CU(cudaStreamBeginCapture(S.st, cudaStreamCaptureModeRelaxed));
     uint32_t caps[3];
-    gate::lane_caps(p.lane[L], caps);
-    unsigned long long *ts = p.d_ts + 16 * L;
-    k_stamp<<<1, 1, 0, p.st>>>(ts, 1);
+    gate::lane_caps(S.lane, caps);
+    unsigned long long *ts = S.d_ts;
+    k_stamp<<<1, 1, 0, S.st>>>(ts, 1);
     const uint32_t SC = p.c.sc;
-    k_begin<<<8, 128, 0, p.st>>>(gate::lane_counts(p.lane[L]), caps[0], caps[1], caps[2], SC, gate::lane_survivors(p.lane[L]), p.seeds, p.ctr);
-    seed_noise_build_dev(p.seeds, p.ctr + C_NS, SC, p.noise, p.st);
-    const int table_launches = scan_seeds_device(p.noise, p.ctr + C_NS, SC, p.tabin, p.tab, p.mx, p.act, p.nact, p.raw, p.nraw, RAWCAP, p.P.sp, p.st);
-    k_stamp<<<1, 1, 0, p.st>>>(ts, 2);
+    k_begin<<<8, 128, 0, S.st>>>(gate::lane_counts(S.lane), caps[0], caps[1], caps[2], SC, gate::lane_survivors(S.lane), S.seeds, S.ctr);
+    seed_noise_build_dev(S.seeds, S.ctr + C_NS, SC, S.noise, S.st);
+    const int table_launches = scan_seeds_device(S.noise, S.ctr + C_NS, SC, S.tabin, S.tab, S.mx, S.act, S.nact, S.raw, S.nraw, RAWCAP, p.P.sp, S.st);
+    k_stamp<<<1, 1, 0, S.st>>>(ts, 2);
     DSG_CU(cudaFuncSetAttribute(k_nms, cudaFuncAttributeMaxDynamicSharedMemorySize, int(NMS_SMEM)));
-    k_nms<<<SC, NMS_THREADS, NMS_SMEM, p.st>>>(p.raw, p.nraw, p.P, p.sites, p.nsites, p.nbuck, p.ctr);
-    k_hot<<<4 * 148, 256, 0, p.st>>>(p.noise, p.sites, p.nsites, p.ctr, p.hot);
-    k_req_pre<<<4 * 148, 256, 0, p.st>>>(p.hot, p.nsites, p.ctr, p.ph[0].ctl, p.meta1, p.f1, p.f2);
+    k_nms<<<SC, NMS_THREADS, NMS_SMEM, S.st>>>(S.raw, S.nraw, p.P, S.sites, S.nsites, S.nbuck, S.ctr);
+    k_hot<<<4 * 148, 256, 0, S.st>>>(S.noise, S.sites, S.nsites, S.ctr, S.hot);
+    k_req_pre<<<4 * 148, 256, 0, S.st>>>(S.hot, S.nsites, S.ctr, S.ph[0].ctl, S.meta1, S.f1, S.f2);
     DSG_CU(cudaGetLastError());
-    k_stamp<<<1, 1, 0, p.st>>>(ts, 3);
-    capture_phase(p, 0);
-    k_stamp<<<1, 1, 0, p.st>>>(ts, 4);
-    k_req_128<<<4 * 148, 256, 0, p.st>>>(p.ph[0].st, p.ph[0].ctl, p.meta1, p.P, p.ctr, p.ph[1].ctl, p.meta2, p.f2);
-    capture_phase(p, 1);
-    k_cover_pairs<<<8 * 148, 256, 0, p.st>>>(p.hot, p.nsites, p.f1, p.f2, FloodView{p.ph[0].ctl, p.ph[0].dir}, FloodView{p.ph[1].ctl, p.ph[1].dir},
-                                              p.ph[0].st, p.pool.T, p.P, p.cvm, p.ctr);
-    k_cover<<<(SC + 7) / 8, 256, 0, p.st>>>(p.hot, p.nsites, p.f1, p.f2, p.ph[0].st, p.ph[1].st, p.P, p.cvm, p.nzone, p.zslot, p.zmslot, p.ctr);
-    k_stamp<<<1, 1, 0, p.st>>>(ts, 5);
-    k_zone_list<<<1, LIST_THREADS, 0, p.st>>>(p.nzone, p.zslot, p.zmslot, p.zfirst, p.zones, p.zmeta, p.chunks, p.ctr, p.c.zcap, p.c.cellcap, p.c.chcap);
+    k_stamp<<<1, 1, 0, S.st>>>(ts, 3);
+    capture_phase(p, S, 0);
+    k_stamp<<<1, 1, 0, S.st>>>(ts, 4);
+    k_req_128<<<4 * 148, 256, 0, S.st>>>(S.ph[0].st, S.ph[0].ctl, S.meta1, p.P, S.ctr, S.ph[1].ctl, S.meta2, S.f2);
+    capture_phase(p, S, 1);
+    k_cover_pairs<<<8 * 148, 256, 0, S.st>>>(S.hot, S.nsites, S.f1, S.f2, FloodView{S.ph[0].ctl, S.ph[0].dir}, FloodView{S.ph[1].ctl, S.ph[1].dir},
+                                              S.ph[0].st, S.pool.T, p.P, S.cvm, S.ctr);
+    k_cover<<<(SC + 7) / 8, 256, 0, S.st>>>(S.hot, S.nsites, S.f1, S.f2, S.ph[0].st, S.ph[1].st, p.P, S.cvm, S.nzone, S.zslot, S.zmslot, S.ctr);
+    k_stamp<<<1, 1, 0, S.st>>>(ts, 5);
+    k_zone_list<<<1, LIST_THREADS, 0, S.st>>>(S.nzone, S.zslot, S.zmslot, S.zfirst, S.zones, S.zmeta, S.chunks, S.ctr, p.c.zcap, p.c.cellcap, p.c.chcap);
     DSG_CU(cudaGetLastError());
-    proxy_components_device(p.noise, p.zones, zones::ZoneWork{p.chunks, p.ctr + C_CHUNKS}, 8 * 148, p.bits, p.par, p.rid, p.cs, p.khi, p.klo,
-                            p.rec, p.ctr + C_PROXY, p.min_cells, p.c.compcap, p.st);
-    DSG_CU(cudaMemsetAsync(p.zcnt, 0, size_t(p.c.zcap + 1) * 4, p.st));
-    DSG_CU(cudaMemsetAsync(p.zfill, 0, size_t(p.c.zcap + 1) * 4, p.st));
-    k_comp_count<<<64, 256, 0, p.st>>>(p.rec, p.ctr, p.zcnt);
-    k_comp_offsets<<<1, LIST_THREADS, 0, p.st>>>(p.zcnt, p.zoff, p.ctr);
-    k_comp_scatter<<<64, 256, 0, p.st>>>(p.rec, p.ctr, p.zoff, p.zfill, p.zcomp);
-    k_evals<<<(SC + 7) / 8, 256, 0, p.st>>>(p.zfirst, p.zones, p.zmeta, p.zoff, p.zcomp, p.rec, p.P, p.evu, p.ev, p.nev, p.sig, p.sidx, p.tries,
-                                             p.ctr);
-    k_ring<<<8 * 148, 128, 0, p.st>>>(p.noise, world_dev(), p.tries, p.ctr);
-    k_req_8<<<32, 256, 0, p.st>>>(p.tries, p.ctr, p.ph[2].ctl, p.f8);
+    proxy_components_device(S.noise, S.zones, zones::ZoneWork{S.chunks, S.ctr + C_CHUNKS}, 8 * 148, S.bits, S.par, S.rid, S.cs, S.khi, S.klo,
+                            S.rec, S.ctr + C_PROXY, p.min_cells, p.c.compcap, S.st);
+    DSG_CU(cudaMemsetAsync(S.zcnt, 0, size_t(p.c.zcap + 1) * 4, S.st));
+    DSG_CU(cudaMemsetAsync(S.zfill, 0, size_t(p.c.zcap + 1) * 4, S.st));
+    k_comp_count<<<64, 256, 0, S.st>>>(S.rec, S.ctr, S.zcnt);
+    k_comp_offsets<<<1, LIST_THREADS, 0, S.st>>>(S.zcnt, S.zoff, S.ctr);
+    k_comp_scatter<<<64, 256, 0, S.st>>>(S.rec, S.ctr, S.zoff, S.zfill, S.zcomp2);
+    k_comp_order<<<4 * 148, 256, 0, S.st>>>(S.rec, S.ctr, S.zoff, S.zcomp2, S.zcomp);
+    DSG_CU(cudaFuncSetAttribute(k_evals, cudaFuncAttributeMaxDynamicSharedMemorySize, int(EV_SMEM)));
+    k_evals<<<(SC + EV_WARPS - 1) / EV_WARPS, EV_WARPS * 32, EV_SMEM, S.st>>>(S.zfirst, S.zones, S.zmeta, S.zoff, S.zcomp, S.rec, p.P, S.evu,
+                                                                             S.ev, S.nev, S.tries, S.ctr);
+    k_ring<<<8 * 148, 128, 0, S.st>>>(S.noise, world_dev(), S.tries, S.ctr);
+    // every start of the retry loop flooded at once (a wave has few exact floods, so the sequential loop's
+    // passes would only add rounds); k_retry then replays the loop over their areas
+    k_req_8<<<32, 256, 0, S.st>>>(S.tries, S.ctr, S.ph[2].ctl, S.f8);
     DSG_CU(cudaGetLastError());
-    k_stamp<<<1, 1, 0, p.st>>>(ts, 6);
-    capture_phase(p, 2);
-    k_stamp<<<1, 1, 0, p.st>>>(ts, 7);
-    k_retry<<<16, 256, 0, p.st>>>(p.tries, p.f8, p.ph[2].st, p.ph[2].ctl, p.ev, p.nev, p.P, p.ctr, p.ph[3].ctl, p.f4);
-    capture_phase(p, 3);
-    k_results<<<(SC + 127) / 128, 128, 0, p.st>>>(p.seeds, p.noise, p.mx, p.nbuck, p.nsites, p.sites, p.ev, p.nev, p.f4, p.ph[3].st, p.P, p.out,
-                                                   p.rows, p.ctr);
-    k_pool_zero<<<8 * 148, 256, 0, p.st>>>(p.pool.T, p.ctr, p.pool.cap);
-    k_wave_end<<<1, 1, 0, p.st>>>(p.ctr);
+    k_stamp<<<1, 1, 0, S.st>>>(ts, 6);
+    capture_phase(p, S, 2);
+    k_stamp<<<1, 1, 0, S.st>>>(ts, 7);
+    k_retry<<<16, 256, 0, S.st>>>(S.tries, S.f8, S.ph[2].st, S.ph[2].ctl, S.ev, S.nev, p.P, S.ctr, S.ph[3].ctl, S.f4);
+    capture_phase(p, S, 3);
+    k_results<<<(SC + 127) / 128, 128, 0, S.st>>>(S.seeds, S.noise, S.mx, S.nbuck, S.nsites, S.sites, S.ev, S.nev, S.f4, S.ph[3].st, p.P, S.out,
+                                                   S.rows, S.ctr);
+    k_pool_zero<<<8 * 148, 256, 0, S.st>>>(S.pool.T, S.ctr, S.pool.cap);
+    k_wave_end<<<1, 1, 0, S.st>>>(S.ctr);
     DSG_CU(cudaGetLastError());
-    k_stamp<<<1, 1, 0, p.st>>>(ts, 8);
+    k_stamp<<<1, 1, 0, S.st>>>(ts, 8);
     // kernels outside the loop bodies: 6 set-up/scan kernels and the table launches, 7 for suppression, hot points,
-    // requests, coverage and zones, 9 for the proxy bitmaps and labelling, 10 for components, exact starts, retries,
+    // requests, coverage and zones, 9 for the proxy bitmaps and labelling, 11 for components, exact starts, retries,
     // results and the wave's end, 5 per flood phase, 8 stage stamps
-    p.graph_kernels = 6 + table_launches + 7 + 9 + 10 + 4 * 5 + 8;
+    p.graph_kernels = 6 + table_launches + 7 + 9 + 11 + 4 * 5 + 8;
     if (p.eager) return;
     cudaGraph_t g = nullptr;
-    DSG_CU(cudaStreamEndCapture(p.st, &g));
-    DSG_CU(cudaGraphInstantiate(&p.exec[L], g, 0));
+    DSG_CU(cudaStreamEndCapture(S.st, &g));
+    DSG_CU(cudaGraphInstantiate(&S.exec, g, 0));
     DSG_CU(cudaGraphDestroy(g));
 }
+void slot_allocate(Pipeline &p, Slot &S);
+void slot_release(Slot &S);
 }  // namespace search
 }  // namespace dsg
 
@@ -937,64 +1025,23 @@ extern "C" int dsg_search_open(const dsg_search_params *q) {
                 for (int dx = -r; dx <= r; dx++)
                     if (std::max(std::abs(dx), std::abs(dz)) == r) { ring[n][0] = int8_t(dx); ring[n][1] = int8_t(dz); n++; }
         DSG_CU(cudaMemcpyToSymbol(c_ring, ring, sizeof ring));
-        int lo, hi;
-        DSG_CU(cudaDeviceGetStreamPriorityRange(&lo, &hi));
-        DSG_CU(cudaStreamCreateWithPriority(&p.st, cudaStreamNonBlocking, hi));
-        DSG_CU(cudaStreamCreateWithFlags(&p.body_st, cudaStreamNonBlocking));
-        for (auto &ln : p.lane) ln = gate::lane_create(p.wave);
-        gate::lane_caps(p.lane[0], p.gcaps);
-        DSG_CU(cudaStreamCreateWithPriority(&p.gst, cudaStreamNonBlocking, lo));
-        p.ctr = dalloc<uint32_t>(C_N);
-        DSG_CU(cudaMemset(p.ctr, 0, C_N * 4));
         p.c = Caps(q->seeds_cap ? q->seeds_cap : SC_MAX);
-        const uint32_t SC = p.c.sc;
-        p.seeds = dalloc<uint64_t>(SC); p.noise = dalloc<SeedNoise>(SC);
-        p.tabin = dalloc<char>(size_t(SC) * 6 * tabin_bytes());
-        p.tab = dalloc<float>(size_t(SC) * 6 * 512 * 512); p.mx = dalloc<float>(2 * SC);
-        p.act = dalloc<int32_t>(size_t(SC) * 512 * 512); p.nact = dalloc<uint32_t>(SC);
-        p.raw = dalloc<dsg_cand>(size_t(SC) * RAWCAP); p.nraw = dalloc<uint32_t>(SC);
-        p.sites = dalloc<Site>(size_t(SC) * MS); p.nsites = dalloc<uint32_t>(SC); p.nbuck = dalloc<uint32_t>(SC); p.hot = dalloc<Hot>(size_t(SC) * MS);
-        p.f1 = dalloc<int32_t>(size_t(SC) * MS); p.f2 = dalloc<int32_t>(size_t(SC) * MS);
-        p.meta1 = dalloc<uint32_t>(size_t(SC) * MS); p.meta2 = dalloc<uint32_t>(size_t(SC) * MS);
-        p.f8 = dalloc<int32_t>(p.c.tries); p.f4 = dalloc<int32_t>(SC * EXN);
-        const uint32_t caps[4] = {SC * MS, SC * MS, p.c.tries, SC * EXN};
-        const int steps[4] = {256, 128, 8, 4};
-        for (int k = 0; k < 4; k++) {
-            const int half = (k < 2 ? 32000 : 16000) / steps[k], tpr = (2 * half + 1 + TILE - 1) / TILE;
-            p.ph[k].per_req = uint32_t(tpr * tpr);
-            p.ph[k].cap = caps[k];
-            p.ph[k].ctl = dalloc<FloodCtl>(caps[k]); p.ph[k].st = dalloc<FloodStat>(caps[k]);
-            p.ph[k].dir = dalloc<int32_t>(size_t(caps[k]) * p.ph[k].per_req);
-        }
-        p.pool.allocate(p.c.pool_tiles);
-        p.evals = dalloc<unsigned long long>(1);
-        round_grids(p.grid_eval, p.grid_conn);
-        p.cvm = dalloc<uint32_t>(size_t(SC) * MS * CW); p.nzone = dalloc<uint32_t>(SC); p.zfirst = dalloc<uint32_t>(SC + 1);
-        p.zslot = dalloc<DZone>(size_t(SC) * ZPS); p.zmslot = dalloc<ZoneMeta>(size_t(SC) * ZPS);
-        p.zones = dalloc<DZone>(p.c.zcap); p.zmeta = dalloc<ZoneMeta>(p.c.zcap); p.chunks = dalloc<uint2>(p.c.chcap);
-        p.bits = dalloc<uint8_t>(p.c.cellcap); p.par = dalloc<int32_t>(p.c.cellcap); p.rid = dalloc<int32_t>(p.c.cellcap);
-        p.cs = dalloc<zones::CompStat>(p.c.compcap); p.khi = dalloc<uint64_t>(p.c.cellcap); p.klo = dalloc<uint32_t>(p.c.cellcap);
-        p.rec = dalloc<dsg_component>(p.c.compcap);
-        p.zcnt = dalloc<uint32_t>(p.c.zcap + 1); p.zoff = dalloc<uint32_t>(p.c.zcap + 1); p.zfill = dalloc<uint32_t>(p.c.zcap + 1);
-        p.zcomp = dalloc<uint32_t>(p.c.compcap);
-        p.evu = dalloc<Eval>(size_t(SC) * EVC); p.ev = dalloc<Eval>(size_t(SC) * EVC); p.nev = dalloc<uint32_t>(SC); p.sig = dalloc<int64_t>(size_t(SC) * EVC);
-        p.sidx = dalloc<uint16_t>(size_t(SC) * EVC);
-        p.tries = dalloc<Try>(p.c.tries);
-        p.out = dalloc<dsg_search_seed>(SC); p.rows = dalloc<dsg_search_row>(ROWCAP);
-        DSG_CU(cudaMallocHost(&p.h_ctr, C_N * 4)); DSG_CU(cudaMallocHost(&p.h_gcnt, 16));
-        DSG_CU(cudaMallocHost(&p.h_out, SC * sizeof(dsg_search_seed))); DSG_CU(cudaMallocHost(&p.h_rows, ROWCAP * sizeof(dsg_search_row)));
-        DSG_CU(cudaMallocHost(&p.h_seeds, SC * 8));
-        DSG_CU(cudaEventCreate(&p.ev_start)); DSG_CU(cudaEventCreate(&p.ev_end));
-        for (int L = 0; L < 2; L++) {
-            DSG_CU(cudaEventCreateWithFlags(&p.ev_gate[L], cudaEventDisableTiming));
-            DSG_CU(cudaEventCreateWithFlags(&p.ev_done[L], cudaEventDisableTiming));
-        }
-        p.d_ts = dalloc<unsigned long long>(32);
-        DSG_CU(cudaMemset(p.d_ts, 0, 32 * 8));
-        DSG_CU(cudaMallocHost(&p.h_ts, 32 * 8));
-        DSG_CU(cudaDeviceSynchronize());
         p.eager = (q->flags & DSG_SEARCH_EAGER) != 0;
-        if (!p.eager) { capture_wave(p, 0); capture_wave(p, 1); }
+        p.nslot = p.eager ? 1 : Pipeline::NSLOT;
+        round_grids(p.grid_eval, p.grid_conn);
+        try {
+            for (int L = 0; L < p.nslot; L++) slot_allocate(p, p.sl[L]);
+            DSG_CU(cudaEventCreate(&p.ev_start)); DSG_CU(cudaEventCreate(&p.ev_end));
+            DSG_CU(cudaDeviceSynchronize());
+            if (!p.eager)
+                for (int L = 0; L < p.nslot; L++) capture_wave(p, p.sl[L]);
+        } catch (...) {                                  // out of memory, say: nothing stays allocated
+            for (Slot &S : p.sl) slot_release(S);
+            if (p.ev_start) cudaEventDestroy(p.ev_start);
+            if (p.ev_end) cudaEventDestroy(p.ev_end);
+            p.ev_start = p.ev_end = nullptr;
+            throw;
+        }
         p.open = true;
         return DSG_OK;
     });
@@ -1002,6 +1049,72 @@ extern "C" int dsg_search_open(const dsg_search_params *q) {
 
 namespace dsg {
 namespace search {
+void slot_allocate(Pipeline &p, Slot &S) {
+    DSG_CU(cudaStreamCreateWithFlags(&S.st, cudaStreamNonBlocking));
+    DSG_CU(cudaStreamCreateWithFlags(&S.body_st, cudaStreamNonBlocking));
+    S.lane = gate::lane_create(p.wave);
+    S.ctr = dalloc<uint32_t>(C_N);
+    DSG_CU(cudaMemset(S.ctr, 0, C_N * 4));
+    const uint32_t SC = p.c.sc;
+    S.seeds = dalloc<uint64_t>(SC); S.noise = dalloc<SeedNoise>(SC);
+    S.tabin = dalloc<char>(size_t(SC) * 6 * tabin_bytes());
+    S.tab = dalloc<float>(size_t(SC) * 6 * 512 * 512); S.mx = dalloc<float>(2 * SC);
+    S.act = dalloc<int32_t>(size_t(SC) * 512 * 512); S.nact = dalloc<uint32_t>(SC);
+    S.raw = dalloc<dsg_cand>(size_t(SC) * RAWCAP); S.nraw = dalloc<uint32_t>(SC);
+    S.sites = dalloc<Site>(size_t(SC) * MS); S.nsites = dalloc<uint32_t>(SC); S.nbuck = dalloc<uint32_t>(SC); S.hot = dalloc<Hot>(size_t(SC) * MS);
+    S.f1 = dalloc<int32_t>(size_t(SC) * MS); S.f2 = dalloc<int32_t>(size_t(SC) * MS);
+    S.meta1 = dalloc<uint32_t>(size_t(SC) * MS); S.meta2 = dalloc<uint32_t>(size_t(SC) * MS);
+    S.f8 = dalloc<int32_t>(p.c.tries); S.f4 = dalloc<int32_t>(SC * EXN);
+    const uint32_t caps[4] = {SC * MS, SC * MS, p.c.tries, SC * EXN};
+    const int steps[4] = {256, 128, 8, 4};
+    for (int k = 0; k < 4; k++) {
+        const int half = (k < 2 ? 32000 : 16000) / steps[k], tpr = (2 * half + 1 + TILE - 1) / TILE;
+        S.ph[k].per_req = uint32_t(tpr * tpr);
+        S.ph[k].cap = caps[k];
+        S.ph[k].ctl = dalloc<FloodCtl>(caps[k]); S.ph[k].st = dalloc<FloodStat>(caps[k]);
+        S.ph[k].dir = dalloc<int32_t>(size_t(caps[k]) * S.ph[k].per_req);
+    }
+    S.pool.allocate(p.c.pool_tiles);
+    S.evals = dalloc<unsigned long long>(1);
+    DSG_CU(cudaMemset(S.evals, 0, 8));
+    S.cvm = dalloc<uint32_t>(size_t(SC) * MS * CW); S.nzone = dalloc<uint32_t>(SC); S.zfirst = dalloc<uint32_t>(SC + 1);
+    S.zslot = dalloc<DZone>(size_t(SC) * ZPS); S.zmslot = dalloc<ZoneMeta>(size_t(SC) * ZPS);
+    S.zones = dalloc<DZone>(p.c.zcap); S.zmeta = dalloc<ZoneMeta>(p.c.zcap); S.chunks = dalloc<uint2>(p.c.chcap);
+    S.bits = dalloc<uint8_t>(p.c.cellcap); S.par = dalloc<int32_t>(p.c.cellcap); S.rid = dalloc<int32_t>(p.c.cellcap);
+    S.cs = dalloc<zones::CompStat>(p.c.compcap); S.khi = dalloc<uint64_t>(p.c.cellcap); S.klo = dalloc<uint32_t>(p.c.cellcap);
+    S.rec = dalloc<dsg_component>(p.c.compcap);
+    S.zcnt = dalloc<uint32_t>(p.c.zcap + 1); S.zoff = dalloc<uint32_t>(p.c.zcap + 1); S.zfill = dalloc<uint32_t>(p.c.zcap + 1);
+    S.zcomp = dalloc<uint32_t>(p.c.compcap); S.zcomp2 = dalloc<uint32_t>(p.c.compcap);
+    S.evu = dalloc<Eval>(size_t(SC) * EVC); S.ev = dalloc<Eval>(size_t(SC) * EVC); S.nev = dalloc<uint32_t>(SC);
+    S.tries = dalloc<Try>(p.c.tries);
+    S.out = dalloc<dsg_search_seed>(SC); S.rows = dalloc<dsg_search_row>(ROWCAP);
+    DSG_CU(cudaMallocHost(&S.h_ctr, C_N * 4)); DSG_CU(cudaMallocHost(&S.h_gcnt, 16));
+    DSG_CU(cudaMallocHost(&S.h_out, SC * sizeof(dsg_search_seed))); DSG_CU(cudaMallocHost(&S.h_rows, ROWCAP * sizeof(dsg_search_row)));
+    DSG_CU(cudaMallocHost(&S.h_seeds, SC * 8));
+    DSG_CU(cudaEventCreateWithFlags(&S.ev_done, cudaEventDisableTiming));
+    S.d_ts = dalloc<unsigned long long>(16);
+    DSG_CU(cudaMemset(S.d_ts, 0, 16 * 8));
+    DSG_CU(cudaMallocHost(&S.h_ts, 16 * 8));
+}
+void slot_release(Slot &S) {
+    if (S.st) cudaStreamSynchronize(S.st);
+    if (S.exec) cudaGraphExecDestroy(S.exec);
+    void *bufs[] = {S.ctr, S.seeds, S.noise, S.tabin, S.tab, S.mx, S.act, S.nact, S.raw, S.nraw, S.sites, S.nsites, S.nbuck, S.hot,
+                    S.f1, S.f2, S.f8, S.f4, S.meta1, S.meta2, S.evals, S.cvm, S.nzone, S.zfirst, S.zslot, S.zmslot, S.zones, S.zmeta,
+                    S.chunks, S.bits, S.par, S.rid, S.cs, S.khi, S.klo, S.rec, S.zcnt, S.zoff, S.zfill, S.zcomp, S.zcomp2, S.evu, S.ev, S.nev,
+                    S.tries, S.out, S.rows, S.d_ts};
+    for (void *b : bufs) cudaFree(b);
+    for (Phase &f : S.ph) { cudaFree(f.ctl); cudaFree(f.st); cudaFree(f.dir); }
+    S.pool.release();
+    void *hbufs[] = {S.h_ctr, S.h_gcnt, S.h_out, S.h_rows, S.h_seeds, S.h_ts};
+    for (void *b : hbufs) cudaFreeHost(b);
+    if (S.ev_done) cudaEventDestroy(S.ev_done);
+    if (S.lane) gate::lane_destroy(S.lane);
+    if (S.st) cudaStreamDestroy(S.st);
+    if (S.body_st) cudaStreamDestroy(S.body_st);
+    S = Slot{};
+}
+
 // Output cursor of one run call.
 struct Out {
     dsg_search_seed *seeds; uint32_t seed_cap, ns = 0;
@@ -1011,45 +1124,51 @@ struct Out {
     bool over = false;
     float ms = 0;
 };
-// The wave whose gated seeds are in gate lane L's survivor list (on p.st, after the gate): its graph, then its
-// records; a flagged wave hands its gated seeds back instead.
-void finish_wave(Pipeline &p, Out &o, uint64_t indices, bool gated_by_lane, int L) {
-    if (p.eager) capture_wave(p, L);
-    else DSG_CU(cudaGraphLaunch(p.exec[L], p.st));
-    DSG_CU(cudaMemcpyAsync(p.h_ts + 16 * L, p.d_ts + 16 * L, 16 * 8, cudaMemcpyDeviceToHost, p.st));
-    DSG_CU(cudaMemcpyAsync(p.h_ctr, p.ctr, C_N * 4, cudaMemcpyDeviceToHost, p.st));
-    DSG_CU(cudaMemcpyAsync(p.h_gcnt, gate::lane_counts(p.lane[L]), 16, cudaMemcpyDeviceToHost, p.st));
-    DSG_CU(cudaMemcpyAsync(p.h_out, p.out, p.c.sc * sizeof(dsg_search_seed), cudaMemcpyDeviceToHost, p.st));
-    DSG_CU(cudaEventRecord(p.ev_done[L], p.st));         // lane L may take the next gate once its graph and copies are done
-    DSG_CU(cudaStreamSynchronize(p.st));
-    const uint32_t wrows = std::min(p.h_ctr[C_ROWS], ROWCAP);
-    if (wrows) DSG_CU(cudaMemcpyAsync(p.h_rows, p.rows, size_t(wrows) * sizeof(dsg_search_row), cudaMemcpyDeviceToHost, p.st));
-    DSG_CU(cudaStreamSynchronize(p.st));
-    const unsigned long long *t = p.h_ts + 16 * L;
-    if (gated_by_lane) p.stage_ms[0] += double(t[9] - t[0]) * 1e-6;
+// Wave on slot S, whose gated seeds are in the slot's gate lane (after its gate, or copied there): its graph and
+// the copies of its counters and records, all on the slot's stream.
+void launch_wave(Pipeline &p, Slot &S, uint64_t indices, bool gated) {
+    S.indices = indices; S.gated = gated;
+    if (p.eager) capture_wave(p, S);
+    else DSG_CU(cudaGraphLaunch(S.exec, S.st));
+    DSG_CU(cudaMemcpyAsync(S.h_ts, S.d_ts, 16 * 8, cudaMemcpyDeviceToHost, S.st));
+    DSG_CU(cudaMemcpyAsync(S.h_ctr, S.ctr, C_N * 4, cudaMemcpyDeviceToHost, S.st));
+    DSG_CU(cudaMemcpyAsync(S.h_gcnt, gate::lane_counts(S.lane), 16, cudaMemcpyDeviceToHost, S.st));
+    DSG_CU(cudaMemcpyAsync(S.h_out, S.out, p.c.sc * sizeof(dsg_search_seed), cudaMemcpyDeviceToHost, S.st));
+}
+// The wave of slot S, once done: its records and rows appended to o; a flagged wave hands its gated seeds back.
+void collect_wave(Pipeline &p, Slot &S, Out &o) {
+    DSG_CU(cudaStreamSynchronize(S.st));
+    const uint32_t wrows = std::min(S.h_ctr[C_ROWS], ROWCAP);
+    if (wrows) {
+        DSG_CU(cudaMemcpyAsync(S.h_rows, S.rows, size_t(wrows) * sizeof(dsg_search_row), cudaMemcpyDeviceToHost, S.st));
+        DSG_CU(cudaStreamSynchronize(S.st));
+    }
+    std::memcpy(p.last_ctr, S.h_ctr, sizeof p.last_ctr);
+    const unsigned long long *t = S.h_ts;
+    if (S.gated) p.stage_ms[0] += double(t[9] - t[0]) * 1e-6;
     for (int k = 1; k < Pipeline::NSTAGE; k++) p.stage_ms[k] += double(t[k + 1] - t[k]) * 1e-6;
-    const uint32_t wS = p.h_ctr[C_NS];
-    o.tot[0] += indices; o.tot[1] += p.h_gcnt[0]; o.tot[2] += p.h_gcnt[1]; o.tot[3] += p.h_gcnt[2];
-    o.tot[8] += p.h_ctr[C_ITERS];
-    o.tot[9] += uint64_t(p.graph_kernels) + uint64_t(BODY_KERNELS) * p.h_ctr[C_ITERS] + (gated_by_lane ? 4 + 2 : 0);   // + gate stamps
-    if (p.h_ctr[C_FLAGS]) {
-        o.tot[7] |= p.h_ctr[C_FLAGS];
-        if (p.h_ctr[C_FLAGS] & F_GATE) { set_error("device search: gate survivors exceed the wave's capacity"); throw ArgFail{}; }
-        DSG_CU(cudaMemcpy(p.h_seeds, p.seeds, size_t(wS) * 8, cudaMemcpyDeviceToHost));
+    const uint32_t wS = S.h_ctr[C_NS];
+    o.tot[0] += S.indices; o.tot[1] += S.h_gcnt[0]; o.tot[2] += S.h_gcnt[1]; o.tot[3] += S.h_gcnt[2];
+    o.tot[8] += S.h_ctr[C_ITERS];
+    o.tot[9] += uint64_t(p.graph_kernels) + uint64_t(BODY_KERNELS) * S.h_ctr[C_ITERS] + (S.gated ? 4 + 2 : 0);   // + gate and its stamps
+    if (S.h_ctr[C_FLAGS]) {
+        o.tot[7] |= S.h_ctr[C_FLAGS];
+        if (S.h_ctr[C_FLAGS] & F_GATE) { set_error("device search: gate survivors exceed the wave's capacity"); throw ArgFail{}; }
+        DSG_CU(cudaMemcpy(S.h_seeds, S.seeds, size_t(wS) * 8, cudaMemcpyDeviceToHost));
         for (uint32_t i = 0; i < wS; i++) {
-            if (o.nu < o.unf_cap) o.unf[o.nu] = p.h_seeds[i];
+            if (o.nu < o.unf_cap) o.unf[o.nu] = S.h_seeds[i];
             else o.over = true;
             o.nu++;
         }
         return;
     }
-    o.tot[4] += p.h_ctr[C_SITES]; o.tot[5] += p.h_ctr[C_NHOT]; o.tot[6] += p.h_ctr[C_NBIG];
+    o.tot[4] += S.h_ctr[C_SITES]; o.tot[5] += S.h_ctr[C_NHOT]; o.tot[6] += S.h_ctr[C_NBIG];
     for (uint32_t i = 0; i < wS; i++) {
-        dsg_search_seed rec = p.h_out[i];
+        dsg_search_seed rec = S.h_out[i];
         const uint32_t r0 = rec.row0;
         rec.row0 = o.nr;
         for (uint32_t k = 0; k < rec.nrows; k++) {
-            if (o.nr < o.row_cap) o.rows[o.nr] = p.h_rows[r0 + k];
+            if (o.nr < o.row_cap) o.rows[o.nr] = S.h_rows[r0 + k];
             else o.over = true;
             o.nr++;
         }
@@ -1057,6 +1176,32 @@ void finish_wave(Pipeline &p, Out &o, uint64_t indices, bool gated_by_lane, int 
         else o.over = true;
         o.ns++;
     }
+}
+// Waves 0..n-1 over the slots in turn: wave k + nslot is launched on wave k's slot as soon as wave k is collected,
+// so the other slot's wave keeps the device busy meanwhile.  `enqueue(k, S)` puts wave k's gated seeds into the
+// slot's gate lane and returns (indices, gated).  Device time from the first launch to the end of the last wave.
+template <class F> void run_waves(Pipeline &p, uint64_t n, Out &o, F enqueue) {
+    if (!n) return;
+    Slot &S0 = p.sl[0];
+    DSG_CU(cudaEventRecord(p.ev_start, S0.st));
+    for (int L = 1; L < p.nslot; L++) DSG_CU(cudaStreamWaitEvent(p.sl[L].st, p.ev_start, 0));
+    auto launch = [&](uint64_t k) {
+        Slot &S = p.sl[k % p.nslot];
+        const std::pair<uint64_t, bool> w = enqueue(k, S);
+        launch_wave(p, S, w.first, w.second);
+    };
+    for (uint64_t k = 0; k < std::min<uint64_t>(n, p.nslot); k++) launch(k);
+    for (uint64_t k = 0; k < n; k++) {
+        collect_wave(p, p.sl[k % p.nslot], o);
+        if (k + p.nslot < n) launch(k + p.nslot);
+    }
+    for (int L = 1; L < p.nslot; L++) {
+        DSG_CU(cudaEventRecord(p.sl[L].ev_done, p.sl[L].st));
+        DSG_CU(cudaStreamWaitEvent(S0.st, p.sl[L].ev_done, 0));
+    }
+    DSG_CU(cudaEventRecord(p.ev_end, S0.st));
+    DSG_CU(cudaEventSynchronize(p.ev_end));
+    DSG_CU(cudaEventElapsedTime(&o.ms, p.ev_start, p.ev_end));
 }
 int report(const Out &o, uint32_t *n_seeds, uint32_t *n_rows, uint32_t *n_unfinished, uint64_t counts[10], float *device_ms) {
     *n_seeds = o.ns; *n_rows = o.nr; *n_unfinished = o.nu;
@@ -1079,31 +1224,14 @@ extern "C" int dsg_search_run(uint64_t start, uint64_t count, dsg_search_seed *s
         DSG_ARG(p.open, "dsg_search_run: dsg_search_open has not been called");
         require_init();
         Out o{seeds_out, seed_cap, 0, rows_out, row_cap, 0, unfinished, unfinished_cap, 0};
-        const uint64_t waves = (count + p.wave - 1) / p.wave;
-        // the gate of wave k on lane k & 1 and the gates' stream, after lane k & 1's previous graph is done
-        auto gate = [&](uint64_t k) {
-            const int L = int(k & 1);
+        // wave k: the gate over its indices on the slot's stream, stamped before and after
+        run_waves(p, (count + p.wave - 1) / p.wave, o, [&](uint64_t k, Slot &S) {
             const uint64_t nb = std::min(p.wave, count - k * p.wave);
-            DSG_CU(cudaStreamWaitEvent(p.gst, p.ev_done[L], 0));
-            k_stamp<<<1, 1, 0, p.gst>>>(p.d_ts + 16 * L, 0);
-            gate::lane_enqueue(p.lane[L], p.gst, start + k * p.wave, nb, p.gcfg);
-            k_stamp<<<1, 1, 0, p.gst>>>(p.d_ts + 16 * L, 9);
-            DSG_CU(cudaEventRecord(p.ev_gate[L], p.gst));
-        };
-        if (waves) {
-            DSG_CU(cudaEventRecord(p.ev_start, p.gst));
-            gate(0);
-        }
-        for (uint64_t k = 0; k < waves; k++) {
-            if (k + 1 < waves) gate(k + 1);                  // overlaps this wave's graph
-            DSG_CU(cudaStreamWaitEvent(p.st, p.ev_gate[k & 1], 0));
-            finish_wave(p, o, std::min(p.wave, count - k * p.wave), true, int(k & 1));
-        }
-        if (waves) {
-            DSG_CU(cudaEventRecord(p.ev_end, p.st));
-            DSG_CU(cudaEventSynchronize(p.ev_end));
-            DSG_CU(cudaEventElapsedTime(&o.ms, p.ev_start, p.ev_end));
-        }
+            k_stamp<<<1, 1, 0, S.st>>>(S.d_ts, 0);
+            gate::lane_enqueue(S.lane, S.st, start + k * p.wave, nb, p.gcfg);
+            k_stamp<<<1, 1, 0, S.st>>>(S.d_ts, 9);
+            return std::make_pair(nb, true);
+        });
         return report(o, n_seeds, n_rows, n_unfinished, counts, device_ms);
     });
 }
@@ -1119,34 +1247,30 @@ extern "C" int dsg_search_seeds(const uint64_t *seeds, uint32_t n, dsg_search_se
         DSG_ARG(p.open, "dsg_search_seeds: dsg_search_open has not been called");
         require_init();
         Out o{seeds_out, seed_cap, 0, rows_out, row_cap, 0, unfinished, unfinished_cap, 0};
-        uint64_t *surv = const_cast<uint64_t *>(gate::lane_survivors(p.lane[0]));
-        DSG_CU(cudaEventRecord(p.ev_start, p.st));
-        for (uint32_t base = 0; base < n; base += p.c.sc) {
-            const uint32_t nb = std::min<uint32_t>(p.c.sc, n - base);
-            // the seeds take the place of lane 0's gate survivors: counts {0, 0, nb}
-            std::memcpy(p.h_seeds, seeds + base, size_t(nb) * 8);
-            p.h_gcnt[0] = 0; p.h_gcnt[1] = 0; p.h_gcnt[2] = nb; p.h_gcnt[3] = 0;
-            DSG_CU(cudaMemcpyAsync(surv, p.h_seeds, size_t(nb) * 8, cudaMemcpyHostToDevice, p.st));
-            DSG_CU(cudaMemcpyAsync(gate::lane_counts(p.lane[0]), p.h_gcnt, 16, cudaMemcpyHostToDevice, p.st));
-            k_stamp<<<1, 1, 0, p.st>>>(p.d_ts, 0);
-            finish_wave(p, o, nb, false, 0);
-        }
-        DSG_CU(cudaEventRecord(p.ev_end, p.st));
-        DSG_CU(cudaEventSynchronize(p.ev_end));
-        DSG_CU(cudaEventElapsedTime(&o.ms, p.ev_start, p.ev_end));
+        // wave k: seeds [k * sc, ...) take the place of the slot's gate survivors, counts {0, 0, nb}
+        run_waves(p, (uint64_t(n) + p.c.sc - 1) / p.c.sc, o, [&](uint64_t k, Slot &S) {
+            const uint32_t base = uint32_t(k) * p.c.sc, nb = std::min<uint32_t>(p.c.sc, n - base);
+            std::memcpy(S.h_seeds, seeds + base, size_t(nb) * 8);
+            S.h_gcnt[0] = 0; S.h_gcnt[1] = 0; S.h_gcnt[2] = nb; S.h_gcnt[3] = 0;
+            DSG_CU(cudaMemcpyAsync(const_cast<uint64_t *>(gate::lane_survivors(S.lane)), S.h_seeds, size_t(nb) * 8, cudaMemcpyHostToDevice, S.st));
+            DSG_CU(cudaMemcpyAsync(gate::lane_counts(S.lane), S.h_gcnt, 16, cudaMemcpyHostToDevice, S.st));
+            k_stamp<<<1, 1, 0, S.st>>>(S.d_ts, 0);
+            return std::make_pair(uint64_t(nb), false);
+        });
         return report(o, n_seeds, n_rows, n_unfinished, counts, device_ms);
     });
 }
 
-extern "C" int dsg_search_last_wave(uint64_t info[10]) {
+extern "C" int dsg_search_last_wave(uint64_t info[22]) {
     return guarded([&] {
         DSG_ARG(info, "dsg_search_last_wave: null pointer");
         Pipeline &p = PL();
         std::lock_guard<std::mutex> l(p.mu);
         DSG_ARG(p.open, "dsg_search_last_wave: dsg_search_open has not been called");
-        const uint32_t *c = p.h_ctr;
+        const uint32_t *c = p.last_ctr;
         const uint64_t v[10] = {c[C_FLAGS], c[C_NS], c[C_SITES], c[C_NHOT], c[C_NBIG], c[C_MAXZ], c[C_ZONES], c[C_CELLS], c[C_KEPT], c[C_MAXEV]};
         std::copy(v, v + 10, info);
+        for (int k = 0; k < 4; k++) { info[10 + k] = c[C_NREQ + k]; info[14 + k] = c[C_PHEV + k]; info[18 + k] = c[C_PHIT + k]; }
         return DSG_OK;
     });
 }
@@ -1167,23 +1291,9 @@ extern "C" int dsg_search_close(void) {
         Pipeline &p = PL();
         std::lock_guard<std::mutex> l(p.mu);
         if (!p.open) return DSG_OK;
-        DSG_CU(cudaStreamSynchronize(p.st));
-        DSG_CU(cudaStreamSynchronize(p.gst));
-        for (auto &e : p.exec) { if (e) cudaGraphExecDestroy(e); e = nullptr; }
-        void *bufs[] = {p.ctr, p.seeds, p.noise, p.tabin, p.tab, p.mx, p.act, p.nact, p.raw, p.nraw, p.sites, p.nsites, p.nbuck, p.hot,
-                        p.f1, p.f2, p.f8, p.f4, p.meta1, p.meta2, p.evals, p.cvm, p.nzone, p.zfirst, p.zslot, p.zmslot, p.zones, p.zmeta,
-                        p.chunks, p.bits, p.par, p.rid, p.cs, p.khi, p.klo, p.rec, p.zcnt, p.zoff, p.zfill, p.zcomp, p.evu, p.ev, p.nev,
-                        p.sidx, p.sig, p.tries, p.out, p.rows};
-        for (void *b : bufs) cudaFree(b);
-        for (Phase &f : p.ph) { cudaFree(f.ctl); cudaFree(f.st); cudaFree(f.dir); f = Phase{}; }
-        p.pool.release();
-        cudaFreeHost(p.h_ctr); cudaFreeHost(p.h_gcnt); cudaFreeHost(p.h_out); cudaFreeHost(p.h_rows); cudaFreeHost(p.h_seeds);
+        for (Slot &S : p.sl) slot_release(S);
         cudaEventDestroy(p.ev_start); cudaEventDestroy(p.ev_end);
-        for (int L = 0; L < 2; L++) { cudaEventDestroy(p.ev_gate[L]); cudaEventDestroy(p.ev_done[L]); }
-        cudaStreamDestroy(p.gst);
-        for (auto &ln : p.lane) { gate::lane_destroy(ln); ln = nullptr; }
-        cudaFree(p.d_ts); cudaFreeHost(p.h_ts);
-        cudaStreamDestroy(p.st); cudaStreamDestroy(p.body_st);
+        p.ev_start = p.ev_end = nullptr;
         p.open = false;
         return DSG_OK;
     });

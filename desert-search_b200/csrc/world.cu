@@ -374,6 +374,19 @@ void world_upload(int device) {
     check_tree(b);
     if (g_cand_ready.valid()) g_cand_ready.wait();       // a build for an earlier dsg_init finishes first
     w.cells = upload(cells); w.tree = upload(b.tree); w.param = upload(b.param); w.spl = upload(b.spl); w.prob = upload(b.prob);
+    std::vector<int4> nbox(3 * b.tree.size());           // each node's six intervals, unpacked for the tree search
+    for (size_t k = 0; k < b.tree.size(); k++) {
+        int32_t lo[6], hi[6];
+        for (int i = 0; i < 6; i++) {
+            const size_t q = size_t((b.tree[k] >> (8 * i)) & 255);
+            if (2 * q + 1 >= b.param.size()) throw std::runtime_error("worldgen blob: tree node names a missing interval");
+            lo[i] = b.param[2 * q]; hi[i] = b.param[2 * q + 1];
+        }
+        nbox[3 * k] = make_int4(lo[0], lo[1], lo[2], lo[3]);
+        nbox[3 * k + 1] = make_int4(lo[4], lo[5], hi[0], hi[1]);
+        nbox[3 * k + 2] = make_int4(hi[2], hi[3], hi[4], hi[5]);
+    }
+    w.nbox = upload(nbox);
     g_prob = b.prob;
     // The exact-classification candidate lists take a few hundred milliseconds of GPU work.  They are built on
     // a worker thread while the caller goes on (the gate, tables and scan do not use them); the entry points

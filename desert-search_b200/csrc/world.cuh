@@ -14,6 +14,7 @@ struct WorldDev {
     const int16_t *cells;        // surface grid: biome id per grid cell, -1 = ambiguous (tree decides)
     const uint64_t *tree;        // biome tree nodes
     const int32_t *param;        // interval k = [param[2k], param[2k+1]]
+    const int4 *nbox;            // box of node k, its six intervals unpacked: nbox[3k..3k+2] = lo[0..5], hi[0..5]
     const SplineDev *spl;        // terrain-offset spline graph (node 0 is the root)
     const float *prob;           // 40 x 40 proxy desert probability (row = C bin, column = E bin)
     const uint32_t *cand_off;    // candidate leaves of candidate-grid cell f: cand[cand_off[f] ..] (cand_n[f] of them)
@@ -59,14 +60,13 @@ __device__ __forceinline__ int grid_lookup(const WorldDev &w, const int64_t *q) 
     return w.cells[f];
 }
 __device__ __forceinline__ uint64_t box_dist(const WorldDev &w, int node, const int64_t *v) {
-    const uint64_t e = w.tree[node];
+    const int4 a = __ldg(&w.nbox[3 * node]), b = __ldg(&w.nbox[3 * node + 1]), c = __ldg(&w.nbox[3 * node + 2]);
+    const int32_t lo[6] = {a.x, a.y, a.z, a.w, b.x, b.y}, hi[6] = {b.z, b.w, c.x, c.y, c.z, c.w};
     uint64_t sum = 0;
     #pragma unroll
     for (int i = 0; i < 6; i++) {
-        const int k = int((e >> (8 * i)) & 255);
-        const int64_t lo = w.param[2 * k], hi = w.param[2 * k + 1];
-        int64_t d = lo - v[i];
-        if (v[i] - hi > d) d = v[i] - hi;
+        int64_t d = int64_t(lo[i]) - v[i];
+        if (v[i] - int64_t(hi[i]) > d) d = v[i] - int64_t(hi[i]);
         if (d < 0) d = 0;
         sum += uint64_t(d * d);
     }
@@ -74,39 +74,45 @@ __device__ __forceinline__ uint64_t box_dist(const WorldDev &w, int node, const 
 }
 // Exact nearest-box search of the biome tree (standalone.hpp:182-196), with an explicit stack in place of
 // the recursion.  Children are visited in order and pruned against the running best distance exactly as
-// the recursive form does (the prune test is re-evaluated when a child is reached).
+// the recursive form does (the prune test is made when a child is reached, against the best distance at
+// that moment).  A node's children's distances do not depend on the search state, so they are computed
+// together when the node is entered: their box loads are independent and overlap, where visiting them one
+// by one would wait on two dependent loads per child.
 __device__ inline int tree_classify(const WorldDev &w, const int64_t *v) {
-    struct Frame { int node, level, child, stride, i; };
+    struct Frame { int level, child0, stride, n, i; uint64_t d[6]; };
     Frame stk[8];
     int sp = 0, best = 0;
-    uint64_t bestd = ~0ull;
-    // enter(node, level): leaf -> compare; inner -> push a frame iterating its children
+    uint64_t bestd = ~0ull, dnode = 0;
+    // enter(node, level): leaf -> compare; inner -> push a frame with its children's distances
     int node = 0, level = 0;
     for (;;) {
         bool descended = false;
-        if ((w.tree[node] >> 56) == 255) {
-            const uint64_t d = box_dist(w, node, v);
-            if (d < bestd) { bestd = d; best = node; }
+        const uint64_t e = __ldg(&w.tree[node]);
+        if ((e >> 56) == 255) {
+            if (dnode < bestd) { bestd = dnode; best = node; }
         } else if (sp < 8) {                       // tree depth is 6; the bound only guards the array
             int stride, lv = level;
             do { stride = w.strides[lv & 7]; lv++; } while (node + stride >= w.ntree && lv < 8);
-            stk[sp++] = {node, lv, int(w.tree[node] >> 48), stride, 0};
+            Frame &f = stk[sp++];
+            f.level = lv; f.child0 = int(e >> 48); f.stride = stride; f.i = 0; f.n = 0;
+            #pragma unroll
+            for (int j = 0; j < 6; j++)
+                if (f.child0 + j * stride < w.ntree) { f.d[j] = box_dist(w, f.child0 + j * stride, v); f.n = j + 1; }
         }
         // advance the innermost frame to its next child that passes the prune test
         while (sp > 0) {
             Frame &f = stk[sp - 1];
             bool found = false;
-            while (f.i < 6 && f.child < w.ntree) {
-                const int c = f.child;
-                f.i++; f.child += f.stride;
-                if (box_dist(w, c, v) < bestd) { node = c; level = f.level; found = true; break; }
+            while (f.i < f.n) {
+                const int j = f.i++;
+                if (f.d[j] < bestd) { node = f.child0 + j * f.stride; dnode = f.d[j]; level = f.level; found = true; break; }
             }
             if (found) { descended = true; break; }
             sp--;
         }
         if (!descended) break;
     }
-    return int((w.tree[best] >> 48) & 255);
+    return int((__ldg(&w.tree[best]) >> 48) & 255);
 }
 // Cell of q in the candidate grid (half-open cells as in grid_locate); false outside it.
 __device__ __forceinline__ bool cand_locate(const WorldDev &w, const int64_t *q, uint32_t &flat) {

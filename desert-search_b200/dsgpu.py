@@ -345,12 +345,12 @@ def search_stage_ms(reset=False):
 
 
 SEARCH_WAVE_INFO = ["flags", "gated", "sites", "hot_floods_used", "big_zones", "max_zones_per_seed", "zones", "proxy_cells", "components",
-                    "max_evals_per_seed"]
+                    "max_evals_per_seed"] + [f"{k}_{ph}" for k in ("floods", "subblocks", "iterations") for ph in ("pre", "step128", "step8", "step4")]
 
 
 def search_last_wave():
     """Counters of the last wave (dsg_search_last_wave) as a dict."""
-    v = np.zeros(10, dtype=np.uint64)
+    v = np.zeros(len(SEARCH_WAVE_INFO), dtype=np.uint64)
     _ck(lib.dsg_search_last_wave(ptr(v, u64p)), "dsg_search_last_wave")
     return dict(zip(SEARCH_WAVE_INFO, (int(x) for x in v)))
 

@@ -281,10 +281,12 @@ typedef struct dsg_search_params {
     double exact_min, refine_mb, csv_min;      /* proxy area for exact floods, step-8 area for step 4, CSV row cut */
     uint64_t wave;                             /* seed indices per wave (0 = 2^22, at most 2^26) */
     uint32_t seeds_cap;                        /* gated seeds per wave (0 = 1,024, the most); the wave's zone, cell and
-                                                  flood-tile capacities scale with it (about 20 GB of device memory at 1,024) */
+                                                  flood-tile capacities scale with it (about 20 GB of device memory per
+                                                  wave in flight at 1,024; two waves are in flight) */
     uint32_t flags;                            /* DSG_SEARCH_EAGER: no graph, the stages launched on a stream per wave
-                                                  and the flood loops driven by the host (for profilers that cannot
-                                                  see the kernels of graphs with conditional nodes) */
+                                                  and the flood loops driven by the host, one wave at a time (for
+                                                  profilers that cannot see the kernels of graphs with conditional
+                                                  nodes) */
 } dsg_search_params;
 #define DSG_SEARCH_EAGER 1u
 /* One gated seed: its PREFIX.seeds.csv line (dsearch_desert.cpp:548), rows[row0 .. row0 + nrows) its CSV rows. */
@@ -305,7 +307,8 @@ typedef struct dsg_search_row {
     double proxy, s8, s4, hot;
     int32_t edge, exact;
 } dsg_search_row;
-/* Allocate the pipeline (about 20 GB of device memory at the default capacity) and capture its graph; needs
+/* Allocate the pipeline and capture its graphs: two wave slots, each with its own streams, buffers (about 20 GB
+ * of device memory at the default capacity) and graph, so that two consecutive waves run concurrently.  Needs
  * dsg_init and dsg_scan_init. */
 int dsg_search_open(const dsg_search_params *p);
 /* Search seeds mix(start + k), k < count, wave by wave.  Gated seeds' records go to seeds_out (their rows to
@@ -313,8 +316,8 @@ int dsg_search_open(const dsg_search_params *p);
  * returns its gated seeds in `unfinished` instead: run them through the per-stage entry points.  counts =
  * {indices, phase-passed, pre-gate passed, gated, sites, hot zones used, big zones, OR of wave flags, flood-loop
  * iterations, kernel launches (gate, graph nodes, loop bodies)};
- * device_ms (may be NULL) = CUDA-event time of the waves on the pipeline's stream.  DSG_OVERFLOW if an output
- * capacity was too small (outputs hold the first items). */
+ * device_ms (may be NULL) = CUDA-event time from the first wave's launch to the last wave's end.  DSG_OVERFLOW if
+ * an output capacity was too small (outputs hold the first items). */
 int dsg_search_run(uint64_t start, uint64_t count, dsg_search_seed *seeds_out, uint32_t seed_cap, uint32_t *n_seeds,
                    dsg_search_row *rows_out, uint32_t row_cap, uint32_t *n_rows, uint64_t *unfinished, uint32_t unfinished_cap,
                    uint32_t *n_unfinished, uint64_t counts[10], float *device_ms);
@@ -324,14 +327,18 @@ int dsg_search_seeds(const uint64_t *seeds, uint32_t n, dsg_search_seed *seeds_o
                      dsg_search_row *rows_out, uint32_t row_cap, uint32_t *n_rows, uint64_t *unfinished, uint32_t unfinished_cap,
                      uint32_t *n_unfinished, uint64_t counts[10], float *device_ms);
 /* Device ms per stage summed over the waves run since dsg_search_open (or the last reset), from the device's
- * global timer stamped by one-thread kernels at the stage boundaries of the wave graph: {gate, tables + scan, suppression + hot points, hot pre-floods, step-128 floods + coverage
- * replay, proxy components + exact-start search, step-8 floods, step-4 floods + results}.  No reference
- * counterpart (the reference prints core-seconds per stage on its progress line, dsearch_desert.cpp:552). */
+ * global timer stamped by one-thread kernels at the stage boundaries of each wave: {gate, tables + scan,
+ * suppression + hot points, hot pre-floods, step-128 floods + coverage replay, proxy components + exact-start
+ * search, step-8 floods, step-4 floods + results}.  Two waves run concurrently, so a stage's time includes the
+ * device it shares with the other wave.  No reference counterpart (the reference prints core-seconds per stage
+ * on its progress line, dsearch_desert.cpp:552). */
 int dsg_search_stage_ms(double ms[8], int reset);
 /* Counters of the last wave, for capacity planning: {wave flags, gated seeds, sites, hot-zone floods used, big
  * zones, most big zones of one seed, zones, proxy cells (saturating at 2^32 - 1), components kept, most
- * evaluations of one seed}. */
-int dsg_search_last_wave(uint64_t info[10]);
+ * evaluations of one seed}, then per flood phase (step-256 pre-floods, step-128 floods, step-8 floods, step-4
+ * floods) its floods [10..13], the 16 x 16-cell sub-blocks it evaluated [14..17] and its loop iterations of 6
+ * rounds [18..21]. */
+int dsg_search_last_wave(uint64_t info[22]);
 int dsg_search_close(void);
 
 #ifdef __cplusplus
