@@ -265,14 +265,28 @@ void check_tree(const Blob &b) {
         for (auto it = kids.rbegin(); it != kids.rend(); ++it) stk.push_back(*it);
     }
 }
-// Candidate grid: the surface grid's cuts plus extra temperature cuts above it, since points inside desert
-// floods often have T > 1, beyond every surface box (up to T = 2; a point past the candidate grid on any
-// axis takes the tree search).
+// Candidate grid: the surface grid's cuts, with
+//  * temperature cut below at 5,500, the only part of the axis desert_state classifies (it returns early for
+//    colder points), and extra cuts above it up to T = 2, since points inside desert floods often have T > 1,
+//    beyond every surface box;
+//  * on continentalness, erosion and weirdness, cells beyond the surface boxes on both sides out to 1.0 past
+//    them: hot inland points reach C = 1.5 and W = +-1.6 (measured on the verified finds' floods), and the
+//    tree search they would otherwise take costs a warp thousands of dependent loads.
+// A point past the candidate grid on any axis takes the tree search.
 void build_cand_grid(WorldDev &w) {
     static const int32_t kHotCuts[] = {11001, 12001, 13001, 14001, 15001, 17001, 20001};
+    static const int32_t kOuter[] = {1500, 3500, 6500, 10000};
     for (int a = 0; a < 5; a++) {
         std::vector<int32_t> c(w.cut[a], w.cut[a] + w.ncut[a]);
-        if (a == 0) c.insert(c.end(), std::begin(kHotCuts), std::end(kHotCuts));
+        if (a == 0) {
+            c.insert(c.end(), std::begin(kHotCuts), std::end(kHotCuts));
+            c.push_back(5500);
+            c.erase(std::remove_if(c.begin(), c.end(), [](int32_t v) { return v < 5500; }), c.end());
+        }
+        if (a >= 2) {
+            const int32_t lo = *std::min_element(c.begin(), c.end()), hi = *std::max_element(c.begin(), c.end());
+            for (int32_t o : kOuter) { c.push_back(lo - o); c.push_back(hi + o); }
+        }
         std::sort(c.begin(), c.end());
         c.erase(std::unique(c.begin(), c.end()), c.end());
         if (c.size() > 48) throw std::runtime_error("candidate grid: too many cuts");

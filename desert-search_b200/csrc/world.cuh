@@ -137,8 +137,8 @@ __device__ __forceinline__ bool cand_locate(const WorldDev &w, const int64_t *q,
 // candidates of a cell are every leaf that can attain it for some point of the cell and any depth
 // (world_upload drops a leaf only when a leaf of the same depth interval is nearer everywhere in the cell, by
 // bounds of the whole cell and by pairwise comparison).
-// Points outside the candidate grid (rare: climate values beyond the surface boxes other than hot
-// temperatures) take the tree search itself.
+// Points outside the candidate grid (rare: humidity beyond the surface boxes, T > 2, or C, E, W more than 1.0
+// past them) take the tree search itself.
 __device__ inline int classify_exact(const WorldDev &w, const int64_t *v) {
     uint32_t f;
     if (!cand_locate(w, v, f)) return tree_classify(w, v);
