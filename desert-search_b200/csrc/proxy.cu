@@ -100,25 +100,71 @@ __device__ __forceinline__ bool interior(const uint8_t *b, const DZone &z, int x
         for (int dx = -1; dx <= 1; dx++) if (!b[int64_t(y + dy) * z.nx + x + dx]) return false;
     return true;
 }
-__global__ void __launch_bounds__(256) k_cc_init(const DZone *__restrict__ zones, const uint8_t *__restrict__ bits, int32_t *__restrict__ par,
-                                                 ZoneWork wk) {
+// Union-find inside one chunk, in shared memory (local indices; same rules as uf_find / uf_union).
+__device__ __forceinline__ int lc_find(volatile int32_t *sp, int x) {
+    for (;;) {
+        const int p = sp[x];
+        if (p == x) return x;
+        const int g = sp[p];
+        sp[x] = g;                                       // x is no root: its parent may move up to an ancestor
+        x = g;
+    }
+}
+__device__ __forceinline__ void lc_union(volatile int32_t *sp, int a, int b, uint32_t *err) {
+    for (uint32_t it = 0; it < kLinkLimit; it++) {
+        a = lc_find(sp, a); b = lc_find(sp, b);
+        if (a == b) return;
+        if (a < b) { const int t = a; a = b; b = t; }
+        const int old = atomicCAS(const_cast<int32_t *>(sp) + a, a, b);
+        if (old == a) return;
+        a = old;
+    }
+    atomicOr(err, 1u);
+}
+// Per chunk: the union-find of the 8-connected pairs inside the chunk, in shared memory; every cell's parent
+// in `par` becomes its chunk-local root (zone-local index), -1 for a clear cell.  Pairs reaching an earlier
+// chunk are joined by k_cc_cross.  Each local root is its set's smallest index, as the global rule wants.
+__global__ void __launch_bounds__(256) k_cc_local(const DZone *__restrict__ zones, const uint8_t *__restrict__ bits, int32_t *__restrict__ par,
+                                                  uint32_t *err, ZoneWork wk) {
+    __shared__ int32_t sp_mem[CHUNK];
+    volatile int32_t *sp = sp_mem;
     each_chunk(zones, wk, [&](uint32_t, const DZone &z, int64_t c0, int64_t c1) {
-        for (int64_t c = c0 + threadIdx.x; c < c1; c += blockDim.x) par[z.off + c] = bits[z.off + c] ? int32_t(c) : -1;
+        const uint8_t *b = bits + z.off;
+        const int n = int(c1 - c0);
+        __syncthreads();                                 // the previous chunk is done with sp
+        for (int i = threadIdx.x; i < n; i += blockDim.x) sp[i] = b[c0 + i] ? i : -1;
+        __syncthreads();
+        for (int i = threadIdx.x; i < n; i += blockDim.x) {
+            if (!b[c0 + i]) continue;
+            const int64_t c = c0 + i;
+            const int x = int(c % z.nx), y = int(c / z.nx);
+            // the four neighbours that come earlier in raster order cover every 8-connected pair once
+            const int64_t nb[4] = {c - 1, c - z.nx - 1, c - z.nx, c - z.nx + 1};
+            const bool ok[4] = {zone_bit(b, z, x - 1, y), zone_bit(b, z, x - 1, y - 1), zone_bit(b, z, x, y - 1), zone_bit(b, z, x + 1, y - 1)};
+            #pragma unroll
+            for (int k = 0; k < 4; k++)
+                if (ok[k] && nb[k] >= c0) lc_union(sp, i, int(nb[k] - c0), err);
+        }
+        __syncthreads();
+        for (int i = threadIdx.x; i < n; i += blockDim.x)
+            par[z.off + c0 + i] = b[c0 + i] ? int32_t(c0 + lc_find(sp, i)) : -1;
     });
 }
-__global__ void __launch_bounds__(256) k_cc_merge(const DZone *__restrict__ zones, const uint8_t *__restrict__ bits, int32_t *__restrict__ par,
+// Pairs whose earlier cell lies in an earlier chunk (the chunk's first row and one cell), joined globally.
+__global__ void __launch_bounds__(256) k_cc_cross(const DZone *__restrict__ zones, const uint8_t *__restrict__ bits, int32_t *__restrict__ par,
                                                   uint32_t *err, ZoneWork wk) {
     each_chunk(zones, wk, [&](uint32_t, const DZone &z, int64_t c0, int64_t c1) {
         const uint8_t *b = bits + z.off;
         int32_t *p = par + z.off;
-        for (int64_t c = c0 + threadIdx.x; c < c1; c += blockDim.x) {
+        const int64_t e = min(c1, c0 + z.nx + 2);
+        for (int64_t c = c0 + threadIdx.x; c < e; c += blockDim.x) {
             if (!b[c]) continue;
             const int x = int(c % z.nx), y = int(c / z.nx);
-            // the four neighbours that come earlier in raster order cover every 8-connected pair once
-            if (zone_bit(b, z, x - 1, y)) uf_union(p, int32_t(c), int32_t(c - 1), err);
-            if (zone_bit(b, z, x - 1, y - 1)) uf_union(p, int32_t(c), int32_t(c - z.nx - 1), err);
-            if (zone_bit(b, z, x, y - 1)) uf_union(p, int32_t(c), int32_t(c - z.nx), err);
-            if (zone_bit(b, z, x + 1, y - 1)) uf_union(p, int32_t(c), int32_t(c - z.nx + 1), err);
+            const int64_t nb[4] = {c - 1, c - z.nx - 1, c - z.nx, c - z.nx + 1};
+            const bool ok[4] = {zone_bit(b, z, x - 1, y), zone_bit(b, z, x - 1, y - 1), zone_bit(b, z, x, y - 1), zone_bit(b, z, x + 1, y - 1)};
+            #pragma unroll
+            for (int k = 0; k < 4; k++)
+                if (ok[k] && nb[k] < c0) uf_union(p, int32_t(c), int32_t(nb[k]), err);
         }
     });
 }
@@ -197,28 +243,49 @@ __global__ void __launch_bounds__(256) k_cc_keys(const DZone *__restrict__ zones
         }
     });
 }
-// One block per kept component: the interior keys at ranks 0, n/3 and 2n/3, by an exact radix selection
-// over the 12 bytes of the key (all three ranks in each pass).
+// One block per kept component: the interior keys at ranks 0, n/3 and 2n/3.  The keys are unique (the raster
+// index is part of them), so a key's rank is the number of smaller keys: up to SEL_DIRECT keys, each thread
+// counts for its key over a shared-memory copy; above that, an exact radix selection over the 12 bytes of the
+// key (all three ranks in each pass), warp k finding rank k's digit by a prefix sum over the histogram.
+constexpr uint32_t SEL_DIRECT = 256;
 __global__ void __launch_bounds__(256) k_cc_select(const CompStat *__restrict__ cs, const uint64_t *__restrict__ khi, const uint32_t *__restrict__ klo,
                                                    const uint32_t *ctr, dsg_component *__restrict__ rec, uint32_t comp_cap) {
     __shared__ uint32_t hist[3][256];
-    __shared__ uint64_t pre_hi[3];
-    __shared__ uint32_t pre_lo[3], want[3];
+    __shared__ uint64_t pre_hi[3], s_kh[SEL_DIRECT];
+    __shared__ uint32_t pre_lo[3], want[3], s_kl[SEL_DIRECT];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const uint32_t ncomp = min(ctr[0], comp_cap);
     for (uint32_t id = blockIdx.x; id < ncomp; id += gridDim.x) {
         const CompStat q = cs[id];
         if (q.kid < 0) continue;
         dsg_component &o = rec[q.kid];
         const uint32_t n = q.inner;
+        const uint32_t w0 = 0, w1 = n / 3, w2 = 2 * (n / 3) + ((2 * (n % 3)) / 3);     // floor(2n/3)
         if (threadIdx.x == 0) {
             o.zone = q.zone; o.first = int32_t(q.first); o.cells = q.cells; o.minx = q.minx; o.minz = q.minz; o.inner = n;
             for (int k = 0; k < 3; k++) { o.pick[k] = -1; pre_hi[k] = 0; pre_lo[k] = 0; }
-            want[0] = 0; want[1] = n / 3; want[2] = 2 * (n / 3) + ((2 * (n % 3)) / 3);   // floor(2n/3)
+            want[0] = w0; want[1] = w1; want[2] = w2;
         }
         __syncthreads();
         if (n == 0) { __syncthreads(); continue; }
         const uint64_t *kh = khi + q.seg;
         const uint32_t *kl = klo + q.seg;
+        if (n <= SEL_DIRECT) {
+            const uint32_t i = threadIdx.x;
+            if (i < n) { s_kh[i] = kh[i]; s_kl[i] = kl[i]; }
+            __syncthreads();
+            if (i < n) {
+                const uint64_t h = s_kh[i];
+                const uint32_t l = s_kl[i];
+                uint32_t r = 0;
+                for (uint32_t j = 0; j < n; j++) r += (s_kh[j] < h) || (s_kh[j] == h && s_kl[j] < l);
+                if (r == w0) o.pick[0] = int32_t(l);
+                if (r == w1) o.pick[1] = int32_t(l);
+                if (r == w2) o.pick[2] = int32_t(l);
+            }
+            __syncthreads();
+            continue;
+        }
         for (int d = 11; d >= 0; d--) {
             for (int i = threadIdx.x; i < 3 * 256; i += blockDim.x) (&hist[0][0])[i] = 0;
             __syncthreads();
@@ -235,16 +302,36 @@ __global__ void __launch_bounds__(256) k_cc_select(const CompStat *__restrict__ 
                 }
             }
             __syncthreads();
-            if (threadIdx.x < 3) {
-                const int k = threadIdx.x;
-                uint32_t below = 0, b = 0;
-                for (; b < 255; b++) {
-                    if (below + hist[k][b] > want[k]) break;
-                    below += hist[k][b];
+            if (warp < 3) {                                     // the first digit whose cumulative count passes want
+                const int k = warp;
+                uint32_t c[8], sum = 0;
+                #pragma unroll
+                for (int j = 0; j < 8; j++) { c[j] = hist[k][lane * 8 + j]; sum += c[j]; }
+                uint32_t incl = sum;
+                #pragma unroll
+                for (int o2 = 1; o2 < 32; o2 <<= 1) { const uint32_t t = __shfl_up_sync(0xffffffffu, incl, o2); if (lane >= o2) incl += t; }
+                const uint32_t wk = want[k], excl = incl - sum;
+                const bool here = excl <= wk && wk < incl;          // the lane holding the digit (one lane at most)
+                const uint32_t owner = __ballot_sync(0xffffffffu, here);
+                // no lane holds it only if want >= the count (cannot happen); digit 255 then, as the scan would give
+                const int src = owner ? __ffs(owner) - 1 : 31;
+                uint32_t b = 255, below = 0;
+                if (lane == src) {
+                    uint32_t acc = excl;
+                    b = uint32_t(lane * 8 + 7);
+                    for (int j = 0; j < 8; j++) {
+                        if (j == 7 || acc + c[j] > wk) { b = uint32_t(lane * 8 + j); break; }
+                        acc += c[j];
+                    }
+                    below = acc;
                 }
-                want[k] -= below;
-                if (d >= 4) pre_hi[k] |= uint64_t(b) << (8 * (d - 4));
-                else pre_lo[k] |= b << (8 * d);
+                b = __shfl_sync(0xffffffffu, b, src);
+                below = __shfl_sync(0xffffffffu, below, src);
+                if (lane == 0) {
+                    want[k] = wk - below;
+                    if (d >= 4) pre_hi[k] |= uint64_t(b) << (8 * (d - 4));
+                    else pre_lo[k] |= b << (8 * d);
+                }
             }
             __syncthreads();
         }
@@ -261,8 +348,8 @@ __global__ void __launch_bounds__(256) k_cc_select(const CompStat *__restrict__ 
 void label_components(const DZone *zones, dim3 grid, const ZoneWork &wk, const uint8_t *bits, int32_t *par, int32_t *rid, CompStat *cs,
                       uint64_t *khi, uint32_t *klo, dsg_component *rec, uint32_t *ctr, uint32_t min_cells, unsigned keep_blocks,
                       unsigned select_blocks, uint32_t comp_cap, cudaStream_t st) {
-    k_cc_init<<<grid, 256, 0, st>>>(zones, bits, par, wk);
-    k_cc_merge<<<grid, 256, 0, st>>>(zones, bits, par, ctr + 3, wk);
+    k_cc_local<<<grid, 256, 0, st>>>(zones, bits, par, ctr + 3, wk);
+    k_cc_cross<<<grid, 256, 0, st>>>(zones, bits, par, ctr + 3, wk);
     k_cc_roots<<<grid, 256, 0, st>>>(zones, par, rid, cs, ctr, wk, comp_cap);
     k_cc_flatten<<<grid, 256, 0, st>>>(zones, par, ctr + 3, wk);
     k_cc_stats<<<grid, 256, 0, st>>>(zones, bits, par, rid, cs, wk);

@@ -117,6 +117,22 @@ __device__ __forceinline__ uint32_t float_order(float f) {               // unsi
     return (b & 0x80000000u) ? ~b : (b | 0x80000000u);
 }
 __device__ __forceinline__ uint32_t hash_slot(uint64_t k) { return uint32_t((k * 0x9E3779B97F4A7C15ull) >> 52) & (HT - 1); }
+// Slot of bucket key k in the open-addressing table, or -1.
+__device__ __forceinline__ int find_slot(const unsigned long long *key, uint64_t k) {
+    uint32_t h = hash_slot(k);
+    for (int probe = 0; probe < HT; probe++, h = (h + 1) & (HT - 1)) {
+        const unsigned long long v = key[h];
+        if (v == k) return int(h);
+        if (v == ~0ull) return -1;
+    }
+    return -1;
+}
+// Key of the d-th (0-7) of the 8 buckets around bucket key k.
+__device__ __forceinline__ uint64_t neighbour_key(uint64_t k, int d) {
+    const int e = d < 4 ? d : d + 1;                            // 3 x 3 block without its centre
+    const uint32_t bx = uint32_t(k >> 32) + uint32_t(e / 3 - 1), bz = uint32_t(k) + uint32_t(e % 3 - 1);
+    return (uint64_t(bx) << 32) | bz;
+}
 
 // One block per seed.  For each NMS bucket: the candidate with the highest score (first in CPU loop order on
 // equal scores) and the loop order of the bucket's first candidate; buckets in that first-seen order, sorted
@@ -236,33 +252,71 @@ __global__ void __launch_bounds__(NMS_THREADS) k_nms(const dsg_cand *__restrict_
         for (uint32_t k = threadIdx.x; k < m; k += blockDim.x) order[k] = uint16_t(best[k]);
     }
     __syncthreads();
-    // the sorted buckets' positions, staged for the walk (the hash keys are no longer needed)
-    int2 *pos = reinterpret_cast<int2 *>(key);
-    for (uint32_t k = threadIdx.x; k < m; k += blockDim.x) {
-        const dsg_cand c = rc[first[order[k]]];
-        pos[k] = make_int2(c.x, c.z);
+    // Greedy suppression (keep a bucket's best unless within nms of an earlier kept one), in parallel.  Two
+    // candidates within nms lie in neighbouring buckets, and a bucket holds one candidate, so each candidate
+    // conflicts with at most 8 earlier ones.  Its decision depends only on theirs: rounds decide every
+    // candidate whose earlier conflicts are all decided (the earliest undecided one always is), which gives
+    // the sequential walk's result.  Truncating to max_sites afterwards equals stopping the walk there.
+    int2 *pos = reinterpret_cast<int2 *>(best);                 // rank -> (x, z) (the score keys are done)
+    uint16_t *rank_of = reinterpret_cast<uint16_t *>(bidx);     // hash slot -> rank
+    uint8_t *cmask = reinterpret_cast<uint8_t *>(sv);           // rank -> conflicting earlier neighbours
+    volatile uint8_t *state = cmask + HT;                       // rank -> 0 undecided, 1 kept, 2 suppressed
+    const int nms = P.nms;
+    for (uint32_t r = threadIdx.x; r < m; r += blockDim.x) {
+        const dsg_cand c = rc[first[order[r]]];
+        pos[r] = make_int2(c.x, c.z);
+        const int h = find_slot(key, bucket_key(c.x, c.z, nms));   // present: every rank is a bucket of the table
+        if (h >= 0) rank_of[h] = uint16_t(r);
     }
     __syncthreads();
-    // greedy suppression: warp 0 walks the sorted buckets, the lanes test the kept sites
+    for (uint32_t r = threadIdx.x; r < m; r += blockDim.x) {
+        const int2 c = pos[r];
+        const uint64_t k = bucket_key(c.x, c.y, nms);
+        uint8_t mk = 0;
+        for (int d = 0; d < 8; d++) {
+            const int h = find_slot(key, neighbour_key(k, d));
+            if (h < 0) continue;
+            const uint32_t q = rank_of[h];
+            if (q < r && abs(pos[q].x - c.x) < nms && abs(pos[q].y - c.y) < nms) mk |= uint8_t(1u << d);
+        }
+        cmask[r] = mk;
+        state[r] = 0;
+    }
+    __syncthreads();
+    for (;;) {
+        bool open = false;
+        for (uint32_t r = threadIdx.x; r < m; r += blockDim.x) {
+            if (state[r]) continue;
+            const uint64_t k = bucket_key(pos[r].x, pos[r].y, nms);
+            bool kept_near = false, all = true;
+            for (uint32_t mk = cmask[r]; mk; mk &= mk - 1) {
+                const int h = find_slot(key, neighbour_key(k, __ffs(mk) - 1));     // found when the mask was made
+                const uint8_t sq = h >= 0 ? state[rank_of[h]] : uint8_t(2);
+                if (sq == 1) { kept_near = true; break; }
+                if (sq == 0) all = false;
+            }
+            if (kept_near) state[r] = 2;
+            else if (all) state[r] = 1;
+            else open = true;
+        }
+        if (!__syncthreads_or(open)) break;
+    }
+    // the first max_sites kept candidates in rank order are the sites
     if (threadIdx.x < 32) {
         const int lane = threadIdx.x;
         uint32_t kept = 0;
-        const int nms = P.nms;
-        for (uint32_t k = 0; k < m && int(kept) < P.max_sites; k++) {
-            const int2 c = pos[k];
-            bool near = false;
-            for (uint32_t q = lane; q < kept; q += 32) near |= abs(kx[q] - c.x) < nms && abs(kz[q] - c.y) < nms;
-            near = __any_sync(0xffffffffu, near);
-            if (!near) {
-                if (lane == 0) {
-                    kx[kept] = c.x; kz[kept] = c.y;
-                    const dsg_cand d = rc[first[order[k]]];
-                    sites[size_t(s) * MS + kept] = {d.s, d.t, d.c, d.e, d.x, d.z};
-                }
-                kept++;
-                __syncwarp();
+        for (uint32_t r0 = 0; r0 < m && int(kept) < P.max_sites; r0 += 32) {
+            const uint32_t r = r0 + lane;
+            const bool kp = r < m && state[r] == 1;
+            const uint32_t b = __ballot_sync(0xffffffffu, kp);
+            const uint32_t idx = kept + __popc(b & ((1u << lane) - 1));
+            if (kp && int(idx) < P.max_sites) {
+                const dsg_cand d = rc[first[order[r]]];
+                sites[size_t(s) * MS + idx] = {d.s, d.t, d.c, d.e, d.x, d.z};
             }
+            kept += __popc(b);
         }
+        kept = min(kept, uint32_t(P.max_sites));
         if (lane == 0) { nsites[s] = kept; nbuck[s] = m; atomicAdd(ctr + C_SITES, kept); }
     }
 }
