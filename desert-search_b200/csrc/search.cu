@@ -247,10 +247,17 @@ __global__ void __launch_bounds__(NMS_THREADS) k_nms(const dsg_cand *__restrict_
         if ((best[k] >> 32) == (best[k - 1] >> 32)) s_flag = 2;
     __syncthreads();
     if (s_flag) {
-        if (threadIdx.x == 0) dsg::stl::sort(order, int64_t(m), [&](uint16_t a, uint16_t b) { return sv[a] > sv[b]; });
-    } else {
-        for (uint32_t k = threadIdx.x; k < m; k += blockDim.x) order[k] = uint16_t(best[k]);
+        // std::sort over (score, position) elements: the comparator sees only the score, so the permutation is
+        // the one of sorting the positions by their scores, without an indirection per comparison
+        for (uint32_t k = threadIdx.x; k < m; k += blockDim.x) best[k] = (uint64_t(__float_as_uint(sv[k])) << 32) | k;
+        __syncthreads();
+        if (threadIdx.x == 0)
+            dsg::stl::sort(best, int64_t(m), [](unsigned long long a, unsigned long long b) {
+                return __uint_as_float(uint32_t(a >> 32)) > __uint_as_float(uint32_t(b >> 32));
+            });
+        __syncthreads();
     }
+    for (uint32_t k = threadIdx.x; k < m; k += blockDim.x) order[k] = uint16_t(best[k]);
     __syncthreads();
     // Greedy suppression (keep a bucket's best unless within nms of an earlier kept one), in parallel.  Two
     // candidates within nms lie in neighbouring buckets, and a bucket holds one candidate, so each candidate
