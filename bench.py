@@ -55,9 +55,10 @@ FP64_FLOPS_PER_CLK_PER_SM = 128  # 64 FP64 FMA lanes per SM (B200) x 2 flops
 # k_pregate DRAM traffic per phase-passed seed from one ncu capture (dram__bytes_read.sum + write.sum =
 # 150.5 MB + 6.1 MB over 241,519 seeds on 2^25 seed indices): the seed's octave table read once
 PRE_DRAM_BYTES_PER_SEED = (150.5e6 + 6.1e6) / 241519
-# k_tile_eval FP64 work per evaluated cell, from one ncu capture of a flood batch (profiles/flood_eval_batch.md:
-# executed DFMA x 2 + DADD + DMUL over the cells of the evaluated 16x16 sub-blocks)
-EVAL_FP64_FLOPS_PER_CELL = None
+# k_tile_eval FP64 work per evaluated cell: executed DADD + DMUL + 2 x DFMA (ncu counters over every k_tile_eval
+# launch) divided by the cells of the evaluated 16x16 sub-blocks, on exact step-1 floods of the 32 largest verified
+# finds (profiles/flood_eval_finds.md; 2,297 on step-8 floods of the 6 largest)
+EVAL_FP64_FLOPS_PER_CELL = 2829
 
 
 def dist():
@@ -501,6 +502,19 @@ def run_ours(args):
     props = torch.cuda.get_device_properties(local)
     sms = props.multi_processor_count
 
+    if args.flood_finds:
+        # exact floods from the first N verified finds at one step, one batch each repetition (for launch lists and
+        # captures of the flood engine on large deserts)
+        if rank == 0:
+            finds = json.load(open(os.path.join(ROOT, "tests", "golden", "finds.json")))[:args.flood_finds]
+            step = args.flood_step
+            reqs = [dsgpu.flood_req(f["seed"], f["x"] >> 2, f["z"] >> 2, step, 16000 // step) for f in finds]
+            for rep in range(3):
+                t0 = time.perf_counter()
+                areas = dsgpu.flood_batch(reqs)
+                print(json.dumps({"flood_finds": len(reqs), "step": step, "rep": rep, "s": time.perf_counter() - t0,
+                                  "stats": dsgpu.flood_last_stats(), "cells": [a[0] for a in areas]}), flush=True)
+        return
     if args.flood_only:
         if rank == 0:
             dsgpu.scan_init_default(); dsgpu.search_open()
@@ -625,6 +639,8 @@ def main():
     ap.add_argument("--flood-large", type=int, default=4096)
     ap.add_argument("--flood-rates", type=float, nargs="+", default=[100.0, 500.0, 1000.0, 2000.0, 3000.0, 5000.0])
     ap.add_argument("--flood-requests", type=int, default=None, help="requests per rate (default: 20 s of arrivals, at most 10^5)")
+    ap.add_argument("--flood-finds", type=int, default=0, help="only: exact floods from the first N verified finds (3 batches)")
+    ap.add_argument("--flood-step", type=int, default=8, help="step of --flood-finds (quarts; window half 16000 / step)")
     ap.add_argument("--no-extras", action="store_true", help="skip the pipeline, default-mode and flood measurements")
     args = ap.parse_args()
     global PER_STEP
