@@ -21,6 +21,7 @@
 #include "flood_kernels.cuh"
 #include "zones.cuh"
 #include "stl_sort.h"
+#include "stl_sort_par.h"
 #include <cub/block/block_scan.cuh>
 #include <algorithm>
 #include <climits>
@@ -139,7 +140,8 @@ __device__ __forceinline__ uint64_t neighbour_key(uint64_t k, int d) {
 // by score with std::sort's algorithm, then kept greedily unless within nms of an earlier kept site, up to
 // max_sites.  Mirrors host/dsearch_desert.cpp (and the reference's S2 loop).
 constexpr int NMS_THREADS = 512;
-constexpr size_t NMS_SMEM = size_t(HT) * (8 + 8 + 4 + 4 + 4 + 2) + size_t(MS) * 8;
+constexpr size_t NMS_BASE = size_t(HT) * (8 + 8 + 4 + 4 + 4 + 2) + size_t(MS) * 8;
+constexpr size_t NMS_SMEM = NMS_BASE + size_t(HT) * (7 * 2 + 4 + 1) + 64 * 4;     // + the parallel sort's scratch
 __global__ void __launch_bounds__(NMS_THREADS) k_nms(const dsg_cand *__restrict__ raw, const uint32_t *__restrict__ nraw, Params P,
                                                      Site *__restrict__ sites, uint32_t *__restrict__ nsites, uint32_t *__restrict__ nbuck,
                                                      uint32_t *ctr) {
@@ -229,7 +231,7 @@ __global__ void __launch_bounds__(NMS_THREADS) k_nms(const dsg_cand *__restrict_
     // scores std::sort's own algorithm decides their order.
     for (uint32_t k = threadIdx.x; k < p2; k += blockDim.x) {
         const float v = k < m ? sv[k] : 0.0f;
-        if (v != v) s_flag = 2;                    // NaN: no strict order, std::sort's algorithm decides
+        if (v != v) atomicMax(&s_flag, 3u);        // NaN: no strict order, std::sort's algorithm on one thread
         best[k] = k < m ? (uint64_t(~float_order(v == 0.0f ? 0.0f : v)) << 32) | k : ~0ull;   // -0 = +0, a tie
     }
     __syncthreads();
@@ -244,18 +246,29 @@ __global__ void __launch_bounds__(NMS_THREADS) k_nms(const dsg_cand *__restrict_
             __syncthreads();
         }
     for (uint32_t k = 1 + threadIdx.x; k < m; k += blockDim.x)
-        if ((best[k] >> 32) == (best[k - 1] >> 32)) s_flag = 2;
+        if ((best[k] >> 32) == (best[k - 1] >> 32)) atomicMax(&s_flag, 2u);
     __syncthreads();
     if (s_flag) {
         // std::sort over (score, position) elements: the comparator sees only the score, so the permutation is
         // the one of sorting the positions by their scores, without an indirection per comparison
         for (uint32_t k = threadIdx.x; k < m; k += blockDim.x) best[k] = (uint64_t(__float_as_uint(sv[k])) << 32) | k;
         __syncthreads();
-        if (threadIdx.x == 0)
-            dsg::stl::sort(best, int64_t(m), [](unsigned long long a, unsigned long long b) {
-                return __uint_as_float(uint32_t(a >> 32)) > __uint_as_float(uint32_t(b >> 32));
-            });
-        __syncthreads();
+        auto by_score = [](unsigned long long a, unsigned long long b) {
+            return __uint_as_float(uint32_t(a >> 32)) > __uint_as_float(uint32_t(b >> 32));
+        };
+        if (s_flag == 3) {
+            if (threadIdx.x == 0) dsg::stl::sort(best, int64_t(m), by_score);
+            __syncthreads();
+        } else {                                   // equal scores: the same permutation by the whole block
+            uint16_t *sc16 = reinterpret_cast<uint16_t *>(nms_smem + NMS_BASE);
+            uint32_t *nsw = reinterpret_cast<uint32_t *>(sc16 + 7 * HT);
+            const dsg::stl::ParScratch sc{reinterpret_cast<uint8_t *>(nsw + HT + 64), sc16, sc16 + HT, sc16 + 2 * HT, sc16 + 3 * HT,
+                                          sc16 + 4 * HT, sc16 + 5 * HT, sc16 + 6 * HT, nsw, nsw + HT};
+            if (!dsg::stl::par_sort(dsg::stl::BlockExec(), best, int(m), by_score, sc)) {   // cannot happen without NaN
+                if (threadIdx.x == 0) { atomicOr(ctr + C_FLAGS, F_HASH); nsites[s] = 0; nbuck[s] = 0; }
+                return;
+            }
+        }
     }
     for (uint32_t k = threadIdx.x; k < m; k += blockDim.x) order[k] = uint16_t(best[k]);
     __syncthreads();
@@ -659,23 +672,22 @@ __global__ void __launch_bounds__(256) k_comp_order(const dsg_component *__restr
 }
 // Warp per seed: components of its zones in (zone, first cell) order, each new one (by its smallest column and
 // row) an evaluation whose start is the interior cell nearest the centroid (alternatives at ranks n/3, 2n/3);
-// evaluations sorted by proxy size with std::sort's algorithm; exact-flood starts of the first exact_n.  The
-// lanes load 32 components at a time; the signatures seen and the sort keys live in shared memory.
+// each with its sort key (cells, index) for k_eval_order.  The lanes load 32 components at a time; the signatures
+// seen live in shared memory.
 constexpr int EV_WARPS = 4;
-constexpr size_t EV_SMEM = size_t(EV_WARPS) * EVC * (8 + 4 + 2);
+constexpr size_t EV_SMEM = size_t(EV_WARPS) * EVC * 8;
 __global__ void __launch_bounds__(EV_WARPS * 32) k_evals(const uint32_t *__restrict__ zfirst, const DZone *__restrict__ zones,
                                                          const ZoneMeta *__restrict__ zmeta, const uint32_t *__restrict__ zoff,
                                                          const uint32_t *__restrict__ zcomp, const dsg_component *__restrict__ rec, Params P,
-                                                         Eval *__restrict__ evu, Eval *__restrict__ ev, uint32_t *__restrict__ nev,
-                                                         Try *__restrict__ tries, uint32_t *ctr) {
+                                                         Eval *__restrict__ evu, unsigned long long *__restrict__ ekey,
+                                                         uint32_t *__restrict__ nev, uint32_t *ctr) {
     extern __shared__ __align__(16) unsigned char ev_smem[];
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
     int64_t *seen = reinterpret_cast<int64_t *>(ev_smem) + size_t(w) * EVC;
-    uint32_t *cellk = reinterpret_cast<uint32_t *>(ev_smem + size_t(EV_WARPS) * EVC * 8) + size_t(w) * EVC;
-    uint16_t *idx = reinterpret_cast<uint16_t *>(ev_smem + size_t(EV_WARPS) * EVC * 12) + size_t(w) * EVC;
     const uint32_t s = blockIdx.x * EV_WARPS + w;
     if (s >= ctr[C_NS]) return;
-    Eval *U = evu + size_t(s) * EVC, *E = ev + size_t(s) * EVC;
+    Eval *U = evu + size_t(s) * EVC;
+    unsigned long long *K = ekey + size_t(s) * EVC;
     uint32_t ne = 0;                                     // evaluations so far (= signatures seen), uniform across the warp
     bool full = false;
     const uint32_t nzw = ctr[C_ZONES];
@@ -703,7 +715,7 @@ __global__ void __launch_bounds__(EV_WARPS * 32) k_evals(const uint32_t *__restr
                 if (ne == EVC) { full = true; continue; }
                 if (uint32_t(lane) == j) {                   // the component's own lane writes its evaluation
                     seen[ne] = sj;
-                    cellk[ne] = c.cells;
+                    K[ne] = (uint64_t(c.cells) << 32) | ne;
                     const int32_t cell = c.inner ? c.pick[0] : c.first;
                     Eval e{};
                     e.rank = m.rank; e.x = z.x0 + (cell % z.nx) * 32; e.z = z.z0 + (cell / z.nx) * 32;
@@ -721,16 +733,36 @@ __global__ void __launch_bounds__(EV_WARPS * 32) k_evals(const uint32_t *__restr
         if (full) atomicOr(ctr + C_FLAGS, F_EVALS);
         atomicMax(ctr + C_MAXEV, ne + (full ? 1 : 0));
         if (s == 0 && ctr[C_PROXY + 3]) atomicOr(ctr + C_FLAGS, F_LABEL);
-        // std::sort(ev, proxy descending): the permutation from the sort, then the records copied out in its order.
-        // The proxy is cells x 16384 / 10^6, strictly increasing in cells, so comparing cells gives the same
-        // comparison results and hence the same permutation.
-        for (uint32_t k = 0; k < ne; k++) idx[k] = uint16_t(k);
-        dsg::stl::sort(idx, int64_t(ne), [&](uint16_t a, uint16_t b) { return cellk[a] > cellk[b]; });
         nev[s] = ne;
     }
-    __syncwarp();
-    for (uint32_t k = lane; k < ne; k += 32) E[k] = U[idx[k]];
-    __syncwarp();
+}
+// Block per seed: std::sort(ev, proxy descending) with the library's permutation, computed by the block
+// (stl_sort_par.h), the records copied out in its order, the exact-flood starts of the first exact_n.  The proxy is
+// cells x 16384 / 10^6, strictly increasing in cells, so comparing cells gives the same comparison results and
+// hence the same permutation.
+constexpr int EVO_THREADS = 256;
+constexpr size_t EVO_SMEM = size_t(EVC) * (8 + 7 * 2 + 4 + 1) + 64 * 4;
+__global__ void __launch_bounds__(EVO_THREADS) k_eval_order(const Eval *__restrict__ evu, const unsigned long long *__restrict__ ekey,
+                                                          const uint32_t *__restrict__ nev, Params P, Eval *__restrict__ ev,
+                                                          Try *__restrict__ tries, uint32_t *ctr) {
+    extern __shared__ __align__(16) unsigned char eo_smem[];
+    unsigned long long *a = reinterpret_cast<unsigned long long *>(eo_smem);
+    uint16_t *sc16 = reinterpret_cast<uint16_t *>(a + EVC);
+    uint32_t *nsw = reinterpret_cast<uint32_t *>(sc16 + 7 * EVC);
+    const dsg::stl::ParScratch sc{reinterpret_cast<uint8_t *>(nsw + EVC + 64), sc16, sc16 + EVC, sc16 + 2 * EVC, sc16 + 3 * EVC,
+                                  sc16 + 4 * EVC, sc16 + 5 * EVC, sc16 + 6 * EVC, nsw, nsw + EVC};
+    const uint32_t s = blockIdx.x;
+    if (s >= ctr[C_NS]) return;
+    const uint32_t ne = nev[s];
+    const Eval *U = evu + size_t(s) * EVC;
+    Eval *E = ev + size_t(s) * EVC;
+    for (uint32_t k = threadIdx.x; k < ne; k += blockDim.x) a[k] = ekey[size_t(s) * EVC + k];
+    __syncthreads();
+    dsg::stl::par_sort(dsg::stl::BlockExec(), a, int(ne), [](unsigned long long x, unsigned long long y) { return (x >> 32) > (y >> 32); },
+                       sc);                              // integer keys: the comparator is consistent, no failure
+    for (uint32_t k = threadIdx.x; k < ne; k += blockDim.x) E[k] = U[uint32_t(a[k])];
+    __syncthreads();
+    const int lane = threadIdx.x;
     if (lane < EXN * 3) {
         const int k2 = lane / 3, t = lane % 3;
         Try &tr = tries[(size_t(s) * EXN + k2) * 3 + t];
@@ -879,6 +911,9 @@ struct Caps {
 // One wave in flight: its streams, gate lane, device buffers (about 20 GB at 1,024 seeds), graph, stage stamps and
 // pinned host copies.  Consecutive waves alternate between two slots that run concurrently, so the
 // latency-bound flood rounds of one wave overlap the throughput-bound stages of the other (gate, tables, proxy).
+#ifndef DSG_SEARCH_SLOTS
+#define DSG_SEARCH_SLOTS 2               // waves in flight (each a complete wave state, about 20 GB at 1,024 seeds)
+#endif
 struct Slot {
     cudaStream_t st = nullptr, body_st = nullptr;
     gate::Lane *lane = nullptr;
@@ -896,7 +931,7 @@ struct Slot {
     DZone *zslot = nullptr, *zones = nullptr; ZoneMeta *zmslot = nullptr, *zmeta = nullptr; uint2 *chunks = nullptr;
     uint8_t *bits = nullptr; int32_t *par = nullptr, *rid = nullptr; zones::CompStat *cs = nullptr; uint64_t *khi = nullptr; uint32_t *klo = nullptr;
     dsg_component *rec = nullptr; uint32_t *zcnt = nullptr, *zoff = nullptr, *zfill = nullptr, *zcomp = nullptr, *zcomp2 = nullptr;
-    Eval *evu = nullptr, *ev = nullptr; uint32_t *nev = nullptr; Try *tries = nullptr;
+    Eval *evu = nullptr, *ev = nullptr; unsigned long long *ekey = nullptr; uint32_t *nev = nullptr; Try *tries = nullptr;
     dsg_search_seed *out = nullptr; dsg_search_row *rows = nullptr;
     cudaGraphExec_t exec = nullptr;
     cudaEvent_t ev_done = nullptr;
@@ -919,7 +954,7 @@ struct Pipeline {
     int grid_eval = 0, grid_conn = 0;
     bool eager = false;                          // no graph: every wave launches the stages on the stream (for profilers)
     uint32_t graph_kernels = 0;                  // kernel nodes of the wave graph outside the loop bodies
-    static constexpr int NSLOT = 2;
+    static constexpr int NSLOT = DSG_SEARCH_SLOTS;
     int nslot = NSLOT;                           // 1 in eager mode (its flood loops synchronise with the host)
     Slot sl[NSLOT];
     cudaEvent_t ev_start = nullptr, ev_end = nullptr;
@@ -1024,7 +1059,9 @@ void capture_wave(Pipeline &p, Slot &S) {
     k_comp_order<<<4 * 148, 256, 0, S.st>>>(S.rec, S.ctr, S.zoff, S.zcomp2, S.zcomp);
     DSG_CU(cudaFuncSetAttribute(k_evals, cudaFuncAttributeMaxDynamicSharedMemorySize, int(EV_SMEM)));
     k_evals<<<(SC + EV_WARPS - 1) / EV_WARPS, EV_WARPS * 32, EV_SMEM, S.st>>>(S.zfirst, S.zones, S.zmeta, S.zoff, S.zcomp, S.rec, p.P, S.evu,
-                                                                             S.ev, S.nev, S.tries, S.ctr);
+                                                                             S.ekey, S.nev, S.ctr);
+    DSG_CU(cudaFuncSetAttribute(k_eval_order, cudaFuncAttributeMaxDynamicSharedMemorySize, int(EVO_SMEM)));
+    k_eval_order<<<SC, EVO_THREADS, EVO_SMEM, S.st>>>(S.evu, S.ekey, S.nev, p.P, S.ev, S.tries, S.ctr);
     k_ring<<<8 * 148, 128, 0, S.st>>>(S.noise, world_dev(), S.tries, S.ctr);
     // every start of the retry loop flooded at once (a wave has few exact floods, so the sequential loop's
     // passes would only add rounds); k_retry then replays the loop over their areas
@@ -1042,9 +1079,9 @@ void capture_wave(Pipeline &p, Slot &S) {
     DSG_CU(cudaGetLastError());
     k_stamp<<<1, 1, 0, S.st>>>(ts, 8);
     // kernels outside the loop bodies: 6 set-up/scan kernels and the table launches, 7 for suppression, hot points,
-    // requests, coverage and zones, 9 for the proxy bitmaps and labelling, 11 for components, exact starts, retries,
-    // results and the wave's end, 5 per flood phase, 8 stage stamps
-    p.graph_kernels = 6 + table_launches + 7 + 9 + 11 + 4 * 5 + 8;
+    // requests, coverage and zones, 9 for the proxy bitmaps and labelling, 12 for components, evaluations and their
+    // order, exact starts, retries, results and the wave's end, 5 per flood phase, 8 stage stamps
+    p.graph_kernels = 6 + table_launches + 7 + 9 + 12 + 4 * 5 + 8;
     if (p.eager) return;
     cudaGraph_t g = nullptr;
     DSG_CU(cudaStreamEndCapture(S.st, &g));
@@ -1147,6 +1184,7 @@ void slot_allocate(Pipeline &p, Slot &S) {
     S.zcnt = dalloc<uint32_t>(p.c.zcap + 1); S.zoff = dalloc<uint32_t>(p.c.zcap + 1); S.zfill = dalloc<uint32_t>(p.c.zcap + 1);
     S.zcomp = dalloc<uint32_t>(p.c.compcap); S.zcomp2 = dalloc<uint32_t>(p.c.compcap);
     S.evu = dalloc<Eval>(size_t(SC) * EVC); S.ev = dalloc<Eval>(size_t(SC) * EVC); S.nev = dalloc<uint32_t>(SC);
+    S.ekey = dalloc<unsigned long long>(size_t(SC) * EVC);
     S.tries = dalloc<Try>(p.c.tries);
     S.out = dalloc<dsg_search_seed>(SC); S.rows = dalloc<dsg_search_row>(ROWCAP);
     DSG_CU(cudaMallocHost(&S.h_ctr, C_N * 4)); DSG_CU(cudaMallocHost(&S.h_gcnt, 16));
@@ -1162,7 +1200,7 @@ void slot_release(Slot &S) {
     if (S.exec) cudaGraphExecDestroy(S.exec);
     void *bufs[] = {S.ctr, S.seeds, S.noise, S.tabin, S.tab, S.mx, S.act, S.nact, S.raw, S.nraw, S.sites, S.nsites, S.nbuck, S.hot,
                     S.f1, S.f2, S.f8, S.f4, S.meta1, S.meta2, S.evals, S.cvm, S.nzone, S.zfirst, S.zslot, S.zmslot, S.zones, S.zmeta,
-                    S.chunks, S.bits, S.par, S.rid, S.cs, S.khi, S.klo, S.rec, S.zcnt, S.zoff, S.zfill, S.zcomp, S.zcomp2, S.evu, S.ev, S.nev,
+                    S.chunks, S.bits, S.par, S.rid, S.cs, S.khi, S.klo, S.rec, S.zcnt, S.zoff, S.zfill, S.zcomp, S.zcomp2, S.evu, S.ev, S.ekey, S.nev,
                     S.tries, S.out, S.rows, S.d_ts};
     for (void *b : bufs) cudaFree(b);
     for (Phase &f : S.ph) { cudaFree(f.ctl); cudaFree(f.st); cudaFree(f.dir); }

@@ -1,6 +1,8 @@
-"""The device stages' sort (csrc/stl_sort.h) leaves elements in the same order as the host library's std::sort,
-equal keys included, so the device searcher keeps the same candidate among equal scores as the host searcher
-and the reference.  Compiled with the host compiler and checked on 8,000 arrays with many equal keys."""
+"""The device stages' sorts leave elements in the same order as the host library's std::sort, equal keys included,
+so the device searcher keeps the same candidate among equal scores as the host searcher and the reference: the
+sequential form (csrc/stl_sort.h) and the block-parallel form (csrc/stl_sort_par.h, run here as one emulated
+thread).  Compiled with the host compiler and checked on 8,000 arrays with many equal keys, some of them built by
+McIlroy's adversary so that the depth budget runs out and the heapsort fallback is taken."""
 import os
 import subprocess
 import tempfile
