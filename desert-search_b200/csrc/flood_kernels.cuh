@@ -484,22 +484,29 @@ inline unsigned dir_chunks(int64_t max_entries) { return unsigned((max_entries +
 // Releasing the tiles is a separate launch (k_tile_release), since the statistics read neighbouring tiles.
 static __global__ void __launch_bounds__(256) k_tile_finish(const FloodCtl *__restrict__ ctl, const uint32_t *__restrict__ slots,
                                                             const int32_t *__restrict__ dir, Tiles T, FloodStat *__restrict__ st,
-                                                            const uint32_t *__restrict__ n_dev = nullptr) {
-    if (n_dev && blockIdx.x >= *n_dev) return;           // requests counted on the device (grid sized for the capacity)
-    const uint32_t r = slots ? slots[blockIdx.x] : blockIdx.x;
-    const FloodCtl c = ctl[r];
+                                                            const uint32_t *__restrict__ n_dev = nullptr, bool warp_req = false) {
+    // Request blockIdx.x of gridDim.x, its directory chunk blockIdx.y; with n_dev (requests counted on the
+    // device) the grid strides over them, and with warp_req each warp takes whole requests (small directories).
+    const uint32_t nreq = n_dev ? *n_dev : gridDim.x;
     const int lane = threadIdx.x & 31;
-    const int64_t entries = min(int64_t(c.tpr) * c.tpr, int64_t(blockIdx.y + 1) * DIR_CHUNK);
-    for (int64_t base = int64_t(blockIdx.y) * DIR_CHUNK + (threadIdx.x & ~31); base < entries; base += blockDim.x) {
-        const int64_t e = base + lane;
-        const int32_t d = e < entries ? __ldcg(dir + c.dir_off + e) : -1;
-        uint32_t m = __ballot_sync(0xffffffffu, d >= 0);
-        while (m) {
-            const int l = __ffs(m) - 1;
-            m &= m - 1;
-            const int32_t t = __shfl_sync(0xffffffffu, d, l);
-            const int64_t te = base + l;
-            tile_stats(c, dir, T, t, int(te % c.tpr), int(te / c.tpr), st[r]);
+    const uint32_t q0 = warp_req ? blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5) : blockIdx.x;
+    const uint32_t dq = warp_req ? gridDim.x * (blockDim.x >> 5) : gridDim.x;
+    const int64_t first = warp_req ? 0 : (threadIdx.x & ~31), stride = warp_req ? 32 : blockDim.x;
+    for (uint32_t q = q0; q < nreq; q += dq) {
+        const uint32_t r = slots ? slots[q] : q;
+        const FloodCtl c = ctl[r];
+        const int64_t entries = min(int64_t(c.tpr) * c.tpr, int64_t(blockIdx.y + 1) * DIR_CHUNK);
+        for (int64_t base = int64_t(blockIdx.y) * DIR_CHUNK + first; base < entries; base += stride) {
+            const int64_t e = base + lane;
+            const int32_t d = e < entries ? __ldcg(dir + c.dir_off + e) : -1;
+            uint32_t m = __ballot_sync(0xffffffffu, d >= 0);
+            while (m) {
+                const int l = __ffs(m) - 1;
+                m &= m - 1;
+                const int32_t t = __shfl_sync(0xffffffffu, d, l);
+                const int64_t te = base + l;
+                tile_stats(c, dir, T, t, int(te % c.tpr), int(te / c.tpr), st[r]);
+            }
         }
     }
 }

@@ -1015,7 +1015,11 @@ void capture_phase(Pipeline &p, Slot &S, int k) {
         cudaGraph_t body_out = nullptr;
         DSG_CU(cudaStreamEndCapture(S.body_st, &body_out));
     }
-    k_tile_finish<<<dim3(f.cap, dir_chunks(f.per_req)), 256, 0, S.st>>>(f.ctl, nullptr, f.dir, S.pool.T, f.st, nreq);
+    // small directories (the hot-zone floods, one per site): a warp per request over a grid striding over them;
+    // large ones (exact floods, few): a block per directory chunk
+    const bool small_dir = f.per_req <= 64;
+    k_tile_finish<<<dim3(small_dir ? std::min(f.cap, 32u * 148u) : f.cap, dir_chunks(f.per_req)), 256, 0, S.st>>>(f.ctl, nullptr, f.dir,
+                                                                                                                 S.pool.T, f.st, nreq, small_dir);
     k_phase_end<<<1, 1, 0, S.st>>>(S.ctr, k, S.evals);
     DSG_CU(cudaGetLastError());
 }

@@ -196,18 +196,20 @@ __global__ void __launch_bounds__(TN, Band<R>::BLOCKS) k_tables(const TabIn *__r
 }
 
 // Active side-A T cells (TA >= ta), compacted per seed in row-major order of discovery.
+// Seeds blockIdx.y, blockIdx.y + gridDim.y, ... below *n_dev (n_dev null: seed blockIdx.y of gridDim.y).
 __global__ void k_active(const float *__restrict__ tabs, float ta, int32_t *__restrict__ act, uint32_t *__restrict__ nact,
                          const uint32_t *__restrict__ n_dev) {
-    if (n_dev && blockIdx.y >= *n_dev) return;
-    const int cell = blockIdx.x * blockDim.x + threadIdx.x, sd = blockIdx.y;
-    const bool on = tabs[size_t(sd) * 6 * TN * TN + cell] >= ta;
-    const uint32_t m = __ballot_sync(0xffffffffu, on);
-    if (!m) return;
-    const int lane = threadIdx.x & 31;
-    uint32_t at = 0;
-    if (lane == __ffs(m) - 1) at = atomicAdd(&nact[sd], uint32_t(__popc(m)));
-    at = __shfl_sync(0xffffffffu, at, __ffs(m) - 1);
-    if (on) act[size_t(sd) * TN * TN + at + __popc(m & ((1u << lane) - 1))] = cell;
+    const uint32_t ns = n_dev ? *n_dev : gridDim.y;
+    const int cell = blockIdx.x * blockDim.x + threadIdx.x, lane = threadIdx.x & 31;
+    for (uint32_t sd = blockIdx.y; sd < ns; sd += gridDim.y) {
+        const bool on = tabs[size_t(sd) * 6 * TN * TN + cell] >= ta;
+        const uint32_t m = __ballot_sync(0xffffffffu, on);
+        if (!m) continue;
+        uint32_t at = 0;
+        if (lane == __ffs(m) - 1) at = atomicAdd(&nact[sd], uint32_t(__popc(m)));
+        at = __shfl_sync(0xffffffffu, at, __ffs(m) - 1);
+        if (on) act[size_t(sd) * TN * TN + at + __popc(m & ((1u << lane) - 1))] = cell;
+    }
 }
 
 // Translation scan of one active cell (dsearch_desert.cpp:257-280): thread = (tz, tx) pair.
@@ -215,8 +217,8 @@ __global__ void __launch_bounds__(256) k_scan(const float *__restrict__ tabs, co
         const int16_t *__restrict__ ibT, const int16_t *__restrict__ ibC, const int8_t *__restrict__ loT, const int8_t *__restrict__ hiT,
         dsg_scan_params sp, ScanConst sc, Cand *__restrict__ out, uint32_t *__restrict__ ncand, uint32_t cap,
         const uint32_t *__restrict__ n_dev) {
-    if (n_dev && blockIdx.y >= *n_dev) return;
-    const int sd = blockIdx.y;
+    const uint32_t ns = n_dev ? *n_dev : gridDim.y;     // seeds blockIdx.y, blockIdx.y + gridDim.y, ...
+    for (uint32_t sd = blockIdx.y; sd < ns; sd += gridDim.y) {
     const uint32_t na = nact[sd];
     for (uint32_t a = blockIdx.x; a < na; a += gridDim.x) {
     const int cell = act[size_t(sd) * TN * TN + a], j = cell >> 9, i = cell & (TN - 1);
@@ -238,6 +240,7 @@ __global__ void __launch_bounds__(256) k_scan(const float *__restrict__ tabs, co
         if (s < tt) continue;
         const uint32_t k = atomicAdd(&ncand[sd], 1u);
         if (k < cap) out[size_t(sd) * cap + k] = {s, tv, cv, ev, i * sc.cell + (tx + sc.kmin) * sc.period, j * sc.cell + (tz + sc.kmin) * sc.period};
+    }
     }
     }
 }
@@ -361,8 +364,8 @@ __global__ void k_fill_f32(float *__restrict__ p, float v, uint32_t n) {
 }  // namespace tables
 
 // Tables, blur, maxima, active cells and the translation scan for seeds whose noise tables and count are on the
-// device (the device-resident searcher): grids cover cap_seeds, blocks of seeds at or beyond *n_dev return at
-// once.  Needs dsg_scan_init.  cand holds cap candidates per seed (dsg_cand layout), ncand the counts (a count
+// device (the device-resident searcher): the grids of the table kernels cover cap_seeds (blocks of seeds at or
+// beyond *n_dev return at once), those of the active cells and the scan stride over the counted seeds.  Needs dsg_scan_init.  cand holds cap candidates per seed (dsg_cand layout), ncand the counts (a count
 // above cap means the seed overflowed).  Everything is enqueued on st; returns the number of k_tables launches.
 int scan_seeds_device(const SeedNoise *noise, const uint32_t *n_dev, uint32_t cap_seeds, void *tabin, float *tab, float *mx, int32_t *act,
                        uint32_t *nact, dsg_cand *cand, uint32_t *ncand, uint32_t cap, const dsg_scan_params &sp, cudaStream_t st) {
@@ -375,8 +378,11 @@ int scan_seeds_device(const SeedNoise *noise, const uint32_t *n_dev, uint32_t ca
     launch_tables(TabJob{g.sc, in, tab, mx, st, n_dev}, cap_seeds);
     DSG_CU(cudaMemsetAsync(nact, 0, size_t(cap_seeds) * 4, st));
     DSG_CU(cudaMemsetAsync(ncand, 0, size_t(cap_seeds) * 4, st));
-    k_active<<<dim3(TN * TN / 256, cap_seeds), 256, 0, st>>>(tab, sp.ta, act, nact, n_dev);
-    k_scan<<<dim3(SCAN_BLOCKS, cap_seeds), 256, 0, st>>>(tab, act, nact, g.d_ibT, g.d_ibC, g.d_loT, g.d_hiT, sp, g.sc,
+    // a wave fills a third or less of its seed capacity: the grids stride over the counted seeds instead of
+    // covering the capacity with blocks that would only return
+    const uint32_t ys = std::min(cap_seeds, 128u);
+    k_active<<<dim3(TN * TN / 256, ys), 256, 0, st>>>(tab, sp.ta, act, nact, n_dev);
+    k_scan<<<dim3(SCAN_BLOCKS, ys), 256, 0, st>>>(tab, act, nact, g.d_ibT, g.d_ibC, g.d_loT, g.d_hiT, sp, g.sc,
                                                          reinterpret_cast<Cand *>(cand), ncand, cap, n_dev);
     DSG_CU(cudaGetLastError());
     return g.sc.rT == g.sc.rC ? 1 : 2;

@@ -811,7 +811,8 @@ int main(int argc, char **argv) {
             sp.max_sites = P.max_sites; sp.nms = P.nms; sp.exact_n = P.exact_n;
             sp.hot_min = P.hot_min; sp.hot_pre = P.hot_pre; sp.exact_min = P.exact_min; sp.refine_mb = P.refine_mb; sp.csv_min = P.csv_min;
             ck(dsg_search_open(&sp), "device search");
-            std::vector<dsg_search_seed> recs(1u << 16); std::vector<dsg_search_row> rows(1u << 18); std::vector<uint64_t> unf(1u << 16);
+            // one call covers up to 16 waves (2^26 indices): at most 16 x 1,024 gated seeds and 16 x 65,536 rows
+            std::vector<dsg_search_seed> recs(1u << 16); std::vector<dsg_search_row> rows(1u << 20); std::vector<uint64_t> unf(1u << 16);
             uint64_t tot[4] = {0, 0, 0, 0};
             const auto tg = Clock::now();
             auto take = [&](uint32_t ns, uint32_t nu, const uint64_t *c) {
@@ -821,7 +822,7 @@ int main(int argc, char **argv) {
                 for (uint32_t i = 0; i < nu && !interrupted; i++) push(unf[i]);
             };
             if (P.gate) {
-                const uint64_t B = 1ull << 24;
+                const uint64_t B = 1ull << 26;               // waves stay in flight across the calls' waves, not between calls
                 for (uint64_t base = 0; base < total && !interrupted; base += B) {
                     const uint64_t nb = std::min(B, total - base);
                     uint32_t ns = 0, nr = 0, nu = 0; uint64_t c[10]; float ms = 0;
