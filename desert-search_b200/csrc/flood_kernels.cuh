@@ -165,14 +165,16 @@ static __global__ void __launch_bounds__(EVAL_THREADS) k_tile_eval(const FloodCt
             const FloodCtl c = ctl[r];
             const int i = int(pos & 0xffff) * TILE + col, j = int(pos >> 16) * TILE + row;
             if (item != begin) __syncthreads();           // the previous item is done with shared memory
-            if (staged != c.noise) {
+            // only the desert predicate batches exact searches; the others need no barrier unless the noise moved
+            const bool exact = c.pred == DSG_PRED_DESERT, stage = staged != c.noise;   // block-uniform
+            if (stage) {
                 const uint4 *src = reinterpret_cast<const uint4 *>(noise + c.noise);
                 uint4 *dst = reinterpret_cast<uint4 *>(&s_noise);
                 for (int k = threadIdx.x; k < int(sizeof(SeedNoise) / 16); k += blockDim.x) dst[k] = __ldg(src + k);
                 staged = c.noise;
             }
-            if (threadIdx.x == 0) s_n = 0;
-            __syncthreads();
+            if (exact && threadIdx.x == 0) s_n = 0;
+            if (stage || exact) __syncthreads();
             int v = 0, slot = -1;
             if (i < c.n && j < c.n) {
                 const int x = c.qx + (i - c.half) * c.step, z = c.qz + (j - c.half) * c.step;
@@ -182,10 +184,12 @@ static __global__ void __launch_bounds__(EVAL_THREADS) k_tile_eval(const FloodCt
                     if (v < 0) { slot = atomicAdd(&s_n, 1); s_pend[slot] = p; }
                 }
             }
-            __syncthreads();
-            if (int(threadIdx.x) < s_n) s_res[threadIdx.x] = int8_t(desert_state_finish(w, s_pend[threadIdx.x]));
-            __syncthreads();
-            if (slot >= 0) v = s_res[slot];
+            if (exact) {
+                __syncthreads();
+                if (int(threadIdx.x) < s_n) s_res[threadIdx.x] = int8_t(desert_state_finish(w, s_pend[threadIdx.x]));
+                __syncthreads();
+                if (slot >= 0) v = s_res[slot];
+            }
             const uint32_t pm = __ballot_sync(0xffffffffu, v > 0), dm = __ballot_sync(0xffffffffu, v == 2);
             if (lane == 0) {                              // lanes 0-15: row `row`, lanes 16-31: row + 1
                 uint16_t *b = reinterpret_cast<uint16_t *>(T.bits + size_t(t) * TILE_U64);
