@@ -122,20 +122,19 @@ def test_dsearch_matches_reference_gpu_searcher(tmp_path):
     # gpucheck: the FP64 proxy equals the CPU proxy on every checked cell
     for d, t in re.findall(r"gpucheck zone \d+x\d+: (\d+)/(\d+) cells differ", a.stderr):
         assert d == "0" and int(t) > 0
-    # proxy components and exact floods: the reference's proxy is FP32, ours FP64 (the CPU proxy's values),
-    # so component areas may differ by a few step-32 cells; exact flood areas from the same start agree
-    ca = list(csv.DictReader(open(tmp_path / "ours.csv")))
-    cb = list(csv.DictReader(open(tmp_path / "ref.csv")))
-    assert ca, "expected CSV rows for the verified finds"
-    idx = {(r["seed"], r["x"], r["z"]): r for r in cb}
-    same = [(r, idx[(r["seed"], r["x"], r["z"])]) for r in ca if (r["seed"], r["x"], r["z"]) in idx]
-    assert len(same) >= len(ca) // 2
-    for r, q in same:
-        assert abs(float(r["proxy"]) - float(q["proxy"])) <= 0.02 * max(1.0, float(q["proxy"]))
-        if float(r["s4"]) > 0 and float(q["s4"]) > 0:
-            assert r["s4"] == q["s4"] and r["s8"] == q["s8"]
+    # every file line for line on the first 48 finds (the production form: the device-resident search).  The
+    # reference's proxy is FP32 and ours FP64 (the CPU proxy's values); a component whose size sits on a cell
+    # where the two disagree could differ (1 row in 1,273 on 2^26 indices of the C2 stream), none does here
+    seeds = "".join(f"{f['seed']}\n" for f in finds()[:48])
+    a = run([os.path.join(BIN, "dsearch_desert"), "0", "0", str(tmp_path / "ours48"), "8"] + opts, stdin=seeds)
+    b = run([ref("dsearch_desert_gpu"), "0", "0", str(tmp_path / "ref48"), "8"] + opts, stdin=seeds)
+    assert a.returncode == 0, a.stderr[-2000:]
+    assert b.returncode == 0, b.stderr[-2000:]
+    for ext in (".csv", ".seeds.csv"):
+        la, lb = rd(str(tmp_path / "ours48") + ext), rd(str(tmp_path / "ref48") + ext)
+        assert len(la) > 40 and la == lb, (ext, sorted(set(la) ^ set(lb))[:6])
     cand = lambda s: sorted(re.findall(r"CANDIDATE step4=[\d.]+M seed=-?\d+ x=-?\d+ z=-?\d+", s))
-    assert set(cand(a.stderr)) >= set(cand(b.stderr)) or set(cand(a.stderr)) <= set(cand(b.stderr))
+    assert cand(a.stderr) == cand(b.stderr) and len(cand(a.stderr)) > 10
 
 
 @pytest.mark.parametrize("opts", [["hot_min=0"], ["hot_min=0", "study=1"], ["hot_min=0", "study=1", "multi=2"]],
