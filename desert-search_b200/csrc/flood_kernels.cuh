@@ -140,7 +140,7 @@ static __global__ void k_tile_start(const FloodCtl *__restrict__ ctl, const uint
 // cannot decide (about one in eight near desert edges) are gathered in shared memory and finished by the
 // first threads of the block, so the exact searches run in full warps instead of as one diverged lane per
 // warp.  Each evaluated sub-block marks its tile and queues it for this round's connect.
-static __global__ void __launch_bounds__(EVAL_THREADS) k_tile_eval(const FloodCtl *__restrict__ ctl, const SeedNoise *__restrict__ noise,
+static __global__ void __launch_bounds__(EVAL_THREADS, DSG_EVAL_MINB) k_tile_eval(const FloodCtl *__restrict__ ctl, const SeedNoise *__restrict__ noise,
                                                                    WorldDev w, Tiles T, Round q) {
     __shared__ SeedNoise s_noise;
     __shared__ PendingState s_pend[EVAL_THREADS];

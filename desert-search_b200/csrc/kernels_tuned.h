@@ -11,6 +11,9 @@
 #ifndef DSG_EVAL_BLOCKS
 #define DSG_EVAL_BLOCKS 0       // k_tile_eval: blocks per SM in a round's grid (0 = the occupancy limit)
 #endif
+#ifndef DSG_EVAL_MINB
+#define DSG_EVAL_MINB 4         // k_tile_eval: resident blocks per SM its register budget is cut for
+#endif
 #ifndef DSG_ZONE_CHUNK
 #define DSG_ZONE_CHUNK 2048     // proxy zone kernels: cells per block step
 #endif
