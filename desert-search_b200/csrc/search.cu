@@ -67,7 +67,7 @@ constexpr int RING = 289;                    // exact-start search points: rings
 
 // wave flags (ctr[C_FLAGS]): a set bit means the wave's results are incomplete
 enum : uint32_t { F_GATE = 1, F_RAW = 2, F_HASH = 4, F_ZONES = 8, F_CELLS = 16, F_EVALS = 32, F_POOL = 64, F_LOOP = 128, F_LABEL = 256,
-                  F_ROWS = 512 };
+                  F_ROWS = 512, F_SEEDS = 1024 /* more gated seeds than seeds_cap: the first seeds_cap are finished */ };
 // device counters
 enum { C_NS = 0, C_NREQ = 1 /* 4 flood phases */, C_ZONES = 5, C_CHUNKS = 6, C_ROWS = 7, C_FLAGS = 8, C_NHOT = 9, C_NBIG = 10, C_SITES = 11,
        C_ROUND = 16 /* 9 round counters */, C_TAKEN = 25, C_FERR = 26, C_BASE = 27, C_LOOPS = 28, C_ITERS = 29, C_PROXY = 32 /* 4 */,
@@ -99,7 +99,8 @@ __global__ void k_begin(const uint32_t *gcount, uint32_t cap1, uint32_t cap2, ui
     if (blockIdx.x == 0 && threadIdx.x == 0) {
         for (int k = 0; k < C_N; k++) if (k != C_TAKEN && k != C_BASE) ctr[k] = 0;
         ctr[C_NS] = nS;
-        if (gcount[0] > cap1 || gcount[1] > cap2 || n3 > cap3 || n3 > sc) ctr[C_FLAGS] |= F_GATE;
+        if (gcount[0] > cap1 || gcount[1] > cap2 || n3 > cap3) ctr[C_FLAGS] |= F_GATE;
+        else if (n3 > sc) ctr[C_FLAGS] |= F_SEEDS;
     }
     for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < nS; i += gridDim.x * blockDim.x) seeds[i] = surv[i];
 }
@@ -1254,15 +1255,25 @@ void collect_wave(Pipeline &p, Slot &S, Out &o) {
     o.tot[0] += S.indices; o.tot[1] += S.h_gcnt[0]; o.tot[2] += S.h_gcnt[1]; o.tot[3] += S.h_gcnt[2];
     o.tot[8] += S.h_ctr[C_ITERS];
     o.tot[9] += uint64_t(p.graph_kernels) + uint64_t(BODY_KERNELS) * S.h_ctr[C_ITERS] + (S.gated ? 4 + 2 : 0);   // + gate and its stamps
-    if (S.h_ctr[C_FLAGS]) {
-        o.tot[7] |= S.h_ctr[C_FLAGS];
-        if (S.h_ctr[C_FLAGS] & F_GATE) { set_error("device search: gate survivors exceed the wave's capacity"); throw ArgFail{}; }
-        DSG_CU(cudaMemcpy(S.h_seeds, S.seeds, size_t(wS) * 8, cudaMemcpyDeviceToHost));
-        for (uint32_t i = 0; i < wS; i++) {
-            if (o.nu < o.unf_cap) o.unf[o.nu] = S.h_seeds[i];
+    const uint32_t fl = S.h_ctr[C_FLAGS];
+    o.tot[7] |= fl;
+    if (fl & F_GATE) { set_error("device search: the gate's survivor lists overflowed"); throw ArgFail{}; }
+    auto hand_back = [&](const uint64_t *h, uint32_t n) {
+        for (uint32_t i = 0; i < n; i++) {
+            if (o.nu < o.unf_cap) o.unf[o.nu] = h[i];
             else o.over = true;
             o.nu++;
         }
+    };
+    if (fl & F_SEEDS) {                                   // gated seeds beyond the wave's capacity: back to the caller
+        const uint32_t n3 = S.h_gcnt[2], extra = n3 - wS;
+        std::vector<uint64_t> h(extra);
+        DSG_CU(cudaMemcpy(h.data(), gate::lane_survivors(S.lane) + wS, size_t(extra) * 8, cudaMemcpyDeviceToHost));
+        hand_back(h.data(), extra);
+    }
+    if (fl & ~F_SEEDS) {                                  // a stage's capacity: the wave's results are incomplete
+        DSG_CU(cudaMemcpy(S.h_seeds, S.seeds, size_t(wS) * 8, cudaMemcpyDeviceToHost));
+        hand_back(S.h_seeds, wS);
         return;
     }
     o.tot[4] += S.h_ctr[C_SITES]; o.tot[5] += S.h_ctr[C_NHOT]; o.tot[6] += S.h_ctr[C_NBIG];

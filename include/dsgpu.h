@@ -280,9 +280,10 @@ typedef struct dsg_search_params {
     double hot_min, hot_pre;                   /* big hot-zone area (M blocks^2, > 0) and pre-flood fraction (> 0) */
     double exact_min, refine_mb, csv_min;      /* proxy area for exact floods, step-8 area for step 4, CSV row cut */
     uint64_t wave;                             /* seed indices per wave (0 = 2^22, at most 2^26) */
-    uint32_t seeds_cap;                        /* gated seeds per wave (0 = 1,024, the most); the wave's zone, cell and
-                                                  flood-tile capacities scale with it (about 20 GB of device memory per
-                                                  wave in flight at 1,024; two waves are in flight) */
+    uint32_t seeds_cap;                        /* gated seeds per wave (0 = 1,024, the most; a wave of 2^22 indices
+                                                  gates about 330); the wave's zone, cell and flood-tile capacities scale
+                                                  with it (about 20 GB of device memory per wave in flight at 1,024; two
+                                                  waves are in flight).  Gated seeds beyond it are handed back */
     uint32_t flags;                            /* DSG_SEARCH_EAGER: no graph, the stages launched on a stream per wave
                                                   and the flood loops driven by the host, one wave at a time (for
                                                   profilers that cannot see the kernels of graphs with conditional
@@ -313,7 +314,8 @@ typedef struct dsg_search_row {
 int dsg_search_open(const dsg_search_params *p);
 /* Search seeds mix(start + k), k < count, wave by wave.  Gated seeds' records go to seeds_out (their rows to
  * rows_out, row0 re-based), in no particular order.  A wave that exceeds a fixed capacity of the pipeline
- * returns its gated seeds in `unfinished` instead: run them through the per-stage entry points.  counts =
+ * returns its gated seeds in `unfinished` instead, and a wave that gates more than seeds_cap seeds finishes the
+ * first seeds_cap and returns the rest there: run them through the per-stage entry points.  counts =
  * {indices, phase-passed, pre-gate passed, gated, sites, hot zones used, big zones, OR of wave flags, flood-loop
  * iterations, kernel launches (gate, graph nodes, loop bodies)};
  * device_ms (may be NULL) = CUDA-event time from the first wave's launch to the last wave's end.  DSG_OVERFLOW if

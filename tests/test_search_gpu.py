@@ -73,6 +73,33 @@ def test_search_run_covers_exactly_the_gate_survivors(dsg):
     assert all(r["row0"] + r["nrows"] <= len(rows) for r in recs)
 
 
+def test_gated_seeds_beyond_the_seed_capacity_are_handed_back(dsg):
+    """A pipeline opened for 64 gated seeds per wave, on waves of 2^22 indices (about 330 gated each): each wave
+    finishes its first 64 seeds and hands the rest back, and together they are exactly the gate's survivors; the
+    finished seeds' records equal those of a pipeline with room for all of them."""
+    start, count = 7 * 10**12, 1 << 23
+    dsg.scan_init_default()
+    dsg.search_open(seeds_cap=64)
+    try:
+        recs, rows, unf, counts, ms = dsg.search_run(start, count)
+    finally:
+        dsg.search_close()
+    surv, _, gc, rc = dsg.gate_run(start, count, batch=1 << 22)
+    assert rc == 0 and len(unf) > 0 and len(recs) == 2 * 64 and counts[7] == 1024, counts
+    assert np.array_equal(np.sort(np.concatenate([recs["seed"], unf])), np.sort(surv))
+    dsg.search_open()
+    try:
+        full, frows, funf, _, _ = dsg.search_run(start, count)
+    finally:
+        dsg.search_close()
+    assert len(funf) == 0
+    byseed = {int(r["seed"]): r for r in full}
+    for r in recs:
+        f = byseed[int(r["seed"])]
+        assert all(r[k] == f[k] for k in ("fya", "fyb", "maxta", "maxtb", "candidates", "sites", "best", "nrows"))
+        assert np.array_equal(rows[r["row0"]:r["row0"] + r["nrows"]], frows[f["row0"]:f["row0"] + f["nrows"]])
+
+
 def test_graph_and_stream_launched_waves_agree(dsg):
     """The wave graph (conditional WHILE nodes for the flood loops) and the same stages launched on a stream with
     the loops driven by the host (the profiling mode) give the same records and rows."""
