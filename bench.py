@@ -5,7 +5,7 @@ Workload (the batched full search): seeds mix(2*10^13 + k) through the productio
 `dsearch_desert START COUNT PREFIX THREADS gate=1 gpu=1 gscan=1` of deploy/gpipe.sh -- on the device-resident
 pipeline (dsg_search_run): GPU gate (y-phase <= 0.06, anti-aliased 256^2 pre-gate >= 0.645, 512^2 gate >= 0.70),
 period tables + blur, translation scan, bucket suppression, hot-zone floods, proxy bitmaps and components, exact
-step-8/step-4 floods.  One step = 2^24 seed indices (four waves of 2^22, each a gate launch and one CUDA graph);
+step-8/step-4 floods.  One step = 2^24 seed indices (two waves of 2^23, each a gate launch and one CUDA graph);
 the metric counts the seeds that pass the gate and are carried through every later stage (about 1 in 13,000).
 `value` = gated seeds / device time (CUDA events on the pipeline's stream); `e2e` = the same over the wall clock
 of the dsg_search_run calls, whose outputs (seed records and CSV rows) land in host memory.  Multi-GPU: one
@@ -529,7 +529,7 @@ def run_ours(args):
     elif args.eager:
         dsgpu.search_open(flags=dsgpu.SEARCH_EAGER)
     else:
-        dsgpu.search_open()
+        dsgpu.search_open(wave=1 << args.wave_log2)
     rep.barrier()
     clk = Clocks(local)
     ms, wall, tot, d2h = search_steps(dsgpu, base, args.steps, args.warmup, PER_STEP)
@@ -559,7 +559,7 @@ def run_ours(args):
         "dtype": "fp32 gate/tables/scan, fp64 floods/proxy", "data": "synthetic",
         "config": {"workload": "batched full search (production command line gate=1 gpu=1 gscan=1) over seeds mix(2e13 + k) on the "
                                "device-resident pipeline: gate, tables/blur, scan, suppression, hot-zone floods, proxy components, exact floods",
-                   "seeds_per_step": PER_STEP, "global_seeds": PER_STEP * args.steps * world, "waves_per_step": PER_STEP >> 22,
+                   "seeds_per_step": PER_STEP, "global_seeds": PER_STEP * args.steps * world, "waves_per_step": max(1, PER_STEP >> args.wave_log2), "wave": 1 << args.wave_log2,
                    "parallelism": f"replicas{world}",
                    "l2": "no input data (seeds generated on the device); each wave writes ~6 MiB of tables per gated seed (GBs per wave), "
                          "larger than L2"},
@@ -629,6 +629,7 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--per-step-log2", type=int, default=24, help="seed indices per step = 2^N")
+    ap.add_argument("--wave-log2", type=int, default=23, help="seed indices per wave of the device search = 2^N")
     ap.add_argument("--profile-run", action="store_true", help="device steps only (no e2e legs, no CPU baseline): for ncu captures")
     ap.add_argument("--small", action="store_true", help="pipeline opened with 128 seeds and 2^20 indices per wave (a few GB), stages "
                                                          "launched on a stream: for ncu captures; use with --per-step-log2 20")

@@ -1117,7 +1117,7 @@ extern "C" int dsg_search_open(const dsg_search_params *q) {
         P.max_sites = q->max_sites; P.nms = q->nms; P.exact_n = q->exact_n;
         P.hot_min = q->hot_min; P.hot_pre = q->hot_pre; P.exact_min = q->exact_min; P.refine_mb = q->refine_mb; P.csv_min = q->csv_min;
         p.gcfg = {q->gate_phase, q->gate_pthr, q->gate_amp, 0};
-        p.wave = q->wave ? q->wave : (uint64_t(1) << 22);
+        p.wave = q->wave ? q->wave : (uint64_t(1) << 23);    // about 630 gated seeds: 2^22 measured 2% slower, 2^21 6%
         DSG_ARG(p.wave <= (uint64_t(1) << 26), "dsg_search_open: wave above 2^26 seed indices");
         p.min_cells = 1;
         while (p.min_cells * 32.0 * 32 * 16 / 1e6 < 1) p.min_cells++;

@@ -279,9 +279,9 @@ typedef struct dsg_search_params {
     int32_t max_sites, nms, exact_n;           /* sites per seed (<= 300), suppression distance, exact floods per seed (<= 2) */
     double hot_min, hot_pre;                   /* big hot-zone area (M blocks^2, > 0) and pre-flood fraction (> 0) */
     double exact_min, refine_mb, csv_min;      /* proxy area for exact floods, step-8 area for step 4, CSV row cut */
-    uint64_t wave;                             /* seed indices per wave (0 = 2^22, at most 2^26) */
-    uint32_t seeds_cap;                        /* gated seeds per wave (0 = 1,024, the most; a wave of 2^22 indices
-                                                  gates about 330); the wave's zone, cell and flood-tile capacities scale
+    uint64_t wave;                             /* seed indices per wave (0 = 2^23, at most 2^26) */
+    uint32_t seeds_cap;                        /* gated seeds per wave (0 = 1,024, the most; a wave of 2^23 indices
+                                                  gates about 630); the wave's zone, cell and flood-tile capacities scale
                                                   with it (about 20 GB of device memory per wave in flight at 1,024; two
                                                   waves are in flight).  Gated seeds beyond it are handed back */
     uint32_t flags;                            /* DSG_SEARCH_EAGER: no graph, the stages launched on a stream per wave

@@ -79,7 +79,7 @@ def test_gated_seeds_beyond_the_seed_capacity_are_handed_back(dsg):
     finished seeds' records equal those of a pipeline with room for all of them."""
     start, count = 7 * 10**12, 1 << 23
     dsg.scan_init_default()
-    dsg.search_open(seeds_cap=64)
+    dsg.search_open(seeds_cap=64, wave=1 << 22)
     try:
         recs, rows, unf, counts, ms = dsg.search_run(start, count)
     finally:
