@@ -103,8 +103,8 @@ template <class Ex> DSG_HD void prefix_counts(const Ex &ex, uint16_t *pl, uint16
 }
 
 // std::sort(a, a + n, less) with the library's permutation; every thread of ex calls it (n <= 65535).  Returns
-// false, with a[] in an unspecified order, only for an inconsistent comparator (a partition without stoppers);
-// the caller then sorts again sequentially from its own copy.
+// false, with a[] in an unspecified order, only for an inconsistent comparator (a partition without stoppers,
+// e.g. NaN keys); a caller that may see such keys sorts them with stl_sort.h instead.
 template <class Ex, class T, class L> DSG_HD bool par_sort(const Ex &ex, T *a, int n, const L &less, const ParScratch &s) {
     if (n < 2) return true;
     int lg = 0;
