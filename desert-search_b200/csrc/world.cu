@@ -115,39 +115,66 @@ __device__ __forceinline__ void leaf_span(const LeafBox &l, const int64_t *A, co
         mn += uint64_t(d0 * d0); mx += uint64_t(d1 * d1);
     }
 }
-// One block per grid cell.  off == nullptr: count the candidates into cnt[cell]; else write them, in leaf
-// order, from cand[off[cell]].
-__global__ void __launch_bounds__(256) k_cand(const LeafBox *__restrict__ leaves, int nleaf, WorldDev w, uint32_t *__restrict__ cnt,
-                                              const uint32_t *__restrict__ off, uint16_t *__restrict__ cand) {
+// A grid over the five axes: cell (i_0 .. i_4), flat index ((i_0 d_1 + i_1) d_2 + ...) d_4 + i_4, covers
+// [cut[a][i_a], cut[a][i_a + 1]) on axis a.
+struct CandGrid { int32_t dim[5]; int32_t cut[5][48]; };
+__device__ __forceinline__ void cell_box(const CandGrid &g, uint32_t r, int64_t *A, int64_t *B, uint32_t *idx) {
+    for (int a = 4; a >= 0; a--) {
+        const uint32_t i = r % uint32_t(g.dim[a]);
+        r /= uint32_t(g.dim[a]);
+        idx[a] = i; A[a] = g.cut[a][i]; B[a] = int64_t(g.cut[a][i + 1]) - 1;
+    }
+}
+// One block per cell of g.  off == nullptr: count the candidates into cnt[cell]; else write them, in leaf order,
+// from cand[off[cell]] (leaf indices when leaf_index, tree nodes otherwise).  The leaves tested are all of them,
+// or (slist given) the list of the coarse cell of sg holding this one, every axis index halved: a leaf dropped
+// from a coarse cell drops from each cell inside it (its min-distance only grows and every max-distance only
+// shrinks), and the leaf of least max-distance of each depth interval in a cell is never dropped from the coarse
+// cell, so both give the same lists.
+__global__ void __launch_bounds__(256) k_cand(const LeafBox *__restrict__ leaves, int nleaf, CandGrid g, CandGrid sg,
+                                              const uint32_t *__restrict__ soff, const uint16_t *__restrict__ slist,
+                                              uint32_t *__restrict__ cnt, const uint32_t *__restrict__ off, uint16_t *__restrict__ cand,
+                                              bool leaf_index) {
     __shared__ unsigned long long s_m[kMaxDepthClasses];
     __shared__ uint32_t s_warp[8];
-    uint32_t r = blockIdx.x;
     int64_t A[5], B[5];
-    for (int a = 4; a >= 0; a--) {
-        const uint32_t i = r % uint32_t(w.cdim[a]);
-        r /= uint32_t(w.cdim[a]);
-        A[a] = w.ccut[a][i]; B[a] = int64_t(w.ccut[a][i + 1]) - 1;
+    uint32_t idx[5];
+    cell_box(g, blockIdx.x, A, B, idx);
+    const uint16_t *src = nullptr;
+    int n = nleaf;
+    if (slist) {
+        uint32_t sc = 0;
+        for (int a = 0; a < 5; a++) sc = sc * uint32_t(sg.dim[a]) + idx[a] / 2;
+        src = slist + soff[sc];
+        n = int(soff[sc + 1] - soff[sc]);
     }
     if (threadIdx.x < kMaxDepthClasses) s_m[threadIdx.x] = ~0ull;
     __syncthreads();
-    for (int k = threadIdx.x; k < nleaf; k += blockDim.x) {
+    for (int k = threadIdx.x; k < n; k += blockDim.x) {
+        const LeafBox &l = leaves[src ? src[k] : k];
         uint64_t mn, mx;
-        leaf_span(leaves[k], A, B, mn, mx);
-        atomicMin(&s_m[leaves[k].cls], mx);
+        leaf_span(l, A, B, mn, mx);
+        atomicMin(&s_m[l.cls], mx);
     }
     __syncthreads();
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     uint32_t base = off ? off[blockIdx.x] : 0;
-    for (int k0 = 0; k0 < nleaf; k0 += blockDim.x) {
+    for (int k0 = 0; k0 < n; k0 += blockDim.x) {
         const int k = k0 + threadIdx.x;
         bool keep = false;
-        if (k < nleaf) { uint64_t mn, mx; leaf_span(leaves[k], A, B, mn, mx); keep = mn <= s_m[leaves[k].cls]; }
+        int leaf = 0;
+        if (k < n) {
+            leaf = src ? src[k] : k;
+            uint64_t mn, mx;
+            leaf_span(leaves[leaf], A, B, mn, mx);
+            keep = mn <= s_m[leaves[leaf].cls];
+        }
         const uint32_t m = __ballot_sync(0xffffffffu, keep);
         if (lane == 0) s_warp[warp] = __popc(m);
         __syncthreads();
         uint32_t before = 0, total = 0;
         for (int q = 0; q < 8; q++) { if (q < warp) before += s_warp[q]; total += s_warp[q]; }
-        if (keep && off) cand[base + before + __popc(m & ((1u << lane) - 1))] = uint16_t(leaves[k].node);
+        if (keep && off) cand[base + before + __popc(m & ((1u << lane) - 1))] = uint16_t(leaf_index ? leaf : leaves[leaf].node);
         base += total;
         __syncthreads();
     }
@@ -314,29 +341,47 @@ void build_candidates(const Blob &b, WorldDev &w, cudaStream_t st) {
         leaves.push_back(l);
     }
     if (classes.size() > size_t(kMaxDepthClasses) || b.tree.size() > 0xffff) throw std::runtime_error("biome tree: too many depth intervals or nodes");
-    uint32_t ncell = 1;
-    for (int a = 0; a < 5; a++) ncell *= uint32_t(w.cdim[a]);
-    LeafBox *d_leaves = nullptr; uint32_t *d_cnt = nullptr, *d_off = nullptr; uint16_t *d_cand = nullptr, *d_leaf_of = nullptr, *d_n = nullptr;
-    try {
-        DSG_CU(cudaMallocAsync(reinterpret_cast<void **>(&d_leaves), leaves.size() * sizeof(LeafBox), st));
-        DSG_CU(cudaMemcpyAsync(d_leaves, leaves.data(), leaves.size() * sizeof(LeafBox), cudaMemcpyHostToDevice, st));
-        DSG_CU(cudaMallocAsync(reinterpret_cast<void **>(&d_cnt), size_t(ncell) * 4, st));
-        k_cand<<<ncell, 256, 0, st>>>(d_leaves, int(leaves.size()), w, d_cnt, nullptr, nullptr);
+    // the cell grid and the coarse grid of every second cut, whose lists (leaf indices) the cells start from
+    CandGrid g{}, sg{};
+    uint32_t ncell = 1, nsuper = 1;
+    for (int a = 0; a < 5; a++) {
+        g.dim[a] = w.cdim[a];
+        std::copy(w.ccut[a], w.ccut[a] + 48, g.cut[a]);
+        sg.dim[a] = (w.cdim[a] + 1) / 2;
+        for (int j = 0; j <= sg.dim[a]; j++) sg.cut[a][j] = w.ccut[a][std::min(2 * j, w.cdim[a])];
+        ncell *= uint32_t(g.dim[a]); nsuper *= uint32_t(sg.dim[a]);
+    }
+    LeafBox *d_leaves = nullptr; uint32_t *d_cnt = nullptr, *d_off = nullptr, *d_soff = nullptr; uint16_t *d_cand = nullptr, *d_leaf_of = nullptr,
+             *d_n = nullptr, *d_slist = nullptr;
+    // counts of one pass, then the offsets (host prefix sums) and the lists of a second pass
+    auto lists = [&](uint32_t cells, const CandGrid &grid, const uint32_t *soff, const uint16_t *slist, bool leaf_index, uint32_t *&off_out,
+                     uint16_t *&list_out) {
+        k_cand<<<cells, 256, 0, st>>>(d_leaves, int(leaves.size()), grid, sg, soff, slist, d_cnt, nullptr, nullptr, leaf_index);
         DSG_CU(cudaGetLastError());
-        std::vector<uint32_t> cnt(ncell), off(size_t(ncell) + 1, 0);
-        DSG_CU(cudaMemcpyAsync(cnt.data(), d_cnt, size_t(ncell) * 4, cudaMemcpyDeviceToHost, st));
+        std::vector<uint32_t> cnt(cells), off(size_t(cells) + 1, 0);
+        DSG_CU(cudaMemcpyAsync(cnt.data(), d_cnt, size_t(cells) * 4, cudaMemcpyDeviceToHost, st));
         DSG_CU(cudaStreamSynchronize(st));
         uint64_t total = 0;
-        for (uint32_t c = 0; c < ncell; c++) {
+        for (uint32_t c = 0; c < cells; c++) {
             total += cnt[c];
             if (total > (uint64_t(1) << 28)) throw std::runtime_error("candidate lists: more than 2^28 entries");
             off[c + 1] = uint32_t(total);
         }
-        DSG_CU(cudaMalloc(&d_off, off.size() * 4));
-        DSG_CU(cudaMemcpyAsync(d_off, off.data(), off.size() * 4, cudaMemcpyHostToDevice, st));
-        DSG_CU(cudaMalloc(&d_cand, size_t(off[ncell]) * 2 + 2));
-        k_cand<<<ncell, 256, 0, st>>>(d_leaves, int(leaves.size()), w, nullptr, d_off, d_cand);
+        DSG_CU(cudaMalloc(&off_out, off.size() * 4));
+        DSG_CU(cudaMemcpyAsync(off_out, off.data(), off.size() * 4, cudaMemcpyHostToDevice, st));
+        DSG_CU(cudaMalloc(&list_out, size_t(off[cells]) * 2 + 2));
+        k_cand<<<cells, 256, 0, st>>>(d_leaves, int(leaves.size()), grid, sg, soff, slist, nullptr, off_out, list_out, leaf_index);
         DSG_CU(cudaGetLastError());
+        DSG_CU(cudaStreamSynchronize(st));              // off: a host vector copied from above
+    };
+    try {
+        DSG_CU(cudaMallocAsync(reinterpret_cast<void **>(&d_leaves), leaves.size() * sizeof(LeafBox), st));
+        DSG_CU(cudaMemcpyAsync(d_leaves, leaves.data(), leaves.size() * sizeof(LeafBox), cudaMemcpyHostToDevice, st));
+        DSG_CU(cudaMallocAsync(reinterpret_cast<void **>(&d_cnt), size_t(std::max(ncell, nsuper)) * 4, st));
+        lists(nsuper, sg, nullptr, nullptr, true, d_soff, d_slist);          // coarse cells: all leaves tested
+        lists(ncell, g, d_soff, d_slist, false, d_off, d_cand);              // cells: their coarse cell's leaves
+        cudaFree(d_soff); d_soff = nullptr;
+        cudaFree(d_slist); d_slist = nullptr;
         std::vector<uint16_t> leaf_of(b.tree.size(), 0);
         for (size_t k = 0; k < leaves.size(); k++) leaf_of[leaves[k].node] = uint16_t(k);
         DSG_CU(cudaMallocAsync(reinterpret_cast<void **>(&d_leaf_of), leaf_of.size() * 2, st));
@@ -353,7 +398,7 @@ void build_candidates(const Blob &b, WorldDev &w, cudaStream_t st) {
         if (d_leaves) cudaFreeAsync(d_leaves, st);
         if (d_cnt) cudaFreeAsync(d_cnt, st);
         if (d_leaf_of) cudaFreeAsync(d_leaf_of, st);
-        cudaFree(d_off); cudaFree(d_cand); cudaFree(d_n);
+        cudaFree(d_off); cudaFree(d_cand); cudaFree(d_n); cudaFree(d_soff); cudaFree(d_slist);
         throw;
     }
     w.cand_off = d_off; w.cand = d_cand; w.cand_n = d_n;
