@@ -40,6 +40,11 @@ __global__ void __launch_bounds__(64) k_seed_noise(const uint64_t *__restrict__ 
         const int span = hi - lo + 1;
         S.factor[t] = (5. * span) / (3. * (span + 1));
     }
+    if (t < 48) {                                        // gradient h = t % 16: u (x or y) and v (y, x or z), signed by bits 0, 1
+        const int h = t & 15, c = t >> 4;
+        const int ui = h < 8 ? 0 : 1, vi = h < 4 ? 1 : ((h == 12 || h == 14) ? 0 : 2);
+        S.grad[c][h] = (ui == c ? ((h & 1) ? -1. : 1.) : 0.) + (vi == c ? ((h & 2) ? -1. : 1.) : 0.);
+    }
     if (t >= NOCT) return;
     int ch = 0;
     while (ch < 5 && t >= kOff[ch + 1]) ch++;

@@ -17,8 +17,11 @@ struct __align__(16) NOct { double ox, oy, oz, freq, amp, fy, vy; int32_t iy, pa
 // All noise of one seed: octave k of channel ch, side s is oct[off[ch] + s * cnt[ch] + k].  Each permutation
 // is stored twice over (perm[k][i] = perm[k][i & 255] for i < 512), so a lattice index masked once can be
 // offset by a hash and a corner step without masking again.
+// grad[c][h] is component c (x, y, z) of Minecraft's gradient h (0 or +-1), the same for every seed: kept with the
+// seed so that it sits in shared memory wherever the octaves do.
 struct __align__(16) SeedNoise {
     NOct oct[NOCT];
+    double grad[3][16];
     uint8_t perm[NOCT][512];
     double factor[6];
     int32_t off[6], cnt[6];
@@ -27,17 +30,17 @@ struct __align__(16) SeedNoise {
 #ifdef __CUDACC__
 __device__ __forceinline__ double fade_d(double t) { return t * t * t * (t * (t * 6. - 15.) + 10.); }
 __device__ __forceinline__ double lerp_d(double t, double a, double b) { return a + t * (b - a); }
-// gx*x + gy*y + gz*z of Minecraft's 16 gradients (components 0/+-1): the two nonzero terms with signs.  A
-// sign is applied by flipping the sign bit, which is what negation does.
-__device__ __forceinline__ double flip_sign(double v, int s) { return __hiloint2double(__double2hiint(v) ^ (s << 31), __double2loint(v)); }
-__device__ __forceinline__ double grad_d(int h, double x, double y, double z) {
+// The reference's grad(h, x, y, z) (standalone.hpp:62-83) is u + v, u and v two of +-x, +-y, +-z picked by h.
+// Here it is gx*x + gy*y + gz*z with G = SeedNoise::grad: each product is exactly +-x, +-y, +-z or a zero, so
+// the two fused multiply-adds round once, on u + v, and give the same double (a zero's sign aside; every sum
+// of octaves starts from +0, which drops it).  Three shared loads and three FP64 instructions replace the
+// integer selects and sign flips, the busiest pipe of the kernels that sample octaves.
+__device__ __forceinline__ double grad_d(const double (&G)[3][16], int h, double x, double y, double z) {
     h &= 15;
-    const double u = h < 8 ? x : y;
-    const double v = h < 4 ? y : ((h == 12 || h == 14) ? x : z);
-    return flip_sign(u, h & 1) + flip_sign(v, (h >> 1) & 1);
+    return fma(G[0][h], x, fma(G[1][h], y, G[2][h] * z));
 }
-// One Perlin octave (standalone.hpp:62-83); P is the doubled permutation of the octave.
-__device__ __forceinline__ double perlin(const NOct &o, const uint8_t *__restrict__ P, double x, double y, double z) {
+// One Perlin octave (standalone.hpp:62-83); P is the doubled permutation of the octave, G the gradients.
+__device__ __forceinline__ double perlin(const NOct &o, const uint8_t *__restrict__ P, const double (&G)[3][16], double x, double y, double z) {
     x += o.ox; z += o.oz;
     const double bx = floor(x), bz = floor(z);
     const int ix = int(bx) & 255, iz = int(bz) & 255;
@@ -48,10 +51,10 @@ __device__ __forceinline__ double perlin(const NOct &o, const uint8_t *__restric
     const int b00 = P[a0 + jy], b01 = P[a0 + jy + 1];
     const int b10 = P[a1 + jy], b11 = P[a1 + jy + 1];
     const double tx = fade_d(x), tz = fade_d(z);
-    const double lo = lerp_d(ty, lerp_d(tx, grad_d(P[b00 + iz], x, dy, z), grad_d(P[b10 + iz], x - 1, dy, z)),
-                                 lerp_d(tx, grad_d(P[b01 + iz], x, dy - 1, z), grad_d(P[b11 + iz], x - 1, dy - 1, z)));
-    const double hi = lerp_d(ty, lerp_d(tx, grad_d(P[b00 + iz + 1], x, dy, z - 1), grad_d(P[b10 + iz + 1], x - 1, dy, z - 1)),
-                                 lerp_d(tx, grad_d(P[b01 + iz + 1], x, dy - 1, z - 1), grad_d(P[b11 + iz + 1], x - 1, dy - 1, z - 1)));
+    const double lo = lerp_d(ty, lerp_d(tx, grad_d(G, P[b00 + iz], x, dy, z), grad_d(G, P[b10 + iz], x - 1, dy, z)),
+                                 lerp_d(tx, grad_d(G, P[b01 + iz], x, dy - 1, z), grad_d(G, P[b11 + iz], x - 1, dy - 1, z)));
+    const double hi = lerp_d(ty, lerp_d(tx, grad_d(G, P[b00 + iz + 1], x, dy, z - 1), grad_d(G, P[b10 + iz + 1], x - 1, dy, z - 1)),
+                                 lerp_d(tx, grad_d(G, P[b01 + iz + 1], x, dy - 1, z - 1), grad_d(G, P[b11 + iz + 1], x - 1, dy - 1, z - 1)));
     return lerp_d(tz, lo, hi);
 }
 // Two-sided channel value (standalone.hpp:140-151): per-side sums, side B at 337/331 scale.
@@ -60,13 +63,13 @@ __device__ __forceinline__ double channel(const SeedNoise &S, int ch, double x, 
     double a0 = 0, a1 = 0;
     for (int j = 0; j < cnt; j++) {
         const NOct &o = S.oct[off + j];
-        a0 += o.amp * perlin(o, S.perm[off + j], x * o.freq, y * o.freq, z * o.freq);
+        a0 += o.amp * perlin(o, S.perm[off + j], S.grad, x * o.freq, y * o.freq, z * o.freq);
     }
     const double s = 337. / 331.;
     const double px = x * s, py = y * s, pz = z * s;
     for (int j = 0; j < cnt; j++) {
         const NOct &o = S.oct[off + cnt + j];
-        a1 += o.amp * perlin(o, S.perm[off + cnt + j], px * o.freq, py * o.freq, pz * o.freq);
+        a1 += o.amp * perlin(o, S.perm[off + cnt + j], S.grad, px * o.freq, py * o.freq, pz * o.freq);
     }
     return (a0 + a1) * S.factor[ch];
 }
@@ -79,7 +82,7 @@ __device__ __forceinline__ double channel_low(const SeedNoise &S, int ch, double
         for (int k = lo; k < hi && k < cnt; k++) {
             const int i = off + side * cnt + k;
             const NOct &o = S.oct[i];
-            s += o.amp * perlin(o, S.perm[i], x * sc * o.freq, 0, z * sc * o.freq);
+            s += o.amp * perlin(o, S.perm[i], S.grad, x * sc * o.freq, 0, z * sc * o.freq);
         }
     }
     return s * S.factor[ch];

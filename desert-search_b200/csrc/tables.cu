@@ -273,7 +273,7 @@ __global__ void __launch_bounds__(256) k_tabins(const SeedNoise *__restrict__ no
         const double tx = fade_d(fx), tz = fade_d(fz), ty = p.vy;
         const int dx = c & 1, dy = (c >> 1) & 1, dz = c >> 2;
         const double wc = (dx ? tx : 1 - tx) * (dy ? ty : 1 - ty) * (dz ? tz : 1 - tz);
-        t.T[px][pz][c][h] = float(w * wc * grad_d(h, fx - dx, p.fy - dy, fz - dz));
+        t.T[px][pz][c][h] = float(w * wc * grad_d(S.grad, h, fx - dx, p.fy - dy, fz - dz));
     }
 }
 
