@@ -14,6 +14,9 @@
 #ifndef DSG_EVAL_MINB
 #define DSG_EVAL_MINB 4         // k_tile_eval: resident blocks per SM its register budget is cut for
 #endif
+#ifndef DSG_PROXY_MINB
+#define DSG_PROXY_MINB 4        // k_proxy: resident blocks per SM its register budget is cut for (1: no cut)
+#endif
 #ifndef DSG_ZONE_CHUNK
 #define DSG_ZONE_CHUNK 2048     // proxy zone kernels: cells per block step
 #endif

@@ -40,10 +40,16 @@ __global__ void __launch_bounds__(64) k_seed_noise(const uint64_t *__restrict__ 
         const int span = hi - lo + 1;
         S.factor[t] = (5. * span) / (3. * (span + 1));
     }
-    if (t < 48) {                                        // gradient h = t % 16: u (x or y) and v (y, x or z), signed by bits 0, 1
-        const int h = t & 15, c = t >> 4;
+    if (t < 16) {                                        // gradient h = t: u (x or y) and v (y, x or z), signed by bits 0, 1
+        const int h = t;
         const int ui = h < 8 ? 0 : 1, vi = h < 4 ? 1 : ((h == 12 || h == 14) ? 0 : 2);
-        S.grad[c][h] = (ui == c ? ((h & 1) ? -1. : 1.) : 0.) + (vi == c ? ((h & 2) ? -1. : 1.) : 0.);
+        uint64_t packed = 0;
+        for (int c = 0; c < 3; c++) {
+            const double g = (ui == c ? ((h & 1) ? -1. : 1.) : 0.) + (vi == c ? ((h & 2) ? -1. : 1.) : 0.);
+            const uint32_t hi = uint32_t(__double2hiint(g));            // low word and low half of the high word: 0
+            packed |= uint64_t(hi >> 16) << (8 + 16 * c);
+        }
+        S.grad[h] = make_uint2(uint32_t(packed), uint32_t(packed >> 32));
     }
     if (t >= NOCT) return;
     int ch = 0;

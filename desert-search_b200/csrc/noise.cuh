@@ -17,11 +17,12 @@ struct __align__(16) NOct { double ox, oy, oz, freq, amp, fy, vy; int32_t iy, pa
 // All noise of one seed: octave k of channel ch, side s is oct[off[ch] + s * cnt[ch] + k].  Each permutation
 // is stored twice over (perm[k][i] = perm[k][i & 255] for i < 512), so a lattice index masked once can be
 // offset by a hash and a corner step without masking again.
-// grad[c][h] is component c (x, y, z) of Minecraft's gradient h (0 or +-1), the same for every seed: kept with the
-// seed so that it sits in shared memory wherever the octaves do.
+// grad[h] holds Minecraft's gradient h (components 0 or +-1, the same for every seed; kept with the seed so that
+// it sits in shared memory wherever the octaves do) as the two upper bytes of each component's high word, the
+// only nonzero bytes of +-1.0 and 0.0: bytes 1-2 for x, 3-4 for y, 5-6 for z, bytes 0 and 7 zero.
 struct __align__(16) SeedNoise {
     NOct oct[NOCT];
-    double grad[3][16];
+    uint2 grad[16];
     uint8_t perm[NOCT][512];
     double factor[6];
     int32_t off[6], cnt[6];
@@ -31,16 +32,19 @@ struct __align__(16) SeedNoise {
 __device__ __forceinline__ double fade_d(double t) { return t * t * t * (t * (t * 6. - 15.) + 10.); }
 __device__ __forceinline__ double lerp_d(double t, double a, double b) { return a + t * (b - a); }
 // The reference's grad(h, x, y, z) (standalone.hpp:62-83) is u + v, u and v two of +-x, +-y, +-z picked by h.
-// Here it is gx*x + gy*y + gz*z with G = SeedNoise::grad: each product is exactly +-x, +-y, +-z or a zero, so
-// the two fused multiply-adds round once, on u + v, and give the same double (a zero's sign aside; every sum
-// of octaves starts from +0, which drops it).  Three shared loads and three FP64 instructions replace the
-// integer selects and sign flips, the busiest pipe of the kernels that sample octaves.
-__device__ __forceinline__ double grad_d(const double (&G)[3][16], int h, double x, double y, double z) {
-    h &= 15;
-    return fma(G[0][h], x, fma(G[1][h], y, G[2][h] * z));
+// Here it is gx*x + gy*y + gz*z with the components from G = SeedNoise::grad: each product is exactly +-x, +-y,
+// +-z or a zero, so the two fused multiply-adds round once, on u + v, and give the same double (a zero's sign
+// aside; every sum of octaves starts from +0, which drops it).  One 8-byte shared load and three byte permutes
+// rebuild the components; three FP64 instructions replace the integer selects and sign flips of u + v.
+__device__ __forceinline__ double grad_d(const uint2 *__restrict__ G, int h, double x, double y, double z) {
+    const uint2 g = G[h & 15];
+    const double gx = __hiloint2double(int(__byte_perm(g.x, g.y, 0x2100)), 0);
+    const double gy = __hiloint2double(int(__byte_perm(g.x, g.y, 0x4300)), 0);
+    const double gz = __hiloint2double(int(__byte_perm(g.x, g.y, 0x6500)), 0);
+    return fma(gx, x, fma(gy, y, gz * z));
 }
 // One Perlin octave (standalone.hpp:62-83); P is the doubled permutation of the octave, G the gradients.
-__device__ __forceinline__ double perlin(const NOct &o, const uint8_t *__restrict__ P, const double (&G)[3][16], double x, double y, double z) {
+__device__ __forceinline__ double perlin(const NOct &o, const uint8_t *__restrict__ P, const uint2 *__restrict__ G, double x, double y, double z) {
     x += o.ox; z += o.oz;
     const double bx = floor(x), bz = floor(z);
     const int ix = int(bx) & 255, iz = int(bz) & 255;

@@ -40,7 +40,7 @@ template <class F> __device__ __forceinline__ void each_chunk(const DZone *__res
     }
 }
 
-__global__ void __launch_bounds__(256) k_proxy(const SeedNoise *__restrict__ noise, const DZone *__restrict__ zones, WorldDev w, float cut,
+__global__ void __launch_bounds__(256, DSG_PROXY_MINB) k_proxy(const SeedNoise *__restrict__ noise, const DZone *__restrict__ zones, WorldDev w, float cut,
                                                uint8_t *__restrict__ out, ZoneWork wk) {
     __shared__ SeedNoise S;                               // the zone's seed: every Perlin lookup from shared memory
     int staged = -1;

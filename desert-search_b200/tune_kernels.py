@@ -6,6 +6,7 @@ Knobs (one varied at a time from the default build):
   DSG_EVAL_RUN     k_tile_eval: most consecutive sub-blocks a block takes from a round's queue at once
   DSG_EVAL_BLOCKS  k_tile_eval: blocks per SM of a round's grid (0 = the occupancy limit)
   DSG_EVAL_MINB    k_tile_eval: resident blocks per SM its register budget is cut for (4: 64 registers, 5: 48)
+  DSG_PROXY_MINB   k_proxy: resident blocks per SM its register budget is cut for (1: none; 4: 64 registers)
   DSG_ZONE_CHUNK   proxy bitmap and labelling kernels: cells per block step
 
 Two phases, so that the compiling happens off the GPU machine:
@@ -33,6 +34,7 @@ KNOBS = {                       # knob -> (candidate values, the first is the de
     "DSG_EVAL_RUN": ([16, 8, 32, 4], "flood"),
     "DSG_EVAL_BLOCKS": ([0, 4, 6, 8], "flood"),
     "DSG_EVAL_MINB": ([4, 5], "flood"),
+    "DSG_PROXY_MINB": ([4, 1], "proxy"),
     "DSG_ZONE_CHUNK": ([2048, 1024, 4096, 8192], "proxy"),
 }
 MIN_GAIN = 0.02
@@ -156,6 +158,7 @@ NOTES = {"DSG_TAB_WAVES": "k_tables: the fewest bands per table (1-8) giving at 
          "DSG_EVAL_RUN": "k_tile_eval: most consecutive sub-blocks a block takes from the round queue at once",
          "DSG_EVAL_BLOCKS": "k_tile_eval: blocks per SM in a round's grid (0 = the occupancy limit)",
          "DSG_EVAL_MINB": "k_tile_eval: resident blocks per SM its register budget is cut for",
+         "DSG_PROXY_MINB": "k_proxy: resident blocks per SM its register budget is cut for (1: no cut)",
          "DSG_ZONE_CHUNK": "proxy zone kernels: cells per block step"}
 
 
