@@ -412,7 +412,7 @@ def bench_floods(dsgpu, sm_mhz, sms, n_small=4096, n_large=4096, rates=(100.0, 5
     if EVAL_FP64_FLOPS_PER_CELL:
         ach = EVAL_FP64_FLOPS_PER_CELL * evaluated / t_batch
         batch["roofline"] = {"bound": "fp64", "kernel": "k_tile_eval", "achieved": ach / 1e12, "peak": peak / 1e12, "unit": "TFLOP/s",
-                             "frac": ach / peak, "note": "executed FP64 flops per evaluated cell (ncu) x cells evaluated / batch wall time; "
+                             "frac": ach / peak, "note": "FP64 flops per evaluated cell in the reference arithmetic (ncu count, one add per gradient) x cells evaluated / batch wall time; "
                                                          "peak = SMs x 64 FP64 FMA/clk x 2 at the sampled clock (nominal rate)"}
     out = {"batch": batch}
     # the reference's dflood on the host cores: a sample of small sites and large sites
