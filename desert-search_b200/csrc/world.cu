@@ -185,7 +185,11 @@ __global__ void __launch_bounds__(256) k_cand(const LeafBox *__restrict__ leaves
 // of (dist_L(v)^2 - dist_K(v)^2) is positive.  On one axis the difference is a piecewise polynomial of degree
 // at most two whose pieces meet at the intervals' ends, and on each piece it is linear, concave, or convex
 // with its vertex at a piece end, so the minimum over the integers of [A, B] is at A, B or an interval end
-// inside [A, B].  Each L is tested first against its class's leaf of least max-distance, then against all.
+// inside [A, B].  The squared distance is a sum over the axes, so the test is exact: K dominates L iff K is
+// nearer at every integer point of the cell, a strict order, hence transitive.  Each L is tested first against
+// its class's leaf of least max-distance (never dominated itself: a dominator has a smaller max-distance);
+// the survivors U are then tested against one another only: a leaf K that dominates L but fell in the first
+// test is dominated by the class's best leaf, which is in U and so dominates L as well.
 // Lists longer than kPruneMax keep the first pass's result.  Survivors keep their order; cnt[cell] = kept.
 constexpr int kPruneMax = 2048;
 __device__ __forceinline__ int64_t axis_min_diff(const LeafBox &L, const LeafBox &K, int a, int64_t A, int64_t B) {
@@ -208,9 +212,10 @@ __device__ __forceinline__ bool dominated_by(const LeafBox &L, const LeafBox &K,
 }
 __global__ void __launch_bounds__(256) k_cand_prune(const LeafBox *__restrict__ leaves, const uint16_t *__restrict__ leaf_of, WorldDev w,
                                                     const uint32_t *__restrict__ off, uint16_t *__restrict__ cand, uint16_t *__restrict__ cnt) {
-    __shared__ uint16_t s_id[kPruneMax];
+    __shared__ uint16_t s_id[kPruneMax], s_u[kPruneMax];
     __shared__ uint8_t s_keep[kPruneMax];
     __shared__ unsigned long long s_best[kMaxDepthClasses];
+    __shared__ uint32_t s_nu;
     uint32_t r = blockIdx.x;
     int64_t A[5], B[5];
     for (int a = 4; a >= 0; a--) {
@@ -240,13 +245,33 @@ __global__ void __launch_bounds__(256) k_cand_prune(const LeafBox *__restrict__ 
     for (uint32_t k = threadIdx.x; k < n; k += blockDim.x) {
         const LeafBox &L = leaves[s_id[k]];
         const uint32_t kb = uint32_t(s_best[L.cls] & 0xffff);
-        bool dom = kb != k && dominated_by(L, leaves[s_id[kb]], A, B);
-        for (uint32_t j = 0; j < n && !dom; j++) {
-            if (j == k) continue;
-            const LeafBox &K = leaves[s_id[j]];
+        s_keep[k] = !(kb != k && dominated_by(L, leaves[s_id[kb]], A, B));
+    }
+    __syncthreads();
+    if (threadIdx.x < 32) {                                    // U: the first test's survivors (first warp)
+        const int lane = threadIdx.x;
+        uint32_t nu = 0;
+        for (uint32_t k0 = 0; k0 < n; k0 += 32) {
+            const uint32_t k = k0 + lane;
+            const bool keep = k < n && s_keep[k];
+            const uint32_t m = __ballot_sync(0xffffffffu, keep);
+            if (keep) s_u[nu + __popc(m & ((1u << lane) - 1))] = uint16_t(k);
+            nu += __popc(m);
+        }
+        if (lane == 0) s_nu = nu;
+    }
+    __syncthreads();
+    const uint32_t nu = s_nu;
+    for (uint32_t q = threadIdx.x; q < nu; q += blockDim.x) {
+        const uint32_t k = s_u[q];
+        const LeafBox &L = leaves[s_id[k]];
+        bool dom = false;
+        for (uint32_t p = 0; p < nu && !dom; p++) {
+            if (p == q) continue;
+            const LeafBox &K = leaves[s_id[s_u[p]]];
             if (K.cls == L.cls && dominated_by(L, K, A, B)) dom = true;
         }
-        s_keep[k] = !dom;
+        if (dom) s_keep[k] = 0;                                // read again only after the barrier below
     }
     __syncthreads();
     if (threadIdx.x < 32) {                                    // in-order compaction by the first warp
