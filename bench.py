@@ -57,8 +57,8 @@ FP64_FLOPS_PER_CLK_PER_SM = 128  # 64 FP64 FMA lanes per SM (B200) x 2 flops
 PRE_DRAM_BYTES_PER_SEED = (150.5e6 + 6.1e6) / 241519
 # k_tile_eval FP64 work per evaluated cell: executed DADD + DMUL + 2 x DFMA (ncu counters over every k_tile_eval
 # launch) divided by the cells of the evaluated 16x16 sub-blocks, on exact step-1 floods of the 32 largest verified
-# finds (profiles/flood_eval_finds.md; 2,297 on step-8 floods of the 6 largest).  Counted with each gradient as one
-# DADD, the reference's arithmetic; the kernel now forms it as a DMUL and two DFMAs, which this count does not credit.
+# finds (2,297 on step-8 floods of the 6 largest).  Counted with each gradient as one DADD, the reference's
+# arithmetic; the kernel now forms it as a DMUL and two DFMAs, which this count does not credit.
 EVAL_FP64_FLOPS_PER_CELL = 2829
 
 
