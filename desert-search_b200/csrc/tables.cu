@@ -250,6 +250,14 @@ constexpr int SCAN_BLOCKS = 512;                    // CTAs per seed of k_scan
 // host (lowfield.hpp:14-33; octave 0 of each side of channels T, C, E, weight factor * amplitude).  Block =
 // (seed, table); thread x = permutation entry x, column-hash entries x of both y offsets, and corner terms
 // x and x + 256 in [px][pz][c][h] order.  The double-precision expressions are the host's, in its order.
+// The reference's gradient as it writes it, u + v with the signs chosen by h (standalone.hpp:62-83).  The corner
+// terms below are stored one by one, not summed from +0, so they follow that form to the sign of a zero.
+__device__ __forceinline__ double grad_uv(int h, double x, double y, double z) {
+    h &= 15;
+    const double u = h < 8 ? x : y;
+    const double v = h < 4 ? y : ((h == 12 || h == 14) ? x : z);
+    return ((h & 1) ? -u : u) + ((h & 2) ? -v : v);
+}
 __global__ void __launch_bounds__(256) k_tabins(const SeedNoise *__restrict__ noise, TabIn *__restrict__ out, const uint32_t *__restrict__ n_dev) {
     constexpr int CH[3] = {CH_T, CH_C, CH_E};
     const uint32_t s = blockIdx.x / 6, k = blockIdx.x % 6;
@@ -273,7 +281,7 @@ __global__ void __launch_bounds__(256) k_tabins(const SeedNoise *__restrict__ no
         const double tx = fade_d(fx), tz = fade_d(fz), ty = p.vy;
         const int dx = c & 1, dy = (c >> 1) & 1, dz = c >> 2;
         const double wc = (dx ? tx : 1 - tx) * (dy ? ty : 1 - ty) * (dz ? tz : 1 - tz);
-        t.T[px][pz][c][h] = float(w * wc * grad_d(S.grad, h, fx - dx, p.fy - dy, fz - dz));
+        t.T[px][pz][c][h] = float(w * wc * grad_uv(h, fx - dx, p.fy - dy, fz - dz));
     }
 }
 
