@@ -26,8 +26,10 @@ def test_default_kept_within_noise():
 
 
 def test_faster_values_chosen_per_knob():
-    c = tk.choose(rows({"DSG_EVAL_RUN=8": {"flood": 1.8}, "DSG_EVAL_RUN=32": {"flood": 1.7}, "DSG_TAB_WAVES=8": {"tables": 0.9}}))
+    c = tk.choose(rows({"DSG_EVAL_RUN=8": {"flood": 1.8}, "DSG_EVAL_RUN=32": {"flood": 1.7}, "DSG_TAB_WAVES=8": {"tables": 0.9},
+                        "DSG_PROXY_MINB=1": {"proxy": 0.45}}))
     assert c["DSG_EVAL_RUN"] == 32 and c["DSG_TAB_WAVES"] == 8 and c["DSG_ZONE_CHUNK"] == 2048 and c["DSG_EVAL_BLOCKS"] == 0
+    assert c["DSG_PROXY_MINB"] == 1                       # the proxy stage's two knobs are chosen independently
 
 
 def test_builds_with_other_outputs_never_chosen():
